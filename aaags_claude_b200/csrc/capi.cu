@@ -1,0 +1,978 @@
+// capi.cu -- the gs3dc_* C ABI (include/gs3d_cuda.h): context, device buffers,
+// stage entry points and the graph-replayed train step.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstddef>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "../../include/gs3d_cuda.h"
+#include "common.cuh"
+#include "kernels.cuh"
+
+using namespace gs3d;
+
+namespace {
+
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    cudaError_t ensure(size_t need) {
+        if (need <= n && p) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+        if (need == 0) return cudaSuccess;
+        cudaError_t e = cudaMalloc(&p, need * sizeof(T));
+        if (e == cudaSuccess) n = need;
+        else p = nullptr;
+        return e;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+};
+
+constexpr int kParamSlots = 4;  // pinned ring of per-step parameter blocks
+
+}  // namespace
+
+struct gs3dc_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+
+    // model (raw when model_raw, else activated)
+    int N = 0, sh_degree = 0, max_coeffs = 1;
+    bool have_model = false, model_raw = false;
+    DevBuf<float> pos, sc, rot, sh, op;
+    // Adam moments + stand-alone gradients
+    DevBuf<float> m_pos, v_pos, m_sc, v_sc, m_rot, v_rot, m_sh, v_sh, m_op, v_op;
+    DevBuf<float> g_pos, g_sc, g_rot, g_sh, g_op;
+    int adam_step = 0;
+    // screen-space records + optional cache
+    DevBuf<float4> rec0, rec1;
+    DevBuf<float> col_b, depth;
+    DevBuf<int> radius, tiles;
+    DevBuf<float> c_cov3D, c_pview, c_phw, c_cov2D, c_det;
+    // screen arrays in the reference layout (stage import / export)
+    DevBuf<float> x_means2D, x_depths, x_conics, x_opac, x_rgb;
+    DevBuf<int> x_radii, x_tiles;
+    // raster gradients
+    DevBuf<float> dm2, dcon, drgb, dop;
+    // pairs
+    DevBuf<unsigned long long> keys[2];
+    DevBuf<unsigned> vals[2];
+    unsigned long long cap = 0, min_cap = 0;
+    int sorted_which = 0;
+    DevBuf<unsigned long long> sort_desc;
+    unsigned long long sort_desc_stride = 0;
+    int sort_passes = 0, sort_num_tiles = 0;
+    // control block + preprocess scan descriptors (one memset)
+    DevBuf<unsigned char> ctrl_region;
+    Control* ctrl = nullptr;
+    unsigned long long* scan_desc = nullptr;
+    Control* ctrl_host = nullptr;  // pinned readback
+    // tiles / pixels
+    int W = 0, H = 0, num_tiles = 0;
+    DevBuf<unsigned> ranges;
+    DevBuf<float> image, T_final, d_image, gt;
+    DevBuf<int> n_contrib;
+    DevBuf<unsigned> last_j;
+    DevBuf<unsigned char> dsign;
+    // per-step parameters: device copy + pinned ring
+    StepParams* sp_dev = nullptr;
+    StepParams* sp_ring = nullptr;
+    cudaEvent_t sp_event[kParamSlots] = {};
+    int sp_slot = 0;
+    // stage state
+    bool have_screen = false, have_pairs = false, have_sorted = false, have_raster = false,
+         have_rgrad = false, have_grads = false;
+    // graph of the train step
+    bool use_graph = true;
+    cudaGraphExec_t graph = nullptr;
+    long long graph_key[8] = {};
+    long long graph_replays = 0;
+    long long graph_kernels = 0;
+    bool pending_check = false;
+    // options / stats
+    unsigned spin_limit = 1u << 22;
+    long long kernels_last = 0;
+    unsigned long long last_pairs = 0;
+};
+
+namespace {
+
+int fail(gs3dc_ctx* c, int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (c) c->err = buf;
+    return code;
+}
+
+#define CK(call)                                                                                  \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess) {                                                                  \
+            if (e_ == cudaErrorMemoryAllocation)                                                  \
+                return fail(c, GS3DC_ERR_OUT_OF_MEMORY, "%s: %s", #call, cudaGetErrorString(e_)); \
+            return fail(c, GS3DC_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_));              \
+        }                                                                                         \
+    } while (0)
+
+int bit_length(unsigned v) {
+    int b = 0;
+    while (v) {
+        b++;
+        v >>= 1;
+    }
+    return b;
+}
+
+// Key bits to sort: 32 depth bits + enough bits for tile ids < num_tiles.
+int sort_passes_for(int num_tiles) {
+    const int bits = 32 + bit_length(num_tiles > 1 ? (unsigned)(num_tiles - 1) : 0u);
+    return (bits + 7) / 8;
+}
+
+ModelPtrs model_ptrs(gs3dc_ctx* c) { return {c->pos.p, c->sc.p, c->rot.p, c->sh.p, c->op.p}; }
+AdamPtrs adam_ptrs(gs3dc_ctx* c) {
+    return {c->m_pos.p, c->v_pos.p, c->m_sc.p, c->v_sc.p, c->m_rot.p,
+            c->v_rot.p, c->m_sh.p,  c->v_sh.p,  c->m_op.p, c->v_op.p};
+}
+GradPtrs grad_ptrs(gs3dc_ctx* c) { return {c->g_pos.p, c->g_sc.p, c->g_rot.p, c->g_sh.p, c->g_op.p}; }
+RGradPtrs rgrad_ptrs(gs3dc_ctx* c) { return {c->dm2.p, c->dcon.p, c->drgb.p, c->dop.p}; }
+ScreenPtrs screen_ptrs(gs3dc_ctx* c, bool cache) {
+    ScreenPtrs s{c->rec0.p, c->rec1.p, c->col_b.p, c->depth.p, c->radius.p, c->tiles.p,
+                 nullptr, nullptr, nullptr, nullptr, nullptr};
+    if (cache) {
+        s.cov3D = c->c_cov3D.p;
+        s.p_view = c->c_pview.p;
+        s.p_hom_w = c->c_phw.p;
+        s.cov2D = c->c_cov2D.p;
+        s.det = c->c_det.p;
+    }
+    return s;
+}
+PixelPtrs pixel_ptrs(gs3dc_ctx* c) {
+    return {c->image.p, c->T_final.p, c->n_contrib.p, c->last_j.p, c->dsign.p, c->d_image.p};
+}
+
+int check_config(gs3dc_ctx* c, const gs3d_camera* cam, const gs3d_render_config* cfg) {
+    if (!cam || !cfg) return fail(c, GS3DC_ERR_INVALID_ARG, "camera and render config are required");
+    if (cam->width <= 0 || cam->height <= 0)
+        return fail(c, GS3DC_ERR_INVALID_ARG, "bad image size %dx%d", cam->width, cam->height);
+    if (cfg->tile_w != kTile || cfg->tile_h != kTile)
+        return fail(c, GS3DC_ERR_INVALID_ARG, "tile size %dx%d: this path is built for 16x16 tiles",
+                    cfg->tile_w, cfg->tile_h);
+    if (cfg->eval_3D)
+        return fail(c, GS3DC_ERR_INVALID_ARG, "eval_3D (3D Gaussian evaluation) is not on this path");
+    return GS3DC_OK;
+}
+
+// Control block + one look-back descriptor per 256-Gaussian CTA.
+int ensure_ctrl(gs3dc_ctx* c, int N) {
+    const size_t blocks = ((size_t)N + kBlock - 1) / kBlock;
+    const size_t head = ((sizeof(Control) + 255) / 256) * 256;
+    const size_t bytes = head + (blocks + 1) * sizeof(unsigned long long);
+    if (bytes > c->ctrl_region.n) {
+        CK(c->ctrl_region.ensure(bytes));
+        CK(cudaMemset(c->ctrl_region.p, 0, bytes));
+    }
+    c->ctrl = reinterpret_cast<Control*>(c->ctrl_region.p);
+    c->scan_desc = reinterpret_cast<unsigned long long*>(c->ctrl_region.p + head);
+    return GS3DC_OK;
+}
+
+// Per-Gaussian buffers for N Gaussians with mc SH bases.
+int ensure_model(gs3dc_ctx* c, int N, int mc) {
+    const size_t n = (size_t)N;
+    CK(c->pos.ensure(3 * n));
+    CK(c->sc.ensure(3 * n));
+    CK(c->rot.ensure(4 * n));
+    CK(c->sh.ensure(3 * n * mc));
+    CK(c->op.ensure(n));
+    CK(c->rec0.ensure(n));
+    CK(c->rec1.ensure(n));
+    CK(c->col_b.ensure(n));
+    CK(c->depth.ensure(n));
+    CK(c->radius.ensure(n));
+    CK(c->tiles.ensure(n));
+    CK(c->dm2.ensure(2 * n));
+    CK(c->dcon.ensure(3 * n));
+    CK(c->drgb.ensure(3 * n));
+    CK(c->dop.ensure(n));
+    return ensure_ctrl(c, N);
+}
+
+int ensure_adam(gs3dc_ctx* c) {
+    const size_t n = (size_t)c->N, mc3 = (size_t)c->max_coeffs * 3;
+    DevBuf<float>* bufs[10] = {&c->m_pos, &c->v_pos, &c->m_sc, &c->v_sc, &c->m_rot,
+                               &c->v_rot, &c->m_sh,  &c->v_sh,  &c->m_op, &c->v_op};
+    const size_t sizes[10] = {3 * n, 3 * n, 3 * n, 3 * n, 4 * n, 4 * n, mc3 * n, mc3 * n, n, n};
+    for (int k = 0; k < 10; k++) CK(bufs[k]->ensure(sizes[k]));
+    return GS3DC_OK;
+}
+
+int zero_adam(gs3dc_ctx* c) {
+    DevBuf<float>* bufs[10] = {&c->m_pos, &c->v_pos, &c->m_sc, &c->v_sc, &c->m_rot,
+                               &c->v_rot, &c->m_sh,  &c->v_sh,  &c->m_op, &c->v_op};
+    for (int k = 0; k < 10; k++)
+        if (bufs[k]->n) CK(cudaMemsetAsync(bufs[k]->p, 0, bufs[k]->n * sizeof(float), c->stream));
+    c->adam_step = 0;
+    return GS3DC_OK;
+}
+
+int ensure_cache(gs3dc_ctx* c) {
+    const size_t n = (size_t)c->N;
+    CK(c->c_cov3D.ensure(6 * n));
+    CK(c->c_pview.ensure(3 * n));
+    CK(c->c_phw.ensure(n));
+    CK(c->c_cov2D.ensure(3 * n));
+    CK(c->c_det.ensure(n));
+    return GS3DC_OK;
+}
+
+int ensure_pixels(gs3dc_ctx* c, int W, int H) {
+    const size_t np = (size_t)W * H;
+    const int gx = (W + kTile - 1) / kTile, gy = (H + kTile - 1) / kTile;
+    CK(c->ranges.ensure(2 * (size_t)gx * gy));
+    CK(c->image.ensure(3 * np));
+    CK(c->T_final.ensure(np));
+    CK(c->n_contrib.ensure(np));
+    CK(c->last_j.ensure(np));
+    CK(c->dsign.ensure(np));
+    c->W = W;
+    c->H = H;
+    c->num_tiles = gx * gy;
+    return GS3DC_OK;
+}
+
+// Pair buffers and sort descriptors for `cap` pairs and `num_tiles` tiles.
+int ensure_pairs(gs3dc_ctx* c, unsigned long long cap, int num_tiles) {
+    if (cap < 4096) cap = 4096;
+    if (cap > 0xFFFFFFFFull)
+        return fail(c, GS3DC_ERR_PAIR_OVERFLOW, "%llu tile pairs exceed the 32-bit tile-range format", cap);
+    if (cap > c->cap) {
+        for (int b = 0; b < 2; b++) {
+            CK(c->keys[b].ensure(cap));
+            CK(c->vals[b].ensure(cap));
+        }
+        c->cap = cap;
+    }
+    const int passes = sort_passes_for(num_tiles);
+    const unsigned long long stride = ((c->cap + kSortTile - 1) / kSortTile) * 256ull;
+    CK(c->sort_desc.ensure((size_t)(passes > 2 ? passes : 2) * stride));
+    c->sort_desc_stride = stride;
+    c->sort_passes = passes;
+    c->sort_num_tiles = num_tiles;
+    return GS3DC_OK;
+}
+
+// Fills the next pinned parameter slot and queues its copy to the device.
+int push_params(gs3dc_ctx* c, const gs3d_camera* cam, const gs3d_render_config* cfg, const gs3d_train_config* tc,
+                int iteration, const float* gt_dev) {
+    const int slot = c->sp_slot;
+    c->sp_slot = (c->sp_slot + 1) % kParamSlots;
+    CK(cudaEventSynchronize(c->sp_event[slot]));  // the slot's previous copy has been consumed
+    StepParams& p = c->sp_ring[slot];
+    std::memset(&p, 0, sizeof(p));
+    p.cam = *cam;
+    p.cfg = *cfg;
+    // preprocessor_cpu.cpp:50-53
+    p.focal_x = (float)cam->width / (2.0f * cam->tan_fovx);
+    p.focal_y = (float)cam->height / (2.0f * cam->tan_fovy);
+    p.grid_x = (cam->width + cfg->tile_w - 1) / cfg->tile_w;
+    p.grid_y = (cam->height + cfg->tile_h - 1) / cfg->tile_h;
+    p.num_tiles = p.grid_x * p.grid_y;
+    p.sh_deg_model = c->sh_degree;
+    p.sh_deg_fwd = cfg->sh_degree < c->sh_degree ? cfg->sh_degree : c->sh_degree;
+    p.max_coeffs = c->max_coeffs;
+    p.num_gaussians = c->N;
+    p.num_pixels = cam->width * cam->height;
+    p.inv_n = 1.0f / (float)(cam->width * cam->height * 3);  // loss.cpp:6
+    p.spin_limit = c->spin_limit;
+    p.sort_passes = sort_passes_for(p.num_tiles);
+    p.sort_bits = 32 + bit_length(p.num_tiles > 1 ? (unsigned)(p.num_tiles - 1) : 0u);
+    p.gt = gt_dev;
+    if (tc) {
+        p.use_adam = tc->use_adam ? 1 : 0;
+        // lr_schedule, train_types.cpp:64-68
+        float t = (float)iteration / (float)tc->max_steps;
+        t = std::max(0.0f, std::min(1.0f, t));
+        p.lr_pos = std::exp(std::log(tc->lr_position_init) * (1.0f - t) + std::log(tc->lr_position_final) * t);
+        p.lr_scale = tc->lr_scaling;
+        p.lr_rot = tc->lr_rotation;
+        p.lr_sh = tc->lr_feature;
+        p.lr_opac = tc->lr_opacity;
+        p.beta1 = tc->adam_beta1;
+        p.beta2 = tc->adam_beta2;
+        p.eps = tc->adam_eps;
+        // optimizer.cpp:75-76 (the step counter was advanced by the caller)
+        p.bc1 = 1.0f / (1.0f - std::pow(tc->adam_beta1, (float)c->adam_step));
+        p.bc2 = 1.0f / (1.0f - std::pow(tc->adam_beta2, (float)c->adam_step));
+    }
+    CK(cudaMemcpyAsync(c->sp_dev, &p, sizeof(StepParams), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaEventRecord(c->sp_event[slot], c->stream));
+    return GS3DC_OK;
+}
+
+// Reads the control block back and turns device status bits into a status.
+int read_control(gs3dc_ctx* c) {
+    CK(cudaMemcpyAsync(c->ctrl_host, c->ctrl, sizeof(Control), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->last_pairs = c->ctrl_host->total_pairs;
+    if (c->ctrl_host->status & kStatusTimeout)
+        return fail(c, GS3DC_ERR_DEVICE_TIMEOUT, "a device-side wait exceeded %u polls", c->spin_limit);
+    return GS3DC_OK;
+}
+
+// ---- launch sequences ----
+
+size_t ctrl_bytes_for(int N) {
+    return ((sizeof(Control) + 255) / 256) * 256 + (((size_t)N + kBlock - 1) / kBlock) * sizeof(unsigned long long);
+}
+
+int seq_preprocess(gs3dc_ctx* c, bool cache) {
+    CK(cudaMemsetAsync(c->ctrl_region.p, 0, ctrl_bytes_for(c->N), c->stream));
+    PairPtrs pr{c->keys[0].p, c->vals[0].p, c->cap, c->scan_desc};
+    CK(launch_preprocess_plain(c->stream, c->sp_dev, c->N, c->model_raw, cache, model_ptrs(c),
+                               screen_ptrs(c, cache), pr, c->ctrl));
+    c->kernels_last += c->N > 0 ? 1 : 0;
+    return GS3DC_OK;
+}
+
+int seq_sort(gs3dc_ctx* c) {
+    // sort scratch: tickets of the passes and the digit histograms
+    CK(cudaMemsetAsync(&c->ctrl->tickets[1], 0,
+                       sizeof(Control) - offsetof(Control, tickets) - sizeof(unsigned), c->stream));
+    CK(cudaMemsetAsync(c->sort_desc.p, 0, (size_t)c->sort_passes * c->sort_desc_stride * sizeof(unsigned long long),
+                       c->stream));
+    CK(cudaMemsetAsync(c->ranges.p, 0, 2 * (size_t)c->num_tiles * sizeof(unsigned), c->stream));
+    int which = 0;
+    CK(launch_radix_sort(c->stream, c->sp_dev, c->sort_passes, c->cap, c->keys[0].p, c->vals[0].p, c->keys[1].p,
+                         c->vals[1].p, c->sort_desc.p, c->sort_desc_stride, c->ctrl, &which));
+    c->sorted_which = which;
+    CK(launch_tile_ranges(c->stream, c->cap, c->keys[which].p, c->ranges.p, c->ctrl));
+    c->kernels_last += 2 + c->sort_passes;
+    return GS3DC_OK;
+}
+
+int seq_train(gs3dc_ctx* c) {
+    int rc = seq_preprocess(c, false);
+    if (rc) return rc;
+    rc = seq_sort(c);
+    if (rc) return rc;
+    const int w = c->sorted_which;
+    CK(launch_raster_fwd_plain(c->stream, c->sp_dev, c->num_tiles, true, c->ranges.p, c->vals[w].p,
+                               screen_ptrs(c, false), pixel_ptrs(c), c->ctrl));
+    CK(launch_raster_bwd_plain(c->stream, c->sp_dev, c->num_tiles, true, c->ranges.p, c->vals[w].p,
+                               screen_ptrs(c, false), pixel_ptrs(c), rgrad_ptrs(c), c->ctrl));
+    CK(launch_preprocess_bwd_plain(c->stream, c->sp_dev, c->N, true, model_ptrs(c), adam_ptrs(c),
+                                   screen_ptrs(c, false), rgrad_ptrs(c), grad_ptrs(c), c->ctrl));
+    c->kernels_last += 3;
+    return GS3DC_OK;
+}
+
+int require_model(gs3dc_ctx* c) {
+    if (!c->have_model) return fail(c, GS3DC_ERR_NO_MODEL, "no model uploaded");
+    return GS3DC_OK;
+}
+
+// Runs the preprocess, growing the pair capacity once if it overflowed.
+int run_preprocess(gs3dc_ctx* c, const gs3d_camera* cam, const gs3d_render_config* cfg, bool cache) {
+    int rc = ensure_pixels(c, cam->width, cam->height);
+    if (rc) return rc;
+    if (c->cap == 0 || c->sort_num_tiles != c->num_tiles) {
+        unsigned long long guess = c->min_cap ? c->min_cap : (unsigned long long)c->N * 8ull;
+        rc = ensure_pairs(c, guess > c->cap ? guess : c->cap, c->num_tiles);
+        if (rc) return rc;
+    }
+    if (cache && (rc = ensure_cache(c))) return rc;
+    for (int attempt = 0; attempt < 2; attempt++) {
+        c->kernels_last = 0;
+        rc = push_params(c, cam, cfg, nullptr, 0, nullptr);
+        if (rc) return rc;
+        rc = seq_preprocess(c, cache);
+        if (rc) return rc;
+        rc = read_control(c);
+        if (rc) return rc;
+        if (c->last_pairs <= c->cap) break;
+        rc = ensure_pairs(c, c->last_pairs + c->last_pairs / 4 + 4096, c->num_tiles);
+        if (rc) return rc;
+    }
+    c->have_screen = true;
+    c->have_pairs = true;
+    c->have_sorted = c->have_raster = c->have_rgrad = false;
+    return GS3DC_OK;
+}
+
+int download(gs3dc_ctx* c, void* host, const void* dev, size_t bytes) {
+    if (!host || bytes == 0) return GS3DC_OK;
+    CK(cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, c->stream));
+    return GS3DC_OK;
+}
+
+int upload_model_arrays(gs3dc_ctx* c, int N, int sh_degree, int mc, const float* p, const float* s, const float* r,
+                        const float* sh, const float* o) {
+    if (N < 0 || mc <= 0 || mc > 16 || sh_degree < 0 || sh_degree > 3 || (sh_degree + 1) * (sh_degree + 1) > mc)
+        return fail(c, GS3DC_ERR_INVALID_ARG, "bad model shape N=%d sh_degree=%d max_coeffs=%d", N, sh_degree, mc);
+    if (N > 0 && (!p || !s || !r || !sh || !o)) return fail(c, GS3DC_ERR_INVALID_ARG, "model arrays must be non-NULL");
+    if (c->graph && (c->N != N || c->max_coeffs != mc)) {
+        cudaGraphExecDestroy(c->graph);
+        c->graph = nullptr;
+    }
+    int rc = ensure_model(c, N, mc);
+    if (rc) return rc;
+    c->N = N;
+    c->sh_degree = sh_degree;
+    c->max_coeffs = mc;
+    const size_t n = (size_t)N;
+    if (N > 0) {
+        CK(cudaMemcpyAsync(c->pos.p, p, 3 * n * 4, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(c->sc.p, s, 3 * n * 4, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(c->rot.p, r, 4 * n * 4, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(c->sh.p, sh, 3 * n * mc * 4, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(c->op.p, o, n * 4, cudaMemcpyHostToDevice, c->stream));
+        // raster-gradient accumulators start at zero (the fused step re-zeroes them)
+        CK(cudaMemsetAsync(c->dm2.p, 0, 2 * n * 4, c->stream));
+        CK(cudaMemsetAsync(c->dcon.p, 0, 3 * n * 4, c->stream));
+        CK(cudaMemsetAsync(c->drgb.p, 0, 3 * n * 4, c->stream));
+        CK(cudaMemsetAsync(c->dop.p, 0, n * 4, c->stream));
+    }
+    c->have_model = true;
+    c->have_screen = c->have_pairs = c->have_sorted = c->have_raster = c->have_rgrad = c->have_grads = false;
+    return GS3DC_OK;
+}
+
+}  // namespace
+
+// ======================================================================
+extern "C" {
+
+const char* gs3dc_status_string(int s) {
+    switch (s) {
+        case GS3DC_OK: return "ok";
+        case GS3DC_ERR_INVALID_ARG: return "invalid argument";
+        case GS3DC_ERR_CUDA: return "CUDA error";
+        case GS3DC_ERR_PAIR_OVERFLOW: return "tile-pair capacity overflow";
+        case GS3DC_ERR_DEVICE_TIMEOUT: return "device-side wait timed out";
+        case GS3DC_ERR_NO_MODEL: return "no model uploaded";
+        case GS3DC_ERR_OUT_OF_MEMORY: return "out of device memory";
+        case GS3DC_ERR_STATE: return "stage called out of order";
+        default: return "unknown status";
+    }
+}
+
+const char* gs3dc_last_error(const gs3dc_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+int gs3dc_create(int device, gs3dc_ctx** out) {
+    if (!out) return GS3DC_ERR_INVALID_ARG;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) return GS3DC_ERR_CUDA;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return GS3DC_ERR_CUDA;
+    if (prop.major != 10) return GS3DC_ERR_CUDA;  // built for sm_100a only; no fallback path exists
+    gs3dc_ctx* c = new gs3dc_ctx();
+    c->device = device;
+    auto bail = [&](int code) {
+        gs3dc_destroy(c);
+        return code;
+    };
+    if (cudaSetDevice(device) != cudaSuccess) return bail(GS3DC_ERR_CUDA);
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(GS3DC_ERR_CUDA);
+    if (cudaMalloc(&c->sp_dev, sizeof(StepParams)) != cudaSuccess) return bail(GS3DC_ERR_OUT_OF_MEMORY);
+    if (cudaMallocHost(&c->sp_ring, kParamSlots * sizeof(StepParams)) != cudaSuccess) return bail(GS3DC_ERR_OUT_OF_MEMORY);
+    if (cudaMallocHost(&c->ctrl_host, sizeof(Control)) != cudaSuccess) return bail(GS3DC_ERR_OUT_OF_MEMORY);
+    for (int k = 0; k < kParamSlots; k++)
+        if (cudaEventCreateWithFlags(&c->sp_event[k], cudaEventDisableTiming) != cudaSuccess) return bail(GS3DC_ERR_CUDA);
+    if (ensure_model(c, 0, 1) != GS3DC_OK) return bail(GS3DC_ERR_OUT_OF_MEMORY);
+    *out = c;
+    return GS3DC_OK;
+}
+
+void gs3dc_destroy(gs3dc_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->graph) cudaGraphExecDestroy(c->graph);
+    DevBuf<float>* fb[] = {&c->pos,    &c->sc,      &c->rot,     &c->sh,     &c->op,      &c->m_pos,  &c->v_pos,
+                           &c->m_sc,   &c->v_sc,    &c->m_rot,   &c->v_rot,  &c->m_sh,    &c->v_sh,   &c->m_op,
+                           &c->v_op,   &c->g_pos,   &c->g_sc,    &c->g_rot,  &c->g_sh,    &c->g_op,   &c->col_b,
+                           &c->depth,  &c->c_cov3D, &c->c_pview, &c->c_phw,  &c->c_cov2D, &c->c_det,  &c->x_means2D,
+                           &c->x_depths, &c->x_conics, &c->x_opac, &c->x_rgb, &c->dm2,    &c->dcon,   &c->drgb,
+                           &c->dop,    &c->image,   &c->T_final, &c->d_image, &c->gt};
+    for (auto* b : fb) b->release();
+    c->rec0.release();
+    c->rec1.release();
+    c->radius.release();
+    c->tiles.release();
+    c->x_radii.release();
+    c->x_tiles.release();
+    c->n_contrib.release();
+    for (int b = 0; b < 2; b++) {
+        c->keys[b].release();
+        c->vals[b].release();
+    }
+    c->sort_desc.release();
+    c->ctrl_region.release();
+    c->ranges.release();
+    c->last_j.release();
+    c->dsign.release();
+    if (c->sp_dev) cudaFree(c->sp_dev);
+    if (c->sp_ring) cudaFreeHost(c->sp_ring);
+    if (c->ctrl_host) cudaFreeHost(c->ctrl_host);
+    for (int k = 0; k < kParamSlots; k++)
+        if (c->sp_event[k]) cudaEventDestroy(c->sp_event[k]);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+int gs3dc_get_stream(gs3dc_ctx* c, void** stream) {
+    if (!c || !stream) return GS3DC_ERR_INVALID_ARG;
+    *stream = (void*)c->stream;
+    return GS3DC_OK;
+}
+
+int gs3dc_set_option(gs3dc_ctx* c, int option, int64_t value) {
+    if (!c) return GS3DC_ERR_INVALID_ARG;
+    switch (option) {
+        case GS3DC_OPT_PAIR_CAPACITY:
+            if (value < 0) return fail(c, GS3DC_ERR_INVALID_ARG, "negative capacity");
+            c->min_cap = (unsigned long long)value;
+            return GS3DC_OK;
+        case GS3DC_OPT_USE_GRAPH:
+            c->use_graph = value != 0;
+            return GS3DC_OK;
+        case GS3DC_OPT_FORM:
+            if (value != GS3DC_FORM_PLAIN_FP32) return fail(c, GS3DC_ERR_INVALID_ARG, "unknown form %lld", (long long)value);
+            return GS3DC_OK;
+        case GS3DC_OPT_SPIN_LIMIT:
+            if (value <= 0) return fail(c, GS3DC_ERR_INVALID_ARG, "spin limit must be positive");
+            c->spin_limit = (unsigned)value;
+            if (c->graph) {
+                cudaGraphExecDestroy(c->graph);
+                c->graph = nullptr;
+            }
+            return GS3DC_OK;
+        default:
+            return fail(c, GS3DC_ERR_INVALID_ARG, "unknown option %d", option);
+    }
+}
+
+int gs3dc_get_stat(gs3dc_ctx* c, int stat, int64_t* value) {
+    if (!c || !value) return GS3DC_ERR_INVALID_ARG;
+    switch (stat) {
+        case GS3DC_STAT_TOTAL_PAIRS: *value = (int64_t)c->last_pairs; return GS3DC_OK;
+        case GS3DC_STAT_PAIR_CAPACITY: *value = (int64_t)c->cap; return GS3DC_OK;
+        case GS3DC_STAT_KERNELS_LAST: *value = c->kernels_last; return GS3DC_OK;
+        case GS3DC_STAT_SORT_PASSES: *value = c->sort_passes; return GS3DC_OK;
+        case GS3DC_STAT_GRAPH_REPLAYS: *value = c->graph_replays; return GS3DC_OK;
+        case GS3DC_STAT_ADAM_STEP: *value = c->adam_step; return GS3DC_OK;
+        default: return fail(c, GS3DC_ERR_INVALID_ARG, "unknown stat %d", stat);
+    }
+}
+
+int gs3dc_set_gaussians(gs3dc_ctx* c, const gs3d_gaussians* g) {
+    if (!c || !g) return GS3DC_ERR_INVALID_ARG;
+    CK(cudaSetDevice(c->device));
+    int rc = upload_model_arrays(c, g->count, g->sh_degree, g->max_coeffs, g->positions, g->scales, g->rotations,
+                                 g->sh_coeffs, g->opacities);
+    if (rc) return rc;
+    c->model_raw = false;
+    CK(cudaStreamSynchronize(c->stream));
+    return GS3DC_OK;
+}
+
+int gs3dc_set_raw_params(gs3dc_ctx* c, const gs3d_raw_params* r) {
+    if (!c || !r) return GS3DC_ERR_INVALID_ARG;
+    CK(cudaSetDevice(c->device));
+    int rc = upload_model_arrays(c, r->count, r->sh_degree, r->max_coeffs, r->raw_positions, r->raw_scales,
+                                 r->raw_rotations, r->raw_sh_coeffs, r->raw_opacities);
+    if (rc) return rc;
+    c->model_raw = true;
+    if ((rc = ensure_adam(c))) return rc;
+    if ((rc = zero_adam(c))) return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    return GS3DC_OK;
+}
+
+int gs3dc_get_raw_params(gs3dc_ctx* c, gs3d_raw_params* r) {
+    if (!c || !r) return GS3DC_ERR_INVALID_ARG;
+    int rc = require_model(c);
+    if (rc) return rc;
+    if (!c->model_raw) return fail(c, GS3DC_ERR_STATE, "the device model is an activated render model");
+    if (r->count != c->N || r->max_coeffs != c->max_coeffs)
+        return fail(c, GS3DC_ERR_INVALID_ARG, "host params have N=%d mc=%d, device N=%d mc=%d", r->count,
+                    r->max_coeffs, c->N, c->max_coeffs);
+    const size_t n = (size_t)c->N;
+    if ((rc = download(c, r->raw_positions, c->pos.p, 3 * n * 4))) return rc;
+    if ((rc = download(c, r->raw_scales, c->sc.p, 3 * n * 4))) return rc;
+    if ((rc = download(c, r->raw_rotations, c->rot.p, 4 * n * 4))) return rc;
+    if ((rc = download(c, r->raw_sh_coeffs, c->sh.p, 3 * n * c->max_coeffs * 4))) return rc;
+    if ((rc = download(c, r->raw_opacities, c->op.p, n * 4))) return rc;
+    return gs3dc_synchronize(c);
+}
+
+int gs3dc_preprocess(gs3dc_ctx* c, const gs3d_camera* cam, const gs3d_render_config* cfg,
+                     const gs3dc_screen_arrays* out) {
+    if (!c) return GS3DC_ERR_INVALID_ARG;
+    int rc;
+    if ((rc = check_config(c, cam, cfg)) || (rc = require_model(c))) return rc;
+    CK(cudaSetDevice(c->device));
+    const bool cache = out && (out->cov3D || out->p_view || out->p_hom_w || out->cov2D || out->cov2D_det);
+    if ((rc = run_preprocess(c, cam, cfg, cache))) return rc;
+    if (out) {
+        const size_t n = (size_t)c->N;
+        CK(c->x_means2D.ensure(2 * n));
+        CK(c->x_depths.ensure(n));
+        CK(c->x_conics.ensure(3 * n));
+        CK(c->x_opac.ensure(n));
+        CK(c->x_rgb.ensure(3 * n));
+        CK(c->x_radii.ensure(n));
+        CK(c->x_tiles.ensure(n));
+        ScreenArrays a{c->x_means2D.p, c->x_depths.p, c->x_conics.p, c->x_opac.p, c->x_rgb.p, c->x_radii.p, c->x_tiles.p};
+        CK(launch_export_screen(c->stream, c->N, screen_ptrs(c, false), a));
+        if ((rc = download(c, out->means2D, a.means2D, 2 * n * 4)) || (rc = download(c, out->depths, a.depths, n * 4)) ||
+            (rc = download(c, out->conics, a.conics, 3 * n * 4)) ||
+            (rc = download(c, out->opacities_2d, a.opac2d, n * 4)) || (rc = download(c, out->rgb, a.rgb, 3 * n * 4)) ||
+            (rc = download(c, out->radii, a.radii, n * 4)) || (rc = download(c, out->tiles_touched, a.tiles, n * 4)))
+            return rc;
+        if (cache) {
+            if ((rc = download(c, out->cov3D, c->c_cov3D.p, 6 * n * 4)) ||
+                (rc = download(c, out->p_view, c->c_pview.p, 3 * n * 4)) ||
+                (rc = download(c, out->p_hom_w, c->c_phw.p, n * 4)) ||
+                (rc = download(c, out->cov2D, c->c_cov2D.p, 3 * n * 4)) ||
+                (rc = download(c, out->cov2D_det, c->c_det.p, n * 4)))
+                return rc;
+        }
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    return GS3DC_OK;
+}
+
+int gs3dc_bin(gs3dc_ctx* c, int num_gaussians, const gs3dc_screen_arrays* in, const gs3d_camera* cam,
+              const gs3d_render_config* cfg, int64_t* total_pairs, uint64_t* keys_unsorted,
+              uint32_t* values_unsorted) {
+    if (!c) return GS3DC_ERR_INVALID_ARG;
+    int rc;
+    if ((rc = check_config(c, cam, cfg))) return rc;
+    CK(cudaSetDevice(c->device));
+    if (!in) {
+        if (!c->have_pairs) return fail(c, GS3DC_ERR_STATE, "gs3dc_bin without arrays needs gs3dc_preprocess first");
+    } else {
+        if (num_gaussians < 0) return fail(c, GS3DC_ERR_INVALID_ARG, "negative num_gaussians");
+        if (num_gaussians > 0 && (!in->means2D || !in->depths || !in->radii || !in->tiles_touched))
+            return fail(c, GS3DC_ERR_INVALID_ARG, "means2D, depths, radii and tiles_touched are required");
+        // the binned set replaces the device model's pairs; per-Gaussian records are not needed
+        const size_t n = (size_t)num_gaussians;
+        if ((rc = ensure_ctrl(c, num_gaussians))) return rc;
+        CK(c->x_means2D.ensure(2 * n));
+        CK(c->x_depths.ensure(n));
+        CK(c->x_radii.ensure(n));
+        CK(c->x_tiles.ensure(n));
+        if ((rc = ensure_pixels(c, cam->width, cam->height))) return rc;
+        if (n) {
+            CK(cudaMemcpyAsync(c->x_means2D.p, in->means2D, 2 * n * 4, cudaMemcpyHostToDevice, c->stream));
+            CK(cudaMemcpyAsync(c->x_depths.p, in->depths, n * 4, cudaMemcpyHostToDevice, c->stream));
+            CK(cudaMemcpyAsync(c->x_radii.p, in->radii, n * 4, cudaMemcpyHostToDevice, c->stream));
+            CK(cudaMemcpyAsync(c->x_tiles.p, in->tiles_touched, n * 4, cudaMemcpyHostToDevice, c->stream));
+        }
+        long long total = 0;
+        for (size_t i = 0; i < n; i++) total += in->tiles_touched[i];
+        if ((rc = ensure_pairs(c, (unsigned long long)total > c->cap ? (unsigned long long)total : c->cap, c->num_tiles)))
+            return rc;
+        if ((rc = push_params(c, cam, cfg, nullptr, 0, nullptr))) return rc;
+        CK(cudaMemsetAsync(c->ctrl_region.p, 0, ctrl_bytes_for(num_gaussians), c->stream));
+        if (total > 0) {
+            // unwritten slots (malformed tiles_touched) read as zero keys
+            CK(cudaMemsetAsync(c->keys[0].p, 0, (size_t)total * 8, c->stream));
+            CK(cudaMemsetAsync(c->vals[0].p, 0, (size_t)total * 4, c->stream));
+        }
+        ScreenArrays a{c->x_means2D.p, c->x_depths.p, nullptr, nullptr, nullptr, c->x_radii.p, c->x_tiles.p};
+        PairPtrs pr{c->keys[0].p, c->vals[0].p, c->cap, c->scan_desc};
+        CK(launch_bin_arrays(c->stream, c->sp_dev, num_gaussians, a, pr, c->ctrl));
+        if ((rc = read_control(c))) return rc;
+        c->have_pairs = true;
+        c->have_screen = false;  // the pairs no longer belong to the device model
+        c->have_sorted = c->have_raster = c->have_rgrad = false;
+    }
+    if (total_pairs) *total_pairs = (int64_t)c->last_pairs;
+    const size_t P = (size_t)c->last_pairs;
+    if ((rc = download(c, keys_unsorted, c->keys[0].p, P * 8))) return rc;
+    if ((rc = download(c, values_unsorted, c->vals[0].p, P * 4))) return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    return GS3DC_OK;
+}
+
+int gs3dc_sort(gs3dc_ctx* c, uint64_t* keys_sorted, uint32_t* values_sorted, uint32_t* tile_ranges) {
+    if (!c) return GS3DC_ERR_INVALID_ARG;
+    if (!c->have_pairs) return fail(c, GS3DC_ERR_STATE, "gs3dc_sort needs pairs (gs3dc_preprocess or gs3dc_bin)");
+    CK(cudaSetDevice(c->device));
+    c->kernels_last = 0;
+    int rc = seq_sort(c);
+    if (rc) return rc;
+    if ((rc = read_control(c))) return rc;
+    const size_t P = (size_t)c->last_pairs;
+    const int w = c->sorted_which;
+    if ((rc = download(c, keys_sorted, c->keys[w].p, P * 8)) || (rc = download(c, values_sorted, c->vals[w].p, P * 4)) ||
+        (rc = download(c, tile_ranges, c->ranges.p, 2 * (size_t)c->num_tiles * 4)))
+        return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    c->have_sorted = true;
+    return GS3DC_OK;
+}
+
+int gs3dc_sort_pairs(gs3dc_ctx* c, int64_t total_pairs, const uint64_t* keys, const uint32_t* values, int num_tiles,
+                     uint64_t* keys_sorted, uint32_t* values_sorted, uint32_t* tile_ranges) {
+    if (!c) return GS3DC_ERR_INVALID_ARG;
+    if (total_pairs < 0 || num_tiles <= 0 || (total_pairs > 0 && (!keys || !values)))
+        return fail(c, GS3DC_ERR_INVALID_ARG, "bad pair input (P=%lld, tiles=%d)", (long long)total_pairs, num_tiles);
+    CK(cudaSetDevice(c->device));
+    const size_t P = (size_t)total_pairs;
+    for (size_t i = 0; i < P; i++)
+        if ((keys[i] >> 32) >= (uint64_t)num_tiles)
+            return fail(c, GS3DC_ERR_INVALID_ARG, "key %zu has tile %llu >= num_tiles %d", i,
+                        (unsigned long long)(keys[i] >> 32), num_tiles);
+    int rc;
+    CK(c->ranges.ensure(2 * (size_t)num_tiles));
+    c->num_tiles = num_tiles;
+    if ((rc = ensure_pairs(c, P > c->cap ? P : c->cap, num_tiles))) return rc;
+    // the sort reads only spin_limit from the parameters
+    const int slot = c->sp_slot;
+    c->sp_slot = (c->sp_slot + 1) % kParamSlots;
+    CK(cudaEventSynchronize(c->sp_event[slot]));
+    std::memset(&c->sp_ring[slot], 0, sizeof(StepParams));
+    c->sp_ring[slot].spin_limit = c->spin_limit;
+    CK(cudaMemcpyAsync(c->sp_dev, &c->sp_ring[slot], sizeof(StepParams), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaEventRecord(c->sp_event[slot], c->stream));
+    CK(cudaMemsetAsync(c->ctrl_region.p, 0, sizeof(Control), c->stream));
+    unsigned long long P64 = (unsigned long long)P;
+    CK(cudaMemcpyAsync(&c->ctrl->total_pairs, &P64, 8, cudaMemcpyHostToDevice, c->stream));
+    if (P) {
+        CK(cudaMemcpyAsync(c->keys[0].p, keys, P * 8, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(c->vals[0].p, values, P * 4, cudaMemcpyHostToDevice, c->stream));
+    }
+    c->have_pairs = true;
+    c->have_screen = false;
+    CK(cudaStreamSynchronize(c->stream));
+    return gs3dc_sort(c, keys_sorted, values_sorted, tile_ranges);
+}
+
+int gs3dc_rasterize(gs3dc_ctx* c, const gs3d_camera* cam, const gs3d_render_config* cfg, float* image,
+                    float* T_final, int* n_contrib) {
+    if (!c) return GS3DC_ERR_INVALID_ARG;
+    int rc;
+    if ((rc = check_config(c, cam, cfg))) return rc;
+    if (!c->have_sorted || !c->have_screen)
+        return fail(c, GS3DC_ERR_STATE, "gs3dc_rasterize needs gs3dc_preprocess and gs3dc_sort of the model");
+    if (cam->width != c->W || cam->height != c->H)
+        return fail(c, GS3DC_ERR_INVALID_ARG, "camera size differs from the preprocessed one");
+    CK(cudaSetDevice(c->device));
+    if ((rc = push_params(c, cam, cfg, nullptr, 0, nullptr))) return rc;
+    const int w = c->sorted_which;
+    CK(launch_raster_fwd_plain(c->stream, c->sp_dev, c->num_tiles, false, c->ranges.p, c->vals[w].p,
+                               screen_ptrs(c, false), pixel_ptrs(c), c->ctrl));
+    const size_t np = (size_t)c->W * c->H;
+    if ((rc = download(c, image, c->image.p, 3 * np * 4)) || (rc = download(c, T_final, c->T_final.p, np * 4)) ||
+        (rc = download(c, n_contrib, c->n_contrib.p, np * 4)))
+        return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    c->have_raster = true;
+    return GS3DC_OK;
+}
+
+int gs3dc_render(gs3dc_ctx* c, const gs3d_gaussians* g, const gs3d_camera* cam, const gs3d_render_config* cfg,
+                 float* image) {
+    if (!c) return GS3DC_ERR_INVALID_ARG;
+    int rc;
+    if ((rc = check_config(c, cam, cfg))) return rc;
+    if (g && (rc = gs3dc_set_gaussians(c, g))) return rc;
+    if ((rc = require_model(c))) return rc;
+    if ((rc = gs3dc_preprocess(c, cam, cfg, nullptr))) return rc;
+    long long k0 = c->kernels_last;
+    if ((rc = gs3dc_sort(c, nullptr, nullptr, nullptr))) return rc;
+    k0 += c->kernels_last;
+    if ((rc = gs3dc_rasterize(c, cam, cfg, image, nullptr, nullptr))) return rc;
+    c->kernels_last = k0 + 1;
+    return GS3DC_OK;
+}
+
+int gs3dc_raster_backward(gs3dc_ctx* c, const gs3d_camera* cam, const gs3d_render_config* cfg, const float* d_image,
+                          float* d_means2D, float* d_conics, float* d_rgb, float* d_opacities_2d) {
+    if (!c || !d_image) return GS3DC_ERR_INVALID_ARG;
+    int rc;
+    if ((rc = check_config(c, cam, cfg))) return rc;
+    if (!c->have_raster) return fail(c, GS3DC_ERR_STATE, "gs3dc_raster_backward needs gs3dc_rasterize first");
+    CK(cudaSetDevice(c->device));
+    const size_t np = (size_t)c->W * c->H, n = (size_t)c->N;
+    CK(c->d_image.ensure(3 * np));
+    CK(cudaMemcpyAsync(c->d_image.p, d_image, 3 * np * 4, cudaMemcpyHostToDevice, c->stream));
+    if ((rc = push_params(c, cam, cfg, nullptr, 0, nullptr))) return rc;
+    CK(cudaMemsetAsync(c->dm2.p, 0, 2 * n * 4, c->stream));
+    CK(cudaMemsetAsync(c->dcon.p, 0, 3 * n * 4, c->stream));
+    CK(cudaMemsetAsync(c->drgb.p, 0, 3 * n * 4, c->stream));
+    CK(cudaMemsetAsync(c->dop.p, 0, n * 4, c->stream));
+    const int w = c->sorted_which;
+    CK(launch_raster_bwd_plain(c->stream, c->sp_dev, c->num_tiles, false, c->ranges.p, c->vals[w].p,
+                               screen_ptrs(c, false), pixel_ptrs(c), rgrad_ptrs(c), c->ctrl));
+    if ((rc = download(c, d_means2D, c->dm2.p, 2 * n * 4)) || (rc = download(c, d_conics, c->dcon.p, 3 * n * 4)) ||
+        (rc = download(c, d_rgb, c->drgb.p, 3 * n * 4)) || (rc = download(c, d_opacities_2d, c->dop.p, n * 4)))
+        return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    c->have_rgrad = true;
+    return GS3DC_OK;
+}
+
+int gs3dc_preprocess_backward(gs3dc_ctx* c, const gs3d_camera* cam, const gs3d_render_config* cfg,
+                              float* d_raw_positions, float* d_raw_scales, float* d_raw_rotations,
+                              float* d_raw_sh_coeffs, float* d_raw_opacities) {
+    if (!c) return GS3DC_ERR_INVALID_ARG;
+    int rc;
+    if ((rc = check_config(c, cam, cfg))) return rc;
+    if (!c->have_rgrad) return fail(c, GS3DC_ERR_STATE, "gs3dc_preprocess_backward needs gs3dc_raster_backward");
+    if (!c->model_raw) return fail(c, GS3DC_ERR_STATE, "gradients are taken w.r.t. a raw model (gs3dc_set_raw_params)");
+    CK(cudaSetDevice(c->device));
+    const size_t n = (size_t)c->N, mc3 = (size_t)c->max_coeffs * 3;
+    CK(c->g_pos.ensure(3 * n));
+    CK(c->g_sc.ensure(3 * n));
+    CK(c->g_rot.ensure(4 * n));
+    CK(c->g_sh.ensure(mc3 * n));
+    CK(c->g_op.ensure(n));
+    if ((rc = push_params(c, cam, cfg, nullptr, 0, nullptr))) return rc;
+    CK(launch_preprocess_bwd_plain(c->stream, c->sp_dev, c->N, false, model_ptrs(c), adam_ptrs(c),
+                                   screen_ptrs(c, false), rgrad_ptrs(c), grad_ptrs(c), c->ctrl));
+    if ((rc = download(c, d_raw_positions, c->g_pos.p, 3 * n * 4)) ||
+        (rc = download(c, d_raw_scales, c->g_sc.p, 3 * n * 4)) ||
+        (rc = download(c, d_raw_rotations, c->g_rot.p, 4 * n * 4)) ||
+        (rc = download(c, d_raw_sh_coeffs, c->g_sh.p, mc3 * n * 4)) ||
+        (rc = download(c, d_raw_opacities, c->g_op.p, n * 4)))
+        return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    c->have_grads = true;
+    return GS3DC_OK;
+}
+
+int gs3dc_optimizer_step(gs3dc_ctx* c, const gs3d_train_config* tc, int iteration) {
+    if (!c || !tc) return GS3DC_ERR_INVALID_ARG;
+    if (!c->have_grads) return fail(c, GS3DC_ERR_STATE, "gs3dc_optimizer_step needs gs3dc_preprocess_backward");
+    CK(cudaSetDevice(c->device));
+    int rc;
+    if ((rc = ensure_adam(c))) return rc;
+    if (tc->use_adam) c->adam_step++;
+    gs3d_camera cam{};
+    cam.width = c->W > 0 ? c->W : 1;
+    cam.height = c->H > 0 ? c->H : 1;
+    cam.tan_fovx = cam.tan_fovy = 1.0f;
+    gs3d_render_config cfg{};
+    cfg.tile_w = cfg.tile_h = kTile;
+    cfg.scale_modifier = 1.0f;
+    if ((rc = push_params(c, &cam, &cfg, tc, iteration, nullptr))) return rc;
+    CK(launch_optimizer_plain(c->stream, c->sp_dev, c->N, c->max_coeffs * 3, model_ptrs(c), adam_ptrs(c), grad_ptrs(c)));
+    CK(cudaStreamSynchronize(c->stream));
+    c->have_screen = c->have_pairs = c->have_sorted = c->have_raster = c->have_rgrad = c->have_grads = false;
+    return GS3DC_OK;
+}
+
+int gs3dc_synchronize(gs3dc_ctx* c) {
+    if (!c) return GS3DC_ERR_INVALID_ARG;
+    CK(cudaSetDevice(c->device));
+    int rc = read_control(c);
+    if (rc) return rc;
+    if (c->pending_check && (c->ctrl_host->status & kStatusOverflow)) {
+        c->pending_check = false;
+        return fail(c, GS3DC_ERR_PAIR_OVERFLOW,
+                    "a train step found %llu tile pairs for a capacity of %llu and was skipped",
+                    (unsigned long long)c->ctrl_host->total_pairs, c->cap);
+    }
+    c->pending_check = false;
+    return GS3DC_OK;
+}
+
+int gs3dc_train_step(gs3dc_ctx* c, const gs3d_camera* cam, const float* gt, int gt_on_device,
+                     const gs3d_render_config* cfg, const gs3d_train_config* tc, int iteration, float* loss) {
+    if (!c || !gt || !tc) return GS3DC_ERR_INVALID_ARG;
+    int rc;
+    if ((rc = check_config(c, cam, cfg)) || (rc = require_model(c))) return rc;
+    if (!c->model_raw) return fail(c, GS3DC_ERR_STATE, "gs3dc_train_step needs a raw model (gs3dc_set_raw_params)");
+    CK(cudaSetDevice(c->device));
+    if ((rc = ensure_adam(c))) return rc;
+    if ((rc = ensure_pixels(c, cam->width, cam->height))) return rc;
+    const size_t np = (size_t)cam->width * cam->height;
+    const float* gt_dev = gt;
+    if (!gt_on_device) {
+        CK(c->gt.ensure(3 * np));
+        CK(cudaMemcpyAsync(c->gt.p, gt, 3 * np * 4, cudaMemcpyHostToDevice, c->stream));
+        gt_dev = c->gt.p;
+    }
+    bool first = c->cap == 0 || c->sort_num_tiles != c->num_tiles;
+    if (first) {
+        unsigned long long guess = c->min_cap ? c->min_cap : (unsigned long long)c->N * 8ull;
+        if ((rc = ensure_pairs(c, guess > c->cap ? guess : c->cap, c->num_tiles))) return rc;
+    }
+    const int step_before = c->adam_step;
+    for (int attempt = 0; attempt < 3; attempt++) {
+        c->adam_step = step_before + (tc->use_adam ? 1 : 0);
+        if ((rc = push_params(c, cam, cfg, tc, iteration, gt_dev))) return rc;
+        const long long key[8] = {c->N, c->max_coeffs, cam->width, cam->height, (long long)c->cap, c->sort_passes,
+                                  (long long)c->spin_limit, 1};
+        const bool key_ok = c->graph && std::memcmp(key, c->graph_key, sizeof(key)) == 0;
+        c->kernels_last = 0;
+        if (c->use_graph && !first && attempt == 0) {
+            if (!key_ok) {
+                if (c->graph) {
+                    cudaGraphExecDestroy(c->graph);
+                    c->graph = nullptr;
+                }
+                cudaGraph_t g;
+                CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+                rc = seq_train(c);
+                cudaError_t ec = cudaStreamEndCapture(c->stream, &g);
+                if (rc) return rc;
+                CK(ec);
+                CK(cudaGraphInstantiate(&c->graph, g, 0));
+                cudaGraphDestroy(g);
+                std::memcpy(c->graph_key, key, sizeof(key));
+                c->graph_kernels = c->kernels_last;
+            }
+            c->kernels_last = c->graph_kernels;
+            CK(cudaGraphLaunch(c->graph, c->stream));
+            c->graph_replays++;
+        } else {
+            if ((rc = seq_train(c))) return rc;
+        }
+        if (!loss && !first) {
+            c->pending_check = true;  // overflow is reported by the next synchronising call
+            return GS3DC_OK;
+        }
+        if ((rc = read_control(c))) {
+            c->adam_step = step_before;
+            return rc;
+        }
+        if (c->ctrl_host->status & kStatusOverflow) {
+            // nothing was updated: the backward and the optimiser skip overflowed steps
+            c->adam_step = step_before;
+            const unsigned long long P = c->ctrl_host->total_pairs;
+            if ((rc = ensure_pairs(c, P + P / 2 + 4096, c->num_tiles))) return rc;
+            first = true;
+            continue;
+        }
+        if (loss) *loss = (float)(c->ctrl_host->loss_sum / (double)(3.0 * (double)np));
+        return GS3DC_OK;
+    }
+    c->adam_step = step_before;
+    return fail(c, GS3DC_ERR_PAIR_OVERFLOW, "tile-pair capacity kept overflowing");
+}
+
+}  // extern "C"

@@ -1,0 +1,144 @@
+// common.cuh -- device-side shared definitions of the 3DGS hot path.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/gs3d_types.h"
+
+namespace gs3d {
+
+constexpr int kTile = 16;            // 16x16 pixel tiles (RenderConfig default, include/types.h:64-65)
+constexpr int kBlock = 256;          // threads per CTA of the per-Gaussian and per-tile kernels
+constexpr int kMaxPasses = 8;        // radix passes (8-bit digits over <= 64 key bits)
+
+// Device-status bits (Control::status).
+constexpr unsigned kStatusOverflow = 1u;  // more tile pairs than capacity
+constexpr unsigned kStatusTimeout = 2u;   // a bounded device-side wait gave up
+
+// Per-step parameters, resident in device memory so that a captured graph
+// reads fresh camera / learning-rate values on every replay.
+struct StepParams {
+    gs3d_camera cam;
+    gs3d_render_config cfg;
+    float focal_x, focal_y;
+    int grid_x, grid_y, num_tiles;
+    int sh_deg_fwd;       // min(cfg.sh_degree, model degree): forward SH degree
+    int sh_deg_model;     // model degree: the backward's SH degree (preprocessor_backward_cpu.cpp:213)
+    int max_coeffs;
+    int num_gaussians;
+    int num_pixels;
+    float inv_n;          // 1.0f / (H*W*3)  (loss.cpp:6)
+    // optimiser
+    int use_adam;
+    float lr_pos, lr_scale, lr_rot, lr_sh, lr_opac;
+    float beta1, beta2, eps, bc1, bc2;
+    // radix sort
+    int sort_bits;        // significant key bits (32 + tile bits)
+    int sort_passes;
+    unsigned spin_limit;  // bounded waits
+    const float* gt;      // [H*W*3] device target of the fused L1 (read per replay)
+};
+
+// Small device control block, zeroed by one memset at the start of a step.
+struct Control {
+    unsigned long long total_pairs;   // written by the last preprocess / bin block
+    unsigned status;                  // kStatus* bits
+    unsigned tickets[16];             // dynamic CTA tickets (0: preprocess/bin, 1..8: sort passes)
+    unsigned pad_;
+    double loss_sum;                  // sum |image - gt| of the fused L1
+    unsigned hist[kMaxPasses][256];   // radix digit histograms of all passes
+};
+
+// ---- relaxed 64-bit accesses for decoupled look-back descriptors ----
+__device__ __forceinline__ unsigned long long ld_relaxed(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Look-back descriptor: flag in bits 62-63, value in bits 0-61.
+constexpr unsigned long long kDescAgg = 1ull << 62;     // this block's aggregate only
+constexpr unsigned long long kDescPrefix = 2ull << 62;  // inclusive prefix through this block
+constexpr unsigned long long kDescValue = (1ull << 62) - 1;
+
+// Decoupled look-back (Merrill & Garland, "Single-pass Parallel Prefix Scan
+// with Decoupled Look-back", 2016), run by one thread for one counter.
+// Descriptor of block b lives at desc[b * stride + lane_off].  Returns the
+// exclusive prefix of block `blk`.  Waits are bounded: after spin_limit polls
+// of a descriptor that is still empty the status word gets kStatusTimeout and
+// the partial prefix is used (the result is then invalid and the host reports
+// GS3DC_ERR_DEVICE_TIMEOUT).  Block indices are tickets taken in launch order,
+// so every predecessor is resident or finished and publishes without waiting.
+__device__ __forceinline__ unsigned long long lookback_exclusive_strided(
+    unsigned long long* desc, int blk, int stride, int lane_off, unsigned long long aggregate,
+    unsigned* status, unsigned spin_limit) {
+    unsigned long long* mine = desc + (size_t)blk * stride + lane_off;
+    if (blk == 0) {
+        st_relaxed(mine, kDescPrefix | aggregate);
+        return 0ull;
+    }
+    st_relaxed(mine, kDescAgg | aggregate);
+    unsigned long long excl = 0;
+    int j = blk - 1;
+    unsigned spins = 0;
+    while (j >= 0) {
+        const unsigned long long d = ld_relaxed(desc + (size_t)j * stride + lane_off);
+        const unsigned long long flag = d & ~kDescValue;
+        if (flag == 0ull) {
+            if (++spins > spin_limit) {
+                atomicOr(status, kStatusTimeout);
+                break;
+            }
+            __nanosleep(32);
+            continue;
+        }
+        excl += d & kDescValue;
+        if (flag == kDescPrefix) break;
+        --j;
+    }
+    st_relaxed(mine, kDescPrefix | (excl + aggregate));
+    return excl;
+}
+
+__device__ __forceinline__ unsigned long long lookback_exclusive(unsigned long long* desc, int blk,
+                                                                 unsigned long long aggregate,
+                                                                 unsigned* status, unsigned spin_limit) {
+    return lookback_exclusive_strided(desc, blk, 1, 0, aggregate, status, spin_limit);
+}
+
+// Correctly rounded float exp (double evaluation, one rounding).  glibc's
+// expf, which the reference calls through std::exp(float), agrees with it on
+// all but ~0.006% of inputs (by 1 ulp there).
+__device__ __forceinline__ float exp_ref(float x) { return (float)exp((double)x); }
+
+// Block-wide inclusive scan of one int per thread (256 threads); returns the
+// inclusive value, *total gets the block sum.  s_warp needs 8 ints.
+__device__ __forceinline__ int block_inclusive_scan(int v, int* s_warp, int* total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int n = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += n;
+    }
+    if (lane == 31) s_warp[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        int w = lane < 8 ? s_warp[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 8; o <<= 1) {
+            int n = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += n;
+        }
+        if (lane < 8) s_warp[lane] = w;
+    }
+    __syncthreads();
+    int add = warp > 0 ? s_warp[warp - 1] : 0;
+    *total = s_warp[7];
+    return v + add;
+}
+
+}  // namespace gs3d

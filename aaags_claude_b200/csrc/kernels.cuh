@@ -1,0 +1,115 @@
+// kernels.cuh -- argument structs and host-side launchers of the 3DGS kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include "common.cuh"
+
+namespace gs3d {
+
+// Model parameters in the reference layouts: raw (training) or activated (render).
+struct ModelPtrs {
+    float* pos;   // [N*3]
+    float* sc;    // [N*3]
+    float* rot;   // [N*4]
+    float* sh;    // [N*K*3]
+    float* op;    // [N]
+};
+
+struct AdamPtrs {
+    float *m_pos, *v_pos, *m_sc, *v_sc, *m_rot, *v_rot, *m_sh, *v_sh, *m_op, *v_op;
+};
+
+// Screen-space records written by the preprocess and read by both rasterisers.
+//   rec0[i] = (mean.x, mean.y, conic.a, conic.b)
+//   rec1[i] = (conic.c, opacity_2d, r, g)
+//   col_b[i] = b
+struct ScreenPtrs {
+    float4* rec0;
+    float4* rec1;
+    float* col_b;
+    float* depth;
+    int* radius;
+    int* tiles;
+    // optional ForwardCache fields (NULL unless requested)
+    float* cov3D;
+    float* p_view;
+    float* p_hom_w;
+    float* cov2D;
+    float* det;
+};
+
+struct PairPtrs {
+    unsigned long long* keys;   // [capacity]
+    unsigned* vals;             // [capacity]
+    unsigned long long capacity;
+    unsigned long long* scan_desc;  // look-back descriptors, one per preprocess CTA
+};
+
+struct PixelPtrs {
+    float* image;          // [H*W*3]
+    float* T_final;        // [H*W]
+    int* n_contrib;        // [H*W] contributor count (ForwardCache::n_contrib)
+    unsigned* last_j;      // [H*W] one past the last contributing pair index
+    unsigned char* dsign;  // [H*W] L1 signs: bits 0-1 ch0, 2-3 ch1, 4-5 ch2 (1:+, 2:-)
+    const float* d_image;  // [H*W*3] explicit image gradient (stage API)
+};
+
+// Screen-space gradients (RasterGradOutput, include/train_types.h:25-32).
+struct RGradPtrs {
+    float* dm2;   // [N*2]
+    float* dcon;  // [N*3]
+    float* drgb;  // [N*3]
+    float* dop;   // [N]
+};
+
+// Raw-parameter gradients (GradientOutput, include/train_types.h:35-43).
+struct GradPtrs {
+    float *g_pos, *g_sc, *g_rot, *g_sh, *g_op;
+};
+
+// Host arrays in PreprocessOutput layout, on the device (export / import).
+struct ScreenArrays {
+    float* means2D;
+    float* depths;
+    float* conics;
+    float* opac2d;
+    float* rgb;
+    int* radii;
+    int* tiles;
+};
+
+// ---- plain FP32 kernels (plain.cu, compiled without FMA contraction) ----
+cudaError_t launch_preprocess_plain(cudaStream_t st, const StepParams* sp, int N, bool train,
+                                    bool cache, ModelPtrs m, ScreenPtrs s, PairPtrs pr, Control* ctrl);
+cudaError_t launch_bin_arrays(cudaStream_t st, const StepParams* sp, int N, ScreenArrays a,
+                              PairPtrs pr, Control* ctrl);
+cudaError_t launch_export_screen(cudaStream_t st, int N, ScreenPtrs s, ScreenArrays a);
+cudaError_t launch_raster_fwd_plain(cudaStream_t st, const StepParams* sp, int num_tiles, bool fused_loss,
+                                    const unsigned* ranges, const unsigned* vals, ScreenPtrs s,
+                                    PixelPtrs px, Control* ctrl);
+cudaError_t launch_raster_bwd_plain(cudaStream_t st, const StepParams* sp, int num_tiles, bool from_sign,
+                                    const unsigned* ranges, const unsigned* vals, ScreenPtrs s,
+                                    PixelPtrs px, RGradPtrs g, Control* ctrl);
+cudaError_t launch_preprocess_bwd_plain(cudaStream_t st, const StepParams* sp, int N, bool fused_adam,
+                                        ModelPtrs raw, AdamPtrs adam, ScreenPtrs s, RGradPtrs rg,
+                                        GradPtrs gout, Control* ctrl);
+cudaError_t launch_optimizer_plain(cudaStream_t st, const StepParams* sp, int N, int mc3, ModelPtrs raw,
+                                   AdamPtrs adam, GradPtrs g);
+
+// ---- radix sort + ranges (sort.cu) ----
+// Sorts (keys, vals) of *P (device) pairs by the low sort_bits key bits with
+// 8-bit LSD passes, ping-ponging between buffer 0 and 1.  Returns in *which
+// the buffer that holds the result.  desc must hold passes * desc_stride
+// descriptors, zeroed by the caller before the call.
+cudaError_t launch_radix_sort(cudaStream_t st, const StepParams* sp, int sort_passes,
+                              unsigned long long capacity, unsigned long long* keys0, unsigned* vals0,
+                              unsigned long long* keys1, unsigned* vals1, unsigned long long* desc,
+                              unsigned long long desc_stride, Control* ctrl, int* which);
+cudaError_t launch_tile_ranges(cudaStream_t st, unsigned long long capacity,
+                               const unsigned long long* keys_sorted, unsigned* ranges, Control* ctrl);
+
+constexpr int kSortThreads = 256;
+constexpr int kSortItems = 16;
+constexpr int kSortTile = kSortThreads * kSortItems;  // keys per onesweep CTA
+
+}  // namespace gs3d

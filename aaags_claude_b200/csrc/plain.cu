@@ -1,0 +1,1143 @@
+// plain.cu -- plain-FP32 form of the 3DGS hot path for sm_100a.
+//
+// Compiled with -fmad=false and IEEE division / square root so that every
+// float operation rounds like the reference's x86 build with
+// -ffp-contract=off (harmonyos_3dgs CMakeLists.txt:19); the operation order
+// below follows the reference's CPU stages line by line, which is what makes
+// depths, radii, tile counts, keys, sorted order and tile ranges bit-exact.
+//
+// Kernels:
+//   k_preprocess    one thread per Gaussian: (activation) -> projection ->
+//                   EWA covariance -> conic / radius / tile rect -> SH colour,
+//                   then a block scan + decoupled look-back over tiles_touched
+//                   and a block-cooperative emission of (tile|depth, index)
+//                   pairs.  Replaces preprocess + prefix sum + binning.
+//   k_bin_arrays    the same scan + emission from host-provided screen arrays.
+//   k_raster_fwd    one CTA per 16x16 tile, one thread per pixel; pairs are
+//                   gathered in batches of 256 into shared memory; CTA-wide
+//                   early exit once every pixel saturated.  Optional fused L1.
+//   k_raster_bwd    reverse traversal from each pixel's last contributor with
+//                   transmittance recovered from the stored T_final; per
+//                   Gaussian the warp's 32 pixel contributions are shuffle-
+//                   reduced and one lane issues the atomics.
+//   k_preprocess_bwd  the full per-Gaussian adjoint chain, fused with Adam.
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace gs3d {
+namespace {
+
+constexpr float kAlphaMin = 1.0f / 255.0f;   // rasterizer_cpu.cpp:150
+constexpr float kTMin = 0.0001f;             // rasterizer_cpu.cpp:165
+
+// ---------------- reference math (float, reference operation order) ----------------
+
+// math_utils.cpp:8-12
+__device__ __forceinline__ void xform4x3(const float p[3], const float* m, float o[3]) {
+    o[0] = m[0] * p[0] + m[4] * p[1] + m[8] * p[2] + m[12];
+    o[1] = m[1] * p[0] + m[5] * p[1] + m[9] * p[2] + m[13];
+    o[2] = m[2] * p[0] + m[6] * p[1] + m[10] * p[2] + m[14];
+}
+// math_utils.cpp:14-19 (w component only; x,y are what the projection uses too)
+__device__ __forceinline__ void xform4x4(const float p[3], const float* m, float o[4]) {
+    o[0] = m[0] * p[0] + m[4] * p[1] + m[8] * p[2] + m[12];
+    o[1] = m[1] * p[0] + m[5] * p[1] + m[9] * p[2] + m[13];
+    o[2] = m[2] * p[0] + m[6] * p[1] + m[10] * p[2] + m[14];
+    o[3] = m[3] * p[0] + m[7] * p[1] + m[11] * p[2] + m[15];
+}
+
+// math_utils.cpp:21-28
+__device__ __forceinline__ void tile_rect(float px, float py, int r, int gx, int gy, int tw, int th,
+                                          int rmn[2], int rmx[2]) {
+    const float fr = (float)r, ftw = (float)tw, fth = (float)th;
+    rmn[0] = min(gx, max(0, (int)((px - fr) / ftw)));
+    rmn[1] = min(gy, max(0, (int)((py - fr) / fth)));
+    rmx[0] = min(gx, max(0, (int)((px + fr + ftw - 1.0f) / ftw)));
+    rmx[1] = min(gy, max(0, (int)((py + fr + fth - 1.0f) / fth)));
+}
+
+__device__ __forceinline__ float fmin_ref(float a, float b) { return (b < a) ? b : a; }  // std::min
+__device__ __forceinline__ float fmax_ref(float a, float b) { return (a < b) ? b : a; }  // std::max
+
+// math_utils.cpp:38-42
+__device__ __forceinline__ void quat_to_R(float r, float x, float y, float z, float R[3][3]) {
+    R[0][0] = 1.f - 2.f * (y * y + z * z);
+    R[0][1] = 2.f * (x * y + r * z);
+    R[0][2] = 2.f * (x * z - r * y);
+    R[1][0] = 2.f * (x * y - r * z);
+    R[1][1] = 1.f - 2.f * (x * x + z * z);
+    R[1][2] = 2.f * (y * z + r * x);
+    R[2][0] = 2.f * (x * z + r * y);
+    R[2][1] = 2.f * (y * z - r * x);
+    R[2][2] = 1.f - 2.f * (x * x + y * y);
+}
+
+// math_utils.cpp:30-62
+__device__ __forceinline__ void cov3d(const float s_in[3], float mod, const float q[4], float cov[6]) {
+    const float s[3] = {mod * s_in[0], mod * s_in[1], mod * s_in[2]};
+    float R[3][3], M[3][3];
+    quat_to_R(q[0], q[1], q[2], q[3], R);
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) M[i][j] = s[i] * R[i][j];
+    cov[0] = M[0][0] * M[0][0] + M[1][0] * M[1][0] + M[2][0] * M[2][0];
+    cov[1] = M[0][0] * M[0][1] + M[1][0] * M[1][1] + M[2][0] * M[2][1];
+    cov[2] = M[0][0] * M[0][2] + M[1][0] * M[1][2] + M[2][0] * M[2][2];
+    cov[3] = M[0][1] * M[0][1] + M[1][1] * M[1][1] + M[2][1] * M[2][1];
+    cov[4] = M[0][1] * M[0][2] + M[1][1] * M[1][2] + M[2][1] * M[2][2];
+    cov[5] = M[0][2] * M[0][2] + M[1][2] * M[1][2] + M[2][2] * M[2][2];
+}
+
+// Clamped view point and T = W J of the EWA projection, [col][row] as in
+// math_utils.cpp:64-110.  txtz / tytz are the unclamped ratios.
+struct Ewa {
+    float t[3];
+    float txtz, tytz, limx, limy;
+    float J[3][3], W[3][3], T[3][3];
+};
+
+__device__ __forceinline__ void ewa_setup(const float pos[3], const float* vm, float fx, float fy,
+                                          float tanx, float tany, Ewa& e) {
+    float t[3];
+    xform4x3(pos, vm, t);
+    e.limx = 1.3f * tanx;
+    e.limy = 1.3f * tany;
+    e.txtz = t[0] / t[2];
+    e.tytz = t[1] / t[2];
+    t[0] = fmin_ref(e.limx, fmax_ref(-e.limx, e.txtz)) * t[2];
+    t[1] = fmin_ref(e.limy, fmax_ref(-e.limy, e.tytz)) * t[2];
+    e.t[0] = t[0];
+    e.t[1] = t[1];
+    e.t[2] = t[2];
+    e.J[0][0] = fx / t[2]; e.J[0][1] = 0.0f; e.J[0][2] = -(fx * t[0]) / (t[2] * t[2]);
+    e.J[1][0] = 0.0f; e.J[1][1] = fy / t[2]; e.J[1][2] = -(fy * t[1]) / (t[2] * t[2]);
+    e.J[2][0] = 0.0f; e.J[2][1] = 0.0f; e.J[2][2] = 0.0f;
+    e.W[0][0] = vm[0]; e.W[0][1] = vm[4]; e.W[0][2] = vm[8];
+    e.W[1][0] = vm[1]; e.W[1][1] = vm[5]; e.W[1][2] = vm[9];
+    e.W[2][0] = vm[2]; e.W[2][1] = vm[6]; e.W[2][2] = vm[10];
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            float acc = 0.0f;
+#pragma unroll
+            for (int k = 0; k < 3; k++) acc += e.W[k][r] * e.J[c][k];
+            e.T[c][r] = acc;
+        }
+}
+
+// math_utils.cpp:111-143
+__device__ __forceinline__ void cov2d(const Ewa& e, const float c3[6], float out[3]) {
+    const float V[3][3] = {{c3[0], c3[1], c3[2]}, {c3[1], c3[3], c3[4]}, {c3[2], c3[4], c3[5]}};
+    float tmp[3][3];
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            float acc = 0.0f;
+#pragma unroll
+            for (int k = 0; k < 3; k++) acc += V[r][k] * e.T[c][k];
+            tmp[c][r] = acc;
+        }
+    float res00 = 0.0f, res10 = 0.0f, res11 = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 3; k++) res00 += e.T[0][k] * tmp[0][k];
+#pragma unroll
+    for (int k = 0; k < 3; k++) res10 += e.T[0][k] * tmp[1][k];
+#pragma unroll
+    for (int k = 0; k < 3; k++) res11 += e.T[1][k] * tmp[1][k];
+    out[0] = res00;
+    out[1] = res10;
+    out[2] = res11;
+}
+
+// SH constants, sh_eval.cpp:5-22
+#define SH_C0 0.28209479177387814f
+#define SH_C1 0.4886025119029199f
+#define SH_C20 1.0925484305920792f
+#define SH_C21 -1.0925484305920792f
+#define SH_C22 0.31539156525252005f
+#define SH_C23 -1.0925484305920792f
+#define SH_C24 0.5462742152960396f
+#define SH_C30 -0.5900435899266435f
+#define SH_C31 2.890611442640554f
+#define SH_C32 -0.4570457994644658f
+#define SH_C33 0.3731763325901154f
+#define SH_C34 -0.4570457994644658f
+#define SH_C35 1.445305721320277f
+#define SH_C36 -0.5900435899266435f
+
+// Normalised view direction (sh_eval.cpp:31-35); returns |pos - cam|.
+__device__ __forceinline__ float view_dir(const float p[3], const float* cam, float d[3]) {
+    const float dx = p[0] - cam[0], dy = p[1] - cam[1], dz = p[2] - cam[2];
+    const float len = sqrtf(dx * dx + dy * dy + dz * dz);
+    d[0] = dx / len;
+    d[1] = dy / len;
+    d[2] = dz / len;
+    return len;
+}
+
+// Pre-clamp SH colour of one channel (sh_eval.cpp:38-81). sh points at this
+// Gaussian's coefficients; stride 3 between bases.
+__device__ __forceinline__ float sh_channel(int deg, const float* __restrict__ sh, int c, float x, float y,
+                                            float z) {
+    float v = SH_C0 * sh[c];
+    if (deg > 0) {
+        v += -SH_C1 * y * sh[3 + c] + SH_C1 * z * sh[6 + c] + -SH_C1 * x * sh[9 + c];
+        if (deg > 1) {
+            const float xx = x * x, yy = y * y, zz = z * z, xy = x * y, yz = y * z, xz = x * z;
+            v += SH_C20 * xy * sh[12 + c] + SH_C21 * yz * sh[15 + c] +
+                 SH_C22 * (2.0f * zz - xx - yy) * sh[18 + c] + SH_C23 * xz * sh[21 + c] +
+                 SH_C24 * (xx - yy) * sh[24 + c];
+            if (deg > 2) {
+                v += SH_C30 * y * (3.0f * xx - yy) * sh[27 + c] + SH_C31 * xy * z * sh[30 + c] +
+                     SH_C32 * y * (4.0f * zz - xx - yy) * sh[33 + c] +
+                     SH_C33 * z * (2.0f * zz - 3.0f * xx - 3.0f * yy) * sh[36 + c] +
+                     SH_C34 * x * (4.0f * zz - xx - yy) * sh[39 + c] + SH_C35 * z * (xx - yy) * sh[42 + c] +
+                     SH_C36 * x * (xx - 3.0f * yy) * sh[45 + c];
+            }
+        }
+    }
+    return v;
+}
+
+// Activation of one Gaussian (train_types.cpp:6-36): exp scales, unit
+// quaternion (length clamped to 1e-12), sigmoid opacity.
+__device__ __forceinline__ void activate_one(const float rsc[3], const float rq[4], float rop, float sc[3],
+                                             float q[4], float* op) {
+#pragma unroll
+    for (int k = 0; k < 3; k++) sc[k] = exp_ref(rsc[k]);
+    float len = sqrtf(rq[0] * rq[0] + rq[1] * rq[1] + rq[2] * rq[2] + rq[3] * rq[3]);
+    if (len < 1e-12f) len = 1e-12f;
+    const float inv = 1.0f / len;
+#pragma unroll
+    for (int k = 0; k < 4; k++) q[k] = rq[k] * inv;
+    *op = 1.0f / (1.0f + exp_ref(-rop));
+}
+
+// Alpha / transmittance decisions of the front-to-back blend
+// (rasterizer_cpu.cpp:149-166).  exp is evaluated with the accurate expf and
+// re-evaluated correctly rounded when alpha or the next transmittance lies
+// within a few ulp of a threshold, so skip / stop decisions follow the
+// reference's glibc-based ones.
+// Returns 0 = skip, 1 = blend, 2 = stop (transmittance would saturate).
+__device__ __forceinline__ int blend_decision(float power, float o, float T, float& alpha, float& e,
+                                              float& test_T) {
+    e = expf(power);
+    alpha = fmin_ref(0.99f, o * e);
+    test_T = T * (1.0f - alpha);
+    if (fabsf(alpha - kAlphaMin) < 1e-8f || fabsf(test_T - kTMin) < 1e-8f) {
+        e = exp_ref(power);
+        alpha = fmin_ref(0.99f, o * e);
+        test_T = T * (1.0f - alpha);
+    }
+    if (alpha < kAlphaMin) return 0;
+    if (test_T < kTMin) return 2;
+    return 1;
+}
+
+// The alpha-only decision of the backward (the forward's last-contributor
+// index already encodes the stop).  Agrees with blend_decision's skip.
+__device__ __forceinline__ bool alpha_accept(float power, float o, float& alpha, float& e) {
+    e = expf(power);
+    alpha = fmin_ref(0.99f, o * e);
+    if (fabsf(alpha - kAlphaMin) < 1e-8f) {
+        e = exp_ref(power);
+        alpha = fmin_ref(0.99f, o * e);
+    }
+    return !(alpha < kAlphaMin);
+}
+
+// ---------------- per-Gaussian forward (preprocessor_cpu.cpp:186-265) ----------------
+
+struct Proj {
+    float px, py, depth, con[3], opac, rgb[3];
+    int radius, rmn[2], rmx[2];
+    float cov3[6], pv[3], phw, cov2[3], det;
+};
+
+// Returns false when the Gaussian is culled.
+__device__ __forceinline__ bool project_one(const StepParams& sp, const float p[3], const float sc[3],
+                                            const float q[4], float op, const float* __restrict__ sh,
+                                            Proj& r) {
+    const gs3d_camera& cam = sp.cam;
+    float pv[3];
+    xform4x3(p, cam.view_matrix, pv);
+    if (pv[2] <= 0.2f) return false;
+    float ph[4];
+    xform4x4(p, cam.viewproj_matrix, ph);
+    const float pw = 1.0f / (ph[3] + 1e-7f);
+    const float ndc_x = ph[0] * pw, ndc_y = ph[1] * pw;
+    const float pix_x = ((ndc_x + 1.0f) * (float)cam.width - 1.0f) * 0.5f;
+    const float pix_y = ((ndc_y + 1.0f) * (float)cam.height - 1.0f) * 0.5f;
+
+    float c3[6];
+    cov3d(sc, sp.cfg.scale_modifier, q, c3);
+    Ewa e;
+    ewa_setup(p, cam.view_matrix, sp.focal_x, sp.focal_y, cam.tan_fovx, cam.tan_fovy, e);
+    float c2[3];
+    cov2d(e, c3, c2);
+    const float det_cov = c2[0] * c2[2] - c2[1] * c2[1];
+    c2[0] += 0.3f;
+    c2[2] += 0.3f;
+    const float det = c2[0] * c2[2] - c2[1] * c2[1];
+    float hconv = 1.0f;
+    if (sp.cfg.antialiasing) hconv = sqrtf(fmax_ref(0.000025f, det_cov / det));
+    if (det == 0.0f) return false;
+    const float dinv = 1.0f / det;
+    const float mid = 0.5f * (c2[0] + c2[2]);
+    const float l1 = mid + sqrtf(fmax_ref(0.1f, mid * mid - det));
+    const float l2 = mid - sqrtf(fmax_ref(0.1f, mid * mid - det));
+    const int radius = (int)ceilf(3.0f * sqrtf(fmax_ref(l1, l2)));
+    if (radius > max(cam.width, cam.height)) return false;
+    tile_rect(pix_x, pix_y, radius, sp.grid_x, sp.grid_y, sp.cfg.tile_w, sp.cfg.tile_h, r.rmn, r.rmx);
+    if ((r.rmx[0] - r.rmn[0]) * (r.rmx[1] - r.rmn[1]) == 0) return false;
+
+    float d[3];
+    view_dir(p, cam.cam_pos, d);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        float v = fmax_ref(0.0f, sh_channel(sp.sh_deg_fwd, sh, c, d[0], d[1], d[2]) + 0.5f);
+        if (!sp.cfg.training) v = fmin_ref(1.0f, v);
+        r.rgb[c] = v;
+    }
+    r.px = pix_x;
+    r.py = pix_y;
+    r.depth = pv[2];
+    r.con[0] = c2[2] * dinv;
+    r.con[1] = -c2[1] * dinv;
+    r.con[2] = c2[0] * dinv;
+    r.opac = op * hconv;
+    r.radius = radius;
+#pragma unroll
+    for (int k = 0; k < 6; k++) r.cov3[k] = c3[k];
+#pragma unroll
+    for (int k = 0; k < 3; k++) r.pv[k] = pv[k];
+    r.phw = ph[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) r.cov2[k] = c2[k];
+    r.det = det;
+    return true;
+}
+
+// ---------------- block scan + look-back + pair emission ----------------
+
+struct EmitShared {
+    int warp[8];
+    int excl[kBlock];
+    int rect[kBlock];      // xmin | ymin << 16
+    int width[kBlock];
+    int limit[kBlock];     // pairs actually emitted (rect area, <= count)
+    unsigned depth[kBlock];
+    unsigned long long base;
+};
+
+// Scans cnt over the CTA, finds the CTA's global offset by decoupled
+// look-back and writes the CTA's pairs with consecutive threads writing
+// consecutive pairs (fully coalesced, balanced however uneven the rects).
+// Pair order: Gaussian-major, then row-major inside the rect
+// (tile_binner_cpu.cpp:90-97).
+__device__ __forceinline__ void scan_and_emit(EmitShared& sm, int blk, int cnt, int emit, int rx, int ry,
+                                              int rw, unsigned dbits, int grid_x, PairPtrs pr,
+                                              Control* ctrl, unsigned spin_limit) {
+    const int tid = threadIdx.x;
+    int total;
+    const int incl = block_inclusive_scan(cnt, sm.warp, &total);
+    sm.excl[tid] = incl - cnt;
+    sm.rect[tid] = rx | (ry << 16);
+    sm.width[tid] = rw;
+    sm.limit[tid] = emit;
+    sm.depth[tid] = dbits;
+    if (tid == 0) {
+        const unsigned long long ex =
+            lookback_exclusive(pr.scan_desc, blk, (unsigned long long)total, &ctrl->status, spin_limit);
+        sm.base = ex;
+        if (blk == (int)gridDim.x - 1) ctrl->total_pairs = ex + (unsigned long long)total;
+        if (ex + (unsigned long long)total > pr.capacity) atomicOr(&ctrl->status, kStatusOverflow);
+    }
+    __syncthreads();
+    const unsigned long long base = sm.base;
+    for (int k = tid; k < total; k += kBlock) {
+        int lo = 0, hi = kBlock;
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (sm.excl[mid] <= k) lo = mid;
+            else hi = mid;
+        }
+        const int local = k - sm.excl[lo];
+        const unsigned long long dst = base + (unsigned long long)k;
+        if (local >= sm.limit[lo] || dst >= pr.capacity) continue;
+        const int w = sm.width[lo];
+        const int r = sm.rect[lo];
+        const int x = (r & 0xffff) + local % w;
+        const int y = (r >> 16) + local / w;
+        const unsigned tile = (unsigned)(y * grid_x + x);
+        pr.keys[dst] = ((unsigned long long)tile << 32) | sm.depth[lo];
+        pr.vals[dst] = (unsigned)(blk * kBlock + lo);
+    }
+}
+
+// ---------------- kernels ----------------
+
+template <bool TRAIN, bool CACHE>
+__global__ void __launch_bounds__(kBlock) k_preprocess(const StepParams* __restrict__ spp, int N, ModelPtrs m,
+                                                       ScreenPtrs s, PairPtrs pr, Control* ctrl) {
+    __shared__ EmitShared sm;
+    __shared__ int s_blk;
+    const StepParams& sp = *spp;
+    if (threadIdx.x == 0) s_blk = (int)atomicAdd(&ctrl->tickets[0], 1u);
+    __syncthreads();
+    const int blk = s_blk;
+    const int i = blk * kBlock + threadIdx.x;
+    int cnt = 0, rx = 0, ry = 0, rw = 1;
+    unsigned dbits = 0;
+    if (i < N) {
+        const int mc3 = sp.max_coeffs * 3;
+        const float p[3] = {m.pos[3 * i], m.pos[3 * i + 1], m.pos[3 * i + 2]};
+        float sc[3], q[4], op;
+        if (TRAIN) {
+            const float rsc[3] = {m.sc[3 * i], m.sc[3 * i + 1], m.sc[3 * i + 2]};
+            const float rq[4] = {m.rot[4 * i], m.rot[4 * i + 1], m.rot[4 * i + 2], m.rot[4 * i + 3]};
+            activate_one(rsc, rq, m.op[i], sc, q, &op);
+        } else {
+#pragma unroll
+            for (int k = 0; k < 3; k++) sc[k] = m.sc[3 * i + k];
+#pragma unroll
+            for (int k = 0; k < 4; k++) q[k] = m.rot[4 * i + k];
+            op = m.op[i];
+        }
+        Proj r;
+        const bool vis = project_one(sp, p, sc, q, op, m.sh + (size_t)mc3 * i, r);
+        if (vis) {
+            cnt = (r.rmx[1] - r.rmn[1]) * (r.rmx[0] - r.rmn[0]);
+            rx = r.rmn[0];
+            ry = r.rmn[1];
+            rw = r.rmx[0] - r.rmn[0];
+            dbits = __float_as_uint(r.depth);
+            s.rec0[i] = make_float4(r.px, r.py, r.con[0], r.con[1]);
+            s.rec1[i] = make_float4(r.con[2], r.opac, r.rgb[0], r.rgb[1]);
+            s.col_b[i] = r.rgb[2];
+            s.depth[i] = r.depth;
+            s.radius[i] = r.radius;
+        } else {
+            s.rec0[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+            s.rec1[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+            s.col_b[i] = 0.f;
+            s.depth[i] = 0.f;
+            s.radius[i] = 0;
+        }
+        s.tiles[i] = cnt;
+        if (CACHE) {
+#pragma unroll
+            for (int k = 0; k < 6; k++) s.cov3D[6 * i + k] = vis ? r.cov3[k] : 0.f;
+#pragma unroll
+            for (int k = 0; k < 3; k++) s.p_view[3 * i + k] = vis ? r.pv[k] : 0.f;
+            s.p_hom_w[i] = vis ? r.phw : 0.f;
+#pragma unroll
+            for (int k = 0; k < 3; k++) s.cov2D[3 * i + k] = vis ? r.cov2[k] : 0.f;
+            s.det[i] = vis ? r.det : 0.f;
+        }
+    }
+    scan_and_emit(sm, blk, cnt, cnt, rx, ry, rw, dbits, sp.grid_x, pr, ctrl, sp.spin_limit);
+}
+
+// TileBinner::bin over host-provided screen arrays (tile_binner_cpu.cpp:33-99):
+// offsets from tiles_touched, pairs from the rect recomputed from (mean, radius).
+__global__ void __launch_bounds__(kBlock) k_bin_arrays(const StepParams* __restrict__ spp, int N,
+                                                       ScreenArrays a, PairPtrs pr, Control* ctrl) {
+    __shared__ EmitShared sm;
+    __shared__ int s_blk;
+    const StepParams& sp = *spp;
+    if (threadIdx.x == 0) s_blk = (int)atomicAdd(&ctrl->tickets[0], 1u);
+    __syncthreads();
+    const int blk = s_blk;
+    const int i = blk * kBlock + threadIdx.x;
+    int cnt = 0, emit = 0, rx = 0, ry = 0, rw = 1;
+    unsigned dbits = 0;
+    if (i < N) {
+        cnt = a.tiles[i];
+        if (a.radii[i] > 0) {
+            int rmn[2], rmx[2];
+            tile_rect(a.means2D[2 * i], a.means2D[2 * i + 1], a.radii[i], sp.grid_x, sp.grid_y,
+                      sp.cfg.tile_w, sp.cfg.tile_h, rmn, rmx);
+            rx = rmn[0];
+            ry = rmn[1];
+            rw = max(1, rmx[0] - rmn[0]);
+            emit = min(cnt, (rmx[0] - rmn[0]) * (rmx[1] - rmn[1]));
+            dbits = __float_as_uint(a.depths[i]);
+        }
+    }
+    scan_and_emit(sm, blk, cnt, emit, rx, ry, rw, dbits, sp.grid_x, pr, ctrl, sp.spin_limit);
+}
+
+// Unpacks the screen records into PreprocessOutput's layout.
+__global__ void k_export_screen(int N, ScreenPtrs s, ScreenArrays a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const float4 r0 = s.rec0[i], r1 = s.rec1[i];
+    a.means2D[2 * i] = r0.x;
+    a.means2D[2 * i + 1] = r0.y;
+    a.conics[3 * i] = r0.z;
+    a.conics[3 * i + 1] = r0.w;
+    a.conics[3 * i + 2] = r1.x;
+    a.opac2d[i] = r1.y;
+    a.rgb[3 * i] = r1.z;
+    a.rgb[3 * i + 1] = r1.w;
+    a.rgb[3 * i + 2] = s.col_b[i];
+    a.depths[i] = s.depth[i];
+    a.radii[i] = s.radius[i];
+    a.tiles[i] = s.tiles[i];
+}
+
+// Rasterizer forward (rasterizer_cpu.cpp:38-53, 137-198).
+template <bool FUSED_LOSS>
+__global__ void __launch_bounds__(kBlock) k_raster_fwd(const StepParams* __restrict__ spp,
+                                                       const unsigned* __restrict__ ranges,
+                                                       const unsigned* __restrict__ vals, ScreenPtrs s,
+                                                       PixelPtrs px, Control* ctrl) {
+    __shared__ float4 s_r0[kBlock];
+    __shared__ float4 s_r1[kBlock];
+    __shared__ float s_b[kBlock];
+    __shared__ double s_loss[kBlock / 32];
+    const StepParams& sp = *spp;
+    const int W = sp.cam.width, H = sp.cam.height;
+    const int tile = blockIdx.x;
+    const int tx = tile % sp.grid_x, ty = tile / sp.grid_x;
+    const int x = tx * kTile + (threadIdx.x & (kTile - 1));
+    const int y = ty * kTile + (threadIdx.x >> 4);
+    const bool inside = x < W && y < H;
+    const unsigned rs = ranges[2 * tile], re = ranges[2 * tile + 1];
+    const float fx = (float)x, fy = (float)y;
+    float T = 1.0f, C0 = 0.0f, C1 = 0.0f, C2 = 0.0f;
+    int cnt = 0;
+    unsigned last = 0;
+    bool done = !inside;
+    for (unsigned b = rs; b < re; b += kBlock) {
+        if (__syncthreads_count(done) == kBlock) break;
+        const unsigned j = b + threadIdx.x;
+        if (j < re) {
+            const unsigned g = vals[j];
+            s_r0[threadIdx.x] = s.rec0[g];
+            s_r1[threadIdx.x] = s.rec1[g];
+            s_b[threadIdx.x] = s.col_b[g];
+        }
+        __syncthreads();
+        const int nb = (int)min((unsigned)kBlock, re - b);
+        if (!done) {
+            for (int k = 0; k < nb; k++) {
+                const float4 a = s_r0[k];
+                const float dx = a.x - fx, dy = a.y - fy;
+                const float4 c = s_r1[k];
+                const float power = -0.5f * (a.z * dx * dx + c.x * dy * dy) - a.w * dx * dy;
+                if (power > 0.0f) continue;
+                float alpha, e, test_T;
+                const int dec = blend_decision(power, c.y, T, alpha, e, test_T);
+                if (dec == 0) continue;
+                if (dec == 2) {
+                    done = true;
+                    break;
+                }
+                C0 += c.z * alpha * T;
+                C1 += c.w * alpha * T;
+                C2 += s_b[k] * alpha * T;
+                T = test_T;
+                cnt++;
+                last = b + (unsigned)k + 1u;
+            }
+        }
+    }
+    double lsum = 0.0;
+    if (inside) {
+        const int pix = y * W + x;
+        const float o0 = C0 + T * sp.cfg.bg_color[0];
+        const float o1 = C1 + T * sp.cfg.bg_color[1];
+        const float o2 = C2 + T * sp.cfg.bg_color[2];
+        px.image[3 * pix] = o0;
+        px.image[3 * pix + 1] = o1;
+        px.image[3 * pix + 2] = o2;
+        if (px.T_final) px.T_final[pix] = T;
+        if (px.n_contrib) px.n_contrib[pix] = cnt;
+        if (px.last_j) px.last_j[pix] = last;
+        if (FUSED_LOSS) {
+            // loss.cpp:8-14: diff = rendered - gt, sign gradient +-1/n
+            const float d0 = o0 - sp.gt[3 * pix], d1 = o1 - sp.gt[3 * pix + 1], d2 = o2 - sp.gt[3 * pix + 2];
+            const unsigned sg = (d0 > 0.f ? 1u : (d0 < 0.f ? 2u : 0u)) | (d1 > 0.f ? 4u : (d1 < 0.f ? 8u : 0u)) |
+                                (d2 > 0.f ? 16u : (d2 < 0.f ? 32u : 0u));
+            px.dsign[pix] = (unsigned char)sg;
+            lsum = (double)fabsf(d0) + (double)fabsf(d1) + (double)fabsf(d2);
+        }
+    }
+    if (FUSED_LOSS) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
+        if ((threadIdx.x & 31) == 0) s_loss[threadIdx.x >> 5] = lsum;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = 0.0;
+#pragma unroll
+            for (int w = 0; w < kBlock / 32; w++) t += s_loss[w];
+            atomicAdd(&ctrl->loss_sum, t);
+        }
+    }
+}
+
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Rasterizer backward (rasterizer_backward_cpu.cpp:20-133): back-to-front
+// over each pixel's contributors, transmittance recovered by division from
+// T_final instead of a replayed per-pixel list.
+template <bool FROM_SIGN>
+__global__ void __launch_bounds__(kBlock) k_raster_bwd(const StepParams* __restrict__ spp,
+                                                       const unsigned* __restrict__ ranges,
+                                                       const unsigned* __restrict__ vals, ScreenPtrs s,
+                                                       PixelPtrs px, RGradPtrs g, Control* ctrl) {
+    __shared__ float4 s_r0[kBlock];
+    __shared__ float4 s_r1[kBlock];
+    __shared__ float s_b[kBlock];
+    __shared__ unsigned s_idx[kBlock];
+    __shared__ unsigned s_maxlast;
+    if (FROM_SIGN && (ctrl->status & kStatusOverflow)) return;
+    const StepParams& sp = *spp;
+    const int W = sp.cam.width, H = sp.cam.height;
+    const int tile = blockIdx.x;
+    const int tx = tile % sp.grid_x, ty = tile / sp.grid_x;
+    const int x = tx * kTile + (threadIdx.x & (kTile - 1));
+    const int y = ty * kTile + (threadIdx.x >> 4);
+    const bool inside = x < W && y < H;
+    const unsigned rs = ranges[2 * tile];
+    const float fx = (float)x, fy = (float)y;
+    const int pix = y * W + x;
+    float T = 0.0f, dC0 = 0.0f, dC1 = 0.0f, dC2 = 0.0f;
+    unsigned last = 0;
+    if (inside) {
+        T = px.T_final[pix];
+        last = px.last_j[pix];
+        if (FROM_SIGN) {
+            const unsigned sg = px.dsign[pix];
+            const float inv_n = sp.inv_n;
+            dC0 = (sg & 1u) ? inv_n : ((sg & 2u) ? -inv_n : 0.0f);
+            dC1 = (sg & 4u) ? inv_n : ((sg & 8u) ? -inv_n : 0.0f);
+            dC2 = (sg & 16u) ? inv_n : ((sg & 32u) ? -inv_n : 0.0f);
+        } else {
+            dC0 = px.d_image[3 * pix];
+            dC1 = px.d_image[3 * pix + 1];
+            dC2 = px.d_image[3 * pix + 2];
+        }
+    }
+    float acc0 = sp.cfg.bg_color[0], acc1 = sp.cfg.bg_color[1], acc2 = sp.cfg.bg_color[2];
+    if (threadIdx.x == 0) s_maxlast = 0;
+    __syncthreads();
+    if (last) atomicMax(&s_maxlast, last);
+    __syncthreads();
+    const unsigned maxlast = s_maxlast;
+    if (maxlast <= rs) return;
+    const unsigned lane = threadIdx.x & 31;
+    // batches [bs, be) walked from the back; the first one ends at maxlast
+    for (unsigned be = maxlast; be > rs;) {
+        const unsigned bs = (be - rs > (unsigned)kBlock) ? be - kBlock : rs;
+        const unsigned j = bs + threadIdx.x;
+        if (j < be) {
+            const unsigned gi = vals[j];
+            s_idx[threadIdx.x] = gi;
+            s_r0[threadIdx.x] = s.rec0[gi];
+            s_r1[threadIdx.x] = s.rec1[gi];
+            s_b[threadIdx.x] = s.col_b[gi];
+        }
+        __syncthreads();
+        for (int k = (int)(be - bs) - 1; k >= 0; k--) {
+            const unsigned jj = bs + (unsigned)k;
+            bool contrib = false;
+            float g_r = 0.f, g_g = 0.f, g_b = 0.f, g_o = 0.f, g_mx = 0.f, g_my = 0.f, g_ca = 0.f, g_cb = 0.f,
+                  g_cc = 0.f;
+            if (jj < last) {
+                const float4 a = s_r0[k];
+                const float4 c = s_r1[k];
+                const float dx = a.x - fx, dy = a.y - fy;
+                const float power = -0.5f * (a.z * dx * dx + c.x * dy * dy) - a.w * dx * dy;
+                float alpha, ep;
+                if (!(power > 0.0f) && alpha_accept(power, c.y, alpha, ep)) {
+                    contrib = true;
+                    const float cb = s_b[k];
+                    const float oma = 1.0f - alpha;
+                    const float Ti = (oma > 1e-6f) ? T / oma : 0.0f;
+                    g_r = alpha * Ti * dC0;
+                    g_g = alpha * Ti * dC1;
+                    g_b = alpha * Ti * dC2;
+                    float d_alpha = 0.0f;
+                    d_alpha += Ti * (c.z - acc0) * dC0;
+                    d_alpha += Ti * (c.w - acc1) * dC1;
+                    d_alpha += Ti * (cb - acc2) * dC2;
+                    acc0 = alpha * c.z + oma * acc0;
+                    acc1 = alpha * c.w + oma * acc1;
+                    acc2 = alpha * cb + oma * acc2;
+                    T = Ti;
+                    float d_power = 0.0f;
+                    if (alpha < 0.99f) {
+                        d_power = d_alpha * c.y * ep;
+                        g_o = d_alpha * ep;
+                    }
+                    g_mx = d_power * (-a.z * dx - a.w * dy);
+                    g_my = d_power * (-c.x * dy - a.w * dx);
+                    g_ca = d_power * (-0.5f * dx * dx);
+                    g_cb = d_power * (-dx * dy);
+                    g_cc = d_power * (-0.5f * dy * dy);
+                }
+            }
+            if (__any_sync(0xffffffffu, contrib)) {
+                g_r = warp_sum(g_r);
+                g_g = warp_sum(g_g);
+                g_b = warp_sum(g_b);
+                g_o = warp_sum(g_o);
+                g_mx = warp_sum(g_mx);
+                g_my = warp_sum(g_my);
+                g_ca = warp_sum(g_ca);
+                g_cb = warp_sum(g_cb);
+                g_cc = warp_sum(g_cc);
+                if (lane == 0) {
+                    const unsigned gi = s_idx[k];
+                    atomicAdd(&g.drgb[3 * gi], g_r);
+                    atomicAdd(&g.drgb[3 * gi + 1], g_g);
+                    atomicAdd(&g.drgb[3 * gi + 2], g_b);
+                    atomicAdd(&g.dop[gi], g_o);
+                    atomicAdd(&g.dm2[2 * gi], g_mx);
+                    atomicAdd(&g.dm2[2 * gi + 1], g_my);
+                    atomicAdd(&g.dcon[3 * gi], g_ca);
+                    atomicAdd(&g.dcon[3 * gi + 1], g_cb);
+                    atomicAdd(&g.dcon[3 * gi + 2], g_cc);
+                }
+            }
+        }
+        __syncthreads();
+        be = bs;
+    }
+}
+
+// Adam element update (optimizer.cpp:32-43), same rounding sequence.
+__device__ __forceinline__ void adam_elem(float* p, float* m, float* v, float g, float lr, float b1, float b2,
+                                          float eps, float bc1, float bc2) {
+    const float mn = b1 * (*m) + (1.0f - b1) * g;
+    const float vn = b2 * (*v) + (1.0f - b2) * g * g;
+    *m = mn;
+    *v = vn;
+    const float mh = mn * bc1;
+    const float vh = vn * bc2;
+    *p = *p - lr * mh / (sqrtf(vh) + eps);
+}
+
+__device__ __forceinline__ void apply_update(const StepParams& sp, float* p, float* m, float* v, float g,
+                                             float lr) {
+    if (sp.use_adam) adam_elem(p, m, v, g, lr, sp.beta1, sp.beta2, sp.eps, sp.bc1, sp.bc2);
+    else *p = *p - lr * g;  // SGD, optimizer.cpp:14-25
+}
+
+// Preprocess backward (preprocessor_backward_cpu.cpp:8-645), optionally fused
+// with the optimiser update of all 59 parameters of the Gaussian.
+template <bool FUSED>
+__global__ void __launch_bounds__(kBlock) k_preprocess_bwd(const StepParams* __restrict__ spp, int N,
+                                                           ModelPtrs raw, AdamPtrs adam, ScreenPtrs s,
+                                                           RGradPtrs rg, GradPtrs gout, Control* ctrl) {
+    const int i = blockIdx.x * kBlock + threadIdx.x;
+    if (i >= N) return;
+    if (FUSED && (ctrl->status & (kStatusOverflow | kStatusTimeout))) return;
+    const StepParams& sp = *spp;
+    const gs3d_camera& cam = sp.cam;
+    const int mc = sp.max_coeffs;
+    const int mc3 = mc * 3;
+    float* shp = raw.sh + (size_t)mc3 * i;
+
+    float gp[3] = {0.f, 0.f, 0.f}, gs[3] = {0.f, 0.f, 0.f}, gq[4] = {0.f, 0.f, 0.f, 0.f}, gop = 0.f;
+    float geff[3] = {0.f, 0.f, 0.f};   // clamp-masked d_rgb (d_sh = basis * geff)
+    float basis[16];
+#pragma unroll
+    for (int k = 0; k < 16; k++) basis[k] = 0.f;
+    const bool vis = s.radius[i] > 0;
+    const float p[3] = {raw.pos[3 * i], raw.pos[3 * i + 1], raw.pos[3 * i + 2]};
+    const float rq[4] = {raw.rot[4 * i], raw.rot[4 * i + 1], raw.rot[4 * i + 2], raw.rot[4 * i + 3]};
+    const float rsc[3] = {raw.sc[3 * i], raw.sc[3 * i + 1], raw.sc[3 * i + 2]};
+    const float rop = raw.op[i];
+    float dm[2] = {0.f, 0.f}, dcn[3] = {0.f, 0.f, 0.f}, drgb[3] = {0.f, 0.f, 0.f}, dop = 0.f;
+    if (vis) {
+        dm[0] = rg.dm2[2 * i];
+        dm[1] = rg.dm2[2 * i + 1];
+        dcn[0] = rg.dcon[3 * i];
+        dcn[1] = rg.dcon[3 * i + 1];
+        dcn[2] = rg.dcon[3 * i + 2];
+        drgb[0] = rg.drgb[3 * i];
+        drgb[1] = rg.drgb[3 * i + 1];
+        drgb[2] = rg.drgb[3 * i + 2];
+        dop = rg.dop[i];
+    }
+    if (FUSED) {
+        // the accumulators start at zero for the next step's raster backward
+        rg.dm2[2 * i] = 0.f;
+        rg.dm2[2 * i + 1] = 0.f;
+        rg.dcon[3 * i] = 0.f;
+        rg.dcon[3 * i + 1] = 0.f;
+        rg.dcon[3 * i + 2] = 0.f;
+        rg.drgb[3 * i] = 0.f;
+        rg.drgb[3 * i + 1] = 0.f;
+        rg.drgb[3 * i + 2] = 0.f;
+        rg.dop[i] = 0.f;
+    }
+    if (vis) {
+        float sc[3], q[4], op;
+        activate_one(rsc, rq, rop, sc, q, &op);
+        const int deg = sp.sh_deg_model;
+        // ---- chain 2: SH (:8-203) ----
+        float d[3];
+        const float len = view_dir(p, cam.cam_pos, d);
+        const float x = d[0], y = d[1], z = d[2];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const float rawc = sh_channel(deg, shp, c, x, y, z);
+            geff[c] = drgb[c] * ((rawc + 0.5f >= 0.0f) ? 1.0f : 0.0f);
+        }
+        basis[0] = SH_C0;
+        if (deg > 0) {
+            basis[1] = -SH_C1 * y;
+            basis[2] = SH_C1 * z;
+            basis[3] = -SH_C1 * x;
+            if (deg > 1) {
+                const float xx = x * x, yy = y * y, zz = z * z, xy = x * y, yz = y * z, xz = x * z;
+                basis[4] = SH_C20 * xy;
+                basis[5] = SH_C21 * yz;
+                basis[6] = SH_C22 * (2.0f * zz - xx - yy);
+                basis[7] = SH_C23 * xz;
+                basis[8] = SH_C24 * (xx - yy);
+                if (deg > 2) {
+                    basis[9] = SH_C30 * y * (3.0f * xx - yy);
+                    basis[10] = SH_C31 * xy * z;
+                    basis[11] = SH_C32 * y * (4.0f * zz - xx - yy);
+                    basis[12] = SH_C33 * z * (2.0f * zz - 3.0f * xx - 3.0f * yy);
+                    basis[13] = SH_C34 * x * (4.0f * zz - xx - yy);
+                    basis[14] = SH_C35 * z * (xx - yy);
+                    basis[15] = SH_C36 * x * (xx - 3.0f * yy);
+                }
+            }
+            // d colour / d dir (:129-189)
+            float dd0[3] = {0.f, 0.f, 0.f}, dd1[3] = {0.f, 0.f, 0.f}, dd2[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                dd0[c] += -SH_C1 * shp[9 + c];
+                dd1[c] += -SH_C1 * shp[3 + c];
+                dd2[c] += SH_C1 * shp[6 + c];
+            }
+            if (deg > 1) {
+                const float xx = x * x, yy = y * y, zz = z * z;
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    const float s4 = shp[12 + c], s5 = shp[15 + c], s6 = shp[18 + c], s7 = shp[21 + c],
+                                s8 = shp[24 + c];
+                    dd0[c] += SH_C20 * y * s4 - 2.0f * SH_C22 * x * s6 + SH_C23 * z * s7 + 2.0f * SH_C24 * x * s8;
+                    dd1[c] += SH_C20 * x * s4 + SH_C21 * z * s5 - 2.0f * SH_C22 * y * s6 - 2.0f * SH_C24 * y * s8;
+                    dd2[c] += SH_C21 * y * s5 + 4.0f * SH_C22 * z * s6 + SH_C23 * x * s7;
+                }
+                if (deg > 2) {
+#pragma unroll
+                    for (int c = 0; c < 3; c++) {
+                        const float s9 = shp[27 + c], s10 = shp[30 + c], s11 = shp[33 + c], s12 = shp[36 + c];
+                        const float s13 = shp[39 + c], s14 = shp[42 + c], s15 = shp[45 + c];
+                        dd0[c] += SH_C30 * 6.0f * x * y * s9 + SH_C31 * y * z * s10 +
+                                  SH_C32 * (-2.0f * x * y) * s11 + SH_C33 * (-6.0f * x * z) * s12 +
+                                  SH_C34 * (4.0f * zz - 3.0f * xx - yy) * s13 + SH_C35 * 2.0f * x * z * s14 +
+                                  SH_C36 * (3.0f * xx - 3.0f * yy) * s15;
+                        dd1[c] += SH_C30 * (3.0f * xx - 3.0f * yy) * s9 + SH_C31 * x * z * s10 +
+                                  SH_C32 * (4.0f * zz - xx - 3.0f * yy) * s11 + SH_C33 * (-6.0f * y * z) * s12 +
+                                  SH_C34 * (-2.0f * x * y) * s13 - SH_C35 * 2.0f * y * z * s14 +
+                                  SH_C36 * (-6.0f * x * y) * s15;
+                        dd2[c] += SH_C31 * x * y * s10 + SH_C32 * 8.0f * y * z * s11 +
+                                  SH_C33 * (6.0f * zz - 3.0f * xx - 3.0f * yy) * s12 +
+                                  SH_C34 * 8.0f * x * z * s13 + SH_C35 * (xx - yy) * s14;
+                    }
+                }
+            }
+            float ddir0 = 0.f, ddir1 = 0.f, ddir2 = 0.f;
+#pragma unroll
+            for (int c = 0; c < 3; c++) ddir0 += geff[c] * dd0[c];
+#pragma unroll
+            for (int c = 0; c < 3; c++) ddir1 += geff[c] * dd1[c];
+#pragma unroll
+            for (int c = 0; c < 3; c++) ddir2 += geff[c] * dd2[c];
+            const float inv_len = 1.0f / len;
+            const float dot = ddir0 * x + ddir1 * y + ddir2 * z;
+            gp[0] += (ddir0 - x * dot) * inv_len;
+            gp[1] += (ddir1 - y * dot) * inv_len;
+            gp[2] += (ddir2 - z * dot) * inv_len;
+        }
+        // ---- chain 3: sigmoid (:231-232) ----
+        gop = dop * op * (1.0f - op);
+        // ---- forward recompute (ForwardCache, preprocessor_cpu.cpp:254-264) ----
+        float c3[6];
+        cov3d(sc, sp.cfg.scale_modifier, q, c3);
+        Ewa e;
+        ewa_setup(p, cam.view_matrix, sp.focal_x, sp.focal_y, cam.tan_fovx, cam.tan_fovy, e);
+        float c2[3];
+        cov2d(e, c3, c2);
+        c2[0] += 0.3f;
+        c2[2] += 0.3f;
+        const float det = c2[0] * c2[2] - c2[1] * c2[1];
+        float ph[4];
+        xform4x4(p, cam.viewproj_matrix, ph);
+        if (det != 0.0f) {
+            // ---- chain 1a: conic -> cov2D (:243-306) ----
+            const float a = c2[0], b = c2[1], c = c2[2];
+            const float inv_det = 1.0f / det;
+            const float id2 = inv_det * inv_det;
+            const float d_a = dcn[0] * (-c * c * id2) + dcn[1] * (b * c * id2) + dcn[2] * (-b * b * id2);
+            const float d_b = dcn[0] * (2.0f * b * c * id2) + dcn[1] * (-(a * c + b * b) * id2) +
+                              dcn[2] * (2.0f * a * b * id2);
+            const float d_c = dcn[0] * (-b * b * id2) + dcn[1] * (a * b * id2) + dcn[2] * (-a * a * id2);
+            // ---- chain 1b: cov2D -> cov3D (:316-380) ----
+            float dV[3][3];
+#pragma unroll
+            for (int k = 0; k < 3; k++)
+#pragma unroll
+                for (int j = 0; j < 3; j++)
+                    dV[k][j] = d_a * e.T[0][k] * e.T[0][j] + d_b * e.T[0][k] * e.T[1][j] +
+                               d_c * e.T[1][k] * e.T[1][j];
+            const float dcov[6] = {dV[0][0], dV[0][1] + dV[1][0], dV[0][2] + dV[2][0],
+                                   dV[1][1], dV[1][2] + dV[2][1], dV[2][2]};
+            // ---- chain 1c: cov3D -> M -> scale, R (:395-442) ----
+            const float mod = sp.cfg.scale_modifier;
+            const float sv[3] = {mod * sc[0], mod * sc[1], mod * sc[2]};
+            const float rr = q[0], xq = q[1], yq = q[2], zq = q[3];
+            float R[3][3], M[3][3];
+            quat_to_R(rr, xq, yq, zq, R);
+#pragma unroll
+            for (int ii = 0; ii < 3; ii++)
+#pragma unroll
+                for (int jj = 0; jj < 3; jj++) M[ii][jj] = sv[ii] * R[ii][jj];
+            float dR[3][3];
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                const float dM0 = 2.0f * dcov[0] * M[k][0] + dcov[1] * M[k][1] + dcov[2] * M[k][2];
+                const float dM1 = dcov[1] * M[k][0] + 2.0f * dcov[3] * M[k][1] + dcov[4] * M[k][2];
+                const float dM2 = dcov[2] * M[k][0] + dcov[4] * M[k][1] + 2.0f * dcov[5] * M[k][2];
+                float ds = 0.0f;
+                ds += dM0 * R[k][0];
+                ds += dM1 * R[k][1];
+                ds += dM2 * R[k][2];
+                dR[k][0] = dM0 * sv[k];
+                dR[k][1] = dM1 * sv[k];
+                dR[k][2] = dM2 * sv[k];
+                gs[k] = ds * mod * sc[k];
+            }
+            // ---- d R -> d unit quaternion (:455-498) ----
+            float dq0 = 0.f, dq1 = 0.f, dq2 = 0.f, dq3 = 0.f;
+            dq2 += dR[0][0] * (-4.0f * yq);
+            dq3 += dR[0][0] * (-4.0f * zq);
+            dq0 += dR[0][1] * 2.0f * zq; dq1 += dR[0][1] * 2.0f * yq;
+            dq2 += dR[0][1] * 2.0f * xq; dq3 += dR[0][1] * 2.0f * rr;
+            dq0 += dR[0][2] * (-2.0f * yq); dq1 += dR[0][2] * 2.0f * zq;
+            dq2 += dR[0][2] * (-2.0f * rr); dq3 += dR[0][2] * 2.0f * xq;
+            dq0 += dR[1][0] * (-2.0f * zq); dq1 += dR[1][0] * 2.0f * yq;
+            dq2 += dR[1][0] * 2.0f * xq; dq3 += dR[1][0] * (-2.0f * rr);
+            dq1 += dR[1][1] * (-4.0f * xq);
+            dq3 += dR[1][1] * (-4.0f * zq);
+            dq0 += dR[1][2] * 2.0f * xq; dq1 += dR[1][2] * 2.0f * rr;
+            dq2 += dR[1][2] * 2.0f * zq; dq3 += dR[1][2] * 2.0f * yq;
+            dq0 += dR[2][0] * 2.0f * yq; dq1 += dR[2][0] * 2.0f * zq;
+            dq2 += dR[2][0] * 2.0f * rr; dq3 += dR[2][0] * 2.0f * xq;
+            dq0 += dR[2][1] * (-2.0f * xq); dq1 += dR[2][1] * (-2.0f * rr);
+            dq2 += dR[2][1] * 2.0f * zq; dq3 += dR[2][1] * 2.0f * yq;
+            dq1 += dR[2][2] * (-4.0f * xq);
+            dq2 += dR[2][2] * (-4.0f * yq);
+            // ---- normalisation backward (:503-519) ----
+            float qlen = sqrtf(rq[0] * rq[0] + rq[1] * rq[1] + rq[2] * rq[2] + rq[3] * rq[3]);
+            if (qlen < 1e-12f) qlen = 1e-12f;
+            const float il = 1.0f / qlen;
+            const float dot = dq0 * rr + dq1 * xq + dq2 * yq + dq3 * zq;
+            gq[0] = (dq0 - rr * dot) * il;
+            gq[1] = (dq1 - xq * dot) * il;
+            gq[2] = (dq2 - yq * dot) * il;
+            gq[3] = (dq3 - zq * dot) * il;
+            // ---- path A: cov2D -> T -> J -> p_view -> position (:536-597) ----
+            const float V[3][3] = {{c3[0], c3[1], c3[2]}, {c3[1], c3[3], c3[4]}, {c3[2], c3[4], c3[5]}};
+            float VT[2][3];
+#pragma unroll
+            for (int col = 0; col < 2; col++)
+#pragma unroll
+                for (int row = 0; row < 3; row++) {
+                    float acc = 0.0f;
+#pragma unroll
+                    for (int k = 0; k < 3; k++) acc += V[row][k] * e.T[col][k];
+                    VT[col][row] = acc;
+                }
+            float dT[2][3];
+#pragma unroll
+            for (int qq = 0; qq < 3; qq++) {
+                dT[0][qq] = 2.0f * d_a * VT[0][qq] + d_b * VT[1][qq];
+                dT[1][qq] = d_b * VT[0][qq] + 2.0f * d_c * VT[1][qq];
+            }
+            float dJ[2][3];
+#pragma unroll
+            for (int col = 0; col < 2; col++)
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    float acc = 0.0f;
+#pragma unroll
+                    for (int row = 0; row < 3; row++) acc += dT[col][row] * e.W[k][row];
+                    dJ[col][k] = acc;
+                }
+            const float* t = e.t;
+            const float tz2 = t[2] * t[2];
+            const float tz3 = tz2 * t[2];
+            const float fx = sp.focal_x, fy = sp.focal_y;
+            float dt0 = dJ[0][2] * (-fx / tz2);
+            float dt1 = dJ[1][2] * (-fy / tz2);
+            const float dt2 = dJ[0][0] * (-fx / tz2) + dJ[1][1] * (-fy / tz2) +
+                              dJ[0][2] * (2.0f * fx * t[0] / tz3) + dJ[1][2] * (2.0f * fy * t[1] / tz3);
+            if (fabsf(e.txtz) >= e.limx) dt0 = 0.0f;
+            if (fabsf(e.tytz) >= e.limy) dt1 = 0.0f;
+            const float* vm = cam.view_matrix;
+#pragma unroll
+            for (int col = 0; col < 3; col++) {
+                gp[col] += dt0 * vm[col * 4 + 0];
+                gp[col] += dt1 * vm[col * 4 + 1];
+                gp[col] += dt2 * vm[col * 4 + 2];
+            }
+            // ---- chain 4: means2D -> ndc -> p_hom -> position (:609-643) ----
+        const float4 r0 = s.rec0[i];
+        const float dndx = dm[0] * (float)cam.width * 0.5f;
+        const float dndy = dm[1] * (float)cam.height * 0.5f;
+        const float wh = ph[3] + 1e-7f;
+        const float iw = 1.0f / wh;
+        const float ndc_x = (2.0f * r0.x + 1.0f) / (float)cam.width - 1.0f;
+        const float ndc_y = (2.0f * r0.y + 1.0f) / (float)cam.height - 1.0f;
+        const float dph0 = dndx * iw, dph1 = dndy * iw, dph2 = 0.0f;
+        const float dph3 = -(ndc_x * dndx + ndc_y * dndy) * iw;
+        const float* VP = cam.viewproj_matrix;
+#pragma unroll
+        for (int dim = 0; dim < 3; dim++)
+            gp[dim] += VP[dim * 4 + 0] * dph0 + VP[dim * 4 + 1] * dph1 + VP[dim * 4 + 2] * dph2 +
+                       VP[dim * 4 + 3] * dph3;
+        }
+    }
+    if (FUSED) {
+#pragma unroll
+        for (int k = 0; k < 3; k++)
+            apply_update(sp, &raw.pos[3 * i + k], &adam.m_pos[3 * i + k], &adam.v_pos[3 * i + k], gp[k], sp.lr_pos);
+#pragma unroll
+        for (int k = 0; k < 3; k++)
+            apply_update(sp, &raw.sc[3 * i + k], &adam.m_sc[3 * i + k], &adam.v_sc[3 * i + k], gs[k], sp.lr_scale);
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+            apply_update(sp, &raw.rot[4 * i + k], &adam.m_rot[4 * i + k], &adam.v_rot[4 * i + k], gq[k], sp.lr_rot);
+        apply_update(sp, &raw.op[i], &adam.m_op[i], &adam.v_op[i], gop, sp.lr_opac);
+        float* msh = adam.m_sh + (size_t)mc3 * i;
+        float* vsh = adam.v_sh + (size_t)mc3 * i;
+        for (int k = 0; k < mc; k++) {
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                const float gsh = k < 16 ? basis[k] * geff[c] : 0.0f;
+                apply_update(sp, &shp[3 * k + c], &msh[3 * k + c], &vsh[3 * k + c], gsh, sp.lr_sh);
+            }
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < 3; k++) gout.g_pos[3 * i + k] = gp[k];
+#pragma unroll
+        for (int k = 0; k < 3; k++) gout.g_sc[3 * i + k] = gs[k];
+#pragma unroll
+        for (int k = 0; k < 4; k++) gout.g_rot[4 * i + k] = gq[k];
+        gout.g_op[i] = gop;
+        float* gsh = gout.g_sh + (size_t)mc3 * i;
+        for (int k = 0; k < mc; k++)
+#pragma unroll
+            for (int c = 0; c < 3; c++) gsh[3 * k + c] = k < 16 ? basis[k] * geff[c] : 0.0f;
+    }
+}
+
+// Stand-alone optimiser step over gradient arrays (optimizer.cpp:9-101).
+__global__ void k_optimizer(const StepParams* __restrict__ spp, long long n_pos, long long n_rot, long long n_sh,
+                            long long n_op, ModelPtrs raw, AdamPtrs adam, GradPtrs g) {
+    const StepParams& sp = *spp;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n_pos; i += stride) {
+        apply_update(sp, &raw.pos[i], &adam.m_pos[i], &adam.v_pos[i], g.g_pos[i], sp.lr_pos);
+        apply_update(sp, &raw.sc[i], &adam.m_sc[i], &adam.v_sc[i], g.g_sc[i], sp.lr_scale);
+    }
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n_rot; i += stride)
+        apply_update(sp, &raw.rot[i], &adam.m_rot[i], &adam.v_rot[i], g.g_rot[i], sp.lr_rot);
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n_sh; i += stride)
+        apply_update(sp, &raw.sh[i], &adam.m_sh[i], &adam.v_sh[i], g.g_sh[i], sp.lr_sh);
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n_op; i += stride)
+        apply_update(sp, &raw.op[i], &adam.m_op[i], &adam.v_op[i], g.g_op[i], sp.lr_opac);
+}
+
+inline int blocks_for(long long n, int t) { return (int)((n + t - 1) / t); }
+
+}  // namespace
+
+cudaError_t launch_preprocess_plain(cudaStream_t st, const StepParams* sp, int N, bool train, bool cache,
+                                    ModelPtrs m, ScreenPtrs s, PairPtrs pr, Control* ctrl) {
+    if (N <= 0) return cudaSuccess;
+    const int grid = blocks_for(N, kBlock);
+    if (train) {
+        if (cache) k_preprocess<true, true><<<grid, kBlock, 0, st>>>(sp, N, m, s, pr, ctrl);
+        else k_preprocess<true, false><<<grid, kBlock, 0, st>>>(sp, N, m, s, pr, ctrl);
+    } else {
+        if (cache) k_preprocess<false, true><<<grid, kBlock, 0, st>>>(sp, N, m, s, pr, ctrl);
+        else k_preprocess<false, false><<<grid, kBlock, 0, st>>>(sp, N, m, s, pr, ctrl);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bin_arrays(cudaStream_t st, const StepParams* sp, int N, ScreenArrays a, PairPtrs pr,
+                              Control* ctrl) {
+    if (N <= 0) return cudaSuccess;
+    k_bin_arrays<<<blocks_for(N, kBlock), kBlock, 0, st>>>(sp, N, a, pr, ctrl);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_export_screen(cudaStream_t st, int N, ScreenPtrs s, ScreenArrays a) {
+    if (N <= 0) return cudaSuccess;
+    k_export_screen<<<blocks_for(N, 256), 256, 0, st>>>(N, s, a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_raster_fwd_plain(cudaStream_t st, const StepParams* sp, int num_tiles, bool fused_loss,
+                                    const unsigned* ranges, const unsigned* vals, ScreenPtrs s, PixelPtrs px,
+                                    Control* ctrl) {
+    if (num_tiles <= 0) return cudaSuccess;
+    if (fused_loss) k_raster_fwd<true><<<num_tiles, kBlock, 0, st>>>(sp, ranges, vals, s, px, ctrl);
+    else k_raster_fwd<false><<<num_tiles, kBlock, 0, st>>>(sp, ranges, vals, s, px, ctrl);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_raster_bwd_plain(cudaStream_t st, const StepParams* sp, int num_tiles, bool from_sign,
+                                    const unsigned* ranges, const unsigned* vals, ScreenPtrs s, PixelPtrs px,
+                                    RGradPtrs g, Control* ctrl) {
+    if (num_tiles <= 0) return cudaSuccess;
+    if (from_sign) k_raster_bwd<true><<<num_tiles, kBlock, 0, st>>>(sp, ranges, vals, s, px, g, ctrl);
+    else k_raster_bwd<false><<<num_tiles, kBlock, 0, st>>>(sp, ranges, vals, s, px, g, ctrl);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_preprocess_bwd_plain(cudaStream_t st, const StepParams* sp, int N, bool fused_adam,
+                                        ModelPtrs raw, AdamPtrs adam, ScreenPtrs s, RGradPtrs rg, GradPtrs gout,
+                                        Control* ctrl) {
+    if (N <= 0) return cudaSuccess;
+    const int grid = blocks_for(N, kBlock);
+    if (fused_adam) k_preprocess_bwd<true><<<grid, kBlock, 0, st>>>(sp, N, raw, adam, s, rg, gout, ctrl);
+    else k_preprocess_bwd<false><<<grid, kBlock, 0, st>>>(sp, N, raw, adam, s, rg, gout, ctrl);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_optimizer_plain(cudaStream_t st, const StepParams* sp, int N, int mc3, ModelPtrs raw,
+                                   AdamPtrs adam, GradPtrs g) {
+    if (N <= 0) return cudaSuccess;
+    const long long n_sh = (long long)N * mc3;
+    k_optimizer<<<4 * 148, 256, 0, st>>>(sp, 3LL * N, 4LL * N, n_sh, (long long)N, raw, adam, g);
+    return cudaGetLastError();
+}
+
+}  // namespace gs3d

@@ -1,0 +1,222 @@
+// sort.cu -- stable LSD radix sort of (tile|depth key, Gaussian index) pairs
+// and tile-range identification, replacing SorterCPU::sort
+// (harmonyos_3dgs src/cpu/sorter_cpu.cpp:6-44).
+//
+// Design (one-sweep, after Adinets & Merrill, "Onesweep: A Faster Least
+// Significant Digit Radix Sort for GPUs", 2022):
+//   k_radix_hist  one read of the keys counts the 8-bit digits of every pass
+//                 (warp-aggregated with __match_any_sync).
+//   k_onesweep    one launch per pass.  A CTA takes the next 4096-key tile by
+//                 ticket, ranks its keys per warp with __match_any_sync /
+//                 popc, publishes its per-digit counts and finds its global
+//                 per-digit offsets by decoupled look-back (bounded waits),
+//                 reorders the tile in shared memory and writes it out in
+//                 digit-contiguous runs.  Ranks follow input order, so the sort
+//                 is stable: equal keys keep the Gaussian order of the binning,
+//                 i.e. the result is the (key, value)-sorted order.
+//   k_ranges      (start, end) per tile from the sorted keys
+//                 (sorter_cpu.cpp:28-43).
+// Only the significant key bits are sorted: 32 depth bits plus
+// ceil(log2(num_tiles)) tile bits.
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace gs3d {
+namespace {
+
+constexpr int kHistThreads = 512;
+
+__global__ void __launch_bounds__(kHistThreads) k_radix_hist(const unsigned long long* __restrict__ keys,
+                                                             unsigned long long capacity, int passes,
+                                                             Control* ctrl) {
+    __shared__ unsigned s_h[kMaxPasses * 256];
+    for (int e = threadIdx.x; e < passes * 256; e += blockDim.x) s_h[e] = 0;
+    __syncthreads();
+    const unsigned long long P = min(ctrl->total_pairs, capacity);
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    const unsigned lane = threadIdx.x & 31;
+    for (unsigned long long base = (unsigned long long)blockIdx.x * blockDim.x; base < P; base += stride) {
+        const unsigned long long i = base + threadIdx.x;
+        const bool valid = i < P;
+        const unsigned mask = __ballot_sync(0xffffffffu, valid);
+        if (valid) {
+            const unsigned long long key = keys[i];
+            for (int p = 0; p < passes; p++) {
+                const unsigned d = (unsigned)(key >> (8 * p)) & 255u;
+                const unsigned peers = __match_any_sync(mask, d);
+                if (lane == (unsigned)(__ffs(peers) - 1)) atomicAdd(&s_h[p * 256 + d], (unsigned)__popc(peers));
+            }
+        }
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < passes * 256; e += blockDim.x)
+        if (s_h[e]) atomicAdd(&ctrl->hist[e >> 8][e & 255], s_h[e]);
+}
+
+// Shared memory of one onesweep CTA (dynamic, ~60 KB).
+struct SweepShared {
+    unsigned long long keys[kSortTile];
+    unsigned vals[kSortTile];
+    unsigned whist[kSortThreads / 32][256];   // per-warp digit counts, then per-warp prefixes
+    unsigned long long gbase[256];            // global output offset of this tile's first key of digit d
+    unsigned dprefix[256];                    // tile-local exclusive prefix over digits
+    unsigned long long scan[8];
+    int tile;
+};
+
+// Exclusive scan over the 256 threads of one 64-bit value each.
+__device__ __forceinline__ unsigned long long block_exclusive_scan64(unsigned long long v, unsigned long long* s_w) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned long long x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long n = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += n;
+    }
+    if (lane == 31) s_w[warp] = x;
+    __syncthreads();
+    unsigned long long add = 0;
+    for (int w = 0; w < warp; w++) add += s_w[w];
+    __syncthreads();
+    return x - v + add;
+}
+
+__global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const StepParams* __restrict__ sp,
+                                                              const unsigned long long* __restrict__ kin,
+                                                              const unsigned* __restrict__ vin,
+                                                              unsigned long long* __restrict__ kout,
+                                                              unsigned* __restrict__ vout,
+                                                              unsigned long long capacity, int pass,
+                                                              unsigned long long* desc, Control* ctrl) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SweepShared& sm = *reinterpret_cast<SweepShared*>(smem_raw);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int shift = 8 * pass;
+    const unsigned long long P = min(ctrl->total_pairs, capacity);
+    if (tid == 0) sm.tile = (int)atomicAdd(&ctrl->tickets[1 + pass], 1u);
+    for (int e = tid; e < (kSortThreads / 32) * 256; e += kSortThreads) (&sm.whist[0][0])[e] = 0;
+    __syncthreads();
+    const int t = sm.tile;
+    const unsigned long long base = (unsigned long long)t * kSortTile;
+    if (base >= P) return;
+
+    unsigned long long key[kSortItems];
+    unsigned val[kSortItems];
+    unsigned rank[kSortItems];
+#pragma unroll
+    for (int it = 0; it < kSortItems; it++) {
+        const unsigned long long idx = base + (unsigned long long)(warp * 32 * kSortItems + it * 32 + lane);
+        const bool valid = idx < P;
+        key[it] = valid ? kin[idx] : ~0ull;   // sentinel: digit 255, ranks after every real key
+        val[it] = valid ? vin[idx] : 0u;
+    }
+    const unsigned lt_mask = (1u << lane) - 1u;
+#pragma unroll
+    for (int it = 0; it < kSortItems; it++) {
+        const unsigned d = (unsigned)(key[it] >> shift) & 255u;
+        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        const unsigned prior = sm.whist[warp][d];
+        __syncwarp();
+        if (lane == (unsigned)(__ffs(peers) - 1)) sm.whist[warp][d] = prior + (unsigned)__popc(peers);
+        __syncwarp();
+        rank[it] = prior + (unsigned)__popc(peers & lt_mask);
+    }
+    __syncthreads();
+    // thread d owns digit d: per-warp exclusive prefixes and the tile count
+    const unsigned d = (unsigned)tid;
+    unsigned run = 0;
+#pragma unroll
+    for (int w = 0; w < kSortThreads / 32; w++) {
+        const unsigned c = sm.whist[w][d];
+        sm.whist[w][d] = run;
+        run += c;
+    }
+    // global offset of digit d for this tile: all smaller digits everywhere,
+    // plus digit d in the tiles before this one (decoupled look-back)
+    const unsigned long long hist_d = ctrl->hist[pass][d];
+    const unsigned long long digit_start = block_exclusive_scan64(hist_d, sm.scan);
+    const unsigned long long tile_excl =
+        lookback_exclusive_strided(desc, t, 256, (int)d, (unsigned long long)run, &ctrl->status, sp->spin_limit);
+    sm.gbase[d] = digit_start + tile_excl;
+    sm.dprefix[d] = (unsigned)block_exclusive_scan64((unsigned long long)run, sm.scan);
+    __syncthreads();
+#pragma unroll
+    for (int it = 0; it < kSortItems; it++) {
+        const unsigned dd = (unsigned)(key[it] >> shift) & 255u;
+        const unsigned pos = sm.dprefix[dd] + sm.whist[warp][dd] + rank[it];
+        sm.keys[pos] = key[it];
+        sm.vals[pos] = val[it];
+    }
+    __syncthreads();
+    const int n_valid = (int)min((unsigned long long)kSortTile, P - base);
+    for (int j = tid; j < n_valid; j += kSortThreads) {
+        const unsigned long long k = sm.keys[j];
+        const unsigned dd = (unsigned)(k >> shift) & 255u;
+        const unsigned long long out = sm.gbase[dd] + (unsigned long long)(j - (int)sm.dprefix[dd]);
+        kout[out] = k;
+        vout[out] = sm.vals[j];
+    }
+}
+
+__global__ void k_ranges(const unsigned long long* __restrict__ keys, unsigned long long capacity,
+                         unsigned* __restrict__ ranges, Control* ctrl) {
+    const unsigned long long P = min(ctrl->total_pairs, capacity);
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < P; i += stride) {
+        const unsigned t = (unsigned)(keys[i] >> 32);
+        if (i == 0 || (unsigned)(keys[i - 1] >> 32) != t) ranges[2 * t] = (unsigned)i;
+        if (i == P - 1 || (unsigned)(keys[i + 1] >> 32) != t) ranges[2 * t + 1] = (unsigned)(i + 1);
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_radix_sort(cudaStream_t st, const StepParams* sp, int passes, unsigned long long capacity,
+                              unsigned long long* keys0, unsigned* vals0, unsigned long long* keys1,
+                              unsigned* vals1, unsigned long long* desc, unsigned long long desc_stride,
+                              Control* ctrl, int* which) {
+    *which = 0;
+    if (capacity == 0 || passes <= 0) return cudaSuccess;
+    static bool attr_set = false;
+    const int smem = (int)sizeof(SweepShared);
+    if (!attr_set) {
+        cudaError_t e = cudaFuncSetAttribute(k_onesweep, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return e;
+        attr_set = true;
+    }
+    k_radix_hist<<<2 * 148, kHistThreads, 0, st>>>(keys0, capacity, passes, ctrl);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const unsigned long long tiles = (capacity + kSortTile - 1) / kSortTile;
+    unsigned long long* kin = keys0;
+    unsigned* vin = vals0;
+    unsigned long long* kout = keys1;
+    unsigned* vout = vals1;
+    for (int p = 0; p < passes; p++) {
+        k_onesweep<<<(unsigned)tiles, kSortThreads, smem, st>>>(sp, kin, vin, kout, vout, capacity, p,
+                                                                desc + (unsigned long long)p * desc_stride,
+                                                                ctrl);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        unsigned long long* tk = kin;
+        kin = kout;
+        kout = tk;
+        unsigned* tv = vin;
+        vin = vout;
+        vout = tv;
+    }
+    *which = passes & 1;
+    return cudaSuccess;
+}
+
+cudaError_t launch_tile_ranges(cudaStream_t st, unsigned long long capacity, const unsigned long long* keys_sorted,
+                               unsigned* ranges, Control* ctrl) {
+    if (capacity == 0) return cudaSuccess;
+    k_ranges<<<4 * 148, 256, 0, st>>>(keys_sorted, capacity, ranges, ctrl);
+    return cudaGetLastError();
+}
+
+}  // namespace gs3d

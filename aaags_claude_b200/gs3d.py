@@ -1,0 +1,290 @@
+"""Python binding of the gs3dc_* C ABI (include/gs3d_cuda.h) over ctypes.
+
+The product path is libgs3d_cuda.so (CUDA, sm_100a).  Nothing here computes on
+the CPU: if the library or a B200-class device is missing, ``Context`` raises.
+
+    ctx = Context(0)
+    ctx.set_raw_params(scene)                 # RawGaussianParams -> device
+    loss = ctx.train_step(cam, gt, cfg, tcfg, iteration)   # Trainer::step
+    img = ctx.render(cam, cfg, gaussians=...) # Renderer::render
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import scenes as S
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libgs3d_cuda.so")
+
+OK = 0
+ERR_INVALID_ARG, ERR_CUDA, ERR_PAIR_OVERFLOW, ERR_DEVICE_TIMEOUT, ERR_NO_MODEL, ERR_OOM, ERR_STATE = range(1, 8)
+OPT_PAIR_CAPACITY, OPT_USE_GRAPH, OPT_FORM, OPT_SPIN_LIMIT = 1, 2, 3, 4
+STAT_TOTAL_PAIRS, STAT_PAIR_CAPACITY, STAT_KERNELS_LAST, STAT_SORT_PASSES, STAT_GRAPH_REPLAYS, STAT_ADAM_STEP = range(1, 7)
+FORM_PLAIN_FP32 = 0
+
+_f = ctypes.POINTER(ctypes.c_float)
+_i = ctypes.POINTER(ctypes.c_int)
+
+
+class ScreenArrays(ctypes.Structure):
+    """Layout of ``gs3dc_screen_arrays``."""
+
+    _fields_ = [(n, _f) for n in ("means2D", "depths", "conics", "opacities_2d", "rgb")] + \
+               [("radii", _i), ("tiles_touched", _i)] + \
+               [(n, _f) for n in ("cov3D", "p_view", "p_hom_w", "cov2D", "cov2D_det")]
+
+
+class Gs3dError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"gs3dc status {status}: {message}")
+        self.status = status
+
+
+_LIB = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Loads libgs3d_cuda.so; raises if it has not been built."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} is missing: run `python -m aaags_claude_b200.build`")
+    L = ctypes.CDLL(path)
+    vp, i64 = ctypes.c_void_p, ctypes.c_int64
+    sig = {
+        "gs3dc_create": ([ctypes.c_int, ctypes.POINTER(vp)], ctypes.c_int),
+        "gs3dc_destroy": ([vp], None),
+        "gs3dc_last_error": ([vp], ctypes.c_char_p),
+        "gs3dc_status_string": ([ctypes.c_int], ctypes.c_char_p),
+        "gs3dc_get_stream": ([vp, ctypes.POINTER(vp)], ctypes.c_int),
+        "gs3dc_set_option": ([vp, ctypes.c_int, i64], ctypes.c_int),
+        "gs3dc_get_stat": ([vp, ctypes.c_int, ctypes.POINTER(i64)], ctypes.c_int),
+        "gs3dc_set_gaussians": ([vp, vp], ctypes.c_int),
+        "gs3dc_set_raw_params": ([vp, vp], ctypes.c_int),
+        "gs3dc_get_raw_params": ([vp, vp], ctypes.c_int),
+        "gs3dc_preprocess": ([vp, vp, vp, vp], ctypes.c_int),
+        "gs3dc_bin": ([vp, ctypes.c_int, vp, vp, vp, ctypes.POINTER(i64), vp, vp], ctypes.c_int),
+        "gs3dc_sort": ([vp, vp, vp, vp], ctypes.c_int),
+        "gs3dc_sort_pairs": ([vp, i64, vp, vp, ctypes.c_int, vp, vp, vp], ctypes.c_int),
+        "gs3dc_rasterize": ([vp, vp, vp, vp, vp, vp], ctypes.c_int),
+        "gs3dc_render": ([vp, vp, vp, vp, vp], ctypes.c_int),
+        "gs3dc_raster_backward": ([vp, vp, vp, vp, vp, vp, vp, vp], ctypes.c_int),
+        "gs3dc_preprocess_backward": ([vp, vp, vp, vp, vp, vp, vp, vp], ctypes.c_int),
+        "gs3dc_optimizer_step": ([vp, vp, ctypes.c_int], ctypes.c_int),
+        "gs3dc_train_step": ([vp, vp, vp, ctypes.c_int, vp, vp, ctypes.c_int, vp], ctypes.c_int),
+        "gs3dc_synchronize": ([vp], ctypes.c_int),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
+    _LIB = L
+    return L
+
+
+def exported_symbols() -> list[str]:
+    """The gs3dc_* names include/gs3d_cuda.h declares."""
+    import re
+    hdr = os.path.join(os.path.dirname(PKG), "include", "gs3d_cuda.h")
+    txt = open(hdr).read()
+    return sorted(set(re.findall(r"\b(gs3dc_[a-z_0-9]+)\s*\(", txt)))
+
+
+def _p(a):
+    return None if a is None else ctypes.c_void_p(a.ctypes.data)
+
+
+def _ref(s):
+    return None if s is None else ctypes.cast(ctypes.pointer(s), ctypes.c_void_p)
+
+
+class Context:
+    """One gs3dc context: a CUDA stream and the device buffers of the path."""
+
+    def __init__(self, device: int = 0):
+        self.L = load_library()
+        h = ctypes.c_void_p()
+        rc = self.L.gs3dc_create(device, ctypes.byref(h))
+        if rc != OK:
+            raise Gs3dError(rc, f"gs3dc_create(device={device}) failed: "
+                                f"{self.L.gs3dc_status_string(rc).decode()} (needs an sm_100 GPU)")
+        self.h = h
+        self._model = None
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.gs3dc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _chk(self, rc: int):
+        if rc != OK:
+            raise Gs3dError(rc, self.L.gs3dc_last_error(self.h).decode())
+
+    # ---- context ----
+    def stream_handle(self) -> int:
+        s = ctypes.c_void_p()
+        self._chk(self.L.gs3dc_get_stream(self.h, ctypes.byref(s)))
+        return int(s.value or 0)
+
+    def set_option(self, opt: int, value: int):
+        self._chk(self.L.gs3dc_set_option(self.h, opt, int(value)))
+
+    def stat(self, which: int) -> int:
+        v = ctypes.c_int64()
+        self._chk(self.L.gs3dc_get_stat(self.h, which, ctypes.byref(v)))
+        return int(v.value)
+
+    def synchronize(self):
+        self._chk(self.L.gs3dc_synchronize(self.h))
+
+    # ---- model ----
+    def set_gaussians(self, scene: S.Scene, act: dict):
+        """Uploads an activated model (act: positions/scales/rotations/sh_coeffs/opacities)."""
+        g = S.GaussianData()
+        g.count, g.sh_degree, g.max_coeffs = scene.count, scene.sh_degree, scene.max_coeffs
+        for k in ("positions", "sh_coeffs", "scales", "rotations", "opacities"):
+            setattr(g, k, S.fptr(np.ascontiguousarray(act[k], np.float32)))
+        self._keep = (act, g)
+        self._chk(self.L.gs3dc_set_gaussians(self.h, _ref(g)))
+        self._model = ("act", scene.count, scene.max_coeffs)
+
+    def set_raw_params(self, scene: S.Scene):
+        r = scene.raw_struct()
+        self._chk(self.L.gs3dc_set_raw_params(self.h, _ref(r)))
+        self._model = ("raw", scene.count, scene.max_coeffs)
+
+    def get_raw_params(self, scene: S.Scene):
+        """Copies the device parameters into scene's arrays (in place)."""
+        r = scene.raw_struct()
+        self._chk(self.L.gs3dc_get_raw_params(self.h, _ref(r)))
+        return scene
+
+    # ---- stages ----
+    def preprocess(self, cam, cfg, want_cache: bool = False) -> dict:
+        n = self._model[1]
+        out = dict(means2D=np.zeros(2 * n, np.float32), depths=np.zeros(n, np.float32),
+                   conics=np.zeros(3 * n, np.float32), opacities_2d=np.zeros(n, np.float32),
+                   rgb=np.zeros(3 * n, np.float32), radii=np.zeros(n, np.int32),
+                   tiles_touched=np.zeros(n, np.int32))
+        if want_cache:
+            out.update(cov3D=np.zeros(6 * n, np.float32), p_view=np.zeros(3 * n, np.float32),
+                       p_hom_w=np.zeros(n, np.float32), cov2D=np.zeros(3 * n, np.float32),
+                       cov2D_det=np.zeros(n, np.float32))
+        sa = ScreenArrays()
+        for k, v in out.items():
+            setattr(sa, k, v.ctypes.data_as(_i if v.dtype == np.int32 else _f))
+        self._chk(self.L.gs3dc_preprocess(self.h, _ref(cam), _ref(cfg), _ref(sa)))
+        return out
+
+    def bin(self, cam, cfg, arrays: dict | None = None):
+        """TileBinner::bin: (total_pairs, keys_unsorted, values_unsorted).
+
+        Without ``arrays`` the pairs of the last preprocess are returned; with
+        host arrays (means2D, depths, radii, tiles_touched) those are binned.
+        """
+        P = ctypes.c_int64()
+        if arrays is not None:
+            sa = ScreenArrays()
+            keep = {}
+            for k in ("means2D", "depths", "radii", "tiles_touched"):
+                v = np.ascontiguousarray(arrays[k], np.int32 if k in ("radii", "tiles_touched") else np.float32)
+                keep[k] = v
+                setattr(sa, k, v.ctypes.data_as(_i if v.dtype == np.int32 else _f))
+            n = int(keep["radii"].shape[0])
+            total = int(keep["tiles_touched"].astype(np.int64).sum())
+            keys = np.zeros(max(total, 1), np.uint64)
+            vals = np.zeros(max(total, 1), np.uint32)
+            self._chk(self.L.gs3dc_bin(self.h, n, _ref(sa), _ref(cam), _ref(cfg), ctypes.byref(P), _p(keys), _p(vals)))
+            return int(P.value), keys[:P.value], vals[:P.value]
+        n = self._model[1]
+        self._chk(self.L.gs3dc_bin(self.h, n, None, _ref(cam), _ref(cfg), ctypes.byref(P), None, None))
+        keys = np.zeros(max(P.value, 1), np.uint64)
+        vals = np.zeros(max(P.value, 1), np.uint32)
+        self._chk(self.L.gs3dc_bin(self.h, n, None, _ref(cam), _ref(cfg), ctypes.byref(P), _p(keys), _p(vals)))
+        return int(P.value), keys[:P.value], vals[:P.value]
+
+    def sort(self, total_pairs: int, num_tiles: int):
+        keys = np.zeros(max(total_pairs, 1), np.uint64)
+        vals = np.zeros(max(total_pairs, 1), np.uint32)
+        ranges = np.zeros(2 * num_tiles, np.uint32)
+        self._chk(self.L.gs3dc_sort(self.h, _p(keys), _p(vals), _p(ranges)))
+        return keys[:total_pairs], vals[:total_pairs], ranges
+
+    def sort_pairs(self, keys: np.ndarray, vals: np.ndarray, num_tiles: int):
+        keys = np.ascontiguousarray(keys, np.uint64)
+        vals = np.ascontiguousarray(vals, np.uint32)
+        P = int(keys.shape[0])
+        ko = np.zeros(max(P, 1), np.uint64)
+        vo = np.zeros(max(P, 1), np.uint32)
+        ranges = np.zeros(2 * num_tiles, np.uint32)
+        self._chk(self.L.gs3dc_sort_pairs(self.h, P, _p(keys) if P else None, _p(vals) if P else None,
+                                          int(num_tiles), _p(ko), _p(vo), _p(ranges)))
+        return ko[:P], vo[:P], ranges
+
+    def rasterize(self, cam, cfg):
+        npx = cam.width * cam.height
+        img = np.zeros(3 * npx, np.float32)
+        T = np.zeros(npx, np.float32)
+        nc = np.zeros(npx, np.int32)
+        self._chk(self.L.gs3dc_rasterize(self.h, _ref(cam), _ref(cfg), _p(img), _p(T), _p(nc)))
+        return img, T, nc
+
+    def render(self, cam, cfg) -> np.ndarray:
+        img = np.zeros(3 * cam.width * cam.height, np.float32)
+        self._chk(self.L.gs3dc_render(self.h, None, _ref(cam), _ref(cfg), _p(img)))
+        return img
+
+    def raster_backward(self, cam, cfg, d_image: np.ndarray) -> dict:
+        n = self._model[1]
+        out = dict(d_means2D=np.zeros(2 * n, np.float32), d_conics=np.zeros(3 * n, np.float32),
+                   d_rgb=np.zeros(3 * n, np.float32), d_opac=np.zeros(n, np.float32))
+        d = np.ascontiguousarray(d_image, np.float32).reshape(-1)
+        self._chk(self.L.gs3dc_raster_backward(self.h, _ref(cam), _ref(cfg), _p(d), _p(out["d_means2D"]),
+                                               _p(out["d_conics"]), _p(out["d_rgb"]), _p(out["d_opac"])))
+        return out
+
+    def preprocess_backward(self, cam, cfg) -> dict:
+        n, mc = self._model[1], self._model[2]
+        out = dict(g_pos=np.zeros(3 * n, np.float32), g_sc=np.zeros(3 * n, np.float32),
+                   g_rot=np.zeros(4 * n, np.float32), g_sh=np.zeros(3 * mc * n, np.float32),
+                   g_op=np.zeros(n, np.float32))
+        self._chk(self.L.gs3dc_preprocess_backward(self.h, _ref(cam), _ref(cfg), *[_p(out[k]) for k in
+                                                   ("g_pos", "g_sc", "g_rot", "g_sh", "g_op")]))
+        return out
+
+    def optimizer_step(self, tcfg, iteration: int):
+        self._chk(self.L.gs3dc_optimizer_step(self.h, _ref(tcfg), int(iteration)))
+
+    def train_step(self, cam, gt, cfg, tcfg, iteration: int, want_loss: bool = True,
+                   gt_device_ptr: int | None = None) -> float | None:
+        """Trainer::step on the device-resident parameters.
+
+        gt is a host float32 array (H*W*3) or, with gt_device_ptr, ignored in
+        favour of that device address.
+        """
+        loss = ctypes.c_float()
+        if gt_device_ptr is not None:
+            gptr, on_dev = ctypes.c_void_p(int(gt_device_ptr)), 1
+        else:
+            gt = np.ascontiguousarray(gt, np.float32)
+            gptr, on_dev = _p(gt), 0
+        self._chk(self.L.gs3dc_train_step(self.h, _ref(cam), gptr, on_dev, _ref(cfg), _ref(tcfg), int(iteration),
+                                          ctypes.byref(loss) if want_loss else None))
+        return float(loss.value) if want_loss else None

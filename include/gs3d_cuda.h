@@ -1,0 +1,179 @@
+/*
+ * gs3d_cuda.h -- C ABI of the B200 (sm_100a) 3D Gaussian Splatting hot path.
+ *
+ * One context owns one CUDA stream on one device and every device buffer of
+ * the path (model, Adam moments, screen-space records, tile/depth pairs, tile
+ * ranges, per-pixel state).  Calls are stream-ordered and synchronous towards
+ * the caller: a call that fills host arrays returns once they are filled.
+ * A context is not thread-safe; use one per host thread.
+ *
+ * Every entry point returns a status (GS3DC_OK == 0).  gs3dc_last_error()
+ * gives the message of the last failure.  There is no CPU fallback: without a
+ * usable sm_100 device gs3dc_create fails.
+ *
+ * The structs are the reference's own layouts (gs3d_types.h).  Each entry point
+ * names the harmonyos_3dgs interface it stands in for; paths are relative to
+ * the harmonyos_3dgs project root.
+ */
+#ifndef GS3D_CUDA_H
+#define GS3D_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include "gs3d_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct gs3dc_ctx gs3dc_ctx;
+
+/* ---- status codes ---- */
+#define GS3DC_OK                 0
+#define GS3DC_ERR_INVALID_ARG    1  /* bad size, NULL where required, unsupported config */
+#define GS3DC_ERR_CUDA           2  /* a CUDA runtime call failed (message has details) */
+#define GS3DC_ERR_PAIR_OVERFLOW  3  /* more tile pairs than the pair capacity could grow to */
+#define GS3DC_ERR_DEVICE_TIMEOUT 4  /* a bounded device-side wait gave up (no hang) */
+#define GS3DC_ERR_NO_MODEL       5  /* the call needs a model that was not uploaded */
+#define GS3DC_ERR_OUT_OF_MEMORY  6  /* device allocation failed */
+#define GS3DC_ERR_STATE          7  /* the call needs a stage that has not run */
+
+/* ---- options (gs3dc_set_option) ---- */
+#define GS3DC_OPT_PAIR_CAPACITY  1  /* minimum tile-pair capacity to preallocate */
+#define GS3DC_OPT_USE_GRAPH      2  /* 1: gs3dc_train_step replays a captured CUDA graph (default 1) */
+#define GS3DC_OPT_FORM           3  /* GS3DC_FORM_* precision form of gs3dc_train_step / gs3dc_render */
+#define GS3DC_OPT_SPIN_LIMIT     4  /* iterations before a device-side wait gives up (test hook) */
+
+#define GS3DC_FORM_PLAIN_FP32    0  /* FP32 everywhere, no FMA contraction: parity form */
+
+/* ---- statistics (gs3dc_get_stat) ---- */
+#define GS3DC_STAT_TOTAL_PAIRS    1  /* tile pairs of the last forward */
+#define GS3DC_STAT_PAIR_CAPACITY  2
+#define GS3DC_STAT_KERNELS_LAST   3  /* kernels launched by the last train step / render */
+#define GS3DC_STAT_SORT_PASSES    4  /* radix passes of the last sort */
+#define GS3DC_STAT_GRAPH_REPLAYS  5
+#define GS3DC_STAT_ADAM_STEP      6  /* Adam step counter (AdamOptimizer::step_count) */
+
+/* Host arrays of PreprocessOutput + the per-Gaussian ForwardCache fields
+ * (include/types.h:69-82, 97-107).  Any pointer may be NULL (not produced). */
+typedef struct gs3dc_screen_arrays {
+    float* means2D;       /* [N*2] */
+    float* depths;        /* [N] */
+    float* conics;        /* [N*3] */
+    float* opacities_2d;  /* [N] */
+    float* rgb;           /* [N*3] */
+    int* radii;           /* [N] */
+    int* tiles_touched;   /* [N] */
+    float* cov3D;         /* [N*6] */
+    float* p_view;        /* [N*3] */
+    float* p_hom_w;       /* [N] */
+    float* cov2D;         /* [N*3] after the +0.3 filter */
+    float* cov2D_det;     /* [N] */
+} gs3dc_screen_arrays;
+
+/* ---- context ---- */
+int gs3dc_create(int device, gs3dc_ctx** out);
+void gs3dc_destroy(gs3dc_ctx* ctx);
+const char* gs3dc_last_error(const gs3dc_ctx* ctx);
+const char* gs3dc_status_string(int status);
+/* The cudaStream_t every call of this context is ordered on. */
+int gs3dc_get_stream(gs3dc_ctx* ctx, void** stream);
+int gs3dc_set_option(gs3dc_ctx* ctx, int option, int64_t value);
+int gs3dc_get_stat(gs3dc_ctx* ctx, int stat, int64_t* value);
+
+/* ---- model ----
+ * gs3dc_set_gaussians: an activated model for rendering (GaussianData,
+ *   include/types.h:34-45); replaces the device copy every call.
+ * gs3dc_set_raw_params: the trainable model (RawGaussianParams,
+ *   include/train_types.h:9-22); zeroes the Adam moments and step counter like
+ *   AdamOptimizer::reset (src/optimizer.cpp:45-58).
+ * gs3dc_get_raw_params: copies the device parameters into the host arrays of
+ *   raw (same count / max_coeffs as uploaded). */
+int gs3dc_set_gaussians(gs3dc_ctx* ctx, const gs3d_gaussians* g);
+int gs3dc_set_raw_params(gs3dc_ctx* ctx, const gs3d_raw_params* raw);
+int gs3dc_get_raw_params(gs3dc_ctx* ctx, gs3d_raw_params* raw);
+
+/* ---- forward stages ----
+ * Preprocessor::process (include/preprocessor.h:7-12; CPU src/cpu/preprocessor_cpu.cpp:11-268).
+ *   Projects the current model (activated, or the raw model activated on the
+ *   device), computes radii / tiles_touched, the prefix sum and the tile
+ *   pairs.  `out` (may be NULL) receives host copies. */
+int gs3dc_preprocess(gs3dc_ctx* ctx, const gs3d_camera* cam, const gs3d_render_config* cfg,
+                     const gs3dc_screen_arrays* out);
+
+/* TileBinner::bin (include/tile_binner.h:7-12; src/cpu/tile_binner_cpu.cpp:6-102).
+ *   in == NULL: the pairs of the last gs3dc_preprocess.  in != NULL: bins the
+ *   host arrays means2D / depths / radii / tiles_touched of N Gaussians
+ *   (uploaded first).  Writes the pair count and, if non-NULL, the unsorted
+ *   keys ((tile << 32) | depth bits) and values (Gaussian index), Gaussian-major
+ *   and row-major inside each rect like the reference. */
+int gs3dc_bin(gs3dc_ctx* ctx, int num_gaussians, const gs3dc_screen_arrays* in,
+              const gs3d_camera* cam, const gs3d_render_config* cfg, int64_t* total_pairs,
+              uint64_t* keys_unsorted, uint32_t* values_unsorted);
+
+/* Sorter::sort (include/sorter.h:7; src/cpu/sorter_cpu.cpp:6-44).
+ *   Stable LSD radix sort of the current pairs by key, then tile ranges.
+ *   Host outputs may be NULL.  tile_ranges has 2*num_tiles entries
+ *   (start, end), zero for empty tiles. */
+int gs3dc_sort(gs3dc_ctx* ctx, uint64_t* keys_sorted, uint32_t* values_sorted,
+               uint32_t* tile_ranges);
+
+/* Sorter::sort on caller-provided pairs (the SorterCPU unit-test form, where
+ * keys need not come from a camera).  Keys' tile fields must be < num_tiles. */
+int gs3dc_sort_pairs(gs3dc_ctx* ctx, int64_t total_pairs, const uint64_t* keys,
+                     const uint32_t* values, int num_tiles, uint64_t* keys_sorted,
+                     uint32_t* values_sorted, uint32_t* tile_ranges);
+
+/* Rasterizer::rasterize (include/rasterizer.h:7-15; src/cpu/rasterizer_cpu.cpp:38-198).
+ *   Front-to-back blend of the sorted pairs.  image is H*W*3 HWC; T_final and
+ *   n_contrib (ForwardCache, include/types.h:98-99) may be NULL. */
+int gs3dc_rasterize(gs3dc_ctx* ctx, const gs3d_camera* cam, const gs3d_render_config* cfg,
+                    float* image, float* T_final, int* n_contrib);
+
+/* Renderer::render (include/renderer.h:17-21; src/renderer.cpp:13-39):
+ *   g (may be NULL to reuse the uploaded model) -> preprocess -> bin -> sort ->
+ *   rasterize -> image (host, H*W*3). */
+int gs3dc_render(gs3dc_ctx* ctx, const gs3d_gaussians* g, const gs3d_camera* cam,
+                 const gs3d_render_config* cfg, float* image);
+
+/* ---- backward stages ----
+ * RasterizerBackwardCPU::backward (src/cpu/rasterizer_backward_cpu.h:7-10;
+ *   src/cpu/rasterizer_backward_cpu.cpp:7-138) for the last rasterize, with
+ *   d_image given on the host (H*W*3).  Outputs RasterGradOutput
+ *   (include/train_types.h:25-32), any may be NULL. */
+int gs3dc_raster_backward(gs3dc_ctx* ctx, const gs3d_camera* cam, const gs3d_render_config* cfg,
+                          const float* d_image, float* d_means2D, float* d_conics, float* d_rgb,
+                          float* d_opacities_2d);
+
+/* PreprocessorBackwardCPU::backward (src/cpu/preprocessor_backward_cpu.h:7-10;
+ *   src/cpu/preprocessor_backward_cpu.cpp:205-645) of the raw model from the
+ *   last raster backward.  Outputs GradientOutput (include/train_types.h:35-43). */
+int gs3dc_preprocess_backward(gs3dc_ctx* ctx, const gs3d_camera* cam,
+                              const gs3d_render_config* cfg, float* d_raw_positions,
+                              float* d_raw_scales, float* d_raw_rotations,
+                              float* d_raw_sh_coeffs, float* d_raw_opacities);
+
+/* AdamOptimizer::step / SGDOptimizer::step (src/optimizer.cpp:9-101) with the
+ *   gradients of the last gs3dc_preprocess_backward, on the device model. */
+int gs3dc_optimizer_step(gs3dc_ctx* ctx, const gs3d_train_config* tc, int iteration);
+
+/* Trainer::step (include/trainer.h:21-23; src/trainer.cpp:7-70) with the
+ *   parameters resident on the device: activate, forward, L1 loss, backward,
+ *   optimiser, fused into a few kernels and replayed as one CUDA graph.
+ *   gt is H*W*3 HWC; gt_on_device != 0 means it is a device pointer.
+ *   loss (may be NULL) receives the mean absolute error; a NULL loss also lets
+ *   the call return without waiting for the device (the next call, or
+ *   gs3dc_get_raw_params, synchronises). */
+int gs3dc_train_step(gs3dc_ctx* ctx, const gs3d_camera* cam, const float* gt, int gt_on_device,
+                     const gs3d_render_config* cfg, const gs3d_train_config* tc, int iteration,
+                     float* loss);
+
+/* Blocks until every call issued on the context's stream has finished and
+ * reports any deferred device-side error (pair overflow, timeout). */
+int gs3dc_synchronize(gs3dc_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GS3D_CUDA_H */

@@ -1,0 +1,236 @@
+// ref_shim.cpp -- TEST INFRASTRUCTURE.  A C ABI over the reference's own CPU
+// stage classes (harmonyos_3dgs src/cpu/*, trainer.cpp, renderer.cpp), linked
+// with the reference sources compiled where they lie into
+// oracle/_ref/libgs3d_ref.so by oracle/Makefile.  Nothing here reimplements
+// the reference: every number comes from its classes.
+//
+//   ref_forward      PreprocessorCPU -> TileBinnerCPU -> SorterCPU -> RasterizerCPU
+//                    (the sequence of Renderer::render, renderer.cpp:13-39, with the
+//                    ForwardCache of Trainer::step, trainer.cpp:38-48)
+//   ref_train_step   Trainer::step's sequence (trainer.cpp:7-70) with every
+//                    intermediate copied out, Adam state kept in a handle
+//   ref_trainer_*    the unmodified Trainer class (timing baseline)
+//   ref_renderer_*   the unmodified Renderer with the CPU stages (timing baseline)
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <vector>
+
+#include "types.h"
+#include "train_types.h"
+#include "renderer.h"
+#include "trainer.h"
+#include "loss.h"
+#include "optimizer.h"
+#include "cpu/preprocessor_cpu.h"
+#include "cpu/tile_binner_cpu.h"
+#include "cpu/sorter_cpu.h"
+#include "cpu/rasterizer_cpu.h"
+#include "cpu/rasterizer_backward_cpu.h"
+#include "cpu/preprocessor_backward_cpu.h"
+
+#include "gs3d_oracle.h"
+
+static_assert(sizeof(Camera) == sizeof(gs3d_camera), "Camera layout");
+static_assert(sizeof(RenderConfig) == sizeof(gs3d_render_config), "RenderConfig layout");
+static_assert(sizeof(GaussianData) == sizeof(gs3d_gaussians), "GaussianData layout");
+static_assert(sizeof(TrainConfig) == sizeof(gs3d_train_config), "TrainConfig layout");
+static_assert(sizeof(RawGaussianParams) == sizeof(gs3d_raw_params), "RawGaussianParams layout");
+
+namespace {
+
+void copy_forward(int N, const PreprocessOutput& pre, const ForwardCache& cache,
+                  const BinningOutput& bin, int num_pixels, const float* img, orc_step_io* io) {
+    std::memcpy(io->means2D, pre.means2D, sizeof(float) * 2 * N);
+    std::memcpy(io->depths, pre.depths, sizeof(float) * N);
+    std::memcpy(io->conics, pre.conics, sizeof(float) * 3 * N);
+    std::memcpy(io->opac2d, pre.opacities_2d, sizeof(float) * N);
+    std::memcpy(io->rgb, pre.rgb, sizeof(float) * 3 * N);
+    std::memcpy(io->radii, pre.radii, sizeof(int) * N);
+    std::memcpy(io->tiles, pre.tiles_touched, sizeof(int) * N);
+    if (io->cov3D) {
+        std::memcpy(io->cov3D, cache.cov3D, sizeof(float) * 6 * N);
+        std::memcpy(io->p_view, cache.p_view, sizeof(float) * 3 * N);
+        std::memcpy(io->p_hom_w, cache.p_hom_w, sizeof(float) * N);
+        std::memcpy(io->cov2D, cache.cov2D, sizeof(float) * 3 * N);
+        std::memcpy(io->det, cache.cov2D_det, sizeof(float) * N);
+    }
+    int64_t P = bin.total_pairs;
+    if (P > 0) {
+        std::memcpy(io->keys_unsorted, bin.keys_unsorted, sizeof(uint64_t) * P);
+        std::memcpy(io->vals_unsorted, bin.values_unsorted, sizeof(uint32_t) * P);
+        std::memcpy(io->keys_sorted, bin.keys_sorted, sizeof(uint64_t) * P);
+        std::memcpy(io->vals_sorted, bin.values_sorted, sizeof(uint32_t) * P);
+    }
+    std::memcpy(io->ranges, bin.tile_ranges, sizeof(uint32_t) * 2 * bin.num_tiles);
+    std::memcpy(io->image, img, sizeof(float) * 3 * num_pixels);
+    if (io->T_final && cache.T_final) {
+        std::memcpy(io->T_final, cache.T_final, sizeof(float) * num_pixels);
+        std::memcpy(io->n_contrib, cache.n_contrib, sizeof(int) * num_pixels);
+    }
+}
+
+// Runs the reference forward with a cache.  Returns 1 if io->pair_capacity is
+// too small (io->total_pairs is set), else 0.
+int run_forward(const GaussianData& g, const Camera& cam, const RenderConfig& cfg,
+                FrameAllocator& alloc, PreprocessOutput& pre, BinningOutput& bin,
+                ForwardCache& cache, float*& rendered, orc_step_io* io) {
+    PreprocessorCPU pp;
+    TileBinnerCPU tb;
+    SorterCPU so;
+    RasterizerCPU ra;
+    cache = ForwardCache{};
+    pre = pp.process(g, cam, cfg, alloc, &cache);
+    bin = tb.bin(pre, g.count, cam, cfg, alloc);
+    io->total_pairs = bin.total_pairs;
+    if (bin.total_pairs > io->pair_capacity) return 1;
+    if (bin.total_pairs > 0) so.sort(bin, alloc);
+    cache.pre = &pre;
+    cache.bin = &bin;
+    int num_pixels = cam.width * cam.height;
+    rendered = alloc.allocate_array<float>(num_pixels * 3);
+    ra.rasterize(pre, bin, cam, cfg, rendered, nullptr, &cache, &alloc);
+    return 0;
+}
+
+size_t arena_bytes(int N, int max_coeffs, int64_t P, int num_pixels) {
+    size_t b = (size_t)N * (size_t)(60 + 4 * max_coeffs * 3) * 8 + (size_t)P * 40 +
+               (size_t)num_pixels * 64 + (64u << 20);
+    return b;
+}
+
+struct AdamHandle {
+    AdamOptimizer adam;
+};
+
+}  // namespace
+
+extern "C" {
+
+int ref_forward(const gs3d_gaussians* gp, const gs3d_camera* camp, const gs3d_render_config* cfgp,
+                orc_step_io* io) {
+    const GaussianData& g = *reinterpret_cast<const GaussianData*>(gp);
+    const Camera& cam = *reinterpret_cast<const Camera*>(camp);
+    const RenderConfig& cfg = *reinterpret_cast<const RenderConfig*>(cfgp);
+    int num_pixels = cam.width * cam.height;
+    FrameAllocator alloc(arena_bytes(g.count, g.max_coeffs, io->pair_capacity, num_pixels));
+    PreprocessOutput pre;
+    BinningOutput bin;
+    ForwardCache cache;
+    float* rendered = nullptr;
+    if (run_forward(g, cam, cfg, alloc, pre, bin, cache, rendered, io)) return 1;
+    copy_forward(g.count, pre, cache, bin, num_pixels, rendered, io);
+    return 0;
+}
+
+void* ref_adam_create(void) { return new (std::nothrow) AdamHandle(); }
+void ref_adam_destroy(void* h) { delete static_cast<AdamHandle*>(h); }
+
+// Trainer::step (trainer.cpp:7-70) with every intermediate copied into io.
+int ref_train_step(void* adam_handle, gs3d_raw_params* rawp, const gs3d_camera* camp,
+                   const float* gt, const gs3d_render_config* cfgp, const gs3d_train_config* tcp,
+                   int iteration, orc_step_io* io) {
+    RawGaussianParams& params = *reinterpret_cast<RawGaussianParams*>(rawp);
+    const Camera& cam = *reinterpret_cast<const Camera*>(camp);
+    const RenderConfig& cfg = *reinterpret_cast<const RenderConfig*>(cfgp);
+    const TrainConfig& tc = *reinterpret_cast<const TrainConfig*>(tcp);
+    int N = params.count, mc3 = params.max_coeffs * 3;
+    int num_pixels = cam.width * cam.height;
+    FrameAllocator alloc(arena_bytes(N, params.max_coeffs, io->pair_capacity, num_pixels));
+    std::vector<float> ap(N * 3), as(N * 3), ar(N * 4), ash((size_t)N * mc3), ao(N);
+    GaussianData g;
+    g.count = N;
+    g.sh_degree = params.sh_degree;
+    g.max_coeffs = params.max_coeffs;
+    g.positions = ap.data();
+    g.scales = as.data();
+    g.rotations = ar.data();
+    g.sh_coeffs = ash.data();
+    g.opacities = ao.data();
+    g.filter_3D = nullptr;
+    params.activate(g);
+    PreprocessOutput pre;
+    BinningOutput bin;
+    ForwardCache cache;
+    float* rendered = nullptr;
+    if (run_forward(g, cam, cfg, alloc, pre, bin, cache, rendered, io)) return 1;
+    copy_forward(N, pre, cache, bin, num_pixels, rendered, io);
+    float* d_image = alloc.allocate_array<float>(num_pixels * 3);
+    io->loss = l1_loss(rendered, gt, cam.height, cam.width, d_image);
+    io->loss_acc64 = l1_loss_double(rendered, gt, cam.height, cam.width, d_image);
+    std::memcpy(io->d_image, d_image, sizeof(float) * 3 * num_pixels);
+    RasterGradOutput rgrad;
+    rgrad.allocate_and_zero(alloc, N);
+    RasterizerBackwardCPU rbw;
+    rbw.backward(pre, bin, cam, cfg, cache, d_image, rgrad);
+    std::memcpy(io->d_means2D, rgrad.d_means2D, sizeof(float) * 2 * N);
+    std::memcpy(io->d_conics, rgrad.d_conics, sizeof(float) * 3 * N);
+    std::memcpy(io->d_rgb, rgrad.d_rgb, sizeof(float) * 3 * N);
+    std::memcpy(io->d_opac, rgrad.d_opacities_2d, sizeof(float) * N);
+    GradientOutput grads;
+    grads.allocate_and_zero(alloc, N, params.max_coeffs);
+    PreprocessorBackwardCPU pbw;
+    pbw.backward(g, cam, cfg, cache, rgrad, params, grads);
+    std::memcpy(io->g_pos, grads.d_raw_positions, sizeof(float) * 3 * N);
+    std::memcpy(io->g_sc, grads.d_raw_scales, sizeof(float) * 3 * N);
+    std::memcpy(io->g_rot, grads.d_raw_rotations, sizeof(float) * 4 * N);
+    std::memcpy(io->g_sh, grads.d_raw_sh_coeffs, sizeof(float) * (size_t)mc3 * N);
+    std::memcpy(io->g_op, grads.d_raw_opacities, sizeof(float) * N);
+    if (tc.use_adam) {
+        static_cast<AdamHandle*>(adam_handle)->adam.step(params, grads, tc, iteration);
+    } else {
+        SGDOptimizer sgd;
+        sgd.step(params, grads, tc, iteration);
+    }
+    return 0;
+}
+
+// The unmodified Trainer (trainer.h:14-50), for timing.
+void* ref_trainer_create(size_t arena_bytes_) {
+    try {
+        return new Trainer(arena_bytes_);
+    } catch (...) {
+        return nullptr;
+    }
+}
+void ref_trainer_destroy(void* t) { delete static_cast<Trainer*>(t); }
+int ref_trainer_step(void* t, gs3d_raw_params* rawp, const gs3d_camera* camp, const float* gt,
+                     const gs3d_render_config* cfgp, const gs3d_train_config* tcp, int iteration,
+                     float* loss_out) {
+    try {
+        auto r = static_cast<Trainer*>(t)->step(*reinterpret_cast<RawGaussianParams*>(rawp),
+                                                *reinterpret_cast<const Camera*>(camp), gt,
+                                                *reinterpret_cast<const RenderConfig*>(cfgp),
+                                                *reinterpret_cast<const TrainConfig*>(tcp), iteration);
+        if (loss_out) *loss_out = r.loss;
+        return 0;
+    } catch (...) {
+        return 1;
+    }
+}
+
+// The unmodified Renderer with the CPU stages (renderer.h:9-29), for timing.
+void* ref_renderer_create(size_t arena_bytes_) {
+    try {
+        return new Renderer(std::make_unique<PreprocessorCPU>(), std::make_unique<TileBinnerCPU>(),
+                            std::make_unique<SorterCPU>(), std::make_unique<RasterizerCPU>(),
+                            arena_bytes_);
+    } catch (...) {
+        return nullptr;
+    }
+}
+void ref_renderer_destroy(void* r) { delete static_cast<Renderer*>(r); }
+int ref_renderer_render(void* r, const gs3d_gaussians* gp, const gs3d_camera* camp,
+                        const gs3d_render_config* cfgp, float* img) {
+    try {
+        static_cast<Renderer*>(r)->render(*reinterpret_cast<const GaussianData*>(gp),
+                                          *reinterpret_cast<const Camera*>(camp),
+                                          *reinterpret_cast<const RenderConfig*>(cfgp), img, nullptr);
+        return 0;
+    } catch (...) {
+        return 1;
+    }
+}
+
+}  // extern "C"
