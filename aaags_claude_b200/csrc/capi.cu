@@ -89,6 +89,8 @@ struct gs3dc_ctx {
     DevBuf<unsigned char> dsign;
     // per-step parameters: device copy + pinned ring
     StepParams* sp_dev = nullptr;
+    Persist* persist = nullptr;       // device
+    Persist* persist_host = nullptr;  // pinned readback
     StepParams* sp_ring = nullptr;
     cudaEvent_t sp_event[kParamSlots] = {};
     int sp_slot = 0;
@@ -102,6 +104,10 @@ struct gs3dc_ctx {
     long long graph_replays = 0;
     long long graph_kernels = 0;
     bool pending_check = false;
+    // stage timing
+    bool stage_timing = false;
+    cudaEvent_t stage_ev[GS3DC_NUM_STAGES + 1] = {};
+    float stage_ms[GS3DC_NUM_STAGES] = {};
     // options / stats
     unsigned spin_limit = 1u << 22;
     long long kernels_last = 0;
@@ -182,7 +188,7 @@ int check_config(gs3dc_ctx* c, const gs3d_camera* cam, const gs3d_render_config*
 
 // Control block + one look-back descriptor per 256-Gaussian CTA.
 int ensure_ctrl(gs3dc_ctx* c, int N) {
-    const size_t blocks = ((size_t)N + kBlock - 1) / kBlock;
+    const size_t blocks = std::max<size_t>(2, ((size_t)N + kBlock - 1) / kBlock);
     const size_t head = ((sizeof(Control) + 255) / 256) * 256;
     const size_t bytes = head + (blocks + 1) * sizeof(unsigned long long);
     if (bytes > c->ctrl_region.n) {
@@ -229,6 +235,7 @@ int zero_adam(gs3dc_ctx* c) {
                                &c->v_rot, &c->m_sh,  &c->v_sh,  &c->m_op, &c->v_op};
     for (int k = 0; k < 10; k++)
         if (bufs[k]->n) CK(cudaMemsetAsync(bufs[k]->p, 0, bufs[k]->n * sizeof(float), c->stream));
+    CK(cudaMemsetAsync(c->persist, 0, sizeof(Persist), c->stream));
     c->adam_step = 0;
     return GS3DC_OK;
 }
@@ -305,6 +312,7 @@ int push_params(gs3dc_ctx* c, const gs3d_camera* cam, const gs3d_render_config* 
     p.sort_passes = sort_passes_for(p.num_tiles);
     p.sort_bits = 32 + bit_length(p.num_tiles > 1 ? (unsigned)(p.num_tiles - 1) : 0u);
     p.gt = gt_dev;
+    p.persist = c->persist;
     if (tc) {
         p.use_adam = tc->use_adam ? 1 : 0;
         // lr_schedule, train_types.cpp:64-68
@@ -329,7 +337,8 @@ int push_params(gs3dc_ctx* c, const gs3d_camera* cam, const gs3d_render_config* 
 
 // Reads the control block back and turns device status bits into a status.
 int read_control(gs3dc_ctx* c) {
-    CK(cudaMemcpyAsync(c->ctrl_host, c->ctrl, sizeof(Control), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(c->ctrl_host, c->ctrl, kControlReadback, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(c->persist_host, c->persist, sizeof(Persist), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     c->last_pairs = c->ctrl_host->total_pairs;
     if (c->ctrl_host->status & kStatusTimeout)
@@ -343,8 +352,18 @@ size_t ctrl_bytes_for(int N) {
     return ((sizeof(Control) + 255) / 256) * 256 + (((size_t)N + kBlock - 1) / kBlock) * sizeof(unsigned long long);
 }
 
+// Records the start of `stage` when stage timing is on (un-captured runs only).
+int mark(gs3dc_ctx* c, int stage) {
+    if (c->stage_timing) CK(cudaEventRecord(c->stage_ev[stage], c->stream));
+    return GS3DC_OK;
+}
+
 int seq_preprocess(gs3dc_ctx* c, bool cache) {
+    int rc = mark(c, GS3DC_STAGE_MEMSETS);
+    if (rc) return rc;
     CK(cudaMemsetAsync(c->ctrl_region.p, 0, ctrl_bytes_for(c->N), c->stream));
+    CK(cudaMemsetAsync(c->ranges.p, 0, 2 * (size_t)c->num_tiles * sizeof(unsigned), c->stream));
+    if ((rc = mark(c, GS3DC_STAGE_PREPROCESS))) return rc;
     PairPtrs pr{c->keys[0].p, c->vals[0].p, c->cap, c->scan_desc};
     CK(launch_preprocess_plain(c->stream, c->sp_dev, c->N, c->model_raw, cache, model_ptrs(c),
                                screen_ptrs(c, cache), pr, c->ctrl));
@@ -352,17 +371,25 @@ int seq_preprocess(gs3dc_ctx* c, bool cache) {
     return GS3DC_OK;
 }
 
-int seq_sort(gs3dc_ctx* c) {
-    // sort scratch: tickets of the passes and the digit histograms
-    CK(cudaMemsetAsync(&c->ctrl->tickets[1], 0,
-                       sizeof(Control) - offsetof(Control, tickets) - sizeof(unsigned), c->stream));
-    CK(cudaMemsetAsync(c->sort_desc.p, 0, (size_t)c->sort_passes * c->sort_desc_stride * sizeof(unsigned long long),
+// Sort scratch zeroing; seq_preprocess already did it for a full step.
+int seq_sort_scratch(gs3dc_ctx* c) {
+    CK(cudaMemsetAsync(&c->ctrl->tickets[1], 0, sizeof(Control) - offsetof(Control, tickets) - sizeof(unsigned),
                        c->stream));
     CK(cudaMemsetAsync(c->ranges.p, 0, 2 * (size_t)c->num_tiles * sizeof(unsigned), c->stream));
+    return GS3DC_OK;
+}
+
+int seq_sort(gs3dc_ctx* c) {
+    CK(cudaMemsetAsync(c->sort_desc.p, 0, (size_t)c->sort_passes * c->sort_desc_stride * sizeof(unsigned long long),
+                       c->stream));
+    int rc = mark(c, GS3DC_STAGE_SORT_HIST);
+    if (rc) return rc;
     int which = 0;
     CK(launch_radix_sort(c->stream, c->sp_dev, c->sort_passes, c->cap, c->keys[0].p, c->vals[0].p, c->keys[1].p,
-                         c->vals[1].p, c->sort_desc.p, c->sort_desc_stride, c->ctrl, &which));
+                         c->vals[1].p, c->sort_desc.p, c->sort_desc_stride, c->ctrl, &which,
+                         c->stage_timing ? c->stage_ev[GS3DC_STAGE_SORT_PASSES] : nullptr));
     c->sorted_which = which;
+    if ((rc = mark(c, GS3DC_STAGE_RANGES))) return rc;
     CK(launch_tile_ranges(c->stream, c->cap, c->keys[which].p, c->ranges.p, c->ctrl));
     c->kernels_last += 2 + c->sort_passes;
     return GS3DC_OK;
@@ -374,12 +401,16 @@ int seq_train(gs3dc_ctx* c) {
     rc = seq_sort(c);
     if (rc) return rc;
     const int w = c->sorted_which;
+    if ((rc = mark(c, GS3DC_STAGE_RASTER_FWD))) return rc;
     CK(launch_raster_fwd_plain(c->stream, c->sp_dev, c->num_tiles, true, c->ranges.p, c->vals[w].p,
                                screen_ptrs(c, false), pixel_ptrs(c), c->ctrl));
+    if ((rc = mark(c, GS3DC_STAGE_RASTER_BWD))) return rc;
     CK(launch_raster_bwd_plain(c->stream, c->sp_dev, c->num_tiles, true, c->ranges.p, c->vals[w].p,
                                screen_ptrs(c, false), pixel_ptrs(c), rgrad_ptrs(c), c->ctrl));
+    if ((rc = mark(c, GS3DC_STAGE_PREPROCESS_BWD))) return rc;
     CK(launch_preprocess_bwd_plain(c->stream, c->sp_dev, c->N, true, model_ptrs(c), adam_ptrs(c),
                                    screen_ptrs(c, false), rgrad_ptrs(c), grad_ptrs(c), c->ctrl));
+    if ((rc = mark(c, GS3DC_NUM_STAGES))) return rc;
     c->kernels_last += 3;
     return GS3DC_OK;
 }
@@ -493,10 +524,16 @@ int gs3dc_create(int device, gs3dc_ctx** out) {
     if (cudaSetDevice(device) != cudaSuccess) return bail(GS3DC_ERR_CUDA);
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(GS3DC_ERR_CUDA);
     if (cudaMalloc(&c->sp_dev, sizeof(StepParams)) != cudaSuccess) return bail(GS3DC_ERR_OUT_OF_MEMORY);
+    if (cudaMalloc(&c->persist, sizeof(Persist)) != cudaSuccess) return bail(GS3DC_ERR_OUT_OF_MEMORY);
+    if (cudaMemset(c->persist, 0, sizeof(Persist)) != cudaSuccess) return bail(GS3DC_ERR_CUDA);
+    if (cudaMallocHost(&c->persist_host, sizeof(Persist)) != cudaSuccess) return bail(GS3DC_ERR_OUT_OF_MEMORY);
+    std::memset(c->persist_host, 0, sizeof(Persist));
     if (cudaMallocHost(&c->sp_ring, kParamSlots * sizeof(StepParams)) != cudaSuccess) return bail(GS3DC_ERR_OUT_OF_MEMORY);
     if (cudaMallocHost(&c->ctrl_host, sizeof(Control)) != cudaSuccess) return bail(GS3DC_ERR_OUT_OF_MEMORY);
     for (int k = 0; k < kParamSlots; k++)
         if (cudaEventCreateWithFlags(&c->sp_event[k], cudaEventDisableTiming) != cudaSuccess) return bail(GS3DC_ERR_CUDA);
+    for (int k = 0; k <= GS3DC_NUM_STAGES; k++)
+        if (cudaEventCreate(&c->stage_ev[k]) != cudaSuccess) return bail(GS3DC_ERR_CUDA);
     if (ensure_model(c, 0, 1) != GS3DC_OK) return bail(GS3DC_ERR_OUT_OF_MEMORY);
     *out = c;
     return GS3DC_OK;
@@ -531,10 +568,14 @@ void gs3dc_destroy(gs3dc_ctx* c) {
     c->last_j.release();
     c->dsign.release();
     if (c->sp_dev) cudaFree(c->sp_dev);
+    if (c->persist) cudaFree(c->persist);
+    if (c->persist_host) cudaFreeHost(c->persist_host);
     if (c->sp_ring) cudaFreeHost(c->sp_ring);
     if (c->ctrl_host) cudaFreeHost(c->ctrl_host);
     for (int k = 0; k < kParamSlots; k++)
         if (c->sp_event[k]) cudaEventDestroy(c->sp_event[k]);
+    for (int k = 0; k <= GS3DC_NUM_STAGES; k++)
+        if (c->stage_ev[k]) cudaEventDestroy(c->stage_ev[k]);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -565,6 +606,9 @@ int gs3dc_set_option(gs3dc_ctx* c, int option, int64_t value) {
                 cudaGraphExecDestroy(c->graph);
                 c->graph = nullptr;
             }
+            return GS3DC_OK;
+        case GS3DC_OPT_STAGE_TIMING:
+            c->stage_timing = value != 0;
             return GS3DC_OK;
         default:
             return fail(c, GS3DC_ERR_INVALID_ARG, "unknown option %d", option);
@@ -721,7 +765,11 @@ int gs3dc_sort(gs3dc_ctx* c, uint64_t* keys_sorted, uint32_t* values_sorted, uin
     if (!c->have_pairs) return fail(c, GS3DC_ERR_STATE, "gs3dc_sort needs pairs (gs3dc_preprocess or gs3dc_bin)");
     CK(cudaSetDevice(c->device));
     c->kernels_last = 0;
-    int rc = seq_sort(c);
+    const bool timing = c->stage_timing;
+    c->stage_timing = false;
+    int rc = seq_sort_scratch(c);
+    if (!rc) rc = seq_sort(c);
+    c->stage_timing = timing;
     if (rc) return rc;
     if ((rc = read_control(c))) return rc;
     const size_t P = (size_t)c->last_pairs;
@@ -885,18 +933,46 @@ int gs3dc_optimizer_step(gs3dc_ctx* c, const gs3d_train_config* tc, int iteratio
     return GS3DC_OK;
 }
 
+int gs3dc_selftest_bounded_wait(gs3dc_ctx* c, uint32_t spin_limit) {
+    if (!c || spin_limit == 0 || spin_limit > (1u << 24)) return GS3DC_ERR_INVALID_ARG;
+    CK(cudaSetDevice(c->device));
+    // two zeroed descriptors at the head of the scan-descriptor area, status word cleared
+    CK(cudaMemsetAsync(c->ctrl_region.p, 0, ctrl_bytes_for(2 * kBlock), c->stream));
+    CK(launch_wait_selftest(c->stream, c->scan_desc, &c->ctrl->status, spin_limit));
+    const int rc = read_control(c);
+    CK(cudaMemsetAsync(c->ctrl_region.p, 0, ctrl_bytes_for(2 * kBlock), c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return rc;
+}
+
+int gs3dc_get_stage_times(gs3dc_ctx* c, float* ms, int n_stages) {
+    if (!c || !ms || n_stages < 0) return GS3DC_ERR_INVALID_ARG;
+    for (int k = 0; k < n_stages && k < GS3DC_NUM_STAGES; k++) ms[k] = c->stage_ms[k];
+    return GS3DC_OK;
+}
+
+// Acknowledges a sticky overflow: the Adam step counter follows the updates
+// the device actually applied, and later steps may update again.
+int acknowledge_overflow(gs3dc_ctx* c) {
+    c->adam_step = (int)c->persist_host->applied_steps;
+    c->persist_host->sticky_overflow = 0;
+    CK(cudaMemsetAsync(&c->persist->sticky_overflow, 0, sizeof(unsigned), c->stream));
+    return GS3DC_OK;
+}
+
 int gs3dc_synchronize(gs3dc_ctx* c) {
     if (!c) return GS3DC_ERR_INVALID_ARG;
     CK(cudaSetDevice(c->device));
     int rc = read_control(c);
     if (rc) return rc;
-    if (c->pending_check && (c->ctrl_host->status & kStatusOverflow)) {
-        c->pending_check = false;
-        return fail(c, GS3DC_ERR_PAIR_OVERFLOW,
-                    "a train step found %llu tile pairs for a capacity of %llu and was skipped",
-                    (unsigned long long)c->ctrl_host->total_pairs, c->cap);
-    }
     c->pending_check = false;
+    if (c->persist_host->sticky_overflow) {
+        if ((rc = acknowledge_overflow(c))) return rc;
+        return fail(c, GS3DC_ERR_PAIR_OVERFLOW,
+                    "a train step found more tile pairs than the capacity of %llu; it and the steps queued "
+                    "after it were skipped (%llu optimiser steps applied)",
+                    c->cap, (unsigned long long)c->persist_host->applied_steps);
+    }
     return GS3DC_OK;
 }
 
@@ -929,7 +1005,7 @@ int gs3dc_train_step(gs3dc_ctx* c, const gs3d_camera* cam, const float* gt, int 
                                   (long long)c->spin_limit, 1};
         const bool key_ok = c->graph && std::memcmp(key, c->graph_key, sizeof(key)) == 0;
         c->kernels_last = 0;
-        if (c->use_graph && !first && attempt == 0) {
+        if (c->use_graph && !c->stage_timing && !first && attempt == 0) {
             if (!key_ok) {
                 if (c->graph) {
                     cudaGraphExecDestroy(c->graph);
@@ -952,7 +1028,7 @@ int gs3dc_train_step(gs3dc_ctx* c, const gs3d_camera* cam, const float* gt, int 
         } else {
             if ((rc = seq_train(c))) return rc;
         }
-        if (!loss && !first) {
+        if (!loss && !first && !c->stage_timing) {
             c->pending_check = true;  // overflow is reported by the next synchronising call
             return GS3DC_OK;
         }
@@ -960,15 +1036,23 @@ int gs3dc_train_step(gs3dc_ctx* c, const gs3d_camera* cam, const float* gt, int 
             c->adam_step = step_before;
             return rc;
         }
-        if (c->ctrl_host->status & kStatusOverflow) {
+        if (c->persist_host->sticky_overflow) {
             // nothing was updated: the backward and the optimiser skip overflowed steps
-            c->adam_step = step_before;
+            if ((rc = acknowledge_overflow(c))) return rc;
             const unsigned long long P = c->ctrl_host->total_pairs;
+            if (!(c->ctrl_host->status & kStatusOverflow)) {
+                // an earlier asynchronous step overflowed: report it, this step was skipped too
+                return fail(c, GS3DC_ERR_PAIR_OVERFLOW, "an earlier queued train step overflowed the pair capacity");
+            }
             if ((rc = ensure_pairs(c, P + P / 2 + 4096, c->num_tiles))) return rc;
             first = true;
             continue;
         }
         if (loss) *loss = (float)(c->ctrl_host->loss_sum / (double)(3.0 * (double)np));
+        if (c->stage_timing) {
+            for (int k = 0; k < GS3DC_NUM_STAGES; k++)
+                CK(cudaEventElapsedTime(&c->stage_ms[k], c->stage_ev[k], c->stage_ev[k + 1]));
+        }
         return GS3DC_OK;
     }
     c->adam_step = step_before;

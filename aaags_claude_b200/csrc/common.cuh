@@ -16,6 +16,13 @@ constexpr int kMaxPasses = 8;        // radix passes (8-bit digits over <= 64 ke
 constexpr unsigned kStatusOverflow = 1u;  // more tile pairs than capacity
 constexpr unsigned kStatusTimeout = 2u;   // a bounded device-side wait gave up
 
+// Device state that survives across steps (zeroed when a model is uploaded).
+struct Persist {
+    unsigned long long applied_steps;  // optimiser updates actually applied
+    unsigned sticky_overflow;          // set by any overflowed step until the host acknowledges it
+    unsigned pad_;
+};
+
 // Per-step parameters, resident in device memory so that a captured graph
 // reads fresh camera / learning-rate values on every replay.
 struct StepParams {
@@ -38,17 +45,20 @@ struct StepParams {
     int sort_passes;
     unsigned spin_limit;  // bounded waits
     const float* gt;      // [H*W*3] device target of the fused L1 (read per replay)
+    Persist* persist;
 };
 
 // Small device control block, zeroed by one memset at the start of a step.
+// The first kControlReadback bytes are what the host reads back per step.
 struct Control {
     unsigned long long total_pairs;   // written by the last preprocess / bin block
     unsigned status;                  // kStatus* bits
-    unsigned tickets[16];             // dynamic CTA tickets (0: preprocess/bin, 1..8: sort passes)
     unsigned pad_;
     double loss_sum;                  // sum |image - gt| of the fused L1
+    unsigned tickets[16];             // dynamic CTA tickets (0: preprocess/bin, 1..8: sort passes)
     unsigned hist[kMaxPasses][256];   // radix digit histograms of all passes
 };
+constexpr size_t kControlReadback = 24;
 
 // ---- relaxed 64-bit accesses for decoupled look-back descriptors ----
 __device__ __forceinline__ unsigned long long ld_relaxed(const unsigned long long* p) {

@@ -104,9 +104,13 @@ cudaError_t launch_optimizer_plain(cudaStream_t st, const StepParams* sp, int N,
 cudaError_t launch_radix_sort(cudaStream_t st, const StepParams* sp, int sort_passes,
                               unsigned long long capacity, unsigned long long* keys0, unsigned* vals0,
                               unsigned long long* keys1, unsigned* vals1, unsigned long long* desc,
-                              unsigned long long desc_stride, Control* ctrl, int* which);
+                              unsigned long long desc_stride, Control* ctrl, int* which,
+                              cudaEvent_t after_hist = nullptr);
 cudaError_t launch_tile_ranges(cudaStream_t st, unsigned long long capacity,
                                const unsigned long long* keys_sorted, unsigned* ranges, Control* ctrl);
+
+// Bounded-wait self-test: desc2 = two zeroed descriptors.
+cudaError_t launch_wait_selftest(cudaStream_t st, unsigned long long* desc2, unsigned* status, unsigned spin_limit);
 
 constexpr int kSortThreads = 256;
 constexpr int kSortItems = 16;

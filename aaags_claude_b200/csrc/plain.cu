@@ -343,7 +343,7 @@ struct EmitShared {
 // (tile_binner_cpu.cpp:90-97).
 __device__ __forceinline__ void scan_and_emit(EmitShared& sm, int blk, int cnt, int emit, int rx, int ry,
                                               int rw, unsigned dbits, int grid_x, PairPtrs pr,
-                                              Control* ctrl, unsigned spin_limit) {
+                                              Control* ctrl, unsigned spin_limit, Persist* persist) {
     const int tid = threadIdx.x;
     int total;
     const int incl = block_inclusive_scan(cnt, sm.warp, &total);
@@ -357,7 +357,10 @@ __device__ __forceinline__ void scan_and_emit(EmitShared& sm, int blk, int cnt, 
             lookback_exclusive(pr.scan_desc, blk, (unsigned long long)total, &ctrl->status, spin_limit);
         sm.base = ex;
         if (blk == (int)gridDim.x - 1) ctrl->total_pairs = ex + (unsigned long long)total;
-        if (ex + (unsigned long long)total > pr.capacity) atomicOr(&ctrl->status, kStatusOverflow);
+        if (ex + (unsigned long long)total > pr.capacity) {
+            atomicOr(&ctrl->status, kStatusOverflow);
+            if (persist) atomicOr(&persist->sticky_overflow, 1u);
+        }
     }
     __syncthreads();
     const unsigned long long base = sm.base;
@@ -442,7 +445,7 @@ __global__ void __launch_bounds__(kBlock) k_preprocess(const StepParams* __restr
             s.det[i] = vis ? r.det : 0.f;
         }
     }
-    scan_and_emit(sm, blk, cnt, cnt, rx, ry, rw, dbits, sp.grid_x, pr, ctrl, sp.spin_limit);
+    scan_and_emit(sm, blk, cnt, cnt, rx, ry, rw, dbits, sp.grid_x, pr, ctrl, sp.spin_limit, sp.persist);
 }
 
 // TileBinner::bin over host-provided screen arrays (tile_binner_cpu.cpp:33-99):
@@ -471,7 +474,7 @@ __global__ void __launch_bounds__(kBlock) k_bin_arrays(const StepParams* __restr
             dbits = __float_as_uint(a.depths[i]);
         }
     }
-    scan_and_emit(sm, blk, cnt, emit, rx, ry, rw, dbits, sp.grid_x, pr, ctrl, sp.spin_limit);
+    scan_and_emit(sm, blk, cnt, emit, rx, ry, rw, dbits, sp.grid_x, pr, ctrl, sp.spin_limit, nullptr);
 }
 
 // Unpacks the screen records into PreprocessOutput's layout.
@@ -604,8 +607,8 @@ __global__ void __launch_bounds__(kBlock) k_raster_bwd(const StepParams* __restr
     __shared__ float s_b[kBlock];
     __shared__ unsigned s_idx[kBlock];
     __shared__ unsigned s_maxlast;
-    if (FROM_SIGN && (ctrl->status & kStatusOverflow)) return;
     const StepParams& sp = *spp;
+    if (FROM_SIGN && ((ctrl->status & kStatusOverflow) || sp.persist->sticky_overflow)) return;
     const int W = sp.cam.width, H = sp.cam.height;
     const int tile = blockIdx.x;
     const int tx = tile % sp.grid_x, ty = tile / sp.grid_x;
@@ -746,8 +749,11 @@ __global__ void __launch_bounds__(kBlock) k_preprocess_bwd(const StepParams* __r
                                                            RGradPtrs rg, GradPtrs gout, Control* ctrl) {
     const int i = blockIdx.x * kBlock + threadIdx.x;
     if (i >= N) return;
-    if (FUSED && (ctrl->status & (kStatusOverflow | kStatusTimeout))) return;
     const StepParams& sp = *spp;
+    // an overflowed (or timed-out) step, or any step after one the host has not
+    // acknowledged yet, updates nothing
+    if (FUSED && ((ctrl->status & (kStatusOverflow | kStatusTimeout)) || sp.persist->sticky_overflow)) return;
+    if (FUSED && i == 0) atomicAdd(&sp.persist->applied_steps, 1ull);
     const gs3d_camera& cam = sp.cam;
     const int mc = sp.max_coeffs;
     const int mc3 = mc * 3;
@@ -1061,6 +1067,7 @@ __global__ void k_optimizer(const StepParams* __restrict__ spp, long long n_pos,
                             long long n_op, ModelPtrs raw, AdamPtrs adam, GradPtrs g) {
     const StepParams& sp = *spp;
     const long long stride = (long long)gridDim.x * blockDim.x;
+    if (blockIdx.x == 0 && threadIdx.x == 0 && sp.use_adam) atomicAdd(&sp.persist->applied_steps, 1ull);
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n_pos; i += stride) {
         apply_update(sp, &raw.pos[i], &adam.m_pos[i], &adam.v_pos[i], g.g_pos[i], sp.lr_pos);
         apply_update(sp, &raw.sc[i], &adam.m_sc[i], &adam.v_sc[i], g.g_sc[i], sp.lr_scale);

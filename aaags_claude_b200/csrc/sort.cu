@@ -172,12 +172,23 @@ __global__ void k_ranges(const unsigned long long* __restrict__ keys, unsigned l
     }
 }
 
+// One CTA plays block 1 of a look-back whose block 0 never publishes: the
+// wait must run out after spin_limit polls and raise kStatusTimeout.
+__global__ void k_wait_selftest(unsigned long long* desc, unsigned* status, unsigned spin_limit) {
+    if (threadIdx.x == 0) lookback_exclusive_strided(desc, 1, 1, 0, 5ull, status, spin_limit);
+}
+
 }  // namespace
+
+cudaError_t launch_wait_selftest(cudaStream_t st, unsigned long long* desc2, unsigned* status, unsigned spin_limit) {
+    k_wait_selftest<<<1, 32, 0, st>>>(desc2, status, spin_limit);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_radix_sort(cudaStream_t st, const StepParams* sp, int passes, unsigned long long capacity,
                               unsigned long long* keys0, unsigned* vals0, unsigned long long* keys1,
                               unsigned* vals1, unsigned long long* desc, unsigned long long desc_stride,
-                              Control* ctrl, int* which) {
+                              Control* ctrl, int* which, cudaEvent_t after_hist) {
     *which = 0;
     if (capacity == 0 || passes <= 0) return cudaSuccess;
     static bool attr_set = false;
@@ -190,6 +201,7 @@ cudaError_t launch_radix_sort(cudaStream_t st, const StepParams* sp, int passes,
     k_radix_hist<<<2 * 148, kHistThreads, 0, st>>>(keys0, capacity, passes, ctrl);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
+    if (after_hist && (e = cudaEventRecord(after_hist, st)) != cudaSuccess) return e;
     const unsigned long long tiles = (capacity + kSortTile - 1) / kSortTile;
     unsigned long long* kin = keys0;
     unsigned* vin = vals0;

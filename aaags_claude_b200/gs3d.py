@@ -22,7 +22,8 @@ LIB_PATH = os.path.join(PKG, "libgs3d_cuda.so")
 
 OK = 0
 ERR_INVALID_ARG, ERR_CUDA, ERR_PAIR_OVERFLOW, ERR_DEVICE_TIMEOUT, ERR_NO_MODEL, ERR_OOM, ERR_STATE = range(1, 8)
-OPT_PAIR_CAPACITY, OPT_USE_GRAPH, OPT_FORM, OPT_SPIN_LIMIT = 1, 2, 3, 4
+OPT_PAIR_CAPACITY, OPT_USE_GRAPH, OPT_FORM, OPT_SPIN_LIMIT, OPT_STAGE_TIMING = 1, 2, 3, 4, 5
+NUM_STAGES = 8
 STAT_TOTAL_PAIRS, STAT_PAIR_CAPACITY, STAT_KERNELS_LAST, STAT_SORT_PASSES, STAT_GRAPH_REPLAYS, STAT_ADAM_STEP = range(1, 7)
 FORM_PLAIN_FP32 = 0
 
@@ -78,6 +79,8 @@ def load_library(path: str = LIB_PATH):
         "gs3dc_optimizer_step": ([vp, vp, ctypes.c_int], ctypes.c_int),
         "gs3dc_train_step": ([vp, vp, vp, ctypes.c_int, vp, vp, ctypes.c_int, vp], ctypes.c_int),
         "gs3dc_synchronize": ([vp], ctypes.c_int),
+        "gs3dc_get_stage_times": ([vp, ctypes.POINTER(ctypes.c_float), ctypes.c_int], ctypes.c_int),
+        "gs3dc_selftest_bounded_wait": ([vp, ctypes.c_uint32], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -153,6 +156,16 @@ class Context:
 
     def synchronize(self):
         self._chk(self.L.gs3dc_synchronize(self.h))
+
+    def selftest_bounded_wait(self, spin_limit: int) -> int:
+        """Status of a device wait on a flag nothing sets (expected: ERR_DEVICE_TIMEOUT)."""
+        return int(self.L.gs3dc_selftest_bounded_wait(self.h, int(spin_limit)))
+
+    def stage_times(self) -> list[float]:
+        """Per-stage device ms of the last train step run with OPT_STAGE_TIMING."""
+        a = (ctypes.c_float * NUM_STAGES)()
+        self._chk(self.L.gs3dc_get_stage_times(self.h, a, NUM_STAGES))
+        return list(a)
 
     # ---- model ----
     def set_gaussians(self, scene: S.Scene, act: dict):

@@ -1,0 +1,429 @@
+#!/usr/bin/env python
+"""Benchmark of the 3DGS training step (Trainer::step) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload: the plain-FP32 training step on 1M Gaussians at 1920x1080 (seeded
+synthetic scene: means ~ N(0, 0.5^2 I3), log-scales ~ N(-4.5, 0.5^2), unit
+N(0, I4) quaternions, opacity logits ~ N(0, 1), SH degree 3; target = render of
+the perturbed scene; one camera on the radius-3 sphere; L1 loss; Adam with
+lr 1.6e-4 for means and 1e-3 for the rest).  A step is preprocess -> binning ->
+radix sort -> tile ranges -> rasterise + L1 -> rasterise backward ->
+preprocess backward + Adam, replayed as one CUDA graph.
+
+Prints ONE JSON line (rank 0).  `value` is whole-job steps/s with inputs
+resident in HBM, timed with CUDA events on the library's stream and maxed over
+ranks; `e2e` is the same step through the public API with the target image
+copied from pinned host memory and the loss read back every step.
+Multi-GPU runs are independent replicas (the path does not shard; no
+collective is on the data path), so scaling is weak.
+
+`--impl reference` times the reference's own CPU Trainer::step (built from its
+sources into oracle/_ref) on the host cores, one process per replica.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "fwd+bwd steps/s & MPix/s, 1M Gaussians 1080p, chosen form vs plain FP32, same GPU"
+WORKLOAD = "train_step_1M_gaussians_1920x1080_sh3_l1_adam"
+STAGES = ["memsets", "preprocess", "sort_hist", "sort_passes", "ranges", "raster_fwd", "raster_bwd",
+          "preprocess_bwd_adam"]
+
+
+def _args(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the timed reference CPU step")
+    ap.add_argument("--gaussians", type=int, default=1_000_000, help="scene size (profiling cases use less)")
+    ap.add_argument("--size", default="1920x1080", help="WxH of the camera")
+    return ap.parse_args(argv)
+
+
+def _dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def _workload(a):
+    """The training workload: 1M Gaussians at 1920x1080 unless --gaussians / --size shrink it."""
+    from aaags_claude_b200 import scenes as S
+    W, H = (int(x) for x in a.size.lower().split("x"))
+    if a.gaussians == 1_000_000 and (W, H) == (1920, 1080):
+        w = S.config_train_1m_1080p()
+    else:
+        sc = S.random_scene(a.gaussians)
+        cam = S.sphere_cameras(1, resolutions=[(W, H)])[0]
+        w = S.Workload(f"train_{a.gaussians}_{W}x{H}", sc, [cam], S.perturbed(sc))
+    return w, S.render_config(True), S.train_config()
+
+
+def _workload_name(a) -> str:
+    if a.gaussians == 1_000_000 and a.size == "1920x1080":
+        return WORKLOAD
+    return f"train_step_{a.gaussians}_gaussians_{a.size}_sh3_l1_adam"
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples every 200 ms during a region."""
+
+    Q = ("index,pci.bus_id,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, bus_id: str | None):
+        self.bus_id = (bus_id or "").lower()
+        self.f = tempfile.TemporaryFile(mode="w+")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self) -> dict:
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.seek(0)
+        rows = []
+        for line in self.f.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 10:
+                continue
+            if self.bus_id and self.bus_id[-12:] not in parts[1].lower():
+                continue
+            rows.append(parts)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        mx = [float(r[3]) for r in rows if r[3].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[6 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def _bus_id(dev: int) -> str | None:
+    try:
+        out = subprocess.run(["nvidia-smi", "--query-gpu=index,pci.bus_id", "--format=csv,noheader"],
+                             capture_output=True, text=True, timeout=20).stdout
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+        phys = int(vis.split(",")[dev]) if vis and vis.split(",")[dev].strip().isdigit() else dev
+        for line in out.splitlines():
+            i, bus = [x.strip() for x in line.split(",")]
+            if int(i) == phys:
+                return bus
+    except Exception:
+        pass
+    return None
+
+
+# ---------------------------------------------------------------- roofline
+def stage_bytes(N: int, P: int, X: int, T: int, passes: int, mc3: int = 48) -> dict:
+    """Algorithmic (compulsory) DRAM bytes of one launch of each stage (plain FP32).
+
+    s_p = 4*(11 + mc3) bytes of parameters per Gaussian, s_m = 2*s_p of Adam
+    moments; P tile pairs; X pixels; T tiles.
+    """
+    sp = 4 * (11 + mc3)
+    return {
+        "preprocess": N * (sp + 48) + P * 12,          # params in; record+depth+radius+tiles out; pairs out
+        "sort_hist": P * 8,                              # keys in
+        "sort_passes": P * 24,                           # per pass: key+value in and out
+        "ranges": P * 8 + T * 8,
+        "raster_fwd": P * 40 + X * 37,                   # index + gathered record; image/T/n/last/sign out, gt in
+        "raster_bwd": P * 40 + X * 9 + N * 36,           # index + record; T/last/sign in; screen grads out
+        "preprocess_bwd_adam": N * (2 * sp + 4 * sp + 2 * 36 + 4 + 16),  # params, m, v in+out; grads in + zeroed
+    }
+
+
+def _traffic_table():
+    p = os.path.join(ROOT, "profiles", "dram_traffic.json")
+    return json.load(open(p)) if os.path.exists(p) else None
+
+
+# ---------------------------------------------------------------- CPU baseline
+def cpu_baseline_reference(w, cfg, tc, gt: np.ndarray) -> dict | None:
+    """One full reference Trainer::step (oracle/_ref) on 1 host core."""
+    from oracle import pyoracle as O
+    import ctypes
+    kind = "reference" if O.have_ref() else "port"
+    scene = w.scene.copy()
+    raw = scene.raw_struct()
+    cam = w.cameras[0]
+    t0 = time.perf_counter()
+    if kind == "reference":
+        L = O.lib_ref()
+        tr = L.ref_trainer_create(ctypes.c_size_t(6 << 30))
+        loss = ctypes.c_float()
+        t0 = time.perf_counter()
+        rc = L.ref_trainer_step(tr, ctypes.addressof(raw), ctypes.addressof(cam), gt.ctypes.data,
+                                ctypes.addressof(cfg), ctypes.addressof(tc), 0, ctypes.addressof(loss))
+        dt = time.perf_counter() - t0
+        L.ref_trainer_destroy(tr)
+        if rc:
+            return None
+    else:
+        st = O.AdamOracle(scene.count, scene.max_coeffs * 3)
+        t0 = time.perf_counter()
+        O.train_step(scene, cam, gt, cfg, tc, 0, st, "c", cap=16_000_000)
+        dt = time.perf_counter() - t0
+    return {"value": 1.0 / dt, "unit": "steps/s", "cores": 1, "kind": kind,
+            "sample": f"1 full Trainer::step (1M Gaussians, 1920x1080, Adam) on 1 thread: {dt:.2f} s"}
+
+
+# ---------------------------------------------------------------- our arm
+def run_ours(a) -> int:
+    import torch
+    rank, world, local = _dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from aaags_claude_b200 import gs3d
+    from aaags_claude_b200 import scenes as S
+
+    w, cfg, tc = _workload(a)
+    cam = w.cameras[0]
+    W, H = cam.width, cam.height
+    ctx = gs3d.Context(local)
+    # target image: the perturbed scene rendered by this library (setup, untimed)
+    ctx.set_raw_params(w.target_scene)
+    gt = ctx.render(cam, S.render_config(False))
+    ctx.set_raw_params(w.scene)
+    gt_dev = torch.from_numpy(gt).to(f"cuda:{local}")
+    gt_pin = torch.from_numpy(gt).pin_memory()
+    stream = torch.cuda.ExternalStream(ctx.stream_handle(), device=f"cuda:{local}")
+
+    it = 0
+    loss0 = ctx.train_step(cam, None, cfg, tc, it, gt_device_ptr=gt_dev.data_ptr())   # sizes the pair buffers
+    it += 1
+    for _ in range(max(a.warmup, 3)):
+        ctx.train_step(cam, None, cfg, tc, it, want_loss=False, gt_device_ptr=gt_dev.data_ptr())
+        it += 1
+    ctx.synchronize()
+    P = ctx.stat(gs3d.STAT_TOTAL_PAIRS)
+    passes = ctx.stat(gs3d.STAT_SORT_PASSES)
+
+    # ---- value: inputs resident in HBM, graph replay, CUDA events on the library stream ----
+    clocks = ClockSampler(_bus_id(local))
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(a.steps):
+        ctx.train_step(cam, None, cfg, tc, it, want_loss=False, gt_device_ptr=gt_dev.data_ptr())
+        it += 1
+    e1.record(stream)
+    ctx.synchronize()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    ms_total = e0.elapsed_time(e1)
+    launches = ctx.stat(gs3d.STAT_KERNELS_LAST) * a.steps
+    graph = ctx.stat(gs3d.STAT_GRAPH_REPLAYS) > 0
+
+    # ---- e2e: pinned host target in, loss out, every step ----
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        loss = ctx.train_step(cam, gt_pin.numpy(), cfg, tc, it)
+        it += 1
+    e2e_s = time.perf_counter() - t0
+
+    # ---- per-stage device times (un-captured steps, events between stages) ----
+    ctx.set_option(gs3d.OPT_STAGE_TIMING, 1)
+    acc = np.zeros(len(STAGES))
+    nt = max(3, min(a.steps, 10))
+    for _ in range(nt):
+        ctx.train_step(cam, None, cfg, tc, it, gt_device_ptr=gt_dev.data_ptr())
+        it += 1
+        acc += np.array(ctx.stage_times())
+    ctx.set_option(gs3d.OPT_STAGE_TIMING, 0)
+    stage_ms = acc / nt
+
+    vals = torch.tensor([ms_total, e2e_s], dtype=torch.float64, device=f"cuda:{local}")
+    if dist:
+        dist.all_reduce(vals, op=dist.ReduceOp.MAX)
+    ms_total, e2e_s = float(vals[0]), float(vals[1])
+
+    if rank == 0:
+        X = W * H
+        T = ((W + 15) // 16) * ((H + 15) // 16)
+        ms_step = ms_total / a.steps
+        value = world * a.steps / (ms_total / 1e3)
+        peak, peak_kind = _peaks()
+        nbytes = stage_bytes(w.scene.count, P, X, T, passes)
+        per_launch_ms = {s: stage_ms[k] / (passes if s == "sort_passes" else 1) for k, s in enumerate(STAGES)}
+        dom = max((s for s in STAGES if s != "memsets"), key=lambda s: stage_ms[STAGES.index(s)])
+        achieved = nbytes[dom] / (per_launch_ms[dom] * 1e-3) / 1e9
+        traffic = None
+        tt = _traffic_table()
+        if tt and dom in tt.get("kernels", {}):
+            k = tt["kernels"][dom]
+            traffic = k["bytes_per_launch"] * (P / k["pairs"] if k.get("scale") == "pairs" else 1.0)
+        step_bytes = sum(nbytes[s] * (passes if s == "sort_passes" else 1) for s in nbytes)
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": "steps/s", "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded; no dataset or checkpoint)",
+            "form": "plain_fp32",
+            "config": {"workload": _workload_name(a), "gaussians": w.scene.count, "sh_degree": 3, "width": W,
+                       "height": H,
+                       "tile": 16, "tile_pairs": P, "sort_passes": passes,
+                       "l2": "working set ~1.6 GB per step > 126 MB L2 (no flush needed)",
+                       "parallelism": f"replicas x{world}", "cuda_graph": graph},
+            "mpix_per_s": round(value * X / 1e6, 2),
+            "e2e": {"value": round(world * a.steps / e2e_s, 3), "unit": "steps/s",
+                    "h2d_bytes_per_step": int(X * 3 * 4 + 512), "d2h_bytes_per_step": 24,
+                    "api": "gs3dc_train_step(gt host pinned, loss read back)"},
+            "gpu_launches": int(launches),
+            "stage_ms": {s: round(float(stage_ms[k]), 4) for k, s in enumerate(STAGES)},
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                         "traffic": traffic, "algorithmic_bytes_per_launch": int(nbytes[dom])},
+            "step_roofline": {"algorithmic_bytes": int(step_bytes),
+                              "frac": round(step_bytes / (ms_step * 1e-3) / 1e9 / peak, 4)},
+            "sort_keys_per_s": round(P * passes / (stage_ms[STAGES.index('sort_passes')] * 1e-3), 1),
+            "loss_first": loss0, "loss_last": loss,
+            "clocks": clk,
+        }
+        if world == 1 and not a.no_cpu_baseline and _workload_name(a) == WORKLOAD:
+            line["cpu_baseline"] = cpu_baseline_reference(w, cfg, tc, gt)
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+# ---------------------------------------------------------------- reference arm
+def _ref_worker(path: str, n_steps: int, barrier, out_q):
+    import ctypes
+    sys.path.insert(0, ROOT)
+    from aaags_claude_b200 import scenes as S
+    from oracle import pyoracle as O
+    z = np.load(path)
+    sc = S.Scene(z["pos"].copy(), z["sc"].copy(), z["rot"].copy(), z["sh"].copy(), z["op"].copy(), 3)
+    cam = S.Camera.from_buffer_copy(z["cam"].tobytes())
+    cfg = S.RenderConfig.from_buffer_copy(z["cfg"].tobytes())
+    tc = S.TrainConfig.from_buffer_copy(z["tc"].tobytes())
+    gt = np.ascontiguousarray(z["gt"])
+    L = O.lib_ref()
+    tr = L.ref_trainer_create(ctypes.c_size_t(6 << 30))
+    raw = sc.raw_struct()
+    loss = ctypes.c_float()
+    args = (ctypes.addressof(raw), ctypes.addressof(cam), gt.ctypes.data, ctypes.addressof(cfg), ctypes.addressof(tc))
+    rc = L.ref_trainer_step(tr, *args, 0, ctypes.addressof(loss))   # warm-up (untimed)
+    barrier.wait()
+    t0 = time.perf_counter()
+    for i in range(n_steps):
+        rc |= L.ref_trainer_step(tr, *args, i + 1, ctypes.addressof(loss))
+    out_q.put((time.perf_counter() - t0, n_steps, rc, float(loss.value)))
+
+
+def run_reference(a) -> int:
+    rank, world, _ = _dist_env()
+    if rank != 0:
+        return 0
+    base = {"metric": METRIC, "impl": "reference", "unit": "steps/s", "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded; no dataset or checkpoint)"}
+    from oracle import pyoracle as O
+    if not O.have_ref():
+        base["unavailable"] = "oracle/_ref/libgs3d_ref.so was not built (needs the reference tree at build time)"
+        print(json.dumps(base), flush=True)
+        return 0
+    import ctypes
+    from aaags_claude_b200 import scenes as S
+    w, cfg, tc = _workload(a)
+    cam = w.cameras[0]
+    # target: the reference renders the perturbed scene (setup, untimed)
+    act = O.activate_ref(w.target_scene)
+    g = O.gaussians_struct(w.target_scene, act)
+    L = O.lib_ref()
+    rend = L.ref_renderer_create(ctypes.c_size_t(4 << 30))
+    gt = np.zeros(cam.width * cam.height * 3, np.float32)
+    L.ref_renderer_render(rend, ctypes.addressof(g), ctypes.addressof(cam), ctypes.addressof(S.render_config(False)),
+                          gt.ctypes.data)
+    L.ref_renderer_destroy(rend)
+    cores = os.cpu_count() or 1
+    try:
+        avail = os.sysconf("SC_AVPHYS_PAGES") * os.sysconf("SC_PAGE_SIZE")
+    except (ValueError, OSError):
+        avail = 64 << 30
+    replicas = max(1, min(cores, a.steps, int(avail // (6 << 30))))
+    shares = [a.steps // replicas + (1 if r < a.steps % replicas else 0) for r in range(replicas)]
+    tmp = os.path.join(tempfile.gettempdir(), f"gs3d_ref_bench_{os.getpid()}.npz")
+    np.savez(tmp, pos=w.scene.positions, sc=w.scene.scales, rot=w.scene.rotations, sh=w.scene.sh,
+             op=w.scene.opacities, cam=np.frombuffer(bytes(cam), np.uint8), cfg=np.frombuffer(bytes(cfg), np.uint8),
+             tc=np.frombuffer(bytes(tc), np.uint8), gt=gt)
+    ctxm = mp.get_context("spawn")
+    barrier = ctxm.Barrier(replicas)
+    q = ctxm.Queue()
+    procs = [ctxm.Process(target=_ref_worker, args=(tmp, shares[r], barrier, q)) for r in range(replicas)]
+    for p in procs:
+        p.start()
+    res = [q.get() for _ in procs]
+    for p in procs:
+        p.join()
+    os.remove(tmp)
+    wall = max(r[0] for r in res)
+    total = sum(r[1] for r in res)
+    value = total / wall
+    base.update({
+        "value": round(value, 5), "ms_per_step": round(1e3 / value, 1),
+        "config": {"workload": _workload_name(a), "gaussians": w.scene.count, "sh_degree": 3, "width": cam.width,
+                   "height": cam.height, "tile": 16, "parallelism": f"{replicas} single-thread replicas"},
+        "cpu_baseline": {"value": round(value, 5), "unit": "steps/s", "cores": replicas, "kind": "reference",
+                         "sample": f"{total} full Trainer::step (1M, 1920x1080, Adam) across {replicas} "
+                                   f"single-thread processes after 1 warm-up step each"},
+        "e2e": {"value": round(value, 5), "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "status": "ok" if all(r[2] == 0 for r in res) else "reference step returned an error",
+    })
+    print(json.dumps(base), flush=True)
+    return 0
+
+
+def main(argv=None) -> int:
+    a = _args(argv)
+    if a.impl == "reference":
+        return run_reference(a)
+    return run_ours(a)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -43,6 +43,7 @@ typedef struct gs3dc_ctx gs3dc_ctx;
 #define GS3DC_OPT_USE_GRAPH      2  /* 1: gs3dc_train_step replays a captured CUDA graph (default 1) */
 #define GS3DC_OPT_FORM           3  /* GS3DC_FORM_* precision form of gs3dc_train_step / gs3dc_render */
 #define GS3DC_OPT_SPIN_LIMIT     4  /* iterations before a device-side wait gives up (test hook) */
+#define GS3DC_OPT_STAGE_TIMING   5  /* 1: train steps run un-captured with CUDA events between stages */
 
 #define GS3DC_FORM_PLAIN_FP32    0  /* FP32 everywhere, no FMA contraction: parity form */
 
@@ -167,6 +168,26 @@ int gs3dc_optimizer_step(gs3dc_ctx* ctx, const gs3d_train_config* tc, int iterat
 int gs3dc_train_step(gs3dc_ctx* ctx, const gs3d_camera* cam, const float* gt, int gt_on_device,
                      const gs3d_render_config* cfg, const gs3d_train_config* tc, int iteration,
                      float* loss);
+
+/* Device time per stage of the last train step run with GS3DC_OPT_STAGE_TIMING,
+ * measured with CUDA events on the context's stream.  ms[k] for k < n_stages,
+ * indexed by GS3DC_STAGE_*. */
+#define GS3DC_STAGE_MEMSETS        0  /* control block, sort scratch, tile ranges */
+#define GS3DC_STAGE_PREPROCESS     1  /* activation + projection + scan + pair emission */
+#define GS3DC_STAGE_SORT_HIST      2
+#define GS3DC_STAGE_SORT_PASSES    3  /* all onesweep passes together */
+#define GS3DC_STAGE_RANGES         4
+#define GS3DC_STAGE_RASTER_FWD     5  /* incl. the fused L1 */
+#define GS3DC_STAGE_RASTER_BWD     6
+#define GS3DC_STAGE_PREPROCESS_BWD 7  /* incl. the fused optimiser */
+#define GS3DC_NUM_STAGES           8
+int gs3dc_get_stage_times(gs3dc_ctx* ctx, float* ms, int n_stages);
+
+/* Runs one device-side wait on a flag that nothing sets, bounded by spin_limit
+ * polls (1..2^24).  Returns GS3DC_ERR_DEVICE_TIMEOUT when the bound works; the
+ * context stays usable afterwards.  No reference counterpart: it exercises the
+ * bounded-wait failure path that every look-back of this library relies on. */
+int gs3dc_selftest_bounded_wait(gs3dc_ctx* ctx, uint32_t spin_limit);
 
 /* Blocks until every call issued on the context's stream has finished and
  * reports any deferred device-side error (pair overflow, timeout). */

@@ -103,6 +103,7 @@ def lib_ref():
         L.ref_renderer_destroy.argtypes = [ctypes.c_void_p]
         L.ref_renderer_render.restype = ctypes.c_int
         L.ref_renderer_render.argtypes = [ctypes.c_void_p] * 5
+        L.ref_activate.argtypes = [ctypes.c_void_p] * 2
         _LIBS["ref"] = L
     return _LIBS["ref"]
 
@@ -201,6 +202,18 @@ def activate(scene):
                                    scene.opacities)],
                        *[_ptr(x, _f) for x in out])
     return dict(positions=out[0], scales=out[1], rotations=out[2], sh_coeffs=out[3], opacities=out[4])
+
+
+def activate_ref(scene):
+    """The reference's own RawGaussianParams::activate (oracle/_ref)."""
+    n, mc3 = scene.count, scene.max_coeffs * 3
+    act = dict(positions=np.empty(3 * n, np.float32), scales=np.empty(3 * n, np.float32),
+               rotations=np.empty(4 * n, np.float32), sh_coeffs=np.empty(mc3 * n, np.float32),
+               opacities=np.empty(n, np.float32))
+    g = gaussians_struct(scene, act)
+    raw = scene.raw_struct()
+    lib_ref().ref_activate(ctypes.addressof(raw), ctypes.addressof(g))
+    return act
 
 
 def gaussians_struct(scene, act: dict):

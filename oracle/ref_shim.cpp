@@ -124,6 +124,11 @@ int ref_forward(const gs3d_gaussians* gp, const gs3d_camera* camp, const gs3d_re
     return 0;
 }
 
+// RawGaussianParams::activate (train_types.cpp:6-36) into caller arrays.
+void ref_activate(const gs3d_raw_params* rawp, gs3d_gaussians* gp) {
+    reinterpret_cast<const RawGaussianParams*>(rawp)->activate(*reinterpret_cast<GaussianData*>(gp));
+}
+
 void* ref_adam_create(void) { return new (std::nothrow) AdamHandle(); }
 void ref_adam_destroy(void* h) { delete static_cast<AdamHandle*>(h); }
 

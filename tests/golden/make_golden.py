@@ -1,0 +1,161 @@
+"""Regenerates the committed golden fixtures under tests/golden/.
+
+    python tests/golden/make_golden.py
+
+Two kinds of fixtures, both produced by the reference itself:
+
+* ref_fixtures/  the reference repository's own golden vectors, copied verbatim
+  (data files only): train/verify_grads_ext/<scene>/ (inputs, cpp_rendered.bin,
+  cpp_loss.bin, cpp_grad_raw_*.bin), train/verify_forward/, and
+  tests/test_data/l1_verify/.
+* seeded/        outputs of the reference's CPU stages (oracle/_ref/libgs3d_ref.so,
+  built from the reference sources by oracle/Makefile) on seeded synthetic
+  scenes, including the edge cases the reference's unit tests cover: ragged
+  tiles, non-black background, antialiasing and scale modifier, SH degrees 0-2,
+  a single Gaussian, every Gaussian culled, oversized splats.
+
+It needs the reference tree at /root/reference (only this script reads it);
+the tests and the GPU runs read the committed copies.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+REF = "/root/reference/harmonyos_3dgs"
+sys.path.insert(0, REPO)
+
+from aaags_claude_b200 import scenes as S  # noqa: E402
+from oracle import pyoracle as O  # noqa: E402
+
+
+def copy_ref_fixtures():
+    dst = os.path.join(HERE, "ref_fixtures")
+    if os.path.isdir(dst):
+        shutil.rmtree(dst)
+    os.makedirs(dst)
+    srcs = {f"verify_grads_ext/{d}": os.path.join(REF, "train", "verify_grads_ext", d)
+            for d in sorted(os.listdir(os.path.join(REF, "train", "verify_grads_ext")))}
+    srcs["verify_forward"] = os.path.join(REF, "train", "verify_forward")
+    srcs["l1_verify"] = os.path.join(REF, "tests", "test_data", "l1_verify")
+    for name, src in srcs.items():
+        out = os.path.join(dst, name)
+        os.makedirs(out, exist_ok=True)
+        for f in sorted(os.listdir(src)):
+            if f.endswith((".bin", ".json")):
+                shutil.copyfile(os.path.join(src, f), os.path.join(out, f))
+
+
+# ---- seeded cases ----
+
+def _single_scene():
+    s = S.random_scene(1, sh_degree=3, seed=11)
+    s.positions[:] = [[0.05, -0.02, 0.0]]
+    s.scales[:] = -2.5
+    s.opacities[:] = 2.0
+    return s
+
+
+def _culled_scene():
+    s = S.random_scene(64, sh_degree=1, seed=12)
+    s.positions[:, 2] = 10.0 + s.positions[:, 2]    # behind a camera at z=+3 that looks towards -z
+    return s
+
+
+def _big_scene():
+    s = S.random_scene(200, sh_degree=2, seed=13)
+    s.scales[:20] = 1.5       # screen radius > max(W, H): culled by the radius test
+    s.scales[20:60] = -1.0    # large but kept
+    return s
+
+
+def _scene_with_degree(n, deg, seed):
+    return S.random_scene(n, sh_degree=deg, seed=seed)
+
+
+def render_cases():
+    """(name, scene, camera, render config) of the forward fixtures."""
+    cam128 = S.look_at_camera((0.0, 0.0, -3.0), 128, 128)
+    cases = [
+        ("render_2k_128x128", S.random_scene(2000), cam128, S.render_config(False)),
+        ("render_ragged_100x37_bg", _scene_with_degree(500, 1, 21),
+         S.look_at_camera((0.4, 0.3, -2.5), 100, 37, 50.0), S.render_config(False, 1, bg=(0.2, 0.5, 0.9))),
+        ("render_deg0_64x48", _scene_with_degree(300, 0, 22), S.look_at_camera((0.0, 0.0, 3.0), 64, 48),
+         S.render_config(False, 0)),
+        ("render_deg2_train_80x80", _scene_with_degree(400, 2, 23), S.look_at_camera((1.0, 1.0, -2.5), 80, 80),
+         S.render_config(True, 2)),
+        ("render_single_33x17", _single_scene(), S.look_at_camera((0.0, 0.0, -3.0), 33, 17),
+         S.render_config(False)),
+        ("render_all_culled_64x64", _culled_scene(), S.look_at_camera((0.0, 0.0, 3.0), 64, 64),
+         S.render_config(False, 1)),
+        ("render_oversized_96x64", _big_scene(), S.look_at_camera((0.0, 0.5, -3.0), 96, 64),
+         S.render_config(False, 2)),
+    ]
+    aa = S.render_config(False)
+    aa.antialiasing = True
+    aa.scale_modifier = 1.7
+    cases.append(("render_aa_scale_64x48", S.random_scene(300, seed=24), S.look_at_camera((0.2, -0.1, -3.0), 64, 48),
+                  aa))
+    return cases
+
+
+def _canon(keys, vals):
+    o = np.lexsort((vals, keys))
+    return keys[o], vals[o]
+
+
+def scene_arrays(s):
+    return dict(in_positions=s.positions, in_scales=s.scales, in_rotations=s.rotations, in_sh=s.sh,
+                in_opacities=s.opacities, in_sh_degree=np.int32(s.sh_degree))
+
+
+def cam_arrays(cam, cfg):
+    return dict(cam_bytes=np.frombuffer(bytes(cam), np.uint8), cfg_bytes=np.frombuffer(bytes(cfg), np.uint8))
+
+
+def make_seeded():
+    dst = os.path.join(HERE, "seeded")
+    os.makedirs(dst, exist_ok=True)
+    for name, sc, cam, cfg in render_cases():
+        r = O.forward(sc, cam, cfg, "ref")
+        ks, vs = _canon(r.keys_sorted, r.vals_sorted)
+        np.savez_compressed(
+            os.path.join(dst, name + ".npz"), **scene_arrays(sc), **cam_arrays(cam, cfg),
+            radii=r.radii, tiles=r.tiles, depths=r.depths, means2D=r.means2D, conics=r.conics,
+            opac2d=r.opac2d, rgb=r.rgb, cov3D=r.cov3D, p_view=r.p_view, p_hom_w=r.p_hom_w, cov2D=r.cov2D,
+            det=r.det, total_pairs=np.int64(r.total_pairs), keys_unsorted=r.keys_unsorted,
+            vals_unsorted=r.vals_unsorted, keys_sorted=ks, vals_sorted=vs, ranges=r.ranges, image=r.image,
+            T_final=r.T_final, n_contrib=r.n_contrib)
+        print(name, "P", r.total_pairs)
+    # training: two Adam steps of Trainer::step on the 2k scene
+    sc = S.random_scene(2000)
+    cam = S.look_at_camera((0.0, 0.0, -3.0), 128, 128)
+    gt = O.forward(S.perturbed(sc), cam, S.render_config(False), "ref").image
+    cfg, tc = S.render_config(True), S.train_config()
+    work = sc.copy()
+    adam = O.RefAdam()
+    out = dict(**scene_arrays(sc), **cam_arrays(cam, cfg), tc_bytes=np.frombuffer(bytes(tc), np.uint8), gt=gt)
+    for it in range(2):
+        r = O.train_step(work, cam, gt, cfg, tc, it, adam, "ref")
+        out.update({f"s{it}_loss": np.float32(r.loss), f"s{it}_loss_acc64": np.float64(r.loss_acc64),
+                    f"s{it}_image": r.image, f"s{it}_d_means2D": r.d_means2D, f"s{it}_d_conics": r.d_conics,
+                    f"s{it}_d_rgb": r.d_rgb, f"s{it}_d_opac": r.d_opac, f"s{it}_g_pos": r.g_pos,
+                    f"s{it}_g_sc": r.g_sc, f"s{it}_g_rot": r.g_rot, f"s{it}_g_sh": r.g_sh, f"s{it}_g_op": r.g_op,
+                    f"s{it}_positions": work.positions.copy(), f"s{it}_scales": work.scales.copy(),
+                    f"s{it}_rotations": work.rotations.copy(), f"s{it}_sh": work.sh.copy(),
+                    f"s{it}_opacities": work.opacities.copy()})
+    np.savez_compressed(os.path.join(dst, "train_2k_128x128_adam.npz"), **out)
+    print("train_2k_128x128_adam")
+
+
+if __name__ == "__main__":
+    O.ensure_built(ref=True)
+    if not O.have_ref():
+        sys.exit("oracle/_ref/libgs3d_ref.so is missing: `make -C oracle ref` needs the reference tree")
+    copy_ref_fixtures()
+    make_seeded()

@@ -1,0 +1,175 @@
+"""CPU: the C ABI library and the host-side logic, without a GPU.
+
+* libgs3d_cuda.so loads and exports every entry point include/gs3d_cuda.h declares;
+* without a usable device gs3dc_create fails with a status, never falls back;
+* the C structs have the reference's layouts (a C probe compiled here prints
+  sizeof / offsetof; the ctypes mirrors and the reference headers must agree);
+* the synthetic workload generators are deterministic and well-formed.
+"""
+import ctypes
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+from aaags_claude_b200 import gs3d
+from aaags_claude_b200 import scenes as S
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF_INCLUDE = "/root/reference/harmonyos_3dgs/include"
+
+
+def _lib_path():
+    if not os.path.exists(gs3d.LIB_PATH):
+        from aaags_claude_b200 import build
+        build.build()
+    return gs3d.LIB_PATH
+
+
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(_lib_path())
+    declared = gs3d.exported_symbols()
+    assert len(declared) >= 20
+    missing = [s for s in declared if not hasattr(lib, s)]
+    assert not missing, missing
+
+
+def test_oracle_libraries_export_their_symbols():
+    from oracle import pyoracle as O
+    L = O.lib_c()
+    for s in ("orc_forward", "orc_train_step", "orc_step_f64", "orc_sort", "orc_bin", "orc_preprocess_f32",
+              "orc_raster_backward_f32", "orc_preprocess_backward_f32", "orc_adam_update_f32"):
+        assert hasattr(L, s), s
+    if O.have_ref():
+        R = O.lib_ref()
+        for s in ("ref_forward", "ref_train_step", "ref_trainer_step", "ref_renderer_render", "ref_activate"):
+            assert hasattr(R, s), s
+
+
+def _has_gpu() -> bool:
+    try:
+        out = subprocess.run(["nvidia-smi", "-L"], capture_output=True, text=True, timeout=10)
+        return out.returncode == 0 and "GPU" in out.stdout
+    except Exception:
+        return False
+
+
+@pytest.mark.skipif(_has_gpu(), reason="a GPU is present")
+def test_create_fails_cleanly_without_a_device():
+    lib = gs3d.load_library()
+    h = ctypes.c_void_p()
+    rc = lib.gs3dc_create(0, ctypes.byref(h))
+    assert rc == gs3d.ERR_CUDA and not h.value
+    with pytest.raises(gs3d.Gs3dError):
+        gs3d.Context(0)
+    assert lib.gs3dc_status_string(gs3d.ERR_PAIR_OVERFLOW) == b"tile-pair capacity overflow"
+
+
+PROBE = r"""
+#include <stdio.h>
+#include <stddef.h>
+#include "gs3d_types.h"
+#include "gs3d_cuda.h"
+#define F(T, m) printf(#T "." #m " %zu\n", offsetof(T, m))
+#define SZ(T) printf(#T " %zu\n", sizeof(T))
+int main(void) {
+  SZ(gs3d_gaussians); F(gs3d_gaussians, positions); F(gs3d_gaussians, filter_3D);
+  SZ(gs3d_camera); F(gs3d_camera, viewproj_matrix); F(gs3d_camera, cam_pos); F(gs3d_camera, tan_fovx);
+  F(gs3d_camera, width); F(gs3d_camera, height);
+  SZ(gs3d_render_config); F(gs3d_render_config, scale_modifier); F(gs3d_render_config, antialiasing);
+  F(gs3d_render_config, training); F(gs3d_render_config, sh_degree); F(gs3d_render_config, tile_h);
+  SZ(gs3d_raw_params); F(gs3d_raw_params, raw_positions); F(gs3d_raw_params, raw_opacities);
+  SZ(gs3d_train_config); F(gs3d_train_config, max_steps); F(gs3d_train_config, use_adam);
+  F(gs3d_train_config, adam_beta1); F(gs3d_train_config, adam_eps);
+  SZ(gs3dc_screen_arrays); F(gs3dc_screen_arrays, cov2D_det);
+  return 0;
+}
+"""
+
+
+def _probe(compiler: str, lang_flags: list[str]) -> dict:
+    with tempfile.TemporaryDirectory() as d:
+        src = os.path.join(d, "probe.c")
+        exe = os.path.join(d, "probe")
+        open(src, "w").write(PROBE)
+        subprocess.run([compiler, *lang_flags, "-I", os.path.join(ROOT, "include"), src, "-o", exe], check=True)
+        out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout
+    return {k: int(v) for k, v in (line.rsplit(" ", 1) for line in out.splitlines())}
+
+
+def test_struct_layouts_c_cpp_ctypes_agree():
+    c = _probe("gcc", ["-std=c11", "-x", "c"])
+    cpp = _probe("g++", ["-std=c++17", "-x", "c++"])
+    assert c == cpp
+    for name, cls in (("gs3d_gaussians", S.GaussianData), ("gs3d_camera", S.Camera),
+                      ("gs3d_render_config", S.RenderConfig), ("gs3d_raw_params", S.RawParams),
+                      ("gs3d_train_config", S.TrainConfig), ("gs3dc_screen_arrays", gs3d.ScreenArrays)):
+        assert ctypes.sizeof(cls) == c[name], name
+        for key, off in c.items():
+            if key.startswith(name + "."):
+                assert getattr(cls, key.split(".", 1)[1]).offset == off, key
+
+
+@pytest.mark.skipif(not os.path.isdir(REF_INCLUDE), reason="reference headers not present")
+def test_layouts_match_the_reference_headers():
+    """static_assert sizeof/offsetof of every struct against the reference's C++ types."""
+    src = r"""
+#include <cstddef>
+#include "types.h"
+#include "train_types.h"
+#include "gs3d_types.h"
+#define SAME(A, B) static_assert(sizeof(A) == sizeof(B), #A)
+#define OFF(A, B, a, b) static_assert(offsetof(A, a) == offsetof(B, b), #A "." #a)
+SAME(GaussianData, gs3d_gaussians); OFF(GaussianData, gs3d_gaussians, sh_coeffs, sh_coeffs);
+OFF(GaussianData, gs3d_gaussians, opacities, opacities); OFF(GaussianData, gs3d_gaussians, filter_3D, filter_3D);
+SAME(Camera, gs3d_camera); OFF(Camera, gs3d_camera, cam_pos, cam_pos); OFF(Camera, gs3d_camera, tan_fovy, tan_fovy);
+OFF(Camera, gs3d_camera, height, height);
+SAME(RenderConfig, gs3d_render_config); OFF(RenderConfig, gs3d_render_config, training, training);
+OFF(RenderConfig, gs3d_render_config, sh_degree, sh_degree); OFF(RenderConfig, gs3d_render_config, tile_h, tile_h);
+SAME(RawGaussianParams, gs3d_raw_params); OFF(RawGaussianParams, gs3d_raw_params, raw_opacities, raw_opacities);
+SAME(TrainConfig, gs3d_train_config); OFF(TrainConfig, gs3d_train_config, use_adam, use_adam);
+OFF(TrainConfig, gs3d_train_config, adam_eps, adam_eps);
+int main() { return 0; }
+"""
+    with tempfile.TemporaryDirectory() as d:
+        p = os.path.join(d, "layout.cpp")
+        open(p, "w").write(src)
+        subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-I", REF_INCLUDE, "-I",
+                        "/root/reference/harmonyos_3dgs/src", "-I", os.path.join(ROOT, "include"), p], check=True)
+
+
+def test_workload_generators_are_seeded_and_well_formed():
+    a, b = S.random_scene(1000), S.random_scene(1000)
+    assert all(np.array_equal(getattr(a, k), getattr(b, k)) for k in ("positions", "scales", "rotations", "sh"))
+    assert np.allclose(np.linalg.norm(a.rotations, axis=1), 1.0, atol=1e-6)
+    assert a.sh.shape == (1000, 16, 3)
+    t = S.perturbed(a)
+    assert 0.005 < np.std(t.positions - a.positions) < 0.015
+    assert np.array_equal(t.sh[:, 1:], a.sh[:, 1:])
+    c = S.clustered_scene(5000)
+    assert c.count == 5000 and np.abs(c.positions).max() < 3.5
+
+
+def test_look_at_camera_projects_the_target_to_the_centre():
+    cam = S.look_at_camera((1.0, 2.0, -2.0), 640, 480, 60.0)
+    vp = np.array(cam.viewproj_matrix, np.float64).reshape(4, 4).T
+    v = np.array(cam.view_matrix, np.float64).reshape(4, 4).T
+    R = v[:3, :3]
+    assert np.allclose(R @ R.T, np.eye(3), atol=1e-6)
+    ph = vp @ np.array([0.0, 0.0, 0.0, 1.0])
+    assert abs(ph[0] / ph[3]) < 1e-6 and abs(ph[1] / ph[3]) < 1e-6
+    assert abs(ph[3] - 3.0) < 1e-5        # w = view depth
+    assert abs(cam.tan_fovy - np.tan(np.radians(30))) < 1e-7
+    assert abs(cam.tan_fovx - cam.tan_fovy * 640 / 480) < 1e-6
+
+
+def test_batched_camera_set_matches_the_config():
+    w = S.config_batched_64()
+    assert len(w.cameras) == 64
+    sizes = {(c.width, c.height) for c in w.cameras}
+    assert sizes <= {(320, 240), (640, 480), (1280, 720), (1920, 1080), (3840, 2160)}
+    for c in w.cameras:
+        assert abs(np.linalg.norm(np.array(c.cam_pos)) - 3.0) < 1e-5
+        assert np.tan(np.radians(22.5)) - 1e-6 <= c.tan_fovy <= np.tan(np.radians(37.5)) + 1e-6

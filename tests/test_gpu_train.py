@@ -1,0 +1,184 @@
+"""GPU parity of the backward, the optimiser and the fused train step.
+
+Tolerances (plain FP32 form): image <= 1e-5 abs; gradients elementwise
+|cuda - ref| <= 1e-4 |ref| + 1e-5 max|ref| (FP32 atomics sum in a different
+order than the reference's serial loops); cosine >= 0.999 against the FP64
+oracle's adjoint.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import gsutil as U
+from aaags_claude_b200 import gs3d
+from aaags_claude_b200 import scenes as S
+from oracle import pyoracle as O
+
+pytestmark = pytest.mark.gpu
+
+GRAD_RTOL, GRAD_ATOL_FRAC = 1e-4, 1e-5
+GRADS = (("g_pos", "grad_raw_positions", "pos"), ("g_sc", "grad_raw_scales", "sc"),
+         ("g_rot", "grad_raw_rotations", "rot"), ("g_sh", "grad_raw_sh_coeffs", "sh"),
+         ("g_op", "grad_raw_opacities", "op"))
+
+
+def _grid(cam):
+    return ((cam.width + 15) // 16) * ((cam.height + 15) // 16)
+
+
+def _l1_grad(img, gt):
+    """d_image of the L1 loss (loss.cpp:4-16), float32."""
+    n = img.size
+    inv_n = np.float32(1.0) / np.float32(n)
+    d = np.where(img > gt, inv_n, np.where(img < gt, -inv_n, np.float32(0))).astype(np.float32)
+    return d
+
+
+def _stage_grads(ctx, sc, cam, cfg, gt):
+    """Stage-level forward + backward through the C ABI: (image, raster grads, raw grads)."""
+    ctx.set_raw_params(sc)
+    ctx.preprocess(cam, cfg)
+    P, _, _ = ctx.bin(cam, cfg)
+    ctx.sort(P, _grid(cam))
+    img, T, nc = ctx.rasterize(cam, cfg)
+    rg = ctx.raster_backward(cam, cfg, _l1_grad(img, gt))
+    g = ctx.preprocess_backward(cam, cfg)
+    return img, rg, g
+
+
+@pytest.mark.parametrize("scene", U.grads_ext_scenes())
+def test_grads_ext_fixture_gradients(ctx, scene):
+    """Reference golden gradients (train/verify_grads_ext/<scene>) through the CUDA backward."""
+    sc, cam, cfg, gt, exp = U.load_grads_fixture(os.path.join(U.REF_FIXTURES, "verify_grads_ext", scene))
+    img, _, g = _stage_grads(ctx, sc, cam, cfg, gt)
+    assert np.abs(img - exp["rendered"]).max() <= 1e-5
+    rtol = 2e-4 if scene in U.STALE_GRAD_SCENES else GRAD_RTOL
+    afrac = 1e-4 if scene in U.STALE_GRAD_SCENES else GRAD_ATOL_FRAC
+    for k, ek, _ in GRADS:
+        ok, worst = U.rel_close(g[k], exp[ek], rtol, afrac)
+        assert ok, (scene, k, worst)
+
+
+def test_stage_backward_matches_oracle(ctx):
+    """RasterizerBackward + PreprocessorBackward vs the oracle on 2k Gaussians, 128x128."""
+    z = np.load(os.path.join(U.SEEDED, "train_2k_128x128_adam.npz"))
+    sc = S.Scene(z["in_positions"].copy(), z["in_scales"].copy(), z["in_rotations"].copy(), z["in_sh"].copy(),
+                 z["in_opacities"].copy(), 3)
+    cam = S.Camera.from_buffer_copy(z["cam_bytes"].tobytes())
+    cfg = S.RenderConfig.from_buffer_copy(z["cfg_bytes"].tobytes())
+    img, rg, g = _stage_grads(ctx, sc, cam, cfg, z["gt"])
+    assert np.abs(img - z["s0_image"]).max() <= 1e-5
+    for k in ("d_means2D", "d_conics", "d_rgb"):
+        ok, worst = U.rel_close(rg[k], z[f"s0_{k}"], GRAD_RTOL, GRAD_ATOL_FRAC)
+        assert ok, (k, worst)
+    ok, worst = U.rel_close(rg["d_opac"], z["s0_d_opac"], GRAD_RTOL, GRAD_ATOL_FRAC)
+    assert ok, ("d_opac", worst)
+    for k, _, _ in GRADS:
+        ok, worst = U.rel_close(g[k], z[f"s0_{k}"], GRAD_RTOL, GRAD_ATOL_FRAC)
+        assert ok, (k, worst)
+
+
+def test_train_step_matches_reference_trajectory(ctx):
+    """Two fused Trainer::step calls (Adam) against the reference's own two steps."""
+    z = np.load(os.path.join(U.SEEDED, "train_2k_128x128_adam.npz"))
+    sc = S.Scene(z["in_positions"].copy(), z["in_scales"].copy(), z["in_rotations"].copy(), z["in_sh"].copy(),
+                 z["in_opacities"].copy(), 3)
+    cam = S.Camera.from_buffer_copy(z["cam_bytes"].tobytes())
+    cfg = S.RenderConfig.from_buffer_copy(z["cfg_bytes"].tobytes())
+    tc = S.TrainConfig.from_buffer_copy(z["tc_bytes"].tobytes())
+    ctx.set_raw_params(sc)
+    for it in range(2):
+        loss = ctx.train_step(cam, z["gt"], cfg, tc, it)
+        assert abs(loss - float(z[f"s{it}_loss_acc64"])) <= 1e-6 * float(z[f"s{it}_loss_acc64"])
+        out = ctx.get_raw_params(sc.copy())
+        for k in ("positions", "scales", "rotations", "sh", "opacities"):
+            d = np.abs(getattr(out, k) - z[f"s{it}_{k}"]).max()
+            assert d <= 1e-5, (it, k, d)
+    assert ctx.stat(gs3d.STAT_ADAM_STEP) == 2
+
+
+def test_train_step_graph_matches_eager(ctx):
+    """CUDA-graph replays give the same trajectory as un-captured steps."""
+    sc = S.random_scene(3000, seed=5)
+    cam = S.look_at_camera((0.3, 0.2, -3.0), 160, 120)
+    gt = O.forward(S.perturbed(sc), cam, S.render_config(False), "c").image
+    cfg, tc = S.render_config(True), S.train_config()
+    res = []
+    for graph in (0, 1):
+        ctx.set_option(gs3d.OPT_USE_GRAPH, graph)
+        ctx.set_raw_params(sc)
+        losses = [ctx.train_step(cam, gt, cfg, tc, it) for it in range(4)]
+        res.append((losses, ctx.get_raw_params(sc.copy())))
+    ctx.set_option(gs3d.OPT_USE_GRAPH, 1)
+    assert np.allclose(res[0][0], res[1][0], rtol=1e-6)
+    for k in ("positions", "scales", "rotations", "sh", "opacities"):
+        assert np.abs(getattr(res[0][1], k) - getattr(res[1][1], k)).max() <= 1e-6
+
+
+def test_optimizer_stage_matches_reference(ctx):
+    """Stage-level AdamOptimizer::step on the device equals the fused step."""
+    z = np.load(os.path.join(U.SEEDED, "train_2k_128x128_adam.npz"))
+    sc = S.Scene(z["in_positions"].copy(), z["in_scales"].copy(), z["in_rotations"].copy(), z["in_sh"].copy(),
+                 z["in_opacities"].copy(), 3)
+    cam = S.Camera.from_buffer_copy(z["cam_bytes"].tobytes())
+    cfg = S.RenderConfig.from_buffer_copy(z["cfg_bytes"].tobytes())
+    tc = S.TrainConfig.from_buffer_copy(z["tc_bytes"].tobytes())
+    _stage_grads(ctx, sc, cam, cfg, z["gt"])
+    ctx.optimizer_step(tc, 0)
+    out = ctx.get_raw_params(sc.copy())
+    for k in ("positions", "scales", "rotations", "sh", "opacities"):
+        assert np.abs(getattr(out, k) - z[f"s0_{k}"]).max() <= 1e-5, k
+
+
+def test_adjoint_against_fp64_oracle_and_finite_differences(ctx):
+    """The differentiation check: N=2k, 128x128.  CUDA adjoint vs the FP64
+    oracle's adjoint (cosine >= 0.999 per parameter group and on 200 random
+    parameters) and vs FP64 central finite differences."""
+    w = S.config_fd_2k()
+    sc, cam = w.scene, w.cameras[0]
+    cfg = S.render_config(True)
+    gt = O.forward(w.target_scene, cam, S.render_config(False), "c").image
+    _, _, g = _stage_grads(ctx, sc, cam, cfg, gt)
+    loss64, _, g64 = O.step_f64(sc, cam, cfg, gt)
+    for k, _, k64 in GRADS:
+        assert U.cosine(g[k], g64[k64]) >= 0.999, k
+    p64 = [np.ascontiguousarray(x, np.float64).reshape(-1).copy() for x in
+           (sc.positions, sc.scales, sc.rotations, sc.sh, sc.opacities)]
+    rng = np.random.default_rng(S.SEED_FD)
+    picks = [(int(rng.integers(5)), None) for _ in range(200)]
+    picks = [(grp, int(rng.integers(len(p64[grp])))) for grp, _ in picks]
+    cuda = np.array([g[GRADS[grp][0]][i] for grp, i in picks])
+    ana = np.array([g64[GRADS[grp][2]][i] for grp, i in picks])
+    assert U.cosine(cuda, ana) >= 0.999
+    for h, min_cos in ((1e-6, 0.999), (1e-4, 0.99)):
+        fd = []
+        for grp, i in picks:
+            o = p64[grp][i]
+            p64[grp][i] = o + h
+            lp, _, _ = O.step_f64(sc, cam, cfg, gt, want_grads=False, params64=p64)
+            p64[grp][i] = o - h
+            lm, _, _ = O.step_f64(sc, cam, cfg, gt, want_grads=False, params64=p64)
+            p64[grp][i] = o
+            fd.append((lp - lm) / (2 * h))
+        fd = np.array(fd)
+        assert U.cosine(cuda, fd) >= min_cos, h
+        # the reference's FD tolerance (tools/verify_gradients_extended.py:455-490)
+        within = np.abs(fd - cuda) <= 5e-5 * np.abs(fd).max() + 0.10 * np.maximum(np.abs(fd), np.abs(cuda))
+        assert within.mean() >= (0.99 if h < 1e-5 else 0.95), h
+
+
+def test_recompute_backward_memory_vs_stored_lists(ctx):
+    """The backward keeps 9 bytes per pixel (T_final, last index, L1 signs)
+    instead of a per-pixel contributor list (index + alpha, 8 bytes per
+    contributor, rasterizer_backward_cpu.cpp:40-67): N=100k at 640x480."""
+    w = S.config_render_100k()
+    cam, cfg = w.cameras[0], S.render_config(True)
+    ctx.set_raw_params(w.scene)
+    ctx.preprocess(cam, cfg)
+    P, _, _ = ctx.bin(cam, cfg)
+    ctx.sort(P, _grid(cam))
+    _, _, nc = ctx.rasterize(cam, cfg)
+    stored_list = int(nc.astype(np.int64).sum()) * 8
+    recompute = cam.width * cam.height * 9
+    assert recompute * 10 < stored_list, (recompute, stored_list)
