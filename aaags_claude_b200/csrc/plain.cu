@@ -220,35 +220,35 @@ __device__ __forceinline__ void activate_one(const float rsc[3], const float rq[
 }
 
 // Alpha / transmittance decisions of the front-to-back blend
-// (rasterizer_cpu.cpp:149-166).  exp is evaluated with the accurate expf and
-// re-evaluated correctly rounded when alpha or the next transmittance lies
-// within a few ulp of a threshold, so skip / stop decisions follow the
-// reference's glibc-based ones.
+// (rasterizer_cpu.cpp:149-166).  A Gaussian that is clearly below the alpha
+// threshold is skipped on the accurate expf alone; every other evaluation --
+// within a few ulp of the threshold, or accepted -- recomputes exp correctly
+// rounded, so alpha, the transmittance chain T and the stop decision follow
+// the reference's glibc-based values (they differ only where glibc's expf is
+// itself 1 ulp off, ~0.006% of inputs).
 // Returns 0 = skip, 1 = blend, 2 = stop (transmittance would saturate).
 __device__ __forceinline__ int blend_decision(float power, float o, float T, float& alpha, float& e,
                                               float& test_T) {
     e = expf(power);
     alpha = fmin_ref(0.99f, o * e);
-    test_T = T * (1.0f - alpha);
-    if (fabsf(alpha - kAlphaMin) < 1e-8f || fabsf(test_T - kTMin) < 1e-8f) {
-        e = exp_ref(power);
-        alpha = fmin_ref(0.99f, o * e);
-        test_T = T * (1.0f - alpha);
-    }
+    if (alpha < kAlphaMin - 1e-8f) return 0;
+    e = exp_ref(power);
+    alpha = fmin_ref(0.99f, o * e);
     if (alpha < kAlphaMin) return 0;
+    test_T = T * (1.0f - alpha);
     if (test_T < kTMin) return 2;
     return 1;
 }
 
 // The alpha-only decision of the backward (the forward's last-contributor
-// index already encodes the stop).  Agrees with blend_decision's skip.
+// index already encodes the stop); agrees with blend_decision's skip and
+// yields the same alpha and exp for accepted Gaussians.
 __device__ __forceinline__ bool alpha_accept(float power, float o, float& alpha, float& e) {
     e = expf(power);
     alpha = fmin_ref(0.99f, o * e);
-    if (fabsf(alpha - kAlphaMin) < 1e-8f) {
-        e = exp_ref(power);
-        alpha = fmin_ref(0.99f, o * e);
-    }
+    if (alpha < kAlphaMin - 1e-8f) return false;
+    e = exp_ref(power);
+    alpha = fmin_ref(0.99f, o * e);
     return !(alpha < kAlphaMin);
 }
 
@@ -594,9 +594,42 @@ __device__ __forceinline__ float warp_sum(float v) {
     return v;
 }
 
+// Sums eight values over the 32 lanes of a warp with 9 shuffles instead of 40:
+// each butterfly stage sends half of the values it still holds to its partner,
+// so the set of values a lane carries halves at every step.  On return lane l
+// holds the warp total of value ((l>>4)&1)*4 + ((l>>3)&1)*2 + ((l>>2)&1)
+// (*idx); lanes with the same bits 2..4 hold the same total.
+__device__ __forceinline__ float warp_sum8(const float v[8], int* idx) {
+    const unsigned lane = threadIdx.x & 31;
+    const bool h16 = lane & 16, h8 = lane & 8, h4 = lane & 4;
+    float a[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const float send = h16 ? v[i] : v[i + 4];
+        const float keep = h16 ? v[i + 4] : v[i];
+        a[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+    }
+    float b[2];
+#pragma unroll
+    for (int i = 0; i < 2; i++) {
+        const float send = h8 ? a[i] : a[i + 2];
+        const float keep = h8 ? a[i + 2] : a[i];
+        b[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+    }
+    const float send = h4 ? b[0] : b[1];
+    float c = (h4 ? b[1] : b[0]) + __shfl_xor_sync(0xffffffffu, send, 4);
+    c += __shfl_xor_sync(0xffffffffu, c, 2);
+    c += __shfl_xor_sync(0xffffffffu, c, 1);
+    *idx = (h16 ? 4 : 0) + (h8 ? 2 : 0) + (h4 ? 1 : 0);
+    return c;
+}
+
 // Rasterizer backward (rasterizer_backward_cpu.cpp:20-133): back-to-front
 // over each pixel's contributors, transmittance recovered by division from
-// T_final instead of a replayed per-pixel list.
+// T_final instead of a replayed per-pixel list.  Per Gaussian of a batch, the
+// 32 pixels of a warp are summed with warp_sum8, the 8 warps of the tile meet
+// in shared-memory accumulators, and each Gaussian gets one set of global
+// atomics per tile.
 template <bool FROM_SIGN>
 __global__ void __launch_bounds__(kBlock) k_raster_bwd(const StepParams* __restrict__ spp,
                                                        const unsigned* __restrict__ ranges,
@@ -606,6 +639,7 @@ __global__ void __launch_bounds__(kBlock) k_raster_bwd(const StepParams* __restr
     __shared__ float4 s_r1[kBlock];
     __shared__ float s_b[kBlock];
     __shared__ unsigned s_idx[kBlock];
+    __shared__ float s_acc[9][kBlock];   // r, g, b, opacity, mean.x, mean.y, conic a, b, c
     __shared__ unsigned s_maxlast;
     const StepParams& sp = *spp;
     if (FROM_SIGN && ((ctrl->status & kStatusOverflow) || sp.persist->sticky_overflow)) return;
@@ -654,12 +688,14 @@ __global__ void __launch_bounds__(kBlock) k_raster_bwd(const StepParams* __restr
             s_r1[threadIdx.x] = s.rec1[gi];
             s_b[threadIdx.x] = s.col_b[gi];
         }
+#pragma unroll
+        for (int v = 0; v < 9; v++) s_acc[v][threadIdx.x] = 0.0f;
         __syncthreads();
         for (int k = (int)(be - bs) - 1; k >= 0; k--) {
             const unsigned jj = bs + (unsigned)k;
             bool contrib = false;
-            float g_r = 0.f, g_g = 0.f, g_b = 0.f, g_o = 0.f, g_mx = 0.f, g_my = 0.f, g_ca = 0.f, g_cb = 0.f,
-                  g_cc = 0.f;
+            float gv[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            float g_cc = 0.f;
             if (jj < last) {
                 const float4 a = s_r0[k];
                 const float4 c = s_r1[k];
@@ -671,9 +707,9 @@ __global__ void __launch_bounds__(kBlock) k_raster_bwd(const StepParams* __restr
                     const float cb = s_b[k];
                     const float oma = 1.0f - alpha;
                     const float Ti = (oma > 1e-6f) ? T / oma : 0.0f;
-                    g_r = alpha * Ti * dC0;
-                    g_g = alpha * Ti * dC1;
-                    g_b = alpha * Ti * dC2;
+                    gv[0] = alpha * Ti * dC0;
+                    gv[1] = alpha * Ti * dC1;
+                    gv[2] = alpha * Ti * dC2;
                     float d_alpha = 0.0f;
                     d_alpha += Ti * (c.z - acc0) * dC0;
                     d_alpha += Ti * (c.w - acc1) * dC1;
@@ -685,37 +721,34 @@ __global__ void __launch_bounds__(kBlock) k_raster_bwd(const StepParams* __restr
                     float d_power = 0.0f;
                     if (alpha < 0.99f) {
                         d_power = d_alpha * c.y * ep;
-                        g_o = d_alpha * ep;
+                        gv[3] = d_alpha * ep;
                     }
-                    g_mx = d_power * (-a.z * dx - a.w * dy);
-                    g_my = d_power * (-c.x * dy - a.w * dx);
-                    g_ca = d_power * (-0.5f * dx * dx);
-                    g_cb = d_power * (-dx * dy);
+                    gv[4] = d_power * (-a.z * dx - a.w * dy);
+                    gv[5] = d_power * (-c.x * dy - a.w * dx);
+                    gv[6] = d_power * (-0.5f * dx * dx);
+                    gv[7] = d_power * (-dx * dy);
                     g_cc = d_power * (-0.5f * dy * dy);
                 }
             }
             if (__any_sync(0xffffffffu, contrib)) {
-                g_r = warp_sum(g_r);
-                g_g = warp_sum(g_g);
-                g_b = warp_sum(g_b);
-                g_o = warp_sum(g_o);
-                g_mx = warp_sum(g_mx);
-                g_my = warp_sum(g_my);
-                g_ca = warp_sum(g_ca);
-                g_cb = warp_sum(g_cb);
-                g_cc = warp_sum(g_cc);
-                if (lane == 0) {
-                    const unsigned gi = s_idx[k];
-                    atomicAdd(&g.drgb[3 * gi], g_r);
-                    atomicAdd(&g.drgb[3 * gi + 1], g_g);
-                    atomicAdd(&g.drgb[3 * gi + 2], g_b);
-                    atomicAdd(&g.dop[gi], g_o);
-                    atomicAdd(&g.dm2[2 * gi], g_mx);
-                    atomicAdd(&g.dm2[2 * gi + 1], g_my);
-                    atomicAdd(&g.dcon[3 * gi], g_ca);
-                    atomicAdd(&g.dcon[3 * gi + 1], g_cb);
-                    atomicAdd(&g.dcon[3 * gi + 2], g_cc);
-                }
+                int idx;
+                const float s8 = warp_sum8(gv, &idx);
+                const float s9 = warp_sum(g_cc);
+                if ((lane & 3) == 0 && s8 != 0.0f) atomicAdd(&s_acc[idx][k], s8);
+                if (lane == 1 && s9 != 0.0f) atomicAdd(&s_acc[8][k], s9);
+            }
+        }
+        __syncthreads();
+        if (j < be) {
+            // thread t flushes batch entry t, which it also zeroes for the next batch
+            const unsigned gi = s_idx[threadIdx.x];
+            float* const dst[9] = {&g.drgb[3 * gi], &g.drgb[3 * gi + 1], &g.drgb[3 * gi + 2], &g.dop[gi],
+                                   &g.dm2[2 * gi], &g.dm2[2 * gi + 1], &g.dcon[3 * gi], &g.dcon[3 * gi + 1],
+                                   &g.dcon[3 * gi + 2]};
+#pragma unroll
+            for (int v = 0; v < 9; v++) {
+                const float a = s_acc[v][threadIdx.x];
+                if (a != 0.0f) atomicAdd(dst[v], a);
             }
         }
         __syncthreads();
@@ -724,341 +757,485 @@ __global__ void __launch_bounds__(kBlock) k_raster_bwd(const StepParams* __restr
 }
 
 // Adam element update (optimizer.cpp:32-43), same rounding sequence.
-__device__ __forceinline__ void adam_elem(float* p, float* m, float* v, float g, float lr, float b1, float b2,
-                                          float eps, float bc1, float bc2) {
-    const float mn = b1 * (*m) + (1.0f - b1) * g;
-    const float vn = b2 * (*v) + (1.0f - b2) * g * g;
-    *m = mn;
-    *v = vn;
-    const float mh = mn * bc1;
-    const float vh = vn * bc2;
-    *p = *p - lr * mh / (sqrtf(vh) + eps);
+__device__ __forceinline__ float adam_elem(float p, float& m, float& v, float g, float lr, float b1, float b2,
+                                           float eps, float bc1, float bc2) {
+    m = b1 * m + (1.0f - b1) * g;
+    v = b2 * v + (1.0f - b2) * g * g;
+    const float mh = m * bc1;
+    const float vh = v * bc2;
+    return p - lr * mh / (sqrtf(vh) + eps);
 }
 
 __device__ __forceinline__ void apply_update(const StepParams& sp, float* p, float* m, float* v, float g,
                                              float lr) {
-    if (sp.use_adam) adam_elem(p, m, v, g, lr, sp.beta1, sp.beta2, sp.eps, sp.bc1, sp.bc2);
-    else *p = *p - lr * g;  // SGD, optimizer.cpp:14-25
+    if (sp.use_adam) {
+        float mm = *m, vv = *v;
+        *p = adam_elem(*p, mm, vv, g, lr, sp.beta1, sp.beta2, sp.eps, sp.bc1, sp.bc2);
+        *m = mm;
+        *v = vv;
+    } else {
+        *p = *p - lr * g;  // SGD, optimizer.cpp:14-25
+    }
 }
 
-// Preprocess backward (preprocessor_backward_cpu.cpp:8-645), optionally fused
-// with the optimiser update of all 59 parameters of the Gaussian.
+// Inputs of one Gaussian's backward: raw parameters and its screen-space gradients.
+struct BwdIn {
+    float p[3], rsc[3], rq[4], rop;
+    const float* sh;   // this Gaussian's SH coefficients, basis-major with stride 3
+    float dm[2], dcn[3], drgb[3], dop;
+};
+
+// Gradients w.r.t. the raw parameters; the SH gradient is basis[k] * geff[c].
+struct BwdOut {
+    float gp[3], gs[3], gq[4], gop, geff[3], basis[16];
+};
+
+// The whole per-Gaussian adjoint chain of PreprocessorBackwardCPU::backward
+// (preprocessor_backward_cpu.cpp:205-645) for a visible Gaussian, with the
+// forward quantities (activation, p_view, cov3D, cov2D, det, means2D)
+// recomputed bit-identically instead of read from a cache.
+__device__ __forceinline__ void backward_one(const StepParams& sp, const BwdIn& in, BwdOut& o) {
+    const gs3d_camera& cam = sp.cam;
+    const float* shp = in.sh;
+    const float* p = in.p;
+    float sc[3], q[4], op;
+    activate_one(in.rsc, in.rq, in.rop, sc, q, &op);
+    const int deg = sp.sh_deg_model;
+    // ---- chain 2: SH (:8-203) ----
+    float d[3];
+    const float len = view_dir(p, cam.cam_pos, d);
+    const float x = d[0], y = d[1], z = d[2];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        const float rawc = sh_channel(deg, shp, c, x, y, z);
+        o.geff[c] = in.drgb[c] * ((rawc + 0.5f >= 0.0f) ? 1.0f : 0.0f);
+    }
+    o.basis[0] = SH_C0;
+    if (deg > 0) {
+        o.basis[1] = -SH_C1 * y;
+        o.basis[2] = SH_C1 * z;
+        o.basis[3] = -SH_C1 * x;
+        if (deg > 1) {
+            const float xx = x * x, yy = y * y, zz = z * z, xy = x * y, yz = y * z, xz = x * z;
+            o.basis[4] = SH_C20 * xy;
+            o.basis[5] = SH_C21 * yz;
+            o.basis[6] = SH_C22 * (2.0f * zz - xx - yy);
+            o.basis[7] = SH_C23 * xz;
+            o.basis[8] = SH_C24 * (xx - yy);
+            if (deg > 2) {
+                o.basis[9] = SH_C30 * y * (3.0f * xx - yy);
+                o.basis[10] = SH_C31 * xy * z;
+                o.basis[11] = SH_C32 * y * (4.0f * zz - xx - yy);
+                o.basis[12] = SH_C33 * z * (2.0f * zz - 3.0f * xx - 3.0f * yy);
+                o.basis[13] = SH_C34 * x * (4.0f * zz - xx - yy);
+                o.basis[14] = SH_C35 * z * (xx - yy);
+                o.basis[15] = SH_C36 * x * (xx - 3.0f * yy);
+            }
+        }
+        // d colour / d dir (:129-189)
+        float dd0[3] = {0.f, 0.f, 0.f}, dd1[3] = {0.f, 0.f, 0.f}, dd2[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            dd0[c] += -SH_C1 * shp[9 + c];
+            dd1[c] += -SH_C1 * shp[3 + c];
+            dd2[c] += SH_C1 * shp[6 + c];
+        }
+        if (deg > 1) {
+            const float xx = x * x, yy = y * y, zz = z * z;
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                const float s4 = shp[12 + c], s5 = shp[15 + c], s6 = shp[18 + c], s7 = shp[21 + c], s8 = shp[24 + c];
+                dd0[c] += SH_C20 * y * s4 - 2.0f * SH_C22 * x * s6 + SH_C23 * z * s7 + 2.0f * SH_C24 * x * s8;
+                dd1[c] += SH_C20 * x * s4 + SH_C21 * z * s5 - 2.0f * SH_C22 * y * s6 - 2.0f * SH_C24 * y * s8;
+                dd2[c] += SH_C21 * y * s5 + 4.0f * SH_C22 * z * s6 + SH_C23 * x * s7;
+            }
+            if (deg > 2) {
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    const float s9 = shp[27 + c], s10 = shp[30 + c], s11 = shp[33 + c], s12 = shp[36 + c];
+                    const float s13 = shp[39 + c], s14 = shp[42 + c], s15 = shp[45 + c];
+                    dd0[c] += SH_C30 * 6.0f * x * y * s9 + SH_C31 * y * z * s10 + SH_C32 * (-2.0f * x * y) * s11 +
+                              SH_C33 * (-6.0f * x * z) * s12 + SH_C34 * (4.0f * zz - 3.0f * xx - yy) * s13 +
+                              SH_C35 * 2.0f * x * z * s14 + SH_C36 * (3.0f * xx - 3.0f * yy) * s15;
+                    dd1[c] += SH_C30 * (3.0f * xx - 3.0f * yy) * s9 + SH_C31 * x * z * s10 +
+                              SH_C32 * (4.0f * zz - xx - 3.0f * yy) * s11 + SH_C33 * (-6.0f * y * z) * s12 +
+                              SH_C34 * (-2.0f * x * y) * s13 - SH_C35 * 2.0f * y * z * s14 +
+                              SH_C36 * (-6.0f * x * y) * s15;
+                    dd2[c] += SH_C31 * x * y * s10 + SH_C32 * 8.0f * y * z * s11 +
+                              SH_C33 * (6.0f * zz - 3.0f * xx - 3.0f * yy) * s12 + SH_C34 * 8.0f * x * z * s13 +
+                              SH_C35 * (xx - yy) * s14;
+                }
+            }
+        }
+        float ddir0 = 0.f, ddir1 = 0.f, ddir2 = 0.f;
+#pragma unroll
+        for (int c = 0; c < 3; c++) ddir0 += o.geff[c] * dd0[c];
+#pragma unroll
+        for (int c = 0; c < 3; c++) ddir1 += o.geff[c] * dd1[c];
+#pragma unroll
+        for (int c = 0; c < 3; c++) ddir2 += o.geff[c] * dd2[c];
+        const float inv_len = 1.0f / len;
+        const float dot = ddir0 * x + ddir1 * y + ddir2 * z;
+        o.gp[0] += (ddir0 - x * dot) * inv_len;
+        o.gp[1] += (ddir1 - y * dot) * inv_len;
+        o.gp[2] += (ddir2 - z * dot) * inv_len;
+    }
+    // ---- chain 3: sigmoid (:231-232) ----
+    o.gop = in.dop * op * (1.0f - op);
+    // ---- forward recompute (the ForwardCache of preprocessor_cpu.cpp:254-264) ----
+    float c3[6];
+    cov3d(sc, sp.cfg.scale_modifier, q, c3);
+    Ewa e;
+    ewa_setup(p, cam.view_matrix, sp.focal_x, sp.focal_y, cam.tan_fovx, cam.tan_fovy, e);
+    float c2[3];
+    cov2d(e, c3, c2);
+    c2[0] += 0.3f;
+    c2[2] += 0.3f;
+    const float det = c2[0] * c2[2] - c2[1] * c2[1];
+    if (det == 0.0f) return;
+    float ph[4];
+    xform4x4(p, cam.viewproj_matrix, ph);
+    // ---- chain 1a: conic -> cov2D (:243-306) ----
+    const float a = c2[0], b = c2[1], c = c2[2];
+    const float inv_det = 1.0f / det;
+    const float id2 = inv_det * inv_det;
+    const float* dcn = in.dcn;
+    const float d_a = dcn[0] * (-c * c * id2) + dcn[1] * (b * c * id2) + dcn[2] * (-b * b * id2);
+    const float d_b = dcn[0] * (2.0f * b * c * id2) + dcn[1] * (-(a * c + b * b) * id2) + dcn[2] * (2.0f * a * b * id2);
+    const float d_c = dcn[0] * (-b * b * id2) + dcn[1] * (a * b * id2) + dcn[2] * (-a * a * id2);
+    // ---- chain 1b: cov2D -> cov3D (:316-380) ----
+    float dV[3][3];
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+#pragma unroll
+        for (int j = 0; j < 3; j++)
+            dV[k][j] = d_a * e.T[0][k] * e.T[0][j] + d_b * e.T[0][k] * e.T[1][j] + d_c * e.T[1][k] * e.T[1][j];
+    const float dcov[6] = {dV[0][0], dV[0][1] + dV[1][0], dV[0][2] + dV[2][0],
+                           dV[1][1], dV[1][2] + dV[2][1], dV[2][2]};
+    // ---- chain 1c: cov3D -> M -> scale, R (:395-442) ----
+    const float mod = sp.cfg.scale_modifier;
+    const float sv[3] = {mod * sc[0], mod * sc[1], mod * sc[2]};
+    const float rr = q[0], xq = q[1], yq = q[2], zq = q[3];
+    float R[3][3], M[3][3];
+    quat_to_R(rr, xq, yq, zq, R);
+#pragma unroll
+    for (int ii = 0; ii < 3; ii++)
+#pragma unroll
+        for (int jj = 0; jj < 3; jj++) M[ii][jj] = sv[ii] * R[ii][jj];
+    float dR[3][3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const float dM0 = 2.0f * dcov[0] * M[k][0] + dcov[1] * M[k][1] + dcov[2] * M[k][2];
+        const float dM1 = dcov[1] * M[k][0] + 2.0f * dcov[3] * M[k][1] + dcov[4] * M[k][2];
+        const float dM2 = dcov[2] * M[k][0] + dcov[4] * M[k][1] + 2.0f * dcov[5] * M[k][2];
+        float ds = 0.0f;
+        ds += dM0 * R[k][0];
+        ds += dM1 * R[k][1];
+        ds += dM2 * R[k][2];
+        dR[k][0] = dM0 * sv[k];
+        dR[k][1] = dM1 * sv[k];
+        dR[k][2] = dM2 * sv[k];
+        o.gs[k] = ds * mod * sc[k];
+    }
+    // ---- d R -> d unit quaternion (:455-498) ----
+    float dq0 = 0.f, dq1 = 0.f, dq2 = 0.f, dq3 = 0.f;
+    dq2 += dR[0][0] * (-4.0f * yq);
+    dq3 += dR[0][0] * (-4.0f * zq);
+    dq0 += dR[0][1] * 2.0f * zq; dq1 += dR[0][1] * 2.0f * yq;
+    dq2 += dR[0][1] * 2.0f * xq; dq3 += dR[0][1] * 2.0f * rr;
+    dq0 += dR[0][2] * (-2.0f * yq); dq1 += dR[0][2] * 2.0f * zq;
+    dq2 += dR[0][2] * (-2.0f * rr); dq3 += dR[0][2] * 2.0f * xq;
+    dq0 += dR[1][0] * (-2.0f * zq); dq1 += dR[1][0] * 2.0f * yq;
+    dq2 += dR[1][0] * 2.0f * xq; dq3 += dR[1][0] * (-2.0f * rr);
+    dq1 += dR[1][1] * (-4.0f * xq);
+    dq3 += dR[1][1] * (-4.0f * zq);
+    dq0 += dR[1][2] * 2.0f * xq; dq1 += dR[1][2] * 2.0f * rr;
+    dq2 += dR[1][2] * 2.0f * zq; dq3 += dR[1][2] * 2.0f * yq;
+    dq0 += dR[2][0] * 2.0f * yq; dq1 += dR[2][0] * 2.0f * zq;
+    dq2 += dR[2][0] * 2.0f * rr; dq3 += dR[2][0] * 2.0f * xq;
+    dq0 += dR[2][1] * (-2.0f * xq); dq1 += dR[2][1] * (-2.0f * rr);
+    dq2 += dR[2][1] * 2.0f * zq; dq3 += dR[2][1] * 2.0f * yq;
+    dq1 += dR[2][2] * (-4.0f * xq);
+    dq2 += dR[2][2] * (-4.0f * yq);
+    // ---- normalisation backward (:503-519) ----
+    const float* rq = in.rq;
+    float qlen = sqrtf(rq[0] * rq[0] + rq[1] * rq[1] + rq[2] * rq[2] + rq[3] * rq[3]);
+    if (qlen < 1e-12f) qlen = 1e-12f;
+    const float il = 1.0f / qlen;
+    const float dot = dq0 * rr + dq1 * xq + dq2 * yq + dq3 * zq;
+    o.gq[0] = (dq0 - rr * dot) * il;
+    o.gq[1] = (dq1 - xq * dot) * il;
+    o.gq[2] = (dq2 - yq * dot) * il;
+    o.gq[3] = (dq3 - zq * dot) * il;
+    // ---- path A: cov2D -> T -> J -> p_view -> position (:536-597) ----
+    const float V[3][3] = {{c3[0], c3[1], c3[2]}, {c3[1], c3[3], c3[4]}, {c3[2], c3[4], c3[5]}};
+    float VT[2][3];
+#pragma unroll
+    for (int col = 0; col < 2; col++)
+#pragma unroll
+        for (int row = 0; row < 3; row++) {
+            float acc = 0.0f;
+#pragma unroll
+            for (int k = 0; k < 3; k++) acc += V[row][k] * e.T[col][k];
+            VT[col][row] = acc;
+        }
+    float dT[2][3];
+#pragma unroll
+    for (int qq = 0; qq < 3; qq++) {
+        dT[0][qq] = 2.0f * d_a * VT[0][qq] + d_b * VT[1][qq];
+        dT[1][qq] = d_b * VT[0][qq] + 2.0f * d_c * VT[1][qq];
+    }
+    float dJ[2][3];
+#pragma unroll
+    for (int col = 0; col < 2; col++)
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            float acc = 0.0f;
+#pragma unroll
+            for (int row = 0; row < 3; row++) acc += dT[col][row] * e.W[k][row];
+            dJ[col][k] = acc;
+        }
+    const float* t = e.t;
+    const float tz2 = t[2] * t[2];
+    const float tz3 = tz2 * t[2];
+    const float fx = sp.focal_x, fy = sp.focal_y;
+    float dt0 = dJ[0][2] * (-fx / tz2);
+    float dt1 = dJ[1][2] * (-fy / tz2);
+    const float dt2 = dJ[0][0] * (-fx / tz2) + dJ[1][1] * (-fy / tz2) + dJ[0][2] * (2.0f * fx * t[0] / tz3) +
+                      dJ[1][2] * (2.0f * fy * t[1] / tz3);
+    if (fabsf(e.txtz) >= e.limx) dt0 = 0.0f;
+    if (fabsf(e.tytz) >= e.limy) dt1 = 0.0f;
+    const float* vm = cam.view_matrix;
+#pragma unroll
+    for (int col = 0; col < 3; col++) {
+        o.gp[col] += dt0 * vm[col * 4 + 0];
+        o.gp[col] += dt1 * vm[col * 4 + 1];
+        o.gp[col] += dt2 * vm[col * 4 + 2];
+    }
+    // ---- chain 4: means2D -> ndc -> p_hom -> position (:609-643) ----
+    // means2D recomputed exactly as the forward wrote it (preprocessor_cpu.cpp:195-203)
+    const float pw = 1.0f / (ph[3] + 1e-7f);
+    const float pix_x = ((ph[0] * pw + 1.0f) * (float)cam.width - 1.0f) * 0.5f;
+    const float pix_y = ((ph[1] * pw + 1.0f) * (float)cam.height - 1.0f) * 0.5f;
+    const float dndx = in.dm[0] * (float)cam.width * 0.5f;
+    const float dndy = in.dm[1] * (float)cam.height * 0.5f;
+    const float wh = ph[3] + 1e-7f;
+    const float iw = 1.0f / wh;
+    const float ndc_x = (2.0f * pix_x + 1.0f) / (float)cam.width - 1.0f;
+    const float ndc_y = (2.0f * pix_y + 1.0f) / (float)cam.height - 1.0f;
+    const float dph0 = dndx * iw, dph1 = dndy * iw, dph2 = 0.0f;
+    const float dph3 = -(ndc_x * dndx + ndc_y * dndy) * iw;
+    const float* VP = cam.viewproj_matrix;
+#pragma unroll
+    for (int dim = 0; dim < 3; dim++)
+        o.gp[dim] += VP[dim * 4 + 0] * dph0 + VP[dim * 4 + 1] * dph1 + VP[dim * 4 + 2] * dph2 + VP[dim * 4 + 3] * dph3;
+}
+
+// ---- fused preprocess backward + optimiser, staged through shared memory ----
+//
+// One CTA owns kBwdG consecutive Gaussians.  Phase 0 loads their parameter
+// slices (positions, scales, rotations, opacities, SH), raster gradients and
+// radii with coalesced vector loads into shared memory (SH with a 49-float
+// row pitch so the per-Gaussian reads of phase 1 are bank-conflict free) and
+// zeroes the gradient accumulators for the next step.  Phase 1 runs the
+// per-Gaussian adjoint chain, one thread per Gaussian, out of shared memory.
+// Phase 2 applies Adam (or SGD) element by element over each parameter array:
+// consecutive threads touch consecutive floats of params, m and v.
+constexpr int kBwdG = 128;         // Gaussians (= threads) per CTA
+constexpr int kShPitch = 49;       // padded SH row (48 floats + 1)
+constexpr int kBasisPitch = 17;
+
+struct BwdShared {
+    float sh[kBwdG * kShPitch];
+    float basis[kBwdG * kBasisPitch];
+    float geff[kBwdG * 3];
+    float pos[kBwdG * 3], sc[kBwdG * 3], rot[kBwdG * 4], op[kBwdG];      // raw parameters
+    float gpos[kBwdG * 3], gsc[kBwdG * 3], grot[kBwdG * 4], gop[kBwdG];  // their gradients
+    float dm2[kBwdG * 2], dcon[kBwdG * 3], drgb[kBwdG * 3], dop[kBwdG];  // screen-space gradients
+    int radius[kBwdG];
+};
+
+// Coalesced copy of n floats from global to shared memory (both 16-byte
+// aligned when n_full is a multiple of 4), zeroing the source if asked.
+__device__ __forceinline__ void stage_in(float* dst, float* src, int n, bool zero_src) {
+    const int n4 = n >> 2;
+    float4* s4 = reinterpret_cast<float4*>(src);
+    for (int q = threadIdx.x; q < n4; q += kBwdG) {
+        const float4 v = s4[q];
+        dst[4 * q] = v.x;
+        dst[4 * q + 1] = v.y;
+        dst[4 * q + 2] = v.z;
+        dst[4 * q + 3] = v.w;
+        if (zero_src) s4[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    for (int e = 4 * n4 + threadIdx.x; e < n; e += kBwdG) {
+        dst[e] = src[e];
+        if (zero_src) src[e] = 0.f;
+    }
+}
+
+// Optimiser over one parameter group slice: params p[0..n), moments m, v, the
+// gradient of element e given by grad(e); the updated parameters go back to p.
+template <class GradFn, class ParamFn>
+__device__ __forceinline__ void update_slice(const StepParams& sp, float* p, float* m, float* v, int n, float lr,
+                                             GradFn grad, ParamFn p_s) {
+    const int n4 = n >> 2;
+    float4* p4 = reinterpret_cast<float4*>(p);
+    float4* m4 = reinterpret_cast<float4*>(m);
+    float4* v4 = reinterpret_cast<float4*>(v);
+    for (int q = threadIdx.x; q < n4; q += kBwdG) {
+        float4 pp, mm, vv;
+        pp.x = p_s(4 * q); pp.y = p_s(4 * q + 1); pp.z = p_s(4 * q + 2); pp.w = p_s(4 * q + 3);
+        if (sp.use_adam) {
+            mm = m4[q];
+            vv = v4[q];
+            pp.x = adam_elem(pp.x, mm.x, vv.x, grad(4 * q), lr, sp.beta1, sp.beta2, sp.eps, sp.bc1, sp.bc2);
+            pp.y = adam_elem(pp.y, mm.y, vv.y, grad(4 * q + 1), lr, sp.beta1, sp.beta2, sp.eps, sp.bc1, sp.bc2);
+            pp.z = adam_elem(pp.z, mm.z, vv.z, grad(4 * q + 2), lr, sp.beta1, sp.beta2, sp.eps, sp.bc1, sp.bc2);
+            pp.w = adam_elem(pp.w, mm.w, vv.w, grad(4 * q + 3), lr, sp.beta1, sp.beta2, sp.eps, sp.bc1, sp.bc2);
+            m4[q] = mm;
+            v4[q] = vv;
+        } else {
+            pp.x = pp.x - lr * grad(4 * q);
+            pp.y = pp.y - lr * grad(4 * q + 1);
+            pp.z = pp.z - lr * grad(4 * q + 2);
+            pp.w = pp.w - lr * grad(4 * q + 3);
+        }
+        p4[q] = pp;
+    }
+    for (int e = 4 * n4 + threadIdx.x; e < n; e += kBwdG) {
+        float pe = p_s(e);
+        if (sp.use_adam) {
+            float mm = m[e], vv = v[e];
+            pe = adam_elem(pe, mm, vv, grad(e), lr, sp.beta1, sp.beta2, sp.eps, sp.bc1, sp.bc2);
+            m[e] = mm;
+            v[e] = vv;
+        } else {
+            pe = pe - lr * grad(e);
+        }
+        p[e] = pe;
+    }
+}
+
+// Preprocess backward (preprocessor_backward_cpu.cpp:8-645), fused with the
+// optimiser update of all parameters (FUSED) or writing GradientOutput.
 template <bool FUSED>
-__global__ void __launch_bounds__(kBlock) k_preprocess_bwd(const StepParams* __restrict__ spp, int N,
-                                                           ModelPtrs raw, AdamPtrs adam, ScreenPtrs s,
-                                                           RGradPtrs rg, GradPtrs gout, Control* ctrl) {
-    const int i = blockIdx.x * kBlock + threadIdx.x;
-    if (i >= N) return;
+__global__ void __launch_bounds__(kBwdG, 4) k_preprocess_bwd(const StepParams* __restrict__ spp, int N, ModelPtrs raw,
+                                                          AdamPtrs adam, ScreenPtrs s, RGradPtrs rg, GradPtrs gout,
+                                                          Control* ctrl) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    BwdShared& sm = *reinterpret_cast<BwdShared*>(smem_raw);
     const StepParams& sp = *spp;
     // an overflowed (or timed-out) step, or any step after one the host has not
     // acknowledged yet, updates nothing
     if (FUSED && ((ctrl->status & (kStatusOverflow | kStatusTimeout)) || sp.persist->sticky_overflow)) return;
-    if (FUSED && i == 0) atomicAdd(&sp.persist->applied_steps, 1ull);
-    const gs3d_camera& cam = sp.cam;
-    const int mc = sp.max_coeffs;
-    const int mc3 = mc * 3;
-    float* shp = raw.sh + (size_t)mc3 * i;
+    if (FUSED && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&sp.persist->applied_steps, 1ull);
+    const int g0 = blockIdx.x * kBwdG;
+    const int ng = min(kBwdG, N - g0);
+    const int mc3 = sp.max_coeffs * 3;
+    const int tid = threadIdx.x;
 
-    float gp[3] = {0.f, 0.f, 0.f}, gs[3] = {0.f, 0.f, 0.f}, gq[4] = {0.f, 0.f, 0.f, 0.f}, gop = 0.f;
-    float geff[3] = {0.f, 0.f, 0.f};   // clamp-masked d_rgb (d_sh = basis * geff)
-    float basis[16];
-#pragma unroll
-    for (int k = 0; k < 16; k++) basis[k] = 0.f;
-    const bool vis = s.radius[i] > 0;
-    const float p[3] = {raw.pos[3 * i], raw.pos[3 * i + 1], raw.pos[3 * i + 2]};
-    const float rq[4] = {raw.rot[4 * i], raw.rot[4 * i + 1], raw.rot[4 * i + 2], raw.rot[4 * i + 3]};
-    const float rsc[3] = {raw.sc[3 * i], raw.sc[3 * i + 1], raw.sc[3 * i + 2]};
-    const float rop = raw.op[i];
-    float dm[2] = {0.f, 0.f}, dcn[3] = {0.f, 0.f, 0.f}, drgb[3] = {0.f, 0.f, 0.f}, dop = 0.f;
-    if (vis) {
-        dm[0] = rg.dm2[2 * i];
-        dm[1] = rg.dm2[2 * i + 1];
-        dcn[0] = rg.dcon[3 * i];
-        dcn[1] = rg.dcon[3 * i + 1];
-        dcn[2] = rg.dcon[3 * i + 2];
-        drgb[0] = rg.drgb[3 * i];
-        drgb[1] = rg.drgb[3 * i + 1];
-        drgb[2] = rg.drgb[3 * i + 2];
-        dop = rg.dop[i];
+    // ---- phase 0: coalesced staging ----
+    stage_in(sm.pos, raw.pos + 3 * (size_t)g0, 3 * ng, false);
+    stage_in(sm.sc, raw.sc + 3 * (size_t)g0, 3 * ng, false);
+    stage_in(sm.rot, raw.rot + 4 * (size_t)g0, 4 * ng, false);
+    stage_in(sm.op, raw.op + (size_t)g0, ng, false);
+    stage_in(sm.dm2, rg.dm2 + 2 * (size_t)g0, 2 * ng, FUSED);
+    stage_in(sm.dcon, rg.dcon + 3 * (size_t)g0, 3 * ng, FUSED);
+    stage_in(sm.drgb, rg.drgb + 3 * (size_t)g0, 3 * ng, FUSED);
+    stage_in(sm.dop, rg.dop + (size_t)g0, ng, FUSED);
+    if (tid < ng) sm.radius[tid] = s.radius[g0 + tid];
+    {
+        const float* src = raw.sh + (size_t)mc3 * g0;
+        const int n = mc3 * ng;
+        if ((mc3 & 3) == 0) {
+            const float4* s4 = reinterpret_cast<const float4*>(src);
+            for (int qd = tid; qd < (n >> 2); qd += kBwdG) {
+                const float4 v = s4[qd];
+                const int e = 4 * qd;
+                const int gg = e / mc3, j = e - gg * mc3;   // 4 | mc3: the float4 stays in one row
+                float* d = sm.sh + gg * kShPitch + j;
+                d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
+            }
+        } else {
+            for (int e = tid; e < n; e += kBwdG) {
+                const int gg = e / mc3, j = e - gg * mc3;
+                sm.sh[gg * kShPitch + j] = src[e];
+            }
+        }
     }
+    __syncthreads();
+
+    // ---- phase 1: per-Gaussian adjoint ----
+    BwdOut o;
+#pragma unroll
+    for (int k = 0; k < 3; k++) { o.gp[k] = 0.f; o.gs[k] = 0.f; o.geff[k] = 0.f; }
+#pragma unroll
+    for (int k = 0; k < 4; k++) o.gq[k] = 0.f;
+    o.gop = 0.f;
+#pragma unroll
+    for (int k = 0; k < 16; k++) o.basis[k] = 0.f;
+    if (tid < ng && sm.radius[tid] > 0) {
+        BwdIn in;
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            in.p[k] = sm.pos[3 * tid + k];
+            in.rsc[k] = sm.sc[3 * tid + k];
+            in.dcn[k] = sm.dcon[3 * tid + k];
+            in.drgb[k] = sm.drgb[3 * tid + k];
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++) in.rq[k] = sm.rot[4 * tid + k];
+        in.rop = sm.op[tid];
+        in.dm[0] = sm.dm2[2 * tid];
+        in.dm[1] = sm.dm2[2 * tid + 1];
+        in.dop = sm.dop[tid];
+        in.sh = sm.sh + tid * kShPitch;
+        backward_one(sp, in, o);
+    }
+    if (tid < ng) {
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            sm.gpos[3 * tid + k] = o.gp[k];
+            sm.gsc[3 * tid + k] = o.gs[k];
+            sm.geff[3 * tid + k] = o.geff[k];
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++) sm.grot[4 * tid + k] = o.gq[k];
+        sm.gop[tid] = o.gop;
+#pragma unroll
+        for (int k = 0; k < 16; k++) sm.basis[tid * kBasisPitch + k] = o.basis[k];
+    }
+    __syncthreads();
+
+    // ---- phase 2: element-wise optimiser (or GradientOutput) ----
+    auto sh_grad = [&](int e) {
+        const int gg = e / mc3, j = e - gg * mc3;
+        const int k = j / 3, c = j - 3 * k;
+        return k < 16 ? sm.basis[gg * kBasisPitch + k] * sm.geff[3 * gg + c] : 0.0f;
+    };
     if (FUSED) {
-        // the accumulators start at zero for the next step's raster backward
-        rg.dm2[2 * i] = 0.f;
-        rg.dm2[2 * i + 1] = 0.f;
-        rg.dcon[3 * i] = 0.f;
-        rg.dcon[3 * i + 1] = 0.f;
-        rg.dcon[3 * i + 2] = 0.f;
-        rg.drgb[3 * i] = 0.f;
-        rg.drgb[3 * i + 1] = 0.f;
-        rg.drgb[3 * i + 2] = 0.f;
-        rg.dop[i] = 0.f;
-    }
-    if (vis) {
-        float sc[3], q[4], op;
-        activate_one(rsc, rq, rop, sc, q, &op);
-        const int deg = sp.sh_deg_model;
-        // ---- chain 2: SH (:8-203) ----
-        float d[3];
-        const float len = view_dir(p, cam.cam_pos, d);
-        const float x = d[0], y = d[1], z = d[2];
-#pragma unroll
-        for (int c = 0; c < 3; c++) {
-            const float rawc = sh_channel(deg, shp, c, x, y, z);
-            geff[c] = drgb[c] * ((rawc + 0.5f >= 0.0f) ? 1.0f : 0.0f);
-        }
-        basis[0] = SH_C0;
-        if (deg > 0) {
-            basis[1] = -SH_C1 * y;
-            basis[2] = SH_C1 * z;
-            basis[3] = -SH_C1 * x;
-            if (deg > 1) {
-                const float xx = x * x, yy = y * y, zz = z * z, xy = x * y, yz = y * z, xz = x * z;
-                basis[4] = SH_C20 * xy;
-                basis[5] = SH_C21 * yz;
-                basis[6] = SH_C22 * (2.0f * zz - xx - yy);
-                basis[7] = SH_C23 * xz;
-                basis[8] = SH_C24 * (xx - yy);
-                if (deg > 2) {
-                    basis[9] = SH_C30 * y * (3.0f * xx - yy);
-                    basis[10] = SH_C31 * xy * z;
-                    basis[11] = SH_C32 * y * (4.0f * zz - xx - yy);
-                    basis[12] = SH_C33 * z * (2.0f * zz - 3.0f * xx - 3.0f * yy);
-                    basis[13] = SH_C34 * x * (4.0f * zz - xx - yy);
-                    basis[14] = SH_C35 * z * (xx - yy);
-                    basis[15] = SH_C36 * x * (xx - 3.0f * yy);
-                }
-            }
-            // d colour / d dir (:129-189)
-            float dd0[3] = {0.f, 0.f, 0.f}, dd1[3] = {0.f, 0.f, 0.f}, dd2[3] = {0.f, 0.f, 0.f};
-#pragma unroll
-            for (int c = 0; c < 3; c++) {
-                dd0[c] += -SH_C1 * shp[9 + c];
-                dd1[c] += -SH_C1 * shp[3 + c];
-                dd2[c] += SH_C1 * shp[6 + c];
-            }
-            if (deg > 1) {
-                const float xx = x * x, yy = y * y, zz = z * z;
-#pragma unroll
-                for (int c = 0; c < 3; c++) {
-                    const float s4 = shp[12 + c], s5 = shp[15 + c], s6 = shp[18 + c], s7 = shp[21 + c],
-                                s8 = shp[24 + c];
-                    dd0[c] += SH_C20 * y * s4 - 2.0f * SH_C22 * x * s6 + SH_C23 * z * s7 + 2.0f * SH_C24 * x * s8;
-                    dd1[c] += SH_C20 * x * s4 + SH_C21 * z * s5 - 2.0f * SH_C22 * y * s6 - 2.0f * SH_C24 * y * s8;
-                    dd2[c] += SH_C21 * y * s5 + 4.0f * SH_C22 * z * s6 + SH_C23 * x * s7;
-                }
-                if (deg > 2) {
-#pragma unroll
-                    for (int c = 0; c < 3; c++) {
-                        const float s9 = shp[27 + c], s10 = shp[30 + c], s11 = shp[33 + c], s12 = shp[36 + c];
-                        const float s13 = shp[39 + c], s14 = shp[42 + c], s15 = shp[45 + c];
-                        dd0[c] += SH_C30 * 6.0f * x * y * s9 + SH_C31 * y * z * s10 +
-                                  SH_C32 * (-2.0f * x * y) * s11 + SH_C33 * (-6.0f * x * z) * s12 +
-                                  SH_C34 * (4.0f * zz - 3.0f * xx - yy) * s13 + SH_C35 * 2.0f * x * z * s14 +
-                                  SH_C36 * (3.0f * xx - 3.0f * yy) * s15;
-                        dd1[c] += SH_C30 * (3.0f * xx - 3.0f * yy) * s9 + SH_C31 * x * z * s10 +
-                                  SH_C32 * (4.0f * zz - xx - 3.0f * yy) * s11 + SH_C33 * (-6.0f * y * z) * s12 +
-                                  SH_C34 * (-2.0f * x * y) * s13 - SH_C35 * 2.0f * y * z * s14 +
-                                  SH_C36 * (-6.0f * x * y) * s15;
-                        dd2[c] += SH_C31 * x * y * s10 + SH_C32 * 8.0f * y * z * s11 +
-                                  SH_C33 * (6.0f * zz - 3.0f * xx - 3.0f * yy) * s12 +
-                                  SH_C34 * 8.0f * x * z * s13 + SH_C35 * (xx - yy) * s14;
-                    }
-                }
-            }
-            float ddir0 = 0.f, ddir1 = 0.f, ddir2 = 0.f;
-#pragma unroll
-            for (int c = 0; c < 3; c++) ddir0 += geff[c] * dd0[c];
-#pragma unroll
-            for (int c = 0; c < 3; c++) ddir1 += geff[c] * dd1[c];
-#pragma unroll
-            for (int c = 0; c < 3; c++) ddir2 += geff[c] * dd2[c];
-            const float inv_len = 1.0f / len;
-            const float dot = ddir0 * x + ddir1 * y + ddir2 * z;
-            gp[0] += (ddir0 - x * dot) * inv_len;
-            gp[1] += (ddir1 - y * dot) * inv_len;
-            gp[2] += (ddir2 - z * dot) * inv_len;
-        }
-        // ---- chain 3: sigmoid (:231-232) ----
-        gop = dop * op * (1.0f - op);
-        // ---- forward recompute (ForwardCache, preprocessor_cpu.cpp:254-264) ----
-        float c3[6];
-        cov3d(sc, sp.cfg.scale_modifier, q, c3);
-        Ewa e;
-        ewa_setup(p, cam.view_matrix, sp.focal_x, sp.focal_y, cam.tan_fovx, cam.tan_fovy, e);
-        float c2[3];
-        cov2d(e, c3, c2);
-        c2[0] += 0.3f;
-        c2[2] += 0.3f;
-        const float det = c2[0] * c2[2] - c2[1] * c2[1];
-        float ph[4];
-        xform4x4(p, cam.viewproj_matrix, ph);
-        if (det != 0.0f) {
-            // ---- chain 1a: conic -> cov2D (:243-306) ----
-            const float a = c2[0], b = c2[1], c = c2[2];
-            const float inv_det = 1.0f / det;
-            const float id2 = inv_det * inv_det;
-            const float d_a = dcn[0] * (-c * c * id2) + dcn[1] * (b * c * id2) + dcn[2] * (-b * b * id2);
-            const float d_b = dcn[0] * (2.0f * b * c * id2) + dcn[1] * (-(a * c + b * b) * id2) +
-                              dcn[2] * (2.0f * a * b * id2);
-            const float d_c = dcn[0] * (-b * b * id2) + dcn[1] * (a * b * id2) + dcn[2] * (-a * a * id2);
-            // ---- chain 1b: cov2D -> cov3D (:316-380) ----
-            float dV[3][3];
-#pragma unroll
-            for (int k = 0; k < 3; k++)
-#pragma unroll
-                for (int j = 0; j < 3; j++)
-                    dV[k][j] = d_a * e.T[0][k] * e.T[0][j] + d_b * e.T[0][k] * e.T[1][j] +
-                               d_c * e.T[1][k] * e.T[1][j];
-            const float dcov[6] = {dV[0][0], dV[0][1] + dV[1][0], dV[0][2] + dV[2][0],
-                                   dV[1][1], dV[1][2] + dV[2][1], dV[2][2]};
-            // ---- chain 1c: cov3D -> M -> scale, R (:395-442) ----
-            const float mod = sp.cfg.scale_modifier;
-            const float sv[3] = {mod * sc[0], mod * sc[1], mod * sc[2]};
-            const float rr = q[0], xq = q[1], yq = q[2], zq = q[3];
-            float R[3][3], M[3][3];
-            quat_to_R(rr, xq, yq, zq, R);
-#pragma unroll
-            for (int ii = 0; ii < 3; ii++)
-#pragma unroll
-                for (int jj = 0; jj < 3; jj++) M[ii][jj] = sv[ii] * R[ii][jj];
-            float dR[3][3];
-#pragma unroll
-            for (int k = 0; k < 3; k++) {
-                const float dM0 = 2.0f * dcov[0] * M[k][0] + dcov[1] * M[k][1] + dcov[2] * M[k][2];
-                const float dM1 = dcov[1] * M[k][0] + 2.0f * dcov[3] * M[k][1] + dcov[4] * M[k][2];
-                const float dM2 = dcov[2] * M[k][0] + dcov[4] * M[k][1] + 2.0f * dcov[5] * M[k][2];
-                float ds = 0.0f;
-                ds += dM0 * R[k][0];
-                ds += dM1 * R[k][1];
-                ds += dM2 * R[k][2];
-                dR[k][0] = dM0 * sv[k];
-                dR[k][1] = dM1 * sv[k];
-                dR[k][2] = dM2 * sv[k];
-                gs[k] = ds * mod * sc[k];
-            }
-            // ---- d R -> d unit quaternion (:455-498) ----
-            float dq0 = 0.f, dq1 = 0.f, dq2 = 0.f, dq3 = 0.f;
-            dq2 += dR[0][0] * (-4.0f * yq);
-            dq3 += dR[0][0] * (-4.0f * zq);
-            dq0 += dR[0][1] * 2.0f * zq; dq1 += dR[0][1] * 2.0f * yq;
-            dq2 += dR[0][1] * 2.0f * xq; dq3 += dR[0][1] * 2.0f * rr;
-            dq0 += dR[0][2] * (-2.0f * yq); dq1 += dR[0][2] * 2.0f * zq;
-            dq2 += dR[0][2] * (-2.0f * rr); dq3 += dR[0][2] * 2.0f * xq;
-            dq0 += dR[1][0] * (-2.0f * zq); dq1 += dR[1][0] * 2.0f * yq;
-            dq2 += dR[1][0] * 2.0f * xq; dq3 += dR[1][0] * (-2.0f * rr);
-            dq1 += dR[1][1] * (-4.0f * xq);
-            dq3 += dR[1][1] * (-4.0f * zq);
-            dq0 += dR[1][2] * 2.0f * xq; dq1 += dR[1][2] * 2.0f * rr;
-            dq2 += dR[1][2] * 2.0f * zq; dq3 += dR[1][2] * 2.0f * yq;
-            dq0 += dR[2][0] * 2.0f * yq; dq1 += dR[2][0] * 2.0f * zq;
-            dq2 += dR[2][0] * 2.0f * rr; dq3 += dR[2][0] * 2.0f * xq;
-            dq0 += dR[2][1] * (-2.0f * xq); dq1 += dR[2][1] * (-2.0f * rr);
-            dq2 += dR[2][1] * 2.0f * zq; dq3 += dR[2][1] * 2.0f * yq;
-            dq1 += dR[2][2] * (-4.0f * xq);
-            dq2 += dR[2][2] * (-4.0f * yq);
-            // ---- normalisation backward (:503-519) ----
-            float qlen = sqrtf(rq[0] * rq[0] + rq[1] * rq[1] + rq[2] * rq[2] + rq[3] * rq[3]);
-            if (qlen < 1e-12f) qlen = 1e-12f;
-            const float il = 1.0f / qlen;
-            const float dot = dq0 * rr + dq1 * xq + dq2 * yq + dq3 * zq;
-            gq[0] = (dq0 - rr * dot) * il;
-            gq[1] = (dq1 - xq * dot) * il;
-            gq[2] = (dq2 - yq * dot) * il;
-            gq[3] = (dq3 - zq * dot) * il;
-            // ---- path A: cov2D -> T -> J -> p_view -> position (:536-597) ----
-            const float V[3][3] = {{c3[0], c3[1], c3[2]}, {c3[1], c3[3], c3[4]}, {c3[2], c3[4], c3[5]}};
-            float VT[2][3];
-#pragma unroll
-            for (int col = 0; col < 2; col++)
-#pragma unroll
-                for (int row = 0; row < 3; row++) {
-                    float acc = 0.0f;
-#pragma unroll
-                    for (int k = 0; k < 3; k++) acc += V[row][k] * e.T[col][k];
-                    VT[col][row] = acc;
-                }
-            float dT[2][3];
-#pragma unroll
-            for (int qq = 0; qq < 3; qq++) {
-                dT[0][qq] = 2.0f * d_a * VT[0][qq] + d_b * VT[1][qq];
-                dT[1][qq] = d_b * VT[0][qq] + 2.0f * d_c * VT[1][qq];
-            }
-            float dJ[2][3];
-#pragma unroll
-            for (int col = 0; col < 2; col++)
-#pragma unroll
-                for (int k = 0; k < 3; k++) {
-                    float acc = 0.0f;
-#pragma unroll
-                    for (int row = 0; row < 3; row++) acc += dT[col][row] * e.W[k][row];
-                    dJ[col][k] = acc;
-                }
-            const float* t = e.t;
-            const float tz2 = t[2] * t[2];
-            const float tz3 = tz2 * t[2];
-            const float fx = sp.focal_x, fy = sp.focal_y;
-            float dt0 = dJ[0][2] * (-fx / tz2);
-            float dt1 = dJ[1][2] * (-fy / tz2);
-            const float dt2 = dJ[0][0] * (-fx / tz2) + dJ[1][1] * (-fy / tz2) +
-                              dJ[0][2] * (2.0f * fx * t[0] / tz3) + dJ[1][2] * (2.0f * fy * t[1] / tz3);
-            if (fabsf(e.txtz) >= e.limx) dt0 = 0.0f;
-            if (fabsf(e.tytz) >= e.limy) dt1 = 0.0f;
-            const float* vm = cam.view_matrix;
-#pragma unroll
-            for (int col = 0; col < 3; col++) {
-                gp[col] += dt0 * vm[col * 4 + 0];
-                gp[col] += dt1 * vm[col * 4 + 1];
-                gp[col] += dt2 * vm[col * 4 + 2];
-            }
-            // ---- chain 4: means2D -> ndc -> p_hom -> position (:609-643) ----
-        const float4 r0 = s.rec0[i];
-        const float dndx = dm[0] * (float)cam.width * 0.5f;
-        const float dndy = dm[1] * (float)cam.height * 0.5f;
-        const float wh = ph[3] + 1e-7f;
-        const float iw = 1.0f / wh;
-        const float ndc_x = (2.0f * r0.x + 1.0f) / (float)cam.width - 1.0f;
-        const float ndc_y = (2.0f * r0.y + 1.0f) / (float)cam.height - 1.0f;
-        const float dph0 = dndx * iw, dph1 = dndy * iw, dph2 = 0.0f;
-        const float dph3 = -(ndc_x * dndx + ndc_y * dndy) * iw;
-        const float* VP = cam.viewproj_matrix;
-#pragma unroll
-        for (int dim = 0; dim < 3; dim++)
-            gp[dim] += VP[dim * 4 + 0] * dph0 + VP[dim * 4 + 1] * dph1 + VP[dim * 4 + 2] * dph2 +
-                       VP[dim * 4 + 3] * dph3;
-        }
-    }
-    if (FUSED) {
-#pragma unroll
-        for (int k = 0; k < 3; k++)
-            apply_update(sp, &raw.pos[3 * i + k], &adam.m_pos[3 * i + k], &adam.v_pos[3 * i + k], gp[k], sp.lr_pos);
-#pragma unroll
-        for (int k = 0; k < 3; k++)
-            apply_update(sp, &raw.sc[3 * i + k], &adam.m_sc[3 * i + k], &adam.v_sc[3 * i + k], gs[k], sp.lr_scale);
-#pragma unroll
-        for (int k = 0; k < 4; k++)
-            apply_update(sp, &raw.rot[4 * i + k], &adam.m_rot[4 * i + k], &adam.v_rot[4 * i + k], gq[k], sp.lr_rot);
-        apply_update(sp, &raw.op[i], &adam.m_op[i], &adam.v_op[i], gop, sp.lr_opac);
-        float* msh = adam.m_sh + (size_t)mc3 * i;
-        float* vsh = adam.v_sh + (size_t)mc3 * i;
-        for (int k = 0; k < mc; k++) {
-#pragma unroll
-            for (int c = 0; c < 3; c++) {
-                const float gsh = k < 16 ? basis[k] * geff[c] : 0.0f;
-                apply_update(sp, &shp[3 * k + c], &msh[3 * k + c], &vsh[3 * k + c], gsh, sp.lr_sh);
-            }
-        }
+        update_slice(sp, raw.pos + 3 * (size_t)g0, adam.m_pos + 3 * (size_t)g0, adam.v_pos + 3 * (size_t)g0,
+                     3 * ng, sp.lr_pos, [&](int e) { return sm.gpos[e]; }, [&](int e) { return sm.pos[e]; });
+        update_slice(sp, raw.sc + 3 * (size_t)g0, adam.m_sc + 3 * (size_t)g0, adam.v_sc + 3 * (size_t)g0,
+                     3 * ng, sp.lr_scale, [&](int e) { return sm.gsc[e]; }, [&](int e) { return sm.sc[e]; });
+        update_slice(sp, raw.rot + 4 * (size_t)g0, adam.m_rot + 4 * (size_t)g0, adam.v_rot + 4 * (size_t)g0,
+                     4 * ng, sp.lr_rot, [&](int e) { return sm.grot[e]; }, [&](int e) { return sm.rot[e]; });
+        update_slice(sp, raw.op + (size_t)g0, adam.m_op + (size_t)g0, adam.v_op + (size_t)g0, ng,
+                     sp.lr_opac, [&](int e) { return sm.gop[e]; }, [&](int e) { return sm.op[e]; });
+        update_slice(sp, raw.sh + (size_t)mc3 * g0, adam.m_sh + (size_t)mc3 * g0, adam.v_sh + (size_t)mc3 * g0,
+                     mc3 * ng, sp.lr_sh, sh_grad, [&](int e) {
+                         const int gg = e / mc3;
+                         return sm.sh[gg * kShPitch + (e - gg * mc3)];
+                     });
     } else {
-#pragma unroll
-        for (int k = 0; k < 3; k++) gout.g_pos[3 * i + k] = gp[k];
-#pragma unroll
-        for (int k = 0; k < 3; k++) gout.g_sc[3 * i + k] = gs[k];
-#pragma unroll
-        for (int k = 0; k < 4; k++) gout.g_rot[4 * i + k] = gq[k];
-        gout.g_op[i] = gop;
-        float* gsh = gout.g_sh + (size_t)mc3 * i;
-        for (int k = 0; k < mc; k++)
-#pragma unroll
-            for (int c = 0; c < 3; c++) gsh[3 * k + c] = k < 16 ? basis[k] * geff[c] : 0.0f;
+        for (int e = tid; e < 3 * ng; e += kBwdG) {
+            gout.g_pos[3 * (size_t)g0 + e] = sm.gpos[e];
+            gout.g_sc[3 * (size_t)g0 + e] = sm.gsc[e];
+        }
+        for (int e = tid; e < 4 * ng; e += kBwdG) gout.g_rot[4 * (size_t)g0 + e] = sm.grot[e];
+        for (int e = tid; e < ng; e += kBwdG) gout.g_op[(size_t)g0 + e] = sm.gop[e];
+        for (int e = tid; e < mc3 * ng; e += kBwdG) gout.g_sh[(size_t)mc3 * g0 + e] = sh_grad(e);
     }
 }
 
@@ -1133,9 +1310,18 @@ cudaError_t launch_preprocess_bwd_plain(cudaStream_t st, const StepParams* sp, i
                                         ModelPtrs raw, AdamPtrs adam, ScreenPtrs s, RGradPtrs rg, GradPtrs gout,
                                         Control* ctrl) {
     if (N <= 0) return cudaSuccess;
-    const int grid = blocks_for(N, kBlock);
-    if (fused_adam) k_preprocess_bwd<true><<<grid, kBlock, 0, st>>>(sp, N, raw, adam, s, rg, gout, ctrl);
-    else k_preprocess_bwd<false><<<grid, kBlock, 0, st>>>(sp, N, raw, adam, s, rg, gout, ctrl);
+    const int grid = blocks_for(N, kBwdG);
+    const int smem = (int)sizeof(BwdShared);
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaError_t e = cudaFuncSetAttribute(k_preprocess_bwd<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_preprocess_bwd<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return e;
+        attr_set = true;
+    }
+    if (fused_adam) k_preprocess_bwd<true><<<grid, kBwdG, smem, st>>>(sp, N, raw, adam, s, rg, gout, ctrl);
+    else k_preprocess_bwd<false><<<grid, kBwdG, smem, st>>>(sp, N, raw, adam, s, rg, gout, ctrl);
     return cudaGetLastError();
 }
 

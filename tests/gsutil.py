@@ -98,3 +98,19 @@ def cosine(a, b) -> float:
     a = np.asarray(a, np.float64).ravel()
     b = np.asarray(b, np.float64).ravel()
     return float(a @ b / (np.linalg.norm(a) * np.linalg.norm(b) + 1e-300))
+
+
+def fd_picks(lengths, n: int = 200, seed: int = 3):
+    """(group, index) of n random raw parameters, groups drawn uniformly."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        grp = int(rng.integers(len(lengths)))
+        out.append((grp, int(rng.integers(lengths[grp]))))
+    return out
+
+
+def fd_within(fd, ana):
+    """The reference's finite-difference tolerance (tools/verify_gradients_extended.py:455-490)."""
+    fd, ana = np.asarray(fd), np.asarray(ana)
+    return np.abs(fd - ana) <= 5e-5 * np.abs(fd).max() + 0.10 * np.maximum(np.abs(fd), np.abs(ana))
