@@ -83,6 +83,7 @@ struct gs3dc_ctx {
     // tiles / pixels
     int W = 0, H = 0, num_tiles = 0;
     DevBuf<unsigned> ranges;
+    DevBuf<unsigned> tile_order;   // heavy-first permutation of the tiles
     DevBuf<float> image, T_final, d_image, gt;
     DevBuf<int> n_contrib;
     DevBuf<unsigned> last_j;
@@ -254,6 +255,7 @@ int ensure_pixels(gs3dc_ctx* c, int W, int H) {
     const size_t np = (size_t)W * H;
     const int gx = (W + kTile - 1) / kTile, gy = (H + kTile - 1) / kTile;
     CK(c->ranges.ensure(2 * (size_t)gx * gy));
+    CK(c->tile_order.ensure((size_t)gx * gy));
     CK(c->image.ensure(3 * np));
     CK(c->T_final.ensure(np));
     CK(c->n_contrib.ensure(np));
@@ -391,7 +393,8 @@ int seq_sort(gs3dc_ctx* c) {
     c->sorted_which = which;
     if ((rc = mark(c, GS3DC_STAGE_RANGES))) return rc;
     CK(launch_tile_ranges(c->stream, c->cap, c->keys[which].p, c->ranges.p, c->ctrl));
-    c->kernels_last += 2 + c->sort_passes;
+    CK(launch_tile_order(c->stream, c->ranges.p, c->num_tiles, c->tile_order.p));
+    c->kernels_last += 3 + c->sort_passes;
     return GS3DC_OK;
 }
 
@@ -402,10 +405,10 @@ int seq_train(gs3dc_ctx* c) {
     if (rc) return rc;
     const int w = c->sorted_which;
     if ((rc = mark(c, GS3DC_STAGE_RASTER_FWD))) return rc;
-    CK(launch_raster_fwd_plain(c->stream, c->sp_dev, c->num_tiles, true, c->ranges.p, c->vals[w].p,
+    CK(launch_raster_fwd_plain(c->stream, c->sp_dev, c->num_tiles, true, c->ranges.p, c->tile_order.p, c->vals[w].p,
                                screen_ptrs(c, false), pixel_ptrs(c), c->ctrl));
     if ((rc = mark(c, GS3DC_STAGE_RASTER_BWD))) return rc;
-    CK(launch_raster_bwd_plain(c->stream, c->sp_dev, c->num_tiles, true, c->ranges.p, c->vals[w].p,
+    CK(launch_raster_bwd_plain(c->stream, c->sp_dev, c->num_tiles, true, c->ranges.p, c->tile_order.p, c->vals[w].p,
                                screen_ptrs(c, false), pixel_ptrs(c), rgrad_ptrs(c), c->ctrl));
     if ((rc = mark(c, GS3DC_STAGE_PREPROCESS_BWD))) return rc;
     CK(launch_preprocess_bwd_plain(c->stream, c->sp_dev, c->N, true, model_ptrs(c), adam_ptrs(c),
@@ -565,6 +568,7 @@ void gs3dc_destroy(gs3dc_ctx* c) {
     c->sort_desc.release();
     c->ctrl_region.release();
     c->ranges.release();
+    c->tile_order.release();
     c->last_j.release();
     c->dsign.release();
     if (c->sp_dev) cudaFree(c->sp_dev);
@@ -795,6 +799,7 @@ int gs3dc_sort_pairs(gs3dc_ctx* c, int64_t total_pairs, const uint64_t* keys, co
                         (unsigned long long)(keys[i] >> 32), num_tiles);
     int rc;
     CK(c->ranges.ensure(2 * (size_t)num_tiles));
+    CK(c->tile_order.ensure((size_t)num_tiles));
     c->num_tiles = num_tiles;
     if ((rc = ensure_pairs(c, P > c->cap ? P : c->cap, num_tiles))) return rc;
     // the sort reads only spin_limit from the parameters
@@ -830,7 +835,7 @@ int gs3dc_rasterize(gs3dc_ctx* c, const gs3d_camera* cam, const gs3d_render_conf
     CK(cudaSetDevice(c->device));
     if ((rc = push_params(c, cam, cfg, nullptr, 0, nullptr))) return rc;
     const int w = c->sorted_which;
-    CK(launch_raster_fwd_plain(c->stream, c->sp_dev, c->num_tiles, false, c->ranges.p, c->vals[w].p,
+    CK(launch_raster_fwd_plain(c->stream, c->sp_dev, c->num_tiles, false, c->ranges.p, c->tile_order.p, c->vals[w].p,
                                screen_ptrs(c, false), pixel_ptrs(c), c->ctrl));
     const size_t np = (size_t)c->W * c->H;
     if ((rc = download(c, image, c->image.p, 3 * np * 4)) || (rc = download(c, T_final, c->T_final.p, np * 4)) ||
@@ -873,7 +878,7 @@ int gs3dc_raster_backward(gs3dc_ctx* c, const gs3d_camera* cam, const gs3d_rende
     CK(cudaMemsetAsync(c->drgb.p, 0, 3 * n * 4, c->stream));
     CK(cudaMemsetAsync(c->dop.p, 0, n * 4, c->stream));
     const int w = c->sorted_which;
-    CK(launch_raster_bwd_plain(c->stream, c->sp_dev, c->num_tiles, false, c->ranges.p, c->vals[w].p,
+    CK(launch_raster_bwd_plain(c->stream, c->sp_dev, c->num_tiles, false, c->ranges.p, c->tile_order.p, c->vals[w].p,
                                screen_ptrs(c, false), pixel_ptrs(c), rgrad_ptrs(c), c->ctrl));
     if ((rc = download(c, d_means2D, c->dm2.p, 2 * n * 4)) || (rc = download(c, d_conics, c->dcon.p, 3 * n * 4)) ||
         (rc = download(c, d_rgb, c->drgb.p, 3 * n * 4)) || (rc = download(c, d_opacities_2d, c->dop.p, n * 4)))

@@ -84,12 +84,13 @@ cudaError_t launch_preprocess_plain(cudaStream_t st, const StepParams* sp, int N
 cudaError_t launch_bin_arrays(cudaStream_t st, const StepParams* sp, int N, ScreenArrays a,
                               PairPtrs pr, Control* ctrl);
 cudaError_t launch_export_screen(cudaStream_t st, int N, ScreenPtrs s, ScreenArrays a);
+// order: tile permutation (heavy first) or NULL for row-major
 cudaError_t launch_raster_fwd_plain(cudaStream_t st, const StepParams* sp, int num_tiles, bool fused_loss,
-                                    const unsigned* ranges, const unsigned* vals, ScreenPtrs s,
-                                    PixelPtrs px, Control* ctrl);
+                                    const unsigned* ranges, const unsigned* order, const unsigned* vals,
+                                    ScreenPtrs s, PixelPtrs px, Control* ctrl);
 cudaError_t launch_raster_bwd_plain(cudaStream_t st, const StepParams* sp, int num_tiles, bool from_sign,
-                                    const unsigned* ranges, const unsigned* vals, ScreenPtrs s,
-                                    PixelPtrs px, RGradPtrs g, Control* ctrl);
+                                    const unsigned* ranges, const unsigned* order, const unsigned* vals,
+                                    ScreenPtrs s, PixelPtrs px, RGradPtrs g, Control* ctrl);
 cudaError_t launch_preprocess_bwd_plain(cudaStream_t st, const StepParams* sp, int N, bool fused_adam,
                                         ModelPtrs raw, AdamPtrs adam, ScreenPtrs s, RGradPtrs rg,
                                         GradPtrs gout, Control* ctrl);
@@ -108,6 +109,9 @@ cudaError_t launch_radix_sort(cudaStream_t st, const StepParams* sp, int sort_pa
                               cudaEvent_t after_hist = nullptr);
 cudaError_t launch_tile_ranges(cudaStream_t st, unsigned long long capacity,
                                const unsigned long long* keys_sorted, unsigned* ranges, Control* ctrl);
+
+// Heavy-first permutation of the tiles (by pair count) for the rasterisers.
+cudaError_t launch_tile_order(cudaStream_t st, const unsigned* ranges, int num_tiles, unsigned* order);
 
 // Bounded-wait self-test: desc2 = two zeroed descriptors.
 cudaError_t launch_wait_selftest(cudaStream_t st, unsigned long long* desc2, unsigned* status, unsigned spin_limit);

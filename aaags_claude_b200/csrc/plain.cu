@@ -240,6 +240,31 @@ __device__ __forceinline__ int blend_decision(float power, float o, float T, flo
     return 1;
 }
 
+// A power below this bound gives alpha = o * exp(power) < 1/255 for certain
+// (ln(1/(255 o)) less a margin far above the rounding of logf / expf), so the
+// blend loops skip such Gaussians without evaluating exp; the skip they take
+// is the one blend_decision / alpha_accept would take.
+__device__ __forceinline__ float skip_threshold(float o) { return logf(kAlphaMin / o) - 1e-3f; }
+
+// Axis-aligned box (xmin, xmax, ymin, ymax) in pixels outside of which the
+// Gaussian's power is below skip_threshold: the ellipse
+// d^T C d <= -2 thr has half extents sqrt(-2 thr * Sigma_xx), sqrt(-2 thr *
+// Sigma_yy) with Sigma = C^-1, widened by one pixel for rounding.  A warp
+// whose pixels all lie outside it skips the Gaussian without evaluating it.
+__device__ __forceinline__ float4 skip_box(float4 r0, float4 r1, float thr) {
+    const float t2 = -2.0f * thr;
+    const float det = r0.z * r1.x - r0.w * r0.w;   // conic a c - b^2
+    if (!(t2 > 0.0f)) return make_float4(1e30f, -1e30f, 1e30f, -1e30f);     // never reaches alpha 1/255
+    if (!(det > 0.0f)) return make_float4(-1e30f, 1e30f, -1e30f, 1e30f);    // not positive definite: no culling
+    const float ex = sqrtf(t2 * r1.x / det) + 1.0f;
+    const float ey = sqrtf(t2 * r0.z / det) + 1.0f;
+    return make_float4(r0.x - ex, r0.x + ex, r0.y - ey, r0.y + ey);
+}
+
+__device__ __forceinline__ bool box_misses(float4 b, float x0, float x1, float y0, float y1) {
+    return b.y < x0 || b.x > x1 || b.w < y0 || b.z > y1;
+}
+
 // The alpha-only decision of the backward (the forward's last-contributor
 // index already encodes the stop); agrees with blend_decision's skip and
 // yields the same alpha and exp for accepted Gaussians.
@@ -500,21 +525,27 @@ __global__ void k_export_screen(int N, ScreenPtrs s, ScreenArrays a) {
 template <bool FUSED_LOSS>
 __global__ void __launch_bounds__(kBlock) k_raster_fwd(const StepParams* __restrict__ spp,
                                                        const unsigned* __restrict__ ranges,
+                                                       const unsigned* __restrict__ order,
                                                        const unsigned* __restrict__ vals, ScreenPtrs s,
                                                        PixelPtrs px, Control* ctrl) {
     __shared__ float4 s_r0[kBlock];
     __shared__ float4 s_r1[kBlock];
     __shared__ float s_b[kBlock];
+    __shared__ float s_thr[kBlock];
+    __shared__ float4 s_box[kBlock];
     __shared__ double s_loss[kBlock / 32];
     const StepParams& sp = *spp;
     const int W = sp.cam.width, H = sp.cam.height;
-    const int tile = blockIdx.x;
+    const int tile = order ? (int)order[blockIdx.x] : (int)blockIdx.x;
     const int tx = tile % sp.grid_x, ty = tile / sp.grid_x;
     const int x = tx * kTile + (threadIdx.x & (kTile - 1));
     const int y = ty * kTile + (threadIdx.x >> 4);
     const bool inside = x < W && y < H;
     const unsigned rs = ranges[2 * tile], re = ranges[2 * tile + 1];
     const float fx = (float)x, fy = (float)y;
+    // this warp's 16x2 pixel strip
+    const float wx0 = (float)(tx * kTile), wx1 = wx0 + (float)(kTile - 1);
+    const float wy0 = (float)(ty * kTile + 2 * (threadIdx.x >> 5)), wy1 = wy0 + 1.0f;
     float T = 1.0f, C0 = 0.0f, C1 = 0.0f, C2 = 0.0f;
     int cnt = 0;
     unsigned last = 0;
@@ -524,19 +555,25 @@ __global__ void __launch_bounds__(kBlock) k_raster_fwd(const StepParams* __restr
         const unsigned j = b + threadIdx.x;
         if (j < re) {
             const unsigned g = vals[j];
-            s_r0[threadIdx.x] = s.rec0[g];
-            s_r1[threadIdx.x] = s.rec1[g];
+            const float4 r0 = s.rec0[g];
+            const float4 r1 = s.rec1[g];
+            const float thr = skip_threshold(r1.y);
+            s_r0[threadIdx.x] = r0;
+            s_r1[threadIdx.x] = r1;
             s_b[threadIdx.x] = s.col_b[g];
+            s_thr[threadIdx.x] = thr;
+            s_box[threadIdx.x] = skip_box(r0, r1, thr);
         }
         __syncthreads();
         const int nb = (int)min((unsigned)kBlock, re - b);
         if (!done) {
             for (int k = 0; k < nb; k++) {
+                if (box_misses(s_box[k], wx0, wx1, wy0, wy1)) continue;   // warp-uniform
                 const float4 a = s_r0[k];
                 const float dx = a.x - fx, dy = a.y - fy;
                 const float4 c = s_r1[k];
                 const float power = -0.5f * (a.z * dx * dx + c.x * dy * dy) - a.w * dx * dy;
-                if (power > 0.0f) continue;
+                if (power < s_thr[k] || power > 0.0f) continue;
                 float alpha, e, test_T;
                 const int dec = blend_decision(power, c.y, T, alpha, e, test_T);
                 if (dec == 0) continue;
@@ -633,18 +670,21 @@ __device__ __forceinline__ float warp_sum8(const float v[8], int* idx) {
 template <bool FROM_SIGN>
 __global__ void __launch_bounds__(kBlock) k_raster_bwd(const StepParams* __restrict__ spp,
                                                        const unsigned* __restrict__ ranges,
+                                                       const unsigned* __restrict__ order,
                                                        const unsigned* __restrict__ vals, ScreenPtrs s,
                                                        PixelPtrs px, RGradPtrs g, Control* ctrl) {
     __shared__ float4 s_r0[kBlock];
     __shared__ float4 s_r1[kBlock];
     __shared__ float s_b[kBlock];
     __shared__ unsigned s_idx[kBlock];
+    __shared__ float s_thr[kBlock];
+    __shared__ float4 s_box[kBlock];
     __shared__ float s_acc[9][kBlock];   // r, g, b, opacity, mean.x, mean.y, conic a, b, c
     __shared__ unsigned s_maxlast;
     const StepParams& sp = *spp;
     if (FROM_SIGN && ((ctrl->status & kStatusOverflow) || sp.persist->sticky_overflow)) return;
     const int W = sp.cam.width, H = sp.cam.height;
-    const int tile = blockIdx.x;
+    const int tile = order ? (int)order[blockIdx.x] : (int)blockIdx.x;
     const int tx = tile % sp.grid_x, ty = tile / sp.grid_x;
     const int x = tx * kTile + (threadIdx.x & (kTile - 1));
     const int y = ty * kTile + (threadIdx.x >> 4);
@@ -677,21 +717,32 @@ __global__ void __launch_bounds__(kBlock) k_raster_bwd(const StepParams* __restr
     const unsigned maxlast = s_maxlast;
     if (maxlast <= rs) return;
     const unsigned lane = threadIdx.x & 31;
+    const unsigned wlast = __reduce_max_sync(0xffffffffu, last);
+    const float wx0 = (float)(tx * kTile), wx1 = wx0 + (float)(kTile - 1);
+    const float wy0 = (float)(ty * kTile + 2 * (threadIdx.x >> 5)), wy1 = wy0 + 1.0f;
     // batches [bs, be) walked from the back; the first one ends at maxlast
     for (unsigned be = maxlast; be > rs;) {
         const unsigned bs = (be - rs > (unsigned)kBlock) ? be - kBlock : rs;
         const unsigned j = bs + threadIdx.x;
         if (j < be) {
             const unsigned gi = vals[j];
+            const float4 r0 = s.rec0[gi];
+            const float4 r1 = s.rec1[gi];
+            const float thr = skip_threshold(r1.y);
             s_idx[threadIdx.x] = gi;
-            s_r0[threadIdx.x] = s.rec0[gi];
-            s_r1[threadIdx.x] = s.rec1[gi];
+            s_r0[threadIdx.x] = r0;
+            s_r1[threadIdx.x] = r1;
             s_b[threadIdx.x] = s.col_b[gi];
+            s_thr[threadIdx.x] = thr;
+            s_box[threadIdx.x] = skip_box(r0, r1, thr);
         }
 #pragma unroll
         for (int v = 0; v < 9; v++) s_acc[v][threadIdx.x] = 0.0f;
         __syncthreads();
-        for (int k = (int)(be - bs) - 1; k >= 0; k--) {
+        // this warp only needs the entries below its own last contributor
+        const int kstart = (int)(min(be, wlast) - min(bs, wlast)) - 1;
+        for (int k = kstart; k >= 0; k--) {
+            if (box_misses(s_box[k], wx0, wx1, wy0, wy1)) continue;   // warp-uniform
             const unsigned jj = bs + (unsigned)k;
             bool contrib = false;
             float gv[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
@@ -702,7 +753,7 @@ __global__ void __launch_bounds__(kBlock) k_raster_bwd(const StepParams* __restr
                 const float dx = a.x - fx, dy = a.y - fy;
                 const float power = -0.5f * (a.z * dx * dx + c.x * dy * dy) - a.w * dx * dy;
                 float alpha, ep;
-                if (!(power > 0.0f) && alpha_accept(power, c.y, alpha, ep)) {
+                if (!(power < s_thr[k]) && !(power > 0.0f) && alpha_accept(power, c.y, alpha, ep)) {
                     contrib = true;
                     const float cb = s_b[k];
                     const float oma = 1.0f - alpha;
@@ -1060,6 +1111,7 @@ struct BwdShared {
 __device__ __forceinline__ void stage_in(float* dst, float* src, int n, bool zero_src) {
     const int n4 = n >> 2;
     float4* s4 = reinterpret_cast<float4*>(src);
+#pragma unroll 4
     for (int q = threadIdx.x; q < n4; q += kBwdG) {
         const float4 v = s4[q];
         dst[4 * q] = v.x;
@@ -1083,6 +1135,7 @@ __device__ __forceinline__ void update_slice(const StepParams& sp, float* p, flo
     float4* p4 = reinterpret_cast<float4*>(p);
     float4* m4 = reinterpret_cast<float4*>(m);
     float4* v4 = reinterpret_cast<float4*>(v);
+#pragma unroll 4
     for (int q = threadIdx.x; q < n4; q += kBwdG) {
         float4 pp, mm, vv;
         pp.x = p_s(4 * q); pp.y = p_s(4 * q + 1); pp.z = p_s(4 * q + 2); pp.w = p_s(4 * q + 3);
@@ -1150,6 +1203,7 @@ __global__ void __launch_bounds__(kBwdG, 4) k_preprocess_bwd(const StepParams* _
         const int n = mc3 * ng;
         if ((mc3 & 3) == 0) {
             const float4* s4 = reinterpret_cast<const float4*>(src);
+#pragma unroll 4
             for (int qd = tid; qd < (n >> 2); qd += kBwdG) {
                 const float4 v = s4[qd];
                 const int e = 4 * qd;
@@ -1289,20 +1343,20 @@ cudaError_t launch_export_screen(cudaStream_t st, int N, ScreenPtrs s, ScreenArr
 }
 
 cudaError_t launch_raster_fwd_plain(cudaStream_t st, const StepParams* sp, int num_tiles, bool fused_loss,
-                                    const unsigned* ranges, const unsigned* vals, ScreenPtrs s, PixelPtrs px,
-                                    Control* ctrl) {
+                                    const unsigned* ranges, const unsigned* order, const unsigned* vals,
+                                    ScreenPtrs s, PixelPtrs px, Control* ctrl) {
     if (num_tiles <= 0) return cudaSuccess;
-    if (fused_loss) k_raster_fwd<true><<<num_tiles, kBlock, 0, st>>>(sp, ranges, vals, s, px, ctrl);
-    else k_raster_fwd<false><<<num_tiles, kBlock, 0, st>>>(sp, ranges, vals, s, px, ctrl);
+    if (fused_loss) k_raster_fwd<true><<<num_tiles, kBlock, 0, st>>>(sp, ranges, order, vals, s, px, ctrl);
+    else k_raster_fwd<false><<<num_tiles, kBlock, 0, st>>>(sp, ranges, order, vals, s, px, ctrl);
     return cudaGetLastError();
 }
 
 cudaError_t launch_raster_bwd_plain(cudaStream_t st, const StepParams* sp, int num_tiles, bool from_sign,
-                                    const unsigned* ranges, const unsigned* vals, ScreenPtrs s, PixelPtrs px,
-                                    RGradPtrs g, Control* ctrl) {
+                                    const unsigned* ranges, const unsigned* order, const unsigned* vals,
+                                    ScreenPtrs s, PixelPtrs px, RGradPtrs g, Control* ctrl) {
     if (num_tiles <= 0) return cudaSuccess;
-    if (from_sign) k_raster_bwd<true><<<num_tiles, kBlock, 0, st>>>(sp, ranges, vals, s, px, g, ctrl);
-    else k_raster_bwd<false><<<num_tiles, kBlock, 0, st>>>(sp, ranges, vals, s, px, g, ctrl);
+    if (from_sign) k_raster_bwd<true><<<num_tiles, kBlock, 0, st>>>(sp, ranges, order, vals, s, px, g, ctrl);
+    else k_raster_bwd<false><<<num_tiles, kBlock, 0, st>>>(sp, ranges, order, vals, s, px, g, ctrl);
     return cudaGetLastError();
 }
 

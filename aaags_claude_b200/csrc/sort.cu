@@ -172,6 +172,36 @@ __global__ void k_ranges(const unsigned long long* __restrict__ keys, unsigned l
     }
 }
 
+// Heavy-first tile order: one CTA buckets the tiles by floor(log2(pairs))
+// and writes them heaviest bucket first, so the rasterisers (one CTA per
+// tile) start the long central tiles before the many short ones instead of
+// finishing on them.  The order inside a bucket does not matter (tiles are
+// independent).
+__global__ void __launch_bounds__(1024) k_tile_order(const unsigned* __restrict__ ranges, int num_tiles,
+                                                     unsigned* __restrict__ order) {
+    __shared__ unsigned s_cnt[33];
+    __shared__ unsigned s_off[33];
+    if (threadIdx.x < 33) s_cnt[threadIdx.x] = 0;
+    __syncthreads();
+    for (int t = threadIdx.x; t < num_tiles; t += blockDim.x) {
+        const unsigned n = ranges[2 * t + 1] - ranges[2 * t];
+        atomicAdd(&s_cnt[n ? 32 - __clz(n) : 0], 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned acc = 0;
+        for (int b = 32; b >= 0; b--) {   // heaviest bucket first
+            s_off[b] = acc;
+            acc += s_cnt[b];
+        }
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < num_tiles; t += blockDim.x) {
+        const unsigned n = ranges[2 * t + 1] - ranges[2 * t];
+        order[atomicAdd(&s_off[n ? 32 - __clz(n) : 0], 1u)] = (unsigned)t;
+    }
+}
+
 // One CTA plays block 1 of a look-back whose block 0 never publishes: the
 // wait must run out after spin_limit polls and raise kStatusTimeout.
 __global__ void k_wait_selftest(unsigned long long* desc, unsigned* status, unsigned spin_limit) {
@@ -228,6 +258,12 @@ cudaError_t launch_tile_ranges(cudaStream_t st, unsigned long long capacity, con
                                unsigned* ranges, Control* ctrl) {
     if (capacity == 0) return cudaSuccess;
     k_ranges<<<4 * 148, 256, 0, st>>>(keys_sorted, capacity, ranges, ctrl);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tile_order(cudaStream_t st, const unsigned* ranges, int num_tiles, unsigned* order) {
+    if (num_tiles <= 0) return cudaSuccess;
+    k_tile_order<<<1, 1024, 0, st>>>(ranges, num_tiles, order);
     return cudaGetLastError();
 }
 
