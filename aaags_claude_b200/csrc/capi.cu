@@ -100,6 +100,7 @@ struct gs3dc_ctx {
          have_rgrad = false, have_grads = false;
     // graph of the train step
     bool use_graph = true;
+    bool fused_adam = false;   // split backward + optimiser by default (faster at this occupancy)
     cudaGraphExec_t graph = nullptr;
     long long graph_key[8] = {};
     long long graph_replays = 0;
@@ -238,6 +239,16 @@ int zero_adam(gs3dc_ctx* c) {
         if (bufs[k]->n) CK(cudaMemsetAsync(bufs[k]->p, 0, bufs[k]->n * sizeof(float), c->stream));
     CK(cudaMemsetAsync(c->persist, 0, sizeof(Persist), c->stream));
     c->adam_step = 0;
+    return GS3DC_OK;
+}
+
+int ensure_grads(gs3dc_ctx* c) {
+    const size_t n = (size_t)c->N, mc3 = (size_t)c->max_coeffs * 3;
+    CK(c->g_pos.ensure(3 * n));
+    CK(c->g_sc.ensure(3 * n));
+    CK(c->g_rot.ensure(4 * n));
+    CK(c->g_sh.ensure(mc3 * n));
+    CK(c->g_op.ensure(n));
     return GS3DC_OK;
 }
 
@@ -411,8 +422,16 @@ int seq_train(gs3dc_ctx* c) {
     CK(launch_raster_bwd_plain(c->stream, c->sp_dev, c->num_tiles, true, c->ranges.p, c->tile_order.p, c->vals[w].p,
                                screen_ptrs(c, false), pixel_ptrs(c), rgrad_ptrs(c), c->ctrl));
     if ((rc = mark(c, GS3DC_STAGE_PREPROCESS_BWD))) return rc;
-    CK(launch_preprocess_bwd_plain(c->stream, c->sp_dev, c->N, true, model_ptrs(c), adam_ptrs(c),
-                                   screen_ptrs(c, false), rgrad_ptrs(c), grad_ptrs(c), c->ctrl));
+    if (c->fused_adam) {
+        CK(launch_preprocess_bwd_plain(c->stream, c->sp_dev, c->N, c->max_coeffs * 3, 1, model_ptrs(c),
+                                       adam_ptrs(c), screen_ptrs(c, false), rgrad_ptrs(c), grad_ptrs(c), c->ctrl));
+    } else {
+        CK(launch_preprocess_bwd_plain(c->stream, c->sp_dev, c->N, c->max_coeffs * 3, 2, model_ptrs(c),
+                                       adam_ptrs(c), screen_ptrs(c, false), rgrad_ptrs(c), grad_ptrs(c), c->ctrl));
+        CK(launch_optimizer_plain(c->stream, c->sp_dev, c->N, c->max_coeffs * 3, model_ptrs(c), adam_ptrs(c),
+                                  grad_ptrs(c), c->ctrl));
+        c->kernels_last += 1;
+    }
     if ((rc = mark(c, GS3DC_NUM_STAGES))) return rc;
     c->kernels_last += 3;
     return GS3DC_OK;
@@ -610,6 +629,9 @@ int gs3dc_set_option(gs3dc_ctx* c, int option, int64_t value) {
                 cudaGraphExecDestroy(c->graph);
                 c->graph = nullptr;
             }
+            return GS3DC_OK;
+        case GS3DC_OPT_FUSED_ADAM:
+            c->fused_adam = value != 0;
             return GS3DC_OK;
         case GS3DC_OPT_STAGE_TIMING:
             c->stage_timing = value != 0;
@@ -904,7 +926,7 @@ int gs3dc_preprocess_backward(gs3dc_ctx* c, const gs3d_camera* cam, const gs3d_r
     CK(c->g_sh.ensure(mc3 * n));
     CK(c->g_op.ensure(n));
     if ((rc = push_params(c, cam, cfg, nullptr, 0, nullptr))) return rc;
-    CK(launch_preprocess_bwd_plain(c->stream, c->sp_dev, c->N, false, model_ptrs(c), adam_ptrs(c),
+    CK(launch_preprocess_bwd_plain(c->stream, c->sp_dev, c->N, c->max_coeffs * 3, 0, model_ptrs(c), adam_ptrs(c),
                                    screen_ptrs(c, false), rgrad_ptrs(c), grad_ptrs(c), c->ctrl));
     if ((rc = download(c, d_raw_positions, c->g_pos.p, 3 * n * 4)) ||
         (rc = download(c, d_raw_scales, c->g_sc.p, 3 * n * 4)) ||
@@ -932,7 +954,8 @@ int gs3dc_optimizer_step(gs3dc_ctx* c, const gs3d_train_config* tc, int iteratio
     cfg.tile_w = cfg.tile_h = kTile;
     cfg.scale_modifier = 1.0f;
     if ((rc = push_params(c, &cam, &cfg, tc, iteration, nullptr))) return rc;
-    CK(launch_optimizer_plain(c->stream, c->sp_dev, c->N, c->max_coeffs * 3, model_ptrs(c), adam_ptrs(c), grad_ptrs(c)));
+    CK(launch_optimizer_plain(c->stream, c->sp_dev, c->N, c->max_coeffs * 3, model_ptrs(c), adam_ptrs(c), grad_ptrs(c),
+                              nullptr));
     CK(cudaStreamSynchronize(c->stream));
     c->have_screen = c->have_pairs = c->have_sorted = c->have_raster = c->have_rgrad = c->have_grads = false;
     return GS3DC_OK;
@@ -989,6 +1012,7 @@ int gs3dc_train_step(gs3dc_ctx* c, const gs3d_camera* cam, const float* gt, int 
     if (!c->model_raw) return fail(c, GS3DC_ERR_STATE, "gs3dc_train_step needs a raw model (gs3dc_set_raw_params)");
     CK(cudaSetDevice(c->device));
     if ((rc = ensure_adam(c))) return rc;
+    if ((rc = ensure_grads(c))) return rc;
     if ((rc = ensure_pixels(c, cam->width, cam->height))) return rc;
     const size_t np = (size_t)cam->width * cam->height;
     const float* gt_dev = gt;
@@ -1007,7 +1031,7 @@ int gs3dc_train_step(gs3dc_ctx* c, const gs3d_camera* cam, const float* gt, int 
         c->adam_step = step_before + (tc->use_adam ? 1 : 0);
         if ((rc = push_params(c, cam, cfg, tc, iteration, gt_dev))) return rc;
         const long long key[8] = {c->N, c->max_coeffs, cam->width, cam->height, (long long)c->cap, c->sort_passes,
-                                  (long long)c->spin_limit, 1};
+                                  (long long)c->spin_limit, c->fused_adam ? 1 : 2};
         const bool key_ok = c->graph && std::memcmp(key, c->graph_key, sizeof(key)) == 0;
         c->kernels_last = 0;
         if (c->use_graph && !c->stage_timing && !first && attempt == 0) {

@@ -120,6 +120,53 @@ __device__ __forceinline__ unsigned long long lookback_exclusive(unsigned long l
     return lookback_exclusive_strided(desc, blk, 1, 0, aggregate, status, spin_limit);
 }
 
+// ---- TMA bulk copies (cp.async.bulk) completing on an mbarrier ----
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+// Makes the initialised barriers visible to the async (TMA) proxy.
+__device__ __forceinline__ void mbar_fence_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// One arrival that also announces `bytes` of transactions to wait for.
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// Global -> shared bulk copy; dst, src 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void tma_load_1d(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned phase) {
+    unsigned done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(smem_addr(bar)), "r"(phase)
+        : "memory");
+    return done != 0;
+}
+
+// Bounded wait for `phase` of the barrier: false (and kStatusTimeout) if the
+// copies have not landed after spin_limit polls.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned phase, unsigned spin_limit,
+                                          unsigned* status) {
+    for (unsigned i = 0; i < spin_limit; i++)
+        if (mbar_try_wait(bar, phase)) return true;
+    atomicOr(status, kStatusTimeout);
+    return false;
+}
+
 // Correctly rounded float exp (double evaluation, one rounding).  glibc's
 // expf, which the reference calls through std::exp(float), agrees with it on
 // all but ~0.006% of inputs (by 1 ulp there).

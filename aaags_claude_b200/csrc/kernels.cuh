@@ -91,11 +91,15 @@ cudaError_t launch_raster_fwd_plain(cudaStream_t st, const StepParams* sp, int n
 cudaError_t launch_raster_bwd_plain(cudaStream_t st, const StepParams* sp, int num_tiles, bool from_sign,
                                     const unsigned* ranges, const unsigned* order, const unsigned* vals,
                                     ScreenPtrs s, PixelPtrs px, RGradPtrs g, Control* ctrl);
-cudaError_t launch_preprocess_bwd_plain(cudaStream_t st, const StepParams* sp, int N, bool fused_adam,
+// mode: 0 = write GradientOutput (stage API), 1 = fused optimiser, 2 = write
+// GradientOutput for a following launch_optimizer_plain and zero the screen
+// gradient accumulators (split train step).  mc3 in {3, 12, 27, 48}.
+cudaError_t launch_preprocess_bwd_plain(cudaStream_t st, const StepParams* sp, int N, int mc3, int mode,
                                         ModelPtrs raw, AdamPtrs adam, ScreenPtrs s, RGradPtrs rg,
                                         GradPtrs gout, Control* ctrl);
+// ctrl != NULL: skip an overflowed / unacknowledged train step.
 cudaError_t launch_optimizer_plain(cudaStream_t st, const StepParams* sp, int N, int mc3, ModelPtrs raw,
-                                   AdamPtrs adam, GradPtrs g);
+                                   AdamPtrs adam, GradPtrs g, const Control* ctrl);
 
 // ---- radix sort + ranges (sort.cu) ----
 // Sorts (keys, vals) of *P (device) pairs by the low sort_bits key bits with

@@ -22,6 +22,7 @@
 //                   reduced and one lane issues the atomics.
 //   k_preprocess_bwd  the full per-Gaussian adjoint chain, fused with Adam.
 #include <cuda_runtime.h>
+#include <cstddef>
 #include <cstdint>
 
 #include "common.cuh"
@@ -1082,143 +1083,186 @@ __device__ __forceinline__ void backward_one(const StepParams& sp, const BwdIn& 
         o.gp[dim] += VP[dim * 4 + 0] * dph0 + VP[dim * 4 + 1] * dph1 + VP[dim * 4 + 2] * dph2 + VP[dim * 4 + 3] * dph3;
 }
 
-// ---- fused preprocess backward + optimiser, staged through shared memory ----
+// ---- fused preprocess backward + optimiser, staged by TMA into shared memory ----
 //
-// One CTA owns kBwdG consecutive Gaussians.  Phase 0 loads their parameter
-// slices (positions, scales, rotations, opacities, SH), raster gradients and
-// radii with coalesced vector loads into shared memory (SH with a 49-float
-// row pitch so the per-Gaussian reads of phase 1 are bank-conflict free) and
-// zeroes the gradient accumulators for the next step.  Phase 1 runs the
-// per-Gaussian adjoint chain, one thread per Gaussian, out of shared memory.
-// Phase 2 applies Adam (or SGD) element by element over each parameter array:
-// consecutive threads touch consecutive floats of params, m and v.
-constexpr int kBwdG = 128;         // Gaussians (= threads) per CTA
-constexpr int kShPitch = 49;       // padded SH row (48 floats + 1)
-constexpr int kBasisPitch = 17;
+// One CTA owns kBwdG consecutive Gaussians.  A single thread issues TMA bulk
+// copies (cp.async.bulk) of the CTA's slices of every parameter array, of the
+// screen-space gradients and of the radii onto mbarrier A, and of the Adam
+// moments onto mbarrier B.  The CTA waits on A, runs the per-Gaussian adjoint
+// (one thread per Gaussian) while the moments are still arriving, then waits on
+// B and applies the optimiser element by element out of shared memory with
+// coalesced vector stores.  The partial slice at the end of the model (sizes
+// not multiples of 16 bytes) is staged with ordinary loads instead.
+constexpr int kBwdG = 128;        // Gaussians (= threads) per CTA
+constexpr int kMaxMc3 = 48;       // SH floats per Gaussian at degree 3
+constexpr int kBasisPitch = 17;   // padded row of the per-Gaussian SH basis values
 
-struct BwdShared {
-    float sh[kBwdG * kShPitch];
-    float basis[kBwdG * kBasisPitch];
-    float geff[kBwdG * 3];
-    float pos[kBwdG * 3], sc[kBwdG * 3], rot[kBwdG * 4], op[kBwdG];      // raw parameters
-    float gpos[kBwdG * 3], gsc[kBwdG * 3], grot[kBwdG * 4], gop[kBwdG];  // their gradients
-    float dm2[kBwdG * 2], dcon[kBwdG * 3], drgb[kBwdG * 3], dop[kBwdG];  // screen-space gradients
+// The Adam moments come last: modes without the fused optimiser launch with
+// offsetof(BwdShared, m_sh) bytes of shared memory and fit more CTAs per SM.
+struct __align__(16) BwdShared {
+    unsigned long long bar_a, bar_b;
+    float sh[kBwdG * kMaxMc3];
+    float pos[kBwdG * 3], sc[kBwdG * 3], rot[kBwdG * 4], op[kBwdG];
+    float dm2[kBwdG * 2], dcon[kBwdG * 3], drgb[kBwdG * 3], dop[kBwdG];
     int radius[kBwdG];
+    float basis[kBwdG * kBasisPitch], geff[kBwdG * 3];
+    float gpos[kBwdG * 3], gsc[kBwdG * 3], grot[kBwdG * 4], gop[kBwdG];
+    float m_sh[kBwdG * kMaxMc3], v_sh[kBwdG * kMaxMc3];
+    float m_pos[kBwdG * 3], v_pos[kBwdG * 3], m_sc[kBwdG * 3], v_sc[kBwdG * 3];
+    float m_rot[kBwdG * 4], v_rot[kBwdG * 4], m_op[kBwdG], v_op[kBwdG];
 };
 
-// Coalesced copy of n floats from global to shared memory (both 16-byte
-// aligned when n_full is a multiple of 4), zeroing the source if asked.
-__device__ __forceinline__ void stage_in(float* dst, float* src, int n, bool zero_src) {
-    const int n4 = n >> 2;
-    float4* s4 = reinterpret_cast<float4*>(src);
-#pragma unroll 4
-    for (int q = threadIdx.x; q < n4; q += kBwdG) {
-        const float4 v = s4[q];
-        dst[4 * q] = v.x;
-        dst[4 * q + 1] = v.y;
-        dst[4 * q + 2] = v.z;
-        dst[4 * q + 3] = v.w;
-        if (zero_src) s4[q] = make_float4(0.f, 0.f, 0.f, 0.f);
-    }
-    for (int e = 4 * n4 + threadIdx.x; e < n; e += kBwdG) {
-        dst[e] = src[e];
-        if (zero_src) src[e] = 0.f;
-    }
+// Ordinary (tail-slice) staging of n floats.
+__device__ __forceinline__ void copy_in(float* dst, const float* src, int n) {
+    for (int e = threadIdx.x; e < n; e += kBwdG) dst[e] = src[e];
 }
 
-// Optimiser over one parameter group slice: params p[0..n), moments m, v, the
-// gradient of element e given by grad(e); the updated parameters go back to p.
-template <class GradFn, class ParamFn>
-__device__ __forceinline__ void update_slice(const StepParams& sp, float* p, float* m, float* v, int n, float lr,
-                                             GradFn grad, ParamFn p_s) {
-    const int n4 = n >> 2;
-    float4* p4 = reinterpret_cast<float4*>(p);
-    float4* m4 = reinterpret_cast<float4*>(m);
-    float4* v4 = reinterpret_cast<float4*>(v);
-#pragma unroll 4
+// Zeroes n floats of a gradient accumulator (coalesced, vectorised when aligned).
+__device__ __forceinline__ void zero_out(float* dst, int n) {
+    const int n4 = (((size_t)dst & 15) == 0) ? (n >> 2) : 0;
+    float4* d4 = reinterpret_cast<float4*>(dst);
+    for (int q = threadIdx.x; q < n4; q += kBwdG) d4[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int e = 4 * n4 + threadIdx.x; e < n; e += kBwdG) dst[e] = 0.f;
+}
+
+// Optimiser over one parameter-group slice of n elements: parameters, moments
+// and gradients read from shared memory, results stored to global memory.
+template <class GradFn>
+__device__ __forceinline__ void update_slice(const StepParams& sp, float* p_g, float* m_g, float* v_g,
+                                             const float* p_s, const float* m_s, const float* v_s, int n,
+                                             float lr, GradFn grad) {
+    const bool vec = (((size_t)p_g | (size_t)m_g | (size_t)v_g) & 15) == 0;
+    const int n4 = vec ? (n >> 2) : 0;
     for (int q = threadIdx.x; q < n4; q += kBwdG) {
-        float4 pp, mm, vv;
-        pp.x = p_s(4 * q); pp.y = p_s(4 * q + 1); pp.z = p_s(4 * q + 2); pp.w = p_s(4 * q + 3);
-        if (sp.use_adam) {
-            mm = m4[q];
-            vv = v4[q];
-            pp.x = adam_elem(pp.x, mm.x, vv.x, grad(4 * q), lr, sp.beta1, sp.beta2, sp.eps, sp.bc1, sp.bc2);
-            pp.y = adam_elem(pp.y, mm.y, vv.y, grad(4 * q + 1), lr, sp.beta1, sp.beta2, sp.eps, sp.bc1, sp.bc2);
-            pp.z = adam_elem(pp.z, mm.z, vv.z, grad(4 * q + 2), lr, sp.beta1, sp.beta2, sp.eps, sp.bc1, sp.bc2);
-            pp.w = adam_elem(pp.w, mm.w, vv.w, grad(4 * q + 3), lr, sp.beta1, sp.beta2, sp.eps, sp.bc1, sp.bc2);
-            m4[q] = mm;
-            v4[q] = vv;
-        } else {
-            pp.x = pp.x - lr * grad(4 * q);
-            pp.y = pp.y - lr * grad(4 * q + 1);
-            pp.z = pp.z - lr * grad(4 * q + 2);
-            pp.w = pp.w - lr * grad(4 * q + 3);
+        float pp[4], mm[4], vv[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int e = 4 * q + u;
+            pp[u] = p_s[e];
+            if (sp.use_adam) {
+                mm[u] = m_s[e];
+                vv[u] = v_s[e];
+                pp[u] = adam_elem(pp[u], mm[u], vv[u], grad(e), lr, sp.beta1, sp.beta2, sp.eps, sp.bc1, sp.bc2);
+            } else {
+                pp[u] = pp[u] - lr * grad(e);
+            }
         }
-        p4[q] = pp;
+        reinterpret_cast<float4*>(p_g)[q] = make_float4(pp[0], pp[1], pp[2], pp[3]);
+        if (sp.use_adam) {
+            reinterpret_cast<float4*>(m_g)[q] = make_float4(mm[0], mm[1], mm[2], mm[3]);
+            reinterpret_cast<float4*>(v_g)[q] = make_float4(vv[0], vv[1], vv[2], vv[3]);
+        }
     }
     for (int e = 4 * n4 + threadIdx.x; e < n; e += kBwdG) {
-        float pe = p_s(e);
+        float pe = p_s[e];
         if (sp.use_adam) {
-            float mm = m[e], vv = v[e];
+            float mm = m_s[e], vv = v_s[e];
             pe = adam_elem(pe, mm, vv, grad(e), lr, sp.beta1, sp.beta2, sp.eps, sp.bc1, sp.bc2);
-            m[e] = mm;
-            v[e] = vv;
+            m_g[e] = mm;
+            v_g[e] = vv;
         } else {
             pe = pe - lr * grad(e);
         }
-        p[e] = pe;
+        p_g[e] = pe;
     }
 }
 
-// Preprocess backward (preprocessor_backward_cpu.cpp:8-645), fused with the
-// optimiser update of all parameters (FUSED) or writing GradientOutput.
-template <bool FUSED>
-__global__ void __launch_bounds__(kBwdG, 4) k_preprocess_bwd(const StepParams* __restrict__ spp, int N, ModelPtrs raw,
-                                                          AdamPtrs adam, ScreenPtrs s, RGradPtrs rg, GradPtrs gout,
-                                                          Control* ctrl) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+// Modes of k_preprocess_bwd.
+constexpr int kBwdGrads = 0;   // stage API: write GradientOutput
+constexpr int kBwdFused = 1;   // train step: apply the optimiser in the same kernel
+constexpr int kBwdSplit = 2;   // train step: write GradientOutput for k_optimizer, zero the accumulators
+
+// Preprocess backward (preprocessor_backward_cpu.cpp:8-645) for models whose
+// SH arrays hold MC3 floats per Gaussian, fused with the optimiser update of all
+// parameters or writing GradientOutput (see the modes above).
+template <int MODE, int MC3>
+__global__ void __launch_bounds__(kBwdG, MODE == 1 ? 2 : 4) k_preprocess_bwd(const StepParams* __restrict__ spp, int N,
+                                                             ModelPtrs raw, AdamPtrs adam, ScreenPtrs s,
+                                                             RGradPtrs rg, GradPtrs gout, Control* ctrl) {
+    constexpr bool FUSED = MODE == kBwdFused;
+    constexpr bool TRAIN = MODE != kBwdGrads;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     BwdShared& sm = *reinterpret_cast<BwdShared*>(smem_raw);
     const StepParams& sp = *spp;
     // an overflowed (or timed-out) step, or any step after one the host has not
     // acknowledged yet, updates nothing
-    if (FUSED && ((ctrl->status & (kStatusOverflow | kStatusTimeout)) || sp.persist->sticky_overflow)) return;
+    if (TRAIN && ((ctrl->status & (kStatusOverflow | kStatusTimeout)) || sp.persist->sticky_overflow)) return;
     if (FUSED && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&sp.persist->applied_steps, 1ull);
-    const int g0 = blockIdx.x * kBwdG;
-    const int ng = min(kBwdG, N - g0);
-    const int mc3 = sp.max_coeffs * 3;
     const int tid = threadIdx.x;
+    const size_t g0 = (size_t)blockIdx.x * kBwdG;
+    const int ng = min(kBwdG, N - (int)g0);
+    constexpr int mc3 = MC3;
+    const bool want_mv = FUSED && sp.use_adam;
+    const bool bulk = ng == kBwdG;   // every slice of a full CTA is a multiple of 512 bytes
 
-    // ---- phase 0: coalesced staging ----
-    stage_in(sm.pos, raw.pos + 3 * (size_t)g0, 3 * ng, false);
-    stage_in(sm.sc, raw.sc + 3 * (size_t)g0, 3 * ng, false);
-    stage_in(sm.rot, raw.rot + 4 * (size_t)g0, 4 * ng, false);
-    stage_in(sm.op, raw.op + (size_t)g0, ng, false);
-    stage_in(sm.dm2, rg.dm2 + 2 * (size_t)g0, 2 * ng, FUSED);
-    stage_in(sm.dcon, rg.dcon + 3 * (size_t)g0, 3 * ng, FUSED);
-    stage_in(sm.drgb, rg.drgb + 3 * (size_t)g0, 3 * ng, FUSED);
-    stage_in(sm.dop, rg.dop + (size_t)g0, ng, FUSED);
-    if (tid < ng) sm.radius[tid] = s.radius[g0 + tid];
-    {
-        const float* src = raw.sh + (size_t)mc3 * g0;
-        const int n = mc3 * ng;
-        if ((mc3 & 3) == 0) {
-            const float4* s4 = reinterpret_cast<const float4*>(src);
-#pragma unroll 4
-            for (int qd = tid; qd < (n >> 2); qd += kBwdG) {
-                const float4 v = s4[qd];
-                const int e = 4 * qd;
-                const int gg = e / mc3, j = e - gg * mc3;   // 4 | mc3: the float4 stays in one row
-                float* d = sm.sh + gg * kShPitch + j;
-                d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
-            }
-        } else {
-            for (int e = tid; e < n; e += kBwdG) {
-                const int gg = e / mc3, j = e - gg * mc3;
-                sm.sh[gg * kShPitch + j] = src[e];
+    // ---- phase 0: staging ----
+    if (bulk) {
+        if (tid == 0) {
+            mbar_init(&sm.bar_a, 1);
+            mbar_init(&sm.bar_b, 1);
+            mbar_fence_init();
+        }
+        __syncthreads();
+        if (tid == 0) {
+            const unsigned B = 4u * kBwdG;   // bytes of one float per Gaussian
+            mbar_arrive_expect_tx(&sm.bar_a, B * (11u + (unsigned)mc3 + 9u + 1u));
+            tma_load_1d(sm.pos, raw.pos + 3 * g0, 3 * B, &sm.bar_a);
+            tma_load_1d(sm.sc, raw.sc + 3 * g0, 3 * B, &sm.bar_a);
+            tma_load_1d(sm.rot, raw.rot + 4 * g0, 4 * B, &sm.bar_a);
+            tma_load_1d(sm.op, raw.op + g0, B, &sm.bar_a);
+            tma_load_1d(sm.sh, raw.sh + (size_t)mc3 * g0, (unsigned)mc3 * B, &sm.bar_a);
+            tma_load_1d(sm.dm2, rg.dm2 + 2 * g0, 2 * B, &sm.bar_a);
+            tma_load_1d(sm.dcon, rg.dcon + 3 * g0, 3 * B, &sm.bar_a);
+            tma_load_1d(sm.drgb, rg.drgb + 3 * g0, 3 * B, &sm.bar_a);
+            tma_load_1d(sm.dop, rg.dop + g0, B, &sm.bar_a);
+            tma_load_1d(sm.radius, s.radius + g0, B, &sm.bar_a);
+            if (want_mv) {
+                mbar_arrive_expect_tx(&sm.bar_b, 2u * B * (11u + (unsigned)mc3));
+                tma_load_1d(sm.m_pos, adam.m_pos + 3 * g0, 3 * B, &sm.bar_b);
+                tma_load_1d(sm.v_pos, adam.v_pos + 3 * g0, 3 * B, &sm.bar_b);
+                tma_load_1d(sm.m_sc, adam.m_sc + 3 * g0, 3 * B, &sm.bar_b);
+                tma_load_1d(sm.v_sc, adam.v_sc + 3 * g0, 3 * B, &sm.bar_b);
+                tma_load_1d(sm.m_rot, adam.m_rot + 4 * g0, 4 * B, &sm.bar_b);
+                tma_load_1d(sm.v_rot, adam.v_rot + 4 * g0, 4 * B, &sm.bar_b);
+                tma_load_1d(sm.m_op, adam.m_op + g0, B, &sm.bar_b);
+                tma_load_1d(sm.v_op, adam.v_op + g0, B, &sm.bar_b);
+                tma_load_1d(sm.m_sh, adam.m_sh + (size_t)mc3 * g0, (unsigned)mc3 * B, &sm.bar_b);
+                tma_load_1d(sm.v_sh, adam.v_sh + (size_t)mc3 * g0, (unsigned)mc3 * B, &sm.bar_b);
             }
         }
+        mbar_wait(&sm.bar_a, 0, sp.spin_limit, &ctrl->status);
+    } else {
+        copy_in(sm.pos, raw.pos + 3 * g0, 3 * ng);
+        copy_in(sm.sc, raw.sc + 3 * g0, 3 * ng);
+        copy_in(sm.rot, raw.rot + 4 * g0, 4 * ng);
+        copy_in(sm.op, raw.op + g0, ng);
+        copy_in(sm.sh, raw.sh + (size_t)mc3 * g0, mc3 * ng);
+        copy_in(sm.dm2, rg.dm2 + 2 * g0, 2 * ng);
+        copy_in(sm.dcon, rg.dcon + 3 * g0, 3 * ng);
+        copy_in(sm.drgb, rg.drgb + 3 * g0, 3 * ng);
+        copy_in(sm.dop, rg.dop + g0, ng);
+        for (int e = tid; e < ng; e += kBwdG) sm.radius[e] = s.radius[g0 + e];
+        if (want_mv) {
+            copy_in(sm.m_pos, adam.m_pos + 3 * g0, 3 * ng);
+            copy_in(sm.v_pos, adam.v_pos + 3 * g0, 3 * ng);
+            copy_in(sm.m_sc, adam.m_sc + 3 * g0, 3 * ng);
+            copy_in(sm.v_sc, adam.v_sc + 3 * g0, 3 * ng);
+            copy_in(sm.m_rot, adam.m_rot + 4 * g0, 4 * ng);
+            copy_in(sm.v_rot, adam.v_rot + 4 * g0, 4 * ng);
+            copy_in(sm.m_op, adam.m_op + g0, ng);
+            copy_in(sm.v_op, adam.v_op + g0, ng);
+            copy_in(sm.m_sh, adam.m_sh + (size_t)mc3 * g0, mc3 * ng);
+            copy_in(sm.v_sh, adam.v_sh + (size_t)mc3 * g0, mc3 * ng);
+        }
+        __syncthreads();
     }
-    __syncthreads();
+    if (TRAIN) {
+        // the screen-gradient accumulators start at zero for the next step's raster backward
+        zero_out(rg.dm2 + 2 * g0, 2 * ng);
+        zero_out(rg.dcon + 3 * g0, 3 * ng);
+        zero_out(rg.drgb + 3 * g0, 3 * ng);
+        zero_out(rg.dop + g0, ng);
+    }
 
     // ---- phase 1: per-Gaussian adjoint ----
     BwdOut o;
@@ -1230,6 +1274,18 @@ __global__ void __launch_bounds__(kBwdG, 4) k_preprocess_bwd(const StepParams* _
 #pragma unroll
     for (int k = 0; k < 16; k++) o.basis[k] = 0.f;
     if (tid < ng && sm.radius[tid] > 0) {
+        float shr[kMaxMc3];
+        if (mc3 == kMaxMc3) {
+            const float4* s4 = reinterpret_cast<const float4*>(sm.sh + tid * kMaxMc3);
+#pragma unroll
+            for (int q = 0; q < kMaxMc3 / 4; q++) {
+                const float4 v = s4[q];
+                shr[4 * q] = v.x; shr[4 * q + 1] = v.y; shr[4 * q + 2] = v.z; shr[4 * q + 3] = v.w;
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < kMaxMc3; k++) shr[k] = k < mc3 ? sm.sh[tid * mc3 + k] : 0.0f;
+        }
         BwdIn in;
 #pragma unroll
         for (int k = 0; k < 3; k++) {
@@ -1244,7 +1300,7 @@ __global__ void __launch_bounds__(kBwdG, 4) k_preprocess_bwd(const StepParams* _
         in.dm[0] = sm.dm2[2 * tid];
         in.dm[1] = sm.dm2[2 * tid + 1];
         in.dop = sm.dop[tid];
-        in.sh = sm.sh + tid * kShPitch;
+        in.sh = shr;
         backward_one(sp, in, o);
     }
     if (tid < ng) {
@@ -1266,49 +1322,77 @@ __global__ void __launch_bounds__(kBwdG, 4) k_preprocess_bwd(const StepParams* _
     auto sh_grad = [&](int e) {
         const int gg = e / mc3, j = e - gg * mc3;
         const int k = j / 3, c = j - 3 * k;
-        return k < 16 ? sm.basis[gg * kBasisPitch + k] * sm.geff[3 * gg + c] : 0.0f;
+        return sm.basis[gg * kBasisPitch + k] * sm.geff[3 * gg + c];
     };
     if (FUSED) {
-        update_slice(sp, raw.pos + 3 * (size_t)g0, adam.m_pos + 3 * (size_t)g0, adam.v_pos + 3 * (size_t)g0,
-                     3 * ng, sp.lr_pos, [&](int e) { return sm.gpos[e]; }, [&](int e) { return sm.pos[e]; });
-        update_slice(sp, raw.sc + 3 * (size_t)g0, adam.m_sc + 3 * (size_t)g0, adam.v_sc + 3 * (size_t)g0,
-                     3 * ng, sp.lr_scale, [&](int e) { return sm.gsc[e]; }, [&](int e) { return sm.sc[e]; });
-        update_slice(sp, raw.rot + 4 * (size_t)g0, adam.m_rot + 4 * (size_t)g0, adam.v_rot + 4 * (size_t)g0,
-                     4 * ng, sp.lr_rot, [&](int e) { return sm.grot[e]; }, [&](int e) { return sm.rot[e]; });
-        update_slice(sp, raw.op + (size_t)g0, adam.m_op + (size_t)g0, adam.v_op + (size_t)g0, ng,
-                     sp.lr_opac, [&](int e) { return sm.gop[e]; }, [&](int e) { return sm.op[e]; });
+        if (bulk && want_mv) mbar_wait(&sm.bar_b, 0, sp.spin_limit, &ctrl->status);
+        update_slice(sp, raw.pos + 3 * g0, adam.m_pos + 3 * g0, adam.v_pos + 3 * g0, sm.pos, sm.m_pos, sm.v_pos,
+                     3 * ng, sp.lr_pos, [&](int e) { return sm.gpos[e]; });
+        update_slice(sp, raw.sc + 3 * g0, adam.m_sc + 3 * g0, adam.v_sc + 3 * g0, sm.sc, sm.m_sc, sm.v_sc, 3 * ng,
+                     sp.lr_scale, [&](int e) { return sm.gsc[e]; });
+        update_slice(sp, raw.rot + 4 * g0, adam.m_rot + 4 * g0, adam.v_rot + 4 * g0, sm.rot, sm.m_rot, sm.v_rot,
+                     4 * ng, sp.lr_rot, [&](int e) { return sm.grot[e]; });
+        update_slice(sp, raw.op + g0, adam.m_op + g0, adam.v_op + g0, sm.op, sm.m_op, sm.v_op, ng, sp.lr_opac,
+                     [&](int e) { return sm.gop[e]; });
         update_slice(sp, raw.sh + (size_t)mc3 * g0, adam.m_sh + (size_t)mc3 * g0, adam.v_sh + (size_t)mc3 * g0,
-                     mc3 * ng, sp.lr_sh, sh_grad, [&](int e) {
-                         const int gg = e / mc3;
-                         return sm.sh[gg * kShPitch + (e - gg * mc3)];
-                     });
+                     sm.sh, sm.m_sh, sm.v_sh, mc3 * ng, sp.lr_sh, sh_grad);
     } else {
         for (int e = tid; e < 3 * ng; e += kBwdG) {
-            gout.g_pos[3 * (size_t)g0 + e] = sm.gpos[e];
-            gout.g_sc[3 * (size_t)g0 + e] = sm.gsc[e];
+            gout.g_pos[3 * g0 + e] = sm.gpos[e];
+            gout.g_sc[3 * g0 + e] = sm.gsc[e];
         }
-        for (int e = tid; e < 4 * ng; e += kBwdG) gout.g_rot[4 * (size_t)g0 + e] = sm.grot[e];
-        for (int e = tid; e < ng; e += kBwdG) gout.g_op[(size_t)g0 + e] = sm.gop[e];
+        for (int e = tid; e < 4 * ng; e += kBwdG) gout.g_rot[4 * g0 + e] = sm.grot[e];
+        for (int e = tid; e < ng; e += kBwdG) gout.g_op[g0 + e] = sm.gop[e];
         for (int e = tid; e < mc3 * ng; e += kBwdG) gout.g_sh[(size_t)mc3 * g0 + e] = sh_grad(e);
     }
 }
 
-// Stand-alone optimiser step over gradient arrays (optimizer.cpp:9-101).
-__global__ void k_optimizer(const StepParams* __restrict__ spp, long long n_pos, long long n_rot, long long n_sh,
-                            long long n_op, ModelPtrs raw, AdamPtrs adam, GradPtrs g) {
-    const StepParams& sp = *spp;
+// Optimiser over one parameter array: element-wise Adam / SGD (optimizer.cpp:9-43)
+// with float4 loads and stores.
+__device__ __forceinline__ void update_array(const StepParams& sp, float* __restrict__ p, float* __restrict__ m,
+                                             float* __restrict__ v, const float* __restrict__ g, long long n,
+                                             float lr) {
     const long long stride = (long long)gridDim.x * blockDim.x;
-    if (blockIdx.x == 0 && threadIdx.x == 0 && sp.use_adam) atomicAdd(&sp.persist->applied_steps, 1ull);
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n_pos; i += stride) {
-        apply_update(sp, &raw.pos[i], &adam.m_pos[i], &adam.v_pos[i], g.g_pos[i], sp.lr_pos);
-        apply_update(sp, &raw.sc[i], &adam.m_sc[i], &adam.v_sc[i], g.g_sc[i], sp.lr_scale);
+    const long long n4 = n >> 2;
+    float4* p4 = reinterpret_cast<float4*>(p);
+    float4* m4 = reinterpret_cast<float4*>(m);
+    float4* v4 = reinterpret_cast<float4*>(v);
+    const float4* g4 = reinterpret_cast<const float4*>(g);
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n4; q += stride) {
+        float4 pp = p4[q];
+        const float4 gg = g4[q];
+        if (sp.use_adam) {
+            float4 mm = m4[q], vv = v4[q];
+            pp.x = adam_elem(pp.x, mm.x, vv.x, gg.x, lr, sp.beta1, sp.beta2, sp.eps, sp.bc1, sp.bc2);
+            pp.y = adam_elem(pp.y, mm.y, vv.y, gg.y, lr, sp.beta1, sp.beta2, sp.eps, sp.bc1, sp.bc2);
+            pp.z = adam_elem(pp.z, mm.z, vv.z, gg.z, lr, sp.beta1, sp.beta2, sp.eps, sp.bc1, sp.bc2);
+            pp.w = adam_elem(pp.w, mm.w, vv.w, gg.w, lr, sp.beta1, sp.beta2, sp.eps, sp.bc1, sp.bc2);
+            m4[q] = mm;
+            v4[q] = vv;
+        } else {
+            pp.x = pp.x - lr * gg.x;
+            pp.y = pp.y - lr * gg.y;
+            pp.z = pp.z - lr * gg.z;
+            pp.w = pp.w - lr * gg.w;
+        }
+        p4[q] = pp;
     }
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n_rot; i += stride)
-        apply_update(sp, &raw.rot[i], &adam.m_rot[i], &adam.v_rot[i], g.g_rot[i], sp.lr_rot);
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n_sh; i += stride)
-        apply_update(sp, &raw.sh[i], &adam.m_sh[i], &adam.v_sh[i], g.g_sh[i], sp.lr_sh);
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n_op; i += stride)
-        apply_update(sp, &raw.op[i], &adam.m_op[i], &adam.v_op[i], g.g_op[i], sp.lr_opac);
+    for (long long i = 4 * n4 + (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        apply_update(sp, &p[i], &m[i], &v[i], g[i], lr);
+}
+
+// Stand-alone optimiser step over the gradient arrays (optimizer.cpp:9-101).
+// With ctrl (the split train step) an overflowed or unacknowledged step updates nothing.
+__global__ void __launch_bounds__(256) k_optimizer(const StepParams* __restrict__ spp, long long n, int mc3,
+                                                   ModelPtrs raw, AdamPtrs adam, GradPtrs g, const Control* ctrl) {
+    const StepParams& sp = *spp;
+    if (ctrl && ((ctrl->status & (kStatusOverflow | kStatusTimeout)) || sp.persist->sticky_overflow)) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0 && sp.use_adam) atomicAdd(&sp.persist->applied_steps, 1ull);
+    update_array(sp, raw.sh, adam.m_sh, adam.v_sh, g.g_sh, n * mc3, sp.lr_sh);
+    update_array(sp, raw.pos, adam.m_pos, adam.v_pos, g.g_pos, 3 * n, sp.lr_pos);
+    update_array(sp, raw.sc, adam.m_sc, adam.v_sc, g.g_sc, 3 * n, sp.lr_scale);
+    update_array(sp, raw.rot, adam.m_rot, adam.v_rot, g.g_rot, 4 * n, sp.lr_rot);
+    update_array(sp, raw.op, adam.m_op, adam.v_op, g.g_op, n, sp.lr_opac);
 }
 
 inline int blocks_for(long long n, int t) { return (int)((n + t - 1) / t); }
@@ -1360,30 +1444,51 @@ cudaError_t launch_raster_bwd_plain(cudaStream_t st, const StepParams* sp, int n
     return cudaGetLastError();
 }
 
-cudaError_t launch_preprocess_bwd_plain(cudaStream_t st, const StepParams* sp, int N, bool fused_adam,
-                                        ModelPtrs raw, AdamPtrs adam, ScreenPtrs s, RGradPtrs rg, GradPtrs gout,
-                                        Control* ctrl) {
-    if (N <= 0) return cudaSuccess;
-    const int grid = blocks_for(N, kBwdG);
-    const int smem = (int)sizeof(BwdShared);
+namespace {
+template <int MODE, int MC3>
+cudaError_t launch_bwd_mc(cudaStream_t st, const StepParams* sp, int N, ModelPtrs raw, AdamPtrs adam, ScreenPtrs s,
+                          RGradPtrs rg, GradPtrs gout, Control* ctrl) {
+    const int smem = MODE == kBwdFused ? (int)sizeof(BwdShared) : (int)offsetof(BwdShared, m_sh);
     static bool attr_set = false;
     if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(k_preprocess_bwd<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(k_preprocess_bwd<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaError_t e =
+            cudaFuncSetAttribute(k_preprocess_bwd<MODE, MC3>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e != cudaSuccess) return e;
         attr_set = true;
     }
-    if (fused_adam) k_preprocess_bwd<true><<<grid, kBwdG, smem, st>>>(sp, N, raw, adam, s, rg, gout, ctrl);
-    else k_preprocess_bwd<false><<<grid, kBwdG, smem, st>>>(sp, N, raw, adam, s, rg, gout, ctrl);
+    k_preprocess_bwd<MODE, MC3><<<blocks_for(N, kBwdG), kBwdG, smem, st>>>(sp, N, raw, adam, s, rg, gout, ctrl);
     return cudaGetLastError();
 }
 
-cudaError_t launch_optimizer_plain(cudaStream_t st, const StepParams* sp, int N, int mc3, ModelPtrs raw,
-                                   AdamPtrs adam, GradPtrs g) {
+template <int MODE>
+cudaError_t launch_bwd_mode(cudaStream_t st, const StepParams* sp, int N, int mc3, ModelPtrs raw, AdamPtrs adam,
+                            ScreenPtrs s, RGradPtrs rg, GradPtrs gout, Control* ctrl) {
+    switch (mc3) {
+        case 3: return launch_bwd_mc<MODE, 3>(st, sp, N, raw, adam, s, rg, gout, ctrl);
+        case 12: return launch_bwd_mc<MODE, 12>(st, sp, N, raw, adam, s, rg, gout, ctrl);
+        case 27: return launch_bwd_mc<MODE, 27>(st, sp, N, raw, adam, s, rg, gout, ctrl);
+        case 48: return launch_bwd_mc<MODE, 48>(st, sp, N, raw, adam, s, rg, gout, ctrl);
+        default: return cudaErrorInvalidValue;
+    }
+}
+}  // namespace
+
+cudaError_t launch_preprocess_bwd_plain(cudaStream_t st, const StepParams* sp, int N, int mc3, int mode,
+                                        ModelPtrs raw, AdamPtrs adam, ScreenPtrs s, RGradPtrs rg, GradPtrs gout,
+                                        Control* ctrl) {
     if (N <= 0) return cudaSuccess;
-    const long long n_sh = (long long)N * mc3;
-    k_optimizer<<<4 * 148, 256, 0, st>>>(sp, 3LL * N, 4LL * N, n_sh, (long long)N, raw, adam, g);
+    switch (mode) {
+        case kBwdGrads: return launch_bwd_mode<kBwdGrads>(st, sp, N, mc3, raw, adam, s, rg, gout, ctrl);
+        case kBwdFused: return launch_bwd_mode<kBwdFused>(st, sp, N, mc3, raw, adam, s, rg, gout, ctrl);
+        case kBwdSplit: return launch_bwd_mode<kBwdSplit>(st, sp, N, mc3, raw, adam, s, rg, gout, ctrl);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_optimizer_plain(cudaStream_t st, const StepParams* sp, int N, int mc3, ModelPtrs raw,
+                                   AdamPtrs adam, GradPtrs g, const Control* ctrl) {
+    if (N <= 0) return cudaSuccess;
+    k_optimizer<<<8 * 148, 256, 0, st>>>(sp, (long long)N, mc3, raw, adam, g, ctrl);
     return cudaGetLastError();
 }
 

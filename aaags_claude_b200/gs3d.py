@@ -22,7 +22,7 @@ LIB_PATH = os.path.join(PKG, "libgs3d_cuda.so")
 
 OK = 0
 ERR_INVALID_ARG, ERR_CUDA, ERR_PAIR_OVERFLOW, ERR_DEVICE_TIMEOUT, ERR_NO_MODEL, ERR_OOM, ERR_STATE = range(1, 8)
-OPT_PAIR_CAPACITY, OPT_USE_GRAPH, OPT_FORM, OPT_SPIN_LIMIT, OPT_STAGE_TIMING = 1, 2, 3, 4, 5
+OPT_PAIR_CAPACITY, OPT_USE_GRAPH, OPT_FORM, OPT_SPIN_LIMIT, OPT_STAGE_TIMING, OPT_FUSED_ADAM = 1, 2, 3, 4, 5, 6
 NUM_STAGES = 8
 STAT_TOTAL_PAIRS, STAT_PAIR_CAPACITY, STAT_KERNELS_LAST, STAT_SORT_PASSES, STAT_GRAPH_REPLAYS, STAT_ADAM_STEP = range(1, 7)
 FORM_PLAIN_FP32 = 0

@@ -54,6 +54,7 @@ def _args(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the timed reference CPU step")
     ap.add_argument("--gaussians", type=int, default=1_000_000, help="scene size (profiling cases use less)")
     ap.add_argument("--size", default="1920x1080", help="WxH of the camera")
+    ap.add_argument("--fused-adam", type=int, default=None, help="1: optimiser fused into the backward kernel")
     return ap.parse_args(argv)
 
 
@@ -218,6 +219,8 @@ def run_ours(a) -> int:
     cam = w.cameras[0]
     W, H = cam.width, cam.height
     ctx = gs3d.Context(local)
+    if a.fused_adam is not None:
+        ctx.set_option(gs3d.OPT_FUSED_ADAM, a.fused_adam)
     # target image: the perturbed scene rendered by this library (setup, untimed)
     ctx.set_raw_params(w.target_scene)
     gt = ctx.render(cam, S.render_config(False))

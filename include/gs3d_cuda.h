@@ -44,6 +44,7 @@ typedef struct gs3dc_ctx gs3dc_ctx;
 #define GS3DC_OPT_FORM           3  /* GS3DC_FORM_* precision form of gs3dc_train_step / gs3dc_render */
 #define GS3DC_OPT_SPIN_LIMIT     4  /* iterations before a device-side wait gives up (test hook) */
 #define GS3DC_OPT_STAGE_TIMING   5  /* 1: train steps run un-captured with CUDA events between stages */
+#define GS3DC_OPT_FUSED_ADAM     6  /* 1: optimiser fused into the preprocess backward; 0 (default): split */
 
 #define GS3DC_FORM_PLAIN_FP32    0  /* FP32 everywhere, no FMA contraction: parity form */
 
