@@ -20,6 +20,8 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(PKG, "csrc")
 BUILD = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libgs3d_cuda.so")
+HOST = os.path.join(PKG, "host")
+DEMO = os.path.join(BUILD, "stages_demo")
 INCLUDE = os.path.join(os.path.dirname(PKG), "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -60,6 +62,15 @@ def build(force: bool = False, verbose: bool = False) -> str:
             subprocess.run(cmd, check=True)
     if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < _newest(objs):
         cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-Xcompiler", "-fPIC"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    # C++ stage adapters (host/) and the driver the adapter tests run
+    host_srcs = [os.path.join(HOST, "gs3d_stages_cuda.cpp"), os.path.join(HOST, "stages_demo.cpp")]
+    deps = host_srcs + glob.glob(os.path.join(HOST, "*.hpp")) + [LIB]
+    if force or not os.path.exists(DEMO) or os.path.getmtime(DEMO) < _newest(deps):
+        cmd = [os.environ.get("CXX", "g++"), "-O2", "-std=c++17", "-Wall", f"-I{INCLUDE}", f"-I{HOST}",
+               *host_srcs, "-o", DEMO, f"-L{PKG}", "-lgs3d_cuda", "-Wl,-rpath,$ORIGIN/.."]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

@@ -85,6 +85,7 @@ struct gs3dc_ctx {
     DevBuf<unsigned> ranges;
     DevBuf<unsigned> tile_order;   // heavy-first permutation of the tiles
     DevBuf<float> image, T_final, d_image, gt;
+    DevBuf<float> raw_rot_tmp;   // raw quaternions for the backward of an activated model
     DevBuf<int> n_contrib;
     DevBuf<unsigned> last_j;
     DevBuf<unsigned char> dsign;
@@ -301,7 +302,7 @@ int ensure_pairs(gs3dc_ctx* c, unsigned long long cap, int num_tiles) {
 
 // Fills the next pinned parameter slot and queues its copy to the device.
 int push_params(gs3dc_ctx* c, const gs3d_camera* cam, const gs3d_render_config* cfg, const gs3d_train_config* tc,
-                int iteration, const float* gt_dev) {
+                int iteration, const float* gt_dev, const float* raw_rot_dev = nullptr) {
     const int slot = c->sp_slot;
     c->sp_slot = (c->sp_slot + 1) % kParamSlots;
     CK(cudaEventSynchronize(c->sp_event[slot]));  // the slot's previous copy has been consumed
@@ -326,6 +327,7 @@ int push_params(gs3dc_ctx* c, const gs3d_camera* cam, const gs3d_render_config* 
     p.sort_bits = 32 + bit_length(p.num_tiles > 1 ? (unsigned)(p.num_tiles - 1) : 0u);
     p.gt = gt_dev;
     p.persist = c->persist;
+    p.raw_rot = raw_rot_dev;
     if (tc) {
         p.use_adam = tc->use_adam ? 1 : 0;
         // lr_schedule, train_types.cpp:64-68
@@ -585,6 +587,7 @@ void gs3dc_destroy(gs3dc_ctx* c) {
         c->vals[b].release();
     }
     c->sort_desc.release();
+    c->raw_rot_tmp.release();
     c->ctrl_region.release();
     c->ranges.release();
     c->tile_order.release();
@@ -674,6 +677,36 @@ int gs3dc_set_raw_params(gs3dc_ctx* c, const gs3d_raw_params* r) {
     c->model_raw = true;
     if ((rc = ensure_adam(c))) return rc;
     if ((rc = zero_adam(c))) return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    return GS3DC_OK;
+}
+
+int gs3dc_update_raw_params(gs3dc_ctx* c, const gs3d_raw_params* r) {
+    if (!c || !r) return GS3DC_ERR_INVALID_ARG;
+    int rc = require_model(c);
+    if (rc) return rc;
+    if (!c->model_raw) return fail(c, GS3DC_ERR_STATE, "the device model is an activated render model");
+    if (r->count != c->N || r->max_coeffs != c->max_coeffs || r->sh_degree != c->sh_degree)
+        return fail(c, GS3DC_ERR_INVALID_ARG, "update needs the uploaded shape (N=%d, mc=%d)", c->N, c->max_coeffs);
+    CK(cudaSetDevice(c->device));
+    const size_t n = (size_t)c->N;
+    if (n) {
+        CK(cudaMemcpyAsync(c->pos.p, r->raw_positions, 3 * n * 4, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(c->sc.p, r->raw_scales, 3 * n * 4, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(c->rot.p, r->raw_rotations, 4 * n * 4, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(c->sh.p, r->raw_sh_coeffs, 3 * n * c->max_coeffs * 4, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(c->op.p, r->raw_opacities, n * 4, cudaMemcpyHostToDevice, c->stream));
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    c->have_screen = c->have_pairs = c->have_sorted = c->have_raster = c->have_rgrad = c->have_grads = false;
+    return GS3DC_OK;
+}
+
+int gs3dc_get_image(gs3dc_ctx* c, float* image) {
+    if (!c || !image) return GS3DC_ERR_INVALID_ARG;
+    if (c->W <= 0 || !c->image.p) return fail(c, GS3DC_ERR_STATE, "nothing has been rendered");
+    CK(cudaSetDevice(c->device));
+    CK(cudaMemcpyAsync(image, c->image.p, (size_t)c->W * c->H * 3 * 4, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     return GS3DC_OK;
 }
@@ -911,21 +944,25 @@ int gs3dc_raster_backward(gs3dc_ctx* c, const gs3d_camera* cam, const gs3d_rende
 }
 
 int gs3dc_preprocess_backward(gs3dc_ctx* c, const gs3d_camera* cam, const gs3d_render_config* cfg,
-                              float* d_raw_positions, float* d_raw_scales, float* d_raw_rotations,
-                              float* d_raw_sh_coeffs, float* d_raw_opacities) {
+                              const float* raw_rotations, float* d_raw_positions, float* d_raw_scales,
+                              float* d_raw_rotations, float* d_raw_sh_coeffs, float* d_raw_opacities) {
     if (!c) return GS3DC_ERR_INVALID_ARG;
     int rc;
     if ((rc = check_config(c, cam, cfg))) return rc;
     if (!c->have_rgrad) return fail(c, GS3DC_ERR_STATE, "gs3dc_preprocess_backward needs gs3dc_raster_backward");
-    if (!c->model_raw) return fail(c, GS3DC_ERR_STATE, "gradients are taken w.r.t. a raw model (gs3dc_set_raw_params)");
+    if (!c->model_raw && !raw_rotations)
+        return fail(c, GS3DC_ERR_INVALID_ARG, "an activated device model needs the raw rotations");
     CK(cudaSetDevice(c->device));
-    const size_t n = (size_t)c->N, mc3 = (size_t)c->max_coeffs * 3;
-    CK(c->g_pos.ensure(3 * n));
-    CK(c->g_sc.ensure(3 * n));
-    CK(c->g_rot.ensure(4 * n));
-    CK(c->g_sh.ensure(mc3 * n));
-    CK(c->g_op.ensure(n));
-    if ((rc = push_params(c, cam, cfg, nullptr, 0, nullptr))) return rc;
+    const size_t n = (size_t)c->N;
+    if ((rc = ensure_grads(c))) return rc;
+    const float* raw_rot_dev = nullptr;
+    if (!c->model_raw) {
+        CK(c->raw_rot_tmp.ensure(4 * n));
+        CK(cudaMemcpyAsync(c->raw_rot_tmp.p, raw_rotations, 4 * n * 4, cudaMemcpyHostToDevice, c->stream));
+        raw_rot_dev = c->raw_rot_tmp.p;
+    }
+    const size_t mc3 = (size_t)c->max_coeffs * 3;
+    if ((rc = push_params(c, cam, cfg, nullptr, 0, nullptr, raw_rot_dev))) return rc;
     CK(launch_preprocess_bwd_plain(c->stream, c->sp_dev, c->N, c->max_coeffs * 3, 0, model_ptrs(c), adam_ptrs(c),
                                    screen_ptrs(c, false), rgrad_ptrs(c), grad_ptrs(c), c->ctrl));
     if ((rc = download(c, d_raw_positions, c->g_pos.p, 3 * n * 4)) ||

@@ -833,6 +833,7 @@ __device__ __forceinline__ void apply_update(const StepParams& sp, float* p, flo
 // Inputs of one Gaussian's backward: raw parameters and its screen-space gradients.
 struct BwdIn {
     float p[3], rsc[3], rq[4], rop;
+    const float* act;  // non-NULL: activated (scale[3], rot[4], opacity) of an activated model; rq stays raw
     const float* sh;   // this Gaussian's SH coefficients, basis-major with stride 3
     float dm[2], dcn[3], drgb[3], dop;
 };
@@ -851,7 +852,15 @@ __device__ __forceinline__ void backward_one(const StepParams& sp, const BwdIn& 
     const float* shp = in.sh;
     const float* p = in.p;
     float sc[3], q[4], op;
-    activate_one(in.rsc, in.rq, in.rop, sc, q, &op);
+    if (in.act) {
+#pragma unroll
+        for (int k = 0; k < 3; k++) sc[k] = in.act[k];
+#pragma unroll
+        for (int k = 0; k < 4; k++) q[k] = in.act[3 + k];
+        op = in.act[7];
+    } else {
+        activate_one(in.rsc, in.rq, in.rop, sc, q, &op);
+    }
     const int deg = sp.sh_deg_model;
     // ---- chain 2: SH (:8-203) ----
     float d[3];
@@ -1297,6 +1306,19 @@ __global__ void __launch_bounds__(kBwdG, MODE == 1 ? 2 : 4) k_preprocess_bwd(con
 #pragma unroll
         for (int k = 0; k < 4; k++) in.rq[k] = sm.rot[4 * tid + k];
         in.rop = sm.op[tid];
+        in.act = nullptr;
+        float act[8];
+        if (MODE == kBwdGrads && sp.raw_rot) {
+            // activated device model (stage API): its values are the activation, raw_rot the raw quaternion
+#pragma unroll
+            for (int k = 0; k < 3; k++) act[k] = sm.sc[3 * tid + k];
+#pragma unroll
+            for (int k = 0; k < 4; k++) act[3 + k] = sm.rot[4 * tid + k];
+            act[7] = sm.op[tid];
+#pragma unroll
+            for (int k = 0; k < 4; k++) in.rq[k] = sp.raw_rot[4 * (g0 + tid) + k];
+            in.act = act;
+        }
         in.dm[0] = sm.dm2[2 * tid];
         in.dm[1] = sm.dm2[2 * tid + 1];
         in.dop = sm.dop[tid];

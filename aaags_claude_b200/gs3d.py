@@ -75,7 +75,9 @@ def load_library(path: str = LIB_PATH):
         "gs3dc_rasterize": ([vp, vp, vp, vp, vp, vp], ctypes.c_int),
         "gs3dc_render": ([vp, vp, vp, vp, vp], ctypes.c_int),
         "gs3dc_raster_backward": ([vp, vp, vp, vp, vp, vp, vp, vp], ctypes.c_int),
-        "gs3dc_preprocess_backward": ([vp, vp, vp, vp, vp, vp, vp, vp], ctypes.c_int),
+        "gs3dc_preprocess_backward": ([vp, vp, vp, vp, vp, vp, vp, vp, vp], ctypes.c_int),
+        "gs3dc_update_raw_params": ([vp, vp], ctypes.c_int),
+        "gs3dc_get_image": ([vp, vp], ctypes.c_int),
         "gs3dc_optimizer_step": ([vp, vp, ctypes.c_int], ctypes.c_int),
         "gs3dc_train_step": ([vp, vp, vp, ctypes.c_int, vp, vp, ctypes.c_int, vp], ctypes.c_int),
         "gs3dc_synchronize": ([vp], ctypes.c_int),
@@ -273,14 +275,25 @@ class Context:
                                                _p(out["d_conics"]), _p(out["d_rgb"]), _p(out["d_opac"])))
         return out
 
-    def preprocess_backward(self, cam, cfg) -> dict:
+    def preprocess_backward(self, cam, cfg, raw_rotations: np.ndarray | None = None) -> dict:
+        """PreprocessorBackward; raw_rotations is needed when the device model is activated."""
         n, mc = self._model[1], self._model[2]
         out = dict(g_pos=np.zeros(3 * n, np.float32), g_sc=np.zeros(3 * n, np.float32),
                    g_rot=np.zeros(4 * n, np.float32), g_sh=np.zeros(3 * mc * n, np.float32),
                    g_op=np.zeros(n, np.float32))
-        self._chk(self.L.gs3dc_preprocess_backward(self.h, _ref(cam), _ref(cfg), *[_p(out[k]) for k in
+        rr = None if raw_rotations is None else np.ascontiguousarray(raw_rotations, np.float32).reshape(-1)
+        self._chk(self.L.gs3dc_preprocess_backward(self.h, _ref(cam), _ref(cfg), _p(rr), *[_p(out[k]) for k in
                                                    ("g_pos", "g_sc", "g_rot", "g_sh", "g_op")]))
         return out
+
+    def update_raw_params(self, scene: S.Scene):
+        r = scene.raw_struct()
+        self._chk(self.L.gs3dc_update_raw_params(self.h, _ref(r)))
+
+    def get_image(self, cam) -> np.ndarray:
+        img = np.zeros(3 * cam.width * cam.height, np.float32)
+        self._chk(self.L.gs3dc_get_image(self.h, _p(img)))
+        return img
 
     def optimizer_step(self, tcfg, iteration: int):
         self._chk(self.L.gs3dc_optimizer_step(self.h, _ref(tcfg), int(iteration)))

@@ -94,6 +94,14 @@ int gs3dc_get_stat(gs3dc_ctx* ctx, int stat, int64_t* value);
 int gs3dc_set_gaussians(gs3dc_ctx* ctx, const gs3d_gaussians* g);
 int gs3dc_set_raw_params(gs3dc_ctx* ctx, const gs3d_raw_params* raw);
 int gs3dc_get_raw_params(gs3dc_ctx* ctx, gs3d_raw_params* raw);
+/* New values for the uploaded raw model (same count / max_coeffs), Adam state
+ * kept: the host side of Trainer::step, which reads the caller's parameters on
+ * every call (src/trainer.cpp:26-36) while AdamOptimizer keeps its moments
+ * unless N changes (src/optimizer.cpp:64-66). */
+int gs3dc_update_raw_params(gs3dc_ctx* ctx, const gs3d_raw_params* raw);
+/* The H*W*3 image of the last rasterize / render / train step
+ * (Trainer::last_rendered, include/trainer.h:32). */
+int gs3dc_get_image(gs3dc_ctx* ctx, float* image);
 
 /* ---- forward stages ----
  * Preprocessor::process (include/preprocessor.h:7-12; CPU src/cpu/preprocessor_cpu.cpp:11-268).
@@ -148,11 +156,15 @@ int gs3dc_raster_backward(gs3dc_ctx* ctx, const gs3d_camera* cam, const gs3d_ren
                           float* d_opacities_2d);
 
 /* PreprocessorBackwardCPU::backward (src/cpu/preprocessor_backward_cpu.h:7-10;
- *   src/cpu/preprocessor_backward_cpu.cpp:205-645) of the raw model from the
- *   last raster backward.  Outputs GradientOutput (include/train_types.h:35-43). */
+ *   src/cpu/preprocessor_backward_cpu.cpp:205-645) from the last raster
+ *   backward.  With a raw device model the activation is recomputed; with an
+ *   activated one (gs3dc_set_gaussians, as a PreprocessorCUDA forward leaves it)
+ *   raw_rotations (host, N*4) supplies the unnormalised quaternions the
+ *   normalisation backward needs.  Outputs GradientOutput
+ *   (include/train_types.h:35-43), any may be NULL. */
 int gs3dc_preprocess_backward(gs3dc_ctx* ctx, const gs3d_camera* cam,
-                              const gs3d_render_config* cfg, float* d_raw_positions,
-                              float* d_raw_scales, float* d_raw_rotations,
+                              const gs3d_render_config* cfg, const float* raw_rotations,
+                              float* d_raw_positions, float* d_raw_scales, float* d_raw_rotations,
                               float* d_raw_sh_coeffs, float* d_raw_opacities);
 
 /* AdamOptimizer::step / SGDOptimizer::step (src/optimizer.cpp:9-101) with the

@@ -173,3 +173,17 @@ def test_batched_camera_set_matches_the_config():
     for c in w.cameras:
         assert abs(np.linalg.norm(np.array(c.cam_pos)) - 3.0) < 1e-5
         assert np.tan(np.radians(22.5)) - 1e-6 <= c.tan_fovy <= np.tan(np.radians(37.5)) + 1e-6
+
+
+def test_stage_adapters_compile_as_a_drop_in():
+    """The C++ adapters derive from the reference's own stage interfaces: they
+    compile against its headers (-DGS3D_WITH_REFERENCE_HEADERS) and against the
+    restated ones used outside the reference tree."""
+    host = os.path.join(ROOT, "aaags_claude_b200", "host")
+    src = os.path.join(host, "gs3d_stages_cuda.cpp")
+    subprocess.run(["g++", "-std=c++17", "-Wall", "-Werror", "-fsyntax-only", "-I", os.path.join(ROOT, "include"),
+                    "-I", host, src], check=True)
+    if os.path.isdir(REF_INCLUDE):
+        subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-DGS3D_WITH_REFERENCE_HEADERS", "-I",
+                        os.path.join(ROOT, "include"), "-I", host, "-I", REF_INCLUDE, "-I",
+                        "/root/reference/harmonyos_3dgs/src", src], check=True)
