@@ -83,6 +83,8 @@ def load_library(path: str = LIB_PATH):
         "gs3dc_synchronize": ([vp], ctypes.c_int),
         "gs3dc_get_stage_times": ([vp, ctypes.POINTER(ctypes.c_float), ctypes.c_int], ctypes.c_int),
         "gs3dc_selftest_bounded_wait": ([vp, ctypes.c_uint32], ctypes.c_int),
+        "gs3dc_sort_pairs_static": ([i64, vp, vp, ctypes.c_int, vp, vp, vp, vp, ctypes.c_char_p, ctypes.c_size_t],
+                                    ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)

@@ -134,6 +134,26 @@ int gs3dc_sort_pairs(gs3dc_ctx* ctx, int64_t total_pairs, const uint64_t* keys,
                      const uint32_t* values, int num_tiles, uint64_t* keys_sorted,
                      uint32_t* values_sorted, uint32_t* tile_ranges);
 
+/* gs3dc_sort_pairs without any device-memory allocation: no counterpart in the
+ * reference.  For callers that must not allocate on their path -- code holding
+ * no gs3dc context (creating one allocates), frame loops under a fixed
+ * device-memory budget, callers that cannot take the device-wide
+ * synchronisation of cudaMalloc / cudaFree.
+ *   keys, values, keys_sorted, values_sorted (total_pairs entries) and
+ *   tile_ranges (2*num_tiles entries) are device memory of the current device;
+ *   the inputs are left unchanged (or may be the same buffers as the outputs).
+ *   The scratch is one static device array of about 16 MiB per device, so
+ *   total_pairs may not exceed GS3DC_STATIC_SORT_MAX_PAIRS
+ *   (GS3DC_ERR_INVALID_ARG otherwise).  All calls on a device share it: calls
+ *   that overlap on the GPU race.  The first call on each device looks up the
+ *   scratch address; make it before any stream capture.  Runs on `stream`
+ *   (a cudaStream_t, NULL = default stream) and returns once the sort is done.
+ *   err (may be NULL) receives a message of at most err_len bytes on failure. */
+#define GS3DC_STATIC_SORT_MAX_PAIRS 1048576
+int gs3dc_sort_pairs_static(int64_t total_pairs, const uint64_t* keys, const uint32_t* values,
+                            int num_tiles, uint64_t* keys_sorted, uint32_t* values_sorted,
+                            uint32_t* tile_ranges, void* stream, char* err, size_t err_len);
+
 /* Rasterizer::rasterize (include/rasterizer.h:7-15; src/cpu/rasterizer_cpu.cpp:38-198).
  *   Front-to-back blend of the sorted pairs.  image is H*W*3 HWC; T_final and
  *   n_contrib (ForwardCache, include/types.h:98-99) may be NULL. */
