@@ -75,6 +75,12 @@ struct gs3dc_ctx {
     DevBuf<unsigned long long> sort_desc;
     unsigned long long sort_desc_stride = 0;
     int sort_passes = 0, sort_num_tiles = 0;
+    // depth-first ordering of the train step: Gaussian depth sort buffers
+    int sort_mode = GS3DC_SORT_DEPTH_FIRST;
+    DevBuf<unsigned long long> dkeys[2];
+    DevBuf<unsigned> dvals[2];
+    DevBuf<unsigned long long> ddesc;
+    unsigned long long ddesc_stride = 0;
     // control block + preprocess scan descriptors (one memset)
     DevBuf<unsigned char> ctrl_region;
     Control* ctrl = nullptr;
@@ -411,11 +417,64 @@ int seq_sort(gs3dc_ctx* c) {
     return GS3DC_OK;
 }
 
+constexpr int kDepthPasses = 4;   // 32 depth bits
+
+int ensure_depth_sort(gs3dc_ctx* c) {
+    const size_t n = c->N > 0 ? (size_t)c->N : 1;
+    for (int b = 0; b < 2; b++) {
+        CK(c->dkeys[b].ensure(n));
+        CK(c->dvals[b].ensure(n));
+    }
+    c->ddesc_stride = ((n + kSortTile - 1) / kSortTile) * 256ull;
+    CK(c->ddesc.ensure(kDepthPasses * c->ddesc_stride));
+    return GS3DC_OK;
+}
+
+// Depth-first front half of a train step: preprocess without emission, stable
+// depth sort of the Gaussians, pair emission in depth order, stable sort of
+// the pairs on the tile bits only (passes kDepthPasses..sort_passes-1 of the
+// full key), tile ranges and order.
+int seq_front_depth_first(gs3dc_ctx* c) {
+    int rc = mark(c, GS3DC_STAGE_MEMSETS);
+    if (rc) return rc;
+    CK(cudaMemsetAsync(c->ctrl_region.p, 0, ctrl_bytes_for(c->N), c->stream));
+    CK(cudaMemsetAsync(c->ranges.p, 0, 2 * (size_t)c->num_tiles * sizeof(unsigned), c->stream));
+    CK(cudaMemsetAsync(c->ddesc.p, 0, kDepthPasses * c->ddesc_stride * sizeof(unsigned long long), c->stream));
+    if (c->sort_passes > kDepthPasses)
+        CK(cudaMemsetAsync(c->sort_desc.p + kDepthPasses * c->sort_desc_stride, 0,
+                           (size_t)(c->sort_passes - kDepthPasses) * c->sort_desc_stride * sizeof(unsigned long long),
+                           c->stream));
+    if ((rc = mark(c, GS3DC_STAGE_PREPROCESS))) return rc;
+    PairPtrs pr{c->keys[0].p, c->vals[0].p, c->cap, c->scan_desc};
+    CK(launch_preprocess_plain(c->stream, c->sp_dev, c->N, c->model_raw, false, model_ptrs(c), screen_ptrs(c, false),
+                               pr, c->ctrl, DepthKeys{c->dkeys[0].p, c->dvals[0].p}));
+    if ((rc = mark(c, GS3DC_STAGE_SORT_HIST))) return rc;
+    int dw = 0;
+    CK(launch_radix_sort(c->stream, c->sp_dev, kDepthPasses, (unsigned long long)c->N, c->dkeys[0].p, c->dvals[0].p,
+                         c->dkeys[1].p, c->dvals[1].p, c->ddesc.p, c->ddesc_stride, c->ctrl, &dw, nullptr, 0,
+                         &c->ctrl->gauss_keys));
+    CK(launch_emit_ranked(c->stream, c->sp_dev, c->N, c->dvals[dw].p, screen_ptrs(c, false), pr, c->ctrl));
+    int which = 0;
+    CK(launch_radix_sort(c->stream, c->sp_dev, c->sort_passes, c->cap, c->keys[0].p, c->vals[0].p, c->keys[1].p,
+                         c->vals[1].p, c->sort_desc.p, c->sort_desc_stride, c->ctrl, &which,
+                         c->stage_timing ? c->stage_ev[GS3DC_STAGE_SORT_PASSES] : nullptr, kDepthPasses));
+    c->sorted_which = which;
+    if ((rc = mark(c, GS3DC_STAGE_RANGES))) return rc;
+    CK(launch_tile_ranges(c->stream, c->cap, c->keys[which].p, c->ranges.p, c->ctrl));
+    CK(launch_tile_order(c->stream, c->ranges.p, c->num_tiles, c->tile_order.p));
+    const int tile_passes = c->sort_passes > kDepthPasses ? c->sort_passes - kDepthPasses : 0;
+    c->kernels_last += c->N > 0 ? 1 + (1 + kDepthPasses) + 1 + (tile_passes ? 1 + tile_passes : 0) + 2 : 2;
+    return GS3DC_OK;
+}
+
 int seq_train(gs3dc_ctx* c) {
-    int rc = seq_preprocess(c, false);
-    if (rc) return rc;
-    rc = seq_sort(c);
-    if (rc) return rc;
+    int rc;
+    if (c->sort_mode == GS3DC_SORT_DEPTH_FIRST) {
+        if ((rc = seq_front_depth_first(c))) return rc;
+    } else {
+        if ((rc = seq_preprocess(c, false))) return rc;
+        if ((rc = seq_sort(c))) return rc;
+    }
     const int w = c->sorted_which;
     if ((rc = mark(c, GS3DC_STAGE_RASTER_FWD))) return rc;
     CK(launch_raster_fwd_plain(c->stream, c->sp_dev, c->num_tiles, true, c->ranges.p, c->tile_order.p, c->vals[w].p,
@@ -638,6 +697,11 @@ int gs3dc_set_option(gs3dc_ctx* c, int option, int64_t value) {
             return GS3DC_OK;
         case GS3DC_OPT_STAGE_TIMING:
             c->stage_timing = value != 0;
+            return GS3DC_OK;
+        case GS3DC_OPT_SORT:
+            if (value != GS3DC_SORT_DEPTH_FIRST && value != GS3DC_SORT_FULL_KEY)
+                return fail(c, GS3DC_ERR_INVALID_ARG, "unknown sort mode %lld", (long long)value);
+            c->sort_mode = (int)value;
             return GS3DC_OK;
         default:
             return fail(c, GS3DC_ERR_INVALID_ARG, "unknown option %d", option);
@@ -1050,6 +1114,7 @@ int gs3dc_train_step(gs3dc_ctx* c, const gs3d_camera* cam, const float* gt, int 
     CK(cudaSetDevice(c->device));
     if ((rc = ensure_adam(c))) return rc;
     if ((rc = ensure_grads(c))) return rc;
+    if ((rc = ensure_depth_sort(c))) return rc;
     if ((rc = ensure_pixels(c, cam->width, cam->height))) return rc;
     const size_t np = (size_t)cam->width * cam->height;
     const float* gt_dev = gt;
@@ -1068,7 +1133,7 @@ int gs3dc_train_step(gs3dc_ctx* c, const gs3d_camera* cam, const float* gt, int 
         c->adam_step = step_before + (tc->use_adam ? 1 : 0);
         if ((rc = push_params(c, cam, cfg, tc, iteration, gt_dev))) return rc;
         const long long key[8] = {c->N, c->max_coeffs, cam->width, cam->height, (long long)c->cap, c->sort_passes,
-                                  (long long)c->spin_limit, c->fused_adam ? 1 : 2};
+                                  (long long)c->spin_limit, (c->fused_adam ? 1 : 2) + 4 * c->sort_mode};
         const bool key_ok = c->graph && std::memcmp(key, c->graph_key, sizeof(key)) == 0;
         c->kernels_last = 0;
         if (c->use_graph && !c->stage_timing && !first && attempt == 0) {

@@ -58,6 +58,7 @@ struct Control {
     double loss_sum;                  // sum |image - gt| of the fused L1
     unsigned tickets[16];             // dynamic CTA tickets (0: preprocess/bin, 1..8: sort passes)
     unsigned hist[kMaxPasses][256];   // radix digit histograms of all passes
+    unsigned long long gauss_keys;    // depth-first pipeline: keys of the Gaussian depth sort
 };
 constexpr size_t kControlReadback = 24;
 

@@ -79,8 +79,20 @@ struct ScreenArrays {
 };
 
 // ---- plain FP32 kernels (plain.cu, compiled without FMA contraction) ----
+// Gaussian depth-sort input written by a preprocess that does not emit pairs.
+struct DepthKeys {
+    unsigned long long* keys;   // [N] depth bits, ~0u for Gaussians without pairs
+    unsigned* vals;             // [N] Gaussian index
+};
+// Preprocess; emits the pairs in Gaussian order, or -- when dk.keys != NULL --
+// writes the depth-sort input instead (pairs come from launch_emit_ranked).
 cudaError_t launch_preprocess_plain(cudaStream_t st, const StepParams* sp, int N, bool train,
-                                    bool cache, ModelPtrs m, ScreenPtrs s, PairPtrs pr, Control* ctrl);
+                                    bool cache, ModelPtrs m, ScreenPtrs s, PairPtrs pr, Control* ctrl,
+                                    DepthKeys dk = DepthKeys{nullptr, nullptr});
+// Emits the pairs of the Gaussians in the order rank_gid lists them
+// (depth order), with the same scan / look-back as the preprocess.
+cudaError_t launch_emit_ranked(cudaStream_t st, const StepParams* sp, int N, const unsigned* rank_gid,
+                               ScreenPtrs s, PairPtrs pr, Control* ctrl);
 cudaError_t launch_bin_arrays(cudaStream_t st, const StepParams* sp, int N, ScreenArrays a,
                               PairPtrs pr, Control* ctrl);
 cudaError_t launch_export_screen(cudaStream_t st, int N, ScreenPtrs s, ScreenArrays a);
@@ -110,7 +122,8 @@ cudaError_t launch_radix_sort(cudaStream_t st, const StepParams* sp, int sort_pa
                               unsigned long long capacity, unsigned long long* keys0, unsigned* vals0,
                               unsigned long long* keys1, unsigned* vals1, unsigned long long* desc,
                               unsigned long long desc_stride, Control* ctrl, int* which,
-                              cudaEvent_t after_hist = nullptr);
+                              cudaEvent_t after_hist = nullptr, int first_pass = 0,
+                              const unsigned long long* count = nullptr);
 cudaError_t launch_tile_ranges(cudaStream_t st, unsigned long long capacity,
                                const unsigned long long* keys_sorted, unsigned* ranges, Control* ctrl);
 

@@ -359,6 +359,7 @@ struct EmitShared {
     int width[kBlock];
     int limit[kBlock];     // pairs actually emitted (rect area, <= count)
     unsigned depth[kBlock];
+    unsigned gid[kBlock];  // Gaussian index written as the pair's value
     unsigned long long base;
 };
 
@@ -367,7 +368,7 @@ struct EmitShared {
 // consecutive pairs (fully coalesced, balanced however uneven the rects).
 // Pair order: Gaussian-major, then row-major inside the rect
 // (tile_binner_cpu.cpp:90-97).
-__device__ __forceinline__ void scan_and_emit(EmitShared& sm, int blk, int cnt, int emit, int rx, int ry,
+__device__ __forceinline__ void scan_and_emit(EmitShared& sm, int blk, unsigned gid, int cnt, int emit, int rx, int ry,
                                               int rw, unsigned dbits, int grid_x, PairPtrs pr,
                                               Control* ctrl, unsigned spin_limit, Persist* persist) {
     const int tid = threadIdx.x;
@@ -378,6 +379,7 @@ __device__ __forceinline__ void scan_and_emit(EmitShared& sm, int blk, int cnt, 
     sm.width[tid] = rw;
     sm.limit[tid] = emit;
     sm.depth[tid] = dbits;
+    sm.gid[tid] = gid;
     if (tid == 0) {
         const unsigned long long ex =
             lookback_exclusive(pr.scan_desc, blk, (unsigned long long)total, &ctrl->status, spin_limit);
@@ -406,21 +408,23 @@ __device__ __forceinline__ void scan_and_emit(EmitShared& sm, int blk, int cnt, 
         const int y = (r >> 16) + local / w;
         const unsigned tile = (unsigned)(y * grid_x + x);
         pr.keys[dst] = ((unsigned long long)tile << 32) | sm.depth[lo];
-        pr.vals[dst] = (unsigned)(blk * kBlock + lo);
+        pr.vals[dst] = sm.gid[lo];
     }
 }
 
 // ---------------- kernels ----------------
 
-template <bool TRAIN, bool CACHE>
+template <bool TRAIN, bool CACHE, bool EMIT>
 __global__ void __launch_bounds__(kBlock) k_preprocess(const StepParams* __restrict__ spp, int N, ModelPtrs m,
-                                                       ScreenPtrs s, PairPtrs pr, Control* ctrl) {
+                                                       ScreenPtrs s, PairPtrs pr, DepthKeys dk, Control* ctrl) {
     __shared__ EmitShared sm;
     __shared__ int s_blk;
     const StepParams& sp = *spp;
-    if (threadIdx.x == 0) s_blk = (int)atomicAdd(&ctrl->tickets[0], 1u);
-    __syncthreads();
-    const int blk = s_blk;
+    if (EMIT) {
+        if (threadIdx.x == 0) s_blk = (int)atomicAdd(&ctrl->tickets[0], 1u);
+        __syncthreads();
+    }
+    const int blk = EMIT ? s_blk : (int)blockIdx.x;
     const int i = blk * kBlock + threadIdx.x;
     int cnt = 0, rx = 0, ry = 0, rw = 1;
     unsigned dbits = 0;
@@ -471,7 +475,48 @@ __global__ void __launch_bounds__(kBlock) k_preprocess(const StepParams* __restr
             s.det[i] = vis ? r.det : 0.f;
         }
     }
-    scan_and_emit(sm, blk, cnt, cnt, rx, ry, rw, dbits, sp.grid_x, pr, ctrl, sp.spin_limit, sp.persist);
+    if (EMIT) {
+        scan_and_emit(sm, blk, (unsigned)i, cnt, cnt, rx, ry, rw, dbits, sp.grid_x, pr, ctrl, sp.spin_limit,
+                      sp.persist);
+    } else if (i < N) {
+        // depth-sort input: Gaussians without pairs sort last (no finite depth has these bits)
+        dk.keys[i] = cnt > 0 ? (unsigned long long)dbits : 0xFFFFFFFFull;
+        dk.vals[i] = (unsigned)i;
+        if (i == 0) ctrl->gauss_keys = (unsigned long long)N;
+    }
+}
+
+// Pair emission in depth order: thread r takes the Gaussian of depth rank r,
+// recomputes its tile rectangle from the stored mean and radius (the same
+// tile_rect the preprocess used) and emits its pairs row-major.  With the
+// Gaussians stably sorted by depth bits, a stable sort of these pairs by tile
+// alone gives the (tile, depth bits, Gaussian index) order of the full-key sort.
+__global__ void __launch_bounds__(kBlock) k_emit_ranked(const StepParams* __restrict__ spp, int N,
+                                                        const unsigned* __restrict__ rank_gid, ScreenPtrs s,
+                                                        PairPtrs pr, Control* ctrl) {
+    __shared__ EmitShared sm;
+    __shared__ int s_blk;
+    const StepParams& sp = *spp;
+    if (threadIdx.x == 0) s_blk = (int)atomicAdd(&ctrl->tickets[0], 1u);
+    __syncthreads();
+    const int blk = s_blk;
+    const int r = blk * kBlock + threadIdx.x;
+    int cnt = 0, rx = 0, ry = 0, rw = 1;
+    unsigned g = 0, dbits = 0;
+    if (r < N) {
+        g = rank_gid[r];
+        cnt = s.tiles[g];
+        if (cnt > 0) {
+            const float4 r0 = s.rec0[g];
+            int rmn[2], rmx[2];
+            tile_rect(r0.x, r0.y, s.radius[g], sp.grid_x, sp.grid_y, sp.cfg.tile_w, sp.cfg.tile_h, rmn, rmx);
+            rx = rmn[0];
+            ry = rmn[1];
+            rw = rmx[0] - rmn[0];
+            dbits = __float_as_uint(s.depth[g]);
+        }
+    }
+    scan_and_emit(sm, blk, g, cnt, cnt, rx, ry, rw, dbits, sp.grid_x, pr, ctrl, sp.spin_limit, sp.persist);
 }
 
 // TileBinner::bin over host-provided screen arrays (tile_binner_cpu.cpp:33-99):
@@ -500,7 +545,7 @@ __global__ void __launch_bounds__(kBlock) k_bin_arrays(const StepParams* __restr
             dbits = __float_as_uint(a.depths[i]);
         }
     }
-    scan_and_emit(sm, blk, cnt, emit, rx, ry, rw, dbits, sp.grid_x, pr, ctrl, sp.spin_limit, nullptr);
+    scan_and_emit(sm, blk, (unsigned)i, cnt, emit, rx, ry, rw, dbits, sp.grid_x, pr, ctrl, sp.spin_limit, nullptr);
 }
 
 // Unpacks the screen records into PreprocessOutput's layout.
@@ -1422,16 +1467,31 @@ inline int blocks_for(long long n, int t) { return (int)((n + t - 1) / t); }
 }  // namespace
 
 cudaError_t launch_preprocess_plain(cudaStream_t st, const StepParams* sp, int N, bool train, bool cache,
-                                    ModelPtrs m, ScreenPtrs s, PairPtrs pr, Control* ctrl) {
+                                    ModelPtrs m, ScreenPtrs s, PairPtrs pr, Control* ctrl, DepthKeys dk) {
     if (N <= 0) return cudaSuccess;
     const int grid = blocks_for(N, kBlock);
-    if (train) {
-        if (cache) k_preprocess<true, true><<<grid, kBlock, 0, st>>>(sp, N, m, s, pr, ctrl);
-        else k_preprocess<true, false><<<grid, kBlock, 0, st>>>(sp, N, m, s, pr, ctrl);
+    if (dk.keys) {
+        if (train) {
+            if (cache) k_preprocess<true, true, false><<<grid, kBlock, 0, st>>>(sp, N, m, s, pr, dk, ctrl);
+            else k_preprocess<true, false, false><<<grid, kBlock, 0, st>>>(sp, N, m, s, pr, dk, ctrl);
+        } else {
+            if (cache) k_preprocess<false, true, false><<<grid, kBlock, 0, st>>>(sp, N, m, s, pr, dk, ctrl);
+            else k_preprocess<false, false, false><<<grid, kBlock, 0, st>>>(sp, N, m, s, pr, dk, ctrl);
+        }
+    } else if (train) {
+        if (cache) k_preprocess<true, true, true><<<grid, kBlock, 0, st>>>(sp, N, m, s, pr, dk, ctrl);
+        else k_preprocess<true, false, true><<<grid, kBlock, 0, st>>>(sp, N, m, s, pr, dk, ctrl);
     } else {
-        if (cache) k_preprocess<false, true><<<grid, kBlock, 0, st>>>(sp, N, m, s, pr, ctrl);
-        else k_preprocess<false, false><<<grid, kBlock, 0, st>>>(sp, N, m, s, pr, ctrl);
+        if (cache) k_preprocess<false, true, true><<<grid, kBlock, 0, st>>>(sp, N, m, s, pr, dk, ctrl);
+        else k_preprocess<false, false, true><<<grid, kBlock, 0, st>>>(sp, N, m, s, pr, dk, ctrl);
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_emit_ranked(cudaStream_t st, const StepParams* sp, int N, const unsigned* rank_gid,
+                               ScreenPtrs s, PairPtrs pr, Control* ctrl) {
+    if (N <= 0) return cudaSuccess;
+    k_emit_ranked<<<blocks_for(N, kBlock), kBlock, 0, st>>>(sp, N, rank_gid, s, pr, ctrl);
     return cudaGetLastError();
 }
 

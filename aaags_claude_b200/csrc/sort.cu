@@ -30,12 +30,12 @@ namespace {
 constexpr int kHistThreads = 512;
 
 __global__ void __launch_bounds__(kHistThreads) k_radix_hist(const unsigned long long* __restrict__ keys,
-                                                             unsigned long long capacity, int passes,
-                                                             Control* ctrl) {
+                                                             unsigned long long capacity, int first, int passes,
+                                                             const unsigned long long* count, Control* ctrl) {
     __shared__ unsigned s_h[kMaxPasses * 256];
-    for (int e = threadIdx.x; e < passes * 256; e += blockDim.x) s_h[e] = 0;
+    for (int e = first * 256 + threadIdx.x; e < passes * 256; e += blockDim.x) s_h[e] = 0;
     __syncthreads();
-    const unsigned long long P = min(ctrl->total_pairs, capacity);
+    const unsigned long long P = min(*count, capacity);
     const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
     const unsigned lane = threadIdx.x & 31;
     for (unsigned long long base = (unsigned long long)blockIdx.x * blockDim.x; base < P; base += stride) {
@@ -44,7 +44,7 @@ __global__ void __launch_bounds__(kHistThreads) k_radix_hist(const unsigned long
         const unsigned mask = __ballot_sync(0xffffffffu, valid);
         if (valid) {
             const unsigned long long key = keys[i];
-            for (int p = 0; p < passes; p++) {
+            for (int p = first; p < passes; p++) {
                 const unsigned d = (unsigned)(key >> (8 * p)) & 255u;
                 const unsigned peers = __match_any_sync(mask, d);
                 if (lane == (unsigned)(__ffs(peers) - 1)) atomicAdd(&s_h[p * 256 + d], (unsigned)__popc(peers));
@@ -52,7 +52,7 @@ __global__ void __launch_bounds__(kHistThreads) k_radix_hist(const unsigned long
         }
     }
     __syncthreads();
-    for (int e = threadIdx.x; e < passes * 256; e += blockDim.x)
+    for (int e = first * 256 + threadIdx.x; e < passes * 256; e += blockDim.x)
         if (s_h[e]) atomicAdd(&ctrl->hist[e >> 8][e & 255], s_h[e]);
 }
 
@@ -90,12 +90,14 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const StepParams* 
                                                               unsigned long long* __restrict__ kout,
                                                               unsigned* __restrict__ vout,
                                                               unsigned long long capacity, int pass,
-                                                              unsigned long long* desc, Control* ctrl) {
+                                                              unsigned long long* desc,
+                                                              const unsigned long long* count,
+                                                              Control* ctrl) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SweepShared& sm = *reinterpret_cast<SweepShared*>(smem_raw);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int shift = 8 * pass;
-    const unsigned long long P = min(ctrl->total_pairs, capacity);
+    const unsigned long long P = min(*count, capacity);
     if (tid == 0) sm.tile = (int)atomicAdd(&ctrl->tickets[1 + pass], 1u);
     for (int e = tid; e < (kSortThreads / 32) * 256; e += kSortThreads) (&sm.whist[0][0])[e] = 0;
     __syncthreads();
@@ -218,9 +220,11 @@ cudaError_t launch_wait_selftest(cudaStream_t st, unsigned long long* desc2, uns
 cudaError_t launch_radix_sort(cudaStream_t st, const StepParams* sp, int passes, unsigned long long capacity,
                               unsigned long long* keys0, unsigned* vals0, unsigned long long* keys1,
                               unsigned* vals1, unsigned long long* desc, unsigned long long desc_stride,
-                              Control* ctrl, int* which, cudaEvent_t after_hist) {
+                              Control* ctrl, int* which, cudaEvent_t after_hist, int first_pass,
+                              const unsigned long long* count) {
     *which = 0;
-    if (capacity == 0 || passes <= 0) return cudaSuccess;
+    if (capacity == 0 || passes <= first_pass) return cudaSuccess;
+    if (!count) count = &ctrl->total_pairs;
     static bool attr_set = false;
     const int smem = (int)sizeof(SweepShared);
     if (!attr_set) {
@@ -228,7 +232,7 @@ cudaError_t launch_radix_sort(cudaStream_t st, const StepParams* sp, int passes,
         if (e != cudaSuccess) return e;
         attr_set = true;
     }
-    k_radix_hist<<<2 * 148, kHistThreads, 0, st>>>(keys0, capacity, passes, ctrl);
+    k_radix_hist<<<2 * 148, kHistThreads, 0, st>>>(keys0, capacity, first_pass, passes, count, ctrl);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     if (after_hist && (e = cudaEventRecord(after_hist, st)) != cudaSuccess) return e;
@@ -237,10 +241,10 @@ cudaError_t launch_radix_sort(cudaStream_t st, const StepParams* sp, int passes,
     unsigned* vin = vals0;
     unsigned long long* kout = keys1;
     unsigned* vout = vals1;
-    for (int p = 0; p < passes; p++) {
+    for (int p = first_pass; p < passes; p++) {
         k_onesweep<<<(unsigned)tiles, kSortThreads, smem, st>>>(sp, kin, vin, kout, vout, capacity, p,
                                                                 desc + (unsigned long long)p * desc_stride,
-                                                                ctrl);
+                                                                count, ctrl);
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
         unsigned long long* tk = kin;
@@ -250,7 +254,7 @@ cudaError_t launch_radix_sort(cudaStream_t st, const StepParams* sp, int passes,
         vin = vout;
         vout = tv;
     }
-    *which = passes & 1;
+    *which = (passes - first_pass) & 1;
     return cudaSuccess;
 }
 

@@ -26,6 +26,8 @@ OPT_PAIR_CAPACITY, OPT_USE_GRAPH, OPT_FORM, OPT_SPIN_LIMIT, OPT_STAGE_TIMING, OP
 NUM_STAGES = 8
 STAT_TOTAL_PAIRS, STAT_PAIR_CAPACITY, STAT_KERNELS_LAST, STAT_SORT_PASSES, STAT_GRAPH_REPLAYS, STAT_ADAM_STEP = range(1, 7)
 FORM_PLAIN_FP32 = 0
+OPT_SORT = 7
+SORT_DEPTH_FIRST, SORT_FULL_KEY = 0, 1
 
 _f = ctypes.POINTER(ctypes.c_float)
 _i = ctypes.POINTER(ctypes.c_int)

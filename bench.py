@@ -55,6 +55,8 @@ def _args(argv=None):
     ap.add_argument("--gaussians", type=int, default=1_000_000, help="scene size (profiling cases use less)")
     ap.add_argument("--size", default="1920x1080", help="WxH of the camera")
     ap.add_argument("--fused-adam", type=int, default=None, help="1: optimiser fused into the backward kernel")
+    ap.add_argument("--sort", choices=("depth-first", "full-key"), default="depth-first",
+                    help="pair ordering of the train step")
     return ap.parse_args(argv)
 
 
@@ -149,16 +151,27 @@ def _bus_id(dev: int) -> str | None:
 
 
 # ---------------------------------------------------------------- roofline
-def stage_bytes(N: int, P: int, X: int, T: int, passes: int, mc3: int = 48) -> dict:
+def stage_bytes(N: int, P: int, X: int, T: int, passes: int, mc3: int = 48, depth_first: bool = True) -> dict:
     """Algorithmic (compulsory) DRAM bytes of one launch of each stage (plain FP32).
 
     s_p = 4*(11 + mc3) bytes of parameters per Gaussian, s_m = 2*s_p of Adam
-    moments; P tile pairs; X pixels; T tiles.
+    moments; P tile pairs; X pixels; T tiles.  Depth-first ordering: the
+    preprocess writes the depth-sort input instead of pairs; "sort_hist" holds
+    the 4-pass depth sort of N keys, the pair emission in depth order and the
+    tile-digit histogram; "sort_passes" are the passes over the tile bits.
     """
     sp = 4 * (11 + mc3)
+    if depth_first:
+        pre = N * (sp + 48) + N * 12                     # params in; records out; depth key + index out
+        hist = (N * 8 + 4 * N * 24                       # depth sort: histogram + 4 passes
+                + N * 24 + P * 12                        # emission: index, tiles, mean, radius, depth in; pairs out
+                + P * 8)                                 # tile-digit histogram
+    else:
+        pre = N * (sp + 48) + P * 12                     # params in; record+depth+radius+tiles out; pairs out
+        hist = P * 8                                     # keys in
     return {
-        "preprocess": N * (sp + 48) + P * 12,          # params in; record+depth+radius+tiles out; pairs out
-        "sort_hist": P * 8,                              # keys in
+        "preprocess": pre,
+        "sort_hist": hist,
         "sort_passes": P * 24,                           # per pass: key+value in and out
         "ranges": P * 8 + T * 8,
         "raster_fwd": P * 40 + X * 37,                   # index + gathered record; image/T/n/last/sign out, gt in
@@ -221,6 +234,8 @@ def run_ours(a) -> int:
     ctx = gs3d.Context(local)
     if a.fused_adam is not None:
         ctx.set_option(gs3d.OPT_FUSED_ADAM, a.fused_adam)
+    depth_first = a.sort == "depth-first"
+    ctx.set_option(gs3d.OPT_SORT, gs3d.SORT_DEPTH_FIRST if depth_first else gs3d.SORT_FULL_KEY)
     # target image: the perturbed scene rendered by this library (setup, untimed)
     ctx.set_raw_params(w.target_scene)
     gt = ctx.render(cam, S.render_config(False))
@@ -238,6 +253,7 @@ def run_ours(a) -> int:
     ctx.synchronize()
     P = ctx.stat(gs3d.STAT_TOTAL_PAIRS)
     passes = ctx.stat(gs3d.STAT_SORT_PASSES)
+    pair_passes = passes - 4 if depth_first else passes   # passes over the pairs
 
     # ---- value: inputs resident in HBM, graph replay, CUDA events on the library stream ----
     clocks = ClockSampler(_bus_id(local))
@@ -289,8 +305,9 @@ def run_ours(a) -> int:
         ms_step = ms_total / a.steps
         value = world * a.steps / (ms_total / 1e3)
         peak, peak_kind = _peaks()
-        nbytes = stage_bytes(w.scene.count, P, X, T, passes)
-        per_launch_ms = {s: stage_ms[k] / (passes if s == "sort_passes" else 1) for k, s in enumerate(STAGES)}
+        nbytes = stage_bytes(w.scene.count, P, X, T, passes, depth_first=depth_first)
+        per_launch_ms = {s: stage_ms[k] / (max(pair_passes, 1) if s == "sort_passes" else 1)
+                         for k, s in enumerate(STAGES)}
         dom = max((s for s in STAGES if s != "memsets"), key=lambda s: stage_ms[STAGES.index(s)])
         achieved = nbytes[dom] / (per_launch_ms[dom] * 1e-3) / 1e9
         traffic = None
@@ -298,7 +315,7 @@ def run_ours(a) -> int:
         if tt and dom in tt.get("kernels", {}):
             k = tt["kernels"][dom]
             traffic = k["bytes_per_launch"] * (P / k["pairs"] if k.get("scale") == "pairs" else 1.0)
-        step_bytes = sum(nbytes[s] * (passes if s == "sort_passes" else 1) for s in nbytes)
+        step_bytes = sum(nbytes[s] * (pair_passes if s == "sort_passes" else 1) for s in nbytes)
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "steps/s", "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak",
@@ -307,6 +324,7 @@ def run_ours(a) -> int:
             "config": {"workload": _workload_name(a), "gaussians": w.scene.count, "sh_degree": 3, "width": W,
                        "height": H,
                        "tile": 16, "tile_pairs": P, "sort_passes": passes,
+                       "pair_order": a.sort,
                        "l2": "working set ~1.6 GB per step > 126 MB L2 (no flush needed)",
                        "parallelism": f"replicas x{world}", "cuda_graph": graph},
             "mpix_per_s": round(value * X / 1e6, 2),
@@ -320,7 +338,8 @@ def run_ours(a) -> int:
                          "traffic": traffic, "algorithmic_bytes_per_launch": int(nbytes[dom])},
             "step_roofline": {"algorithmic_bytes": int(step_bytes),
                               "frac": round(step_bytes / (ms_step * 1e-3) / 1e9 / peak, 4)},
-            "sort_keys_per_s": round(P * passes / (stage_ms[STAGES.index('sort_passes')] * 1e-3), 1),
+            "sort_keys_per_s": (round(P * pair_passes / (stage_ms[STAGES.index('sort_passes')] * 1e-3), 1)
+                                if stage_ms[STAGES.index('sort_passes')] > 0 else None),
             "loss_first": loss0, "loss_last": loss,
             "clocks": clk,
         }

@@ -45,6 +45,13 @@ typedef struct gs3dc_ctx gs3dc_ctx;
 #define GS3DC_OPT_SPIN_LIMIT     4  /* iterations before a device-side wait gives up (test hook) */
 #define GS3DC_OPT_STAGE_TIMING   5  /* 1: train steps run un-captured with CUDA events between stages */
 #define GS3DC_OPT_FUSED_ADAM     6  /* 1: optimiser fused into the preprocess backward; 0 (default): split */
+#define GS3DC_OPT_SORT           7  /* GS3DC_SORT_*: how gs3dc_train_step orders its pairs (same result) */
+
+/* Depth-first (default): the Gaussians are stably sorted by depth, their pairs
+ * emitted in that order and stably sorted by the tile bits alone.  Full key:
+ * pairs emitted in Gaussian order and sorted on all tile and depth bits. */
+#define GS3DC_SORT_DEPTH_FIRST   0
+#define GS3DC_SORT_FULL_KEY      1
 
 #define GS3DC_FORM_PLAIN_FP32    0  /* FP32 everywhere, no FMA contraction: parity form */
 
@@ -207,8 +214,8 @@ int gs3dc_train_step(gs3dc_ctx* ctx, const gs3d_camera* cam, const float* gt, in
  * indexed by GS3DC_STAGE_*. */
 #define GS3DC_STAGE_MEMSETS        0  /* control block, sort scratch, tile ranges */
 #define GS3DC_STAGE_PREPROCESS     1  /* activation + projection + scan + pair emission */
-#define GS3DC_STAGE_SORT_HIST      2
-#define GS3DC_STAGE_SORT_PASSES    3  /* all onesweep passes together */
+#define GS3DC_STAGE_SORT_HIST      2  /* digit histograms; depth-first: also the Gaussian depth sort + pair emission */
+#define GS3DC_STAGE_SORT_PASSES    3  /* all onesweep passes over the pairs together */
 #define GS3DC_STAGE_RANGES         4
 #define GS3DC_STAGE_RASTER_FWD     5  /* incl. the fused L1 */
 #define GS3DC_STAGE_RASTER_BWD     6

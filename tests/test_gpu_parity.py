@@ -98,11 +98,14 @@ def test_sort_pairs_known_answers(ctx, case):
     assert list(vo) == exp_vals and list(rg) == exp_ranges and list(ko) == sorted(keys)
 
 
+# (1, 1): a single pair; 4095 / 4097: around the 4096-key onesweep CTA tile;
+# (60_000, 5) / (150_000, 3): few tiles of ~12K / ~50K pairs each
 @pytest.mark.parametrize("P,num_tiles,dups", [(1, 1, False), (4095, 7, True), (4097, 3000, False),
+                                              (60_000, 5, True), (150_000, 3, True),
                                               (300_001, 8160, True), (2_000_000, 32400, True)])
 def test_sort_pairs_random_stable(ctx, P, num_tiles, dups):
-    """Random keys, ragged sizes around the 4096-key CTA tile, duplicate keys:
-    the CUDA result equals the stable (key, index) order."""
+    """Random keys, ragged sizes around the 4096-key CTA tile, duplicate keys,
+    very full tiles: the CUDA result equals the stable (key, index) order."""
     rng = np.random.default_rng(P)
     tiles = rng.integers(0, num_tiles, P).astype(np.uint64)
     depth = rng.integers(0x3E4CCCCD, 0x40C00000, P).astype(np.uint64)

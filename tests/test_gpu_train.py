@@ -116,6 +116,39 @@ def test_train_step_graph_matches_eager(ctx):
         assert np.abs(getattr(res[0][1], k) - getattr(res[1][1], k)).max() <= 1e-6
 
 
+@pytest.mark.parametrize("tied", [False, True])
+def test_train_step_sort_modes_agree(ctx, tied):
+    """Depth-first ordering (Gaussians sorted by depth, pairs sorted by tile
+    only) renders bit-identically to the full-key sort, also when every
+    Gaussian has the same depth bits (a plane facing the camera), where only
+    the Gaussian-index tie-break decides the blend order."""
+    sc = S.random_scene(20000, seed=21)
+    if tied:
+        sc.positions[:, 2] = 0.0
+    cam = S.look_at_camera((0.0, 0.0, -3.0), 320, 240)
+    cfg, tc = S.render_config(True), S.train_config()
+    gt = O.forward(S.perturbed(sc), cam, S.render_config(False), "c").image
+    ref = O.forward(sc, cam, cfg, "c")
+    if tied:
+        assert len(np.unique(ref.keys_sorted & np.uint64(0xFFFFFFFF))) == 1
+    out = {}
+    for mode in (gs3d.SORT_FULL_KEY, gs3d.SORT_DEPTH_FIRST):
+        ctx.set_option(gs3d.OPT_SORT, mode)
+        ctx.set_raw_params(sc)
+        loss0 = ctx.train_step(cam, gt, cfg, tc, 0)
+        img0 = ctx.get_image(cam)
+        for it in range(1, 3):
+            ctx.train_step(cam, gt, cfg, tc, it)
+        out[mode] = (loss0, img0, ctx.get_raw_params(sc.copy()))
+    ctx.set_option(gs3d.OPT_SORT, gs3d.SORT_DEPTH_FIRST)
+    (la, ia, pa), (lb, ib, pb) = out[gs3d.SORT_FULL_KEY], out[gs3d.SORT_DEPTH_FIRST]
+    assert U.bits_equal(ia, ib)
+    assert np.abs(ib - ref.image).max() <= 1e-5
+    assert abs(la - lb) <= 1e-6 * abs(la)
+    for k in ("positions", "scales", "rotations", "sh", "opacities"):
+        assert np.abs(getattr(pa, k) - getattr(pb, k)).max() <= 1e-6, k
+
+
 def test_optimizer_stage_matches_reference(ctx):
     """Stage-level AdamOptimizer::step on the device equals the fused step."""
     z = np.load(os.path.join(U.SEEDED, "train_2k_128x128_adam.npz"))

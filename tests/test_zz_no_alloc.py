@@ -26,7 +26,9 @@ def _pairs(P: int, num_tiles: int, seed: int):
     # depths rounded to 1/64 so that many keys are equal and stability shows
     depth = (np.round(rng.uniform(0.2, 20.0, P) * 64) / 64).astype(np.float32)
     keys = (tiles << np.uint64(32)) | depth.view(np.uint32).astype(np.uint64)
-    vals = rng.integers(0, 1 << 20, P, dtype=np.uint32)
+    # non-decreasing values (Gaussian indices in emission order, as the binner
+    # writes them): equal keys then have one order however the sort breaks ties
+    vals = np.sort(rng.integers(0, 1 << 20, P, dtype=np.uint32))
     return keys, vals
 
 
