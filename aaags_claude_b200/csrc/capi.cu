@@ -417,7 +417,6 @@ int seq_sort(gs3dc_ctx* c) {
     return GS3DC_OK;
 }
 
-constexpr int kDepthPasses = 4;   // 32 depth bits
 
 int ensure_depth_sort(gs3dc_ctx* c) {
     const size_t n = c->N > 0 ? (size_t)c->N : 1;
@@ -426,44 +425,45 @@ int ensure_depth_sort(gs3dc_ctx* c) {
         CK(c->dvals[b].ensure(n));
     }
     c->ddesc_stride = ((n + kSortTile - 1) / kSortTile) * 256ull;
-    CK(c->ddesc.ensure(kDepthPasses * c->ddesc_stride));
+    CK(c->ddesc.ensure(kDepthDigits * c->ddesc_stride));
     return GS3DC_OK;
 }
 
 // Depth-first front half of a train step: preprocess without emission, stable
 // depth sort of the Gaussians, pair emission in depth order, stable sort of
-// the pairs on the tile bits only (passes kDepthPasses..sort_passes-1 of the
+// the pairs on the tile bits only (passes kDepthDigits..sort_passes-1 of the
 // full key), tile ranges and order.
 int seq_front_depth_first(gs3dc_ctx* c) {
     int rc = mark(c, GS3DC_STAGE_MEMSETS);
     if (rc) return rc;
     CK(cudaMemsetAsync(c->ctrl_region.p, 0, ctrl_bytes_for(c->N), c->stream));
     CK(cudaMemsetAsync(c->ranges.p, 0, 2 * (size_t)c->num_tiles * sizeof(unsigned), c->stream));
-    CK(cudaMemsetAsync(c->ddesc.p, 0, kDepthPasses * c->ddesc_stride * sizeof(unsigned long long), c->stream));
-    if (c->sort_passes > kDepthPasses)
-        CK(cudaMemsetAsync(c->sort_desc.p + kDepthPasses * c->sort_desc_stride, 0,
-                           (size_t)(c->sort_passes - kDepthPasses) * c->sort_desc_stride * sizeof(unsigned long long),
+    CK(cudaMemsetAsync(c->ddesc.p, 0, kDepthDigits * c->ddesc_stride * sizeof(unsigned long long), c->stream));
+    const int tile_digits = c->sort_passes - kDepthDigits;
+    if (tile_digits > 0)
+        CK(cudaMemsetAsync(c->sort_desc.p, 0, (size_t)tile_digits * c->sort_desc_stride * sizeof(unsigned long long),
                            c->stream));
     if ((rc = mark(c, GS3DC_STAGE_PREPROCESS))) return rc;
-    PairPtrs pr{c->keys[0].p, c->vals[0].p, c->cap, c->scan_desc};
+    // tile-only keys live in the (otherwise unused) 64-bit key buffers
+    unsigned* tk[2] = {reinterpret_cast<unsigned*>(c->keys[0].p), reinterpret_cast<unsigned*>(c->keys[1].p)};
+    PairPtrs pr{c->keys[0].p, c->vals[0].p, c->cap, c->scan_desc, tk[0]};
     CK(launch_preprocess_plain(c->stream, c->sp_dev, c->N, c->model_raw, false, model_ptrs(c), screen_ptrs(c, false),
                                pr, c->ctrl, DepthKeys{c->dkeys[0].p, c->dvals[0].p}));
     if ((rc = mark(c, GS3DC_STAGE_SORT_HIST))) return rc;
     int dw = 0;
-    CK(launch_radix_sort(c->stream, c->sp_dev, kDepthPasses, (unsigned long long)c->N, c->dkeys[0].p, c->dvals[0].p,
+    CK(launch_radix_sort(c->stream, c->sp_dev, kDepthDigits, (unsigned long long)c->N, c->dkeys[0].p, c->dvals[0].p,
                          c->dkeys[1].p, c->dvals[1].p, c->ddesc.p, c->ddesc_stride, c->ctrl, &dw, nullptr, 0,
                          &c->ctrl->gauss_keys));
     CK(launch_emit_ranked(c->stream, c->sp_dev, c->N, c->dvals[dw].p, screen_ptrs(c, false), pr, c->ctrl));
+    if ((rc = mark(c, GS3DC_STAGE_SORT_PASSES))) return rc;
     int which = 0;
-    CK(launch_radix_sort(c->stream, c->sp_dev, c->sort_passes, c->cap, c->keys[0].p, c->vals[0].p, c->keys[1].p,
-                         c->vals[1].p, c->sort_desc.p, c->sort_desc_stride, c->ctrl, &which,
-                         c->stage_timing ? c->stage_ev[GS3DC_STAGE_SORT_PASSES] : nullptr, kDepthPasses));
+    CK(launch_radix_sort32(c->stream, c->sp_dev, tile_digits, kDepthDigits, true, c->cap, tk[0], c->vals[0].p, tk[1],
+                           c->vals[1].p, c->sort_desc.p, c->sort_desc_stride, c->ctrl, &which));
     c->sorted_which = which;
     if ((rc = mark(c, GS3DC_STAGE_RANGES))) return rc;
-    CK(launch_tile_ranges(c->stream, c->cap, c->keys[which].p, c->ranges.p, c->ctrl));
+    CK(launch_tile_ranges32(c->stream, c->cap, tk[which], c->ranges.p, c->ctrl));
     CK(launch_tile_order(c->stream, c->ranges.p, c->num_tiles, c->tile_order.p));
-    const int tile_passes = c->sort_passes > kDepthPasses ? c->sort_passes - kDepthPasses : 0;
-    c->kernels_last += c->N > 0 ? 1 + (1 + kDepthPasses) + 1 + (tile_passes ? 1 + tile_passes : 0) + 2 : 2;
+    c->kernels_last += c->N > 0 ? 1 + (1 + kDepthDigits) + 1 + (tile_digits > 0 ? tile_digits : 0) + 2 : 2;
     return GS3DC_OK;
 }
 

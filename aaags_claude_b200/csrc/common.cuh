@@ -10,7 +10,9 @@ namespace gs3d {
 
 constexpr int kTile = 16;            // 16x16 pixel tiles (RenderConfig default, include/types.h:64-65)
 constexpr int kBlock = 256;          // threads per CTA of the per-Gaussian and per-tile kernels
-constexpr int kMaxPasses = 8;        // radix passes (8-bit digits over <= 64 key bits)
+constexpr int kMaxPasses = 8;         // radix passes (8-bit digits over <= 64 key bits)
+constexpr int kDepthDigits = 4;       // depth-first ordering: digits of the Gaussian depth sort (control slots
+                                      // 0..3); the pair sort on the tile bits uses slots kDepthDigits..
 
 // Device-status bits (Control::status).
 constexpr unsigned kStatusOverflow = 1u;  // more tile pairs than capacity

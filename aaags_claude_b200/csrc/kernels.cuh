@@ -43,6 +43,7 @@ struct PairPtrs {
     unsigned* vals;             // [capacity]
     unsigned long long capacity;
     unsigned long long* scan_desc;  // look-back descriptors, one per preprocess CTA
+    unsigned* tiles32 = nullptr;    // depth-ordered emission: tile-only keys [capacity] instead of keys
 };
 
 struct PixelPtrs {
@@ -90,7 +91,9 @@ cudaError_t launch_preprocess_plain(cudaStream_t st, const StepParams* sp, int N
                                     bool cache, ModelPtrs m, ScreenPtrs s, PairPtrs pr, Control* ctrl,
                                     DepthKeys dk = DepthKeys{nullptr, nullptr});
 // Emits the pairs of the Gaussians in the order rank_gid lists them
-// (depth order), with the same scan / look-back as the preprocess.
+// (depth order), with the same scan / look-back as the preprocess: tile-only
+// keys to pr.tiles32, and the tile-digit histograms into control slots
+// kDepthDigits.. for launch_radix_sort32.
 cudaError_t launch_emit_ranked(cudaStream_t st, const StepParams* sp, int N, const unsigned* rank_gid,
                                ScreenPtrs s, PairPtrs pr, Control* ctrl);
 cudaError_t launch_bin_arrays(cudaStream_t st, const StepParams* sp, int N, ScreenArrays a,
@@ -126,6 +129,16 @@ cudaError_t launch_radix_sort(cudaStream_t st, const StepParams* sp, int sort_pa
                               const unsigned long long* count = nullptr);
 cudaError_t launch_tile_ranges(cudaStream_t st, unsigned long long capacity,
                                const unsigned long long* keys_sorted, unsigned* ranges, Control* ctrl);
+
+// Stable LSD sort of 32-bit keys (tile ids) over digits [0, digits), control
+// slots slot_base..; hist_done: the digit histograms are already in those slots.
+// desc holds digits * desc_stride zeroed descriptors.
+cudaError_t launch_radix_sort32(cudaStream_t st, const StepParams* sp, int digits, int slot_base, bool hist_done,
+                                unsigned long long capacity, unsigned* keys0, unsigned* vals0, unsigned* keys1,
+                                unsigned* vals1, unsigned long long* desc, unsigned long long desc_stride,
+                                Control* ctrl, int* which, cudaEvent_t after_hist = nullptr);
+cudaError_t launch_tile_ranges32(cudaStream_t st, unsigned long long capacity, const unsigned* tiles_sorted,
+                                 unsigned* ranges, Control* ctrl);
 
 // Heavy-first permutation of the tiles (by pair count) for the rasterisers.
 cudaError_t launch_tile_order(cudaStream_t st, const unsigned* ranges, int num_tiles, unsigned* order);

@@ -368,9 +368,12 @@ struct EmitShared {
 // consecutive pairs (fully coalesced, balanced however uneven the rects).
 // Pair order: Gaussian-major, then row-major inside the rect
 // (tile_binner_cpu.cpp:90-97).
+// With pr.tiles32 set, writes tile-only keys and counts the first nd 8-bit
+// digits of every tile into thist[nd][256] (shared memory).
 __device__ __forceinline__ void scan_and_emit(EmitShared& sm, int blk, unsigned gid, int cnt, int emit, int rx, int ry,
                                               int rw, unsigned dbits, int grid_x, PairPtrs pr,
-                                              Control* ctrl, unsigned spin_limit, Persist* persist) {
+                                              Control* ctrl, unsigned spin_limit, Persist* persist,
+                                              unsigned* thist = nullptr, int nd = 0) {
     const int tid = threadIdx.x;
     int total;
     const int incl = block_inclusive_scan(cnt, sm.warp, &total);
@@ -407,7 +410,12 @@ __device__ __forceinline__ void scan_and_emit(EmitShared& sm, int blk, unsigned 
         const int x = (r & 0xffff) + local % w;
         const int y = (r >> 16) + local / w;
         const unsigned tile = (unsigned)(y * grid_x + x);
-        pr.keys[dst] = ((unsigned long long)tile << 32) | sm.depth[lo];
+        if (pr.tiles32) {
+            pr.tiles32[dst] = tile;
+            for (int d = 0; d < nd; d++) atomicAdd(&thist[d * 256 + ((tile >> (8 * d)) & 255u)], 1u);
+        } else {
+            pr.keys[dst] = ((unsigned long long)tile << 32) | sm.depth[lo];
+        }
         pr.vals[dst] = sm.gid[lo];
     }
 }
@@ -496,7 +504,10 @@ __global__ void __launch_bounds__(kBlock) k_emit_ranked(const StepParams* __rest
                                                         PairPtrs pr, Control* ctrl) {
     __shared__ EmitShared sm;
     __shared__ int s_blk;
+    __shared__ unsigned s_thist[kMaxPasses - kDepthDigits][256];
     const StepParams& sp = *spp;
+    const int nd = sp.sort_passes - kDepthDigits;   // 8-bit digits of the tile ids
+    for (int e = threadIdx.x; e < nd * 256; e += kBlock) (&s_thist[0][0])[e] = 0;
     if (threadIdx.x == 0) s_blk = (int)atomicAdd(&ctrl->tickets[0], 1u);
     __syncthreads();
     const int blk = s_blk;
@@ -516,7 +527,13 @@ __global__ void __launch_bounds__(kBlock) k_emit_ranked(const StepParams* __rest
             dbits = __float_as_uint(s.depth[g]);
         }
     }
-    scan_and_emit(sm, blk, g, cnt, cnt, rx, ry, rw, dbits, sp.grid_x, pr, ctrl, sp.spin_limit, sp.persist);
+    scan_and_emit(sm, blk, g, cnt, cnt, rx, ry, rw, dbits, sp.grid_x, pr, ctrl, sp.spin_limit, sp.persist,
+                  &s_thist[0][0], nd);
+    __syncthreads();
+    for (int e = threadIdx.x; e < nd * 256; e += kBlock) {
+        const unsigned v = (&s_thist[0][0])[e];
+        if (v) atomicAdd(&ctrl->hist[kDepthDigits + (e >> 8)][e & 255], v);
+    }
 }
 
 // TileBinner::bin over host-provided screen arrays (tile_binner_cpu.cpp:33-99):

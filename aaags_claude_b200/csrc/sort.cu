@@ -29,9 +29,13 @@ namespace {
 
 constexpr int kHistThreads = 512;
 
-__global__ void __launch_bounds__(kHistThreads) k_radix_hist(const unsigned long long* __restrict__ keys,
+// Digit histograms of digits [first, passes) (digit d = key bits 8d..8d+7)
+// into ctrl->hist[slot_base + d - first].
+template <typename K>
+__global__ void __launch_bounds__(kHistThreads) k_radix_hist(const K* __restrict__ keys,
                                                              unsigned long long capacity, int first, int passes,
-                                                             const unsigned long long* count, Control* ctrl) {
+                                                             int slot_base, const unsigned long long* count,
+                                                             Control* ctrl) {
     __shared__ unsigned s_h[kMaxPasses * 256];
     for (int e = first * 256 + threadIdx.x; e < passes * 256; e += blockDim.x) s_h[e] = 0;
     __syncthreads();
@@ -43,7 +47,7 @@ __global__ void __launch_bounds__(kHistThreads) k_radix_hist(const unsigned long
         const bool valid = i < P;
         const unsigned mask = __ballot_sync(0xffffffffu, valid);
         if (valid) {
-            const unsigned long long key = keys[i];
+            const K key = keys[i];
             for (int p = first; p < passes; p++) {
                 const unsigned d = (unsigned)(key >> (8 * p)) & 255u;
                 const unsigned peers = __match_any_sync(mask, d);
@@ -53,12 +57,13 @@ __global__ void __launch_bounds__(kHistThreads) k_radix_hist(const unsigned long
     }
     __syncthreads();
     for (int e = first * 256 + threadIdx.x; e < passes * 256; e += blockDim.x)
-        if (s_h[e]) atomicAdd(&ctrl->hist[e >> 8][e & 255], s_h[e]);
+        if (s_h[e]) atomicAdd(&ctrl->hist[slot_base + (e >> 8) - first][e & 255], s_h[e]);
 }
 
-// Shared memory of one onesweep CTA (dynamic, ~60 KB).
+// Shared memory of one onesweep CTA (dynamic; ~60 KB for 64-bit keys, ~44 KB for 32-bit).
+template <typename K>
 struct SweepShared {
-    unsigned long long keys[kSortTile];
+    K keys[kSortTile];
     unsigned vals[kSortTile];
     unsigned whist[kSortThreads / 32][256];   // per-warp digit counts, then per-warp prefixes
     unsigned long long gbase[256];            // global output offset of this tile's first key of digit d
@@ -84,35 +89,38 @@ __device__ __forceinline__ unsigned long long block_exclusive_scan64(unsigned lo
     return x - v + add;
 }
 
+// One pass over digit `pass` (key bits 8*pass..); `slot` selects the digit
+// histogram and CTA ticket in the control block.
+template <typename K>
 __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const StepParams* __restrict__ sp,
-                                                              const unsigned long long* __restrict__ kin,
+                                                              const K* __restrict__ kin,
                                                               const unsigned* __restrict__ vin,
-                                                              unsigned long long* __restrict__ kout,
+                                                              K* __restrict__ kout,
                                                               unsigned* __restrict__ vout,
-                                                              unsigned long long capacity, int pass,
+                                                              unsigned long long capacity, int pass, int slot,
                                                               unsigned long long* desc,
                                                               const unsigned long long* count,
                                                               Control* ctrl) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    SweepShared& sm = *reinterpret_cast<SweepShared*>(smem_raw);
+    SweepShared<K>& sm = *reinterpret_cast<SweepShared<K>*>(smem_raw);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int shift = 8 * pass;
     const unsigned long long P = min(*count, capacity);
-    if (tid == 0) sm.tile = (int)atomicAdd(&ctrl->tickets[1 + pass], 1u);
+    if (tid == 0) sm.tile = (int)atomicAdd(&ctrl->tickets[1 + slot], 1u);
     for (int e = tid; e < (kSortThreads / 32) * 256; e += kSortThreads) (&sm.whist[0][0])[e] = 0;
     __syncthreads();
     const int t = sm.tile;
     const unsigned long long base = (unsigned long long)t * kSortTile;
     if (base >= P) return;
 
-    unsigned long long key[kSortItems];
+    K key[kSortItems];
     unsigned val[kSortItems];
     unsigned rank[kSortItems];
 #pragma unroll
     for (int it = 0; it < kSortItems; it++) {
         const unsigned long long idx = base + (unsigned long long)(warp * 32 * kSortItems + it * 32 + lane);
         const bool valid = idx < P;
-        key[it] = valid ? kin[idx] : ~0ull;   // sentinel: digit 255, ranks after every real key
+        key[it] = valid ? kin[idx] : (K)~(K)0;   // sentinel: digit 255, ranks after every real key
         val[it] = valid ? vin[idx] : 0u;
     }
     const unsigned lt_mask = (1u << lane) - 1u;
@@ -138,7 +146,7 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const StepParams* 
     }
     // global offset of digit d for this tile: all smaller digits everywhere,
     // plus digit d in the tiles before this one (decoupled look-back)
-    const unsigned long long hist_d = ctrl->hist[pass][d];
+    const unsigned long long hist_d = ctrl->hist[slot][d];
     const unsigned long long digit_start = block_exclusive_scan64(hist_d, sm.scan);
     const unsigned long long tile_excl =
         lookback_exclusive_strided(desc, t, 256, (int)d, (unsigned long long)run, &ctrl->status, sp->spin_limit);
@@ -155,7 +163,7 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const StepParams* 
     __syncthreads();
     const int n_valid = (int)min((unsigned long long)kSortTile, P - base);
     for (int j = tid; j < n_valid; j += kSortThreads) {
-        const unsigned long long k = sm.keys[j];
+        const K k = sm.keys[j];
         const unsigned dd = (unsigned)(k >> shift) & 255u;
         const unsigned long long out = sm.gbase[dd] + (unsigned long long)(j - (int)sm.dprefix[dd]);
         kout[out] = k;
@@ -163,14 +171,18 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const StepParams* 
     }
 }
 
-__global__ void k_ranges(const unsigned long long* __restrict__ keys, unsigned long long capacity,
-                         unsigned* __restrict__ ranges, Control* ctrl) {
+__device__ __forceinline__ unsigned tile_of(unsigned long long key) { return (unsigned)(key >> 32); }
+__device__ __forceinline__ unsigned tile_of(unsigned key) { return key; }   // tile-only keys
+
+template <typename K>
+__global__ void k_ranges(const K* __restrict__ keys, unsigned long long capacity, unsigned* __restrict__ ranges,
+                         Control* ctrl) {
     const unsigned long long P = min(ctrl->total_pairs, capacity);
     const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
     for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < P; i += stride) {
-        const unsigned t = (unsigned)(keys[i] >> 32);
-        if (i == 0 || (unsigned)(keys[i - 1] >> 32) != t) ranges[2 * t] = (unsigned)i;
-        if (i == P - 1 || (unsigned)(keys[i + 1] >> 32) != t) ranges[2 * t + 1] = (unsigned)(i + 1);
+        const unsigned t = tile_of(keys[i]);
+        if (i == 0 || tile_of(keys[i - 1]) != t) ranges[2 * t] = (unsigned)i;
+        if (i == P - 1 || tile_of(keys[i + 1]) != t) ranges[2 * t + 1] = (unsigned)(i + 1);
     }
 }
 
@@ -217,51 +229,85 @@ cudaError_t launch_wait_selftest(cudaStream_t st, unsigned long long* desc2, uns
     return cudaGetLastError();
 }
 
-cudaError_t launch_radix_sort(cudaStream_t st, const StepParams* sp, int passes, unsigned long long capacity,
-                              unsigned long long* keys0, unsigned* vals0, unsigned long long* keys1,
-                              unsigned* vals1, unsigned long long* desc, unsigned long long desc_stride,
-                              Control* ctrl, int* which, cudaEvent_t after_hist, int first_pass,
-                              const unsigned long long* count) {
+namespace {
+
+// Digits [first, passes) of the keys, slots slot_base..; desc holds
+// (passes - first) * desc_stride zeroed descriptors.
+template <typename K>
+cudaError_t radix_sort_impl(cudaStream_t st, const StepParams* sp, int first, int passes, int slot_base,
+                            bool hist_done, unsigned long long capacity, K* keys0, unsigned* vals0, K* keys1,
+                            unsigned* vals1, unsigned long long* desc, unsigned long long desc_stride,
+                            Control* ctrl, int* which, cudaEvent_t after_hist, const unsigned long long* count) {
     *which = 0;
-    if (capacity == 0 || passes <= first_pass) return cudaSuccess;
+    if (capacity == 0 || passes <= first) return cudaSuccess;
     if (!count) count = &ctrl->total_pairs;
     static bool attr_set = false;
-    const int smem = (int)sizeof(SweepShared);
+    const int smem = (int)sizeof(SweepShared<K>);
     if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(k_onesweep, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaError_t e = cudaFuncSetAttribute(k_onesweep<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e != cudaSuccess) return e;
         attr_set = true;
     }
-    k_radix_hist<<<2 * 148, kHistThreads, 0, st>>>(keys0, capacity, first_pass, passes, count, ctrl);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
+    cudaError_t e;
+    if (!hist_done) {
+        k_radix_hist<K><<<2 * 148, kHistThreads, 0, st>>>(keys0, capacity, first, passes, slot_base, count, ctrl);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
     if (after_hist && (e = cudaEventRecord(after_hist, st)) != cudaSuccess) return e;
     const unsigned long long tiles = (capacity + kSortTile - 1) / kSortTile;
-    unsigned long long* kin = keys0;
+    K* kin = keys0;
     unsigned* vin = vals0;
-    unsigned long long* kout = keys1;
+    K* kout = keys1;
     unsigned* vout = vals1;
-    for (int p = first_pass; p < passes; p++) {
-        k_onesweep<<<(unsigned)tiles, kSortThreads, smem, st>>>(sp, kin, vin, kout, vout, capacity, p,
-                                                                desc + (unsigned long long)p * desc_stride,
-                                                                count, ctrl);
-        e = cudaGetLastError();
-        if (e != cudaSuccess) return e;
-        unsigned long long* tk = kin;
+    for (int p = first; p < passes; p++) {
+        const int slot = slot_base + p - first;
+        k_onesweep<K><<<(unsigned)tiles, kSortThreads, smem, st>>>(
+            sp, kin, vin, kout, vout, capacity, p, slot, desc + (unsigned long long)(p - first) * desc_stride, count,
+            ctrl);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        K* tk = kin;
         kin = kout;
         kout = tk;
         unsigned* tv = vin;
         vin = vout;
         vout = tv;
     }
-    *which = (passes - first_pass) & 1;
+    *which = (passes - first) & 1;
     return cudaSuccess;
+}
+
+}  // namespace
+
+cudaError_t launch_radix_sort(cudaStream_t st, const StepParams* sp, int passes, unsigned long long capacity,
+                              unsigned long long* keys0, unsigned* vals0, unsigned long long* keys1,
+                              unsigned* vals1, unsigned long long* desc, unsigned long long desc_stride,
+                              Control* ctrl, int* which, cudaEvent_t after_hist, int first_pass,
+                              const unsigned long long* count) {
+    // 64-bit keys: digit p uses slot p, descriptors from desc + p * desc_stride
+    return radix_sort_impl<unsigned long long>(st, sp, first_pass, passes, first_pass, false, capacity, keys0,
+                                               vals0, keys1, vals1, desc + (unsigned long long)first_pass * desc_stride,
+                                               desc_stride, ctrl, which, after_hist, count);
+}
+
+cudaError_t launch_radix_sort32(cudaStream_t st, const StepParams* sp, int digits, int slot_base, bool hist_done,
+                                unsigned long long capacity, unsigned* keys0, unsigned* vals0, unsigned* keys1,
+                                unsigned* vals1, unsigned long long* desc, unsigned long long desc_stride,
+                                Control* ctrl, int* which, cudaEvent_t after_hist) {
+    return radix_sort_impl<unsigned>(st, sp, 0, digits, slot_base, hist_done, capacity, keys0, vals0, keys1, vals1,
+                                     desc, desc_stride, ctrl, which, after_hist, nullptr);
 }
 
 cudaError_t launch_tile_ranges(cudaStream_t st, unsigned long long capacity, const unsigned long long* keys_sorted,
                                unsigned* ranges, Control* ctrl) {
     if (capacity == 0) return cudaSuccess;
     k_ranges<<<4 * 148, 256, 0, st>>>(keys_sorted, capacity, ranges, ctrl);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tile_ranges32(cudaStream_t st, unsigned long long capacity, const unsigned* tiles_sorted,
+                                 unsigned* ranges, Control* ctrl) {
+    if (capacity == 0) return cudaSuccess;
+    k_ranges<<<4 * 148, 256, 0, st>>>(tiles_sorted, capacity, ranges, ctrl);
     return cudaGetLastError();
 }
 
