@@ -29,6 +29,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=o
 # per-source extra flags
 SOURCES = {
     "plain.cu": ["-fmad=false", "-prec-div=true", "-prec-sqrt=true"],
+    "raster_bwd.cu": [],   # gradients: FMA contraction allowed
     "sort.cu": [],
     "sort_static.cu": [],
     "capi.cu": [],

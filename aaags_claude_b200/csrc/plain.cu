@@ -16,10 +16,7 @@
 //   k_raster_fwd    one CTA per 16x16 tile, one thread per pixel; pairs are
 //                   gathered in batches of 256 into shared memory; CTA-wide
 //                   early exit once every pixel saturated.  Optional fused L1.
-//   k_raster_bwd    reverse traversal from each pixel's last contributor with
-//                   transmittance recovered from the stored T_final; per
-//                   Gaussian the warp's 32 pixel contributions are shuffle-
-//                   reduced and one lane issues the atomics.
+//   (k_raster_bwd lives in raster_bwd.cu, compiled with FMA contraction.)
 //   k_preprocess_bwd  the full per-Gaussian adjoint chain, fused with Adam.
 #include <cuda_runtime.h>
 #include <cstddef>
@@ -27,12 +24,10 @@
 
 #include "common.cuh"
 #include "kernels.cuh"
+#include "raster_common.cuh"
 
 namespace gs3d {
 namespace {
-
-constexpr float kAlphaMin = 1.0f / 255.0f;   // rasterizer_cpu.cpp:150
-constexpr float kTMin = 0.0001f;             // rasterizer_cpu.cpp:165
 
 // ---------------- reference math (float, reference operation order) ----------------
 
@@ -60,7 +55,6 @@ __device__ __forceinline__ void tile_rect(float px, float py, int r, int gx, int
     rmx[1] = min(gy, max(0, (int)((py + fr + fth - 1.0f) / fth)));
 }
 
-__device__ __forceinline__ float fmin_ref(float a, float b) { return (b < a) ? b : a; }  // std::min
 __device__ __forceinline__ float fmax_ref(float a, float b) { return (a < b) ? b : a; }  // std::max
 
 // math_utils.cpp:38-42
@@ -239,43 +233,6 @@ __device__ __forceinline__ int blend_decision(float power, float o, float T, flo
     test_T = T * (1.0f - alpha);
     if (test_T < kTMin) return 2;
     return 1;
-}
-
-// A power below this bound gives alpha = o * exp(power) < 1/255 for certain
-// (ln(1/(255 o)) less a margin far above the rounding of logf / expf), so the
-// blend loops skip such Gaussians without evaluating exp; the skip they take
-// is the one blend_decision / alpha_accept would take.
-__device__ __forceinline__ float skip_threshold(float o) { return logf(kAlphaMin / o) - 1e-3f; }
-
-// Axis-aligned box (xmin, xmax, ymin, ymax) in pixels outside of which the
-// Gaussian's power is below skip_threshold: the ellipse
-// d^T C d <= -2 thr has half extents sqrt(-2 thr * Sigma_xx), sqrt(-2 thr *
-// Sigma_yy) with Sigma = C^-1, widened by one pixel for rounding.  A warp
-// whose pixels all lie outside it skips the Gaussian without evaluating it.
-__device__ __forceinline__ float4 skip_box(float4 r0, float4 r1, float thr) {
-    const float t2 = -2.0f * thr;
-    const float det = r0.z * r1.x - r0.w * r0.w;   // conic a c - b^2
-    if (!(t2 > 0.0f)) return make_float4(1e30f, -1e30f, 1e30f, -1e30f);     // never reaches alpha 1/255
-    if (!(det > 0.0f)) return make_float4(-1e30f, 1e30f, -1e30f, 1e30f);    // not positive definite: no culling
-    const float ex = sqrtf(t2 * r1.x / det) + 1.0f;
-    const float ey = sqrtf(t2 * r0.z / det) + 1.0f;
-    return make_float4(r0.x - ex, r0.x + ex, r0.y - ey, r0.y + ey);
-}
-
-__device__ __forceinline__ bool box_misses(float4 b, float x0, float x1, float y0, float y1) {
-    return b.y < x0 || b.x > x1 || b.w < y0 || b.z > y1;
-}
-
-// The alpha-only decision of the backward (the forward's last-contributor
-// index already encodes the stop); agrees with blend_decision's skip and
-// yields the same alpha and exp for accepted Gaussians.
-__device__ __forceinline__ bool alpha_accept(float power, float o, float& alpha, float& e) {
-    e = expf(power);
-    alpha = fmin_ref(0.99f, o * e);
-    if (alpha < kAlphaMin - 1e-8f) return false;
-    e = exp_ref(power);
-    alpha = fmin_ref(0.99f, o * e);
-    return !(alpha < kAlphaMin);
 }
 
 // ---------------- per-Gaussian forward (preprocessor_cpu.cpp:186-265) ----------------
@@ -635,7 +592,7 @@ __global__ void __launch_bounds__(kBlock) k_raster_fwd(const StepParams* __restr
                 const float4 a = s_r0[k];
                 const float dx = a.x - fx, dy = a.y - fy;
                 const float4 c = s_r1[k];
-                const float power = -0.5f * (a.z * dx * dx + c.x * dy * dy) - a.w * dx * dy;
+                const float power = power_rn(a, c, dx, dy);
                 if (power < s_thr[k] || power > 0.0f) continue;
                 float alpha, e, test_T;
                 const int dec = blend_decision(power, c.y, T, alpha, e, test_T);
@@ -685,188 +642,6 @@ __global__ void __launch_bounds__(kBlock) k_raster_fwd(const StepParams* __restr
             for (int w = 0; w < kBlock / 32; w++) t += s_loss[w];
             atomicAdd(&ctrl->loss_sum, t);
         }
-    }
-}
-
-__device__ __forceinline__ float warp_sum(float v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
-
-// Sums eight values over the 32 lanes of a warp with 9 shuffles instead of 40:
-// each butterfly stage sends half of the values it still holds to its partner,
-// so the set of values a lane carries halves at every step.  On return lane l
-// holds the warp total of value ((l>>4)&1)*4 + ((l>>3)&1)*2 + ((l>>2)&1)
-// (*idx); lanes with the same bits 2..4 hold the same total.
-__device__ __forceinline__ float warp_sum8(const float v[8], int* idx) {
-    const unsigned lane = threadIdx.x & 31;
-    const bool h16 = lane & 16, h8 = lane & 8, h4 = lane & 4;
-    float a[4];
-#pragma unroll
-    for (int i = 0; i < 4; i++) {
-        const float send = h16 ? v[i] : v[i + 4];
-        const float keep = h16 ? v[i + 4] : v[i];
-        a[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
-    }
-    float b[2];
-#pragma unroll
-    for (int i = 0; i < 2; i++) {
-        const float send = h8 ? a[i] : a[i + 2];
-        const float keep = h8 ? a[i + 2] : a[i];
-        b[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
-    }
-    const float send = h4 ? b[0] : b[1];
-    float c = (h4 ? b[1] : b[0]) + __shfl_xor_sync(0xffffffffu, send, 4);
-    c += __shfl_xor_sync(0xffffffffu, c, 2);
-    c += __shfl_xor_sync(0xffffffffu, c, 1);
-    *idx = (h16 ? 4 : 0) + (h8 ? 2 : 0) + (h4 ? 1 : 0);
-    return c;
-}
-
-// Rasterizer backward (rasterizer_backward_cpu.cpp:20-133): back-to-front
-// over each pixel's contributors, transmittance recovered by division from
-// T_final instead of a replayed per-pixel list.  Per Gaussian of a batch, the
-// 32 pixels of a warp are summed with warp_sum8, the 8 warps of the tile meet
-// in shared-memory accumulators, and each Gaussian gets one set of global
-// atomics per tile.
-template <bool FROM_SIGN>
-__global__ void __launch_bounds__(kBlock) k_raster_bwd(const StepParams* __restrict__ spp,
-                                                       const unsigned* __restrict__ ranges,
-                                                       const unsigned* __restrict__ order,
-                                                       const unsigned* __restrict__ vals, ScreenPtrs s,
-                                                       PixelPtrs px, RGradPtrs g, Control* ctrl) {
-    __shared__ float4 s_r0[kBlock];
-    __shared__ float4 s_r1[kBlock];
-    __shared__ float s_b[kBlock];
-    __shared__ unsigned s_idx[kBlock];
-    __shared__ float s_thr[kBlock];
-    __shared__ float4 s_box[kBlock];
-    __shared__ float s_acc[9][kBlock];   // r, g, b, opacity, mean.x, mean.y, conic a, b, c
-    __shared__ unsigned s_maxlast;
-    const StepParams& sp = *spp;
-    if (FROM_SIGN && ((ctrl->status & kStatusOverflow) || sp.persist->sticky_overflow)) return;
-    const int W = sp.cam.width, H = sp.cam.height;
-    const int tile = order ? (int)order[blockIdx.x] : (int)blockIdx.x;
-    const int tx = tile % sp.grid_x, ty = tile / sp.grid_x;
-    const int x = tx * kTile + (threadIdx.x & (kTile - 1));
-    const int y = ty * kTile + (threadIdx.x >> 4);
-    const bool inside = x < W && y < H;
-    const unsigned rs = ranges[2 * tile];
-    const float fx = (float)x, fy = (float)y;
-    const int pix = y * W + x;
-    float T = 0.0f, dC0 = 0.0f, dC1 = 0.0f, dC2 = 0.0f;
-    unsigned last = 0;
-    if (inside) {
-        T = px.T_final[pix];
-        last = px.last_j[pix];
-        if (FROM_SIGN) {
-            const unsigned sg = px.dsign[pix];
-            const float inv_n = sp.inv_n;
-            dC0 = (sg & 1u) ? inv_n : ((sg & 2u) ? -inv_n : 0.0f);
-            dC1 = (sg & 4u) ? inv_n : ((sg & 8u) ? -inv_n : 0.0f);
-            dC2 = (sg & 16u) ? inv_n : ((sg & 32u) ? -inv_n : 0.0f);
-        } else {
-            dC0 = px.d_image[3 * pix];
-            dC1 = px.d_image[3 * pix + 1];
-            dC2 = px.d_image[3 * pix + 2];
-        }
-    }
-    float acc0 = sp.cfg.bg_color[0], acc1 = sp.cfg.bg_color[1], acc2 = sp.cfg.bg_color[2];
-    if (threadIdx.x == 0) s_maxlast = 0;
-    __syncthreads();
-    if (last) atomicMax(&s_maxlast, last);
-    __syncthreads();
-    const unsigned maxlast = s_maxlast;
-    if (maxlast <= rs) return;
-    const unsigned lane = threadIdx.x & 31;
-    const unsigned wlast = __reduce_max_sync(0xffffffffu, last);
-    const float wx0 = (float)(tx * kTile), wx1 = wx0 + (float)(kTile - 1);
-    const float wy0 = (float)(ty * kTile + 2 * (threadIdx.x >> 5)), wy1 = wy0 + 1.0f;
-    // batches [bs, be) walked from the back; the first one ends at maxlast
-    for (unsigned be = maxlast; be > rs;) {
-        const unsigned bs = (be - rs > (unsigned)kBlock) ? be - kBlock : rs;
-        const unsigned j = bs + threadIdx.x;
-        if (j < be) {
-            const unsigned gi = vals[j];
-            const float4 r0 = s.rec0[gi];
-            const float4 r1 = s.rec1[gi];
-            const float thr = skip_threshold(r1.y);
-            s_idx[threadIdx.x] = gi;
-            s_r0[threadIdx.x] = r0;
-            s_r1[threadIdx.x] = r1;
-            s_b[threadIdx.x] = s.col_b[gi];
-            s_thr[threadIdx.x] = thr;
-            s_box[threadIdx.x] = skip_box(r0, r1, thr);
-        }
-#pragma unroll
-        for (int v = 0; v < 9; v++) s_acc[v][threadIdx.x] = 0.0f;
-        __syncthreads();
-        // this warp only needs the entries below its own last contributor
-        const int kstart = (int)(min(be, wlast) - min(bs, wlast)) - 1;
-        for (int k = kstart; k >= 0; k--) {
-            if (box_misses(s_box[k], wx0, wx1, wy0, wy1)) continue;   // warp-uniform
-            const unsigned jj = bs + (unsigned)k;
-            bool contrib = false;
-            float gv[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-            float g_cc = 0.f;
-            if (jj < last) {
-                const float4 a = s_r0[k];
-                const float4 c = s_r1[k];
-                const float dx = a.x - fx, dy = a.y - fy;
-                const float power = -0.5f * (a.z * dx * dx + c.x * dy * dy) - a.w * dx * dy;
-                float alpha, ep;
-                if (!(power < s_thr[k]) && !(power > 0.0f) && alpha_accept(power, c.y, alpha, ep)) {
-                    contrib = true;
-                    const float cb = s_b[k];
-                    const float oma = 1.0f - alpha;
-                    const float Ti = (oma > 1e-6f) ? T / oma : 0.0f;
-                    gv[0] = alpha * Ti * dC0;
-                    gv[1] = alpha * Ti * dC1;
-                    gv[2] = alpha * Ti * dC2;
-                    float d_alpha = 0.0f;
-                    d_alpha += Ti * (c.z - acc0) * dC0;
-                    d_alpha += Ti * (c.w - acc1) * dC1;
-                    d_alpha += Ti * (cb - acc2) * dC2;
-                    acc0 = alpha * c.z + oma * acc0;
-                    acc1 = alpha * c.w + oma * acc1;
-                    acc2 = alpha * cb + oma * acc2;
-                    T = Ti;
-                    float d_power = 0.0f;
-                    if (alpha < 0.99f) {
-                        d_power = d_alpha * c.y * ep;
-                        gv[3] = d_alpha * ep;
-                    }
-                    gv[4] = d_power * (-a.z * dx - a.w * dy);
-                    gv[5] = d_power * (-c.x * dy - a.w * dx);
-                    gv[6] = d_power * (-0.5f * dx * dx);
-                    gv[7] = d_power * (-dx * dy);
-                    g_cc = d_power * (-0.5f * dy * dy);
-                }
-            }
-            if (__any_sync(0xffffffffu, contrib)) {
-                int idx;
-                const float s8 = warp_sum8(gv, &idx);
-                const float s9 = warp_sum(g_cc);
-                if ((lane & 3) == 0 && s8 != 0.0f) atomicAdd(&s_acc[idx][k], s8);
-                if (lane == 1 && s9 != 0.0f) atomicAdd(&s_acc[8][k], s9);
-            }
-        }
-        __syncthreads();
-        if (j < be) {
-            // thread t flushes batch entry t, which it also zeroes for the next batch
-            const unsigned gi = s_idx[threadIdx.x];
-            float* const dst[9] = {&g.drgb[3 * gi], &g.drgb[3 * gi + 1], &g.drgb[3 * gi + 2], &g.dop[gi],
-                                   &g.dm2[2 * gi], &g.dm2[2 * gi + 1], &g.dcon[3 * gi], &g.dcon[3 * gi + 1],
-                                   &g.dcon[3 * gi + 2]};
-#pragma unroll
-            for (int v = 0; v < 9; v++) {
-                const float a = s_acc[v][threadIdx.x];
-                if (a != 0.0f) atomicAdd(dst[v], a);
-            }
-        }
-        __syncthreads();
-        be = bs;
     }
 }
 
@@ -1531,15 +1306,6 @@ cudaError_t launch_raster_fwd_plain(cudaStream_t st, const StepParams* sp, int n
     if (num_tiles <= 0) return cudaSuccess;
     if (fused_loss) k_raster_fwd<true><<<num_tiles, kBlock, 0, st>>>(sp, ranges, order, vals, s, px, ctrl);
     else k_raster_fwd<false><<<num_tiles, kBlock, 0, st>>>(sp, ranges, order, vals, s, px, ctrl);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_raster_bwd_plain(cudaStream_t st, const StepParams* sp, int num_tiles, bool from_sign,
-                                    const unsigned* ranges, const unsigned* order, const unsigned* vals,
-                                    ScreenPtrs s, PixelPtrs px, RGradPtrs g, Control* ctrl) {
-    if (num_tiles <= 0) return cudaSuccess;
-    if (from_sign) k_raster_bwd<true><<<num_tiles, kBlock, 0, st>>>(sp, ranges, order, vals, s, px, g, ctrl);
-    else k_raster_bwd<false><<<num_tiles, kBlock, 0, st>>>(sp, ranges, order, vals, s, px, g, ctrl);
     return cudaGetLastError();
 }
 

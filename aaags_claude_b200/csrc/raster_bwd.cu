@@ -1,0 +1,193 @@
+// raster_bwd.cu -- Rasterizer backward (rasterizer_backward_cpu.cpp:20-133)
+// for sm_100a, plain FP32 form.
+//
+// Unlike plain.cu this file is compiled with FMA contraction: its outputs are
+// gradients, held to a relative tolerance, not bit-exact screen data.  What
+// must match the forward exactly -- which (pixel, Gaussian) pairs blended --
+// is decided on power_rn (explicit rounding, identical to the forward's value)
+// and on alpha_accept_fast below, which agrees with the forward's exact test.
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+#include "kernels.cuh"
+#include "raster_common.cuh"
+
+namespace gs3d {
+namespace {
+
+// alpha = min(0.99, o exp(power)) and whether it reaches 1/255, on the fast
+// expf.  expf is within a few ulp of exp, so o*expf(power) decides both the
+// 1/255 threshold and the 0.99 clamp exactly unless it lies within a relative
+// 2e-6 (about 16 ulp) of either bound; there the exact exp (exp_ref, the
+// forward's) is recomputed.  Accepted unclamped pairs keep the fast alpha,
+// a few ulp from the forward's: the transmittance recovered from it and the
+// gradients stay within their tolerance.
+__device__ __forceinline__ bool alpha_accept_fast(float power, float o, float& alpha, float& e) {
+    e = expf(power);
+    float a = o * e;
+    if (fabsf(a - kAlphaMin) <= 2e-6f * kAlphaMin || fabsf(a - 0.99f) <= 2e-6f) {
+        e = exp_ref(power);
+        a = o * e;
+    }
+    alpha = fmin_ref(0.99f, a);
+    return !(alpha < kAlphaMin);
+}
+
+// Rasterizer backward (rasterizer_backward_cpu.cpp:20-133): back-to-front
+// over each pixel's contributors, transmittance recovered by division from
+// T_final instead of a replayed per-pixel list.  Per Gaussian of a batch, the
+// 32 pixels of a warp are summed with warp_sum8, the 8 warps of the tile meet
+// in shared-memory accumulators, and each Gaussian gets one set of global
+// atomics per tile.
+template <bool FROM_SIGN>
+__global__ void __launch_bounds__(kBlock) k_raster_bwd(const StepParams* __restrict__ spp,
+                                                       const unsigned* __restrict__ ranges,
+                                                       const unsigned* __restrict__ order,
+                                                       const unsigned* __restrict__ vals, ScreenPtrs s,
+                                                       PixelPtrs px, RGradPtrs g, Control* ctrl) {
+    __shared__ float4 s_r0[kBlock];
+    __shared__ float4 s_r1[kBlock];
+    __shared__ float s_b[kBlock];
+    __shared__ unsigned s_idx[kBlock];
+    __shared__ float s_thr[kBlock];
+    __shared__ float4 s_box[kBlock];
+    __shared__ float s_acc[9][kBlock];   // r, g, b, opacity, mean.x, mean.y, conic a, b, c
+    __shared__ unsigned s_maxlast;
+    const StepParams& sp = *spp;
+    if (FROM_SIGN && ((ctrl->status & kStatusOverflow) || sp.persist->sticky_overflow)) return;
+    const int W = sp.cam.width, H = sp.cam.height;
+    const int tile = order ? (int)order[blockIdx.x] : (int)blockIdx.x;
+    const int tx = tile % sp.grid_x, ty = tile / sp.grid_x;
+    const int x = tx * kTile + (threadIdx.x & (kTile - 1));
+    const int y = ty * kTile + (threadIdx.x >> 4);
+    const bool inside = x < W && y < H;
+    const unsigned rs = ranges[2 * tile];
+    const float fx = (float)x, fy = (float)y;
+    const int pix = y * W + x;
+    float T = 0.0f, dC0 = 0.0f, dC1 = 0.0f, dC2 = 0.0f;
+    unsigned last = 0;
+    if (inside) {
+        T = px.T_final[pix];
+        last = px.last_j[pix];
+        if (FROM_SIGN) {
+            const unsigned sg = px.dsign[pix];
+            const float inv_n = sp.inv_n;
+            dC0 = (sg & 1u) ? inv_n : ((sg & 2u) ? -inv_n : 0.0f);
+            dC1 = (sg & 4u) ? inv_n : ((sg & 8u) ? -inv_n : 0.0f);
+            dC2 = (sg & 16u) ? inv_n : ((sg & 32u) ? -inv_n : 0.0f);
+        } else {
+            dC0 = px.d_image[3 * pix];
+            dC1 = px.d_image[3 * pix + 1];
+            dC2 = px.d_image[3 * pix + 2];
+        }
+    }
+    float acc0 = sp.cfg.bg_color[0], acc1 = sp.cfg.bg_color[1], acc2 = sp.cfg.bg_color[2];
+    if (threadIdx.x == 0) s_maxlast = 0;
+    __syncthreads();
+    if (last) atomicMax(&s_maxlast, last);
+    __syncthreads();
+    const unsigned maxlast = s_maxlast;
+    if (maxlast <= rs) return;
+    const unsigned lane = threadIdx.x & 31;
+    const unsigned wlast = __reduce_max_sync(0xffffffffu, last);
+    const float wx0 = (float)(tx * kTile), wx1 = wx0 + (float)(kTile - 1);
+    const float wy0 = (float)(ty * kTile + 2 * (threadIdx.x >> 5)), wy1 = wy0 + 1.0f;
+    // batches [bs, be) walked from the back; the first one ends at maxlast
+    for (unsigned be = maxlast; be > rs;) {
+        const unsigned bs = (be - rs > (unsigned)kBlock) ? be - kBlock : rs;
+        const unsigned j = bs + threadIdx.x;
+        if (j < be) {
+            const unsigned gi = vals[j];
+            const float4 r0 = s.rec0[gi];
+            const float4 r1 = s.rec1[gi];
+            const float thr = skip_threshold(r1.y);
+            s_idx[threadIdx.x] = gi;
+            s_r0[threadIdx.x] = r0;
+            s_r1[threadIdx.x] = r1;
+            s_b[threadIdx.x] = s.col_b[gi];
+            s_thr[threadIdx.x] = thr;
+            s_box[threadIdx.x] = skip_box(r0, r1, thr);
+        }
+#pragma unroll
+        for (int v = 0; v < 9; v++) s_acc[v][threadIdx.x] = 0.0f;
+        __syncthreads();
+        // this warp only needs the entries below its own last contributor
+        const int kstart = (int)(min(be, wlast) - min(bs, wlast)) - 1;
+        for (int k = kstart; k >= 0; k--) {
+            if (box_misses(s_box[k], wx0, wx1, wy0, wy1)) continue;   // warp-uniform
+            const unsigned jj = bs + (unsigned)k;
+            bool contrib = false;
+            float gv[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            float g_cc = 0.f;
+            if (jj < last) {
+                const float4 a = s_r0[k];
+                const float4 c = s_r1[k];
+                const float dx = a.x - fx, dy = a.y - fy;
+                const float power = power_rn(a, c, dx, dy);
+                float alpha, ep;
+                if (!(power < s_thr[k]) && !(power > 0.0f) && alpha_accept_fast(power, c.y, alpha, ep)) {
+                    contrib = true;
+                    const float cb = s_b[k];
+                    const float oma = 1.0f - alpha;
+                    const float Ti = (oma > 1e-6f) ? T / oma : 0.0f;
+                    gv[0] = alpha * Ti * dC0;
+                    gv[1] = alpha * Ti * dC1;
+                    gv[2] = alpha * Ti * dC2;
+                    float d_alpha = 0.0f;
+                    d_alpha += Ti * (c.z - acc0) * dC0;
+                    d_alpha += Ti * (c.w - acc1) * dC1;
+                    d_alpha += Ti * (cb - acc2) * dC2;
+                    acc0 = alpha * c.z + oma * acc0;
+                    acc1 = alpha * c.w + oma * acc1;
+                    acc2 = alpha * cb + oma * acc2;
+                    T = Ti;
+                    float d_power = 0.0f;
+                    if (alpha < 0.99f) {
+                        d_power = d_alpha * c.y * ep;
+                        gv[3] = d_alpha * ep;
+                    }
+                    gv[4] = d_power * (-a.z * dx - a.w * dy);
+                    gv[5] = d_power * (-c.x * dy - a.w * dx);
+                    gv[6] = d_power * (-0.5f * dx * dx);
+                    gv[7] = d_power * (-dx * dy);
+                    g_cc = d_power * (-0.5f * dy * dy);
+                }
+            }
+            if (__any_sync(0xffffffffu, contrib)) {
+                int idx;
+                const float s8 = warp_sum8(gv, &idx);
+                const float s9 = warp_sum(g_cc);
+                if ((lane & 3) == 0 && s8 != 0.0f) atomicAdd(&s_acc[idx][k], s8);
+                if (lane == 1 && s9 != 0.0f) atomicAdd(&s_acc[8][k], s9);
+            }
+        }
+        __syncthreads();
+        if (j < be) {
+            // thread t flushes batch entry t, which it also zeroes for the next batch
+            const unsigned gi = s_idx[threadIdx.x];
+            float* const dst[9] = {&g.drgb[3 * gi], &g.drgb[3 * gi + 1], &g.drgb[3 * gi + 2], &g.dop[gi],
+                                   &g.dm2[2 * gi], &g.dm2[2 * gi + 1], &g.dcon[3 * gi], &g.dcon[3 * gi + 1],
+                                   &g.dcon[3 * gi + 2]};
+#pragma unroll
+            for (int v = 0; v < 9; v++) {
+                const float a = s_acc[v][threadIdx.x];
+                if (a != 0.0f) atomicAdd(dst[v], a);
+            }
+        }
+        __syncthreads();
+        be = bs;
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_raster_bwd_plain(cudaStream_t st, const StepParams* sp, int num_tiles, bool from_sign,
+                                    const unsigned* ranges, const unsigned* order, const unsigned* vals,
+                                    ScreenPtrs s, PixelPtrs px, RGradPtrs g, Control* ctrl) {
+    if (num_tiles <= 0) return cudaSuccess;
+    if (from_sign) k_raster_bwd<true><<<num_tiles, kBlock, 0, st>>>(sp, ranges, order, vals, s, px, g, ctrl);
+    else k_raster_bwd<false><<<num_tiles, kBlock, 0, st>>>(sp, ranges, order, vals, s, px, g, ctrl);
+    return cudaGetLastError();
+}
+
+}  // namespace gs3d
