@@ -35,122 +35,144 @@ __device__ __forceinline__ bool alpha_accept_fast(float power, float o, float& a
 
 // Rasterizer backward (rasterizer_backward_cpu.cpp:20-133): back-to-front
 // over each pixel's contributors, transmittance recovered by division from
-// T_final instead of a replayed per-pixel list.  Per Gaussian of a batch, the
-// 32 pixels of a warp are summed with warp_sum8, the 8 warps of the tile meet
-// in shared-memory accumulators, and each Gaussian gets one set of global
-// atomics per tile.
+// T_final instead of a replayed per-pixel list.  One CTA of 128 threads per
+// 16x16 tile, two pixels per thread: warp w owns the 16x4 strip of rows
+// 4w..4w+3, a thread the pixels (x, 4w + lane/16) and (x, 4w + 2 + lane/16).
+// Per Gaussian of a batch a thread adds its two pixels' contributions, the
+// warp sums its 64 pixels with warp_sum8 + warp_sum, the 4 warps meet in
+// shared-memory accumulators and each Gaussian gets one set of global atomics
+// per tile.
+constexpr int kBwdThreads = 128;
+constexpr int kBwdBatch = 256;
+
 template <bool FROM_SIGN>
-__global__ void __launch_bounds__(kBlock) k_raster_bwd(const StepParams* __restrict__ spp,
-                                                       const unsigned* __restrict__ ranges,
-                                                       const unsigned* __restrict__ order,
-                                                       const unsigned* __restrict__ vals, ScreenPtrs s,
-                                                       PixelPtrs px, RGradPtrs g, Control* ctrl) {
-    __shared__ float4 s_r0[kBlock];
-    __shared__ float4 s_r1[kBlock];
-    __shared__ float s_b[kBlock];
-    __shared__ unsigned s_idx[kBlock];
-    __shared__ float s_thr[kBlock];
-    __shared__ float4 s_box[kBlock];
-    __shared__ float s_acc[9][kBlock];   // r, g, b, opacity, mean.x, mean.y, conic a, b, c
+__global__ void __launch_bounds__(kBwdThreads) k_raster_bwd(const StepParams* __restrict__ spp,
+                                                            const unsigned* __restrict__ ranges,
+                                                            const unsigned* __restrict__ order,
+                                                            const unsigned* __restrict__ vals, ScreenPtrs s,
+                                                            PixelPtrs px, RGradPtrs g, Control* ctrl) {
+    __shared__ float4 s_r0[kBwdBatch];
+    __shared__ float4 s_r1[kBwdBatch];
+    __shared__ float s_b[kBwdBatch];
+    __shared__ unsigned s_idx[kBwdBatch];
+    __shared__ float s_thr[kBwdBatch];
+    __shared__ float4 s_box[kBwdBatch];
+    __shared__ float s_acc[9][kBwdBatch];   // r, g, b, opacity, mean.x, mean.y, conic a, b, c
     __shared__ unsigned s_maxlast;
     const StepParams& sp = *spp;
     if (FROM_SIGN && ((ctrl->status & kStatusOverflow) || sp.persist->sticky_overflow)) return;
     const int W = sp.cam.width, H = sp.cam.height;
     const int tile = order ? (int)order[blockIdx.x] : (int)blockIdx.x;
     const int tx = tile % sp.grid_x, ty = tile / sp.grid_x;
-    const int x = tx * kTile + (threadIdx.x & (kTile - 1));
-    const int y = ty * kTile + (threadIdx.x >> 4);
-    const bool inside = x < W && y < H;
+    const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int x = tx * kTile + (int)(lane & 15);
+    const int ybase = ty * kTile + 4 * (int)warp + (int)(lane >> 4);
     const unsigned rs = ranges[2 * tile];
-    const float fx = (float)x, fy = (float)y;
-    const int pix = y * W + x;
-    float T = 0.0f, dC0 = 0.0f, dC1 = 0.0f, dC2 = 0.0f;
-    unsigned last = 0;
-    if (inside) {
-        T = px.T_final[pix];
-        last = px.last_j[pix];
-        if (FROM_SIGN) {
-            const unsigned sg = px.dsign[pix];
-            const float inv_n = sp.inv_n;
-            dC0 = (sg & 1u) ? inv_n : ((sg & 2u) ? -inv_n : 0.0f);
-            dC1 = (sg & 4u) ? inv_n : ((sg & 8u) ? -inv_n : 0.0f);
-            dC2 = (sg & 16u) ? inv_n : ((sg & 32u) ? -inv_n : 0.0f);
-        } else {
-            dC0 = px.d_image[3 * pix];
-            dC1 = px.d_image[3 * pix + 1];
-            dC2 = px.d_image[3 * pix + 2];
+    const float fx = (float)x;
+    float fy[2], T[2], dC[2][3], acc[2][3];
+    unsigned last[2];
+#pragma unroll
+    for (int p = 0; p < 2; p++) {
+        const int y = ybase + 2 * p;
+        fy[p] = (float)y;
+        T[p] = 0.0f;
+        last[p] = 0;
+        dC[p][0] = dC[p][1] = dC[p][2] = 0.0f;
+        if (x < W && y < H) {
+            const int pix = y * W + x;
+            T[p] = px.T_final[pix];
+            last[p] = px.last_j[pix];
+            if (FROM_SIGN) {
+                const unsigned sg = px.dsign[pix];
+                const float inv_n = sp.inv_n;
+                dC[p][0] = (sg & 1u) ? inv_n : ((sg & 2u) ? -inv_n : 0.0f);
+                dC[p][1] = (sg & 4u) ? inv_n : ((sg & 8u) ? -inv_n : 0.0f);
+                dC[p][2] = (sg & 16u) ? inv_n : ((sg & 32u) ? -inv_n : 0.0f);
+            } else {
+                dC[p][0] = px.d_image[3 * pix];
+                dC[p][1] = px.d_image[3 * pix + 1];
+                dC[p][2] = px.d_image[3 * pix + 2];
+            }
         }
+#pragma unroll
+        for (int ch = 0; ch < 3; ch++) acc[p][ch] = sp.cfg.bg_color[ch];
     }
-    float acc0 = sp.cfg.bg_color[0], acc1 = sp.cfg.bg_color[1], acc2 = sp.cfg.bg_color[2];
     if (threadIdx.x == 0) s_maxlast = 0;
     __syncthreads();
-    if (last) atomicMax(&s_maxlast, last);
+    const unsigned mylast = max(last[0], last[1]);
+    if (mylast) atomicMax(&s_maxlast, mylast);
     __syncthreads();
     const unsigned maxlast = s_maxlast;
     if (maxlast <= rs) return;
-    const unsigned lane = threadIdx.x & 31;
-    const unsigned wlast = __reduce_max_sync(0xffffffffu, last);
+    const unsigned wlast = __reduce_max_sync(0xffffffffu, mylast);
     const float wx0 = (float)(tx * kTile), wx1 = wx0 + (float)(kTile - 1);
-    const float wy0 = (float)(ty * kTile + 2 * (threadIdx.x >> 5)), wy1 = wy0 + 1.0f;
+    const float wy0 = (float)(ty * kTile + 4 * (int)warp), wy1 = wy0 + 3.0f;
     // batches [bs, be) walked from the back; the first one ends at maxlast
     for (unsigned be = maxlast; be > rs;) {
-        const unsigned bs = (be - rs > (unsigned)kBlock) ? be - kBlock : rs;
-        const unsigned j = bs + threadIdx.x;
-        if (j < be) {
-            const unsigned gi = vals[j];
-            const float4 r0 = s.rec0[gi];
-            const float4 r1 = s.rec1[gi];
-            const float thr = skip_threshold(r1.y);
-            s_idx[threadIdx.x] = gi;
-            s_r0[threadIdx.x] = r0;
-            s_r1[threadIdx.x] = r1;
-            s_b[threadIdx.x] = s.col_b[gi];
-            s_thr[threadIdx.x] = thr;
-            s_box[threadIdx.x] = skip_box(r0, r1, thr);
-        }
+        const unsigned bs = (be - rs > (unsigned)kBwdBatch) ? be - kBwdBatch : rs;
 #pragma unroll
-        for (int v = 0; v < 9; v++) s_acc[v][threadIdx.x] = 0.0f;
+        for (int e = threadIdx.x; e < kBwdBatch; e += kBwdThreads) {
+            const unsigned j = bs + (unsigned)e;
+            if (j < be) {
+                const unsigned gi = vals[j];
+                const float4 r0 = s.rec0[gi];
+                const float4 r1 = s.rec1[gi];
+                const float thr = skip_threshold(r1.y);
+                s_idx[e] = gi;
+                s_r0[e] = r0;
+                s_r1[e] = r1;
+                s_b[e] = s.col_b[gi];
+                s_thr[e] = thr;
+                s_box[e] = skip_box(r0, r1, thr);
+            }
+#pragma unroll
+            for (int v = 0; v < 9; v++) s_acc[v][e] = 0.0f;
+        }
         __syncthreads();
         // this warp only needs the entries below its own last contributor
         const int kstart = (int)(min(be, wlast) - min(bs, wlast)) - 1;
         for (int k = kstart; k >= 0; k--) {
             if (box_misses(s_box[k], wx0, wx1, wy0, wy1)) continue;   // warp-uniform
             const unsigned jj = bs + (unsigned)k;
+            const float4 a = s_r0[k];
+            const float4 c = s_r1[k];
+            const float cb = s_b[k];
+            const float thr = s_thr[k];
             bool contrib = false;
             float gv[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
             float g_cc = 0.f;
-            if (jj < last) {
-                const float4 a = s_r0[k];
-                const float4 c = s_r1[k];
-                const float dx = a.x - fx, dy = a.y - fy;
-                const float power = power_rn(a, c, dx, dy);
-                float alpha, ep;
-                if (!(power < s_thr[k]) && !(power > 0.0f) && alpha_accept_fast(power, c.y, alpha, ep)) {
-                    contrib = true;
-                    const float cb = s_b[k];
-                    const float oma = 1.0f - alpha;
-                    const float Ti = (oma > 1e-6f) ? T / oma : 0.0f;
-                    gv[0] = alpha * Ti * dC0;
-                    gv[1] = alpha * Ti * dC1;
-                    gv[2] = alpha * Ti * dC2;
-                    float d_alpha = 0.0f;
-                    d_alpha += Ti * (c.z - acc0) * dC0;
-                    d_alpha += Ti * (c.w - acc1) * dC1;
-                    d_alpha += Ti * (cb - acc2) * dC2;
-                    acc0 = alpha * c.z + oma * acc0;
-                    acc1 = alpha * c.w + oma * acc1;
-                    acc2 = alpha * cb + oma * acc2;
-                    T = Ti;
-                    float d_power = 0.0f;
-                    if (alpha < 0.99f) {
-                        d_power = d_alpha * c.y * ep;
-                        gv[3] = d_alpha * ep;
+#pragma unroll
+            for (int p = 0; p < 2; p++) {
+                if (jj < last[p]) {
+                    const float dx = a.x - fx, dy = a.y - fy[p];
+                    const float power = power_rn(a, c, dx, dy);
+                    float alpha, ep;
+                    if (!(power < thr) && !(power > 0.0f) && alpha_accept_fast(power, c.y, alpha, ep)) {
+                        contrib = true;
+                        const float oma = 1.0f - alpha;
+                        const float Ti = (oma > 1e-6f) ? T[p] / oma : 0.0f;
+                        const float aT = alpha * Ti;
+                        gv[0] += aT * dC[p][0];
+                        gv[1] += aT * dC[p][1];
+                        gv[2] += aT * dC[p][2];
+                        float d_alpha = 0.0f;
+                        d_alpha += Ti * (c.z - acc[p][0]) * dC[p][0];
+                        d_alpha += Ti * (c.w - acc[p][1]) * dC[p][1];
+                        d_alpha += Ti * (cb - acc[p][2]) * dC[p][2];
+                        acc[p][0] = alpha * c.z + oma * acc[p][0];
+                        acc[p][1] = alpha * c.w + oma * acc[p][1];
+                        acc[p][2] = alpha * cb + oma * acc[p][2];
+                        T[p] = Ti;
+                        if (alpha < 0.99f) {
+                            const float d_power = d_alpha * c.y * ep;
+                            gv[3] += d_alpha * ep;
+                            gv[4] += d_power * (-a.z * dx - a.w * dy);
+                            gv[5] += d_power * (-c.x * dy - a.w * dx);
+                            gv[6] += d_power * (-0.5f * dx * dx);
+                            gv[7] += d_power * (-dx * dy);
+                            g_cc += d_power * (-0.5f * dy * dy);
+                        }
                     }
-                    gv[4] = d_power * (-a.z * dx - a.w * dy);
-                    gv[5] = d_power * (-c.x * dy - a.w * dx);
-                    gv[6] = d_power * (-0.5f * dx * dx);
-                    gv[7] = d_power * (-dx * dy);
-                    g_cc = d_power * (-0.5f * dy * dy);
                 }
             }
             if (__any_sync(0xffffffffu, contrib)) {
@@ -162,16 +184,18 @@ __global__ void __launch_bounds__(kBlock) k_raster_bwd(const StepParams* __restr
             }
         }
         __syncthreads();
-        if (j < be) {
-            // thread t flushes batch entry t, which it also zeroes for the next batch
-            const unsigned gi = s_idx[threadIdx.x];
-            float* const dst[9] = {&g.drgb[3 * gi], &g.drgb[3 * gi + 1], &g.drgb[3 * gi + 2], &g.dop[gi],
-                                   &g.dm2[2 * gi], &g.dm2[2 * gi + 1], &g.dcon[3 * gi], &g.dcon[3 * gi + 1],
-                                   &g.dcon[3 * gi + 2]};
 #pragma unroll
-            for (int v = 0; v < 9; v++) {
-                const float a = s_acc[v][threadIdx.x];
-                if (a != 0.0f) atomicAdd(dst[v], a);
+        for (int e = threadIdx.x; e < kBwdBatch; e += kBwdThreads) {
+            if (bs + (unsigned)e < be) {
+                const unsigned gi = s_idx[e];
+                float* const dst[9] = {&g.drgb[3 * gi], &g.drgb[3 * gi + 1], &g.drgb[3 * gi + 2], &g.dop[gi],
+                                       &g.dm2[2 * gi], &g.dm2[2 * gi + 1], &g.dcon[3 * gi], &g.dcon[3 * gi + 1],
+                                       &g.dcon[3 * gi + 2]};
+#pragma unroll
+                for (int v = 0; v < 9; v++) {
+                    const float av = s_acc[v][e];
+                    if (av != 0.0f) atomicAdd(dst[v], av);
+                }
             }
         }
         __syncthreads();
@@ -185,8 +209,8 @@ cudaError_t launch_raster_bwd_plain(cudaStream_t st, const StepParams* sp, int n
                                     const unsigned* ranges, const unsigned* order, const unsigned* vals,
                                     ScreenPtrs s, PixelPtrs px, RGradPtrs g, Control* ctrl) {
     if (num_tiles <= 0) return cudaSuccess;
-    if (from_sign) k_raster_bwd<true><<<num_tiles, kBlock, 0, st>>>(sp, ranges, order, vals, s, px, g, ctrl);
-    else k_raster_bwd<false><<<num_tiles, kBlock, 0, st>>>(sp, ranges, order, vals, s, px, g, ctrl);
+    if (from_sign) k_raster_bwd<true><<<num_tiles, kBwdThreads, 0, st>>>(sp, ranges, order, vals, s, px, g, ctrl);
+    else k_raster_bwd<false><<<num_tiles, kBwdThreads, 0, st>>>(sp, ranges, order, vals, s, px, g, ctrl);
     return cudaGetLastError();
 }
 
