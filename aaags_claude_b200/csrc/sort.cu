@@ -91,8 +91,9 @@ __device__ __forceinline__ unsigned long long block_exclusive_scan64(unsigned lo
 
 // One pass over digit `pass` (key bits 8*pass..); `slot` selects the digit
 // histogram and CTA ticket in the control block.
+// 64-bit keys: 2 CTAs per SM (register-bound); 32-bit keys: 4.
 template <typename K>
-__global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const StepParams* __restrict__ sp,
+__global__ void __launch_bounds__(kSortThreads, sizeof(K) == 4 ? 4 : 2) k_onesweep(const StepParams* __restrict__ sp,
                                                               const K* __restrict__ kin,
                                                               const unsigned* __restrict__ vin,
                                                               K* __restrict__ kout,
@@ -174,16 +175,18 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const StepParams* 
 __device__ __forceinline__ unsigned tile_of(unsigned long long key) { return (unsigned)(key >> 32); }
 __device__ __forceinline__ unsigned tile_of(unsigned key) { return key; }   // tile-only keys
 
+// One thread per key (the grid covers the capacity): a tile's range starts
+// where its key differs from the previous one and ends where it differs
+// from the next.
 template <typename K>
 __global__ void k_ranges(const K* __restrict__ keys, unsigned long long capacity, unsigned* __restrict__ ranges,
                          Control* ctrl) {
     const unsigned long long P = min(ctrl->total_pairs, capacity);
-    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
-    for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < P; i += stride) {
-        const unsigned t = tile_of(keys[i]);
-        if (i == 0 || tile_of(keys[i - 1]) != t) ranges[2 * t] = (unsigned)i;
-        if (i == P - 1 || tile_of(keys[i + 1]) != t) ranges[2 * t + 1] = (unsigned)(i + 1);
-    }
+    const unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P) return;
+    const unsigned t = tile_of(keys[i]);
+    if (i == 0 || tile_of(keys[i - 1]) != t) ranges[2 * t] = (unsigned)i;
+    if (i == P - 1 || tile_of(keys[i + 1]) != t) ranges[2 * t + 1] = (unsigned)(i + 1);
 }
 
 // Heavy-first tile order: one CTA buckets the tiles by floor(log2(pairs))
@@ -300,14 +303,14 @@ cudaError_t launch_radix_sort32(cudaStream_t st, const StepParams* sp, int digit
 cudaError_t launch_tile_ranges(cudaStream_t st, unsigned long long capacity, const unsigned long long* keys_sorted,
                                unsigned* ranges, Control* ctrl) {
     if (capacity == 0) return cudaSuccess;
-    k_ranges<<<4 * 148, 256, 0, st>>>(keys_sorted, capacity, ranges, ctrl);
+    k_ranges<<<(unsigned)((capacity + 255) / 256), 256, 0, st>>>(keys_sorted, capacity, ranges, ctrl);
     return cudaGetLastError();
 }
 
 cudaError_t launch_tile_ranges32(cudaStream_t st, unsigned long long capacity, const unsigned* tiles_sorted,
                                  unsigned* ranges, Control* ctrl) {
     if (capacity == 0) return cudaSuccess;
-    k_ranges<<<4 * 148, 256, 0, st>>>(tiles_sorted, capacity, ranges, ctrl);
+    k_ranges<<<(unsigned)((capacity + 255) / 256), 256, 0, st>>>(tiles_sorted, capacity, ranges, ctrl);
     return cudaGetLastError();
 }
 
