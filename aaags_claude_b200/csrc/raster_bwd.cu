@@ -15,18 +15,22 @@
 namespace gs3d {
 namespace {
 
-// alpha = min(0.99, o exp(power)) and whether it reaches 1/255, on the fast
-// expf.  expf is within a few ulp of exp, so o*expf(power) decides both the
-// 1/255 threshold and the 0.99 clamp exactly unless it lies within a relative
-// 2e-6 (about 16 ulp) of either bound; there the exact exp (exp_ref, the
-// forward's) is recomputed.  Accepted unclamped pairs keep the fast alpha,
-// a few ulp from the forward's: the transmittance recovered from it and the
-// gradients stay within their tolerance.
+// alpha = min(0.99, o exp(power)) and whether it reaches 1/255.  For power in
+// [skip_threshold, 0] (|power| < 6) __expf is within 6e-7 relative of exp, so
+// o*__expf(power) decides the 1/255 threshold and the 0.99 clamp exactly
+// unless it lies within a relative 2e-6 of either bound; there the exact exp
+// (exp_ref, the forward's) is recomputed.  Above alpha 0.5 the transmittance
+// recovered by dividing by 1 - alpha magnifies alpha's error, so those pairs
+// take the accurate expf (a few ulp).  Either way alpha is within the
+// gradients' tolerance of the forward's.
 __device__ __forceinline__ bool alpha_accept_fast(float power, float o, float& alpha, float& e) {
-    e = expf(power);
+    e = __expf(power);
     float a = o * e;
     if (fabsf(a - kAlphaMin) <= 2e-6f * kAlphaMin || fabsf(a - 0.99f) <= 2e-6f) {
         e = exp_ref(power);
+        a = o * e;
+    } else if (a > 0.5f) {
+        e = expf(power);
         a = o * e;
     }
     alpha = fmin_ref(0.99f, a);
@@ -150,7 +154,7 @@ __global__ void __launch_bounds__(kBwdThreads) k_raster_bwd(const StepParams* __
                     if (!(power < thr) && !(power > 0.0f) && alpha_accept_fast(power, c.y, alpha, ep)) {
                         contrib = true;
                         const float oma = 1.0f - alpha;
-                        const float Ti = (oma > 1e-6f) ? T[p] / oma : 0.0f;
+                        const float Ti = (oma > 1e-6f) ? __fdividef(T[p], oma) : 0.0f;
                         const float aT = alpha * Ti;
                         gv[0] += aT * dC[p][0];
                         gv[1] += aT * dC[p][1];
