@@ -399,7 +399,8 @@ def run_reference(a) -> int:
     L = O.lib_ref()
     rend = L.ref_renderer_create(ctypes.c_size_t(4 << 30))
     gt = np.zeros(cam.width * cam.height * 3, np.float32)
-    L.ref_renderer_render(rend, ctypes.addressof(g), ctypes.addressof(cam), ctypes.addressof(S.render_config(False)),
+    render_cfg = S.render_config(False)   # kept alive across the call
+    L.ref_renderer_render(rend, ctypes.addressof(g), ctypes.addressof(cam), ctypes.addressof(render_cfg),
                           gt.ctypes.data)
     L.ref_renderer_destroy(rend)
     cores = os.cpu_count() or 1
