@@ -38,6 +38,7 @@ struct DevBuf {
         p = nullptr;
         n = 0;
     }
+    ~DevBuf() { release(); }
 };
 
 constexpr int kParamSlots = 4;  // pinned ring of per-step parameter blocks
@@ -81,6 +82,12 @@ struct gs3dc_ctx {
     DevBuf<unsigned> dvals[2];
     DevBuf<unsigned long long> ddesc;
     unsigned long long ddesc_stride = 0;
+    // reduced-storage form (GS3DC_FORM_BF16 / _FP16); the FP32 model arrays above stage uploads
+    int form = GS3DC_FORM_PLAIN_FP32;
+    bool chosen_ready = false;   // the chosen buffers hold the current model
+    DevBuf<float> c_pos, cm_pos, cv_pos;
+    DevBuf<unsigned short> c_attr, c_sh, cm_attr, cv_attr, cm_sh, cv_sh;
+    DevBuf<uint2> c_rects;
     // control block + preprocess scan descriptors (one memset)
     DevBuf<unsigned char> ctrl_region;
     Control* ctrl = nullptr;
@@ -108,6 +115,8 @@ struct gs3dc_ctx {
     // graph of the train step
     bool use_graph = true;
     bool fused_adam = false;   // split backward + optimiser by default (faster at this occupancy)
+    bool keep_grads = false;   // GS3DC_OPT_KEEP_GRADIENTS
+    bool have_step_grads = false;
     cudaGraphExec_t graph = nullptr;
     long long graph_key[8] = {};
     long long graph_replays = 0;
@@ -249,6 +258,54 @@ int zero_adam(gs3dc_ctx* c) {
     return GS3DC_OK;
 }
 
+bool chosen_form(const gs3dc_ctx* c) { return c->form != GS3DC_FORM_PLAIN_FP32; }
+
+ChosenPtrs chosen_ptrs(gs3dc_ctx* c) {
+    return {c->c_pos.p, c->c_attr.p, c->c_sh.p, c->cm_pos.p, c->cv_pos.p,
+            c->cm_attr.p, c->cv_attr.p, c->cm_sh.p, c->cv_sh.p};
+}
+
+// Reduced-storage buffers for the current N and SH width, filled from the FP32
+// model arrays (round to nearest), optimiser state zeroed.
+int load_chosen(gs3dc_ctx* c) {
+    const size_t n = (size_t)c->N, mc3 = (size_t)c->max_coeffs * 3;
+    CK(c->c_pos.ensure(3 * n));
+    CK(c->cm_pos.ensure(3 * n));
+    CK(c->cv_pos.ensure(3 * n));
+    CK(c->c_attr.ensure(8 * n));
+    CK(c->cm_attr.ensure(8 * n));
+    CK(c->cv_attr.ensure(8 * n));
+    CK(c->c_sh.ensure(mc3 * n));
+    CK(c->cm_sh.ensure(mc3 * n));
+    CK(c->cv_sh.ensure(mc3 * n));
+    CK(c->c_rects.ensure(n ? n : 1));
+    if (n) {
+        CK(launch_chosen_from_raw(c->stream, c->N, (int)mc3, c->form == GS3DC_FORM_FP16,
+                                  ModelPtrs{c->pos.p, c->sc.p, c->rot.p, c->sh.p, c->op.p}, chosen_ptrs(c)));
+        CK(cudaMemsetAsync(c->cm_pos.p, 0, 3 * n * 4, c->stream));
+        CK(cudaMemsetAsync(c->cv_pos.p, 0, 3 * n * 4, c->stream));
+        CK(cudaMemsetAsync(c->cm_attr.p, 0, 8 * n * 2, c->stream));
+        CK(cudaMemsetAsync(c->cv_attr.p, 0, 8 * n * 2, c->stream));
+        CK(cudaMemsetAsync(c->cm_sh.p, 0, mc3 * n * 2, c->stream));
+        CK(cudaMemsetAsync(c->cv_sh.p, 0, mc3 * n * 2, c->stream));
+    }
+    c->chosen_ready = true;
+    return GS3DC_OK;
+}
+
+// The reduced-storage model back into the FP32 model arrays.
+int unload_chosen(gs3dc_ctx* c) {
+    if (!c->chosen_ready || c->N <= 0) return GS3DC_OK;
+    CK(launch_chosen_to_raw(c->stream, c->N, c->max_coeffs * 3, c->form == GS3DC_FORM_FP16, chosen_ptrs(c),
+                            ModelPtrs{c->pos.p, c->sc.p, c->rot.p, c->sh.p, c->op.p}));
+    return GS3DC_OK;
+}
+
+int require_plain(gs3dc_ctx* c, const char* what) {
+    if (chosen_form(c)) return fail(c, GS3DC_ERR_STATE, "%s needs GS3DC_FORM_PLAIN_FP32", what);
+    return GS3DC_OK;
+}
+
 int ensure_grads(gs3dc_ctx* c) {
     const size_t n = (size_t)c->N, mc3 = (size_t)c->max_coeffs * 3;
     CK(c->g_pos.ensure(3 * n));
@@ -334,6 +391,7 @@ int push_params(gs3dc_ctx* c, const gs3d_camera* cam, const gs3d_render_config* 
     p.gt = gt_dev;
     p.persist = c->persist;
     p.raw_rot = raw_rot_dev;
+    p.seed = (unsigned)iteration * 2654435761u + (unsigned)c->adam_step * 40503u + 1u;
     if (tc) {
         p.use_adam = tc->use_adam ? 1 : 0;
         // lr_schedule, train_types.cpp:64-68
@@ -447,14 +505,21 @@ int seq_front_depth_first(gs3dc_ctx* c) {
     // tile-only keys live in the (otherwise unused) 64-bit key buffers
     unsigned* tk[2] = {reinterpret_cast<unsigned*>(c->keys[0].p), reinterpret_cast<unsigned*>(c->keys[1].p)};
     PairPtrs pr{c->keys[0].p, c->vals[0].p, c->cap, c->scan_desc, tk[0]};
-    CK(launch_preprocess_plain(c->stream, c->sp_dev, c->N, c->model_raw, false, model_ptrs(c), screen_ptrs(c, false),
-                               pr, c->ctrl, DepthKeys{c->dkeys[0].p, c->dvals[0].p}));
+    const bool chosen = chosen_form(c);
+    if (chosen)
+        CK(launch_chosen_preprocess(c->stream, c->sp_dev, c->N, c->form == GS3DC_FORM_FP16, chosen_ptrs(c),
+                                    screen_ptrs(c, false), DepthKeys{c->dkeys[0].p, c->dvals[0].p}, c->c_rects.p,
+                                    c->ctrl));
+    else
+        CK(launch_preprocess_plain(c->stream, c->sp_dev, c->N, c->model_raw, false, model_ptrs(c),
+                                   screen_ptrs(c, false), pr, c->ctrl, DepthKeys{c->dkeys[0].p, c->dvals[0].p}));
     if ((rc = mark(c, GS3DC_STAGE_SORT_HIST))) return rc;
     int dw = 0;
     CK(launch_radix_sort(c->stream, c->sp_dev, kDepthDigits, (unsigned long long)c->N, c->dkeys[0].p, c->dvals[0].p,
                          c->dkeys[1].p, c->dvals[1].p, c->ddesc.p, c->ddesc_stride, c->ctrl, &dw, nullptr, 0,
                          &c->ctrl->gauss_keys));
-    CK(launch_emit_ranked(c->stream, c->sp_dev, c->N, c->dvals[dw].p, screen_ptrs(c, false), pr, c->ctrl));
+    CK(launch_emit_ranked(c->stream, c->sp_dev, c->N, c->dvals[dw].p, screen_ptrs(c, false), pr, c->ctrl,
+                          chosen ? c->c_rects.p : nullptr));
     if ((rc = mark(c, GS3DC_STAGE_SORT_PASSES))) return rc;
     int which = 0;
     CK(launch_radix_sort32(c->stream, c->sp_dev, tile_digits, kDepthDigits, true, c->cap, tk[0], c->vals[0].p, tk[1],
@@ -467,8 +532,31 @@ int seq_front_depth_first(gs3dc_ctx* c) {
     return GS3DC_OK;
 }
 
+// Train step of the reduced-storage form: depth-first front half with the
+// chosen preprocess, fast-exp rasterisers, fused adjoint + Adam.
+int seq_train_chosen(gs3dc_ctx* c) {
+    int rc = seq_front_depth_first(c);
+    if (rc) return rc;
+    const int w = c->sorted_which;
+    if ((rc = mark(c, GS3DC_STAGE_RASTER_FWD))) return rc;
+    CK(launch_raster_fwd_fast(c->stream, c->sp_dev, c->num_tiles, c->ranges.p, c->tile_order.p, c->vals[w].p,
+                              screen_ptrs(c, false), pixel_ptrs(c), c->ctrl));
+    if ((rc = mark(c, GS3DC_STAGE_RASTER_BWD))) return rc;
+    CK(launch_raster_bwd_fast(c->stream, c->sp_dev, c->num_tiles, c->ranges.p, c->tile_order.p, c->vals[w].p,
+                              screen_ptrs(c, false), pixel_ptrs(c), rgrad_ptrs(c), c->ctrl));
+    if ((rc = mark(c, GS3DC_STAGE_PREPROCESS_BWD))) return rc;
+    CK(launch_chosen_backward_adam(c->stream, c->sp_dev, c->N, c->max_coeffs * 3, c->form == GS3DC_FORM_FP16,
+                                   chosen_ptrs(c), rgrad_ptrs(c),
+                                   c->keep_grads ? grad_ptrs(c) : GradPtrs{nullptr, nullptr, nullptr, nullptr, nullptr},
+                                   c->ctrl));
+    if ((rc = mark(c, GS3DC_NUM_STAGES))) return rc;
+    c->kernels_last += 3;
+    return GS3DC_OK;
+}
+
 int seq_train(gs3dc_ctx* c) {
     int rc;
+    if (chosen_form(c)) return seq_train_chosen(c);
     if (c->sort_mode == GS3DC_SORT_DEPTH_FIRST) {
         if ((rc = seq_front_depth_first(c))) return rc;
     } else {
@@ -483,7 +571,7 @@ int seq_train(gs3dc_ctx* c) {
     CK(launch_raster_bwd_plain(c->stream, c->sp_dev, c->num_tiles, true, c->ranges.p, c->tile_order.p, c->vals[w].p,
                                screen_ptrs(c, false), pixel_ptrs(c), rgrad_ptrs(c), c->ctrl));
     if ((rc = mark(c, GS3DC_STAGE_PREPROCESS_BWD))) return rc;
-    if (c->fused_adam) {
+    if (c->fused_adam && !c->keep_grads) {
         CK(launch_preprocess_bwd_plain(c->stream, c->sp_dev, c->N, c->max_coeffs * 3, 1, model_ptrs(c),
                                        adam_ptrs(c), screen_ptrs(c, false), rgrad_ptrs(c), grad_ptrs(c), c->ctrl));
     } else {
@@ -681,9 +769,28 @@ int gs3dc_set_option(gs3dc_ctx* c, int option, int64_t value) {
         case GS3DC_OPT_USE_GRAPH:
             c->use_graph = value != 0;
             return GS3DC_OK;
-        case GS3DC_OPT_FORM:
-            if (value != GS3DC_FORM_PLAIN_FP32) return fail(c, GS3DC_ERR_INVALID_ARG, "unknown form %lld", (long long)value);
+        case GS3DC_OPT_FORM: {
+            if (value != GS3DC_FORM_PLAIN_FP32 && value != GS3DC_FORM_BF16 && value != GS3DC_FORM_FP16)
+                return fail(c, GS3DC_ERR_INVALID_ARG, "unknown form %lld", (long long)value);
+            if (value == c->form) return GS3DC_OK;
+            CK(cudaSetDevice(c->device));
+            int rc;
+            if (c->graph) {
+                cudaGraphExecDestroy(c->graph);
+                c->graph = nullptr;
+            }
+            if (c->have_model && !c->model_raw && value != GS3DC_FORM_PLAIN_FP32)
+                return fail(c, GS3DC_ERR_STATE, "the device model is an activated render model");
+            // the model moves to the new form; the optimiser restarts
+            if ((rc = unload_chosen(c))) return rc;
+            c->form = (int)value;
+            c->chosen_ready = false;
+            if (c->have_model && chosen_form(c) && (rc = load_chosen(c))) return rc;
+            if (c->have_model && (rc = zero_adam(c))) return rc;
+            c->have_screen = c->have_pairs = c->have_sorted = c->have_raster = c->have_rgrad = c->have_grads = false;
+            CK(cudaStreamSynchronize(c->stream));
             return GS3DC_OK;
+        }
         case GS3DC_OPT_SPIN_LIMIT:
             if (value <= 0) return fail(c, GS3DC_ERR_INVALID_ARG, "spin limit must be positive");
             c->spin_limit = (unsigned)value;
@@ -697,6 +804,13 @@ int gs3dc_set_option(gs3dc_ctx* c, int option, int64_t value) {
             return GS3DC_OK;
         case GS3DC_OPT_STAGE_TIMING:
             c->stage_timing = value != 0;
+            return GS3DC_OK;
+        case GS3DC_OPT_KEEP_GRADIENTS:
+            c->keep_grads = value != 0;
+            if (c->graph) {
+                cudaGraphExecDestroy(c->graph);
+                c->graph = nullptr;
+            }
             return GS3DC_OK;
         case GS3DC_OPT_SORT:
             if (value != GS3DC_SORT_DEPTH_FIRST && value != GS3DC_SORT_FULL_KEY)
@@ -723,6 +837,7 @@ int gs3dc_get_stat(gs3dc_ctx* c, int stat, int64_t* value) {
 
 int gs3dc_set_gaussians(gs3dc_ctx* c, const gs3d_gaussians* g) {
     if (!c || !g) return GS3DC_ERR_INVALID_ARG;
+    if (int rc_ = require_plain(c, "gs3dc_set_gaussians")) return rc_;
     CK(cudaSetDevice(c->device));
     int rc = upload_model_arrays(c, g->count, g->sh_degree, g->max_coeffs, g->positions, g->scales, g->rotations,
                                  g->sh_coeffs, g->opacities);
@@ -741,6 +856,8 @@ int gs3dc_set_raw_params(gs3dc_ctx* c, const gs3d_raw_params* r) {
     c->model_raw = true;
     if ((rc = ensure_adam(c))) return rc;
     if ((rc = zero_adam(c))) return rc;
+    c->chosen_ready = false;
+    if (chosen_form(c) && (rc = load_chosen(c))) return rc;
     CK(cudaStreamSynchronize(c->stream));
     return GS3DC_OK;
 }
@@ -760,10 +877,29 @@ int gs3dc_update_raw_params(gs3dc_ctx* c, const gs3d_raw_params* r) {
         CK(cudaMemcpyAsync(c->rot.p, r->raw_rotations, 4 * n * 4, cudaMemcpyHostToDevice, c->stream));
         CK(cudaMemcpyAsync(c->sh.p, r->raw_sh_coeffs, 3 * n * c->max_coeffs * 4, cudaMemcpyHostToDevice, c->stream));
         CK(cudaMemcpyAsync(c->op.p, r->raw_opacities, n * 4, cudaMemcpyHostToDevice, c->stream));
+        if (chosen_form(c))
+            CK(launch_chosen_from_raw(c->stream, c->N, c->max_coeffs * 3, c->form == GS3DC_FORM_FP16,
+                                      ModelPtrs{c->pos.p, c->sc.p, c->rot.p, c->sh.p, c->op.p}, chosen_ptrs(c)));
     }
     CK(cudaStreamSynchronize(c->stream));
     c->have_screen = c->have_pairs = c->have_sorted = c->have_raster = c->have_rgrad = c->have_grads = false;
     return GS3DC_OK;
+}
+
+int gs3dc_get_gradients(gs3dc_ctx* c, float* d_raw_positions, float* d_raw_scales, float* d_raw_rotations,
+                        float* d_raw_sh_coeffs, float* d_raw_opacities) {
+    if (!c) return GS3DC_ERR_INVALID_ARG;
+    if (!c->have_step_grads)
+        return fail(c, GS3DC_ERR_STATE, "no gradients kept: run gs3dc_train_step with GS3DC_OPT_KEEP_GRADIENTS");
+    CK(cudaSetDevice(c->device));
+    const size_t n = (size_t)c->N;
+    int rc;
+    if ((rc = download(c, d_raw_positions, c->g_pos.p, 3 * n * 4)) || (rc = download(c, d_raw_scales, c->g_sc.p, 3 * n * 4)) ||
+        (rc = download(c, d_raw_rotations, c->g_rot.p, 4 * n * 4)) ||
+        (rc = download(c, d_raw_sh_coeffs, c->g_sh.p, 3 * n * c->max_coeffs * 4)) ||
+        (rc = download(c, d_raw_opacities, c->g_op.p, n * 4)))
+        return rc;
+    return gs3dc_synchronize(c);
 }
 
 int gs3dc_get_image(gs3dc_ctx* c, float* image) {
@@ -784,6 +920,7 @@ int gs3dc_get_raw_params(gs3dc_ctx* c, gs3d_raw_params* r) {
         return fail(c, GS3DC_ERR_INVALID_ARG, "host params have N=%d mc=%d, device N=%d mc=%d", r->count,
                     r->max_coeffs, c->N, c->max_coeffs);
     const size_t n = (size_t)c->N;
+    if (chosen_form(c) && (rc = unload_chosen(c))) return rc;
     if ((rc = download(c, r->raw_positions, c->pos.p, 3 * n * 4))) return rc;
     if ((rc = download(c, r->raw_scales, c->sc.p, 3 * n * 4))) return rc;
     if ((rc = download(c, r->raw_rotations, c->rot.p, 4 * n * 4))) return rc;
@@ -795,6 +932,7 @@ int gs3dc_get_raw_params(gs3dc_ctx* c, gs3d_raw_params* r) {
 int gs3dc_preprocess(gs3dc_ctx* c, const gs3d_camera* cam, const gs3d_render_config* cfg,
                      const gs3dc_screen_arrays* out) {
     if (!c) return GS3DC_ERR_INVALID_ARG;
+    if (int rc_ = require_plain(c, "gs3dc_preprocess")) return rc_;
     int rc;
     if ((rc = check_config(c, cam, cfg)) || (rc = require_model(c))) return rc;
     CK(cudaSetDevice(c->device));
@@ -833,6 +971,7 @@ int gs3dc_bin(gs3dc_ctx* c, int num_gaussians, const gs3dc_screen_arrays* in, co
               const gs3d_render_config* cfg, int64_t* total_pairs, uint64_t* keys_unsorted,
               uint32_t* values_unsorted) {
     if (!c) return GS3DC_ERR_INVALID_ARG;
+    if (int rc_ = require_plain(c, "gs3dc_bin")) return rc_;
     int rc;
     if ((rc = check_config(c, cam, cfg))) return rc;
     CK(cudaSetDevice(c->device));
@@ -945,6 +1084,7 @@ int gs3dc_sort_pairs(gs3dc_ctx* c, int64_t total_pairs, const uint64_t* keys, co
 int gs3dc_rasterize(gs3dc_ctx* c, const gs3d_camera* cam, const gs3d_render_config* cfg, float* image,
                     float* T_final, int* n_contrib) {
     if (!c) return GS3DC_ERR_INVALID_ARG;
+    if (int rc_ = require_plain(c, "gs3dc_rasterize")) return rc_;
     int rc;
     if ((rc = check_config(c, cam, cfg))) return rc;
     if (!c->have_sorted || !c->have_screen)
@@ -968,6 +1108,7 @@ int gs3dc_rasterize(gs3dc_ctx* c, const gs3d_camera* cam, const gs3d_render_conf
 int gs3dc_render(gs3dc_ctx* c, const gs3d_gaussians* g, const gs3d_camera* cam, const gs3d_render_config* cfg,
                  float* image) {
     if (!c) return GS3DC_ERR_INVALID_ARG;
+    if (int rc_ = require_plain(c, "gs3dc_render")) return rc_;
     int rc;
     if ((rc = check_config(c, cam, cfg))) return rc;
     if (g && (rc = gs3dc_set_gaussians(c, g))) return rc;
@@ -984,6 +1125,7 @@ int gs3dc_render(gs3dc_ctx* c, const gs3d_gaussians* g, const gs3d_camera* cam, 
 int gs3dc_raster_backward(gs3dc_ctx* c, const gs3d_camera* cam, const gs3d_render_config* cfg, const float* d_image,
                           float* d_means2D, float* d_conics, float* d_rgb, float* d_opacities_2d) {
     if (!c || !d_image) return GS3DC_ERR_INVALID_ARG;
+    if (int rc_ = require_plain(c, "gs3dc_raster_backward")) return rc_;
     int rc;
     if ((rc = check_config(c, cam, cfg))) return rc;
     if (!c->have_raster) return fail(c, GS3DC_ERR_STATE, "gs3dc_raster_backward needs gs3dc_rasterize first");
@@ -1011,6 +1153,7 @@ int gs3dc_preprocess_backward(gs3dc_ctx* c, const gs3d_camera* cam, const gs3d_r
                               const float* raw_rotations, float* d_raw_positions, float* d_raw_scales,
                               float* d_raw_rotations, float* d_raw_sh_coeffs, float* d_raw_opacities) {
     if (!c) return GS3DC_ERR_INVALID_ARG;
+    if (int rc_ = require_plain(c, "gs3dc_preprocess_backward")) return rc_;
     int rc;
     if ((rc = check_config(c, cam, cfg))) return rc;
     if (!c->have_rgrad) return fail(c, GS3DC_ERR_STATE, "gs3dc_preprocess_backward needs gs3dc_raster_backward");
@@ -1042,6 +1185,7 @@ int gs3dc_preprocess_backward(gs3dc_ctx* c, const gs3d_camera* cam, const gs3d_r
 
 int gs3dc_optimizer_step(gs3dc_ctx* c, const gs3d_train_config* tc, int iteration) {
     if (!c || !tc) return GS3DC_ERR_INVALID_ARG;
+    if (int rc_ = require_plain(c, "gs3dc_optimizer_step")) return rc_;
     if (!c->have_grads) return fail(c, GS3DC_ERR_STATE, "gs3dc_optimizer_step needs gs3dc_preprocess_backward");
     CK(cudaSetDevice(c->device));
     int rc;
@@ -1115,6 +1259,7 @@ int gs3dc_train_step(gs3dc_ctx* c, const gs3d_camera* cam, const float* gt, int 
     if ((rc = ensure_adam(c))) return rc;
     if ((rc = ensure_grads(c))) return rc;
     if ((rc = ensure_depth_sort(c))) return rc;
+    if (chosen_form(c) && !c->chosen_ready) return fail(c, GS3DC_ERR_NO_MODEL, "no reduced-storage model loaded");
     if ((rc = ensure_pixels(c, cam->width, cam->height))) return rc;
     const size_t np = (size_t)cam->width * cam->height;
     const float* gt_dev = gt;
@@ -1133,7 +1278,8 @@ int gs3dc_train_step(gs3dc_ctx* c, const gs3d_camera* cam, const float* gt, int 
         c->adam_step = step_before + (tc->use_adam ? 1 : 0);
         if ((rc = push_params(c, cam, cfg, tc, iteration, gt_dev))) return rc;
         const long long key[8] = {c->N, c->max_coeffs, cam->width, cam->height, (long long)c->cap, c->sort_passes,
-                                  (long long)c->spin_limit, (c->fused_adam ? 1 : 2) + 4 * c->sort_mode};
+                                  (long long)c->spin_limit,
+                                  (c->fused_adam ? 1 : 2) + 4 * c->sort_mode + 16 * c->form + 64 * (c->keep_grads ? 1 : 0)};
         const bool key_ok = c->graph && std::memcmp(key, c->graph_key, sizeof(key)) == 0;
         c->kernels_last = 0;
         if (c->use_graph && !c->stage_timing && !first && attempt == 0) {
@@ -1159,6 +1305,7 @@ int gs3dc_train_step(gs3dc_ctx* c, const gs3d_camera* cam, const float* gt, int 
         } else {
             if ((rc = seq_train(c))) return rc;
         }
+        c->have_step_grads = c->keep_grads;
         if (!loss && !first && !c->stage_timing) {
             c->pending_check = true;  // overflow is reported by the next synchronising call
             return GS3DC_OK;

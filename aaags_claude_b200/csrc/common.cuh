@@ -49,6 +49,7 @@ struct StepParams {
     const float* gt;      // [H*W*3] device target of the fused L1 (read per replay)
     Persist* persist;
     const float* raw_rot; // [N*4] raw quaternions when the device model is an activated one (backward only)
+    unsigned seed;        // per-step seed of the reduced-storage form's stochastic rounding
 };
 
 // Small device control block, zeroed by one memset at the start of a step.

@@ -79,12 +79,49 @@ struct ScreenArrays {
     int* tiles;
 };
 
-// ---- plain FP32 kernels (plain.cu, compiled without FMA contraction) ----
 // Gaussian depth-sort input written by a preprocess that does not emit pairs.
 struct DepthKeys {
     unsigned long long* keys;   // [N] depth bits, ~0u for Gaussians without pairs
     unsigned* vals;             // [N] Gaussian index
 };
+
+// Reduced-storage ("chosen") form: positions FP32, the other attributes and the
+// SH coefficients 16-bit (BF16 or FP16), Adam moments BF16 (positions: FP32).
+struct ChosenPtrs {
+    float* pos;     // [N*3]
+    void* attr;     // [N*8] 16-bit: raw scale[3], raw opacity, raw rotation[4] (16 bytes per Gaussian)
+    void* sh;       // [N*mc3] 16-bit, the reference's basis-interleaved order
+    float* m_pos;   // [N*3] Adam moments of the positions
+    float* v_pos;
+    void* m_attr;   // [N*8] BF16
+    void* v_attr;
+    void* m_sh;     // [N*mc3] BF16
+    void* v_sh;
+};
+
+// FP32 raw arrays (reference layout) -> reduced storage (round to nearest) and back.
+cudaError_t launch_chosen_from_raw(cudaStream_t st, int N, int mc3, bool fp16, ModelPtrs raw, ChosenPtrs c);
+cudaError_t launch_chosen_to_raw(cudaStream_t st, int N, int mc3, bool fp16, ChosenPtrs c, ModelPtrs raw);
+// Preprocess of the reduced-storage model: screen records, depth-sort input
+// and tile rectangles (the reference's rectangle cut to the box of the
+// ellipse where alpha can reach 1/255).
+cudaError_t launch_chosen_preprocess(cudaStream_t st, const StepParams* sp, int N, bool fp16, ChosenPtrs c,
+                                     ScreenPtrs s, DepthKeys dk, uint2* rects, Control* ctrl);
+// Forward rasteriser with the fast-exp blend decision and fused L1.
+cudaError_t launch_raster_fwd_fast(cudaStream_t st, const StepParams* sp, int num_tiles, const unsigned* ranges,
+                                   const unsigned* order, const unsigned* vals, ScreenPtrs s, PixelPtrs px,
+                                   Control* ctrl);
+// Backward rasteriser deciding acceptance like launch_raster_fwd_fast.
+cudaError_t launch_raster_bwd_fast(cudaStream_t st, const StepParams* sp, int num_tiles, const unsigned* ranges,
+                                   const unsigned* order, const unsigned* vals, ScreenPtrs s, PixelPtrs px,
+                                   RGradPtrs g, Control* ctrl);
+// Per-Gaussian adjoint fused with Adam (stochastic rounding into the 16-bit
+// parameters and BF16 moments); zeroes the screen-gradient accumulators.
+// With gout.g_pos != NULL the FP32 raw-parameter gradients are stored too.
+cudaError_t launch_chosen_backward_adam(cudaStream_t st, const StepParams* sp, int N, int mc3, bool fp16,
+                                        ChosenPtrs c, RGradPtrs rg, GradPtrs gout, Control* ctrl);
+
+// ---- plain FP32 kernels (plain.cu, compiled without FMA contraction) ----
 // Preprocess; emits the pairs in Gaussian order, or -- when dk.keys != NULL --
 // writes the depth-sort input instead (pairs come from launch_emit_ranked).
 cudaError_t launch_preprocess_plain(cudaStream_t st, const StepParams* sp, int N, bool train,
@@ -94,8 +131,11 @@ cudaError_t launch_preprocess_plain(cudaStream_t st, const StepParams* sp, int N
 // (depth order), with the same scan / look-back as the preprocess: tile-only
 // keys to pr.tiles32, and the tile-digit histograms into control slots
 // kDepthDigits.. for launch_radix_sort32.
+// rects (optional): per-Gaussian tile rectangles (xmin | ymin << 16,
+// xmax | ymax << 16) written by the reduced-storage preprocess; without them
+// the rectangle is recomputed from the stored mean and radius.
 cudaError_t launch_emit_ranked(cudaStream_t st, const StepParams* sp, int N, const unsigned* rank_gid,
-                               ScreenPtrs s, PairPtrs pr, Control* ctrl);
+                               ScreenPtrs s, PairPtrs pr, Control* ctrl, const uint2* rects = nullptr);
 cudaError_t launch_bin_arrays(cudaStream_t st, const StepParams* sp, int N, ScreenArrays a,
                               PairPtrs pr, Control* ctrl);
 cudaError_t launch_export_screen(cudaStream_t st, int N, ScreenPtrs s, ScreenArrays a);

@@ -37,6 +37,22 @@ __device__ __forceinline__ bool alpha_accept_fast(float power, float o, float& a
     return !(alpha < kAlphaMin);
 }
 
+// Acceptance policies: the one of the plain form agrees with its exact
+// forward; the reduced-storage form's forward decides on o * __expf(power)
+// alone, and so does its backward (same power_rn, same __expf, same product).
+struct PlainAccept {
+    __device__ __forceinline__ static bool accept(float power, float o, float& alpha, float& e) {
+        return alpha_accept_fast(power, o, alpha, e);
+    }
+};
+struct FastAccept {
+    __device__ __forceinline__ static bool accept(float power, float o, float& alpha, float& e) {
+        e = __expf(power);
+        alpha = fmin_ref(0.99f, o * e);
+        return !(alpha < kAlphaMin);
+    }
+};
+
 // Rasterizer backward (rasterizer_backward_cpu.cpp:20-133): back-to-front
 // over each pixel's contributors, transmittance recovered by division from
 // T_final instead of a replayed per-pixel list.  One CTA of 128 threads per
@@ -49,7 +65,7 @@ __device__ __forceinline__ bool alpha_accept_fast(float power, float o, float& a
 constexpr int kBwdThreads = 128;
 constexpr int kBwdBatch = 256;
 
-template <bool FROM_SIGN>
+template <bool FROM_SIGN, class Accept>
 __global__ void __launch_bounds__(kBwdThreads) k_raster_bwd(const StepParams* __restrict__ spp,
                                                             const unsigned* __restrict__ ranges,
                                                             const unsigned* __restrict__ order,
@@ -151,7 +167,7 @@ __global__ void __launch_bounds__(kBwdThreads) k_raster_bwd(const StepParams* __
                     const float dx = a.x - fx, dy = a.y - fy[p];
                     const float power = power_rn(a, c, dx, dy);
                     float alpha, ep;
-                    if (!(power < thr) && !(power > 0.0f) && alpha_accept_fast(power, c.y, alpha, ep)) {
+                    if (!(power < thr) && !(power > 0.0f) && Accept::accept(power, c.y, alpha, ep)) {
                         contrib = true;
                         const float oma = 1.0f - alpha;
                         const float Ti = (oma > 1e-6f) ? __fdividef(T[p], oma) : 0.0f;
@@ -213,8 +229,18 @@ cudaError_t launch_raster_bwd_plain(cudaStream_t st, const StepParams* sp, int n
                                     const unsigned* ranges, const unsigned* order, const unsigned* vals,
                                     ScreenPtrs s, PixelPtrs px, RGradPtrs g, Control* ctrl) {
     if (num_tiles <= 0) return cudaSuccess;
-    if (from_sign) k_raster_bwd<true><<<num_tiles, kBwdThreads, 0, st>>>(sp, ranges, order, vals, s, px, g, ctrl);
-    else k_raster_bwd<false><<<num_tiles, kBwdThreads, 0, st>>>(sp, ranges, order, vals, s, px, g, ctrl);
+    if (from_sign)
+        k_raster_bwd<true, PlainAccept><<<num_tiles, kBwdThreads, 0, st>>>(sp, ranges, order, vals, s, px, g, ctrl);
+    else
+        k_raster_bwd<false, PlainAccept><<<num_tiles, kBwdThreads, 0, st>>>(sp, ranges, order, vals, s, px, g, ctrl);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_raster_bwd_fast(cudaStream_t st, const StepParams* sp, int num_tiles, const unsigned* ranges,
+                                   const unsigned* order, const unsigned* vals, ScreenPtrs s, PixelPtrs px,
+                                   RGradPtrs g, Control* ctrl) {
+    if (num_tiles <= 0) return cudaSuccess;
+    k_raster_bwd<true, FastAccept><<<num_tiles, kBwdThreads, 0, st>>>(sp, ranges, order, vals, s, px, g, ctrl);
     return cudaGetLastError();
 }
 

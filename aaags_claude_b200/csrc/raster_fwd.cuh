@@ -1,0 +1,152 @@
+// raster_fwd.cuh -- the forward rasteriser kernel, shared by the plain FP32
+// unit (plain.cu, exact blend decision, no FMA contraction) and the
+// reduced-storage unit (chosen.cu, fast exp, FMA contraction).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+#include "kernels.cuh"
+#include "raster_common.cuh"
+
+namespace gs3d {
+namespace {
+
+// Rasterizer forward (rasterizer_cpu.cpp:38-53, 137-198).  Blend::decide is
+// the alpha / transmittance decision (0 skip, 1 blend, 2 stop): exact in the
+// plain form, fast exp in the reduced-storage form.  One CTA of 128
+// threads per 16x16 tile, two pixels per thread: warp w owns the 16x4 strip
+// of rows 4w..4w+3, a thread the pixels (x, 4w + lane/16) and
+// (x, 4w + 2 + lane/16).  Batches of 256 records are gathered into shared
+// memory; a warp skips a Gaussian whose skip box misses its strip; the CTA
+// stops once every pixel saturated.  Optional fused L1 (sign byte per pixel,
+// double-precision loss sum).
+constexpr int kFwdThreads = 128;
+constexpr int kFwdBatch = 256;
+
+template <bool FUSED_LOSS, class Blend>
+__global__ void __launch_bounds__(kFwdThreads) k_raster_fwd(const StepParams* __restrict__ spp,
+                                                            const unsigned* __restrict__ ranges,
+                                                            const unsigned* __restrict__ order,
+                                                            const unsigned* __restrict__ vals, ScreenPtrs s,
+                                                            PixelPtrs px, Control* ctrl) {
+    __shared__ float4 s_r0[kFwdBatch];
+    __shared__ float4 s_r1[kFwdBatch];
+    __shared__ float s_b[kFwdBatch];
+    __shared__ float s_thr[kFwdBatch];
+    __shared__ float4 s_box[kFwdBatch];
+    __shared__ double s_loss[kFwdThreads / 32];
+    const StepParams& sp = *spp;
+    const int W = sp.cam.width, H = sp.cam.height;
+    const int tile = order ? (int)order[blockIdx.x] : (int)blockIdx.x;
+    const int tx = tile % sp.grid_x, ty = tile / sp.grid_x;
+    const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int x = tx * kTile + (int)(lane & 15);
+    const int ybase = ty * kTile + 4 * (int)warp + (int)(lane >> 4);
+    const unsigned rs = ranges[2 * tile], re = ranges[2 * tile + 1];
+    const float fx = (float)x;
+    const float wx0 = (float)(tx * kTile), wx1 = wx0 + (float)(kTile - 1);
+    const float wy0 = (float)(ty * kTile + 4 * (int)warp), wy1 = wy0 + 3.0f;
+    float fy[2], T[2], C[2][3];
+    int cnt[2];
+    unsigned last[2];
+    bool done[2];
+#pragma unroll
+    for (int p = 0; p < 2; p++) {
+        const int y = ybase + 2 * p;
+        fy[p] = (float)y;
+        T[p] = 1.0f;
+        C[p][0] = C[p][1] = C[p][2] = 0.0f;
+        cnt[p] = 0;
+        last[p] = 0;
+        done[p] = !(x < W && y < H);
+    }
+    for (unsigned b = rs; b < re; b += kFwdBatch) {
+        if (__syncthreads_count(done[0] && done[1]) == kFwdThreads) break;
+#pragma unroll
+        for (int e = threadIdx.x; e < kFwdBatch; e += kFwdThreads) {
+            const unsigned j = b + (unsigned)e;
+            if (j < re) {
+                const unsigned g = vals[j];
+                const float4 r0 = s.rec0[g];
+                const float4 r1 = s.rec1[g];
+                const float thr = skip_threshold(r1.y);
+                s_r0[e] = r0;
+                s_r1[e] = r1;
+                s_b[e] = s.col_b[g];
+                s_thr[e] = thr;
+                s_box[e] = skip_box(r0, r1, thr);
+            }
+        }
+        __syncthreads();
+        const int nb = (int)min((unsigned)kFwdBatch, re - b);
+        for (int k = 0; k < nb; k++) {
+            if (done[0] && done[1]) break;
+            if (box_misses(s_box[k], wx0, wx1, wy0, wy1)) continue;
+            const float4 a = s_r0[k];
+            const float4 c = s_r1[k];
+            const float thr = s_thr[k];
+            const float dx = a.x - fx;
+#pragma unroll
+            for (int p = 0; p < 2; p++) {
+                if (done[p]) continue;
+                const float dy = a.y - fy[p];
+                const float power = power_rn(a, c, dx, dy);
+                if (power < thr || power > 0.0f) continue;
+                float alpha, e, test_T;
+                const int dec = Blend::decide(power, c.y, T[p], alpha, e, test_T);
+                if (dec == 0) continue;
+                if (dec == 2) {
+                    done[p] = true;
+                    continue;
+                }
+                C[p][0] += c.z * alpha * T[p];
+                C[p][1] += c.w * alpha * T[p];
+                C[p][2] += s_b[k] * alpha * T[p];
+                T[p] = test_T;
+                cnt[p]++;
+                last[p] = b + (unsigned)k + 1u;
+            }
+        }
+    }
+    double lsum = 0.0;
+#pragma unroll
+    for (int p = 0; p < 2; p++) {
+        const int y = ybase + 2 * p;
+        if (x < W && y < H) {
+            const int pix = y * W + x;
+            const float o0 = C[p][0] + T[p] * sp.cfg.bg_color[0];
+            const float o1 = C[p][1] + T[p] * sp.cfg.bg_color[1];
+            const float o2 = C[p][2] + T[p] * sp.cfg.bg_color[2];
+            px.image[3 * pix] = o0;
+            px.image[3 * pix + 1] = o1;
+            px.image[3 * pix + 2] = o2;
+            if (px.T_final) px.T_final[pix] = T[p];
+            if (px.n_contrib) px.n_contrib[pix] = cnt[p];
+            if (px.last_j) px.last_j[pix] = last[p];
+            if (FUSED_LOSS) {
+                // loss.cpp:8-14: diff = rendered - gt, sign gradient +-1/n
+                const float d0 = o0 - sp.gt[3 * pix], d1 = o1 - sp.gt[3 * pix + 1], d2 = o2 - sp.gt[3 * pix + 2];
+                const unsigned sg = (d0 > 0.f ? 1u : (d0 < 0.f ? 2u : 0u)) | (d1 > 0.f ? 4u : (d1 < 0.f ? 8u : 0u)) |
+                                    (d2 > 0.f ? 16u : (d2 < 0.f ? 32u : 0u));
+                px.dsign[pix] = (unsigned char)sg;
+                lsum += (double)fabsf(d0) + (double)fabsf(d1) + (double)fabsf(d2);
+            }
+        }
+    }
+    if (FUSED_LOSS) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
+        if (lane == 0) s_loss[warp] = lsum;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = 0.0;
+#pragma unroll
+            for (int w = 0; w < kFwdThreads / 32; w++) t += s_loss[w];
+            atomicAdd(&ctrl->loss_sum, t);
+        }
+    }
+}
+
+}  // namespace
+}  // namespace gs3d

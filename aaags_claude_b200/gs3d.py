@@ -25,8 +25,9 @@ ERR_INVALID_ARG, ERR_CUDA, ERR_PAIR_OVERFLOW, ERR_DEVICE_TIMEOUT, ERR_NO_MODEL, 
 OPT_PAIR_CAPACITY, OPT_USE_GRAPH, OPT_FORM, OPT_SPIN_LIMIT, OPT_STAGE_TIMING, OPT_FUSED_ADAM = 1, 2, 3, 4, 5, 6
 NUM_STAGES = 8
 STAT_TOTAL_PAIRS, STAT_PAIR_CAPACITY, STAT_KERNELS_LAST, STAT_SORT_PASSES, STAT_GRAPH_REPLAYS, STAT_ADAM_STEP = range(1, 7)
-FORM_PLAIN_FP32 = 0
+FORM_PLAIN_FP32, FORM_BF16, FORM_FP16 = 0, 1, 2
 OPT_SORT = 7
+OPT_KEEP_GRADIENTS = 8
 SORT_DEPTH_FIRST, SORT_FULL_KEY = 0, 1
 
 _f = ctypes.POINTER(ctypes.c_float)
@@ -85,6 +86,7 @@ def load_library(path: str = LIB_PATH):
         "gs3dc_synchronize": ([vp], ctypes.c_int),
         "gs3dc_get_stage_times": ([vp, ctypes.POINTER(ctypes.c_float), ctypes.c_int], ctypes.c_int),
         "gs3dc_selftest_bounded_wait": ([vp, ctypes.c_uint32], ctypes.c_int),
+        "gs3dc_get_gradients": ([vp, vp, vp, vp, vp, vp], ctypes.c_int),
         "gs3dc_sort_pairs_static": ([i64, vp, vp, ctypes.c_int, vp, vp, vp, vp, ctypes.c_char_p, ctypes.c_size_t],
                                     ctypes.c_int),
     }
@@ -293,6 +295,14 @@ class Context:
     def update_raw_params(self, scene: S.Scene):
         r = scene.raw_struct()
         self._chk(self.L.gs3dc_update_raw_params(self.h, _ref(r)))
+
+    def get_gradients(self) -> dict:
+        """Raw-parameter gradients of the last train step (GS3DC_OPT_KEEP_GRADIENTS)."""
+        n, mc3 = self._model[1], self._model[2] * 3
+        g = dict(pos=np.zeros(3 * n, np.float32), sc=np.zeros(3 * n, np.float32), rot=np.zeros(4 * n, np.float32),
+                 sh=np.zeros(mc3 * n, np.float32), op=np.zeros(n, np.float32))
+        self._chk(self.L.gs3dc_get_gradients(self.h, *[_p(g[k]) for k in ("pos", "sc", "rot", "sh", "op")]))
+        return g
 
     def get_image(self, cam) -> np.ndarray:
         img = np.zeros(3 * cam.width * cam.height, np.float32)

@@ -57,6 +57,8 @@ def _args(argv=None):
     ap.add_argument("--fused-adam", type=int, default=None, help="1: optimiser fused into the backward kernel")
     ap.add_argument("--sort", choices=("depth-first", "full-key"), default="depth-first",
                     help="pair ordering of the train step")
+    ap.add_argument("--form", choices=("plain", "bf16", "fp16"), default="plain",
+                    help="plain FP32 (parity) or the reduced-storage form of the train step")
     return ap.parse_args(argv)
 
 
@@ -236,9 +238,11 @@ def run_ours(a) -> int:
         ctx.set_option(gs3d.OPT_FUSED_ADAM, a.fused_adam)
     depth_first = a.sort == "depth-first"
     ctx.set_option(gs3d.OPT_SORT, gs3d.SORT_DEPTH_FIRST if depth_first else gs3d.SORT_FULL_KEY)
-    # target image: the perturbed scene rendered by this library (setup, untimed)
+    # target image: the perturbed scene rendered by this library's plain form (setup, untimed)
     ctx.set_raw_params(w.target_scene)
     gt = ctx.render(cam, S.render_config(False))
+    ctx.set_option(gs3d.OPT_FORM, {"plain": gs3d.FORM_PLAIN_FP32, "bf16": gs3d.FORM_BF16,
+                                   "fp16": gs3d.FORM_FP16}[a.form])
     ctx.set_raw_params(w.scene)
     gt_dev = torch.from_numpy(gt).to(f"cuda:{local}")
     gt_pin = torch.from_numpy(gt).pin_memory()
@@ -319,8 +323,9 @@ def run_ours(a) -> int:
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "steps/s", "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded; no dataset or checkpoint)",
-            "form": "plain_fp32",
+            "vs_baseline": None, "dtype": "f32" if a.form == "plain" else a.form + "-storage/f32",
+            "data": "synthetic (seeded; no dataset or checkpoint)",
+            "form": "plain_fp32" if a.form == "plain" else a.form,
             "config": {"workload": _workload_name(a), "gaussians": w.scene.count, "sh_degree": 3, "width": W,
                        "height": H,
                        "tile": 16, "tile_pairs": P, "sort_passes": passes,

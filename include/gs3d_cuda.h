@@ -46,6 +46,7 @@ typedef struct gs3dc_ctx gs3dc_ctx;
 #define GS3DC_OPT_STAGE_TIMING   5  /* 1: train steps run un-captured with CUDA events between stages */
 #define GS3DC_OPT_FUSED_ADAM     6  /* 1: optimiser fused into the preprocess backward; 0 (default): split */
 #define GS3DC_OPT_SORT           7  /* GS3DC_SORT_*: how gs3dc_train_step orders its pairs (same result) */
+#define GS3DC_OPT_KEEP_GRADIENTS 8  /* 1: gs3dc_train_step keeps its raw-parameter gradients (gs3dc_get_gradients) */
 
 /* Depth-first (default): the Gaussians are stably sorted by depth, their pairs
  * emitted in that order and stably sorted by the tile bits alone.  Full key:
@@ -54,6 +55,16 @@ typedef struct gs3dc_ctx gs3dc_ctx;
 #define GS3DC_SORT_FULL_KEY      1
 
 #define GS3DC_FORM_PLAIN_FP32    0  /* FP32 everywhere, no FMA contraction: parity form */
+/* Reduced storage ("chosen" form) of gs3dc_train_step: positions FP32; raw
+ * scales, opacity, rotation and SH coefficients 16-bit; Adam moments BF16 (FP32
+ * for positions); FP32 blending and gradients with FMA and fast exp; tile
+ * rectangles cut to where alpha can reach 1/255; parameters written back with
+ * stochastic rounding.  gs3dc_set_raw_params / gs3dc_get_raw_params convert
+ * from / to FP32.  The stage calls (preprocess ... optimizer_step, render)
+ * need the plain form.  Changing the form keeps the model (converted) and
+ * restarts the optimiser state. */
+#define GS3DC_FORM_BF16          1
+#define GS3DC_FORM_FP16          2
 
 /* ---- statistics (gs3dc_get_stat) ---- */
 #define GS3DC_STAT_TOTAL_PAIRS    1  /* tile pairs of the last forward */
@@ -228,6 +239,13 @@ int gs3dc_get_stage_times(gs3dc_ctx* ctx, float* ms, int n_stages);
  * context stays usable afterwards.  No reference counterpart: it exercises the
  * bounded-wait failure path that every look-back of this library relies on. */
 int gs3dc_selftest_bounded_wait(gs3dc_ctx* ctx, uint32_t spin_limit);
+
+/* The raw-parameter gradients (FP32, reference layouts) of the last
+ * gs3dc_train_step run with GS3DC_OPT_KEEP_GRADIENTS.  No reference
+ * counterpart: Trainer::step keeps its GradientOutput internal.  Host arrays
+ * may be NULL. */
+int gs3dc_get_gradients(gs3dc_ctx* ctx, float* d_raw_positions, float* d_raw_scales,
+                        float* d_raw_rotations, float* d_raw_sh_coeffs, float* d_raw_opacities);
 
 /* Blocks until every call issued on the context's stream has finished and
  * reports any deferred device-side error (pair overflow, timeout). */
