@@ -30,7 +30,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=o
 SOURCES = {
     "plain.cu": ["-fmad=false", "-prec-div=true", "-prec-sqrt=true"],
     "raster_bwd.cu": [],   # gradients: FMA contraction allowed
-    "chosen.cu": [],       # reduced-storage form: FMA contraction, fast exp
+    "chosen.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"],   # reduced-storage form: fast math
     "sort.cu": [],
     "sort_static.cu": [],
     "capi.cu": [],

@@ -546,11 +546,9 @@ int seq_train_chosen(gs3dc_ctx* c) {
                               screen_ptrs(c, false), pixel_ptrs(c), rgrad_ptrs(c), c->ctrl));
     if ((rc = mark(c, GS3DC_STAGE_PREPROCESS_BWD))) return rc;
     CK(launch_chosen_backward_adam(c->stream, c->sp_dev, c->N, c->max_coeffs * 3, c->form == GS3DC_FORM_FP16,
-                                   chosen_ptrs(c), rgrad_ptrs(c),
-                                   c->keep_grads ? grad_ptrs(c) : GradPtrs{nullptr, nullptr, nullptr, nullptr, nullptr},
-                                   c->ctrl));
+                                   chosen_ptrs(c), rgrad_ptrs(c), grad_ptrs(c), c->ctrl));
     if ((rc = mark(c, GS3DC_NUM_STAGES))) return rc;
-    c->kernels_last += 3;
+    c->kernels_last += 4;
     return GS3DC_OK;
 }
 

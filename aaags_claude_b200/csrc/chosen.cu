@@ -207,7 +207,148 @@ __global__ void __launch_bounds__(kBlock) k_chosen_preprocess(const StepParams* 
     dk.vals[i] = (unsigned)i;
 }
 
-// ---- fused adjoint + Adam ----
+// ---- adjoint (staged, coalesced) ----
+
+constexpr int kCB = 128;          // Gaussians (= threads) per CTA of the adjoint
+constexpr int kShPitch = 49;      // padded row of the per-Gaussian SH gradients in shared memory
+
+template <typename S>
+struct __align__(16) ChosenBwdShared {
+    uint4 sh[kCB * 6];            // 16-bit SH, up to 48 per Gaussian (6 x 16 bytes)
+    uint4 attr[kCB];              // 16-bit attributes, 8 per Gaussian
+    float pos[3 * kCB];
+    float dm2[2 * kCB], dcon[3 * kCB], drgb[3 * kCB], dop[kCB];
+    float g_pos[3 * kCB], g_sc[3 * kCB], g_rot[4 * kCB], g_op[kCB];
+    float g_sh[kShPitch * kCB];
+    unsigned long long bar;       // completion of the bulk copies into the arrays above
+};
+
+// One CTA per 128 consecutive Gaussians: coalesced loads of their parameters
+// and screen gradients into shared memory (the accumulators are zeroed for the
+// next step), the per-Gaussian adjoint of PreprocessorBackwardCPU::backward
+// (preprocessor_backward_cpu.cpp:205-645) from there, and coalesced stores of
+// the FP32 raw-parameter gradients.
+template <typename S>
+__global__ void __launch_bounds__(kCB) k_chosen_backward(const StepParams* __restrict__ spp, int N, int mc3,
+                                                         ChosenPtrs c, RGradPtrs rg, GradPtrs gout, Control* ctrl) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    ChosenBwdShared<S>& sm = *reinterpret_cast<ChosenBwdShared<S>*>(smem_raw);
+    const StepParams& sp = *spp;
+    if ((ctrl->status & (kStatusOverflow | kStatusTimeout)) || sp.persist->sticky_overflow) return;
+    const int tid = threadIdx.x;
+    const long long g0 = (long long)blockIdx.x * kCB;
+    const int ng = (int)min((long long)kCB, (long long)N - g0);
+    // ---- phase 0: staging ----
+    const S* shg = static_cast<const S*>(c.sh) + (size_t)mc3 * g0;
+    if (ng == kCB) {
+        // a full CTA: every slice is a multiple of 16 bytes at a 16-byte aligned offset -> bulk copies
+        if (tid == 0) {
+            mbar_init(&sm.bar, 1);
+            mbar_fence_init();
+        }
+        __syncthreads();
+        if (tid == 0) {
+            const unsigned sh_bytes = (unsigned)(kCB * mc3 * (int)sizeof(S));
+            mbar_arrive_expect_tx(&sm.bar, sh_bytes + (unsigned)kCB * (16u + 12u + 8u + 12u + 12u + 4u));
+            tma_load_1d(sm.sh, shg, sh_bytes, &sm.bar);
+            tma_load_1d(sm.attr, reinterpret_cast<const uint4*>(c.attr) + g0, 16u * kCB, &sm.bar);
+            tma_load_1d(sm.pos, c.pos + 3 * g0, 12u * kCB, &sm.bar);
+            tma_load_1d(sm.dm2, rg.dm2 + 2 * g0, 8u * kCB, &sm.bar);
+            tma_load_1d(sm.dcon, rg.dcon + 3 * g0, 12u * kCB, &sm.bar);
+            tma_load_1d(sm.drgb, rg.drgb + 3 * g0, 12u * kCB, &sm.bar);
+            tma_load_1d(sm.dop, rg.dop + g0, 4u * kCB, &sm.bar);
+        }
+        mbar_wait(&sm.bar, 0, sp.spin_limit, &ctrl->status);
+    } else {
+        S* shs = reinterpret_cast<S*>(sm.sh);
+        for (int e = tid; e < mc3 * ng; e += kCB) shs[e] = shg[e];
+        for (int e = tid; e < ng; e += kCB) sm.attr[e] = reinterpret_cast<const uint4*>(c.attr)[g0 + e];
+        for (int e = tid; e < 3 * ng; e += kCB) sm.pos[e] = c.pos[3 * g0 + e];
+        for (int e = tid; e < 2 * ng; e += kCB) sm.dm2[e] = rg.dm2[2 * g0 + e];
+        for (int e = tid; e < 3 * ng; e += kCB) {
+            sm.dcon[e] = rg.dcon[3 * g0 + e];
+            sm.drgb[e] = rg.drgb[3 * g0 + e];
+        }
+        for (int e = tid; e < ng; e += kCB) sm.dop[e] = rg.dop[g0 + e];
+        __syncthreads();
+    }
+    // the screen-gradient accumulators restart at zero for the next step
+    for (int e = tid; e < 2 * ng; e += kCB) rg.dm2[2 * g0 + e] = 0.f;
+    for (int e = tid; e < 3 * ng; e += kCB) {
+        rg.dcon[3 * g0 + e] = 0.f;
+        rg.drgb[3 * g0 + e] = 0.f;
+    }
+    for (int e = tid; e < ng; e += kCB) rg.dop[g0 + e] = 0.f;
+    // ---- phase 1: per-Gaussian adjoint ----
+    if (tid < ng) {
+        BwdIn in;
+        BwdOut o;
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            in.p[k] = sm.pos[3 * tid + k];
+            in.dcn[k] = sm.dcon[3 * tid + k];
+            in.drgb[k] = sm.drgb[3 * tid + k];
+            o.gp[k] = o.gs[k] = o.geff[k] = 0.f;
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++) o.gq[k] = 0.f;
+        o.gop = 0.f;
+#pragma unroll
+        for (int k = 0; k < 16; k++) o.basis[k] = 0.f;
+        in.dm[0] = sm.dm2[2 * tid];
+        in.dm[1] = sm.dm2[2 * tid + 1];
+        in.dop = sm.dop[tid];
+        in.act = nullptr;
+        load_attr<S>(sm.attr, tid, in.rsc, &in.rop, in.rq);
+        // every gradient is linear in the screen gradients: a Gaussian without any has none
+        const bool any = in.dm[0] != 0.f || in.dm[1] != 0.f || in.dcn[0] != 0.f || in.dcn[1] != 0.f ||
+                         in.dcn[2] != 0.f || in.drgb[0] != 0.f || in.drgb[1] != 0.f || in.drgb[2] != 0.f ||
+                         in.dop != 0.f;
+        if (any) {
+            float shf[48];
+            if (mc3 == 48) {
+                // this Gaussian's 96 SH bytes as six 16-byte loads
+                const uint4* row = sm.sh + 6 * tid;
+#pragma unroll
+                for (int q = 0; q < 6; q++) {
+                    const uint4 v = row[q];
+                    const S* h = reinterpret_cast<const S*>(&v);
+#pragma unroll
+                    for (int k = 0; k < 8; k++) shf[8 * q + k] = ldf(h[k]);
+                }
+            } else {
+                const S* shs = reinterpret_cast<const S*>(sm.sh) + mc3 * tid;
+#pragma unroll
+                for (int k = 0; k < 48; k++) shf[k] = k < mc3 ? ldf(shs[k]) : 0.f;
+            }
+            in.sh = shf;
+            backward_one(sp, in, o);
+        }
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            sm.g_pos[3 * tid + k] = o.gp[k];
+            sm.g_sc[3 * tid + k] = o.gs[k];
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++) sm.g_rot[4 * tid + k] = o.gq[k];
+        sm.g_op[tid] = o.gop;
+        for (int k = 0; k < mc3; k++) sm.g_sh[kShPitch * tid + k] = o.basis[k / 3] * o.geff[k % 3];
+    }
+    __syncthreads();
+    // ---- phase 2: coalesced stores ----
+    for (int e = tid; e < 3 * ng; e += kCB) {
+        gout.g_pos[3 * g0 + e] = sm.g_pos[e];
+        gout.g_sc[3 * g0 + e] = sm.g_sc[e];
+    }
+    for (int e = tid; e < 4 * ng; e += kCB) gout.g_rot[4 * g0 + e] = sm.g_rot[e];
+    for (int e = tid; e < ng; e += kCB) gout.g_op[g0 + e] = sm.g_op[e];
+    for (int e = tid; e < mc3 * ng; e += kCB) {
+        const int t = e / mc3, k = e - t * mc3;
+        gout.g_sh[(size_t)mc3 * g0 + e] = sm.g_sh[kShPitch * t + k];
+    }
+}
+
+// ---- optimiser (streaming) ----
 
 // Adam (optimizer.cpp:32-43 in FP32) or SGD on one element; the moments come
 // in and go out as floats.
@@ -216,121 +357,72 @@ __device__ __forceinline__ float opt_elem(const StepParams& sp, float p, float& 
     return p - lr * g;
 }
 
-constexpr int kCBwdThreads = 128;
+// Eight consecutive 16-bit parameters with their BF16 moments and FP32
+// gradients: one 16-byte load / store per array, stochastic rounding.
+template <typename S>
+__device__ __forceinline__ void opt8(const StepParams& sp, uint4* p16, uint4* m16, uint4* v16, const float* g,
+                                     const float* lr, unsigned e0, unsigned salt) {
+    uint4 praw = *p16, mraw = *m16, vraw = *v16;
+    S* pb = reinterpret_cast<S*>(&praw);
+    __nv_bfloat16* mb = reinterpret_cast<__nv_bfloat16*>(&mraw);
+    __nv_bfloat16* vb = reinterpret_cast<__nv_bfloat16*>(&vraw);
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        float m = __bfloat162float(mb[k]), v = __bfloat162float(vb[k]);
+        const float pn = opt_elem(sp, ldf(pb[k]), m, v, g[k], lr[k]);
+        const unsigned e = (e0 + (unsigned)k) ^ salt;
+        pb[k] = cvt_sr<S>(pn, mix32(e, sp.seed));
+        mb[k] = cvt_sr<__nv_bfloat16>(m, mix32(e, sp.seed ^ 0x68E31DA4u));
+        vb[k] = cvt_sr<__nv_bfloat16>(v, mix32(e, sp.seed ^ 0xB5297A4Du));
+    }
+    *p16 = praw;
+    *m16 = mraw;
+    *v16 = vraw;
+}
 
 template <typename S>
-__global__ void __launch_bounds__(kCBwdThreads) k_chosen_backward_adam(const StepParams* __restrict__ spp, int N,
-                                                                       int mc3, ChosenPtrs c, RGradPtrs rg,
-                                                                       GradPtrs gout, Control* ctrl) {
+__global__ void __launch_bounds__(256) k_chosen_adam(const StepParams* __restrict__ spp, int N, int mc3,
+                                                     ChosenPtrs c, GradPtrs g, const Control* ctrl) {
     const StepParams& sp = *spp;
-    // an overflowed (or timed-out) step, or any step after one the host has not
-    // acknowledged yet, updates nothing
     if ((ctrl->status & (kStatusOverflow | kStatusTimeout)) || sp.persist->sticky_overflow) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i == 0 && sp.use_adam) atomicAdd(&sp.persist->applied_steps, 1ull);
-    if (i >= N) return;
-    const unsigned seed = sp.seed;
-
-    // screen gradients of this Gaussian; the accumulators restart at zero
-    float dm[2] = {rg.dm2[2 * i], rg.dm2[2 * i + 1]};
-    float dcn[3] = {rg.dcon[3 * i], rg.dcon[3 * i + 1], rg.dcon[3 * i + 2]};
-    float drgb[3] = {rg.drgb[3 * i], rg.drgb[3 * i + 1], rg.drgb[3 * i + 2]};
-    const float dop = rg.dop[i];
-    rg.dm2[2 * i] = rg.dm2[2 * i + 1] = 0.f;
-    rg.dcon[3 * i] = rg.dcon[3 * i + 1] = rg.dcon[3 * i + 2] = 0.f;
-    rg.drgb[3 * i] = rg.drgb[3 * i + 1] = rg.drgb[3 * i + 2] = 0.f;
-    rg.dop[i] = 0.f;
-
-    BwdIn in;
-    BwdOut o;
-#pragma unroll
-    for (int k = 0; k < 3; k++) {
-        in.p[k] = c.pos[3 * i + k];
-        o.gp[k] = o.gs[k] = o.geff[k] = 0.f;
-        in.dcn[k] = dcn[k];
-        in.drgb[k] = drgb[k];
+    if (blockIdx.x == 0 && threadIdx.x == 0 && sp.use_adam) atomicAdd(&sp.persist->applied_steps, 1ull);
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    // SH: chunks of 8 consecutive coefficients
+    const long long n_sh = (long long)N * mc3;
+    const float lr_sh[8] = {sp.lr_sh, sp.lr_sh, sp.lr_sh, sp.lr_sh, sp.lr_sh, sp.lr_sh, sp.lr_sh, sp.lr_sh};
+    for (long long q = t0; q < n_sh / 8; q += stride) {
+        const float4 ga = reinterpret_cast<const float4*>(g.g_sh)[2 * q];
+        const float4 gb = reinterpret_cast<const float4*>(g.g_sh)[2 * q + 1];
+        const float gg[8] = {ga.x, ga.y, ga.z, ga.w, gb.x, gb.y, gb.z, gb.w};
+        opt8<S>(sp, reinterpret_cast<uint4*>(c.sh) + q, reinterpret_cast<uint4*>(c.m_sh) + q,
+                reinterpret_cast<uint4*>(c.v_sh) + q, gg, lr_sh, (unsigned)(8 * q), 0x5bd1e995u);
     }
-#pragma unroll
-    for (int k = 0; k < 4; k++) o.gq[k] = 0.f;
-    o.gop = 0.f;
-#pragma unroll
-    for (int k = 0; k < 16; k++) o.basis[k] = 0.f;
-    load_attr<S>(c.attr, i, in.rsc, &in.rop, in.rq);
-    in.dm[0] = dm[0];
-    in.dm[1] = dm[1];
-    in.dop = dop;
-    in.act = nullptr;
-    const S* shp = static_cast<const S*>(c.sh) + (size_t)mc3 * i;
-    float shf[48];
-#pragma unroll
-    for (int k = 0; k < 48; k++) shf[k] = k < mc3 ? ldf(shp[k]) : 0.f;
-    in.sh = shf;
-    // every gradient is linear in the screen gradients: a Gaussian without any has none
-    const bool any = dm[0] != 0.f || dm[1] != 0.f || dcn[0] != 0.f || dcn[1] != 0.f || dcn[2] != 0.f ||
-                     drgb[0] != 0.f || drgb[1] != 0.f || drgb[2] != 0.f || dop != 0.f;
-    if (any) backward_one(sp, in, o);
-    if (gout.g_pos) {
-#pragma unroll
-        for (int k = 0; k < 3; k++) {
-            gout.g_pos[3 * i + k] = o.gp[k];
-            gout.g_sc[3 * i + k] = o.gs[k];
-        }
-#pragma unroll
-        for (int k = 0; k < 4; k++) gout.g_rot[4 * i + k] = o.gq[k];
-        gout.g_op[i] = o.gop;
-        for (int k = 0; k < mc3; k++) gout.g_sh[(size_t)mc3 * i + k] = o.basis[k / 3] * o.geff[k % 3];
+    for (long long e = 8 * (n_sh / 8) + t0; e < n_sh; e += stride) {
+        S* p = static_cast<S*>(c.sh) + e;
+        __nv_bfloat16* mp = static_cast<__nv_bfloat16*>(c.m_sh) + e;
+        __nv_bfloat16* vp = static_cast<__nv_bfloat16*>(c.v_sh) + e;
+        float m = __bfloat162float(*mp), v = __bfloat162float(*vp);
+        const float pn = opt_elem(sp, ldf(*p), m, v, g.g_sh[e], sp.lr_sh);
+        const unsigned h = (unsigned)e ^ 0x5bd1e995u;
+        *p = cvt_sr<S>(pn, mix32(h, sp.seed));
+        *mp = cvt_sr<__nv_bfloat16>(m, mix32(h, sp.seed ^ 0x68E31DA4u));
+        *vp = cvt_sr<__nv_bfloat16>(v, mix32(h, sp.seed ^ 0xB5297A4Du));
     }
-
-    // ---- optimiser: positions (FP32 state) ----
-#pragma unroll
-    for (int k = 0; k < 3; k++) {
-        float m = c.m_pos[3 * i + k], v = c.v_pos[3 * i + k];
-        c.pos[3 * i + k] = opt_elem(sp, in.p[k], m, v, o.gp[k], sp.lr_pos);
-        c.m_pos[3 * i + k] = m;
-        c.v_pos[3 * i + k] = v;
+    // attributes: one 16-byte record per Gaussian; positions: FP32
+    const float lra[8] = {sp.lr_scale, sp.lr_scale, sp.lr_scale, sp.lr_opac, sp.lr_rot, sp.lr_rot, sp.lr_rot,
+                          sp.lr_rot};
+    for (long long i = t0; i < N; i += stride) {
+        const float gg[8] = {g.g_sc[3 * i], g.g_sc[3 * i + 1], g.g_sc[3 * i + 2], g.g_op[i],
+                             g.g_rot[4 * i], g.g_rot[4 * i + 1], g.g_rot[4 * i + 2], g.g_rot[4 * i + 3]};
+        opt8<S>(sp, reinterpret_cast<uint4*>(c.attr) + i, reinterpret_cast<uint4*>(c.m_attr) + i,
+                reinterpret_cast<uint4*>(c.v_attr) + i, gg, lra, (unsigned)(8 * i), 0u);
     }
-    // ---- attributes: 8 x 16-bit, moments BF16 ----
-    {
-        const float pa[8] = {in.rsc[0], in.rsc[1], in.rsc[2], in.rop, in.rq[0], in.rq[1], in.rq[2], in.rq[3]};
-        const float ga[8] = {o.gs[0], o.gs[1], o.gs[2], o.gop, o.gq[0], o.gq[1], o.gq[2], o.gq[3]};
-        const float lra[8] = {sp.lr_scale, sp.lr_scale, sp.lr_scale, sp.lr_opac, sp.lr_rot, sp.lr_rot, sp.lr_rot,
-                              sp.lr_rot};
-        uint4 mraw = reinterpret_cast<const uint4*>(c.m_attr)[i];
-        uint4 vraw = reinterpret_cast<const uint4*>(c.v_attr)[i];
-        __nv_bfloat16* mb = reinterpret_cast<__nv_bfloat16*>(&mraw);
-        __nv_bfloat16* vb = reinterpret_cast<__nv_bfloat16*>(&vraw);
-        uint4 praw;
-        S* pb = reinterpret_cast<S*>(&praw);
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-            float m = __bfloat162float(mb[k]), v = __bfloat162float(vb[k]);
-            const float pn = opt_elem(sp, pa[k], m, v, ga[k], lra[k]);
-            const unsigned e = (unsigned)(8 * i + k);
-            pb[k] = cvt_sr<S>(pn, mix32(e, seed));
-            mb[k] = cvt_sr<__nv_bfloat16>(m, mix32(e, seed ^ 0x68E31DA4u));
-            vb[k] = cvt_sr<__nv_bfloat16>(v, mix32(e, seed ^ 0xB5297A4Du));
-        }
-        reinterpret_cast<uint4*>(c.attr)[i] = praw;
-        reinterpret_cast<uint4*>(c.m_attr)[i] = mraw;
-        reinterpret_cast<uint4*>(c.v_attr)[i] = vraw;
-    }
-    // ---- SH: gradient basis[k] * geff[channel], moments BF16 ----
-    {
-        S* shw = static_cast<S*>(c.sh) + (size_t)mc3 * i;
-        __nv_bfloat16* msh = static_cast<__nv_bfloat16*>(c.m_sh) + (size_t)mc3 * i;
-        __nv_bfloat16* vsh = static_cast<__nv_bfloat16*>(c.v_sh) + (size_t)mc3 * i;
-#pragma unroll
-        for (int k = 0; k < 48; k++) {
-            if (k < mc3) {
-                const float g = o.basis[k / 3] * o.geff[k % 3];
-                float m = __bfloat162float(msh[k]), v = __bfloat162float(vsh[k]);
-                const float pn = opt_elem(sp, shf[k], m, v, g, sp.lr_sh);
-                const unsigned e = (unsigned)((size_t)mc3 * i + k) ^ 0x5bd1e995u;
-                shw[k] = cvt_sr<S>(pn, mix32(e, seed));
-                msh[k] = cvt_sr<__nv_bfloat16>(m, mix32(e, seed ^ 0x68E31DA4u));
-                vsh[k] = cvt_sr<__nv_bfloat16>(v, mix32(e, seed ^ 0xB5297A4Du));
-            }
-        }
+    for (long long e = t0; e < 3LL * N; e += stride) {
+        float m = c.m_pos[e], v = c.v_pos[e];
+        c.pos[e] = opt_elem(sp, c.pos[e], m, v, g.g_pos[e], sp.lr_pos);
+        c.m_pos[e] = m;
+        c.v_pos[e] = v;
     }
 }
 
@@ -371,12 +463,26 @@ cudaError_t launch_raster_fwd_fast(cudaStream_t st, const StepParams* sp, int nu
 }
 
 cudaError_t launch_chosen_backward_adam(cudaStream_t st, const StepParams* sp, int N, int mc3, bool fp16,
-                                        ChosenPtrs c, RGradPtrs rg, GradPtrs gout, Control* ctrl) {
+                                        ChosenPtrs c, RGradPtrs rg, GradPtrs g, Control* ctrl) {
     if (N <= 0) return cudaSuccess;
-    if (mc3 > 48) return cudaErrorInvalidValue;
-    const int grid = grid_for(N, kCBwdThreads);
-    if (fp16) k_chosen_backward_adam<__half><<<grid, kCBwdThreads, 0, st>>>(sp, N, mc3, c, rg, gout, ctrl);
-    else k_chosen_backward_adam<__nv_bfloat16><<<grid, kCBwdThreads, 0, st>>>(sp, N, mc3, c, rg, gout, ctrl);
+    if (mc3 > 48 || !g.g_pos) return cudaErrorInvalidValue;
+    const int grid = grid_for(N, kCB);
+    const int smem = (int)sizeof(ChosenBwdShared<__half>);   // same size for both 16-bit types
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaError_t e1 = cudaFuncSetAttribute(k_chosen_backward<__half>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaError_t e2 =
+            cudaFuncSetAttribute(k_chosen_backward<__nv_bfloat16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e1 != cudaSuccess) return e1;
+        if (e2 != cudaSuccess) return e2;
+        attr_set = true;
+    }
+    if (fp16) k_chosen_backward<__half><<<grid, kCB, smem, st>>>(sp, N, mc3, c, rg, g, ctrl);
+    else k_chosen_backward<__nv_bfloat16><<<grid, kCB, smem, st>>>(sp, N, mc3, c, rg, g, ctrl);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    if (fp16) k_chosen_adam<__half><<<8 * 148, 256, 0, st>>>(sp, N, mc3, c, g, ctrl);
+    else k_chosen_adam<__nv_bfloat16><<<8 * 148, 256, 0, st>>>(sp, N, mc3, c, g, ctrl);
     return cudaGetLastError();
 }
 

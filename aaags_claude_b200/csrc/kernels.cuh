@@ -115,9 +115,9 @@ cudaError_t launch_raster_fwd_fast(cudaStream_t st, const StepParams* sp, int nu
 cudaError_t launch_raster_bwd_fast(cudaStream_t st, const StepParams* sp, int num_tiles, const unsigned* ranges,
                                    const unsigned* order, const unsigned* vals, ScreenPtrs s, PixelPtrs px,
                                    RGradPtrs g, Control* ctrl);
-// Per-Gaussian adjoint fused with Adam (stochastic rounding into the 16-bit
-// parameters and BF16 moments); zeroes the screen-gradient accumulators.
-// With gout.g_pos != NULL the FP32 raw-parameter gradients are stored too.
+// Per-Gaussian adjoint (FP32 raw-parameter gradients into g; zeroes the
+// screen-gradient accumulators) then the streaming optimiser (stochastic
+// rounding into the 16-bit parameters and BF16 moments).
 cudaError_t launch_chosen_backward_adam(cudaStream_t st, const StepParams* sp, int N, int mc3, bool fp16,
                                         ChosenPtrs c, RGradPtrs rg, GradPtrs gout, Control* ctrl);
 
