@@ -78,7 +78,7 @@ struct gs3dc_ctx {
     int sort_passes = 0, sort_num_tiles = 0;
     // depth-first ordering of the train step: Gaussian depth sort buffers
     int sort_mode = GS3DC_SORT_DEPTH_FIRST;
-    DevBuf<unsigned long long> dkeys[2];
+    DevBuf<unsigned> dkeys[2];
     DevBuf<unsigned> dvals[2];
     DevBuf<unsigned long long> ddesc;
     unsigned long long ddesc_stride = 0;
@@ -515,9 +515,9 @@ int seq_front_depth_first(gs3dc_ctx* c) {
                                    screen_ptrs(c, false), pr, c->ctrl, DepthKeys{c->dkeys[0].p, c->dvals[0].p}));
     if ((rc = mark(c, GS3DC_STAGE_SORT_HIST))) return rc;
     int dw = 0;
-    CK(launch_radix_sort(c->stream, c->sp_dev, kDepthDigits, (unsigned long long)c->N, c->dkeys[0].p, c->dvals[0].p,
-                         c->dkeys[1].p, c->dvals[1].p, c->ddesc.p, c->ddesc_stride, c->ctrl, &dw, nullptr, 0,
-                         &c->ctrl->gauss_keys));
+    CK(launch_radix_sort32(c->stream, c->sp_dev, kDepthDigits, 0, false, (unsigned long long)c->N, c->dkeys[0].p,
+                           c->dvals[0].p, c->dkeys[1].p, c->dvals[1].p, c->ddesc.p, c->ddesc_stride, c->ctrl, &dw,
+                           nullptr, &c->ctrl->gauss_keys));
     CK(launch_emit_ranked(c->stream, c->sp_dev, c->N, c->dvals[dw].p, screen_ptrs(c, false), pr, c->ctrl,
                           chosen ? c->c_rects.p : nullptr));
     if ((rc = mark(c, GS3DC_STAGE_SORT_PASSES))) return rc;
@@ -546,9 +546,11 @@ int seq_train_chosen(gs3dc_ctx* c) {
                               screen_ptrs(c, false), pixel_ptrs(c), rgrad_ptrs(c), c->ctrl));
     if ((rc = mark(c, GS3DC_STAGE_PREPROCESS_BWD))) return rc;
     CK(launch_chosen_backward_adam(c->stream, c->sp_dev, c->N, c->max_coeffs * 3, c->form == GS3DC_FORM_FP16,
-                                   chosen_ptrs(c), rgrad_ptrs(c), grad_ptrs(c), c->ctrl));
+                                   chosen_ptrs(c), rgrad_ptrs(c),
+                                   c->keep_grads ? grad_ptrs(c) : GradPtrs{nullptr, nullptr, nullptr, nullptr, nullptr},
+                                   c->ctrl));
     if ((rc = mark(c, GS3DC_NUM_STAGES))) return rc;
-    c->kernels_last += 4;
+    c->kernels_last += 3;
     return GS3DC_OK;
 }
 

@@ -203,8 +203,45 @@ __global__ void __launch_bounds__(kBlock) k_chosen_preprocess(const StepParams* 
     }
     s.tiles[i] = cnt;
     rects[i] = rect;
-    dk.keys[i] = cnt > 0 ? (unsigned long long)dbits : 0xFFFFFFFFull;
+    dk.keys[i] = cnt > 0 ? dbits : 0xFFFFFFFFu;
     dk.vals[i] = (unsigned)i;
+}
+
+// ---- optimiser helpers ----
+
+// Adam (optimizer.cpp:32-43 in FP32) or SGD on one element; the moments come
+// in and go out as floats.
+__device__ __forceinline__ float opt_elem(const StepParams& sp, float p, float& m, float& v, float g, float lr) {
+    if (sp.use_adam) return adam_elem(p, m, v, g, lr, sp.beta1, sp.beta2, sp.eps, sp.bc1, sp.bc2);
+    return p - lr * g;
+}
+
+// Random words of one element's three roundings: the hash of (element, step)
+// and two LCG steps from it.
+__device__ __forceinline__ void sr_words(unsigned e, unsigned seed, unsigned& rp, unsigned& rm, unsigned& rv) {
+    rp = mix32(e, seed);
+    rm = rp * 0x2C1B3C6Du + 0x297A2D39u;
+    rv = rm * 0x2C1B3C6Du + 0x297A2D39u;
+}
+
+// Eight consecutive 16-bit parameters (p) with their BF16 moments (m, v),
+// updated in registers; e0 = the first element's global index.
+template <typename S>
+__device__ __forceinline__ void opt8(const StepParams& sp, uint4& p, uint4& m, uint4& v, const float g[8],
+                                     const float lr[8], unsigned e0, unsigned salt) {
+    S* pb = reinterpret_cast<S*>(&p);
+    __nv_bfloat16* mb = reinterpret_cast<__nv_bfloat16*>(&m);
+    __nv_bfloat16* vb = reinterpret_cast<__nv_bfloat16*>(&v);
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        float mm = __bfloat162float(mb[k]), vv = __bfloat162float(vb[k]);
+        const float pn = opt_elem(sp, ldf(pb[k]), mm, vv, g[k], lr[k]);
+        unsigned rp, rm, rv;
+        sr_words((e0 + (unsigned)k) ^ salt, sp.seed, rp, rm, rv);
+        pb[k] = cvt_sr<S>(pn, rp);
+        mb[k] = cvt_sr<__nv_bfloat16>(mm, rm);
+        vb[k] = cvt_sr<__nv_bfloat16>(vv, rv);
+    }
 }
 
 // ---- adjoint (staged, coalesced) ----
@@ -223,11 +260,12 @@ struct __align__(16) ChosenBwdShared {
     unsigned long long bar;       // completion of the bulk copies into the arrays above
 };
 
-// One CTA per 128 consecutive Gaussians: coalesced loads of their parameters
-// and screen gradients into shared memory (the accumulators are zeroed for the
+// One CTA per 128 consecutive Gaussians: bulk copies of their parameters and
+// screen gradients into shared memory (the accumulators are zeroed for the
 // next step), the per-Gaussian adjoint of PreprocessorBackwardCPU::backward
-// (preprocessor_backward_cpu.cpp:205-645) from there, and coalesced stores of
-// the FP32 raw-parameter gradients.
+// (preprocessor_backward_cpu.cpp:205-645) from there into shared-memory
+// gradients, then Adam over the CTA's contiguous parameter slice with 16-byte
+// accesses and stochastic rounding (and, when asked, the FP32 gradients).
 template <typename S>
 __global__ void __launch_bounds__(kCB) k_chosen_backward(const StepParams* __restrict__ spp, int N, int mc3,
                                                          ChosenPtrs c, RGradPtrs rg, GradPtrs gout, Control* ctrl) {
@@ -236,6 +274,7 @@ __global__ void __launch_bounds__(kCB) k_chosen_backward(const StepParams* __res
     const StepParams& sp = *spp;
     if ((ctrl->status & (kStatusOverflow | kStatusTimeout)) || sp.persist->sticky_overflow) return;
     const int tid = threadIdx.x;
+    if (blockIdx.x == 0 && tid == 0 && sp.use_adam) atomicAdd(&sp.persist->applied_steps, 1ull);
     const long long g0 = (long long)blockIdx.x * kCB;
     const int ng = (int)min((long long)kCB, (long long)N - g0);
     // ---- phase 0: staging ----
@@ -335,94 +374,78 @@ __global__ void __launch_bounds__(kCB) k_chosen_backward(const StepParams* __res
         for (int k = 0; k < mc3; k++) sm.g_sh[kShPitch * tid + k] = o.basis[k / 3] * o.geff[k % 3];
     }
     __syncthreads();
-    // ---- phase 2: coalesced stores ----
-    for (int e = tid; e < 3 * ng; e += kCB) {
-        gout.g_pos[3 * g0 + e] = sm.g_pos[e];
-        gout.g_sc[3 * g0 + e] = sm.g_sc[e];
+    // ---- phase 2: optimiser over this CTA's slice (and the gradients, when kept) ----
+    if (gout.g_pos) {
+        for (int e = tid; e < 3 * ng; e += kCB) {
+            gout.g_pos[3 * g0 + e] = sm.g_pos[e];
+            gout.g_sc[3 * g0 + e] = sm.g_sc[e];
+        }
+        for (int e = tid; e < 4 * ng; e += kCB) gout.g_rot[4 * g0 + e] = sm.g_rot[e];
+        for (int e = tid; e < ng; e += kCB) gout.g_op[g0 + e] = sm.g_op[e];
+        for (int e = tid; e < mc3 * ng; e += kCB) {
+            const int t = e / mc3, k = e - t * mc3;
+            gout.g_sh[(size_t)mc3 * g0 + e] = sm.g_sh[kShPitch * t + k];
+        }
     }
-    for (int e = tid; e < 4 * ng; e += kCB) gout.g_rot[4 * g0 + e] = sm.g_rot[e];
-    for (int e = tid; e < ng; e += kCB) gout.g_op[g0 + e] = sm.g_op[e];
-    for (int e = tid; e < mc3 * ng; e += kCB) {
-        const int t = e / mc3, k = e - t * mc3;
-        gout.g_sh[(size_t)mc3 * g0 + e] = sm.g_sh[kShPitch * t + k];
-    }
-}
-
-// ---- optimiser (streaming) ----
-
-// Adam (optimizer.cpp:32-43 in FP32) or SGD on one element; the moments come
-// in and go out as floats.
-__device__ __forceinline__ float opt_elem(const StepParams& sp, float p, float& m, float& v, float g, float lr) {
-    if (sp.use_adam) return adam_elem(p, m, v, g, lr, sp.beta1, sp.beta2, sp.eps, sp.bc1, sp.bc2);
-    return p - lr * g;
-}
-
-// Eight consecutive 16-bit parameters with their BF16 moments and FP32
-// gradients: one 16-byte load / store per array, stochastic rounding.
-template <typename S>
-__device__ __forceinline__ void opt8(const StepParams& sp, uint4* p16, uint4* m16, uint4* v16, const float* g,
-                                     const float* lr, unsigned e0, unsigned salt) {
-    uint4 praw = *p16, mraw = *m16, vraw = *v16;
-    S* pb = reinterpret_cast<S*>(&praw);
-    __nv_bfloat16* mb = reinterpret_cast<__nv_bfloat16*>(&mraw);
-    __nv_bfloat16* vb = reinterpret_cast<__nv_bfloat16*>(&vraw);
-#pragma unroll
-    for (int k = 0; k < 8; k++) {
-        float m = __bfloat162float(mb[k]), v = __bfloat162float(vb[k]);
-        const float pn = opt_elem(sp, ldf(pb[k]), m, v, g[k], lr[k]);
-        const unsigned e = (e0 + (unsigned)k) ^ salt;
-        pb[k] = cvt_sr<S>(pn, mix32(e, sp.seed));
-        mb[k] = cvt_sr<__nv_bfloat16>(m, mix32(e, sp.seed ^ 0x68E31DA4u));
-        vb[k] = cvt_sr<__nv_bfloat16>(v, mix32(e, sp.seed ^ 0xB5297A4Du));
-    }
-    *p16 = praw;
-    *m16 = mraw;
-    *v16 = vraw;
-}
-
-template <typename S>
-__global__ void __launch_bounds__(256) k_chosen_adam(const StepParams* __restrict__ spp, int N, int mc3,
-                                                     ChosenPtrs c, GradPtrs g, const Control* ctrl) {
-    const StepParams& sp = *spp;
-    if ((ctrl->status & (kStatusOverflow | kStatusTimeout)) || sp.persist->sticky_overflow) return;
-    if (blockIdx.x == 0 && threadIdx.x == 0 && sp.use_adam) atomicAdd(&sp.persist->applied_steps, 1ull);
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    // SH: chunks of 8 consecutive coefficients
-    const long long n_sh = (long long)N * mc3;
+    const long long sh0 = (long long)mc3 * g0;
+    S* shw = static_cast<S*>(c.sh);
+    __nv_bfloat16* msh = static_cast<__nv_bfloat16*>(c.m_sh);
+    __nv_bfloat16* vsh = static_cast<__nv_bfloat16*>(c.v_sh);
     const float lr_sh[8] = {sp.lr_sh, sp.lr_sh, sp.lr_sh, sp.lr_sh, sp.lr_sh, sp.lr_sh, sp.lr_sh, sp.lr_sh};
-    for (long long q = t0; q < n_sh / 8; q += stride) {
-        const float4 ga = reinterpret_cast<const float4*>(g.g_sh)[2 * q];
-        const float4 gb = reinterpret_cast<const float4*>(g.g_sh)[2 * q + 1];
-        const float gg[8] = {ga.x, ga.y, ga.z, ga.w, gb.x, gb.y, gb.z, gb.w};
-        opt8<S>(sp, reinterpret_cast<uint4*>(c.sh) + q, reinterpret_cast<uint4*>(c.m_sh) + q,
-                reinterpret_cast<uint4*>(c.v_sh) + q, gg, lr_sh, (unsigned)(8 * q), 0x5bd1e995u);
+    if (ng == kCB) {
+        // SH: 16 * mc3 chunks of 8 coefficients (16-byte aligned: the slice starts at 256 * mc3 * blockIdx
+        // bytes); the parameters are already in shared memory
+        const int nq = (kCB * mc3) / 8;
+        uint4* m4 = reinterpret_cast<uint4*>(msh + sh0);
+        uint4* v4 = reinterpret_cast<uint4*>(vsh + sh0);
+        uint4* p4 = reinterpret_cast<uint4*>(shw + sh0);
+        for (int q = tid; q < nq; q += kCB) {
+            uint4 pp = sm.sh[q], mm = m4[q], vv = v4[q];
+            float gg[8];
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                const int e = 8 * q + k, t = e / mc3;
+                gg[k] = sm.g_sh[kShPitch * t + (e - t * mc3)];
+            }
+            opt8<S>(sp, pp, mm, vv, gg, lr_sh, (unsigned)(sh0 + 8 * q), 0x5bd1e995u);
+            p4[q] = pp;
+            m4[q] = mm;
+            v4[q] = vv;
+        }
+    } else {
+        const S* shs = reinterpret_cast<const S*>(sm.sh);
+        for (int e = tid; e < mc3 * ng; e += kCB) {
+            const int t = e / mc3;
+            float m = __bfloat162float(msh[sh0 + e]), v = __bfloat162float(vsh[sh0 + e]);
+            const float pn = opt_elem(sp, ldf(shs[e]), m, v, sm.g_sh[kShPitch * t + (e - t * mc3)], sp.lr_sh);
+            unsigned rp, rm, rv;
+            sr_words((unsigned)(sh0 + e) ^ 0x5bd1e995u, sp.seed, rp, rm, rv);
+            shw[sh0 + e] = cvt_sr<S>(pn, rp);
+            msh[sh0 + e] = cvt_sr<__nv_bfloat16>(m, rm);
+            vsh[sh0 + e] = cvt_sr<__nv_bfloat16>(v, rv);
+        }
     }
-    for (long long e = 8 * (n_sh / 8) + t0; e < n_sh; e += stride) {
-        S* p = static_cast<S*>(c.sh) + e;
-        __nv_bfloat16* mp = static_cast<__nv_bfloat16*>(c.m_sh) + e;
-        __nv_bfloat16* vp = static_cast<__nv_bfloat16*>(c.v_sh) + e;
-        float m = __bfloat162float(*mp), v = __bfloat162float(*vp);
-        const float pn = opt_elem(sp, ldf(*p), m, v, g.g_sh[e], sp.lr_sh);
-        const unsigned h = (unsigned)e ^ 0x5bd1e995u;
-        *p = cvt_sr<S>(pn, mix32(h, sp.seed));
-        *mp = cvt_sr<__nv_bfloat16>(m, mix32(h, sp.seed ^ 0x68E31DA4u));
-        *vp = cvt_sr<__nv_bfloat16>(v, mix32(h, sp.seed ^ 0xB5297A4Du));
-    }
-    // attributes: one 16-byte record per Gaussian; positions: FP32
+    // attributes: one 16-byte record per Gaussian
     const float lra[8] = {sp.lr_scale, sp.lr_scale, sp.lr_scale, sp.lr_opac, sp.lr_rot, sp.lr_rot, sp.lr_rot,
                           sp.lr_rot};
-    for (long long i = t0; i < N; i += stride) {
-        const float gg[8] = {g.g_sc[3 * i], g.g_sc[3 * i + 1], g.g_sc[3 * i + 2], g.g_op[i],
-                             g.g_rot[4 * i], g.g_rot[4 * i + 1], g.g_rot[4 * i + 2], g.g_rot[4 * i + 3]};
-        opt8<S>(sp, reinterpret_cast<uint4*>(c.attr) + i, reinterpret_cast<uint4*>(c.m_attr) + i,
-                reinterpret_cast<uint4*>(c.v_attr) + i, gg, lra, (unsigned)(8 * i), 0u);
+    for (int t = tid; t < ng; t += kCB) {
+        const float gg[8] = {sm.g_sc[3 * t], sm.g_sc[3 * t + 1], sm.g_sc[3 * t + 2], sm.g_op[t],
+                             sm.g_rot[4 * t], sm.g_rot[4 * t + 1], sm.g_rot[4 * t + 2], sm.g_rot[4 * t + 3]};
+        uint4 pp = sm.attr[t];
+        uint4 mm = reinterpret_cast<const uint4*>(c.m_attr)[g0 + t];
+        uint4 vv = reinterpret_cast<const uint4*>(c.v_attr)[g0 + t];
+        opt8<S>(sp, pp, mm, vv, gg, lra, (unsigned)(8 * (g0 + t)), 0u);
+        reinterpret_cast<uint4*>(c.attr)[g0 + t] = pp;
+        reinterpret_cast<uint4*>(c.m_attr)[g0 + t] = mm;
+        reinterpret_cast<uint4*>(c.v_attr)[g0 + t] = vv;
     }
-    for (long long e = t0; e < 3LL * N; e += stride) {
-        float m = c.m_pos[e], v = c.v_pos[e];
-        c.pos[e] = opt_elem(sp, c.pos[e], m, v, g.g_pos[e], sp.lr_pos);
-        c.m_pos[e] = m;
-        c.v_pos[e] = v;
+    // positions: FP32 parameters and moments
+    for (int e = tid; e < 3 * ng; e += kCB) {
+        const long long ge = 3 * g0 + e;
+        float m = c.m_pos[ge], v = c.v_pos[ge];
+        c.pos[ge] = opt_elem(sp, sm.pos[e], m, v, sm.g_pos[e], sp.lr_pos);
+        c.m_pos[ge] = m;
+        c.v_pos[ge] = v;
     }
 }
 
@@ -465,7 +488,7 @@ cudaError_t launch_raster_fwd_fast(cudaStream_t st, const StepParams* sp, int nu
 cudaError_t launch_chosen_backward_adam(cudaStream_t st, const StepParams* sp, int N, int mc3, bool fp16,
                                         ChosenPtrs c, RGradPtrs rg, GradPtrs g, Control* ctrl) {
     if (N <= 0) return cudaSuccess;
-    if (mc3 > 48 || !g.g_pos) return cudaErrorInvalidValue;
+    if (mc3 > 48) return cudaErrorInvalidValue;
     const int grid = grid_for(N, kCB);
     const int smem = (int)sizeof(ChosenBwdShared<__half>);   // same size for both 16-bit types
     static bool attr_set = false;
@@ -479,10 +502,6 @@ cudaError_t launch_chosen_backward_adam(cudaStream_t st, const StepParams* sp, i
     }
     if (fp16) k_chosen_backward<__half><<<grid, kCB, smem, st>>>(sp, N, mc3, c, rg, g, ctrl);
     else k_chosen_backward<__nv_bfloat16><<<grid, kCB, smem, st>>>(sp, N, mc3, c, rg, g, ctrl);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    if (fp16) k_chosen_adam<__half><<<8 * 148, 256, 0, st>>>(sp, N, mc3, c, g, ctrl);
-    else k_chosen_adam<__nv_bfloat16><<<8 * 148, 256, 0, st>>>(sp, N, mc3, c, g, ctrl);
     return cudaGetLastError();
 }
 

@@ -81,7 +81,7 @@ struct ScreenArrays {
 
 // Gaussian depth-sort input written by a preprocess that does not emit pairs.
 struct DepthKeys {
-    unsigned long long* keys;   // [N] depth bits, ~0u for Gaussians without pairs
+    unsigned* keys;             // [N] depth bits, ~0u for Gaussians without pairs
     unsigned* vals;             // [N] Gaussian index
 };
 
@@ -115,9 +115,9 @@ cudaError_t launch_raster_fwd_fast(cudaStream_t st, const StepParams* sp, int nu
 cudaError_t launch_raster_bwd_fast(cudaStream_t st, const StepParams* sp, int num_tiles, const unsigned* ranges,
                                    const unsigned* order, const unsigned* vals, ScreenPtrs s, PixelPtrs px,
                                    RGradPtrs g, Control* ctrl);
-// Per-Gaussian adjoint (FP32 raw-parameter gradients into g; zeroes the
-// screen-gradient accumulators) then the streaming optimiser (stochastic
-// rounding into the 16-bit parameters and BF16 moments).
+// Per-Gaussian adjoint fused with Adam (stochastic rounding into the 16-bit
+// parameters and BF16 moments); zeroes the screen-gradient accumulators.
+// With g.g_pos != NULL the FP32 raw-parameter gradients are stored too.
 cudaError_t launch_chosen_backward_adam(cudaStream_t st, const StepParams* sp, int N, int mc3, bool fp16,
                                         ChosenPtrs c, RGradPtrs rg, GradPtrs gout, Control* ctrl);
 
@@ -173,10 +173,12 @@ cudaError_t launch_tile_ranges(cudaStream_t st, unsigned long long capacity,
 // Stable LSD sort of 32-bit keys (tile ids) over digits [0, digits), control
 // slots slot_base..; hist_done: the digit histograms are already in those slots.
 // desc holds digits * desc_stride zeroed descriptors.
+// count (optional): device word with the number of keys (default: the pair count).
 cudaError_t launch_radix_sort32(cudaStream_t st, const StepParams* sp, int digits, int slot_base, bool hist_done,
                                 unsigned long long capacity, unsigned* keys0, unsigned* vals0, unsigned* keys1,
                                 unsigned* vals1, unsigned long long* desc, unsigned long long desc_stride,
-                                Control* ctrl, int* which, cudaEvent_t after_hist = nullptr);
+                                Control* ctrl, int* which, cudaEvent_t after_hist = nullptr,
+                                const unsigned long long* count = nullptr);
 cudaError_t launch_tile_ranges32(cudaStream_t st, unsigned long long capacity, const unsigned* tiles_sorted,
                                  unsigned* ranges, Control* ctrl);
 

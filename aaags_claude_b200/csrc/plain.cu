@@ -205,7 +205,7 @@ __global__ void __launch_bounds__(kBlock) k_preprocess(const StepParams* __restr
                       sp.persist);
     } else if (i < N) {
         // depth-sort input: Gaussians without pairs sort last (no finite depth has these bits)
-        dk.keys[i] = cnt > 0 ? (unsigned long long)dbits : 0xFFFFFFFFull;
+        dk.keys[i] = cnt > 0 ? dbits : 0xFFFFFFFFu;
         dk.vals[i] = (unsigned)i;
         if (i == 0) ctrl->gauss_keys = (unsigned long long)N;
     }

@@ -295,9 +295,9 @@ cudaError_t launch_radix_sort(cudaStream_t st, const StepParams* sp, int passes,
 cudaError_t launch_radix_sort32(cudaStream_t st, const StepParams* sp, int digits, int slot_base, bool hist_done,
                                 unsigned long long capacity, unsigned* keys0, unsigned* vals0, unsigned* keys1,
                                 unsigned* vals1, unsigned long long* desc, unsigned long long desc_stride,
-                                Control* ctrl, int* which, cudaEvent_t after_hist) {
+                                Control* ctrl, int* which, cudaEvent_t after_hist, const unsigned long long* count) {
     return radix_sort_impl<unsigned>(st, sp, 0, digits, slot_base, hist_done, capacity, keys0, vals0, keys1, vals1,
-                                     desc, desc_stride, ctrl, which, after_hist, nullptr);
+                                     desc, desc_stride, ctrl, which, after_hist, count);
 }
 
 cudaError_t launch_tile_ranges(cudaStream_t st, unsigned long long capacity, const unsigned long long* keys_sorted,
