@@ -3,7 +3,7 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Workload: the plain-FP32 training step on 1M Gaussians at 1920x1080 (seeded
+Workload: the training step on 1M Gaussians at 1920x1080 (seeded
 synthetic scene: means ~ N(0, 0.5^2 I3), log-scales ~ N(-4.5, 0.5^2), unit
 N(0, I4) quaternions, opacity logits ~ N(0, 1), SH degree 3; target = render of
 the perturbed scene; one camera on the radius-3 sphere; L1 loss; Adam with
@@ -11,10 +11,15 @@ lr 1.6e-4 for means and 1e-3 for the rest).  A step is preprocess -> binning ->
 radix sort -> tile ranges -> rasterise + L1 -> rasterise backward ->
 preprocess backward + Adam, replayed as one CUDA graph.
 
-Prints ONE JSON line (rank 0).  `value` is whole-job steps/s with inputs
-resident in HBM, timed with CUDA events on the library's stream and maxed over
-ranks; `e2e` is the same step through the public API with the target image
-copied from pinned host memory and the loss read back every step.
+Both forms are timed in the same run on the same GPU: the chosen form
+(--form, default BF16: positions FP32, other attributes and SH coefficients
+BF16, Adam moments BF16, FP32 blending and gradients) and the plain FP32 form
+(bit-exact with the reference).  Prints ONE JSON line (rank 0).  `value` is the
+chosen form's whole-job steps/s with inputs resident in HBM, timed with CUDA
+events on the library's stream and maxed over ranks; `e2e` is the same step
+through the public API with the target image copied from pinned host memory
+and the loss read back every step; `plain_fp32` holds the same numbers for the
+plain form and `chosen_vs_plain` their ratio.
 Multi-GPU runs are independent replicas (the path does not shard; no
 collective is on the data path), so scaling is weak.
 
@@ -48,7 +53,7 @@ STAGES = ["memsets", "preprocess", "sort_hist", "sort_passes", "ranges", "raster
 def _args(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the timed reference CPU step")
@@ -57,8 +62,10 @@ def _args(argv=None):
     ap.add_argument("--fused-adam", type=int, default=None, help="1: optimiser fused into the backward kernel")
     ap.add_argument("--sort", choices=("depth-first", "full-key"), default="depth-first",
                     help="pair ordering of the train step")
-    ap.add_argument("--form", choices=("plain", "bf16", "fp16"), default="plain",
-                    help="plain FP32 (parity) or the reduced-storage form of the train step")
+    ap.add_argument("--form", choices=("plain", "bf16", "fp16"), default="bf16",
+                    help="the chosen form timed against plain FP32 (plain: the plain form alone)")
+    ap.add_argument("--plain-only-line", dest="plain_only_line", action="store_true",
+                    help="time only --form (no plain comparison)")
     return ap.parse_args(argv)
 
 
@@ -153,7 +160,8 @@ def _bus_id(dev: int) -> str | None:
 
 
 # ---------------------------------------------------------------- roofline
-def stage_bytes(N: int, P: int, X: int, T: int, passes: int, mc3: int = 48, depth_first: bool = True) -> dict:
+def stage_bytes(N: int, P: int, X: int, T: int, passes: int, mc3: int = 48, depth_first: bool = True,
+                form: str = "plain") -> dict:
     """Algorithmic (compulsory) DRAM bytes of one launch of each stage (plain FP32).
 
     s_p = 4*(11 + mc3) bytes of parameters per Gaussian, s_m = 2*s_p of Adam
@@ -163,6 +171,19 @@ def stage_bytes(N: int, P: int, X: int, T: int, passes: int, mc3: int = 48, dept
     tile-digit histogram; "sort_passes" are the passes over the tile bits.
     """
     sp = 4 * (11 + mc3)
+    if form != "plain":
+        # reduced storage: 12 B positions + 16 B attributes + 2*mc3 B SH; BF16 moments (FP32 for positions)
+        s16 = 12 + 16 + 2 * mc3
+        m16 = 24 + 2 * (16 + 2 * mc3)
+        return {
+            "preprocess": N * (s16 + 48 + 8 + 8),        # params in; records, depth key + index, rect out
+            "sort_hist": N * 4 + 4 * N * 16 + N * 32 + P * 8 + P * 4,
+            "sort_passes": P * 16,
+            "ranges": P * 4 + T * 8,
+            "raster_fwd": P * 40 + X * 37,
+            "raster_bwd": P * 40 + X * 9 + N * 36,
+            "preprocess_bwd_adam": N * (2 * s16 + 2 * m16 + 2 * 36),   # params, moments in+out; screen grads in+zeroed
+        }
     if depth_first:
         pre = N * (sp + 48) + N * 12                     # params in; records out; depth key + index out
         hist = (N * 8 + 4 * N * 24                       # depth sort: histogram + 4 passes
@@ -218,6 +239,108 @@ def cpu_baseline_reference(w, cfg, tc, gt: np.ndarray) -> dict | None:
 
 
 # ---------------------------------------------------------------- our arm
+FORMS = {"plain": 0, "bf16": 1, "fp16": 2}
+
+
+def _measure_form(a, ctx, form, w, cam, cfg, tc, gt_dev, gt_pin, local, dist):
+    """Warm-up, graph-replayed timed steps, e2e steps and per-stage times of one form."""
+    import torch
+    from aaags_claude_b200 import gs3d
+    ctx.set_option(gs3d.OPT_FORM, FORMS[form])
+    ctx.set_raw_params(w.scene)
+    stream = torch.cuda.ExternalStream(ctx.stream_handle(), device=f"cuda:{local}")
+    it = 0
+    loss0 = ctx.train_step(cam, None, cfg, tc, it, gt_device_ptr=gt_dev.data_ptr())   # sizes the pair buffers
+    it += 1
+    for _ in range(max(a.warmup, 3)):
+        ctx.train_step(cam, None, cfg, tc, it, want_loss=False, gt_device_ptr=gt_dev.data_ptr())
+        it += 1
+    ctx.synchronize()
+    r = {"form": form, "loss_first": loss0, "tile_pairs": ctx.stat(gs3d.STAT_TOTAL_PAIRS),
+         "sort_passes": ctx.stat(gs3d.STAT_SORT_PASSES)}
+    # ---- value: inputs resident in HBM, graph replay, CUDA events on the library stream ----
+    clocks = ClockSampler(_bus_id(local))
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(a.steps):
+        ctx.train_step(cam, None, cfg, tc, it, want_loss=False, gt_device_ptr=gt_dev.data_ptr())
+        it += 1
+    e1.record(stream)
+    ctx.synchronize()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    r["clocks"] = clocks.stop()
+    r["ms_total"] = e0.elapsed_time(e1)
+    r["launches"] = ctx.stat(gs3d.STAT_KERNELS_LAST) * a.steps
+    r["graph"] = ctx.stat(gs3d.STAT_GRAPH_REPLAYS) > 0
+    # ---- e2e: pinned host target in, loss out, every step ----
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    loss = None
+    for _ in range(a.steps):
+        loss = ctx.train_step(cam, gt_pin.numpy(), cfg, tc, it)
+        it += 1
+    r["e2e_s"] = time.perf_counter() - t0
+    r["loss_last"] = loss
+    # ---- per-stage device times (un-captured steps, events between stages) ----
+    ctx.set_option(gs3d.OPT_STAGE_TIMING, 1)
+    acc = np.zeros(len(STAGES))
+    nt = max(3, min(a.steps, 10))
+    for _ in range(nt):
+        ctx.train_step(cam, None, cfg, tc, it, gt_device_ptr=gt_dev.data_ptr())
+        it += 1
+        acc += np.array(ctx.stage_times())
+    ctx.set_option(gs3d.OPT_STAGE_TIMING, 0)
+    r["stage_ms"] = acc / nt
+    if dist:
+        v = torch.tensor([r["ms_total"], r["e2e_s"]], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(v, op=dist.ReduceOp.MAX)
+        r["ms_total"], r["e2e_s"] = float(v[0]), float(v[1])
+    return r
+
+
+def _summary(a, r, world, X, N, T, depth_first, peak):
+    """Steps/s, e2e, stage times and the roofline of one measured form."""
+    P = r["tile_pairs"]
+    passes = r["sort_passes"]
+    pair_passes = passes - 4 if depth_first else passes
+    stage_ms = r["stage_ms"]
+    ms_step = r["ms_total"] / a.steps
+    value = world * a.steps / (r["ms_total"] / 1e3)
+    nbytes = stage_bytes(N, P, X, T, passes, depth_first=depth_first, form=r["form"])
+    per_launch_ms = {s: stage_ms[k] / (max(pair_passes, 1) if s == "sort_passes" else 1)
+                     for k, s in enumerate(STAGES)}
+    dom = max((s for s in STAGES if s != "memsets"), key=lambda s: stage_ms[STAGES.index(s)])
+    achieved = nbytes[dom] / (per_launch_ms[dom] * 1e-3) / 1e9
+    traffic = None
+    tt = _traffic_table()
+    if tt and dom in tt.get("kernels", {}):
+        k = tt["kernels"][dom]
+        traffic = k["bytes_per_launch"] * (P / k["pairs"] if k.get("scale") == "pairs" else 1.0)
+    step_bytes = sum(nbytes[s] * (pair_passes if s == "sort_passes" else 1) for s in nbytes)
+    sp_ms = stage_ms[STAGES.index("sort_passes")]
+    return {
+        "value": round(value, 3), "ms_per_step": round(ms_step, 4), "mpix_per_s": round(value * X / 1e6, 2),
+        "e2e": {"value": round(world * a.steps / r["e2e_s"], 3), "unit": "steps/s",
+                "h2d_bytes_per_step": int(X * 3 * 4 + 512), "d2h_bytes_per_step": 24,
+                "api": "gs3dc_train_step(gt host pinned, loss read back)"},
+        "gpu_launches": int(r["launches"]), "tile_pairs": P,
+        "stage_ms": {s: round(float(stage_ms[k]), 4) for k, s in enumerate(STAGES)},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak[0],
+                     "peak_kind": peak[1], "unit": "GB/s", "frac": round(achieved / peak[0], 4),
+                     "traffic": traffic, "algorithmic_bytes_per_launch": int(nbytes[dom])},
+        "step_roofline": {"algorithmic_bytes": int(step_bytes),
+                          "frac": round(step_bytes / (ms_step * 1e-3) / 1e9 / peak[0], 4)},
+        "sort_keys_per_s": round(P * pair_passes / (sp_ms * 1e-3), 1) if sp_ms > 0 else None,
+        "loss_first": r["loss_first"], "loss_last": r["loss_last"], "clocks": r["clocks"],
+        "cuda_graph": r["graph"], "sort_passes": passes,
+    }
+
+
 def run_ours(a) -> int:
     import torch
     rank, world, local = _dist_env()
@@ -241,113 +364,52 @@ def run_ours(a) -> int:
     # target image: the perturbed scene rendered by this library's plain form (setup, untimed)
     ctx.set_raw_params(w.target_scene)
     gt = ctx.render(cam, S.render_config(False))
-    ctx.set_option(gs3d.OPT_FORM, {"plain": gs3d.FORM_PLAIN_FP32, "bf16": gs3d.FORM_BF16,
-                                   "fp16": gs3d.FORM_FP16}[a.form])
-    ctx.set_raw_params(w.scene)
     gt_dev = torch.from_numpy(gt).to(f"cuda:{local}")
     gt_pin = torch.from_numpy(gt).pin_memory()
-    stream = torch.cuda.ExternalStream(ctx.stream_handle(), device=f"cuda:{local}")
 
-    it = 0
-    loss0 = ctx.train_step(cam, None, cfg, tc, it, gt_device_ptr=gt_dev.data_ptr())   # sizes the pair buffers
-    it += 1
-    for _ in range(max(a.warmup, 3)):
-        ctx.train_step(cam, None, cfg, tc, it, want_loss=False, gt_device_ptr=gt_dev.data_ptr())
-        it += 1
-    ctx.synchronize()
-    P = ctx.stat(gs3d.STAT_TOTAL_PAIRS)
-    passes = ctx.stat(gs3d.STAT_SORT_PASSES)
-    pair_passes = passes - 4 if depth_first else passes   # passes over the pairs
-
-    # ---- value: inputs resident in HBM, graph replay, CUDA events on the library stream ----
-    clocks = ClockSampler(_bus_id(local))
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(a.steps):
-        ctx.train_step(cam, None, cfg, tc, it, want_loss=False, gt_device_ptr=gt_dev.data_ptr())
-        it += 1
-    e1.record(stream)
-    ctx.synchronize()
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    clk = clocks.stop()
-    ms_total = e0.elapsed_time(e1)
-    launches = ctx.stat(gs3d.STAT_KERNELS_LAST) * a.steps
-    graph = ctx.stat(gs3d.STAT_GRAPH_REPLAYS) > 0
-
-    # ---- e2e: pinned host target in, loss out, every step ----
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(a.steps):
-        loss = ctx.train_step(cam, gt_pin.numpy(), cfg, tc, it)
-        it += 1
-    e2e_s = time.perf_counter() - t0
-
-    # ---- per-stage device times (un-captured steps, events between stages) ----
-    ctx.set_option(gs3d.OPT_STAGE_TIMING, 1)
-    acc = np.zeros(len(STAGES))
-    nt = max(3, min(a.steps, 10))
-    for _ in range(nt):
-        ctx.train_step(cam, None, cfg, tc, it, gt_device_ptr=gt_dev.data_ptr())
-        it += 1
-        acc += np.array(ctx.stage_times())
-    ctx.set_option(gs3d.OPT_STAGE_TIMING, 0)
-    stage_ms = acc / nt
-
-    vals = torch.tensor([ms_total, e2e_s], dtype=torch.float64, device=f"cuda:{local}")
-    if dist:
-        dist.all_reduce(vals, op=dist.ReduceOp.MAX)
-    ms_total, e2e_s = float(vals[0]), float(vals[1])
+    # the chosen form (--form, default BF16 storage) against the plain FP32 form, same GPU, same run
+    forms = ["plain"] if a.form == "plain" else ["plain", a.form]
+    if a.plain_only_line:
+        forms = [a.form] if a.form != "plain" else ["plain"]
+    res = {f: _measure_form(a, ctx, f, w, cam, cfg, tc, gt_dev, gt_pin, local, dist) for f in forms}
 
     if rank == 0:
         X = W * H
         T = ((W + 15) // 16) * ((H + 15) // 16)
-        ms_step = ms_total / a.steps
-        value = world * a.steps / (ms_total / 1e3)
-        peak, peak_kind = _peaks()
-        nbytes = stage_bytes(w.scene.count, P, X, T, passes, depth_first=depth_first)
-        per_launch_ms = {s: stage_ms[k] / (max(pair_passes, 1) if s == "sort_passes" else 1)
-                         for k, s in enumerate(STAGES)}
-        dom = max((s for s in STAGES if s != "memsets"), key=lambda s: stage_ms[STAGES.index(s)])
-        achieved = nbytes[dom] / (per_launch_ms[dom] * 1e-3) / 1e9
-        traffic = None
-        tt = _traffic_table()
-        if tt and dom in tt.get("kernels", {}):
-            k = tt["kernels"][dom]
-            traffic = k["bytes_per_launch"] * (P / k["pairs"] if k.get("scale") == "pairs" else 1.0)
-        step_bytes = sum(nbytes[s] * (pair_passes if s == "sort_passes" else 1) for s in nbytes)
+        peak = _peaks()
+        summ = {f: _summary(a, res[f], world, X, w.scene.count, T, depth_first, peak) for f in forms}
+        head = summ[forms[-1]]
+        chosen = forms[-1]
         line = {
-            "metric": METRIC, "value": round(value, 3), "unit": "steps/s", "n_gpus": world, "steps": a.steps,
-            "warmup": a.warmup, "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32" if a.form == "plain" else a.form + "-storage/f32",
+            "metric": METRIC, "value": head["value"], "unit": "steps/s", "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded; no dataset or checkpoint)",
-            "form": "plain_fp32" if a.form == "plain" else a.form,
+            "form": "plain_fp32" if chosen == "plain" else f"{chosen}_storage",
             "config": {"workload": _workload_name(a), "gaussians": w.scene.count, "sh_degree": 3, "width": W,
-                       "height": H,
-                       "tile": 16, "tile_pairs": P, "sort_passes": passes,
+                       "height": H, "tile": 16, "tile_pairs": head["tile_pairs"], "sort_passes": head["sort_passes"],
                        "pair_order": a.sort,
+                       "storage": ("FP32" if chosen == "plain" else
+                                   f"positions FP32, other attributes + SH {chosen.upper()}, Adam moments BF16"),
+                       "arithmetic": "FP32 blending, transmittance and gradients",
                        "l2": "working set ~1.6 GB per step > 126 MB L2 (no flush needed)",
-                       "parallelism": f"replicas x{world}", "cuda_graph": graph},
-            "mpix_per_s": round(value * X / 1e6, 2),
-            "e2e": {"value": round(world * a.steps / e2e_s, 3), "unit": "steps/s",
-                    "h2d_bytes_per_step": int(X * 3 * 4 + 512), "d2h_bytes_per_step": 24,
-                    "api": "gs3dc_train_step(gt host pinned, loss read back)"},
-            "gpu_launches": int(launches),
-            "stage_ms": {s: round(float(stage_ms[k]), 4) for k, s in enumerate(STAGES)},
-            "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
-                         "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                         "traffic": traffic, "algorithmic_bytes_per_launch": int(nbytes[dom])},
-            "step_roofline": {"algorithmic_bytes": int(step_bytes),
-                              "frac": round(step_bytes / (ms_step * 1e-3) / 1e9 / peak, 4)},
-            "sort_keys_per_s": (round(P * pair_passes / (stage_ms[STAGES.index('sort_passes')] * 1e-3), 1)
-                                if stage_ms[STAGES.index('sort_passes')] > 0 else None),
-            "loss_first": loss0, "loss_last": loss,
-            "clocks": clk,
+                       "parallelism": f"replicas x{world}", "cuda_graph": head["cuda_graph"]},
+            "mpix_per_s": head["mpix_per_s"],
+            "e2e": head["e2e"],
+            "gpu_launches": head["gpu_launches"],
+            "stage_ms": head["stage_ms"],
+            "roofline": head["roofline"],
+            "step_roofline": head["step_roofline"],
+            "sort_keys_per_s": head["sort_keys_per_s"],
+            "loss_first": head["loss_first"], "loss_last": head["loss_last"],
+            "clocks": head["clocks"],
         }
+        if chosen != "plain":
+            p = summ["plain"]
+            line["plain_fp32"] = {k: p[k] for k in ("value", "ms_per_step", "mpix_per_s", "e2e", "gpu_launches",
+                                                    "tile_pairs", "stage_ms", "roofline", "clocks")}
+            line["chosen_vs_plain"] = round(head["value"] / p["value"], 3)
+            line["gpu_launches"] = head["gpu_launches"] + p["gpu_launches"]
         if world == 1 and not a.no_cpu_baseline and _workload_name(a) == WORKLOAD:
             line["cpu_baseline"] = cpu_baseline_reference(w, cfg, tc, gt)
         print(json.dumps(line), flush=True)
