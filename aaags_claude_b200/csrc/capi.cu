@@ -117,7 +117,15 @@ struct gs3dc_ctx {
     bool fused_adam = false;   // split backward + optimiser by default (faster at this occupancy)
     bool keep_grads = false;   // GS3DC_OPT_KEEP_GRADIENTS
     bool have_step_grads = false;
-    cudaGraphExec_t graph = nullptr;
+    cudaGraphExec_t graph = nullptr;        // front half: preprocess .. tile ranges
+    cudaGraphExec_t graph_back = nullptr;   // back half: rasterisers, backward, optimiser
+    // host targets: copied on their own stream into alternating buffers while the front half runs
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ev_gt_ready = nullptr;
+    cudaEvent_t ev_gt_free[2] = {};
+    bool gt_free_recorded[2] = {false, false};
+    int gt_slot = 0;
+    DevBuf<float> gtb[2];
     long long graph_key[8] = {};
     long long graph_replays = 0;
     long long graph_kernels = 0;
@@ -142,6 +150,12 @@ int fail(gs3dc_ctx* c, int code, const char* fmt, ...) {
     va_end(ap);
     if (c) c->err = buf;
     return code;
+}
+
+void drop_graphs(gs3dc_ctx* c) {
+    if (c->graph) cudaGraphExecDestroy(c->graph);
+    if (c->graph_back) cudaGraphExecDestroy(c->graph_back);
+    c->graph = c->graph_back = nullptr;
 }
 
 #define CK(call)                                                                                  \
@@ -532,11 +546,10 @@ int seq_front_depth_first(gs3dc_ctx* c) {
     return GS3DC_OK;
 }
 
-// Train step of the reduced-storage form: depth-first front half with the
-// chosen preprocess, fast-exp rasterisers, fused adjoint + Adam.
-int seq_train_chosen(gs3dc_ctx* c) {
-    int rc = seq_front_depth_first(c);
-    if (rc) return rc;
+// Back half of a train step of the reduced-storage form: fast-exp
+// rasterisers, fused adjoint + Adam.
+int seq_back_chosen(gs3dc_ctx* c) {
+    int rc;
     const int w = c->sorted_which;
     if ((rc = mark(c, GS3DC_STAGE_RASTER_FWD))) return rc;
     CK(launch_raster_fwd_fast(c->stream, c->sp_dev, c->num_tiles, c->ranges.p, c->tile_order.p, c->vals[w].p,
@@ -554,15 +567,23 @@ int seq_train_chosen(gs3dc_ctx* c) {
     return GS3DC_OK;
 }
 
-int seq_train(gs3dc_ctx* c) {
+// Front half of a train step: preprocess, pair emission, sort, tile ranges.
+int seq_train_front(gs3dc_ctx* c) {
     int rc;
-    if (chosen_form(c)) return seq_train_chosen(c);
-    if (c->sort_mode == GS3DC_SORT_DEPTH_FIRST) {
+    if (chosen_form(c) || c->sort_mode == GS3DC_SORT_DEPTH_FIRST) {
         if ((rc = seq_front_depth_first(c))) return rc;
     } else {
         if ((rc = seq_preprocess(c, false))) return rc;
         if ((rc = seq_sort(c))) return rc;
     }
+    return GS3DC_OK;
+}
+
+// Back half: forward rasteriser with the fused L1 (the only reader of the
+// target), backward rasteriser, preprocess backward, optimiser.
+int seq_train_back(gs3dc_ctx* c) {
+    int rc;
+    if (chosen_form(c)) return seq_back_chosen(c);
     const int w = c->sorted_which;
     if ((rc = mark(c, GS3DC_STAGE_RASTER_FWD))) return rc;
     CK(launch_raster_fwd_plain(c->stream, c->sp_dev, c->num_tiles, true, c->ranges.p, c->tile_order.p, c->vals[w].p,
@@ -630,10 +651,7 @@ int upload_model_arrays(gs3dc_ctx* c, int N, int sh_degree, int mc, const float*
     if (N < 0 || mc <= 0 || mc > 16 || sh_degree < 0 || sh_degree > 3 || (sh_degree + 1) * (sh_degree + 1) > mc)
         return fail(c, GS3DC_ERR_INVALID_ARG, "bad model shape N=%d sh_degree=%d max_coeffs=%d", N, sh_degree, mc);
     if (N > 0 && (!p || !s || !r || !sh || !o)) return fail(c, GS3DC_ERR_INVALID_ARG, "model arrays must be non-NULL");
-    if (c->graph && (c->N != N || c->max_coeffs != mc)) {
-        cudaGraphExecDestroy(c->graph);
-        c->graph = nullptr;
-    }
+    if (c->N != N || c->max_coeffs != mc) drop_graphs(c);
     int rc = ensure_model(c, N, mc);
     if (rc) return rc;
     c->N = N;
@@ -694,6 +712,11 @@ int gs3dc_create(int device, gs3dc_ctx** out) {
     };
     if (cudaSetDevice(device) != cudaSuccess) return bail(GS3DC_ERR_CUDA);
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(GS3DC_ERR_CUDA);
+    if (cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking) != cudaSuccess) return bail(GS3DC_ERR_CUDA);
+    if (cudaEventCreateWithFlags(&c->ev_gt_ready, cudaEventDisableTiming) != cudaSuccess) return bail(GS3DC_ERR_CUDA);
+    for (int b = 0; b < 2; b++)
+        if (cudaEventCreateWithFlags(&c->ev_gt_free[b], cudaEventDisableTiming) != cudaSuccess)
+            return bail(GS3DC_ERR_CUDA);
     if (cudaMalloc(&c->sp_dev, sizeof(StepParams)) != cudaSuccess) return bail(GS3DC_ERR_OUT_OF_MEMORY);
     if (cudaMalloc(&c->persist, sizeof(Persist)) != cudaSuccess) return bail(GS3DC_ERR_OUT_OF_MEMORY);
     if (cudaMemset(c->persist, 0, sizeof(Persist)) != cudaSuccess) return bail(GS3DC_ERR_CUDA);
@@ -714,7 +737,8 @@ void gs3dc_destroy(gs3dc_ctx* c) {
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    if (c->graph) cudaGraphExecDestroy(c->graph);
+    if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
+    drop_graphs(c);
     DevBuf<float>* fb[] = {&c->pos,    &c->sc,      &c->rot,     &c->sh,     &c->op,      &c->m_pos,  &c->v_pos,
                            &c->m_sc,   &c->v_sc,    &c->m_rot,   &c->v_rot,  &c->m_sh,    &c->v_sh,   &c->m_op,
                            &c->v_op,   &c->g_pos,   &c->g_sc,    &c->g_rot,  &c->g_sh,    &c->g_op,   &c->col_b,
@@ -749,6 +773,10 @@ void gs3dc_destroy(gs3dc_ctx* c) {
         if (c->sp_event[k]) cudaEventDestroy(c->sp_event[k]);
     for (int k = 0; k <= GS3DC_NUM_STAGES; k++)
         if (c->stage_ev[k]) cudaEventDestroy(c->stage_ev[k]);
+    if (c->ev_gt_ready) cudaEventDestroy(c->ev_gt_ready);
+    for (int b = 0; b < 2; b++)
+        if (c->ev_gt_free[b]) cudaEventDestroy(c->ev_gt_free[b]);
+    if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -775,10 +803,7 @@ int gs3dc_set_option(gs3dc_ctx* c, int option, int64_t value) {
             if (value == c->form) return GS3DC_OK;
             CK(cudaSetDevice(c->device));
             int rc;
-            if (c->graph) {
-                cudaGraphExecDestroy(c->graph);
-                c->graph = nullptr;
-            }
+            drop_graphs(c);
             if (c->have_model && !c->model_raw && value != GS3DC_FORM_PLAIN_FP32)
                 return fail(c, GS3DC_ERR_STATE, "the device model is an activated render model");
             // the model moves to the new form; the optimiser restarts
@@ -794,10 +819,7 @@ int gs3dc_set_option(gs3dc_ctx* c, int option, int64_t value) {
         case GS3DC_OPT_SPIN_LIMIT:
             if (value <= 0) return fail(c, GS3DC_ERR_INVALID_ARG, "spin limit must be positive");
             c->spin_limit = (unsigned)value;
-            if (c->graph) {
-                cudaGraphExecDestroy(c->graph);
-                c->graph = nullptr;
-            }
+            drop_graphs(c);
             return GS3DC_OK;
         case GS3DC_OPT_FUSED_ADAM:
             c->fused_adam = value != 0;
@@ -807,10 +829,7 @@ int gs3dc_set_option(gs3dc_ctx* c, int option, int64_t value) {
             return GS3DC_OK;
         case GS3DC_OPT_KEEP_GRADIENTS:
             c->keep_grads = value != 0;
-            if (c->graph) {
-                cudaGraphExecDestroy(c->graph);
-                c->graph = nullptr;
-            }
+            drop_graphs(c);
             return GS3DC_OK;
         case GS3DC_OPT_SORT:
             if (value != GS3DC_SORT_DEPTH_FIRST && value != GS3DC_SORT_FULL_KEY)
@@ -1263,10 +1282,18 @@ int gs3dc_train_step(gs3dc_ctx* c, const gs3d_camera* cam, const float* gt, int 
     if ((rc = ensure_pixels(c, cam->width, cam->height))) return rc;
     const size_t np = (size_t)cam->width * cam->height;
     const float* gt_dev = gt;
-    if (!gt_on_device) {
-        CK(c->gt.ensure(3 * np));
-        CK(cudaMemcpyAsync(c->gt.p, gt, 3 * np * 4, cudaMemcpyHostToDevice, c->stream));
-        gt_dev = c->gt.p;
+    const bool host_gt = !gt_on_device;
+    int gslot = 0;
+    if (host_gt) {
+        // the copy runs on its own stream, overlapping the front half of the step; buffer gslot
+        // is reused only after the step that last read it has passed its back half
+        gslot = c->gt_slot;
+        c->gt_slot ^= 1;
+        CK(c->gtb[gslot].ensure(3 * np));
+        if (c->gt_free_recorded[gslot]) CK(cudaStreamWaitEvent(c->copy_stream, c->ev_gt_free[gslot], 0));
+        CK(cudaMemcpyAsync(c->gtb[gslot].p, gt, 3 * np * 4, cudaMemcpyHostToDevice, c->copy_stream));
+        CK(cudaEventRecord(c->ev_gt_ready, c->copy_stream));
+        gt_dev = c->gtb[gslot].p;
     }
     bool first = c->cap == 0 || c->sort_num_tiles != c->num_tiles;
     if (first) {
@@ -1284,26 +1311,40 @@ int gs3dc_train_step(gs3dc_ctx* c, const gs3d_camera* cam, const float* gt, int 
         c->kernels_last = 0;
         if (c->use_graph && !c->stage_timing && !first && attempt == 0) {
             if (!key_ok) {
-                if (c->graph) {
-                    cudaGraphExecDestroy(c->graph);
-                    c->graph = nullptr;
-                }
+                drop_graphs(c);
                 cudaGraph_t g;
                 CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-                rc = seq_train(c);
+                rc = seq_train_front(c);
                 cudaError_t ec = cudaStreamEndCapture(c->stream, &g);
                 if (rc) return rc;
                 CK(ec);
                 CK(cudaGraphInstantiate(&c->graph, g, 0));
                 cudaGraphDestroy(g);
+                const long long k_front = c->kernels_last;
+                CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+                rc = seq_train_back(c);
+                ec = cudaStreamEndCapture(c->stream, &g);
+                if (rc) return rc;
+                CK(ec);
+                CK(cudaGraphInstantiate(&c->graph_back, g, 0));
+                cudaGraphDestroy(g);
                 std::memcpy(c->graph_key, key, sizeof(key));
                 c->graph_kernels = c->kernels_last;
+                (void)k_front;
             }
             c->kernels_last = c->graph_kernels;
             CK(cudaGraphLaunch(c->graph, c->stream));
+            if (host_gt) CK(cudaStreamWaitEvent(c->stream, c->ev_gt_ready, 0));
+            CK(cudaGraphLaunch(c->graph_back, c->stream));
             c->graph_replays++;
         } else {
-            if ((rc = seq_train(c))) return rc;
+            if ((rc = seq_train_front(c))) return rc;
+            if (host_gt) CK(cudaStreamWaitEvent(c->stream, c->ev_gt_ready, 0));
+            if ((rc = seq_train_back(c))) return rc;
+        }
+        if (host_gt) {
+            CK(cudaEventRecord(c->ev_gt_free[gslot], c->stream));
+            c->gt_free_recorded[gslot] = true;
         }
         c->have_step_grads = c->keep_grads;
         if (!loss && !first && !c->stage_timing) {
