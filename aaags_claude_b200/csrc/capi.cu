@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "../../include/gs3d_cuda.h"
 #include "common.cuh"
@@ -42,6 +43,7 @@ struct DevBuf {
 };
 
 constexpr int kParamSlots = 4;  // pinned ring of per-step parameter blocks
+constexpr int kMaxBatchViews = 255;   // views per multi-view step (one 8-bit radix digit)
 
 }  // namespace
 
@@ -134,6 +136,28 @@ struct gs3dc_ctx {
     bool stage_timing = false;
     cudaEvent_t stage_ev[GS3DC_NUM_STAGES + 1] = {};
     float stage_ms[GS3DC_NUM_STAGES] = {};
+    // multi-view train step (gs3dc_train_step_batch): (view, Gaussian) entries view * N + i
+    struct Batch {
+        DevBuf<StepParams> views;                  // per-view parameters (device)
+        StepParams* views_host = nullptr;          // pinned staging, kMaxBatchViews entries
+        cudaEvent_t views_event = nullptr;         // the staging's last copy has been consumed
+        DevBuf<float4> rec0, rec1;
+        DevBuf<float> col_b, depth, dm2, dcon, drgb, dop;
+        DevBuf<int> radius, tiles;
+        DevBuf<uint2> rects;
+        DevBuf<unsigned long long> dkeys[2];
+        DevBuf<unsigned> dvals[2];
+        DevBuf<unsigned long long> ddesc, sort_desc;
+        DevBuf<unsigned> keys[2], vals[2];
+        unsigned long long cap = 0;
+        DevBuf<float> image, T, gt;
+        DevBuf<unsigned> last;
+        DevBuf<unsigned char> dsign;
+        DevBuf<unsigned> ranges, order;
+        size_t grads_zeroed = 0;                   // entries of the screen-gradient accumulators known zero
+        cudaGraphExec_t graph = nullptr;
+        long long key[8] = {};
+    } batch;
     // options / stats
     unsigned spin_limit = 1u << 22;
     long long kernels_last = 0;
@@ -155,7 +179,8 @@ int fail(gs3dc_ctx* c, int code, const char* fmt, ...) {
 void drop_graphs(gs3dc_ctx* c) {
     if (c->graph) cudaGraphExecDestroy(c->graph);
     if (c->graph_back) cudaGraphExecDestroy(c->graph_back);
-    c->graph = c->graph_back = nullptr;
+    if (c->batch.graph) cudaGraphExecDestroy(c->batch.graph);
+    c->graph = c->graph_back = c->batch.graph = nullptr;
 }
 
 #define CK(call)                                                                                  \
@@ -377,13 +402,9 @@ int ensure_pairs(gs3dc_ctx* c, unsigned long long cap, int num_tiles) {
     return GS3DC_OK;
 }
 
-// Fills the next pinned parameter slot and queues its copy to the device.
-int push_params(gs3dc_ctx* c, const gs3d_camera* cam, const gs3d_render_config* cfg, const gs3d_train_config* tc,
-                int iteration, const float* gt_dev, const float* raw_rot_dev = nullptr) {
-    const int slot = c->sp_slot;
-    c->sp_slot = (c->sp_slot + 1) % kParamSlots;
-    CK(cudaEventSynchronize(c->sp_event[slot]));  // the slot's previous copy has been consumed
-    StepParams& p = c->sp_ring[slot];
+// The per-step parameters of one camera.
+void fill_params(gs3dc_ctx* c, StepParams& p, const gs3d_camera* cam, const gs3d_render_config* cfg,
+                 const gs3d_train_config* tc, int iteration, const float* gt_dev, const float* raw_rot_dev) {
     std::memset(&p, 0, sizeof(p));
     p.cam = *cam;
     p.cfg = *cfg;
@@ -423,6 +444,16 @@ int push_params(gs3dc_ctx* c, const gs3d_camera* cam, const gs3d_render_config* 
         p.bc1 = 1.0f / (1.0f - std::pow(tc->adam_beta1, (float)c->adam_step));
         p.bc2 = 1.0f / (1.0f - std::pow(tc->adam_beta2, (float)c->adam_step));
     }
+}
+
+// Fills the next pinned parameter slot and queues its copy to the device.
+int push_params(gs3dc_ctx* c, const gs3d_camera* cam, const gs3d_render_config* cfg, const gs3d_train_config* tc,
+                int iteration, const float* gt_dev, const float* raw_rot_dev = nullptr) {
+    const int slot = c->sp_slot;
+    c->sp_slot = (c->sp_slot + 1) % kParamSlots;
+    CK(cudaEventSynchronize(c->sp_event[slot]));  // the slot's previous copy has been consumed
+    StepParams& p = c->sp_ring[slot];
+    fill_params(c, p, cam, cfg, tc, iteration, gt_dev, raw_rot_dev);
     CK(cudaMemcpyAsync(c->sp_dev, &p, sizeof(StepParams), cudaMemcpyHostToDevice, c->stream));
     CK(cudaEventRecord(c->sp_event[slot], c->stream));
     return GS3DC_OK;
@@ -675,6 +706,133 @@ int upload_model_arrays(gs3dc_ctx* c, int N, int sh_degree, int mc, const float*
     return GS3DC_OK;
 }
 
+// ---- multi-view train step ----
+
+struct BatchShape {
+    int V = 0;
+    long long VN = 0;
+    unsigned tiles = 0;        // all views' tiles
+    unsigned long long pix = 0;  // all views' pixels
+    int tile_digits = 0;
+};
+
+ScreenPtrs batch_screen(gs3dc_ctx* c) {
+    auto& b = c->batch;
+    return {b.rec0.p, b.rec1.p, b.col_b.p, b.depth.p, b.radius.p, b.tiles.p, nullptr, nullptr, nullptr, nullptr, nullptr};
+}
+PixelPtrs batch_pixels(gs3dc_ctx* c) {
+    auto& b = c->batch;
+    return {b.image.p, b.T.p, nullptr, b.last.p, b.dsign.p, nullptr};
+}
+RGradPtrs batch_rgrads(gs3dc_ctx* c) {
+    auto& b = c->batch;
+    return {b.dm2.p, b.dcon.p, b.drgb.p, b.dop.p};
+}
+
+// Pair buffers and tile-sort descriptors of the multi-view step.
+int batch_pairs(gs3dc_ctx* c, unsigned long long cap, int digits) {
+    auto& b = c->batch;
+    if (cap > 0xFFFFFFFFull)
+        return fail(c, GS3DC_ERR_PAIR_OVERFLOW, "%llu tile pairs exceed the 32-bit tile-range format", cap);
+    if (cap > b.cap) {
+        for (int k = 0; k < 2; k++) {
+            CK(b.keys[k].ensure(cap));
+            CK(b.vals[k].ensure(cap));
+        }
+        b.cap = cap;
+    }
+    const unsigned long long stride = ((b.cap + kSortTile - 1) / kSortTile) * 256ull;
+    CK(b.sort_desc.ensure((size_t)(digits > 1 ? digits : 1) * stride));
+    return GS3DC_OK;
+}
+
+// Buffers of a multi-view step with the given shape.
+int batch_buffers(gs3dc_ctx* c, const BatchShape& sh) {
+    auto& b = c->batch;
+    const size_t vn = (size_t)sh.VN;
+    CK(b.views.ensure((size_t)sh.V));
+    CK(b.rec0.ensure(vn));
+    CK(b.rec1.ensure(vn));
+    CK(b.col_b.ensure(vn));
+    CK(b.depth.ensure(vn));
+    CK(b.radius.ensure(vn));
+    CK(b.tiles.ensure(vn));
+    CK(b.rects.ensure(vn));
+    if (b.dm2.n < 2 * vn) b.grads_zeroed = 0;
+    CK(b.dm2.ensure(2 * vn));
+    CK(b.dcon.ensure(3 * vn));
+    CK(b.drgb.ensure(3 * vn));
+    CK(b.dop.ensure(vn));
+    if (b.grads_zeroed < vn) {
+        // the accumulators start at zero; the backward re-zeroes what it reads
+        CK(cudaMemsetAsync(b.dm2.p, 0, b.dm2.n * 4, c->stream));
+        CK(cudaMemsetAsync(b.dcon.p, 0, b.dcon.n * 4, c->stream));
+        CK(cudaMemsetAsync(b.drgb.p, 0, b.drgb.n * 4, c->stream));
+        CK(cudaMemsetAsync(b.dop.p, 0, b.dop.n * 4, c->stream));
+        b.grads_zeroed = b.dop.n;
+    }
+    for (int k = 0; k < 2; k++) {
+        CK(b.dkeys[k].ensure(vn));
+        CK(b.dvals[k].ensure(vn));
+    }
+    CK(b.ddesc.ensure(5 * ((vn + kSortTile - 1) / kSortTile) * 256));
+    CK(b.image.ensure(3 * sh.pix));
+    CK(b.T.ensure(sh.pix));
+    CK(b.last.ensure(sh.pix));
+    CK(b.dsign.ensure(sh.pix));
+    CK(b.ranges.ensure(2 * (size_t)sh.tiles));
+    CK(b.order.ensure(sh.tiles));
+    Control* before = c->ctrl;
+    int rc = ensure_ctrl(c, (int)std::min<long long>(sh.VN, 0x7fffffffLL));
+    if (rc) return rc;
+    if (c->ctrl != before) drop_graphs(c);   // captured launches hold the control block's address
+    return GS3DC_OK;
+}
+
+// One multi-view step: preprocess of every (view, Gaussian), stable sort by
+// (view, depth) in 5 passes, emission in that order with global tile ids,
+// stable sort of the pairs on the tile bits, ranges and a heavy-first order of
+// all views' tiles, persistent forward and backward rasterisers over that
+// order, then the adjoint summed over the views and one Adam step.
+int seq_batch(gs3dc_ctx* c, const BatchShape& sh) {
+    auto& b = c->batch;
+    const StepParams* views = b.views.p;
+    const unsigned long long vn = (unsigned long long)sh.VN;
+    const unsigned long long dstride = ((vn + kSortTile - 1) / kSortTile) * 256ull;
+    const unsigned long long pstride = ((b.cap + kSortTile - 1) / kSortTile) * 256ull;
+    CK(cudaMemsetAsync(c->ctrl_region.p, 0, ctrl_bytes_for((int)std::min<long long>(sh.VN, 0x7fffffffLL)),
+                       c->stream));
+    CK(cudaMemsetAsync(b.ranges.p, 0, 2 * (size_t)sh.tiles * sizeof(unsigned), c->stream));
+    CK(cudaMemsetAsync(b.ddesc.p, 0, 5 * dstride * sizeof(unsigned long long), c->stream));
+    if (sh.tile_digits > 0)
+        CK(cudaMemsetAsync(b.sort_desc.p, 0, (size_t)sh.tile_digits * pstride * sizeof(unsigned long long),
+                           c->stream));
+    CK(launch_chosen_preprocess(c->stream, views, c->N, c->form == GS3DC_FORM_FP16, chosen_ptrs(c), batch_screen(c),
+                                DepthKeys{nullptr, b.dvals[0].p, b.dkeys[0].p}, b.rects.p, c->ctrl, sh.V));
+    // digits 0..3: depth bits, digit 4: the view
+    int dw = 0;
+    CK(launch_radix_sort(c->stream, views, 5, vn, b.dkeys[0].p, b.dvals[0].p, b.dkeys[1].p, b.dvals[1].p, b.ddesc.p,
+                         dstride, c->ctrl, &dw, nullptr, 0, &c->ctrl->gauss_keys));
+    PairPtrs pr{nullptr, b.vals[0].p, b.cap, c->scan_desc, b.keys[0].p};
+    CK(launch_emit_ranked(c->stream, views, (int)vn, b.dvals[dw].p, batch_screen(c), pr, c->ctrl, b.rects.p, c->N,
+                          5));
+    int which = 0;
+    CK(launch_radix_sort32(c->stream, views, sh.tile_digits, 5, true, b.cap, b.keys[0].p, b.vals[0].p, b.keys[1].p,
+                           b.vals[1].p, b.sort_desc.p, pstride, c->ctrl, &which));
+    CK(launch_tile_ranges32(c->stream, b.cap, b.keys[which].p, b.ranges.p, c->ctrl));
+    CK(launch_tile_order(c->stream, b.ranges.p, (int)sh.tiles, b.order.p));
+    CK(launch_raster_fwd_fast_multi(c->stream, views, sh.V, sh.tiles, b.ranges.p, b.order.p, b.vals[which].p,
+                                    batch_screen(c), batch_pixels(c), c->ctrl));
+    CK(launch_raster_bwd_fast_multi(c->stream, views, sh.V, sh.tiles, b.ranges.p, b.order.p, b.vals[which].p,
+                                    batch_screen(c), batch_pixels(c), batch_rgrads(c), c->ctrl));
+    CK(launch_chosen_backward_adam(c->stream, views, c->N, c->max_coeffs * 3, c->form == GS3DC_FORM_FP16,
+                                   chosen_ptrs(c), batch_rgrads(c),
+                                   c->keep_grads ? grad_ptrs(c) : GradPtrs{nullptr, nullptr, nullptr, nullptr, nullptr},
+                                   c->ctrl, sh.V));
+    c->kernels_last = 1 + 1 + 5 + 1 + (sh.tile_digits > 0 ? sh.tile_digits : 0) + 2 + 3;
+    return GS3DC_OK;
+}
+
 }  // namespace
 
 // ======================================================================
@@ -773,6 +931,8 @@ void gs3dc_destroy(gs3dc_ctx* c) {
         if (c->sp_event[k]) cudaEventDestroy(c->sp_event[k]);
     for (int k = 0; k <= GS3DC_NUM_STAGES; k++)
         if (c->stage_ev[k]) cudaEventDestroy(c->stage_ev[k]);
+    if (c->batch.views_event) cudaEventDestroy(c->batch.views_event);
+    if (c->batch.views_host) cudaFreeHost(c->batch.views_host);
     if (c->ev_gt_ready) cudaEventDestroy(c->ev_gt_ready);
     for (int b = 0; b < 2; b++)
         if (c->ev_gt_free[b]) cudaEventDestroy(c->ev_gt_free[b]);
@@ -1372,6 +1532,116 @@ int gs3dc_train_step(gs3dc_ctx* c, const gs3d_camera* cam, const float* gt, int 
             for (int k = 0; k < GS3DC_NUM_STAGES; k++)
                 CK(cudaEventElapsedTime(&c->stage_ms[k], c->stage_ev[k], c->stage_ev[k + 1]));
         }
+        return GS3DC_OK;
+    }
+    c->adam_step = step_before;
+    return fail(c, GS3DC_ERR_PAIR_OVERFLOW, "tile-pair capacity kept overflowing");
+}
+
+int gs3dc_train_step_batch(gs3dc_ctx* c, int n_views, const gs3d_camera* cams, const float* gt, int gt_on_device,
+                           const gs3d_render_config* cfg, const gs3d_train_config* tc, int iteration, float* loss) {
+    if (!c || !cams || !gt || !cfg || !tc) return GS3DC_ERR_INVALID_ARG;
+    if (n_views < 1 || n_views > kMaxBatchViews)
+        return fail(c, GS3DC_ERR_INVALID_ARG, "n_views %d outside 1..%d", n_views, kMaxBatchViews);
+    int rc;
+    if ((rc = require_model(c))) return rc;
+    if (!chosen_form(c) || !c->chosen_ready)
+        return fail(c, GS3DC_ERR_STATE, "multi-view steps run in the reduced-storage form (GS3DC_FORM_BF16 / _FP16)");
+    for (int v = 0; v < n_views; v++)
+        if ((rc = check_config(c, &cams[v], cfg))) return rc;
+    CK(cudaSetDevice(c->device));
+    auto& b = c->batch;
+    BatchShape sh;
+    sh.V = n_views;
+    sh.VN = (long long)c->N * n_views;
+    if (sh.VN >= (1LL << 31)) return fail(c, GS3DC_ERR_INVALID_ARG, "%lld (view, Gaussian) entries exceed 2^31", sh.VN);
+    std::vector<unsigned> tile_base(n_views), pix_base(n_views);
+    unsigned long long tiles = 0, pix = 0;
+    for (int v = 0; v < n_views; v++) {
+        const int gx = (cams[v].width + cfg->tile_w - 1) / cfg->tile_w, gy = (cams[v].height + cfg->tile_h - 1) / cfg->tile_h;
+        tile_base[v] = (unsigned)tiles;
+        pix_base[v] = (unsigned)pix;
+        tiles += (unsigned long long)gx * gy;
+        pix += (unsigned long long)cams[v].width * cams[v].height;
+    }
+    if (tiles >= (1ull << 24) || pix >= (1ull << 31))
+        return fail(c, GS3DC_ERR_INVALID_ARG, "the views' %llu tiles / %llu pixels exceed 2^24 / 2^31", tiles, pix);
+    sh.tiles = (unsigned)tiles;
+    sh.pix = pix;
+    sh.tile_digits = (bit_length(sh.tiles > 1 ? sh.tiles - 1 : 0u) + 7) / 8;
+    if ((rc = batch_buffers(c, sh))) return rc;
+    if (c->keep_grads && (rc = ensure_grads(c))) return rc;
+    const bool shape_new = b.cap == 0 || b.key[0] != c->N || b.key[1] != n_views || b.key[2] != (long long)sh.tiles ||
+                           b.key[3] != (long long)sh.pix;
+    if ((rc = batch_pairs(c, b.cap ? b.cap : (unsigned long long)sh.VN * 8ull + 4096ull, sh.tile_digits))) return rc;
+    const float* gt_dev = gt;
+    if (!gt_on_device) {
+        CK(b.gt.ensure(3 * pix));
+        CK(cudaMemcpyAsync(b.gt.p, gt, 3 * pix * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+        gt_dev = b.gt.p;
+    }
+    if (!b.views_host) {
+        CK(cudaMallocHost(&b.views_host, kMaxBatchViews * sizeof(StepParams)));
+        CK(cudaEventCreateWithFlags(&b.views_event, cudaEventDisableTiming));
+    }
+    bool first = shape_new;
+    const int step_before = c->adam_step;
+    for (int attempt = 0; attempt < 3; attempt++) {
+        c->adam_step = step_before + (tc->use_adam ? 1 : 0);
+        CK(cudaEventSynchronize(b.views_event));   // the staging's previous copy has been consumed
+        for (int v = 0; v < n_views; v++) {
+            StepParams& p = b.views_host[v];
+            fill_params(c, p, &cams[v], cfg, tc, iteration, gt_dev, nullptr);
+            // each view's L1 mean enters the loss with weight 1 / n_views
+            p.inv_n = 1.0f / ((float)n_views * 3.0f * (float)cams[v].width * (float)cams[v].height);
+            p.tile_base = tile_base[v];
+            p.pix_base = pix_base[v];
+            p.sort_passes = kDepthDigits + sh.tile_digits;
+        }
+        CK(cudaMemcpyAsync(b.views.p, b.views_host, (size_t)n_views * sizeof(StepParams), cudaMemcpyHostToDevice,
+                           c->stream));
+        CK(cudaEventRecord(b.views_event, c->stream));
+        const long long key[8] = {c->N, n_views, (long long)sh.tiles, (long long)sh.pix, (long long)b.cap,
+                                  c->form, (long long)c->spin_limit, c->max_coeffs + 1000 * (c->keep_grads ? 1 : 0)};
+        if (c->use_graph && !first && attempt == 0) {
+            if (!b.graph || std::memcmp(key, b.key, sizeof(key)) != 0) {
+                if (b.graph) cudaGraphExecDestroy(b.graph);
+                b.graph = nullptr;
+                cudaGraph_t g;
+                CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+                rc = seq_batch(c, sh);
+                cudaError_t ec = cudaStreamEndCapture(c->stream, &g);
+                if (rc) return rc;
+                CK(ec);
+                CK(cudaGraphInstantiate(&b.graph, g, 0));
+                cudaGraphDestroy(g);
+            }
+            CK(cudaGraphLaunch(b.graph, c->stream));
+            c->graph_replays++;
+        } else {
+            if ((rc = seq_batch(c, sh))) return rc;
+        }
+        std::memcpy(b.key, key, sizeof(key));
+        c->have_step_grads = c->keep_grads;
+        if (!loss && !first) {
+            c->pending_check = true;   // overflow is reported by the next synchronising call
+            return GS3DC_OK;
+        }
+        if ((rc = read_control(c))) {
+            c->adam_step = step_before;
+            return rc;
+        }
+        if (c->persist_host->sticky_overflow) {
+            if ((rc = acknowledge_overflow(c))) return rc;
+            const unsigned long long P = c->ctrl_host->total_pairs;
+            if (!(c->ctrl_host->status & kStatusOverflow))
+                return fail(c, GS3DC_ERR_PAIR_OVERFLOW, "an earlier queued train step overflowed the pair capacity");
+            if ((rc = batch_pairs(c, P + P / 4 + 4096, sh.tile_digits))) return rc;
+            first = true;
+            continue;
+        }
+        if (loss) *loss = (float)c->ctrl_host->loss_sum;
+        c->have_screen = c->have_pairs = c->have_sorted = c->have_raster = c->have_rgrad = c->have_grads = false;
         return GS3DC_OK;
     }
     c->adam_step = step_before;

@@ -148,10 +148,13 @@ template <typename S>
 __global__ void __launch_bounds__(kBlock) k_chosen_preprocess(const StepParams* __restrict__ spp, int N, ChosenPtrs c,
                                                               ScreenPtrs s, DepthKeys dk, uint2* __restrict__ rects,
                                                               Control* ctrl) {
-    const StepParams& sp = *spp;
+    // several views: blockIdx.y is the view, entries are view * N + i
+    const int view = blockIdx.y;
+    const StepParams& sp = spp[view];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i == 0) ctrl->gauss_keys = (unsigned long long)N;
+    if (i == 0 && view == 0) ctrl->gauss_keys = (unsigned long long)N * gridDim.y;
     if (i >= N) return;
+    const long long o = (long long)view * N + i;   // output entry
     const int mc3 = sp.max_coeffs * 3;
     const float p[3] = {c.pos[3 * i], c.pos[3 * i + 1], c.pos[3 * i + 2]};
     float rsc[3], rq[4], rop, sc[3], q[4], op;
@@ -189,22 +192,24 @@ __global__ void __launch_bounds__(kBlock) k_chosen_preprocess(const StepParams* 
                 dbits = __float_as_uint(r.depth);
             }
         }
-        s.rec0[i] = make_float4(r.px, r.py, r.con[0], r.con[1]);
-        s.rec1[i] = make_float4(r.con[2], r.opac, r.rgb[0], r.rgb[1]);
-        s.col_b[i] = r.rgb[2];
-        s.depth[i] = r.depth;
-        s.radius[i] = r.radius;
+        s.rec0[o] = make_float4(r.px, r.py, r.con[0], r.con[1]);
+        s.rec1[o] = make_float4(r.con[2], r.opac, r.rgb[0], r.rgb[1]);
+        s.col_b[o] = r.rgb[2];
+        s.depth[o] = r.depth;
+        s.radius[o] = r.radius;
     } else {
-        s.rec0[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-        s.rec1[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-        s.col_b[i] = 0.f;
-        s.depth[i] = 0.f;
-        s.radius[i] = 0;
+        s.rec0[o] = make_float4(0.f, 0.f, 0.f, 0.f);
+        s.rec1[o] = make_float4(0.f, 0.f, 0.f, 0.f);
+        s.col_b[o] = 0.f;
+        s.depth[o] = 0.f;
+        s.radius[o] = 0;
     }
-    s.tiles[i] = cnt;
-    rects[i] = rect;
-    dk.keys[i] = cnt > 0 ? dbits : 0xFFFFFFFFu;
-    dk.vals[i] = (unsigned)i;
+    s.tiles[o] = cnt;
+    rects[o] = rect;
+    const unsigned key = cnt > 0 ? dbits : 0xFFFFFFFFu;
+    if (dk.keys64) dk.keys64[o] = ((unsigned long long)view << 32) | key;
+    else dk.keys[o] = key;
+    dk.vals[o] = (unsigned)o;
 }
 
 // ---- optimiser helpers ----
@@ -266,9 +271,10 @@ struct __align__(16) ChosenBwdShared {
 // (preprocessor_backward_cpu.cpp:205-645) from there into shared-memory
 // gradients, then Adam over the CTA's contiguous parameter slice with 16-byte
 // accesses and stochastic rounding (and, when asked, the FP32 gradients).
-template <typename S>
+template <typename S, bool MULTI>
 __global__ void __launch_bounds__(kCB) k_chosen_backward(const StepParams* __restrict__ spp, int N, int mc3,
-                                                         ChosenPtrs c, RGradPtrs rg, GradPtrs gout, Control* ctrl) {
+                                                         ChosenPtrs c, RGradPtrs rg, GradPtrs gout, Control* ctrl,
+                                                         int n_views) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     ChosenBwdShared<S>& sm = *reinterpret_cast<ChosenBwdShared<S>*>(smem_raw);
     const StepParams& sp = *spp;
@@ -281,6 +287,7 @@ __global__ void __launch_bounds__(kCB) k_chosen_backward(const StepParams* __res
     const S* shg = static_cast<const S*>(c.sh) + (size_t)mc3 * g0;
     if (ng == kCB) {
         // a full CTA: every slice is a multiple of 16 bytes at a 16-byte aligned offset -> bulk copies
+        // (several views: the screen gradients follow per view below)
         if (tid == 0) {
             mbar_init(&sm.bar, 1);
             mbar_fence_init();
@@ -288,14 +295,17 @@ __global__ void __launch_bounds__(kCB) k_chosen_backward(const StepParams* __res
         __syncthreads();
         if (tid == 0) {
             const unsigned sh_bytes = (unsigned)(kCB * mc3 * (int)sizeof(S));
-            mbar_arrive_expect_tx(&sm.bar, sh_bytes + (unsigned)kCB * (16u + 12u + 8u + 12u + 12u + 4u));
+            const unsigned grad_bytes = MULTI ? 0u : (unsigned)kCB * (8u + 12u + 12u + 4u);
+            mbar_arrive_expect_tx(&sm.bar, sh_bytes + (unsigned)kCB * (16u + 12u) + grad_bytes);
             tma_load_1d(sm.sh, shg, sh_bytes, &sm.bar);
             tma_load_1d(sm.attr, reinterpret_cast<const uint4*>(c.attr) + g0, 16u * kCB, &sm.bar);
             tma_load_1d(sm.pos, c.pos + 3 * g0, 12u * kCB, &sm.bar);
-            tma_load_1d(sm.dm2, rg.dm2 + 2 * g0, 8u * kCB, &sm.bar);
-            tma_load_1d(sm.dcon, rg.dcon + 3 * g0, 12u * kCB, &sm.bar);
-            tma_load_1d(sm.drgb, rg.drgb + 3 * g0, 12u * kCB, &sm.bar);
-            tma_load_1d(sm.dop, rg.dop + g0, 4u * kCB, &sm.bar);
+            if (!MULTI) {
+                tma_load_1d(sm.dm2, rg.dm2 + 2 * g0, 8u * kCB, &sm.bar);
+                tma_load_1d(sm.dcon, rg.dcon + 3 * g0, 12u * kCB, &sm.bar);
+                tma_load_1d(sm.drgb, rg.drgb + 3 * g0, 12u * kCB, &sm.bar);
+                tma_load_1d(sm.dop, rg.dop + g0, 4u * kCB, &sm.bar);
+            }
         }
         mbar_wait(&sm.bar, 0, sp.spin_limit, &ctrl->status);
     } else {
@@ -303,75 +313,100 @@ __global__ void __launch_bounds__(kCB) k_chosen_backward(const StepParams* __res
         for (int e = tid; e < mc3 * ng; e += kCB) shs[e] = shg[e];
         for (int e = tid; e < ng; e += kCB) sm.attr[e] = reinterpret_cast<const uint4*>(c.attr)[g0 + e];
         for (int e = tid; e < 3 * ng; e += kCB) sm.pos[e] = c.pos[3 * g0 + e];
-        for (int e = tid; e < 2 * ng; e += kCB) sm.dm2[e] = rg.dm2[2 * g0 + e];
-        for (int e = tid; e < 3 * ng; e += kCB) {
-            sm.dcon[e] = rg.dcon[3 * g0 + e];
-            sm.drgb[e] = rg.drgb[3 * g0 + e];
+        if (!MULTI) {
+            for (int e = tid; e < 2 * ng; e += kCB) sm.dm2[e] = rg.dm2[2 * g0 + e];
+            for (int e = tid; e < 3 * ng; e += kCB) {
+                sm.dcon[e] = rg.dcon[3 * g0 + e];
+                sm.drgb[e] = rg.drgb[3 * g0 + e];
+            }
+            for (int e = tid; e < ng; e += kCB) sm.dop[e] = rg.dop[g0 + e];
         }
-        for (int e = tid; e < ng; e += kCB) sm.dop[e] = rg.dop[g0 + e];
         __syncthreads();
     }
-    // the screen-gradient accumulators restart at zero for the next step
-    for (int e = tid; e < 2 * ng; e += kCB) rg.dm2[2 * g0 + e] = 0.f;
-    for (int e = tid; e < 3 * ng; e += kCB) {
-        rg.dcon[3 * g0 + e] = 0.f;
-        rg.drgb[3 * g0 + e] = 0.f;
-    }
-    for (int e = tid; e < ng; e += kCB) rg.dop[g0 + e] = 0.f;
-    // ---- phase 1: per-Gaussian adjoint ----
+    // ---- phase 1: per-Gaussian adjoint (summed over the views) ----
+    BwdIn in;
+    float shf[48];
     if (tid < ng) {
-        BwdIn in;
-        BwdOut o;
 #pragma unroll
-        for (int k = 0; k < 3; k++) {
-            in.p[k] = sm.pos[3 * tid + k];
-            in.dcn[k] = sm.dcon[3 * tid + k];
-            in.drgb[k] = sm.drgb[3 * tid + k];
-            o.gp[k] = o.gs[k] = o.geff[k] = 0.f;
-        }
-#pragma unroll
-        for (int k = 0; k < 4; k++) o.gq[k] = 0.f;
-        o.gop = 0.f;
-#pragma unroll
-        for (int k = 0; k < 16; k++) o.basis[k] = 0.f;
-        in.dm[0] = sm.dm2[2 * tid];
-        in.dm[1] = sm.dm2[2 * tid + 1];
-        in.dop = sm.dop[tid];
+        for (int k = 0; k < 3; k++) in.p[k] = sm.pos[3 * tid + k];
         in.act = nullptr;
         load_attr<S>(sm.attr, tid, in.rsc, &in.rop, in.rq);
-        // every gradient is linear in the screen gradients: a Gaussian without any has none
-        const bool any = in.dm[0] != 0.f || in.dm[1] != 0.f || in.dcn[0] != 0.f || in.dcn[1] != 0.f ||
-                         in.dcn[2] != 0.f || in.drgb[0] != 0.f || in.drgb[1] != 0.f || in.drgb[2] != 0.f ||
-                         in.dop != 0.f;
-        if (any) {
-            float shf[48];
-            if (mc3 == 48) {
-                // this Gaussian's 96 SH bytes as six 16-byte loads
-                const uint4* row = sm.sh + 6 * tid;
+        if (mc3 == 48) {
+            // this Gaussian's 96 SH bytes as six 16-byte loads
+            const uint4* row = sm.sh + 6 * tid;
 #pragma unroll
-                for (int q = 0; q < 6; q++) {
-                    const uint4 v = row[q];
-                    const S* h = reinterpret_cast<const S*>(&v);
+            for (int q = 0; q < 6; q++) {
+                const uint4 v = row[q];
+                const S* h = reinterpret_cast<const S*>(&v);
 #pragma unroll
-                    for (int k = 0; k < 8; k++) shf[8 * q + k] = ldf(h[k]);
-                }
-            } else {
-                const S* shs = reinterpret_cast<const S*>(sm.sh) + mc3 * tid;
-#pragma unroll
-                for (int k = 0; k < 48; k++) shf[k] = k < mc3 ? ldf(shs[k]) : 0.f;
+                for (int k = 0; k < 8; k++) shf[8 * q + k] = ldf(h[k]);
             }
-            in.sh = shf;
-            backward_one(sp, in, o);
-        }
+        } else {
+            const S* shs = reinterpret_cast<const S*>(sm.sh) + mc3 * tid;
 #pragma unroll
-        for (int k = 0; k < 3; k++) {
-            sm.g_pos[3 * tid + k] = o.gp[k];
-            sm.g_sc[3 * tid + k] = o.gs[k];
+            for (int k = 0; k < 48; k++) shf[k] = k < mc3 ? ldf(shs[k]) : 0.f;
         }
+        in.sh = shf;
 #pragma unroll
-        for (int k = 0; k < 4; k++) sm.g_rot[4 * tid + k] = o.gq[k];
-        sm.g_op[tid] = o.gop;
-        for (int k = 0; k < mc3; k++) sm.g_sh[kShPitch * tid + k] = o.basis[k / 3] * o.geff[k % 3];
+        for (int k = 0; k < 3; k++) sm.g_pos[3 * tid + k] = sm.g_sc[3 * tid + k] = 0.f;
+#pragma unroll
+        for (int k = 0; k < 4; k++) sm.g_rot[4 * tid + k] = 0.f;
+        sm.g_op[tid] = 0.f;
+        for (int k = 0; k < mc3; k++) sm.g_sh[kShPitch * tid + k] = 0.f;
+    }
+    for (int v = 0; v < (MULTI ? n_views : 1); v++) {
+        const long long e0 = (long long)v * N + g0;   // this view's first (view, Gaussian) entry
+        if (MULTI) {
+            __syncthreads();   // the previous view's screen gradients have been read
+            for (int e = tid; e < 2 * ng; e += kCB) sm.dm2[e] = rg.dm2[2 * e0 + e];
+            for (int e = tid; e < 3 * ng; e += kCB) {
+                sm.dcon[e] = rg.dcon[3 * e0 + e];
+                sm.drgb[e] = rg.drgb[3 * e0 + e];
+            }
+            for (int e = tid; e < ng; e += kCB) sm.dop[e] = rg.dop[e0 + e];
+            __syncthreads();
+        }
+        // the screen-gradient accumulators restart at zero for the next step
+        for (int e = tid; e < 2 * ng; e += kCB) rg.dm2[2 * e0 + e] = 0.f;
+        for (int e = tid; e < 3 * ng; e += kCB) {
+            rg.dcon[3 * e0 + e] = 0.f;
+            rg.drgb[3 * e0 + e] = 0.f;
+        }
+        for (int e = tid; e < ng; e += kCB) rg.dop[e0 + e] = 0.f;
+        if (tid < ng) {
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                in.dcn[k] = sm.dcon[3 * tid + k];
+                in.drgb[k] = sm.drgb[3 * tid + k];
+            }
+            in.dm[0] = sm.dm2[2 * tid];
+            in.dm[1] = sm.dm2[2 * tid + 1];
+            in.dop = sm.dop[tid];
+            // every gradient is linear in the screen gradients: a view without any adds none
+            const bool any = in.dm[0] != 0.f || in.dm[1] != 0.f || in.dcn[0] != 0.f || in.dcn[1] != 0.f ||
+                             in.dcn[2] != 0.f || in.drgb[0] != 0.f || in.drgb[1] != 0.f || in.drgb[2] != 0.f ||
+                             in.dop != 0.f;
+            if (any) {
+                BwdOut o;
+#pragma unroll
+                for (int k = 0; k < 3; k++) o.gp[k] = o.gs[k] = o.geff[k] = 0.f;
+#pragma unroll
+                for (int k = 0; k < 4; k++) o.gq[k] = 0.f;
+                o.gop = 0.f;
+#pragma unroll
+                for (int k = 0; k < 16; k++) o.basis[k] = 0.f;
+                backward_one(spp[v], in, o);
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    sm.g_pos[3 * tid + k] += o.gp[k];
+                    sm.g_sc[3 * tid + k] += o.gs[k];
+                }
+#pragma unroll
+                for (int k = 0; k < 4; k++) sm.g_rot[4 * tid + k] += o.gq[k];
+                sm.g_op[tid] += o.gop;
+                for (int k = 0; k < mc3; k++) sm.g_sh[kShPitch * tid + k] += o.basis[k / 3] * o.geff[k % 3];
+            }
+        }
     }
     __syncthreads();
     // ---- phase 2: optimiser over this CTA's slice (and the gradients, when kept) ----
@@ -470,10 +505,21 @@ cudaError_t launch_chosen_to_raw(cudaStream_t st, int N, int mc3, bool fp16, Cho
 }
 
 cudaError_t launch_chosen_preprocess(cudaStream_t st, const StepParams* sp, int N, bool fp16, ChosenPtrs c,
-                                     ScreenPtrs s, DepthKeys dk, uint2* rects, Control* ctrl) {
-    if (N <= 0) return cudaSuccess;
-    if (fp16) k_chosen_preprocess<__half><<<grid_for(N, kBlock), kBlock, 0, st>>>(sp, N, c, s, dk, rects, ctrl);
-    else k_chosen_preprocess<__nv_bfloat16><<<grid_for(N, kBlock), kBlock, 0, st>>>(sp, N, c, s, dk, rects, ctrl);
+                                     ScreenPtrs s, DepthKeys dk, uint2* rects, Control* ctrl, int n_views) {
+    if (N <= 0 || n_views <= 0) return cudaSuccess;
+    const dim3 grid((unsigned)grid_for(N, kBlock), (unsigned)n_views);
+    if (fp16) k_chosen_preprocess<__half><<<grid, kBlock, 0, st>>>(sp, N, c, s, dk, rects, ctrl);
+    else k_chosen_preprocess<__nv_bfloat16><<<grid, kBlock, 0, st>>>(sp, N, c, s, dk, rects, ctrl);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_raster_fwd_fast_multi(cudaStream_t st, const StepParams* views, int n_views, unsigned n_tiles,
+                                         const unsigned* ranges, const unsigned* order, const unsigned* vals,
+                                         ScreenPtrs s, PixelPtrs px, Control* ctrl) {
+    if (n_tiles == 0) return cudaSuccess;
+    // persistent: as many CTAs as fit resident (9 per SM at this kernel's registers)
+    k_raster_fwd<true, FastBlend, true><<<9 * 148, kFwdThreads, 0, st>>>(views, ranges, order, vals, s, px, ctrl,
+                                                                       n_views, n_tiles);
     return cudaGetLastError();
 }
 
@@ -486,22 +532,31 @@ cudaError_t launch_raster_fwd_fast(cudaStream_t st, const StepParams* sp, int nu
 }
 
 cudaError_t launch_chosen_backward_adam(cudaStream_t st, const StepParams* sp, int N, int mc3, bool fp16,
-                                        ChosenPtrs c, RGradPtrs rg, GradPtrs g, Control* ctrl) {
+                                        ChosenPtrs c, RGradPtrs rg, GradPtrs g, Control* ctrl, int n_views) {
     if (N <= 0) return cudaSuccess;
     if (mc3 > 48) return cudaErrorInvalidValue;
     const int grid = grid_for(N, kCB);
     const int smem = (int)sizeof(ChosenBwdShared<__half>);   // same size for both 16-bit types
     static bool attr_set = false;
     if (!attr_set) {
-        cudaError_t e1 = cudaFuncSetAttribute(k_chosen_backward<__half>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        cudaError_t e2 =
-            cudaFuncSetAttribute(k_chosen_backward<__nv_bfloat16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e1 != cudaSuccess) return e1;
-        if (e2 != cudaSuccess) return e2;
+        cudaError_t e[4] = {
+            cudaFuncSetAttribute(k_chosen_backward<__half, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+            cudaFuncSetAttribute(k_chosen_backward<__nv_bfloat16, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 smem),
+            cudaFuncSetAttribute(k_chosen_backward<__half, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+            cudaFuncSetAttribute(k_chosen_backward<__nv_bfloat16, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 smem)};
+        for (cudaError_t x : e)
+            if (x != cudaSuccess) return x;
         attr_set = true;
     }
-    if (fp16) k_chosen_backward<__half><<<grid, kCB, smem, st>>>(sp, N, mc3, c, rg, g, ctrl);
-    else k_chosen_backward<__nv_bfloat16><<<grid, kCB, smem, st>>>(sp, N, mc3, c, rg, g, ctrl);
+    if (n_views > 1) {
+        if (fp16) k_chosen_backward<__half, true><<<grid, kCB, smem, st>>>(sp, N, mc3, c, rg, g, ctrl, n_views);
+        else k_chosen_backward<__nv_bfloat16, true><<<grid, kCB, smem, st>>>(sp, N, mc3, c, rg, g, ctrl, n_views);
+    } else {
+        if (fp16) k_chosen_backward<__half, false><<<grid, kCB, smem, st>>>(sp, N, mc3, c, rg, g, ctrl, 1);
+        else k_chosen_backward<__nv_bfloat16, false><<<grid, kCB, smem, st>>>(sp, N, mc3, c, rg, g, ctrl, 1);
+    }
     return cudaGetLastError();
 }
 

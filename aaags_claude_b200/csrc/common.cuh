@@ -50,6 +50,10 @@ struct StepParams {
     Persist* persist;
     const float* raw_rot; // [N*4] raw quaternions when the device model is an activated one (backward only)
     unsigned seed;        // per-step seed of the reduced-storage form's stochastic rounding
+    // multi-view steps (one StepParams per view; zero for a single view): the view's
+    // first global tile id and first pixel in the concatenated per-view buffers
+    unsigned tile_base;
+    unsigned pix_base;
 };
 
 // Small device control block, zeroed by one memset at the start of a step.
@@ -62,6 +66,7 @@ struct Control {
     unsigned tickets[16];             // dynamic CTA tickets (0: preprocess/bin, 1..8: sort passes)
     unsigned hist[kMaxPasses][256];   // radix digit histograms of all passes
     unsigned long long gauss_keys;    // depth-first pipeline: keys of the Gaussian depth sort
+    unsigned work[2];                 // persistent multi-view rasterisers: next tile of the forward / backward
 };
 constexpr size_t kControlReadback = 24;
 

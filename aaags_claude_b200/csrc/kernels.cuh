@@ -83,6 +83,7 @@ struct ScreenArrays {
 struct DepthKeys {
     unsigned* keys;             // [N] depth bits, ~0u for Gaussians without pairs
     unsigned* vals;             // [N] Gaussian index
+    unsigned long long* keys64 = nullptr;   // several views: (view << 32 | depth bits) instead of keys
 };
 
 // Reduced-storage ("chosen") form: positions FP32, the other attributes and the
@@ -105,12 +106,22 @@ cudaError_t launch_chosen_to_raw(cudaStream_t st, int N, int mc3, bool fp16, Cho
 // Preprocess of the reduced-storage model: screen records, depth-sort input
 // and tile rectangles (the reference's rectangle cut to the box of the
 // ellipse where alpha can reach 1/255).
+// n_views > 1: sp is the views' parameter array; the outputs hold (view,
+// Gaussian) entries view * N + i and the depth keys go to dk.keys64.
 cudaError_t launch_chosen_preprocess(cudaStream_t st, const StepParams* sp, int N, bool fp16, ChosenPtrs c,
-                                     ScreenPtrs s, DepthKeys dk, uint2* rects, Control* ctrl);
+                                     ScreenPtrs s, DepthKeys dk, uint2* rects, Control* ctrl, int n_views = 1);
 // Forward rasteriser with the fast-exp blend decision and fused L1.
 cudaError_t launch_raster_fwd_fast(cudaStream_t st, const StepParams* sp, int num_tiles, const unsigned* ranges,
                                    const unsigned* order, const unsigned* vals, ScreenPtrs s, PixelPtrs px,
                                    Control* ctrl);
+// One persistent launch over all tiles of n_views views (views = their
+// parameter array, order = all global tiles, heavy first).
+cudaError_t launch_raster_fwd_fast_multi(cudaStream_t st, const StepParams* views, int n_views, unsigned n_tiles,
+                                         const unsigned* ranges, const unsigned* order, const unsigned* vals,
+                                         ScreenPtrs s, PixelPtrs px, Control* ctrl);
+cudaError_t launch_raster_bwd_fast_multi(cudaStream_t st, const StepParams* views, int n_views, unsigned n_tiles,
+                                         const unsigned* ranges, const unsigned* order, const unsigned* vals,
+                                         ScreenPtrs s, PixelPtrs px, RGradPtrs g, Control* ctrl);
 // Backward rasteriser deciding acceptance like launch_raster_fwd_fast.
 cudaError_t launch_raster_bwd_fast(cudaStream_t st, const StepParams* sp, int num_tiles, const unsigned* ranges,
                                    const unsigned* order, const unsigned* vals, ScreenPtrs s, PixelPtrs px,
@@ -118,8 +129,10 @@ cudaError_t launch_raster_bwd_fast(cudaStream_t st, const StepParams* sp, int nu
 // Per-Gaussian adjoint fused with Adam (stochastic rounding into the 16-bit
 // parameters and BF16 moments); zeroes the screen-gradient accumulators.
 // With g.g_pos != NULL the FP32 raw-parameter gradients are stored too.
+// n_views > 1: sp is the views' parameter array and rg holds (view, Gaussian)
+// entries; each Gaussian's gradient is the sum over the views.
 cudaError_t launch_chosen_backward_adam(cudaStream_t st, const StepParams* sp, int N, int mc3, bool fp16,
-                                        ChosenPtrs c, RGradPtrs rg, GradPtrs gout, Control* ctrl);
+                                        ChosenPtrs c, RGradPtrs rg, GradPtrs gout, Control* ctrl, int n_views = 1);
 
 // ---- plain FP32 kernels (plain.cu, compiled without FMA contraction) ----
 // Preprocess; emits the pairs in Gaussian order, or -- when dk.keys != NULL --
@@ -134,8 +147,12 @@ cudaError_t launch_preprocess_plain(cudaStream_t st, const StepParams* sp, int N
 // rects (optional): per-Gaussian tile rectangles (xmin | ymin << 16,
 // xmax | ymax << 16) written by the reduced-storage preprocess; without them
 // the rectangle is recomputed from the stored mean and radius.
+// n_per_view > 0: several views; N counts (view, Gaussian) entries
+// view * n_per_view + i, and sp is the views' parameter array (the tile ids
+// emitted are global: the view's tile_base plus its local tile).
 cudaError_t launch_emit_ranked(cudaStream_t st, const StepParams* sp, int N, const unsigned* rank_gid,
-                               ScreenPtrs s, PairPtrs pr, Control* ctrl, const uint2* rects = nullptr);
+                               ScreenPtrs s, PairPtrs pr, Control* ctrl, const uint2* rects = nullptr,
+                               int n_per_view = 0, int hist_slot = kDepthDigits);
 cudaError_t launch_bin_arrays(cudaStream_t st, const StepParams* sp, int N, ScreenArrays a,
                               PairPtrs pr, Control* ctrl);
 cudaError_t launch_export_screen(cudaStream_t st, int N, ScreenPtrs s, ScreenArrays a);

@@ -77,6 +77,8 @@ struct EmitShared {
     int limit[kBlock];     // pairs actually emitted (rect area, <= count)
     unsigned depth[kBlock];
     unsigned gid[kBlock];  // Gaussian index written as the pair's value
+    unsigned tbase[kBlock];  // first global tile id of the Gaussian's view (0 for one view)
+    int gx[kBlock];          // tile-grid width of the Gaussian's view
     unsigned long long base;
 };
 
@@ -90,7 +92,8 @@ struct EmitShared {
 __device__ __forceinline__ void scan_and_emit(EmitShared& sm, int blk, unsigned gid, int cnt, int emit, int rx, int ry,
                                               int rw, unsigned dbits, int grid_x, PairPtrs pr,
                                               Control* ctrl, unsigned spin_limit, Persist* persist,
-                                              unsigned* thist = nullptr, int nd = 0) {
+                                              unsigned* thist = nullptr, int nd = 0, unsigned tile_base_t = 0u,
+                                              int grid_x_t = -1) {
     const int tid = threadIdx.x;
     int total;
     const int incl = block_inclusive_scan(cnt, sm.warp, &total);
@@ -100,6 +103,8 @@ __device__ __forceinline__ void scan_and_emit(EmitShared& sm, int blk, unsigned 
     sm.limit[tid] = emit;
     sm.depth[tid] = dbits;
     sm.gid[tid] = gid;
+    sm.tbase[tid] = tile_base_t;
+    sm.gx[tid] = grid_x_t < 0 ? grid_x : grid_x_t;
     if (tid == 0) {
         const unsigned long long ex =
             lookback_exclusive(pr.scan_desc, blk, (unsigned long long)total, &ctrl->status, spin_limit);
@@ -126,7 +131,7 @@ __device__ __forceinline__ void scan_and_emit(EmitShared& sm, int blk, unsigned 
         const int r = sm.rect[lo];
         const int x = (r & 0xffff) + local % w;
         const int y = (r >> 16) + local / w;
-        const unsigned tile = (unsigned)(y * grid_x + x);
+        const unsigned tile = sm.tbase[lo] + (unsigned)(y * sm.gx[lo] + x);
         if (pr.tiles32) {
             pr.tiles32[dst] = tile;
             for (int d = 0; d < nd; d++) atomicAdd(&thist[d * 256 + ((tile >> (8 * d)) & 255u)], 1u);
@@ -219,21 +224,27 @@ __global__ void __launch_bounds__(kBlock) k_preprocess(const StepParams* __restr
 __global__ void __launch_bounds__(kBlock) k_emit_ranked(const StepParams* __restrict__ spp, int N,
                                                         const unsigned* __restrict__ rank_gid, ScreenPtrs s,
                                                         PairPtrs pr, const uint2* __restrict__ rects,
-                                                        Control* ctrl) {
+                                                        Control* ctrl, int n_per_view, int hist_slot) {
     __shared__ EmitShared sm;
     __shared__ int s_blk;
     __shared__ unsigned s_thist[kMaxPasses - kDepthDigits][256];
     const StepParams& sp = *spp;
-    const int nd = sp.sort_passes - kDepthDigits;   // 8-bit digits of the tile ids
+    const int nd = sp.sort_passes - kDepthDigits;   // 8-bit digits of the tile ids (control slots hist_slot..)
     for (int e = threadIdx.x; e < nd * 256; e += kBlock) (&s_thist[0][0])[e] = 0;
     if (threadIdx.x == 0) s_blk = (int)atomicAdd(&ctrl->tickets[0], 1u);
     __syncthreads();
     const int blk = s_blk;
     const int r = blk * kBlock + threadIdx.x;
-    int cnt = 0, rx = 0, ry = 0, rw = 1;
-    unsigned g = 0, dbits = 0;
+    int cnt = 0, rx = 0, ry = 0, rw = 1, gx = sp.grid_x;
+    unsigned g = 0, dbits = 0, tbase = 0;
     if (r < N) {
         g = rank_gid[r];
+        if (n_per_view > 0) {
+            // several views: entry g = view * n_per_view + Gaussian, spp is the views' parameter array
+            const StepParams& vp = spp[g / (unsigned)n_per_view];
+            gx = vp.grid_x;
+            tbase = vp.tile_base;
+        }
         cnt = s.tiles[g];
         if (cnt > 0) {
             if (rects) {
@@ -254,11 +265,11 @@ __global__ void __launch_bounds__(kBlock) k_emit_ranked(const StepParams* __rest
         }
     }
     scan_and_emit(sm, blk, g, cnt, cnt, rx, ry, rw, dbits, sp.grid_x, pr, ctrl, sp.spin_limit, sp.persist,
-                  &s_thist[0][0], nd);
+                  &s_thist[0][0], nd, tbase, gx);
     __syncthreads();
     for (int e = threadIdx.x; e < nd * 256; e += kBlock) {
         const unsigned v = (&s_thist[0][0])[e];
-        if (v) atomicAdd(&ctrl->hist[kDepthDigits + (e >> 8)][e & 255], v);
+        if (v) atomicAdd(&ctrl->hist[hist_slot + (e >> 8)][e & 255], v);
     }
 }
 
@@ -663,9 +674,11 @@ cudaError_t launch_preprocess_plain(cudaStream_t st, const StepParams* sp, int N
 }
 
 cudaError_t launch_emit_ranked(cudaStream_t st, const StepParams* sp, int N, const unsigned* rank_gid,
-                               ScreenPtrs s, PairPtrs pr, Control* ctrl, const uint2* rects) {
+                               ScreenPtrs s, PairPtrs pr, Control* ctrl, const uint2* rects, int n_per_view,
+                               int hist_slot) {
     if (N <= 0) return cudaSuccess;
-    k_emit_ranked<<<blocks_for(N, kBlock), kBlock, 0, st>>>(sp, N, rank_gid, s, pr, rects, ctrl);
+    k_emit_ranked<<<blocks_for(N, kBlock), kBlock, 0, st>>>(sp, N, rank_gid, s, pr, rects, ctrl, n_per_view,
+                                                            hist_slot);
     return cudaGetLastError();
 }
 

@@ -65,12 +65,18 @@ struct FastAccept {
 constexpr int kBwdThreads = 128;
 constexpr int kBwdBatch = 256;
 
-template <bool FROM_SIGN, class Accept>
+//
+// MULTI: one persistent launch over the tiles of several views (spp = the views'
+// parameters); a CTA takes the next entry of `order` from a work counter and
+// renders the tile with its view's camera and pixel slice.  The screen
+// gradients then belong to (view, Gaussian) entries: vals holds view * N + i.
+template <bool FROM_SIGN, class Accept, bool MULTI = false>
 __global__ void __launch_bounds__(kBwdThreads) k_raster_bwd(const StepParams* __restrict__ spp,
                                                             const unsigned* __restrict__ ranges,
                                                             const unsigned* __restrict__ order,
                                                             const unsigned* __restrict__ vals, ScreenPtrs s,
-                                                            PixelPtrs px, RGradPtrs g, Control* ctrl) {
+                                                            PixelPtrs px, RGradPtrs g, Control* ctrl,
+                                                            int n_views = 1, unsigned n_tiles = 0) {
     __shared__ float4 s_r0[kBwdBatch];
     __shared__ float4 s_r1[kBwdBatch];
     __shared__ float s_b[kBwdBatch];
@@ -79,11 +85,35 @@ __global__ void __launch_bounds__(kBwdThreads) k_raster_bwd(const StepParams* __
     __shared__ float4 s_box[kBwdBatch];
     __shared__ float s_acc[9][kBwdBatch];   // r, g, b, opacity, mean.x, mean.y, conic a, b, c
     __shared__ unsigned s_maxlast;
-    const StepParams& sp = *spp;
-    if (FROM_SIGN && ((ctrl->status & kStatusOverflow) || sp.persist->sticky_overflow)) return;
+    __shared__ unsigned s_next;
+    if (FROM_SIGN && ((ctrl->status & kStatusOverflow) || spp->persist->sticky_overflow)) return;
+    for (int iter = 0;; iter++) {
+    int tile;
+    if (MULTI) {
+        if (threadIdx.x == 0) s_next = atomicAdd(&ctrl->work[1], 1u);
+        __syncthreads();
+        const unsigned t = s_next;
+        __syncthreads();
+        if (t >= n_tiles) break;
+        tile = (int)order[t];
+    } else {
+        if (iter > 0) break;
+        tile = order ? (int)order[blockIdx.x] : (int)blockIdx.x;
+    }
+    int view = 0;
+    if (MULTI) {
+        int lo = 0, hi = n_views;   // last view whose tile_base <= tile
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (spp[mid].tile_base <= (unsigned)tile) lo = mid;
+            else hi = mid;
+        }
+        view = lo;
+    }
+    const StepParams& sp = spp[view];
     const int W = sp.cam.width, H = sp.cam.height;
-    const int tile = order ? (int)order[blockIdx.x] : (int)blockIdx.x;
-    const int tx = tile % sp.grid_x, ty = tile / sp.grid_x;
+    const int ltile = tile - (int)sp.tile_base;
+    const int tx = ltile % sp.grid_x, ty = ltile / sp.grid_x;
     const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int x = tx * kTile + (int)(lane & 15);
     const int ybase = ty * kTile + 4 * (int)warp + (int)(lane >> 4);
@@ -99,7 +129,7 @@ __global__ void __launch_bounds__(kBwdThreads) k_raster_bwd(const StepParams* __
         last[p] = 0;
         dC[p][0] = dC[p][1] = dC[p][2] = 0.0f;
         if (x < W && y < H) {
-            const int pix = y * W + x;
+            const int pix = (int)sp.pix_base + y * W + x;
             T[p] = px.T_final[pix];
             last[p] = px.last_j[pix];
             if (FROM_SIGN) {
@@ -123,7 +153,7 @@ __global__ void __launch_bounds__(kBwdThreads) k_raster_bwd(const StepParams* __
     if (mylast) atomicMax(&s_maxlast, mylast);
     __syncthreads();
     const unsigned maxlast = s_maxlast;
-    if (maxlast <= rs) return;
+    if (maxlast <= rs) continue;   // uniform: nothing of this tile contributed
     const unsigned wlast = __reduce_max_sync(0xffffffffu, mylast);
     const float wx0 = (float)(tx * kTile), wx1 = wx0 + (float)(kTile - 1);
     const float wy0 = (float)(ty * kTile + 4 * (int)warp), wy1 = wy0 + 3.0f;
@@ -221,6 +251,7 @@ __global__ void __launch_bounds__(kBwdThreads) k_raster_bwd(const StepParams* __
         __syncthreads();
         be = bs;
     }
+    }
 }
 
 }  // namespace
@@ -241,6 +272,16 @@ cudaError_t launch_raster_bwd_fast(cudaStream_t st, const StepParams* sp, int nu
                                    RGradPtrs g, Control* ctrl) {
     if (num_tiles <= 0) return cudaSuccess;
     k_raster_bwd<true, FastAccept><<<num_tiles, kBwdThreads, 0, st>>>(sp, ranges, order, vals, s, px, g, ctrl);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_raster_bwd_fast_multi(cudaStream_t st, const StepParams* views, int n_views, unsigned n_tiles,
+                                         const unsigned* ranges, const unsigned* order, const unsigned* vals,
+                                         ScreenPtrs s, PixelPtrs px, RGradPtrs g, Control* ctrl) {
+    if (n_tiles == 0) return cudaSuccess;
+    // persistent: as many CTAs as fit resident (6 per SM at this kernel's registers)
+    k_raster_bwd<true, FastAccept, true><<<6 * 148, kBwdThreads, 0, st>>>(views, ranges, order, vals, s, px, g, ctrl,
+                                                                        n_views, n_tiles);
     return cudaGetLastError();
 }
 

@@ -24,22 +24,54 @@ namespace {
 constexpr int kFwdThreads = 128;
 constexpr int kFwdBatch = 256;
 
-template <bool FUSED_LOSS, class Blend>
+//
+// MULTI: one persistent launch over the tiles of several views.  spp is then
+// the array of the views' parameters; a CTA takes the next entry of `order`
+// (all views' tiles, heavy first) from a work counter, finds the tile's view
+// by its global id and renders it with that view's camera into the view's
+// slice of the concatenated pixel buffers.  The fused loss adds each view's
+// sum weighted by its inv_n.
+template <bool FUSED_LOSS, class Blend, bool MULTI = false>
 __global__ void __launch_bounds__(kFwdThreads) k_raster_fwd(const StepParams* __restrict__ spp,
                                                             const unsigned* __restrict__ ranges,
                                                             const unsigned* __restrict__ order,
                                                             const unsigned* __restrict__ vals, ScreenPtrs s,
-                                                            PixelPtrs px, Control* ctrl) {
+                                                            PixelPtrs px, Control* ctrl, int n_views = 1,
+                                                            unsigned n_tiles = 0) {
     __shared__ float4 s_r0[kFwdBatch];
     __shared__ float4 s_r1[kFwdBatch];
     __shared__ float s_b[kFwdBatch];
     __shared__ float s_thr[kFwdBatch];
     __shared__ float4 s_box[kFwdBatch];
     __shared__ double s_loss[kFwdThreads / 32];
-    const StepParams& sp = *spp;
+    __shared__ unsigned s_next;
+    for (int iter = 0;; iter++) {
+    int tile;
+    if (MULTI) {
+        if (threadIdx.x == 0) s_next = atomicAdd(&ctrl->work[0], 1u);
+        __syncthreads();
+        const unsigned t = s_next;
+        __syncthreads();
+        if (t >= n_tiles) break;
+        tile = (int)order[t];
+    } else {
+        if (iter > 0) break;
+        tile = order ? (int)order[blockIdx.x] : (int)blockIdx.x;
+    }
+    int view = 0;
+    if (MULTI) {
+        int lo = 0, hi = n_views;   // last view whose tile_base <= tile
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (spp[mid].tile_base <= (unsigned)tile) lo = mid;
+            else hi = mid;
+        }
+        view = lo;
+    }
+    const StepParams& sp = spp[view];
     const int W = sp.cam.width, H = sp.cam.height;
-    const int tile = order ? (int)order[blockIdx.x] : (int)blockIdx.x;
-    const int tx = tile % sp.grid_x, ty = tile / sp.grid_x;
+    const int ltile = tile - (int)sp.tile_base;
+    const int tx = ltile % sp.grid_x, ty = ltile / sp.grid_x;
     const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int x = tx * kTile + (int)(lane & 15);
     const int ybase = ty * kTile + 4 * (int)warp + (int)(lane >> 4);
@@ -114,7 +146,7 @@ __global__ void __launch_bounds__(kFwdThreads) k_raster_fwd(const StepParams* __
     for (int p = 0; p < 2; p++) {
         const int y = ybase + 2 * p;
         if (x < W && y < H) {
-            const int pix = y * W + x;
+            const int pix = (int)sp.pix_base + y * W + x;
             const float o0 = C[p][0] + T[p] * sp.cfg.bg_color[0];
             const float o1 = C[p][1] + T[p] * sp.cfg.bg_color[1];
             const float o2 = C[p][2] + T[p] * sp.cfg.bg_color[2];
@@ -143,8 +175,10 @@ __global__ void __launch_bounds__(kFwdThreads) k_raster_fwd(const StepParams* __
             double t = 0.0;
 #pragma unroll
             for (int w = 0; w < kFwdThreads / 32; w++) t += s_loss[w];
-            atomicAdd(&ctrl->loss_sum, t);
+            atomicAdd(&ctrl->loss_sum, MULTI ? t * (double)sp.inv_n : t);
         }
+        __syncthreads();
+    }
     }
 }
 

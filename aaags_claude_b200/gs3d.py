@@ -87,6 +87,8 @@ def load_library(path: str = LIB_PATH):
         "gs3dc_get_stage_times": ([vp, ctypes.POINTER(ctypes.c_float), ctypes.c_int], ctypes.c_int),
         "gs3dc_selftest_bounded_wait": ([vp, ctypes.c_uint32], ctypes.c_int),
         "gs3dc_get_gradients": ([vp, vp, vp, vp, vp, vp], ctypes.c_int),
+        "gs3dc_train_step_batch": ([vp, ctypes.c_int, vp, vp, ctypes.c_int, vp, vp, ctypes.c_int, vp],
+                                   ctypes.c_int),
         "gs3dc_sort_pairs_static": ([i64, vp, vp, ctypes.c_int, vp, vp, vp, vp, ctypes.c_char_p, ctypes.c_size_t],
                                     ctypes.c_int),
     }
@@ -295,6 +297,20 @@ class Context:
     def update_raw_params(self, scene: S.Scene):
         r = scene.raw_struct()
         self._chk(self.L.gs3dc_update_raw_params(self.h, _ref(r)))
+
+    def train_step_batch(self, cams, gt, cfg, tcfg, iteration: int, want_loss: bool = True,
+                         gt_device_ptr: int | None = None) -> float | None:
+        """One step over several views (reduced-storage form); gt = targets concatenated view-major."""
+        arr = (S.Camera * len(cams))(*cams)
+        loss = ctypes.c_float()
+        if gt_device_ptr is not None:
+            gp, on_dev = ctypes.c_void_p(gt_device_ptr), 1
+        else:
+            gt = np.ascontiguousarray(gt, np.float32)
+            gp, on_dev = _p(gt), 0
+        self._chk(self.L.gs3dc_train_step_batch(self.h, len(cams), ctypes.byref(arr), gp, on_dev, _ref(cfg), _ref(tcfg),
+                                                int(iteration), ctypes.byref(loss) if want_loss else None))
+        return float(loss.value) if want_loss else None
 
     def get_gradients(self) -> dict:
         """Raw-parameter gradients of the last train step (GS3DC_OPT_KEEP_GRADIENTS)."""

@@ -220,6 +220,21 @@ int gs3dc_train_step(gs3dc_ctx* ctx, const gs3d_camera* cam, const float* gt, in
                      const gs3d_render_config* cfg, const gs3d_train_config* tc, int iteration,
                      float* loss);
 
+/* One training step over several views at once (no reference counterpart: the
+ * reference's Trainer::step takes one camera).  n_views cameras (1..255, any
+ * mix of resolutions), gt = their targets concatenated (view-major, each
+ * H*W*3 HWC; gt_on_device != 0: a device pointer).  The loss is the mean over
+ * the views of each view's L1 mean; one Adam step follows the gradients summed
+ * that way.  Runs in the reduced-storage form (GS3DC_FORM_BF16 / _FP16): every
+ * (view, Gaussian) is preprocessed, sorted by (view, depth), emitted with
+ * global (view, tile) ids and tile-sorted once; persistent rasterisers take the
+ * views' tiles heavy-first from a work counter; the whole step is replayed as
+ * one CUDA graph once its shape (views' sizes, N) repeats.  loss may be NULL
+ * (no wait for the device, as gs3dc_train_step). */
+int gs3dc_train_step_batch(gs3dc_ctx* ctx, int n_views, const gs3d_camera* cams, const float* gt,
+                           int gt_on_device, const gs3d_render_config* cfg,
+                           const gs3d_train_config* tc, int iteration, float* loss);
+
 /* Device time per stage of the last train step run with GS3DC_OPT_STAGE_TIMING,
  * measured with CUDA events on the context's stream.  ms[k] for k < n_stages,
  * indexed by GS3DC_STAGE_*. */

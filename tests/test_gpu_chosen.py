@@ -18,7 +18,8 @@ from oracle import pyoracle as O
 pytestmark = pytest.mark.gpu
 
 FORMS = {"bf16": gs3d.FORM_BF16, "fp16": gs3d.FORM_FP16}
-ZERO_LR = dict(lr_pos=0.0, lr_rest=0.0)
+# learning rates that leave every parameter unchanged (lr_schedule takes log(lr_pos): not 0)
+ZERO_LR = dict(lr_pos=1e-30, lr_rest=0.0)
 
 
 @pytest.fixture(params=sorted(FORMS))
