@@ -66,6 +66,10 @@ def _args(argv=None):
                     help="the chosen form timed against plain FP32 (plain: the plain form alone)")
     ap.add_argument("--plain-only-line", dest="plain_only_line", action="store_true",
                     help="time only --form (no plain comparison)")
+    ap.add_argument("--batched-steps", dest="batched_steps", type=int, default=5,
+                    help="timed steps of the 64-view step (0: skip it)")
+    ap.add_argument("--only-batched", dest="only_batched", action="store_true",
+                    help="print only the 64-view measurement (profiling runs)")
     return ap.parse_args(argv)
 
 
@@ -345,6 +349,9 @@ def run_ours(a) -> int:
     import torch
     rank, world, local = _dist_env()
     torch.cuda.set_device(local)
+    if a.only_batched:
+        print(json.dumps({"metric": METRIC, "batched_64_views": measure_batched(a, local)}), flush=True)
+        return 0
     dist = None
     if world > 1:
         import datetime
@@ -412,11 +419,84 @@ def run_ours(a) -> int:
             line["gpu_launches"] = head["gpu_launches"] + p["gpu_launches"]
         if world == 1 and not a.no_cpu_baseline and _workload_name(a) == WORKLOAD:
             line["cpu_baseline"] = cpu_baseline_reference(w, cfg, tc, gt)
+        if world == 1 and a.batched_steps > 0 and _workload_name(a) == WORKLOAD:
+            ctx.close()
+            line["batched_64_views"] = measure_batched(a, local)
         print(json.dumps(line), flush=True)
     ctx.close()
     if dist:
         dist.destroy_process_group()
     return 0
+
+
+# ---------------------------------------------------------------- multi-view step
+def measure_batched(a, local: int) -> dict:
+    """64-view step (1M Gaussians, mixed resolutions, BF16 storage) against the
+    plain FP32 path training the same 64 views one by one; MPix/s of each."""
+    import torch
+    from aaags_claude_b200 import gs3d
+    from aaags_claude_b200 import scenes as S
+    w = S.config_batched_64()
+    cams = w.cameras
+    cfg, tc = S.render_config(True), S.train_config()
+    ctx = gs3d.Context(local)
+    ctx.set_raw_params(w.target_scene)
+    gts = [ctx.render(cam, S.render_config(False)) for cam in cams]   # targets (setup, untimed)
+    offs = np.cumsum([0] + [g.size for g in gts])
+    gt_dev = torch.from_numpy(np.concatenate(gts)).to(f"cuda:{local}")
+    del gts
+    pix = int(sum(cam.width * cam.height for cam in cams))
+    stream = torch.cuda.ExternalStream(ctx.stream_handle(), device=f"cuda:{local}")
+    steps = max(3, min(a.batched_steps, 50))
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for k in range(steps):
+            fn(k)
+        e1.record(stream)
+        ctx.synchronize()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    # the chosen form, all 64 views per step
+    ctx.set_option(gs3d.OPT_FORM, gs3d.FORM_BF16)
+    ctx.set_raw_params(w.scene)
+    it = [0]
+
+    def batched(_k):
+        ctx.train_step_batch(cams, None, cfg, tc, it[0], want_loss=False, gt_device_ptr=gt_dev.data_ptr())
+        it[0] += 1
+    loss0 = ctx.train_step_batch(cams, None, cfg, tc, it[0], gt_device_ptr=gt_dev.data_ptr())
+    it[0] += 1
+    for k in range(3):
+        batched(k)
+    ctx.synchronize()
+    ms_b = timed(batched)
+    loss_b = ctx.train_step_batch(cams, None, cfg, tc, it[0], gt_device_ptr=gt_dev.data_ptr())
+    launches_b = ctx.stat(gs3d.STAT_KERNELS_LAST)
+
+    # the plain FP32 path, the same views one by one (one optimiser step per view)
+    ctx.set_option(gs3d.OPT_FORM, gs3d.FORM_PLAIN_FP32)
+    ctx.set_raw_params(w.scene)
+
+    def one_by_one(_k):
+        for v, cam in enumerate(cams):
+            ctx.train_step(cam, None, cfg, tc, it[0], want_loss=False,
+                           gt_device_ptr=gt_dev.data_ptr() + 4 * int(offs[v]))
+            it[0] += 1
+    one_by_one(0)
+    ctx.synchronize()
+    ms_p = timed(one_by_one)
+    ctx.close()
+    return {"workload": "batched_64views_1M_gaussians_mixed_320x240_to_3840x2160", "views": len(cams),
+            "mpix_per_step": round(pix / 1e6, 2), "steps": steps,
+            "batched_bf16": {"ms_per_step": round(ms_b, 3), "mpix_per_s": round(pix / 1e6 / (ms_b * 1e-3), 1),
+                             "gpu_launches_per_step": launches_b, "loss_first": loss0, "loss_last": loss_b},
+            "plain_fp32_one_by_one": {"ms_per_64_views": round(ms_p, 3),
+                                      "mpix_per_s": round(pix / 1e6 / (ms_p * 1e-3), 1)},
+            "mpix_ratio": round(ms_p / ms_b, 3)}
 
 
 # ---------------------------------------------------------------- reference arm
