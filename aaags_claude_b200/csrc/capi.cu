@@ -819,7 +819,8 @@ int seq_batch(gs3dc_ctx* c, const BatchShape& sh) {
     int which = 0;
     CK(launch_radix_sort32(c->stream, views, sh.tile_digits, 5, true, b.cap, b.keys[0].p, b.vals[0].p, b.keys[1].p,
                            b.vals[1].p, b.sort_desc.p, pstride, c->ctrl, &which));
-    CK(launch_tile_ranges32(c->stream, b.cap, b.keys[which].p, b.ranges.p, c->ctrl));
+    CK(launch_tile_ranges_views(c->stream, b.cap, b.keys[which].p, b.vals[which].p, views, c->N, b.ranges.p,
+                                c->ctrl));
     CK(launch_tile_order(c->stream, b.ranges.p, (int)sh.tiles, b.order.p));
     CK(launch_raster_fwd_fast_multi(c->stream, views, sh.V, sh.tiles, b.ranges.p, b.order.p, b.vals[which].p,
                                     batch_screen(c), batch_pixels(c), c->ctrl));
@@ -1556,19 +1557,21 @@ int gs3dc_train_step_batch(gs3dc_ctx* c, int n_views, const gs3d_camera* cams, c
     sh.VN = (long long)c->N * n_views;
     if (sh.VN >= (1LL << 31)) return fail(c, GS3DC_ERR_INVALID_ARG, "%lld (view, Gaussian) entries exceed 2^31", sh.VN);
     std::vector<unsigned> tile_base(n_views), pix_base(n_views);
-    unsigned long long tiles = 0, pix = 0;
+    unsigned long long tiles = 0, pix = 0, max_view_tiles = 0;
     for (int v = 0; v < n_views; v++) {
         const int gx = (cams[v].width + cfg->tile_w - 1) / cfg->tile_w, gy = (cams[v].height + cfg->tile_h - 1) / cfg->tile_h;
         tile_base[v] = (unsigned)tiles;
         pix_base[v] = (unsigned)pix;
         tiles += (unsigned long long)gx * gy;
+        max_view_tiles = std::max(max_view_tiles, (unsigned long long)gx * gy);
         pix += (unsigned long long)cams[v].width * cams[v].height;
     }
     if (tiles >= (1ull << 24) || pix >= (1ull << 31))
         return fail(c, GS3DC_ERR_INVALID_ARG, "the views' %llu tiles / %llu pixels exceed 2^24 / 2^31", tiles, pix);
     sh.tiles = (unsigned)tiles;
     sh.pix = pix;
-    sh.tile_digits = (bit_length(sh.tiles > 1 ? sh.tiles - 1 : 0u) + 7) / 8;
+    // the pairs are sorted on the views' local tile ids
+    sh.tile_digits = (bit_length(max_view_tiles > 1 ? (unsigned)(max_view_tiles - 1) : 0u) + 7) / 8;
     if ((rc = batch_buffers(c, sh))) return rc;
     if (c->keep_grads && (rc = ensure_grads(c))) return rc;
     const bool shape_new = b.cap == 0 || b.key[0] != c->N || b.key[1] != n_views || b.key[2] != (long long)sh.tiles ||

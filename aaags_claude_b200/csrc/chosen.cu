@@ -324,29 +324,7 @@ __global__ void __launch_bounds__(kCB) k_chosen_backward(const StepParams* __res
         __syncthreads();
     }
     // ---- phase 1: per-Gaussian adjoint (summed over the views) ----
-    BwdIn in;
-    float shf[48];
     if (tid < ng) {
-#pragma unroll
-        for (int k = 0; k < 3; k++) in.p[k] = sm.pos[3 * tid + k];
-        in.act = nullptr;
-        load_attr<S>(sm.attr, tid, in.rsc, &in.rop, in.rq);
-        if (mc3 == 48) {
-            // this Gaussian's 96 SH bytes as six 16-byte loads
-            const uint4* row = sm.sh + 6 * tid;
-#pragma unroll
-            for (int q = 0; q < 6; q++) {
-                const uint4 v = row[q];
-                const S* h = reinterpret_cast<const S*>(&v);
-#pragma unroll
-                for (int k = 0; k < 8; k++) shf[8 * q + k] = ldf(h[k]);
-            }
-        } else {
-            const S* shs = reinterpret_cast<const S*>(sm.sh) + mc3 * tid;
-#pragma unroll
-            for (int k = 0; k < 48; k++) shf[k] = k < mc3 ? ldf(shs[k]) : 0.f;
-        }
-        in.sh = shf;
 #pragma unroll
         for (int k = 0; k < 3; k++) sm.g_pos[3 * tid + k] = sm.g_sc[3 * tid + k] = 0.f;
 #pragma unroll
@@ -374,6 +352,7 @@ __global__ void __launch_bounds__(kCB) k_chosen_backward(const StepParams* __res
         }
         for (int e = tid; e < ng; e += kCB) rg.dop[e0 + e] = 0.f;
         if (tid < ng) {
+            BwdIn in;
 #pragma unroll
             for (int k = 0; k < 3; k++) {
                 in.dcn[k] = sm.dcon[3 * tid + k];
@@ -387,6 +366,28 @@ __global__ void __launch_bounds__(kCB) k_chosen_backward(const StepParams* __res
                              in.dcn[2] != 0.f || in.drgb[0] != 0.f || in.drgb[1] != 0.f || in.drgb[2] != 0.f ||
                              in.dop != 0.f;
             if (any) {
+                // parameters from shared memory, per view: nothing stays live across the view loop
+#pragma unroll
+                for (int k = 0; k < 3; k++) in.p[k] = sm.pos[3 * tid + k];
+                in.act = nullptr;
+                load_attr<S>(sm.attr, tid, in.rsc, &in.rop, in.rq);
+                float shf[48];
+                if (mc3 == 48) {
+                    // this Gaussian's 96 SH bytes as six 16-byte loads
+                    const uint4* row = sm.sh + 6 * tid;
+#pragma unroll
+                    for (int q = 0; q < 6; q++) {
+                        const uint4 vv = row[q];
+                        const S* h = reinterpret_cast<const S*>(&vv);
+#pragma unroll
+                        for (int k = 0; k < 8; k++) shf[8 * q + k] = ldf(h[k]);
+                    }
+                } else {
+                    const S* shs = reinterpret_cast<const S*>(sm.sh) + mc3 * tid;
+#pragma unroll
+                    for (int k = 0; k < 48; k++) shf[k] = k < mc3 ? ldf(shs[k]) : 0.f;
+                }
+                in.sh = shf;
                 BwdOut o;
 #pragma unroll
                 for (int k = 0; k < 3; k++) o.gp[k] = o.gs[k] = o.geff[k] = 0.f;

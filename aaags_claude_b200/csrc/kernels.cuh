@@ -148,8 +148,10 @@ cudaError_t launch_preprocess_plain(cudaStream_t st, const StepParams* sp, int N
 // xmax | ymax << 16) written by the reduced-storage preprocess; without them
 // the rectangle is recomputed from the stored mean and radius.
 // n_per_view > 0: several views; N counts (view, Gaussian) entries
-// view * n_per_view + i, and sp is the views' parameter array (the tile ids
-// emitted are global: the view's tile_base plus its local tile).
+// view * n_per_view + i, and sp is the views' parameter array.  The keys are
+// the views' local tile ids: the emission order groups the pairs by view, so a
+// stable sort on the local id leaves every (view, tile) run contiguous
+// (launch_tile_ranges_views).
 cudaError_t launch_emit_ranked(cudaStream_t st, const StepParams* sp, int N, const unsigned* rank_gid,
                                ScreenPtrs s, PairPtrs pr, Control* ctrl, const uint2* rects = nullptr,
                                int n_per_view = 0, int hist_slot = kDepthDigits);
@@ -198,6 +200,12 @@ cudaError_t launch_radix_sort32(cudaStream_t st, const StepParams* sp, int digit
                                 const unsigned long long* count = nullptr);
 cudaError_t launch_tile_ranges32(cudaStream_t st, unsigned long long capacity, const unsigned* tiles_sorted,
                                  unsigned* ranges, Control* ctrl);
+// Ranges of global tile ids (the view's tile_base + local id) over pairs
+// sorted stably by local tile id from a view-grouped emission: the view of a
+// pair is its value / n_per_view.
+cudaError_t launch_tile_ranges_views(cudaStream_t st, unsigned long long capacity, const unsigned* tiles_sorted,
+                                     const unsigned* vals_sorted, const StepParams* views, int n_per_view,
+                                     unsigned* ranges, Control* ctrl);
 
 // Heavy-first permutation of the tiles (by pair count) for the rasterisers.
 cudaError_t launch_tile_order(cudaStream_t st, const unsigned* ranges, int num_tiles, unsigned* order);

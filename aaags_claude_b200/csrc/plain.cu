@@ -240,10 +240,9 @@ __global__ void __launch_bounds__(kBlock) k_emit_ranked(const StepParams* __rest
     if (r < N) {
         g = rank_gid[r];
         if (n_per_view > 0) {
-            // several views: entry g = view * n_per_view + Gaussian, spp is the views' parameter array
-            const StepParams& vp = spp[g / (unsigned)n_per_view];
-            gx = vp.grid_x;
-            tbase = vp.tile_base;
+            // several views: entry g = view * n_per_view + Gaussian, spp is the views' parameter array;
+            // the key is the view's local tile id (the value tells the views apart)
+            gx = spp[g / (unsigned)n_per_view].grid_x;
         }
         cnt = s.tiles[g];
         if (cnt > 0) {

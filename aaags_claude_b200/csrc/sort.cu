@@ -178,6 +178,23 @@ __device__ __forceinline__ unsigned tile_of(unsigned key) { return key; }   // t
 // One thread per key (the grid covers the capacity): a tile's range starts
 // where its key differs from the previous one and ends where it differs
 // from the next.
+__device__ __forceinline__ unsigned global_tile(const unsigned* keys, const unsigned* vals, const StepParams* views,
+                                                unsigned n_per_view, unsigned long long i) {
+    return views[vals[i] / n_per_view].tile_base + keys[i];
+}
+
+// Ranges of (view, tile) runs: a run starts / ends where the global id changes.
+__global__ void k_ranges_views(const unsigned* __restrict__ keys, const unsigned* __restrict__ vals,
+                               const StepParams* __restrict__ views, unsigned n_per_view,
+                               unsigned long long capacity, unsigned* __restrict__ ranges, Control* ctrl) {
+    const unsigned long long P = min(ctrl->total_pairs, capacity);
+    const unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P) return;
+    const unsigned t = global_tile(keys, vals, views, n_per_view, i);
+    if (i == 0 || global_tile(keys, vals, views, n_per_view, i - 1) != t) ranges[2 * t] = (unsigned)i;
+    if (i == P - 1 || global_tile(keys, vals, views, n_per_view, i + 1) != t) ranges[2 * t + 1] = (unsigned)(i + 1);
+}
+
 template <typename K>
 __global__ void k_ranges(const K* __restrict__ keys, unsigned long long capacity, unsigned* __restrict__ ranges,
                          Control* ctrl) {
@@ -304,6 +321,15 @@ cudaError_t launch_tile_ranges(cudaStream_t st, unsigned long long capacity, con
                                unsigned* ranges, Control* ctrl) {
     if (capacity == 0) return cudaSuccess;
     k_ranges<<<(unsigned)((capacity + 255) / 256), 256, 0, st>>>(keys_sorted, capacity, ranges, ctrl);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tile_ranges_views(cudaStream_t st, unsigned long long capacity, const unsigned* tiles_sorted,
+                                     const unsigned* vals_sorted, const StepParams* views, int n_per_view,
+                                     unsigned* ranges, Control* ctrl) {
+    if (capacity == 0 || n_per_view <= 0) return cudaSuccess;
+    k_ranges_views<<<(unsigned)((capacity + 255) / 256), 256, 0, st>>>(tiles_sorted, vals_sorted, views,
+                                                                       (unsigned)n_per_view, capacity, ranges, ctrl);
     return cudaGetLastError();
 }
 
