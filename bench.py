@@ -59,6 +59,8 @@ def _args(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the timed reference CPU step")
     ap.add_argument("--gaussians", type=int, default=1_000_000, help="scene size (profiling cases use less)")
     ap.add_argument("--size", default="1920x1080", help="WxH of the camera")
+    ap.add_argument("--scene", choices=("random", "clustered"), default="random",
+                    help="clustered: 64 clusters (sigma 0.15) as in the mixed-precision configuration")
     ap.add_argument("--fused-adam", type=int, default=None, help="1: optimiser fused into the backward kernel")
     ap.add_argument("--sort", choices=("depth-first", "full-key"), default="depth-first",
                     help="pair ordering of the train step")
@@ -89,19 +91,21 @@ def _workload(a):
     """The training workload: 1M Gaussians at 1920x1080 unless --gaussians / --size shrink it."""
     from aaags_claude_b200 import scenes as S
     W, H = (int(x) for x in a.size.lower().split("x"))
-    if a.gaussians == 1_000_000 and (W, H) == (1920, 1080):
+    if a.gaussians == 1_000_000 and (W, H) == (1920, 1080) and a.scene == "random":
         w = S.config_train_1m_1080p()
+    elif a.gaussians == 3_000_000 and (W, H) == (1920, 1080) and a.scene == "clustered":
+        w = S.config_clustered_3m()
     else:
-        sc = S.random_scene(a.gaussians)
+        sc = S.random_scene(a.gaussians) if a.scene == "random" else S.clustered_scene(a.gaussians)
         cam = S.sphere_cameras(1, resolutions=[(W, H)])[0]
         w = S.Workload(f"train_{a.gaussians}_{W}x{H}", sc, [cam], S.perturbed(sc))
     return w, S.render_config(True), S.train_config()
 
 
 def _workload_name(a) -> str:
-    if a.gaussians == 1_000_000 and a.size == "1920x1080":
+    if a.gaussians == 1_000_000 and a.size == "1920x1080" and a.scene == "random":
         return WORKLOAD
-    return f"train_step_{a.gaussians}_gaussians_{a.size}_sh3_l1_adam"
+    return f"train_step_{a.gaussians}_{a.scene}_gaussians_{a.size}_sh3_l1_adam"
 
 
 # ---------------------------------------------------------------- clocks
