@@ -44,6 +44,9 @@ struct DevBuf {
 
 constexpr int kParamSlots = 4;  // pinned ring of per-step parameter blocks
 constexpr int kMaxBatchViews = 255;   // views per multi-view step (one 8-bit radix digit)
+constexpr int kTunePpt[3] = {1, 2, 4};   // autotuner candidates: pixels per thread of the rasterisers
+constexpr int kTuneReps = 2;             // timed steps per candidate
+constexpr int kTuneSteps = 3 * kTuneReps;
 
 }  // namespace
 
@@ -158,6 +161,20 @@ struct gs3dc_ctx {
         cudaGraphExec_t graph = nullptr;
         long long key[8] = {};
     } batch;
+    // rasteriser pixels per thread in use (set per step; 2 unless the autotuner chose otherwise)
+    int fwd_ppt = 2, bwd_ppt = 2;
+    // online autotuner (GS3DC_OPT_AUTOTUNE): per workload shape, the first kTuneSteps train steps
+    // cycle through the candidate pixels-per-thread and time both rasterisers; the fastest stay
+    struct Tune {
+        long long key[6] = {};
+        int trial = 0;
+        float fwd_ms[3] = {}, bwd_ms[3] = {};
+        int fwd_ppt = 2, bwd_ppt = 2;
+        bool done = false;
+    };
+    bool autotune = false;
+    Tune tune_single, tune_batch;
+    cudaEvent_t tune_ev[3] = {};
     // options / stats
     unsigned spin_limit = 1u << 22;
     long long kernels_last = 0;
@@ -470,6 +487,45 @@ int read_control(gs3dc_ctx* c) {
     return GS3DC_OK;
 }
 
+// ---- autotuner ----
+
+// The pixels per thread of this step: the tuned values, or the next
+// candidate while the workload shape is being tuned (returns true then).
+bool tune_begin(gs3dc_ctx* c, gs3dc_ctx::Tune& t, const long long key[6]) {
+    if (!c->autotune) {
+        c->fwd_ppt = c->bwd_ppt = 2;
+        return false;
+    }
+    if (std::memcmp(t.key, key, sizeof(t.key)) != 0) {
+        t = gs3dc_ctx::Tune();
+        std::memcpy(t.key, key, sizeof(t.key));
+    }
+    if (t.done) {
+        c->fwd_ppt = t.fwd_ppt;
+        c->bwd_ppt = t.bwd_ppt;
+        return false;
+    }
+    c->fwd_ppt = c->bwd_ppt = kTunePpt[t.trial / kTuneReps];
+    return true;
+}
+
+// Adds a trial's rasteriser times; after the last trial keeps the fastest.
+void tune_end(gs3dc_ctx* c, gs3dc_ctx::Tune& t, float fwd_ms, float bwd_ms) {
+    const int k = t.trial / kTuneReps;
+    t.fwd_ms[k] += fwd_ms;
+    t.bwd_ms[k] += bwd_ms;
+    if (++t.trial < kTuneSteps) return;
+    int bf = 0, bb = 0;
+    for (int i = 1; i < 3; i++) {
+        if (t.fwd_ms[i] < t.fwd_ms[bf]) bf = i;
+        if (t.bwd_ms[i] < t.bwd_ms[bb]) bb = i;
+    }
+    t.fwd_ppt = kTunePpt[bf];
+    t.bwd_ppt = kTunePpt[bb];
+    t.done = true;
+    drop_graphs(c);   // the next step captures the chosen kernels
+}
+
 // ---- launch sequences ----
 
 size_t ctrl_bytes_for(int N) {
@@ -584,10 +640,10 @@ int seq_back_chosen(gs3dc_ctx* c) {
     const int w = c->sorted_which;
     if ((rc = mark(c, GS3DC_STAGE_RASTER_FWD))) return rc;
     CK(launch_raster_fwd_fast(c->stream, c->sp_dev, c->num_tiles, c->ranges.p, c->tile_order.p, c->vals[w].p,
-                              screen_ptrs(c, false), pixel_ptrs(c), c->ctrl));
+                              screen_ptrs(c, false), pixel_ptrs(c), c->ctrl, c->fwd_ppt));
     if ((rc = mark(c, GS3DC_STAGE_RASTER_BWD))) return rc;
     CK(launch_raster_bwd_fast(c->stream, c->sp_dev, c->num_tiles, c->ranges.p, c->tile_order.p, c->vals[w].p,
-                              screen_ptrs(c, false), pixel_ptrs(c), rgrad_ptrs(c), c->ctrl));
+                              screen_ptrs(c, false), pixel_ptrs(c), rgrad_ptrs(c), c->ctrl, c->bwd_ppt));
     if ((rc = mark(c, GS3DC_STAGE_PREPROCESS_BWD))) return rc;
     CK(launch_chosen_backward_adam(c->stream, c->sp_dev, c->N, c->max_coeffs * 3, c->form == GS3DC_FORM_FP16,
                                    chosen_ptrs(c), rgrad_ptrs(c),
@@ -618,10 +674,10 @@ int seq_train_back(gs3dc_ctx* c) {
     const int w = c->sorted_which;
     if ((rc = mark(c, GS3DC_STAGE_RASTER_FWD))) return rc;
     CK(launch_raster_fwd_plain(c->stream, c->sp_dev, c->num_tiles, true, c->ranges.p, c->tile_order.p, c->vals[w].p,
-                               screen_ptrs(c, false), pixel_ptrs(c), c->ctrl));
+                               screen_ptrs(c, false), pixel_ptrs(c), c->ctrl, c->fwd_ppt));
     if ((rc = mark(c, GS3DC_STAGE_RASTER_BWD))) return rc;
     CK(launch_raster_bwd_plain(c->stream, c->sp_dev, c->num_tiles, true, c->ranges.p, c->tile_order.p, c->vals[w].p,
-                               screen_ptrs(c, false), pixel_ptrs(c), rgrad_ptrs(c), c->ctrl));
+                               screen_ptrs(c, false), pixel_ptrs(c), rgrad_ptrs(c), c->ctrl, c->bwd_ppt));
     if ((rc = mark(c, GS3DC_STAGE_PREPROCESS_BWD))) return rc;
     if (c->fused_adam && !c->keep_grads) {
         CK(launch_preprocess_bwd_plain(c->stream, c->sp_dev, c->N, c->max_coeffs * 3, 1, model_ptrs(c),
@@ -822,10 +878,14 @@ int seq_batch(gs3dc_ctx* c, const BatchShape& sh) {
     CK(launch_tile_ranges_views(c->stream, b.cap, b.keys[which].p, b.vals[which].p, views, c->N, b.ranges.p,
                                 c->ctrl));
     CK(launch_tile_order(c->stream, b.ranges.p, (int)sh.tiles, b.order.p));
+    const bool tuning = c->autotune && !c->tune_batch.done;
+    if (tuning) CK(cudaEventRecord(c->tune_ev[0], c->stream));
     CK(launch_raster_fwd_fast_multi(c->stream, views, sh.V, sh.tiles, b.ranges.p, b.order.p, b.vals[which].p,
-                                    batch_screen(c), batch_pixels(c), c->ctrl));
+                                    batch_screen(c), batch_pixels(c), c->ctrl, c->fwd_ppt));
+    if (tuning) CK(cudaEventRecord(c->tune_ev[1], c->stream));
     CK(launch_raster_bwd_fast_multi(c->stream, views, sh.V, sh.tiles, b.ranges.p, b.order.p, b.vals[which].p,
-                                    batch_screen(c), batch_pixels(c), batch_rgrads(c), c->ctrl));
+                                    batch_screen(c), batch_pixels(c), batch_rgrads(c), c->ctrl, c->bwd_ppt));
+    if (tuning) CK(cudaEventRecord(c->tune_ev[2], c->stream));
     CK(launch_chosen_backward_adam(c->stream, views, c->N, c->max_coeffs * 3, c->form == GS3DC_FORM_FP16,
                                    chosen_ptrs(c), batch_rgrads(c),
                                    c->keep_grads ? grad_ptrs(c) : GradPtrs{nullptr, nullptr, nullptr, nullptr, nullptr},
@@ -873,6 +933,8 @@ int gs3dc_create(int device, gs3dc_ctx** out) {
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(GS3DC_ERR_CUDA);
     if (cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking) != cudaSuccess) return bail(GS3DC_ERR_CUDA);
     if (cudaEventCreateWithFlags(&c->ev_gt_ready, cudaEventDisableTiming) != cudaSuccess) return bail(GS3DC_ERR_CUDA);
+    for (int k = 0; k < 3; k++)
+        if (cudaEventCreate(&c->tune_ev[k]) != cudaSuccess) return bail(GS3DC_ERR_CUDA);
     for (int b = 0; b < 2; b++)
         if (cudaEventCreateWithFlags(&c->ev_gt_free[b], cudaEventDisableTiming) != cudaSuccess)
             return bail(GS3DC_ERR_CUDA);
@@ -935,6 +997,8 @@ void gs3dc_destroy(gs3dc_ctx* c) {
     if (c->batch.views_event) cudaEventDestroy(c->batch.views_event);
     if (c->batch.views_host) cudaFreeHost(c->batch.views_host);
     if (c->ev_gt_ready) cudaEventDestroy(c->ev_gt_ready);
+    for (int k = 0; k < 3; k++)
+        if (c->tune_ev[k]) cudaEventDestroy(c->tune_ev[k]);
     for (int b = 0; b < 2; b++)
         if (c->ev_gt_free[b]) cudaEventDestroy(c->ev_gt_free[b]);
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
@@ -988,6 +1052,12 @@ int gs3dc_set_option(gs3dc_ctx* c, int option, int64_t value) {
         case GS3DC_OPT_STAGE_TIMING:
             c->stage_timing = value != 0;
             return GS3DC_OK;
+        case GS3DC_OPT_AUTOTUNE:
+            c->autotune = value != 0;
+            c->tune_single = gs3dc_ctx::Tune();
+            c->tune_batch = gs3dc_ctx::Tune();
+            drop_graphs(c);
+            return GS3DC_OK;
         case GS3DC_OPT_KEEP_GRADIENTS:
             c->keep_grads = value != 0;
             drop_graphs(c);
@@ -1006,6 +1076,8 @@ int gs3dc_get_stat(gs3dc_ctx* c, int stat, int64_t* value) {
     if (!c || !value) return GS3DC_ERR_INVALID_ARG;
     switch (stat) {
         case GS3DC_STAT_TOTAL_PAIRS: *value = (int64_t)c->last_pairs; return GS3DC_OK;
+        case GS3DC_STAT_FWD_PPT: *value = c->fwd_ppt; return GS3DC_OK;
+        case GS3DC_STAT_BWD_PPT: *value = c->bwd_ppt; return GS3DC_OK;
         case GS3DC_STAT_PAIR_CAPACITY: *value = (int64_t)c->cap; return GS3DC_OK;
         case GS3DC_STAT_KERNELS_LAST: *value = c->kernels_last; return GS3DC_OK;
         case GS3DC_STAT_SORT_PASSES: *value = c->sort_passes; return GS3DC_OK;
@@ -1462,12 +1534,22 @@ int gs3dc_train_step(gs3dc_ctx* c, const gs3d_camera* cam, const float* gt, int 
         if ((rc = ensure_pairs(c, guess > c->cap ? guess : c->cap, c->num_tiles))) return rc;
     }
     const int step_before = c->adam_step;
+    const long long tkey[6] = {c->N, cam->width, cam->height, c->form, c->sort_mode, c->fused_adam ? 1 : 0};
+    const bool tuning = tune_begin(c, c->tune_single, tkey);
+    const bool user_timing = c->stage_timing;
+    if (tuning) c->stage_timing = true;   // the trial step runs un-captured with events between stages
+    struct RestoreTiming {
+        gs3dc_ctx* c;
+        bool v;
+        ~RestoreTiming() { c->stage_timing = v; }
+    } restore_timing{c, user_timing};
     for (int attempt = 0; attempt < 3; attempt++) {
         c->adam_step = step_before + (tc->use_adam ? 1 : 0);
         if ((rc = push_params(c, cam, cfg, tc, iteration, gt_dev))) return rc;
         const long long key[8] = {c->N, c->max_coeffs, cam->width, cam->height, (long long)c->cap, c->sort_passes,
                                   (long long)c->spin_limit,
-                                  (c->fused_adam ? 1 : 2) + 4 * c->sort_mode + 16 * c->form + 64 * (c->keep_grads ? 1 : 0)};
+                                  (c->fused_adam ? 1 : 2) + 4 * c->sort_mode + 16 * c->form + 64 * (c->keep_grads ? 1 : 0) +
+                                      128 * c->fwd_ppt + 1024 * c->bwd_ppt};
         const bool key_ok = c->graph && std::memcmp(key, c->graph_key, sizeof(key)) == 0;
         c->kernels_last = 0;
         if (c->use_graph && !c->stage_timing && !first && attempt == 0) {
@@ -1533,6 +1615,8 @@ int gs3dc_train_step(gs3dc_ctx* c, const gs3d_camera* cam, const float* gt, int 
             for (int k = 0; k < GS3DC_NUM_STAGES; k++)
                 CK(cudaEventElapsedTime(&c->stage_ms[k], c->stage_ev[k], c->stage_ev[k + 1]));
         }
+        if (tuning)
+            tune_end(c, c->tune_single, c->stage_ms[GS3DC_STAGE_RASTER_FWD], c->stage_ms[GS3DC_STAGE_RASTER_BWD]);
         return GS3DC_OK;
     }
     c->adam_step = step_before;
@@ -1589,6 +1673,8 @@ int gs3dc_train_step_batch(gs3dc_ctx* c, int n_views, const gs3d_camera* cams, c
     }
     bool first = shape_new;
     const int step_before = c->adam_step;
+    const long long tkey[6] = {c->N, n_views, (long long)sh.tiles, (long long)sh.pix, c->form, 1};
+    const bool tuning = tune_begin(c, c->tune_batch, tkey);
     for (int attempt = 0; attempt < 3; attempt++) {
         c->adam_step = step_before + (tc->use_adam ? 1 : 0);
         CK(cudaEventSynchronize(b.views_event));   // the staging's previous copy has been consumed
@@ -1605,8 +1691,9 @@ int gs3dc_train_step_batch(gs3dc_ctx* c, int n_views, const gs3d_camera* cams, c
                            c->stream));
         CK(cudaEventRecord(b.views_event, c->stream));
         const long long key[8] = {c->N, n_views, (long long)sh.tiles, (long long)sh.pix, (long long)b.cap,
-                                  c->form, (long long)c->spin_limit, c->max_coeffs + 1000 * (c->keep_grads ? 1 : 0)};
-        if (c->use_graph && !first && attempt == 0) {
+                                  c->form, (long long)c->spin_limit,
+                                  c->max_coeffs + 1000 * (c->keep_grads ? 1 : 0) + 2000 * c->fwd_ppt + 20000 * c->bwd_ppt};
+        if (c->use_graph && !first && !tuning && attempt == 0) {
             if (!b.graph || std::memcmp(key, b.key, sizeof(key)) != 0) {
                 if (b.graph) cudaGraphExecDestroy(b.graph);
                 b.graph = nullptr;
@@ -1626,7 +1713,7 @@ int gs3dc_train_step_batch(gs3dc_ctx* c, int n_views, const gs3d_camera* cams, c
         }
         std::memcpy(b.key, key, sizeof(key));
         c->have_step_grads = c->keep_grads;
-        if (!loss && !first) {
+        if (!loss && !first && !tuning) {
             c->pending_check = true;   // overflow is reported by the next synchronising call
             return GS3DC_OK;
         }
@@ -1644,6 +1731,12 @@ int gs3dc_train_step_batch(gs3dc_ctx* c, int n_views, const gs3d_camera* cams, c
             continue;
         }
         if (loss) *loss = (float)c->ctrl_host->loss_sum;
+        if (tuning) {
+            float f = 0.f, bw = 0.f;
+            CK(cudaEventElapsedTime(&f, c->tune_ev[0], c->tune_ev[1]));
+            CK(cudaEventElapsedTime(&bw, c->tune_ev[1], c->tune_ev[2]));
+            tune_end(c, c->tune_batch, f, bw);
+        }
         c->have_screen = c->have_pairs = c->have_sorted = c->have_raster = c->have_rgrad = c->have_grads = false;
         return GS3DC_OK;
     }

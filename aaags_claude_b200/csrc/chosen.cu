@@ -514,21 +514,44 @@ cudaError_t launch_chosen_preprocess(cudaStream_t st, const StepParams* sp, int 
     return cudaGetLastError();
 }
 
+namespace {
+template <int PPT>
+cudaError_t fwd_multi(cudaStream_t st, const StepParams* views, int n_views, unsigned n_tiles,
+                      const unsigned* ranges, const unsigned* order, const unsigned* vals, ScreenPtrs s, PixelPtrs px,
+                      Control* ctrl) {
+    static int per_sm = 0;
+    if (!per_sm) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_raster_fwd<true, FastBlend, true, PPT>, 256 / PPT,
+                                                          0) != cudaSuccess ||
+            per_sm < 1)
+            per_sm = 1;
+    }
+    k_raster_fwd<true, FastBlend, true, PPT><<<per_sm * 148, 256 / PPT, 0, st>>>(views, ranges, order, vals, s, px,
+                                                                                ctrl, n_views, n_tiles);
+    return cudaGetLastError();
+}
+}  // namespace
+
 cudaError_t launch_raster_fwd_fast_multi(cudaStream_t st, const StepParams* views, int n_views, unsigned n_tiles,
                                          const unsigned* ranges, const unsigned* order, const unsigned* vals,
-                                         ScreenPtrs s, PixelPtrs px, Control* ctrl) {
+                                         ScreenPtrs s, PixelPtrs px, Control* ctrl, int ppt) {
     if (n_tiles == 0) return cudaSuccess;
-    // persistent: as many CTAs as fit resident (9 per SM at this kernel's registers)
-    k_raster_fwd<true, FastBlend, true><<<9 * 148, kFwdThreads, 0, st>>>(views, ranges, order, vals, s, px, ctrl,
-                                                                       n_views, n_tiles);
-    return cudaGetLastError();
+    // persistent: as many CTAs as fit resident
+    if (ppt == 1) return fwd_multi<1>(st, views, n_views, n_tiles, ranges, order, vals, s, px, ctrl);
+    if (ppt == 4) return fwd_multi<4>(st, views, n_views, n_tiles, ranges, order, vals, s, px, ctrl);
+    return fwd_multi<2>(st, views, n_views, n_tiles, ranges, order, vals, s, px, ctrl);
 }
 
 cudaError_t launch_raster_fwd_fast(cudaStream_t st, const StepParams* sp, int num_tiles, const unsigned* ranges,
                                    const unsigned* order, const unsigned* vals, ScreenPtrs s, PixelPtrs px,
-                                   Control* ctrl) {
+                                   Control* ctrl, int ppt) {
     if (num_tiles <= 0) return cudaSuccess;
-    k_raster_fwd<true, FastBlend><<<num_tiles, kFwdThreads, 0, st>>>(sp, ranges, order, vals, s, px, ctrl);
+    if (ppt == 1)
+        k_raster_fwd<true, FastBlend, false, 1><<<num_tiles, 256, 0, st>>>(sp, ranges, order, vals, s, px, ctrl);
+    else if (ppt == 4)
+        k_raster_fwd<true, FastBlend, false, 4><<<num_tiles, 64, 0, st>>>(sp, ranges, order, vals, s, px, ctrl);
+    else
+        k_raster_fwd<true, FastBlend, false, 2><<<num_tiles, 128, 0, st>>>(sp, ranges, order, vals, s, px, ctrl);
     return cudaGetLastError();
 }
 

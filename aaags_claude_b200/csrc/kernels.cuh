@@ -113,19 +113,19 @@ cudaError_t launch_chosen_preprocess(cudaStream_t st, const StepParams* sp, int 
 // Forward rasteriser with the fast-exp blend decision and fused L1.
 cudaError_t launch_raster_fwd_fast(cudaStream_t st, const StepParams* sp, int num_tiles, const unsigned* ranges,
                                    const unsigned* order, const unsigned* vals, ScreenPtrs s, PixelPtrs px,
-                                   Control* ctrl);
+                                   Control* ctrl, int ppt = 2);
 // One persistent launch over all tiles of n_views views (views = their
 // parameter array, order = all global tiles, heavy first).
 cudaError_t launch_raster_fwd_fast_multi(cudaStream_t st, const StepParams* views, int n_views, unsigned n_tiles,
                                          const unsigned* ranges, const unsigned* order, const unsigned* vals,
-                                         ScreenPtrs s, PixelPtrs px, Control* ctrl);
+                                         ScreenPtrs s, PixelPtrs px, Control* ctrl, int ppt = 2);
 cudaError_t launch_raster_bwd_fast_multi(cudaStream_t st, const StepParams* views, int n_views, unsigned n_tiles,
                                          const unsigned* ranges, const unsigned* order, const unsigned* vals,
-                                         ScreenPtrs s, PixelPtrs px, RGradPtrs g, Control* ctrl);
+                                         ScreenPtrs s, PixelPtrs px, RGradPtrs g, Control* ctrl, int ppt = 2);
 // Backward rasteriser deciding acceptance like launch_raster_fwd_fast.
 cudaError_t launch_raster_bwd_fast(cudaStream_t st, const StepParams* sp, int num_tiles, const unsigned* ranges,
                                    const unsigned* order, const unsigned* vals, ScreenPtrs s, PixelPtrs px,
-                                   RGradPtrs g, Control* ctrl);
+                                   RGradPtrs g, Control* ctrl, int ppt = 2);
 // Per-Gaussian adjoint fused with Adam (stochastic rounding into the 16-bit
 // parameters and BF16 moments); zeroes the screen-gradient accumulators.
 // With g.g_pos != NULL the FP32 raw-parameter gradients are stored too.
@@ -135,6 +135,9 @@ cudaError_t launch_chosen_backward_adam(cudaStream_t st, const StepParams* sp, i
                                         ChosenPtrs c, RGradPtrs rg, GradPtrs gout, Control* ctrl, int n_views = 1);
 
 // ---- plain FP32 kernels (plain.cu, compiled without FMA contraction) ----
+// The rasterisers' ppt (pixels per thread: 1, 2 or 4) sets 256 / ppt threads
+// per 16x16 tile; the results do not depend on it (the backward's FP32 sums
+// only change order).
 // Preprocess; emits the pairs in Gaussian order, or -- when dk.keys != NULL --
 // writes the depth-sort input instead (pairs come from launch_emit_ranked).
 cudaError_t launch_preprocess_plain(cudaStream_t st, const StepParams* sp, int N, bool train,
@@ -161,10 +164,10 @@ cudaError_t launch_export_screen(cudaStream_t st, int N, ScreenPtrs s, ScreenArr
 // order: tile permutation (heavy first) or NULL for row-major
 cudaError_t launch_raster_fwd_plain(cudaStream_t st, const StepParams* sp, int num_tiles, bool fused_loss,
                                     const unsigned* ranges, const unsigned* order, const unsigned* vals,
-                                    ScreenPtrs s, PixelPtrs px, Control* ctrl);
+                                    ScreenPtrs s, PixelPtrs px, Control* ctrl, int ppt = 2);
 cudaError_t launch_raster_bwd_plain(cudaStream_t st, const StepParams* sp, int num_tiles, bool from_sign,
                                     const unsigned* ranges, const unsigned* order, const unsigned* vals,
-                                    ScreenPtrs s, PixelPtrs px, RGradPtrs g, Control* ctrl);
+                                    ScreenPtrs s, PixelPtrs px, RGradPtrs g, Control* ctrl, int ppt = 2);
 // mode: 0 = write GradientOutput (stage API), 1 = fused optimiser, 2 = write
 // GradientOutput for a following launch_optimizer_plain and zero the screen
 // gradient accumulators (split train step).  mc3 in {3, 12, 27, 48}.

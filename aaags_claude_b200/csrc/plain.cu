@@ -696,12 +696,20 @@ cudaError_t launch_export_screen(cudaStream_t st, int N, ScreenPtrs s, ScreenArr
 
 cudaError_t launch_raster_fwd_plain(cudaStream_t st, const StepParams* sp, int num_tiles, bool fused_loss,
                                     const unsigned* ranges, const unsigned* order, const unsigned* vals,
-                                    ScreenPtrs s, PixelPtrs px, Control* ctrl) {
+                                    ScreenPtrs s, PixelPtrs px, Control* ctrl, int ppt) {
     if (num_tiles <= 0) return cudaSuccess;
-    if (fused_loss)
-        k_raster_fwd<true, ExactBlend><<<num_tiles, kFwdThreads, 0, st>>>(sp, ranges, order, vals, s, px, ctrl);
-    else
-        k_raster_fwd<false, ExactBlend><<<num_tiles, kFwdThreads, 0, st>>>(sp, ranges, order, vals, s, px, ctrl);
+#define GS3D_FWD(FL, P) \
+    k_raster_fwd<FL, ExactBlend, false, P><<<num_tiles, 256 / P, 0, st>>>(sp, ranges, order, vals, s, px, ctrl)
+    if (fused_loss) {
+        if (ppt == 1) GS3D_FWD(true, 1);
+        else if (ppt == 4) GS3D_FWD(true, 4);
+        else GS3D_FWD(true, 2);
+    } else {
+        if (ppt == 1) GS3D_FWD(false, 1);
+        else if (ppt == 4) GS3D_FWD(false, 4);
+        else GS3D_FWD(false, 2);
+    }
+#undef GS3D_FWD
     return cudaGetLastError();
 }
 

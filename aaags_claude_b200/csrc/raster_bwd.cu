@@ -55,14 +55,13 @@ struct FastAccept {
 
 // Rasterizer backward (rasterizer_backward_cpu.cpp:20-133): back-to-front
 // over each pixel's contributors, transmittance recovered by division from
-// T_final instead of a replayed per-pixel list.  One CTA of 128 threads per
-// 16x16 tile, two pixels per thread: warp w owns the 16x4 strip of rows
-// 4w..4w+3, a thread the pixels (x, 4w + lane/16) and (x, 4w + 2 + lane/16).
-// Per Gaussian of a batch a thread adds its two pixels' contributions, the
-// warp sums its 64 pixels with warp_sum8 + warp_sum, the 4 warps meet in
+// T_final instead of a replayed per-pixel list.  One CTA of 256 / PPT threads
+// per 16x16 tile, PPT pixels per thread: warp w owns the strip of rows
+// 2*PPT*w .. 2*PPT*w + 2*PPT - 1, a thread the pixels (x, 2*PPT*w + lane/16 + 2p).
+// Per Gaussian of a batch a thread adds its pixels' contributions, the warp
+// sums its 32 * PPT pixels with warp_sum8 + warp_sum, the warps meet in
 // shared-memory accumulators and each Gaussian gets one set of global atomics
-// per tile.
-constexpr int kBwdThreads = 128;
+// per tile.  PPT = 2 by default; the autotuner may pick 1 or 4.
 constexpr int kBwdBatch = 256;
 
 //
@@ -70,8 +69,8 @@ constexpr int kBwdBatch = 256;
 // parameters); a CTA takes the next entry of `order` from a work counter and
 // renders the tile with its view's camera and pixel slice.  The screen
 // gradients then belong to (view, Gaussian) entries: vals holds view * N + i.
-template <bool FROM_SIGN, class Accept, bool MULTI = false>
-__global__ void __launch_bounds__(kBwdThreads) k_raster_bwd(const StepParams* __restrict__ spp,
+template <bool FROM_SIGN, class Accept, bool MULTI = false, int PPT = 2>
+__global__ void __launch_bounds__(256 / PPT) k_raster_bwd(const StepParams* __restrict__ spp,
                                                             const unsigned* __restrict__ ranges,
                                                             const unsigned* __restrict__ order,
                                                             const unsigned* __restrict__ vals, ScreenPtrs s,
@@ -86,6 +85,7 @@ __global__ void __launch_bounds__(kBwdThreads) k_raster_bwd(const StepParams* __
     __shared__ float s_acc[9][kBwdBatch];   // r, g, b, opacity, mean.x, mean.y, conic a, b, c
     __shared__ unsigned s_maxlast;
     __shared__ unsigned s_next;
+    constexpr int kBwdThreads = 256 / PPT;
     if (FROM_SIGN && ((ctrl->status & kStatusOverflow) || spp->persist->sticky_overflow)) return;
     for (int iter = 0;; iter++) {
     int tile;
@@ -116,13 +116,13 @@ __global__ void __launch_bounds__(kBwdThreads) k_raster_bwd(const StepParams* __
     const int tx = ltile % sp.grid_x, ty = ltile / sp.grid_x;
     const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int x = tx * kTile + (int)(lane & 15);
-    const int ybase = ty * kTile + 4 * (int)warp + (int)(lane >> 4);
+    const int ybase = ty * kTile + 2 * PPT * (int)warp + (int)(lane >> 4);
     const unsigned rs = ranges[2 * tile];
     const float fx = (float)x;
-    float fy[2], T[2], dC[2][3], acc[2][3];
-    unsigned last[2];
+    float fy[PPT], T[PPT], dC[PPT][3], acc[PPT][3];
+    unsigned last[PPT];
 #pragma unroll
-    for (int p = 0; p < 2; p++) {
+    for (int p = 0; p < PPT; p++) {
         const int y = ybase + 2 * p;
         fy[p] = (float)y;
         T[p] = 0.0f;
@@ -149,14 +149,16 @@ __global__ void __launch_bounds__(kBwdThreads) k_raster_bwd(const StepParams* __
     }
     if (threadIdx.x == 0) s_maxlast = 0;
     __syncthreads();
-    const unsigned mylast = max(last[0], last[1]);
+    unsigned mylast = 0;
+#pragma unroll
+    for (int p = 0; p < PPT; p++) mylast = max(mylast, last[p]);
     if (mylast) atomicMax(&s_maxlast, mylast);
     __syncthreads();
     const unsigned maxlast = s_maxlast;
     if (maxlast <= rs) continue;   // uniform: nothing of this tile contributed
     const unsigned wlast = __reduce_max_sync(0xffffffffu, mylast);
     const float wx0 = (float)(tx * kTile), wx1 = wx0 + (float)(kTile - 1);
-    const float wy0 = (float)(ty * kTile + 4 * (int)warp), wy1 = wy0 + 3.0f;
+    const float wy0 = (float)(ty * kTile + 2 * PPT * (int)warp), wy1 = wy0 + (float)(2 * PPT - 1);
     // batches [bs, be) walked from the back; the first one ends at maxlast
     for (unsigned be = maxlast; be > rs;) {
         const unsigned bs = (be - rs > (unsigned)kBwdBatch) ? be - kBwdBatch : rs;
@@ -192,7 +194,7 @@ __global__ void __launch_bounds__(kBwdThreads) k_raster_bwd(const StepParams* __
             float gv[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
             float g_cc = 0.f;
 #pragma unroll
-            for (int p = 0; p < 2; p++) {
+            for (int p = 0; p < PPT; p++) {
                 if (jj < last[p]) {
                     const float dx = a.x - fx, dy = a.y - fy[p];
                     const float power = power_rn(a, c, dx, dy);
@@ -256,33 +258,65 @@ __global__ void __launch_bounds__(kBwdThreads) k_raster_bwd(const StepParams* __
 
 }  // namespace
 
+namespace {
+
+// Resident CTAs per SM of a kernel at its block size (persistent launches).
+template <class F>
+int resident_ctas(F kernel, int threads) {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, 0) != cudaSuccess || n < 1) n = 1;
+    return n;
+}
+
+template <bool FROM_SIGN, class Accept, int PPT>
+cudaError_t bwd_single(cudaStream_t st, const StepParams* sp, int num_tiles, const unsigned* ranges,
+                       const unsigned* order, const unsigned* vals, ScreenPtrs s, PixelPtrs px, RGradPtrs g,
+                       Control* ctrl) {
+    k_raster_bwd<FROM_SIGN, Accept, false, PPT><<<num_tiles, 256 / PPT, 0, st>>>(sp, ranges, order, vals, s, px, g,
+                                                                                ctrl);
+    return cudaGetLastError();
+}
+
+template <int PPT>
+cudaError_t bwd_multi(cudaStream_t st, const StepParams* views, int n_views, unsigned n_tiles,
+                      const unsigned* ranges, const unsigned* order, const unsigned* vals, ScreenPtrs s, PixelPtrs px,
+                      RGradPtrs g, Control* ctrl) {
+    static int per_sm = 0;
+    if (!per_sm) per_sm = resident_ctas(k_raster_bwd<true, FastAccept, true, PPT>, 256 / PPT);
+    k_raster_bwd<true, FastAccept, true, PPT><<<per_sm * 148, 256 / PPT, 0, st>>>(views, ranges, order, vals, s, px,
+                                                                                 g, ctrl, n_views, n_tiles);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
 cudaError_t launch_raster_bwd_plain(cudaStream_t st, const StepParams* sp, int num_tiles, bool from_sign,
                                     const unsigned* ranges, const unsigned* order, const unsigned* vals,
-                                    ScreenPtrs s, PixelPtrs px, RGradPtrs g, Control* ctrl) {
+                                    ScreenPtrs s, PixelPtrs px, RGradPtrs g, Control* ctrl, int ppt) {
     if (num_tiles <= 0) return cudaSuccess;
-    if (from_sign)
-        k_raster_bwd<true, PlainAccept><<<num_tiles, kBwdThreads, 0, st>>>(sp, ranges, order, vals, s, px, g, ctrl);
-    else
-        k_raster_bwd<false, PlainAccept><<<num_tiles, kBwdThreads, 0, st>>>(sp, ranges, order, vals, s, px, g, ctrl);
-    return cudaGetLastError();
+#define GS3D_BWD(FS, P) bwd_single<FS, PlainAccept, P>(st, sp, num_tiles, ranges, order, vals, s, px, g, ctrl)
+    if (from_sign) return ppt == 1 ? GS3D_BWD(true, 1) : ppt == 4 ? GS3D_BWD(true, 4) : GS3D_BWD(true, 2);
+    return ppt == 1 ? GS3D_BWD(false, 1) : ppt == 4 ? GS3D_BWD(false, 4) : GS3D_BWD(false, 2);
+#undef GS3D_BWD
 }
 
 cudaError_t launch_raster_bwd_fast(cudaStream_t st, const StepParams* sp, int num_tiles, const unsigned* ranges,
                                    const unsigned* order, const unsigned* vals, ScreenPtrs s, PixelPtrs px,
-                                   RGradPtrs g, Control* ctrl) {
+                                   RGradPtrs g, Control* ctrl, int ppt) {
     if (num_tiles <= 0) return cudaSuccess;
-    k_raster_bwd<true, FastAccept><<<num_tiles, kBwdThreads, 0, st>>>(sp, ranges, order, vals, s, px, g, ctrl);
-    return cudaGetLastError();
+#define GS3D_BWD(P) bwd_single<true, FastAccept, P>(st, sp, num_tiles, ranges, order, vals, s, px, g, ctrl)
+    return ppt == 1 ? GS3D_BWD(1) : ppt == 4 ? GS3D_BWD(4) : GS3D_BWD(2);
+#undef GS3D_BWD
 }
 
 cudaError_t launch_raster_bwd_fast_multi(cudaStream_t st, const StepParams* views, int n_views, unsigned n_tiles,
                                          const unsigned* ranges, const unsigned* order, const unsigned* vals,
-                                         ScreenPtrs s, PixelPtrs px, RGradPtrs g, Control* ctrl) {
+                                         ScreenPtrs s, PixelPtrs px, RGradPtrs g, Control* ctrl, int ppt) {
     if (n_tiles == 0) return cudaSuccess;
-    // persistent: as many CTAs as fit resident (6 per SM at this kernel's registers)
-    k_raster_bwd<true, FastAccept, true><<<6 * 148, kBwdThreads, 0, st>>>(views, ranges, order, vals, s, px, g, ctrl,
-                                                                        n_views, n_tiles);
-    return cudaGetLastError();
+    // persistent: as many CTAs as fit resident
+#define GS3D_BWD(P) bwd_multi<P>(st, views, n_views, n_tiles, ranges, order, vals, s, px, g, ctrl)
+    return ppt == 1 ? GS3D_BWD(1) : ppt == 4 ? GS3D_BWD(4) : GS3D_BWD(2);
+#undef GS3D_BWD
 }
 
 }  // namespace gs3d

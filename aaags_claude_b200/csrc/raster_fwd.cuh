@@ -21,7 +21,9 @@ namespace {
 // memory; a warp skips a Gaussian whose skip box misses its strip; the CTA
 // stops once every pixel saturated.  Optional fused L1 (sign byte per pixel,
 // double-precision loss sum).
-constexpr int kFwdThreads = 128;
+//
+// PPT (pixels per thread: 1, 2 or 4) sets the threads per tile (256 / PPT)
+// and each warp's strip (16 x 2*PPT rows); the results do not depend on it.
 constexpr int kFwdBatch = 256;
 
 //
@@ -31,8 +33,8 @@ constexpr int kFwdBatch = 256;
 // by its global id and renders it with that view's camera into the view's
 // slice of the concatenated pixel buffers.  The fused loss adds each view's
 // sum weighted by its inv_n.
-template <bool FUSED_LOSS, class Blend, bool MULTI = false>
-__global__ void __launch_bounds__(kFwdThreads) k_raster_fwd(const StepParams* __restrict__ spp,
+template <bool FUSED_LOSS, class Blend, bool MULTI = false, int PPT = 2>
+__global__ void __launch_bounds__(256 / PPT) k_raster_fwd(const StepParams* __restrict__ spp,
                                                             const unsigned* __restrict__ ranges,
                                                             const unsigned* __restrict__ order,
                                                             const unsigned* __restrict__ vals, ScreenPtrs s,
@@ -43,6 +45,7 @@ __global__ void __launch_bounds__(kFwdThreads) k_raster_fwd(const StepParams* __
     __shared__ float s_b[kFwdBatch];
     __shared__ float s_thr[kFwdBatch];
     __shared__ float4 s_box[kFwdBatch];
+    constexpr int kFwdThreads = 256 / PPT;
     __shared__ double s_loss[kFwdThreads / 32];
     __shared__ unsigned s_next;
     for (int iter = 0;; iter++) {
@@ -74,17 +77,17 @@ __global__ void __launch_bounds__(kFwdThreads) k_raster_fwd(const StepParams* __
     const int tx = ltile % sp.grid_x, ty = ltile / sp.grid_x;
     const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int x = tx * kTile + (int)(lane & 15);
-    const int ybase = ty * kTile + 4 * (int)warp + (int)(lane >> 4);
+    const int ybase = ty * kTile + 2 * PPT * (int)warp + (int)(lane >> 4);
     const unsigned rs = ranges[2 * tile], re = ranges[2 * tile + 1];
     const float fx = (float)x;
     const float wx0 = (float)(tx * kTile), wx1 = wx0 + (float)(kTile - 1);
-    const float wy0 = (float)(ty * kTile + 4 * (int)warp), wy1 = wy0 + 3.0f;
-    float fy[2], T[2], C[2][3];
-    int cnt[2];
-    unsigned last[2];
-    bool done[2];
+    const float wy0 = (float)(ty * kTile + 2 * PPT * (int)warp), wy1 = wy0 + (float)(2 * PPT - 1);
+    float fy[PPT], T[PPT], C[PPT][3];
+    int cnt[PPT];
+    unsigned last[PPT];
+    bool done[PPT];
 #pragma unroll
-    for (int p = 0; p < 2; p++) {
+    for (int p = 0; p < PPT; p++) {
         const int y = ybase + 2 * p;
         fy[p] = (float)y;
         T[p] = 1.0f;
@@ -94,7 +97,10 @@ __global__ void __launch_bounds__(kFwdThreads) k_raster_fwd(const StepParams* __
         done[p] = !(x < W && y < H);
     }
     for (unsigned b = rs; b < re; b += kFwdBatch) {
-        if (__syncthreads_count(done[0] && done[1]) == kFwdThreads) break;
+        bool all_done = true;
+#pragma unroll
+        for (int p = 0; p < PPT; p++) all_done = all_done && done[p];
+        if (__syncthreads_count(all_done) == kFwdThreads) break;
 #pragma unroll
         for (int e = threadIdx.x; e < kFwdBatch; e += kFwdThreads) {
             const unsigned j = b + (unsigned)e;
@@ -113,14 +119,17 @@ __global__ void __launch_bounds__(kFwdThreads) k_raster_fwd(const StepParams* __
         __syncthreads();
         const int nb = (int)min((unsigned)kFwdBatch, re - b);
         for (int k = 0; k < nb; k++) {
-            if (done[0] && done[1]) break;
+            bool thread_done = true;
+#pragma unroll
+            for (int p = 0; p < PPT; p++) thread_done = thread_done && done[p];
+            if (thread_done) break;
             if (box_misses(s_box[k], wx0, wx1, wy0, wy1)) continue;
             const float4 a = s_r0[k];
             const float4 c = s_r1[k];
             const float thr = s_thr[k];
             const float dx = a.x - fx;
 #pragma unroll
-            for (int p = 0; p < 2; p++) {
+            for (int p = 0; p < PPT; p++) {
                 if (done[p]) continue;
                 const float dy = a.y - fy[p];
                 const float power = power_rn(a, c, dx, dy);
@@ -143,7 +152,7 @@ __global__ void __launch_bounds__(kFwdThreads) k_raster_fwd(const StepParams* __
     }
     double lsum = 0.0;
 #pragma unroll
-    for (int p = 0; p < 2; p++) {
+    for (int p = 0; p < PPT; p++) {
         const int y = ybase + 2 * p;
         if (x < W && y < H) {
             const int pix = (int)sp.pix_base + y * W + x;

@@ -47,6 +47,9 @@ typedef struct gs3dc_ctx gs3dc_ctx;
 #define GS3DC_OPT_FUSED_ADAM     6  /* 1: optimiser fused into the preprocess backward; 0 (default): split */
 #define GS3DC_OPT_SORT           7  /* GS3DC_SORT_*: how gs3dc_train_step orders its pairs (same result) */
 #define GS3DC_OPT_KEEP_GRADIENTS 8  /* 1: gs3dc_train_step keeps its raw-parameter gradients (gs3dc_get_gradients) */
+#define GS3DC_OPT_AUTOTUNE       9  /* 1: tune the rasterisers' threads per tile (pixels per thread 1 / 2 / 4) online:
+                                       per workload shape the first 6 train steps try each setting twice (timed with
+                                       events, un-captured) and the fastest forward / backward stay; 0 (default): 2 */
 
 /* Depth-first (default): the Gaussians are stably sorted by depth, their pairs
  * emitted in that order and stably sorted by the tile bits alone.  Full key:
@@ -73,6 +76,8 @@ typedef struct gs3dc_ctx gs3dc_ctx;
 #define GS3DC_STAT_SORT_PASSES    4  /* radix passes of the last sort */
 #define GS3DC_STAT_GRAPH_REPLAYS  5
 #define GS3DC_STAT_ADAM_STEP      6  /* Adam step counter (AdamOptimizer::step_count) */
+#define GS3DC_STAT_FWD_PPT        7  /* pixels per thread of the forward rasteriser in the last train step */
+#define GS3DC_STAT_BWD_PPT        8  /* pixels per thread of the backward rasteriser in the last train step */
 
 /* Host arrays of PreprocessOutput + the per-Gaussian ForwardCache fields
  * (include/types.h:69-82, 97-107).  Any pointer may be NULL (not produced). */

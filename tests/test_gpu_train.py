@@ -215,3 +215,36 @@ def test_recompute_backward_memory_vs_stored_lists(ctx):
     stored_list = int(nc.astype(np.int64).sum()) * 8
     recompute = cam.width * cam.height * 9
     assert recompute * 10 < stored_list, (recompute, stored_list)
+
+
+@pytest.mark.parametrize("form", [gs3d.FORM_PLAIN_FP32, gs3d.FORM_BF16])
+def test_autotuner_picks_a_setting_and_keeps_results(ctx, form):
+    """GS3DC_OPT_AUTOTUNE: the first 6 steps try 1 / 2 / 4 pixels per thread,
+    then the picks stay; the forward image does not depend on the setting and
+    the trajectory matches an untuned run to FP32-summation level."""
+    sc = S.random_scene(20000, seed=51)
+    cam = S.look_at_camera((0.3, 0.2, -3.0), 320, 240)
+    gt = O.forward(S.perturbed(sc), cam, S.render_config(False), "c").image
+    cfg, tc = S.render_config(True), S.train_config()
+    ctx.set_option(gs3d.OPT_FORM, form)
+    res = []
+    try:
+        for tune in (0, 1):
+            ctx.set_option(gs3d.OPT_AUTOTUNE, tune)
+            ctx.set_raw_params(sc)
+            losses = [ctx.train_step(cam, gt, cfg, tc, it) for it in range(10)]
+            res.append((losses, ctx.get_raw_params(sc.copy()),
+                        (ctx.stat(gs3d.STAT_FWD_PPT), ctx.stat(gs3d.STAT_BWD_PPT))))
+    finally:
+        ctx.set_option(gs3d.OPT_AUTOTUNE, 0)
+        ctx.set_option(gs3d.OPT_FORM, gs3d.FORM_PLAIN_FP32)
+    (l0, p0, k0), (l1, p1, k1) = res
+    print(f"form {form}: autotuner picked forward {k1[0]}, backward {k1[1]} pixels per thread")
+    assert k0 == (2, 2) and k1[0] in (1, 2, 4) and k1[1] in (1, 2, 4)
+    assert abs(l0[0] - l1[0]) <= 1e-6 * l0[0]     # same first forward whatever the setting
+    assert np.allclose(l0, l1, rtol=2e-3)
+    if form == gs3d.FORM_PLAIN_FP32:
+        # the backward's FP32 sums change order with the setting; Adam moves by at most lr per step.
+        # (In BF16 a stochastic-rounding decision can flip by one 16-bit ulp: only the losses compare.)
+        for k in ("positions", "scales", "rotations", "sh", "opacities"):
+            assert np.abs(getattr(p0, k) - getattr(p1, k)).max() <= 5e-3, k
