@@ -70,6 +70,8 @@ def _args(argv=None):
                     help="time only --form (no plain comparison)")
     ap.add_argument("--batched-steps", dest="batched_steps", type=int, default=5,
                     help="timed steps of the 64-view step (0: skip it)")
+    ap.add_argument("--autotune", type=int, default=1,
+                    help="1: let the library tune the rasterisers' threads per tile during the warm-up")
     ap.add_argument("--only-batched", dest="only_batched", action="store_true",
                     help="print only the 64-view measurement (profiling runs)")
     return ap.parse_args(argv)
@@ -255,17 +257,20 @@ def _measure_form(a, ctx, form, w, cam, cfg, tc, gt_dev, gt_pin, local, dist):
     import torch
     from aaags_claude_b200 import gs3d
     ctx.set_option(gs3d.OPT_FORM, FORMS[form])
+    ctx.set_option(gs3d.OPT_AUTOTUNE, a.autotune)
     ctx.set_raw_params(w.scene)
     stream = torch.cuda.ExternalStream(ctx.stream_handle(), device=f"cuda:{local}")
     it = 0
     loss0 = ctx.train_step(cam, None, cfg, tc, it, gt_device_ptr=gt_dev.data_ptr())   # sizes the pair buffers
     it += 1
-    for _ in range(max(a.warmup, 3)):
+    for _ in range(max(a.warmup, 3) + (6 if a.autotune else 0)):   # the autotuner's 6 trial steps first
         ctx.train_step(cam, None, cfg, tc, it, want_loss=False, gt_device_ptr=gt_dev.data_ptr())
         it += 1
     ctx.synchronize()
     r = {"form": form, "loss_first": loss0, "tile_pairs": ctx.stat(gs3d.STAT_TOTAL_PAIRS),
-         "sort_passes": ctx.stat(gs3d.STAT_SORT_PASSES)}
+         "sort_passes": ctx.stat(gs3d.STAT_SORT_PASSES),
+         "raster_pixels_per_thread": {"forward": ctx.stat(gs3d.STAT_FWD_PPT), "backward": ctx.stat(gs3d.STAT_BWD_PPT),
+                                      "autotuned": bool(a.autotune)}}
     # ---- value: inputs resident in HBM, graph replay, CUDA events on the library stream ----
     clocks = ClockSampler(_bus_id(local))
     if dist:
@@ -346,6 +351,7 @@ def _summary(a, r, world, X, N, T, depth_first, peak):
         "sort_keys_per_s": round(P * pair_passes / (sp_ms * 1e-3), 1) if sp_ms > 0 else None,
         "loss_first": r["loss_first"], "loss_last": r["loss_last"], "clocks": r["clocks"],
         "cuda_graph": r["graph"], "sort_passes": passes,
+        "raster_pixels_per_thread": r["raster_pixels_per_thread"],
     }
 
 
@@ -404,7 +410,8 @@ def run_ours(a) -> int:
                                    f"positions FP32, other attributes + SH {chosen.upper()}, Adam moments BF16"),
                        "arithmetic": "FP32 blending, transmittance and gradients",
                        "l2": "working set ~1.6 GB per step > 126 MB L2 (no flush needed)",
-                       "parallelism": f"replicas x{world}", "cuda_graph": head["cuda_graph"]},
+                       "parallelism": f"replicas x{world}", "cuda_graph": head["cuda_graph"],
+                       "raster_pixels_per_thread": head["raster_pixels_per_thread"]},
             "mpix_per_s": head["mpix_per_s"],
             "e2e": head["e2e"],
             "gpu_launches": head["gpu_launches"],
@@ -418,7 +425,8 @@ def run_ours(a) -> int:
         if chosen != "plain":
             p = summ["plain"]
             line["plain_fp32"] = {k: p[k] for k in ("value", "ms_per_step", "mpix_per_s", "e2e", "gpu_launches",
-                                                    "tile_pairs", "stage_ms", "roofline", "clocks")}
+                                                    "tile_pairs", "stage_ms", "roofline", "clocks",
+                                                    "raster_pixels_per_thread")}
             line["chosen_vs_plain"] = round(head["value"] / p["value"], 3)
             line["gpu_launches"] = head["gpu_launches"] + p["gpu_launches"]
         if world == 1 and not a.no_cpu_baseline and _workload_name(a) == WORKLOAD:
@@ -466,6 +474,7 @@ def measure_batched(a, local: int) -> dict:
 
     # the chosen form, all 64 views per step
     ctx.set_option(gs3d.OPT_FORM, gs3d.FORM_BF16)
+    ctx.set_option(gs3d.OPT_AUTOTUNE, a.autotune)
     ctx.set_raw_params(w.scene)
     it = [0]
 
@@ -474,14 +483,16 @@ def measure_batched(a, local: int) -> dict:
         it[0] += 1
     loss0 = ctx.train_step_batch(cams, None, cfg, tc, it[0], gt_device_ptr=gt_dev.data_ptr())
     it[0] += 1
-    for k in range(3):
+    for k in range(3 + (6 if a.autotune else 0)):   # the autotuner's 6 trial steps first
         batched(k)
     ctx.synchronize()
+    ppt_b = {"forward": ctx.stat(gs3d.STAT_FWD_PPT), "backward": ctx.stat(gs3d.STAT_BWD_PPT)}
     ms_b = timed(batched)
     loss_b = ctx.train_step_batch(cams, None, cfg, tc, it[0], gt_device_ptr=gt_dev.data_ptr())
     launches_b = ctx.stat(gs3d.STAT_KERNELS_LAST)
 
-    # the plain FP32 path, the same views one by one (one optimiser step per view)
+    # the plain FP32 path, the same views one by one (one optimiser step per view, fixed 2 pixels per thread)
+    ctx.set_option(gs3d.OPT_AUTOTUNE, 0)
     ctx.set_option(gs3d.OPT_FORM, gs3d.FORM_PLAIN_FP32)
     ctx.set_raw_params(w.scene)
 
@@ -497,7 +508,8 @@ def measure_batched(a, local: int) -> dict:
     return {"workload": "batched_64views_1M_gaussians_mixed_320x240_to_3840x2160", "views": len(cams),
             "mpix_per_step": round(pix / 1e6, 2), "steps": steps,
             "batched_bf16": {"ms_per_step": round(ms_b, 3), "mpix_per_s": round(pix / 1e6 / (ms_b * 1e-3), 1),
-                             "gpu_launches_per_step": launches_b, "loss_first": loss0, "loss_last": loss_b},
+                             "gpu_launches_per_step": launches_b, "loss_first": loss0, "loss_last": loss_b,
+                             "raster_pixels_per_thread": ppt_b},
             "plain_fp32_one_by_one": {"ms_per_64_views": round(ms_p, 3),
                                       "mpix_per_s": round(pix / 1e6 / (ms_p * 1e-3), 1)},
             "mpix_ratio": round(ms_p / ms_b, 3)}
