@@ -248,6 +248,16 @@ def cpu_baseline_reference(w, cfg, tc, gt: np.ndarray) -> dict | None:
             "sample": f"1 full Trainer::step (1M Gaussians, 1920x1080, Adam) on 1 thread: {dt:.2f} s"}
 
 
+# ---------------------------------------------------------------- ranks
+def max_over_ranks(values, dist, device: str) -> list:
+    """Elementwise maximum of per-rank timings over all ranks (replica timing:
+    the job is as slow as its slowest rank)."""
+    import torch
+    v = torch.tensor([float(x) for x in values], dtype=torch.float64, device=device)
+    dist.all_reduce(v, op=dist.ReduceOp.MAX)
+    return [float(x) for x in v.tolist()]
+
+
 # ---------------------------------------------------------------- our arm
 FORMS = {"plain": 0, "bf16": 1, "fp16": 2}
 
@@ -310,9 +320,7 @@ def _measure_form(a, ctx, form, w, cam, cfg, tc, gt_dev, gt_pin, local, dist):
     ctx.set_option(gs3d.OPT_STAGE_TIMING, 0)
     r["stage_ms"] = acc / nt
     if dist:
-        v = torch.tensor([r["ms_total"], r["e2e_s"]], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(v, op=dist.ReduceOp.MAX)
-        r["ms_total"], r["e2e_s"] = float(v[0]), float(v[1])
+        r["ms_total"], r["e2e_s"] = max_over_ranks([r["ms_total"], r["e2e_s"]], dist, f"cuda:{local}")
     return r
 
 
