@@ -306,6 +306,14 @@ __global__ void __launch_bounds__(kCB) k_chosen_backward(const StepParams* __res
                 tma_load_1d(sm.drgb, rg.drgb + 3 * g0, 12u * kCB, &sm.bar);
                 tma_load_1d(sm.dop, rg.dop + g0, 4u * kCB, &sm.bar);
             }
+            // the optimiser's moments of this slice travel to L2 while the adjoint computes
+            const unsigned mv_sh = (unsigned)(kCB * mc3) * 2u;
+            prefetch_l2(static_cast<const __nv_bfloat16*>(c.m_sh) + (size_t)mc3 * g0, mv_sh);
+            prefetch_l2(static_cast<const __nv_bfloat16*>(c.v_sh) + (size_t)mc3 * g0, mv_sh);
+            prefetch_l2(reinterpret_cast<const uint4*>(c.m_attr) + g0, 16u * kCB);
+            prefetch_l2(reinterpret_cast<const uint4*>(c.v_attr) + g0, 16u * kCB);
+            prefetch_l2(c.m_pos + 3 * g0, 12u * kCB);
+            prefetch_l2(c.v_pos + 3 * g0, 12u * kCB);
         }
         mbar_wait(&sm.bar, 0, sp.spin_limit, &ctrl->status);
     } else {

@@ -169,6 +169,12 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned 
 
 // Bounded wait for `phase` of the barrier: false (and kStatusTimeout) if the
 // copies have not landed after spin_limit polls.
+// Bulk prefetch of [src, src + bytes) into L2 (no shared memory, no completion
+// to wait for); src 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void prefetch_l2(const void* src, unsigned bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
+
 __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned phase, unsigned spin_limit,
                                           unsigned* status) {
     for (unsigned i = 0; i < spin_limit; i++)
