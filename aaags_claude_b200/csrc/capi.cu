@@ -762,6 +762,36 @@ int upload_model_arrays(gs3dc_ctx* c, int N, int sh_degree, int mc, const float*
     return GS3DC_OK;
 }
 
+// ---- checkpoint / resume ----
+
+constexpr char kCkptMagic[8] = {'G', 'S', '3', 'D', 'C', 'K', 'P', 'T'};
+constexpr uint32_t kCkptVersion = 1;
+
+struct CkptHeader {
+    char magic[8];
+    uint32_t version;
+    int32_t form, count, sh_degree, max_coeffs, adam_step;
+    int32_t reserved[4];
+};
+
+// The byte sizes of a form's arrays, in file order.
+std::vector<size_t> state_sizes(int form, size_t n, size_t mc3) {
+    if (form != GS3DC_FORM_PLAIN_FP32)   // 16-bit model, BF16 moments, FP32 positions and their moments
+        return {12 * n, 16 * n, 2 * mc3 * n, 12 * n, 12 * n, 16 * n, 16 * n, 2 * mc3 * n, 2 * mc3 * n};
+    return {12 * n, 12 * n, 16 * n, 4 * mc3 * n, 4 * n,                 // positions, scales, rotations, SH, opacity
+            12 * n, 12 * n, 12 * n, 12 * n, 16 * n, 16 * n,             // their first / second moments
+            4 * mc3 * n, 4 * mc3 * n, 4 * n, 4 * n};
+}
+
+// The device arrays of the current form, in file order.
+std::vector<void*> state_arrays(gs3dc_ctx* c) {
+    if (chosen_form(c))
+        return {c->c_pos.p, c->c_attr.p, c->c_sh.p, c->cm_pos.p, c->cv_pos.p,
+                c->cm_attr.p, c->cv_attr.p, c->cm_sh.p, c->cv_sh.p};
+    return {c->pos.p, c->sc.p, c->rot.p, c->sh.p, c->op.p, c->m_pos.p, c->v_pos.p, c->m_sc.p,
+            c->v_sc.p, c->m_rot.p, c->v_rot.p, c->m_sh.p, c->v_sh.p, c->m_op.p, c->v_op.p};
+}
+
 // ---- multi-view train step ----
 
 struct BatchShape {
@@ -1742,6 +1772,112 @@ int gs3dc_train_step_batch(gs3dc_ctx* c, int n_views, const gs3d_camera* cams, c
     }
     c->adam_step = step_before;
     return fail(c, GS3DC_ERR_PAIR_OVERFLOW, "tile-pair capacity kept overflowing");
+}
+
+int gs3dc_save_state(gs3dc_ctx* c, const char* path) {
+    if (!c || !path) return GS3DC_ERR_INVALID_ARG;
+    int rc;
+    if ((rc = require_model(c))) return rc;
+    if (!c->model_raw) return fail(c, GS3DC_ERR_STATE, "the device model is an activated render model");
+    if (chosen_form(c) && !c->chosen_ready) return fail(c, GS3DC_ERR_STATE, "no reduced-storage model loaded");
+    CK(cudaSetDevice(c->device));
+    if ((rc = gs3dc_synchronize(c))) return rc;   // queued steps and their overflow bookkeeping first
+    if ((rc = ensure_adam(c))) return rc;
+    CkptHeader h{};
+    std::memcpy(h.magic, kCkptMagic, 8);
+    h.version = kCkptVersion;
+    h.form = c->form;
+    h.count = c->N;
+    h.sh_degree = c->sh_degree;
+    h.max_coeffs = c->max_coeffs;
+    h.adam_step = c->adam_step;
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return fail(c, GS3DC_ERR_INVALID_ARG, "cannot open %s for writing", path);
+    bool ok = std::fwrite(&h, sizeof(h), 1, f) == 1;
+    std::vector<unsigned char> buf;
+    const std::vector<void*> arrays = state_arrays(c);
+    const std::vector<size_t> sizes = state_sizes(c->form, (size_t)c->N, (size_t)c->max_coeffs * 3);
+    for (size_t k = 0; k < arrays.size() && ok; k++) {
+        void* p = arrays[k];
+        const size_t bytes = sizes[k];
+        buf.resize(bytes);
+        if (bytes && cudaMemcpy(buf.data(), p, bytes, cudaMemcpyDeviceToHost) != cudaSuccess) {
+            std::fclose(f);
+            return fail(c, GS3DC_ERR_CUDA, "download of the training state failed");
+        }
+        ok = bytes == 0 || std::fwrite(buf.data(), 1, bytes, f) == bytes;
+    }
+    ok = (std::fclose(f) == 0) && ok;
+    if (!ok) return fail(c, GS3DC_ERR_INVALID_ARG, "write to %s failed", path);
+    return GS3DC_OK;
+}
+
+int gs3dc_load_state(gs3dc_ctx* c, const char* path) {
+    if (!c || !path) return GS3DC_ERR_INVALID_ARG;
+    CK(cudaSetDevice(c->device));
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return fail(c, GS3DC_ERR_INVALID_ARG, "cannot open %s", path);
+    CkptHeader h{};
+    if (std::fread(&h, sizeof(h), 1, f) != 1 || std::memcmp(h.magic, kCkptMagic, 8) != 0 ||
+        h.version != kCkptVersion || h.count < 0 || h.max_coeffs < 1 || h.max_coeffs > 16 ||
+        (h.form != GS3DC_FORM_PLAIN_FP32 && h.form != GS3DC_FORM_BF16 && h.form != GS3DC_FORM_FP16)) {
+        std::fclose(f);
+        return fail(c, GS3DC_ERR_INVALID_ARG, "%s is not a gs3dc training-state file", path);
+    }
+    // the file holds exactly the arrays its header describes: checked before the model is touched
+    const size_t n = (size_t)h.count, mc3 = (size_t)h.max_coeffs * 3;
+    const std::vector<size_t> sizes = state_sizes(h.form, n, mc3);
+    size_t expect = sizeof(CkptHeader);
+    for (size_t b : sizes) expect += b;
+    if (std::fseek(f, 0, SEEK_END) != 0 || std::ftell(f) != (long)expect ||
+        std::fseek(f, (long)sizeof(CkptHeader), SEEK_SET) != 0) {
+        std::fclose(f);
+        return fail(c, GS3DC_ERR_INVALID_ARG, "%s does not hold the %zu bytes its header describes", path, expect);
+    }
+    // the model's shape and form first (zeros), then every array from the file
+    std::vector<float> z(std::max<size_t>(1, std::max(mc3, (size_t)4) * n), 0.0f);
+    int rc = upload_model_arrays(c, h.count, h.sh_degree, h.max_coeffs, z.data(), z.data(), z.data(), z.data(),
+                                 z.data());
+    if (rc) {
+        std::fclose(f);
+        return rc;
+    }
+    c->model_raw = true;
+    drop_graphs(c);
+    c->form = h.form;
+    c->chosen_ready = false;
+    if ((rc = ensure_adam(c)) || (rc = zero_adam(c)) || (chosen_form(c) && (rc = load_chosen(c)))) {
+        std::fclose(f);
+        return rc;
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    std::vector<unsigned char> buf;
+    const std::vector<void*> arrays = state_arrays(c);
+    for (size_t k = 0; k < arrays.size(); k++) {
+        void* p = arrays[k];
+        const size_t bytes = sizes[k];
+        buf.resize(bytes);
+        if (bytes && std::fread(buf.data(), 1, bytes, f) != bytes) {
+            std::fclose(f);
+            return fail(c, GS3DC_ERR_INVALID_ARG, "%s is truncated", path);
+        }
+        if (bytes && cudaMemcpy(p, buf.data(), bytes, cudaMemcpyHostToDevice) != cudaSuccess) {
+            std::fclose(f);
+            return fail(c, GS3DC_ERR_CUDA, "upload of the training state failed");
+        }
+    }
+    std::fclose(f);
+    c->adam_step = h.adam_step;
+    // the device's count of applied Adam steps follows the restored counter
+    Persist ps{};
+    ps.applied_steps = (unsigned long long)h.adam_step;
+    CK(cudaMemcpy(c->persist, &ps, sizeof(Persist), cudaMemcpyHostToDevice));
+    *c->persist_host = ps;
+    // the FP32 model arrays mirror the restored reduced-storage model
+    if (chosen_form(c) && (rc = unload_chosen(c))) return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    c->have_screen = c->have_pairs = c->have_sorted = c->have_raster = c->have_rgrad = c->have_grads = false;
+    return GS3DC_OK;
 }
 
 }  // extern "C"

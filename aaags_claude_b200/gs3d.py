@@ -11,6 +11,7 @@ the CPU: if the library or a B200-class device is missing, ``Context`` raises.
 from __future__ import annotations
 
 import ctypes
+import struct
 import os
 
 import numpy as np
@@ -89,6 +90,8 @@ def load_library(path: str = LIB_PATH):
         "gs3dc_get_stage_times": ([vp, ctypes.POINTER(ctypes.c_float), ctypes.c_int], ctypes.c_int),
         "gs3dc_selftest_bounded_wait": ([vp, ctypes.c_uint32], ctypes.c_int),
         "gs3dc_get_gradients": ([vp, vp, vp, vp, vp, vp], ctypes.c_int),
+        "gs3dc_save_state": ([vp, ctypes.c_char_p], ctypes.c_int),
+        "gs3dc_load_state": ([vp, ctypes.c_char_p], ctypes.c_int),
         "gs3dc_train_step_batch": ([vp, ctypes.c_int, vp, vp, ctypes.c_int, vp, vp, ctypes.c_int, vp],
                                    ctypes.c_int),
         "gs3dc_sort_pairs_static": ([i64, vp, vp, ctypes.c_int, vp, vp, vp, vp, ctypes.c_char_p, ctypes.c_size_t],
@@ -313,6 +316,17 @@ class Context:
         self._chk(self.L.gs3dc_train_step_batch(self.h, len(cams), ctypes.byref(arr), gp, on_dev, _ref(cfg), _ref(tcfg),
                                                 int(iteration), ctypes.byref(loss) if want_loss else None))
         return float(loss.value) if want_loss else None
+
+    def save_state(self, path: str):
+        """Model, optimiser moments and step counter to a file (gs3dc_save_state)."""
+        self._chk(self.L.gs3dc_save_state(self.h, str(path).encode()))
+
+    def load_state(self, path: str):
+        """Restores a saved training state; the context takes the saved form and shape."""
+        self._chk(self.L.gs3dc_load_state(self.h, str(path).encode()))
+        with open(path, "rb") as f:
+            _, _, _, count, _, max_coeffs, _ = struct.unpack("<8sIiiiii", f.read(32))
+        self._model = ("raw", count, max_coeffs)
 
     def get_gradients(self) -> dict:
         """Raw-parameter gradients of the last train step (GS3DC_OPT_KEEP_GRADIENTS)."""

@@ -430,7 +430,7 @@ def run_ours(a) -> int:
             "loss_first": head["loss_first"], "loss_last": head["loss_last"],
             "clocks": head["clocks"],
         }
-        if chosen != "plain":
+        if chosen != "plain" and "plain" in summ:
             p = summ["plain"]
             line["plain_fp32"] = {k: p[k] for k in ("value", "ms_per_step", "mpix_per_s", "e2e", "gpu_launches",
                                                     "tile_pairs", "stage_ms", "roofline", "clocks",

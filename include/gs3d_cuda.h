@@ -267,6 +267,15 @@ int gs3dc_selftest_bounded_wait(gs3dc_ctx* ctx, uint32_t spin_limit);
 int gs3dc_get_gradients(gs3dc_ctx* ctx, float* d_raw_positions, float* d_raw_scales,
                         float* d_raw_rotations, float* d_raw_sh_coeffs, float* d_raw_opacities);
 
+/* Checkpoint / resume of the whole training state: the model in its current
+ * form's storage (FP32, or the 16-bit arrays), the optimiser moments and the
+ * Adam step counter, so that a resumed run continues exactly where the saved
+ * one stopped.  No reference counterpart (the reference's train driver saves
+ * the parameters only, src/train_main.cpp:670-674).  gs3dc_load_state
+ * replaces the model and switches the context to the saved form. */
+int gs3dc_save_state(gs3dc_ctx* ctx, const char* path);
+int gs3dc_load_state(gs3dc_ctx* ctx, const char* path);
+
 /* Blocks until every call issued on the context's stream has finished and
  * reports any deferred device-side error (pair overflow, timeout). */
 int gs3dc_synchronize(gs3dc_ctx* ctx);
