@@ -93,6 +93,11 @@ struct gs3dc_ctx {
     DevBuf<float> c_pos, cm_pos, cv_pos;
     DevBuf<unsigned short> c_attr, c_sh, cm_attr, cv_attr, cm_sh, cv_sh;
     DevBuf<uint2> c_rects;
+    // 3D-evaluation mode (RenderConfig::eval_3D): per-Gaussian records, tile rays, view
+    DevBuf<float4> e3_rec, e3_tdir;
+    DevBuf<float> e3_g2s, e3_ci, e3_mo, e3_view, filt3d;
+    bool have_filt3d = false;   // the activated model came with GaussianData::filter_3D
+    bool mode_e3 = false;       // the current screen records and pairs are of the 3D mode
     // control block + preprocess scan descriptors (one memset)
     DevBuf<unsigned char> ctrl_region;
     Control* ctrl = nullptr;
@@ -248,15 +253,17 @@ PixelPtrs pixel_ptrs(gs3dc_ctx* c) {
     return {c->image.p, c->T_final.p, c->n_contrib.p, c->last_j.p, c->dsign.p, c->d_image.p};
 }
 
-int check_config(gs3dc_ctx* c, const gs3d_camera* cam, const gs3d_render_config* cfg) {
+// eval_3D (the reference's AAA-Gaussians mode) renders only: the reference has
+// no backward for it and its train drivers set it false (train_main.cpp:495).
+int check_config(gs3dc_ctx* c, const gs3d_camera* cam, const gs3d_render_config* cfg, bool render_only = false) {
     if (!cam || !cfg) return fail(c, GS3DC_ERR_INVALID_ARG, "camera and render config are required");
     if (cam->width <= 0 || cam->height <= 0)
         return fail(c, GS3DC_ERR_INVALID_ARG, "bad image size %dx%d", cam->width, cam->height);
     if (cfg->tile_w != kTile || cfg->tile_h != kTile)
         return fail(c, GS3DC_ERR_INVALID_ARG, "tile size %dx%d: this path is built for 16x16 tiles",
                     cfg->tile_w, cfg->tile_h);
-    if (cfg->eval_3D)
-        return fail(c, GS3DC_ERR_INVALID_ARG, "eval_3D (3D Gaussian evaluation) is not on this path");
+    if (cfg->eval_3D && !render_only)
+        return fail(c, GS3DC_ERR_INVALID_ARG, "eval_3D renders only: the 3D-evaluation mode has no backward");
     return GS3DC_OK;
 }
 
@@ -395,6 +402,20 @@ int ensure_pixels(gs3dc_ctx* c, int W, int H) {
     c->W = W;
     c->H = H;
     c->num_tiles = gx * gy;
+    return GS3DC_OK;
+}
+
+E3Ptrs e3_ptrs(gs3dc_ctx* c) { return {c->e3_rec.p, c->e3_g2s.p, c->e3_ci.p, c->e3_mo.p, c->e3_tdir.p, c->e3_view.p}; }
+
+// Buffers of the 3D-evaluation mode for N Gaussians and the current tiles.
+int ensure_e3(gs3dc_ctx* c, int N) {
+    const size_t n = N > 0 ? (size_t)N : 1;
+    CK(c->e3_rec.ensure(7 * n));
+    CK(c->e3_g2s.ensure(16 * n));
+    CK(c->e3_ci.ensure(6 * n));
+    CK(c->e3_mo.ensure(3 * n));
+    CK(c->e3_tdir.ensure(c->num_tiles > 0 ? (size_t)c->num_tiles : 1));
+    CK(c->e3_view.ensure(32));
     return GS3DC_OK;
 }
 
@@ -545,6 +566,14 @@ int seq_preprocess(gs3dc_ctx* c, bool cache) {
     CK(cudaMemsetAsync(c->ranges.p, 0, 2 * (size_t)c->num_tiles * sizeof(unsigned), c->stream));
     if ((rc = mark(c, GS3DC_STAGE_PREPROCESS))) return rc;
     PairPtrs pr{c->keys[0].p, c->vals[0].p, c->cap, c->scan_desc};
+    if (c->mode_e3) {
+        CK(launch_e3_view(c->stream, c->sp_dev, c->num_tiles, e3_ptrs(c)));
+        CK(launch_preprocess_e3(c->stream, c->sp_dev, c->N, c->model_raw, model_ptrs(c),
+                                c->have_filt3d && !c->model_raw ? c->filt3d.p : nullptr, screen_ptrs(c, false),
+                                e3_ptrs(c), pr, c->ctrl));
+        c->kernels_last += 1 + (c->N > 0 ? 1 : 0);
+        return GS3DC_OK;
+    }
     CK(launch_preprocess_plain(c->stream, c->sp_dev, c->N, c->model_raw, cache, model_ptrs(c),
                                screen_ptrs(c, cache), pr, c->ctrl));
     c->kernels_last += c->N > 0 ? 1 : 0;
@@ -657,6 +686,7 @@ int seq_back_chosen(gs3dc_ctx* c) {
 // Front half of a train step: preprocess, pair emission, sort, tile ranges.
 int seq_train_front(gs3dc_ctx* c) {
     int rc;
+    c->mode_e3 = false;   // training is the 2D path only
     if (chosen_form(c) || c->sort_mode == GS3DC_SORT_DEPTH_FIRST) {
         if ((rc = seq_front_depth_first(c))) return rc;
     } else {
@@ -703,6 +733,12 @@ int require_model(gs3dc_ctx* c) {
 int run_preprocess(gs3dc_ctx* c, const gs3d_camera* cam, const gs3d_render_config* cfg, bool cache) {
     int rc = ensure_pixels(c, cam->width, cam->height);
     if (rc) return rc;
+    // the 3D mode keeps no 2D ForwardCache (preprocessor_cpu.cpp:36)
+    c->mode_e3 = cfg->eval_3D;
+    if (c->mode_e3) {
+        cache = false;
+        if ((rc = ensure_e3(c, c->N))) return rc;
+    }
     if (c->cap == 0 || c->sort_num_tiles != c->num_tiles) {
         unsigned long long guess = c->min_cap ? c->min_cap : (unsigned long long)c->N * 8ull;
         rc = ensure_pairs(c, guess > c->cap ? guess : c->cap, c->num_tiles);
@@ -1125,6 +1161,12 @@ int gs3dc_set_gaussians(gs3dc_ctx* c, const gs3d_gaussians* g) {
                                  g->sh_coeffs, g->opacities);
     if (rc) return rc;
     c->model_raw = false;
+    // GaussianData::filter_3D (the 3D mode's per-Gaussian mip filter; include/types.h:44)
+    c->have_filt3d = g->filter_3D != nullptr && g->count > 0;
+    if (c->have_filt3d) {
+        CK(c->filt3d.ensure((size_t)g->count));
+        CK(cudaMemcpyAsync(c->filt3d.p, g->filter_3D, (size_t)g->count * 4, cudaMemcpyHostToDevice, c->stream));
+    }
     CK(cudaStreamSynchronize(c->stream));
     return GS3DC_OK;
 }
@@ -1136,6 +1178,7 @@ int gs3dc_set_raw_params(gs3dc_ctx* c, const gs3d_raw_params* r) {
                                  r->raw_rotations, r->raw_sh_coeffs, r->raw_opacities);
     if (rc) return rc;
     c->model_raw = true;
+    c->have_filt3d = false;
     if ((rc = ensure_adam(c))) return rc;
     if ((rc = zero_adam(c))) return rc;
     c->chosen_ready = false;
@@ -1216,9 +1259,10 @@ int gs3dc_preprocess(gs3dc_ctx* c, const gs3d_camera* cam, const gs3d_render_con
     if (!c) return GS3DC_ERR_INVALID_ARG;
     if (int rc_ = require_plain(c, "gs3dc_preprocess")) return rc_;
     int rc;
-    if ((rc = check_config(c, cam, cfg)) || (rc = require_model(c))) return rc;
+    if ((rc = check_config(c, cam, cfg, true)) || (rc = require_model(c))) return rc;
     CK(cudaSetDevice(c->device));
-    const bool cache = out && (out->cov3D || out->p_view || out->p_hom_w || out->cov2D || out->cov2D_det);
+    const bool cache = !cfg->eval_3D && out &&
+                       (out->cov3D || out->p_view || out->p_hom_w || out->cov2D || out->cov2D_det);
     if ((rc = run_preprocess(c, cam, cfg, cache))) return rc;
     if (out) {
         const size_t n = (size_t)c->N;
@@ -1235,6 +1279,10 @@ int gs3dc_preprocess(gs3dc_ctx* c, const gs3d_camera* cam, const gs3d_render_con
             (rc = download(c, out->conics, a.conics, 3 * n * 4)) ||
             (rc = download(c, out->opacities_2d, a.opac2d, n * 4)) || (rc = download(c, out->rgb, a.rgb, 3 * n * 4)) ||
             (rc = download(c, out->radii, a.radii, n * 4)) || (rc = download(c, out->tiles_touched, a.tiles, n * 4)))
+            return rc;
+        if (c->mode_e3 && ((rc = download(c, out->gauss2screen, c->e3_g2s.p, 16 * n * 4)) ||
+                           (rc = download(c, out->cov3D_inv, c->e3_ci.p, 6 * n * 4)) ||
+                           (rc = download(c, out->mean_offset, c->e3_mo.p, 3 * n * 4))))
             return rc;
         if (cache) {
             if ((rc = download(c, out->cov3D, c->c_cov3D.p, 6 * n * 4)) ||
@@ -1255,7 +1303,7 @@ int gs3dc_bin(gs3dc_ctx* c, int num_gaussians, const gs3dc_screen_arrays* in, co
     if (!c) return GS3DC_ERR_INVALID_ARG;
     if (int rc_ = require_plain(c, "gs3dc_bin")) return rc_;
     int rc;
-    if ((rc = check_config(c, cam, cfg))) return rc;
+    if ((rc = check_config(c, cam, cfg, true))) return rc;
     CK(cudaSetDevice(c->device));
     if (!in) {
         if (!c->have_pairs) return fail(c, GS3DC_ERR_STATE, "gs3dc_bin without arrays needs gs3dc_preprocess first");
@@ -1263,6 +1311,8 @@ int gs3dc_bin(gs3dc_ctx* c, int num_gaussians, const gs3dc_screen_arrays* in, co
         if (num_gaussians < 0) return fail(c, GS3DC_ERR_INVALID_ARG, "negative num_gaussians");
         if (num_gaussians > 0 && (!in->means2D || !in->depths || !in->radii || !in->tiles_touched))
             return fail(c, GS3DC_ERR_INVALID_ARG, "means2D, depths, radii and tiles_touched are required");
+        if (num_gaussians > 0 && cfg->eval_3D && (!in->cov3D_inv || !in->mean_offset))
+            return fail(c, GS3DC_ERR_INVALID_ARG, "eval_3D binning needs cov3D_inv and mean_offset");
         // the binned set replaces the device model's pairs; per-Gaussian records are not needed
         const size_t n = (size_t)num_gaussians;
         if ((rc = ensure_ctrl(c, num_gaussians))) return rc;
@@ -1290,7 +1340,19 @@ int gs3dc_bin(gs3dc_ctx* c, int num_gaussians, const gs3dc_screen_arrays* in, co
         }
         ScreenArrays a{c->x_means2D.p, c->x_depths.p, nullptr, nullptr, nullptr, c->x_radii.p, c->x_tiles.p};
         PairPtrs pr{c->keys[0].p, c->vals[0].p, c->cap, c->scan_desc};
-        CK(launch_bin_arrays(c->stream, c->sp_dev, num_gaussians, a, pr, c->ctrl));
+        c->mode_e3 = cfg->eval_3D;
+        if (c->mode_e3) {
+            // per-tile depth keys from the caller's inverse covariances and mean offsets
+            if ((rc = ensure_e3(c, num_gaussians))) return rc;
+            if (n) {
+                CK(cudaMemcpyAsync(c->e3_ci.p, in->cov3D_inv, 6 * n * 4, cudaMemcpyHostToDevice, c->stream));
+                CK(cudaMemcpyAsync(c->e3_mo.p, in->mean_offset, 3 * n * 4, cudaMemcpyHostToDevice, c->stream));
+            }
+            CK(launch_e3_view(c->stream, c->sp_dev, c->num_tiles, e3_ptrs(c)));
+            CK(launch_bin_arrays_e3(c->stream, c->sp_dev, num_gaussians, a, e3_ptrs(c), pr, c->ctrl));
+        } else {
+            CK(launch_bin_arrays(c->stream, c->sp_dev, num_gaussians, a, pr, c->ctrl));
+        }
         if ((rc = read_control(c))) return rc;
         c->have_pairs = true;
         c->have_screen = false;  // the pairs no longer belong to the device model
@@ -1368,16 +1430,22 @@ int gs3dc_rasterize(gs3dc_ctx* c, const gs3d_camera* cam, const gs3d_render_conf
     if (!c) return GS3DC_ERR_INVALID_ARG;
     if (int rc_ = require_plain(c, "gs3dc_rasterize")) return rc_;
     int rc;
-    if ((rc = check_config(c, cam, cfg))) return rc;
+    if ((rc = check_config(c, cam, cfg, true))) return rc;
     if (!c->have_sorted || !c->have_screen)
         return fail(c, GS3DC_ERR_STATE, "gs3dc_rasterize needs gs3dc_preprocess and gs3dc_sort of the model");
+    if (cfg->eval_3D != c->mode_e3)
+        return fail(c, GS3DC_ERR_STATE, "eval_3D differs between gs3dc_preprocess and gs3dc_rasterize");
     if (cam->width != c->W || cam->height != c->H)
         return fail(c, GS3DC_ERR_INVALID_ARG, "camera size differs from the preprocessed one");
     CK(cudaSetDevice(c->device));
     if ((rc = push_params(c, cam, cfg, nullptr, 0, nullptr))) return rc;
     const int w = c->sorted_which;
-    CK(launch_raster_fwd_plain(c->stream, c->sp_dev, c->num_tiles, false, c->ranges.p, c->tile_order.p, c->vals[w].p,
-                               screen_ptrs(c, false), pixel_ptrs(c), c->ctrl));
+    if (c->mode_e3)
+        CK(launch_raster_e3(c->stream, c->sp_dev, c->num_tiles, c->ranges.p, c->tile_order.p, c->vals[w].p,
+                            e3_ptrs(c), pixel_ptrs(c), c->ctrl));
+    else
+        CK(launch_raster_fwd_plain(c->stream, c->sp_dev, c->num_tiles, false, c->ranges.p, c->tile_order.p,
+                                   c->vals[w].p, screen_ptrs(c, false), pixel_ptrs(c), c->ctrl));
     const size_t np = (size_t)c->W * c->H;
     if ((rc = download(c, image, c->image.p, 3 * np * 4)) || (rc = download(c, T_final, c->T_final.p, np * 4)) ||
         (rc = download(c, n_contrib, c->n_contrib.p, np * 4)))
@@ -1392,7 +1460,7 @@ int gs3dc_render(gs3dc_ctx* c, const gs3d_gaussians* g, const gs3d_camera* cam, 
     if (!c) return GS3DC_ERR_INVALID_ARG;
     if (int rc_ = require_plain(c, "gs3dc_render")) return rc_;
     int rc;
-    if ((rc = check_config(c, cam, cfg))) return rc;
+    if ((rc = check_config(c, cam, cfg, true))) return rc;
     if (g && (rc = gs3dc_set_gaussians(c, g))) return rc;
     if ((rc = require_model(c))) return rc;
     if ((rc = gs3dc_preprocess(c, cam, cfg, nullptr))) return rc;

@@ -69,6 +69,17 @@ struct GradPtrs {
 };
 
 // Host arrays in PreprocessOutput layout, on the device (export / import).
+// Per-Gaussian arrays of the 3D-evaluation mode (RenderConfig::eval_3D).
+struct E3Ptrs {
+    float4* rec;      // [N*7] raster record: gauss2screen rows 0, 1, 3; cov3D_inv; mean_offset,
+                      // opacity, depth, rgb
+    float* g2s;       // [N*16] gauss2screen (row-major), zero for culled Gaussians
+    float* ci;        // [N*6] inverse 3D covariance (upper triangle)
+    float* mo;        // [N*3] position - camera position
+    float4* tdir;     // [num_tiles] unit ray through each tile centre, w = 1 when defined
+    float* view;      // [17] inverse view-projection (column-major) and its validity flag
+};
+
 struct ScreenArrays {
     float* means2D;
     float* depths;
@@ -161,6 +172,17 @@ cudaError_t launch_emit_ranked(cudaStream_t st, const StepParams* sp, int N, con
 cudaError_t launch_bin_arrays(cudaStream_t st, const StepParams* sp, int N, ScreenArrays a,
                               PairPtrs pr, Control* ctrl);
 cudaError_t launch_export_screen(cudaStream_t st, int N, ScreenPtrs s, ScreenArrays a);
+// 3D-evaluation mode: view setup (inverse view-projection, tile rays), the
+// fused preprocess + pair emission (raw: activate the device model first;
+// filt: per-Gaussian 3D filter or NULL), the emission from host arrays (a.means2D,
+// depths, radii, tiles with e.ci / e.mo) and the buffered rasteriser.
+cudaError_t launch_e3_view(cudaStream_t st, const StepParams* sp, int num_tiles, E3Ptrs e);
+cudaError_t launch_preprocess_e3(cudaStream_t st, const StepParams* sp, int N, bool raw, ModelPtrs m,
+                                 const float* filt, ScreenPtrs s, E3Ptrs e, PairPtrs pr, Control* ctrl);
+cudaError_t launch_bin_arrays_e3(cudaStream_t st, const StepParams* sp, int N, ScreenArrays a, E3Ptrs e,
+                                 PairPtrs pr, Control* ctrl);
+cudaError_t launch_raster_e3(cudaStream_t st, const StepParams* sp, int num_tiles, const unsigned* ranges,
+                             const unsigned* order, const unsigned* vals, E3Ptrs e, PixelPtrs px, Control* ctrl);
 // order: tile permutation (heavy first) or NULL for row-major
 cudaError_t launch_raster_fwd_plain(cudaStream_t st, const StepParams* sp, int num_tiles, bool fused_loss,
                                     const unsigned* ranges, const unsigned* order, const unsigned* vals,

@@ -89,11 +89,19 @@ struct EmitShared {
 // (tile_binner_cpu.cpp:90-97).
 // With pr.tiles32 set, writes tile-only keys and counts the first nd 8-bit
 // digits of every tile into thist[nd][256] (shared memory).
+//
+// DepthFn(dbits, gid, tile) gives the low 32 key bits of each pair: the
+// Gaussian's depth bits here, a depth per tile in the 3D-evaluation mode.
+struct KeepDepth {
+    __device__ __forceinline__ unsigned operator()(unsigned dbits, unsigned, unsigned) const { return dbits; }
+};
+
+template <class DepthFn = KeepDepth>
 __device__ __forceinline__ void scan_and_emit(EmitShared& sm, int blk, unsigned gid, int cnt, int emit, int rx, int ry,
                                               int rw, unsigned dbits, int grid_x, PairPtrs pr,
                                               Control* ctrl, unsigned spin_limit, Persist* persist,
                                               unsigned* thist = nullptr, int nd = 0, unsigned tile_base_t = 0u,
-                                              int grid_x_t = -1) {
+                                              int grid_x_t = -1, DepthFn depth_fn = DepthFn()) {
     const int tid = threadIdx.x;
     int total;
     const int incl = block_inclusive_scan(cnt, sm.warp, &total);
@@ -136,7 +144,7 @@ __device__ __forceinline__ void scan_and_emit(EmitShared& sm, int blk, unsigned 
             pr.tiles32[dst] = tile;
             for (int d = 0; d < nd; d++) atomicAdd(&thist[d * 256 + ((tile >> (8 * d)) & 255u)], 1u);
         } else {
-            pr.keys[dst] = ((unsigned long long)tile << 32) | sm.depth[lo];
+            pr.keys[dst] = ((unsigned long long)tile << 32) | depth_fn(sm.depth[lo], sm.gid[lo], tile);
         }
         pr.vals[dst] = sm.gid[lo];
     }
@@ -649,6 +657,11 @@ __global__ void __launch_bounds__(256) k_optimizer(const StepParams* __restrict_
 inline int blocks_for(long long n, int t) { return (int)((n + t - 1) / t); }
 
 }  // namespace
+}  // namespace gs3d
+
+#include "eval3d.cuh"
+
+namespace gs3d {
 
 cudaError_t launch_preprocess_plain(cudaStream_t st, const StepParams* sp, int N, bool train, bool cache,
                                     ModelPtrs m, ScreenPtrs s, PairPtrs pr, Control* ctrl, DepthKeys dk) {
@@ -691,6 +704,40 @@ cudaError_t launch_bin_arrays(cudaStream_t st, const StepParams* sp, int N, Scre
 cudaError_t launch_export_screen(cudaStream_t st, int N, ScreenPtrs s, ScreenArrays a) {
     if (N <= 0) return cudaSuccess;
     k_export_screen<<<blocks_for(N, 256), 256, 0, st>>>(N, s, a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_e3_view(cudaStream_t st, const StepParams* sp, int num_tiles, E3Ptrs e) {
+    k_e3_view<<<blocks_for(num_tiles > 0 ? num_tiles : 1, 256), 256, 0, st>>>(sp, e.tdir, e.view);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_preprocess_e3(cudaStream_t st, const StepParams* sp, int N, bool raw, ModelPtrs m,
+                                 const float* filt, ScreenPtrs s, E3Ptrs e, PairPtrs pr, Control* ctrl) {
+    if (N <= 0) return cudaSuccess;
+    if (raw) k_preprocess_e3<true><<<blocks_for(N, kBlock), kBlock, 0, st>>>(sp, N, m, filt, s, e, pr, ctrl);
+    else k_preprocess_e3<false><<<blocks_for(N, kBlock), kBlock, 0, st>>>(sp, N, m, filt, s, e, pr, ctrl);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bin_arrays_e3(cudaStream_t st, const StepParams* sp, int N, ScreenArrays a, E3Ptrs e,
+                                 PairPtrs pr, Control* ctrl) {
+    if (N <= 0) return cudaSuccess;
+    k_bin_arrays_e3<<<blocks_for(N, kBlock), kBlock, 0, st>>>(sp, N, a, e.ci, e.mo, e.tdir, pr, ctrl);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_raster_e3(cudaStream_t st, const StepParams* sp, int num_tiles, const unsigned* ranges,
+                             const unsigned* order, const unsigned* vals, E3Ptrs e, PixelPtrs px, Control* ctrl) {
+    if (num_tiles <= 0) return cudaSuccess;
+    static bool attr_set = false;   // per process: the kernel's dynamic shared memory above 48 KB
+    if (!attr_set) {
+        cudaError_t err =
+            cudaFuncSetAttribute(k_raster_e3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kE3RasterSmem);
+        if (err != cudaSuccess) return err;
+        attr_set = true;
+    }
+    k_raster_e3<<<num_tiles, kE3Threads, kE3RasterSmem, st>>>(sp, ranges, order, vals, e, px, ctrl);
     return cudaGetLastError();
 }
 

@@ -42,7 +42,8 @@ class ScreenArrays(ctypes.Structure):
 
     _fields_ = [(n, _f) for n in ("means2D", "depths", "conics", "opacities_2d", "rgb")] + \
                [("radii", _i), ("tiles_touched", _i)] + \
-               [(n, _f) for n in ("cov3D", "p_view", "p_hom_w", "cov2D", "cov2D_det")]
+               [(n, _f) for n in ("cov3D", "p_view", "p_hom_w", "cov2D", "cov2D_det",
+                                  "gauss2screen", "cov3D_inv", "mean_offset")]
 
 
 class Gs3dError(RuntimeError):
@@ -183,13 +184,20 @@ class Context:
         return list(a)
 
     # ---- model ----
-    def set_gaussians(self, scene: S.Scene, act: dict):
-        """Uploads an activated model (act: positions/scales/rotations/sh_coeffs/opacities)."""
+    def set_gaussians(self, scene: S.Scene, act: dict, filter_3d: np.ndarray | None = None):
+        """Uploads an activated model (act: positions/scales/rotations/sh_coeffs/opacities);
+        filter_3d: GaussianData::filter_3D of the eval_3D mode, or None."""
         g = S.GaussianData()
         g.count, g.sh_degree, g.max_coeffs = scene.count, scene.sh_degree, scene.max_coeffs
-        for k in ("positions", "sh_coeffs", "scales", "rotations", "opacities"):
-            setattr(g, k, S.fptr(np.ascontiguousarray(act[k], np.float32)))
-        self._keep = (act, g)
+        arrs = {k: np.ascontiguousarray(act[k], np.float32) for k in
+                ("positions", "sh_coeffs", "scales", "rotations", "opacities")}
+        for k, v in arrs.items():
+            setattr(g, k, S.fptr(v))
+        f3 = None
+        if filter_3d is not None:
+            f3 = np.ascontiguousarray(filter_3d, np.float32)
+            g.filter_3D = S.fptr(f3)
+        self._keep = (arrs, f3, g)
         self._chk(self.L.gs3dc_set_gaussians(self.h, _ref(g)))
         self._model = ("act", scene.count, scene.max_coeffs)
 
@@ -206,11 +214,15 @@ class Context:
 
     # ---- stages ----
     def preprocess(self, cam, cfg, want_cache: bool = False) -> dict:
+        """Preprocessor::process; with cfg.eval_3D also gauss2screen / cov3D_inv / mean_offset."""
         n = self._model[1]
         out = dict(means2D=np.zeros(2 * n, np.float32), depths=np.zeros(n, np.float32),
                    conics=np.zeros(3 * n, np.float32), opacities_2d=np.zeros(n, np.float32),
                    rgb=np.zeros(3 * n, np.float32), radii=np.zeros(n, np.int32),
                    tiles_touched=np.zeros(n, np.int32))
+        if cfg.eval_3D:
+            out.update(gauss2screen=np.zeros(16 * n, np.float32), cov3D_inv=np.zeros(6 * n, np.float32),
+                       mean_offset=np.zeros(3 * n, np.float32))
         if want_cache:
             out.update(cov3D=np.zeros(6 * n, np.float32), p_view=np.zeros(3 * n, np.float32),
                        p_hom_w=np.zeros(n, np.float32), cov2D=np.zeros(3 * n, np.float32),
@@ -231,8 +243,11 @@ class Context:
         if arrays is not None:
             sa = ScreenArrays()
             keep = {}
-            for k in ("means2D", "depths", "radii", "tiles_touched"):
+            names = ("means2D", "depths", "radii", "tiles_touched") + (
+                ("cov3D_inv", "mean_offset") if cfg.eval_3D else ())
+            for k in names:
                 v = np.ascontiguousarray(arrays[k], np.int32 if k in ("radii", "tiles_touched") else np.float32)
+                v = v.reshape(-1)
                 keep[k] = v
                 setattr(sa, k, v.ctypes.data_as(_i if v.dtype == np.int32 else _f))
             n = int(keep["radii"].shape[0])

@@ -59,8 +59,17 @@ PreprocessOutput PreprocessorCUDA::process(const GaussianData& g, const Camera& 
     out.radii = alloc.allocate_array<int>(N);
     out.tiles_touched = alloc.allocate_array<int>(N);
     out.gauss2screen = out.cov3D_inv = out.mean_offset = nullptr;
-    out.eval_3D = false;
+    out.eval_3D = cfg.eval_3D;
     gs3dc_screen_arrays a{};
+    if (cfg.eval_3D) {   // the 3D mode's arrays (preprocessor_cpu.cpp:25-29); it keeps no 2D cache
+        out.gauss2screen = alloc.allocate_array<float>((size_t)N * 16);
+        out.cov3D_inv = alloc.allocate_array<float>((size_t)N * 6);
+        out.mean_offset = alloc.allocate_array<float>((size_t)N * 3);
+        a.gauss2screen = out.gauss2screen;
+        a.cov3D_inv = out.cov3D_inv;
+        a.mean_offset = out.mean_offset;
+        cache = nullptr;
+    }
     a.means2D = out.means2D;
     a.depths = out.depths;
     a.conics = out.conics;
@@ -98,6 +107,8 @@ BinningOutput TileBinnerCUDA::bin(const PreprocessOutput& pre, int N, const Came
         a.depths = pre.depths;
         a.radii = pre.radii;
         a.tiles_touched = pre.tiles_touched;
+        a.cov3D_inv = pre.cov3D_inv;
+        a.mean_offset = pre.mean_offset;
         int64_t total = 0;
         for (int i = 0; i < N; i++) total += pre.tiles_touched[i];
         out.keys_unsorted = total ? alloc.allocate_array<uint64_t>((size_t)total) : nullptr;

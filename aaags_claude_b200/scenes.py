@@ -170,6 +170,26 @@ def random_scene(n: int, sh_degree: int = 3, seed: int = SEED_SCENE) -> Scene:
     return Scene(pos, sc, rot, sh, op, sh_degree)
 
 
+def eval3d_scene(n: int, seed: int = SEED_SCENE, spread: float = 1.5, sh_degree: int = 3) -> Scene:
+    """A scene that reaches every branch of the 3D-evaluation mode's preprocess:
+    means ~ N(0, spread^2 I3) (many outside the view frustum, some behind or close to
+    the camera), log-scales ~ N(-2.5, 1) (large Gaussians crossing the screen border and
+    the near plane, so the view-space bounding box is used), and 5 % with opacity logits
+    near -7 (below 1/255 once the mip filter dilates them)."""
+    rng = np.random.default_rng(seed)
+    pos = rng.normal(0.0, spread, size=(n, 3)).astype(np.float32)
+    sc, rot, sh, op = _draw_attributes(rng, n, sh_degree)
+    sc = rng.normal(-2.5, 1.0, size=(n, 3)).astype(np.float32)
+    low = rng.random(n) < 0.05
+    op[low] = rng.normal(-7.0, 0.5, size=int(low.sum())).astype(np.float32)
+    return Scene(pos, sc, rot, sh, op, sh_degree)
+
+
+def filter_3d_values(n: int, seed: int = SEED_SCENE) -> np.ndarray:
+    """Per-Gaussian 3D mip filter sizes (GaussianData::filter_3D): |N(0, 0.01^2)|."""
+    return np.abs(np.random.default_rng(seed + 1).normal(0.0, 0.01, size=n)).astype(np.float32)
+
+
 def clustered_scene(n: int, clusters: int = 64, sigma: float = 0.15, sh_degree: int = 3,
                     seed: int = SEED_SCENE) -> Scene:
     rng = np.random.default_rng(seed)
@@ -298,6 +318,13 @@ def config_render_100k() -> Workload:
     s = random_scene(100_000)
     cam = look_at_camera((0.0, 0.0, -3.0), 640, 480, 60.0)
     return Workload("render_100k_640x480", s, [cam])
+
+
+def config_render_eval3d() -> Workload:
+    """3D-evaluation render (eval_3D): N=100k random Gaussians, one 640x480 camera 3 units away."""
+    s = random_scene(100_000)
+    cam = look_at_camera((0.0, 0.0, -3.0), 640, 480, 60.0)
+    return Workload("render_eval3d_100k_640x480", s, [cam])
 
 
 def config_train_1m_1080p() -> Workload:

@@ -94,6 +94,11 @@ typedef struct gs3dc_screen_arrays {
     float* p_hom_w;       /* [N] */
     float* cov2D;         /* [N*3] after the +0.3 filter */
     float* cov2D_det;     /* [N] */
+    /* RenderConfig::eval_3D only (PreprocessOutput, include/types.h:77-79):
+     * gs3dc_preprocess fills them; gs3dc_bin reads cov3D_inv and mean_offset */
+    float* gauss2screen;  /* [N*16] row-major, zero for culled Gaussians */
+    float* cov3D_inv;     /* [N*6] inverse 3D covariance, upper triangle */
+    float* mean_offset;   /* [N*3] position - camera position */
 } gs3dc_screen_arrays;
 
 /* ---- context ---- */

@@ -44,7 +44,7 @@ typedef struct gs3d_gaussians {
     float* scales;        /* [N*3] exp()-activated */
     float* rotations;     /* [N*4] unit quaternion (r,x,y,z) */
     float* opacities;     /* [N] sigmoid()-activated */
-    float* filter_3D;     /* [N] or NULL (unused on this path) */
+    float* filter_3D;     /* [N] or NULL: 3D mip filter of the eval_3D mode */
 } gs3d_gaussians;
 
 /* Pinhole camera: world->view and world->clip, both column-major. */
@@ -61,7 +61,7 @@ typedef struct gs3d_render_config {
     float bg_color[3];
     float scale_modifier;
     bool antialiasing;
-    bool eval_3D;         /* must be false: the 3D-evaluation mode is not on this path */
+    bool eval_3D;         /* AAA-Gaussians 3D evaluation: render calls only (no backward) */
     bool training;        /* true: no upper clamp on SH colour */
     int sh_degree;
     int tile_w;

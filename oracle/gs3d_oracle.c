@@ -48,6 +48,9 @@
 #undef REAL
 #undef SFX
 
+/* ---------- 3D evaluation (eval_3D), float only ---------- */
+#include "gs3d_oracle_eval3d.inc"
+
 /* ---------- binning: tile_binner_cpu.cpp:33-99 ---------- */
 
 /* Inclusive scan of tiles_touched (:33-42); returns total pairs. */
@@ -145,6 +148,27 @@ int orc_forward(const gs3d_gaussians* g, const gs3d_camera* cam, const gs3d_rend
              grid_x * grid_y, io->ranges);
     orc_rasterize_f32(io->means2D, io->conics, io->opac2d, io->rgb, io->vals_sorted, io->ranges, cam,
                       cfg, io->image, io->T_final, io->n_contrib);
+    return 0;
+}
+
+/* Forward of the 3D-evaluation mode (cfg->eval_3D): the same sequence with
+ * the eval_3D preprocess, per-tile depth keys and the buffered blend.
+ * g2s[16N], ci[6N], mo[3N] receive the mode's extra per-Gaussian outputs. */
+int orc_forward_eval3d(const gs3d_gaussians* g, const gs3d_camera* cam, const gs3d_render_config* cfg,
+                       orc_step_io* io, float* g2s, float* ci, float* mo) {
+    int N = g->count;
+    orc_preprocess_eval3d(g, cam, cfg, io->means2D, io->depths, io->conics, io->opac2d, io->rgb, io->radii,
+                          io->tiles, g2s, ci, mo);
+    io->total_pairs = orc_scan_tiles(N, io->tiles, NULL);
+    if (io->total_pairs > io->pair_capacity) return 1;
+    orc_bin_eval3d(N, io->means2D, io->depths, io->radii, io->tiles, ci, mo, cam, cfg, io->keys_unsorted,
+                   io->vals_unsorted);
+    int grid_x = (cam->width + cfg->tile_w - 1) / cfg->tile_w;
+    int grid_y = (cam->height + cfg->tile_h - 1) / cfg->tile_h;
+    orc_sort(io->total_pairs, io->keys_unsorted, io->vals_unsorted, io->keys_sorted, io->vals_sorted,
+             grid_x * grid_y, io->ranges);
+    orc_rasterize_eval3d(g2s, io->opac2d, io->rgb, io->depths, ci, mo, io->vals_sorted, io->ranges, cam, cfg,
+                         io->image, io->T_final, io->n_contrib);
     return 0;
 }
 

@@ -246,6 +246,40 @@ def forward(scene, cam, cfg, impl: str = "c", act: dict | None = None, cap: int 
     raise RuntimeError("oracle forward: pair capacity retry failed")
 
 
+def forward_eval3d(scene, cam, cfg, impl: str = "c", act: dict | None = None, cap: int | None = None,
+                   filter_3d: np.ndarray | None = None):
+    """Forward of the 3D-evaluation mode (cfg.eval_3D) of an activated scene.
+
+    Returns (StepResult, extras) with extras = dict(gauss2screen [N,16],
+    cov3D_inv [N,6], mean_offset [N,3]); conics and the 2D cache stay zero.
+    impl "c" is the C restatement, "ref" the reference's own stages.
+    """
+    act = act if act is not None else activate(scene)
+    g = gaussians_struct(scene, act)
+    if filter_3d is not None:
+        f3 = np.ascontiguousarray(filter_3d, np.float32)
+        g.filter_3D = _ptr(f3, _f)
+        g._keep_f3 = f3
+    n, mc3 = scene.count, scene.max_coeffs * 3
+    npx, nt = cam.width * cam.height, _grid(cam, cfg)
+    cap = cap if cap is not None else max(16, 8 * n)
+    for _ in range(2):
+        io, a = _alloc_io(n, mc3, npx, nt, cap, False)
+        io.cov3D = None
+        ex = dict(gauss2screen=np.zeros(16 * n, np.float32), cov3D_inv=np.zeros(6 * n, np.float32),
+                  mean_offset=np.zeros(3 * n, np.float32))
+        args = (ctypes.byref(g), ctypes.byref(cam), ctypes.byref(cfg), ctypes.byref(io),
+                *[_ptr(ex[k], _f) for k in ("gauss2screen", "cov3D_inv", "mean_offset")])
+        rc = (lib_c().orc_forward_eval3d if impl == "c" else lib_ref().ref_forward_eval3d)(*args)
+        if rc == 0:
+            ex = {k: v.reshape(n, -1) for k, v in ex.items()}
+            return _result(io, a, False), ex
+        if rc != 1:
+            raise RuntimeError(f"eval_3D forward failed ({rc})")
+        cap = int(io.total_pairs)
+    raise RuntimeError("oracle forward: pair capacity retry failed")
+
+
 class AdamOracle:
     """Adam moments for the C oracle's train step (zero-initialised)."""
 

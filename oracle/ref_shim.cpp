@@ -124,6 +124,30 @@ int ref_forward(const gs3d_gaussians* gp, const gs3d_camera* camp, const gs3d_re
     return 0;
 }
 
+// The forward with cfg.eval_3D set (the reference's AAA-Gaussians mode): the
+// same stage sequence, plus the mode's per-Gaussian gauss2screen, cov3D_inv
+// and mean_offset arrays.  io->cov3D must be NULL (the mode keeps no 2D cache).
+int ref_forward_eval3d(const gs3d_gaussians* gp, const gs3d_camera* camp, const gs3d_render_config* cfgp,
+                       orc_step_io* io, float* g2s, float* cov3D_inv, float* mean_offset) {
+    const GaussianData& g = *reinterpret_cast<const GaussianData*>(gp);
+    const Camera& cam = *reinterpret_cast<const Camera*>(camp);
+    const RenderConfig& cfg = *reinterpret_cast<const RenderConfig*>(cfgp);
+    if (!cfg.eval_3D || io->cov3D) return 2;
+    int num_pixels = cam.width * cam.height;
+    FrameAllocator alloc(arena_bytes(g.count, g.max_coeffs, io->pair_capacity, num_pixels) +
+                         (size_t)g.count * 25 * sizeof(float));
+    PreprocessOutput pre;
+    BinningOutput bin;
+    ForwardCache cache;
+    float* rendered = nullptr;
+    if (run_forward(g, cam, cfg, alloc, pre, bin, cache, rendered, io)) return 1;
+    copy_forward(g.count, pre, cache, bin, num_pixels, rendered, io);
+    std::memcpy(g2s, pre.gauss2screen, sizeof(float) * 16 * (size_t)g.count);
+    std::memcpy(cov3D_inv, pre.cov3D_inv, sizeof(float) * 6 * (size_t)g.count);
+    std::memcpy(mean_offset, pre.mean_offset, sizeof(float) * 3 * (size_t)g.count);
+    return 0;
+}
+
 // RawGaussianParams::activate (train_types.cpp:6-36) into caller arrays.
 void ref_activate(const gs3d_raw_params* rawp, gs3d_gaussians* gp) {
     reinterpret_cast<const RawGaussianParams*>(rawp)->activate(*reinterpret_cast<GaussianData*>(gp));

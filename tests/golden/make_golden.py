@@ -12,7 +12,9 @@ Two kinds of fixtures, both produced by the reference itself:
   built from the reference sources by oracle/Makefile) on seeded synthetic
   scenes, including the edge cases the reference's unit tests cover: ragged
   tiles, non-black background, antialiasing and scale modifier, SH degrees 0-2,
-  a single Gaussian, every Gaussian culled, oversized splats.
+  a single Gaussian, every Gaussian culled, oversized splats; and the 3D-evaluation
+  mode (eval_3D) on scenes that reach its frustum culling, camera-inside test and
+  view-space bounding box, with and without a 3D filter.
 
 It needs the reference tree at /root/reference (only this script reads it);
 the tests and the GPU runs read the committed copies.
@@ -104,6 +106,46 @@ def render_cases():
     return cases
 
 
+def eval3d_cases():
+    """(name, scene, filter_3D or None, camera, render config) of the eval_3D forward fixtures."""
+    def e3(cfg):
+        cfg.eval_3D = True
+        return cfg
+    culled = S.eval3d_scene(300, seed=34)
+    culled.positions[:, 2] = -6.0 - np.abs(culled.positions[:, 2])   # all behind the camera at z = -3
+    bg = e3(S.render_config(True, 1, bg=(0.3, 0.1, 0.6)))
+    bg.scale_modifier = 1.3
+    return [
+        ("eval3d_2k_128x96", S.eval3d_scene(2000, seed=31), S.filter_3d_values(2000, seed=31),
+         S.look_at_camera((0.3, 0.2, -3.0), 128, 96), e3(S.render_config(False))),
+        ("eval3d_near_96x64", S.eval3d_scene(1500, seed=32), S.filter_3d_values(1500, seed=32),
+         S.look_at_camera((0.1, 0.0, -0.6), 96, 64, 70.0), e3(S.render_config(False))),
+        ("eval3d_ragged_bg_100x37", S.random_scene(800, sh_degree=1, seed=33), None,
+         S.look_at_camera((0.4, 0.3, -2.5), 100, 37, 50.0), bg),
+        ("eval3d_all_culled_48x32", culled, None, S.look_at_camera((0.0, 0.0, -3.0), 48, 32),
+         e3(S.render_config(False))),
+    ]
+
+
+def make_eval3d():
+    dst = os.path.join(HERE, "seeded")
+    os.makedirs(dst, exist_ok=True)
+    for name, sc, f3, cam, cfg in eval3d_cases():
+        r, ex = O.forward_eval3d(sc, cam, cfg, "ref", filter_3d=f3)
+        ks, vs = _canon(r.keys_sorted, r.vals_sorted)
+        vis = r.radii > 0
+        np.savez_compressed(
+            os.path.join(dst, name + ".npz"), **scene_arrays(sc), **cam_arrays(cam, cfg),
+            filter_3d=np.zeros(0, np.float32) if f3 is None else f3,
+            radii=r.radii, tiles=r.tiles, depths=r.depths, means2D=r.means2D, opac2d=r.opac2d, rgb=r.rgb,
+            gauss2screen=np.where(vis[:, None], ex["gauss2screen"], 0).astype(np.float32),
+            cov3D_inv=ex["cov3D_inv"], mean_offset=ex["mean_offset"],
+            total_pairs=np.int64(r.total_pairs), keys_unsorted=r.keys_unsorted, vals_unsorted=r.vals_unsorted,
+            keys_sorted=ks, vals_sorted=vs, ranges=r.ranges, image=r.image, T_final=r.T_final,
+            n_contrib=r.n_contrib)
+        print(name, "visible", int(vis.sum()), "P", r.total_pairs)
+
+
 def _canon(keys, vals):
     o = np.lexsort((vals, keys))
     return keys[o], vals[o]
@@ -159,3 +201,4 @@ if __name__ == "__main__":
         sys.exit("oracle/_ref/libgs3d_ref.so is missing: `make -C oracle ref` needs the reference tree")
     copy_ref_fixtures()
     make_seeded()
+    make_eval3d()

@@ -68,6 +68,35 @@ def load_seeded(name: str):
     return sc, cam, cfg, z
 
 
+def activate_cr(scene) -> dict:
+    """RawGaussianParams::activate (train_types.cpp:6-36) in float32 with a correctly
+    rounded exp -- the device's activation -- for checks of the raw-model path
+    (glibc's expf, which the reference and the C oracle call, is 1 ulp off on a
+    few inputs in 1e5)."""
+    f = np.float32
+    q = np.ascontiguousarray(scene.rotations, f).reshape(-1, 4)
+    ln = np.sqrt(((q[:, 0] * q[:, 0] + q[:, 1] * q[:, 1]) + q[:, 2] * q[:, 2]) + q[:, 3] * q[:, 3])
+    ln = np.where(ln < f(1e-12), f(1e-12), ln).astype(f)
+    inv = (f(1.0) / ln).astype(f)
+    e = np.exp(-np.asarray(scene.opacities, np.float64)).astype(f)
+    return dict(positions=np.ascontiguousarray(scene.positions, f).reshape(-1),
+                scales=np.exp(np.asarray(scene.scales, np.float64)).astype(f).reshape(-1),
+                rotations=(q * inv[:, None]).astype(f).reshape(-1),
+                sh_coeffs=np.ascontiguousarray(scene.sh, f).reshape(-1),
+                opacities=(f(1.0) / (f(1.0) + e)).astype(f))
+
+
+def eval3d_cases():
+    return sorted(f[:-4] for f in os.listdir(SEEDED) if f.startswith("eval3d_"))
+
+
+def load_eval3d(name: str):
+    """(scene, filter_3D or None, camera, render config, fixture) of an eval_3D golden case."""
+    sc, cam, cfg, z = load_seeded(name)
+    f3 = z["filter_3d"] if z["filter_3d"].size else None
+    return sc, f3, cam, cfg, z
+
+
 def canon(keys, vals):
     """(key, value)-sorted order: the reference's std::sort leaves equal keys unordered."""
     o = np.lexsort((vals, keys))

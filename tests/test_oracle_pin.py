@@ -107,6 +107,45 @@ def test_seeded_train_matches_reference():
             assert U.bits_equal(getattr(sc, k), z[f"s{it}_{k}"]), (it, k)
 
 
+@pytest.mark.parametrize("name", U.eval3d_cases())
+def test_eval3d_oracle_matches_reference_fixture(name):
+    """The C restatement of the eval_3D forward against the reference's own outputs."""
+    sc, f3, cam, cfg, z = U.load_eval3d(name)
+    r, ex = O.forward_eval3d(sc, cam, cfg, "c", filter_3d=f3)
+    vis = z["radii"] > 0
+    assert U.bits_equal(r.radii, z["radii"]) and U.bits_equal(r.tiles, z["tiles"])
+    for k, w in (("depths", 1), ("means2D", 2), ("opac2d", 1), ("rgb", 3)):
+        assert U.bits_equal(getattr(r, k).reshape(-1, w)[vis], z[k].reshape(-1, w)[vis]), k
+    for k in ("gauss2screen", "cov3D_inv", "mean_offset"):
+        assert U.bits_equal(ex[k][vis], z[k].reshape(len(vis), -1)[vis]), k
+    assert r.total_pairs == int(z["total_pairs"])
+    assert U.bits_equal(r.keys_unsorted, z["keys_unsorted"]) and U.bits_equal(r.vals_unsorted, z["vals_unsorted"])
+    assert U.bits_equal(r.keys_sorted, z["keys_sorted"]) and U.bits_equal(r.vals_sorted, z["vals_sorted"])
+    assert U.bits_equal(r.ranges, z["ranges"])
+    assert U.bits_equal(r.image, z["image"]) and U.bits_equal(r.T_final, z["T_final"])
+    assert U.bits_equal(r.n_contrib, z["n_contrib"])
+
+
+@pytest.mark.skipif(not O.have_ref(), reason="oracle/_ref not built (needs the reference tree)")
+def test_eval3d_oracle_matches_reference_live():
+    """A fresh seed of the eval_3D forward, both oracles side by side (20k Gaussians, 160x120)."""
+    sc = S.eval3d_scene(20_000, seed=98)
+    f3 = S.filter_3d_values(20_000, seed=98)
+    cam = S.look_at_camera((0.6, -0.3, -2.2), 160, 120, 65.0)
+    cfg = S.render_config(False)
+    cfg.eval_3D = True
+    (a, ea), (b, eb) = (O.forward_eval3d(sc, cam, cfg, impl, filter_3d=f3) for impl in ("c", "ref"))
+    vis = b.radii > 0
+    assert U.bits_equal(a.radii, b.radii) and U.bits_equal(a.depths[vis], b.depths[vis])
+    assert U.bits_equal(ea["gauss2screen"][vis], eb["gauss2screen"][vis])
+    assert U.bits_equal(a.keys_unsorted, b.keys_unsorted)
+    ka, va = U.canon(a.keys_sorted, a.vals_sorted)
+    kb, vb = U.canon(b.keys_sorted, b.vals_sorted)
+    assert U.bits_equal(ka, kb) and U.bits_equal(va, vb)
+    assert U.bits_equal(a.ranges, b.ranges)
+    assert U.bits_equal(a.image, b.image) and U.bits_equal(a.n_contrib, b.n_contrib)
+
+
 @pytest.mark.skipif(not O.have_ref(), reason="oracle/_ref not built (needs the reference tree)")
 def test_oracle_matches_reference_live():
     """A fresh seed, both oracles side by side (forward of 20k Gaussians, 320x240)."""
