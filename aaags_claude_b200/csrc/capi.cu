@@ -410,7 +410,7 @@ E3Ptrs e3_ptrs(gs3dc_ctx* c) { return {c->e3_rec.p, c->e3_g2s.p, c->e3_ci.p, c->
 // Buffers of the 3D-evaluation mode for N Gaussians and the current tiles.
 int ensure_e3(gs3dc_ctx* c, int N) {
     const size_t n = N > 0 ? (size_t)N : 1;
-    CK(c->e3_rec.ensure(7 * n));
+    CK(c->e3_rec.ensure((size_t)kE3Rec * n));
     CK(c->e3_g2s.ensure(16 * n));
     CK(c->e3_ci.ensure(6 * n));
     CK(c->e3_mo.ensure(3 * n));

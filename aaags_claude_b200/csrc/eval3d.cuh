@@ -31,9 +31,8 @@ namespace {
 
 constexpr float kE3Pi = 3.14159265358979323846f;   // (float)M_PI
 constexpr int kKBuf = 16;                           // StopThePop buffer (rasterizer_cpu.cpp:63)
-constexpr int kE3Batch = 128;                       // records staged per batch
+constexpr int kE3Batch = 64;                        // records staged per batch
 constexpr int kE3Threads = 256;                     // one thread per pixel of a 16x16 tile
-constexpr int kE3Rec = 7;                           // float4s per raster record
 
 // x86 float -> int32 truncation (cvttss2si): NaN and out-of-range give INT_MIN.
 __device__ __forceinline__ int cvt_trunc_x86(float f) {
@@ -442,6 +441,36 @@ __device__ bool invert4_e3(const float* m, float inv[16]) {
     return true;
 }
 
+// Conservative pixel box (xmin, xmax, ymin, ymax of pixel indices) outside of
+// which no pixel's ray gets within squared distance 2 thr of the Gaussian,
+// i.e. where alpha stays below 1/255: the projected bounding box of the
+// ellipsoid q <= 2 thr (1 + 1e-4) + 1e-3 (the construction of aabb_screen_e3,
+// evaluated in FP64), shifted by the half-pixel of the ray's pixel centre and
+// widened by one pixel.  No box (never skipped) when the ellipsoid reaches the
+// camera plane.  Used only to skip work: it never changes a result.
+__device__ float4 e3_skip_box(const float g2s[16], float thr) {
+    const float4 none = make_float4(-1e30f, 1e30f, -1e30f, 1e30f);
+    const double c = 2.0 * (double)thr * (1.0 + 1e-4) + 1e-3;
+    const double t[4] = {c, c, c, -1.0};
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) s += t[k] * (double)g2s[12 + k] * (double)g2s[12 + k];
+    if (!(s < 0.0)) return none;
+    double p0 = 0.0, p1 = 0.0, h0 = 0.0, h1 = 0.0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const double f = t[k] / s, r3 = g2s[12 + k], r0 = g2s[k], r1 = g2s[4 + k];
+        p0 += f * r0 * r3;
+        p1 += f * r1 * r3;
+        h0 += f * r0 * r0;
+        h1 += f * r1 * r1;
+    }
+    const double e0 = sqrt(fmax(0.0, p0 * p0 - h0)), e1 = sqrt(fmax(0.0, p1 * p1 - h1));
+    const double x0 = p0 - e0 - 1.5, x1 = p0 + e0 + 0.5, y0 = p1 - e1 - 1.5, y1 = p1 + e1 + 0.5;
+    if (!(fabs(x0) < 1e30 && fabs(x1) < 1e30 && fabs(y0) < 1e30 && fabs(y1) < 1e30)) return none;
+    return make_float4((float)x0, (float)x1, (float)y0, (float)y1);
+}
+
 // ---------------- kernels ----------------
 
 // view[0..15] = inverse view-projection (zero when singular), view[16] = 1 when
@@ -522,7 +551,7 @@ __global__ void __launch_bounds__(kBlock) k_preprocess_e3(const StepParams* __re
         }
         bool vis = false;
         float g2s[16], ci[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, mo[3] = {0.f, 0.f, 0.f};
-        float pix_x = 0.f, pix_y = 0.f, depth = 0.f, opacity = 0.f, rgb[3] = {0.f, 0.f, 0.f};
+        float pix_x = 0.f, pix_y = 0.f, depth = 0.f, opacity = 0.f, rgb[3] = {0.f, 0.f, 0.f}, thr_k = 0.f;
         int radius = 0, rmn[2] = {0, 0}, rmx[2] = {0, 0};
         float pv[3];
         xform4x3(p, cam.view_matrix, pv);
@@ -537,6 +566,7 @@ __global__ void __launch_bounds__(kBlock) k_preprocess_e3(const StepParams* __re
             opacity *= dil;
             if (opacity < kAlphaMin) break;                                   // :82-84
             const float thr = log_ref(opacity / kAlphaMin);
+            thr_k = thr;
             const float cutoff = fmin_ref(11.11f, 2.0f * thr);
             float R[3][3];
             quat2mat_e3(q, R);
@@ -619,7 +649,8 @@ __global__ void __launch_bounds__(kBlock) k_preprocess_e3(const StepParams* __re
         rc[3] = make_float4(ci[0], ci[1], ci[2], ci[3]);
         rc[4] = make_float4(ci[4], ci[5], mo[0], mo[1]);
         rc[5] = make_float4(mo[2], opacity, depth, rgb[0]);
-        rc[6] = make_float4(rgb[1], rgb[2], 0.f, 0.f);
+        rc[6] = make_float4(rgb[1], rgb[2], thr_k, 0.f);
+        rc[7] = vis ? e3_skip_box(g2s, thr_k) : make_float4(1e30f, -1e30f, 1e30f, -1e30f);
     }
     scan_and_emit(sm, blk, (unsigned)i, cnt, cnt, rx, ry, rw, dbits, sp.grid_x, pr, ctrl, sp.spin_limit, nullptr,
                   nullptr, 0, 0u, -1, RayDepth{e.ci, e.mo, e.tdir});
@@ -686,6 +717,9 @@ __global__ void __launch_bounds__(kE3Threads) k_raster_e3(const StepParams* __re
         pixel_dir_e3((float)x + 0.5f, (float)y + 0.5f, W, H, ivp, sp.cam.cam_pos, ray);
     }
     const float fpx = (float)x + 0.5f, fpy = (float)y + 0.5f;
+    // this warp's 16x2 strip of pixel indices, for the per-Gaussian skip boxes
+    const float wx0 = (float)(tx * kTile), wx1 = wx0 + (float)(kTile - 1);
+    const float wy0 = (float)(ty * kTile + 2 * (tid >> 5)), wy1 = wy0 + 1.0f;
     float T = 1.0f, C0 = 0.0f, C1 = 0.0f, C2 = 0.0f;
     int cnt = 0, kc = 0, head = 0;
     bool done = !inside;
@@ -699,16 +733,29 @@ __global__ void __launch_bounds__(kE3Threads) k_raster_e3(const StepParams* __re
         __syncthreads();
         const int nb = (int)min((unsigned)kE3Batch, re - b);
         for (int k = 0; k < nb && !done; k++) {
+            if (box_misses(s_rec[7 * kE3Batch + k], wx0, wx1, wy0, wy1)) continue;   // warp-uniform
             const float4 r0 = s_rec[k], r1 = s_rec[kE3Batch + k], r3 = s_rec[2 * kE3Batch + k];
             const float plx[4] = {r0.x - r3.x * fpx, r0.y - r3.y * fpx, r0.z - r3.z * fpx, r0.w - r3.w * fpx};
             const float ply[4] = {r1.x - r3.x * fpy, r1.y - r3.y * fpy, r1.z - r3.z * fpy, r1.w - r3.w * fpy};
+            {
+                // screening: the squared distance with one fast division is within a
+                // few ulps of the exact one (all terms are non-negative); beyond
+                // 2 thr + 1e-3 alpha is certainly below 1/255
+                const float dx = plx[1] * ply[2] - plx[2] * ply[1];
+                const float dy = plx[2] * ply[0] - plx[0] * ply[2];
+                const float dz = plx[0] * ply[1] - plx[1] * ply[0];
+                const float mx = plx[3] * ply[0] - plx[0] * ply[3];
+                const float my = plx[3] * ply[1] - plx[1] * ply[3];
+                const float mz = plx[3] * ply[2] - plx[2] * ply[3];
+                const float dd = dx * dx + dy * dy + dz * dz;
+                const float sm = mx * mx + my * my + mz * mz;
+                const float lim = 2.0f * s_rec[6 * kE3Batch + k].z + 1e-3f;
+                if (sm < 1e30f && dd > 1e-30f && dd < 1e30f && __fdividef(sm, dd) * (1.0f - 1e-5f) > lim) continue;
+            }
             const float power = -0.5f * ray_dist_e3(plx, ply);
             if (power > 0.0f) continue;
             const float4 r5 = s_rec[5 * kE3Batch + k];
             const float o = r5.y;
-            // screening on the fast exp (its relative error is far below the
-            // 4e-6 band wherever o*exp(power) is near 1/255), then exact exp
-            if (o * __expf(power) < kAlphaMin * (1.0f - 4e-6f)) continue;
             const float alpha = fmin_ref(0.99f, o * exp_ref(power));
             if (alpha < kAlphaMin) continue;
             const float4 r3c = s_rec[3 * kE3Batch + k], r4 = s_rec[4 * kE3Batch + k];

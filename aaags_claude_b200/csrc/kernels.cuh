@@ -70,9 +70,10 @@ struct GradPtrs {
 
 // Host arrays in PreprocessOutput layout, on the device (export / import).
 // Per-Gaussian arrays of the 3D-evaluation mode (RenderConfig::eval_3D).
+constexpr int kE3Rec = 8;   // float4s per raster record
 struct E3Ptrs {
-    float4* rec;      // [N*7] raster record: gauss2screen rows 0, 1, 3; cov3D_inv; mean_offset,
-                      // opacity, depth, rgb
+    float4* rec;      // [N*kE3Rec] raster record: gauss2screen rows 0, 1, 3; cov3D_inv; mean_offset,
+                      // opacity, depth, rgb, alpha threshold; skip box
     float* g2s;       // [N*16] gauss2screen (row-major), zero for culled Gaussians
     float* ci;        // [N*6] inverse 3D covariance (upper triangle)
     float* mo;        // [N*3] position - camera position

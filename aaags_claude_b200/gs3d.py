@@ -289,9 +289,10 @@ class Context:
         self._chk(self.L.gs3dc_rasterize(self.h, _ref(cam), _ref(cfg), _p(img), _p(T), _p(nc)))
         return img, T, nc
 
-    def render(self, cam, cfg) -> np.ndarray:
-        img = np.zeros(3 * cam.width * cam.height, np.float32)
-        self._chk(self.L.gs3dc_render(self.h, None, _ref(cam), _ref(cfg), _p(img)))
+    def render(self, cam, cfg, download: bool = True) -> np.ndarray | None:
+        """Renderer::render of the device model; download=False leaves the image on the device."""
+        img = np.zeros(3 * cam.width * cam.height, np.float32) if download else None
+        self._chk(self.L.gs3dc_render(self.h, None, _ref(cam), _ref(cfg), _p(img) if download else None))
         return img
 
     def raster_backward(self, cam, cfg, d_image: np.ndarray) -> dict:

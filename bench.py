@@ -72,6 +72,10 @@ def _args(argv=None):
                     help="timed steps of the 64-view step (0: skip it)")
     ap.add_argument("--autotune", type=int, default=1,
                     help="1: let the library tune the rasterisers' threads per tile during the warm-up")
+    ap.add_argument("--eval3d", type=int, default=1,
+                    help="1: also time the 3D-evaluation (eval_3D) render of 100k Gaussians at 640x480")
+    ap.add_argument("--only-eval3d", dest="only_eval3d", action="store_true",
+                    help="print only the eval_3D render measurement (profiling runs)")
     ap.add_argument("--only-batched", dest="only_batched", action="store_true",
                     help="print only the 64-view measurement (profiling runs)")
     return ap.parse_args(argv)
@@ -370,6 +374,10 @@ def run_ours(a) -> int:
     if a.only_batched:
         print(json.dumps({"metric": METRIC, "batched_64_views": measure_batched(a, local)}), flush=True)
         return 0
+    if a.only_eval3d:
+        print(json.dumps({"metric": METRIC, "eval3d_render": measure_eval3d(a, local, cpu=not a.no_cpu_baseline)}),
+              flush=True)
+        return 0
     dist = None
     if world > 1:
         import datetime
@@ -442,6 +450,8 @@ def run_ours(a) -> int:
         if world == 1 and a.batched_steps > 0 and _workload_name(a) == WORKLOAD:
             ctx.close()
             line["batched_64_views"] = measure_batched(a, local)
+        if world == 1 and a.eval3d and _workload_name(a) == WORKLOAD:
+            line["eval3d_render"] = measure_eval3d(a, local, cpu=not a.no_cpu_baseline)
         print(json.dumps(line), flush=True)
     ctx.close()
     if dist:
@@ -521,6 +531,79 @@ def measure_batched(a, local: int) -> dict:
             "plain_fp32_one_by_one": {"ms_per_64_views": round(ms_p, 3),
                                       "mpix_per_s": round(pix / 1e6 / (ms_p * 1e-3), 1)},
             "mpix_ratio": round(ms_p / ms_b, 3)}
+
+
+# ---------------------------------------------------------------- 3D-evaluation render
+def measure_eval3d(a, local: int, cpu: bool) -> dict:
+    """Renderer::render in the 3D-evaluation mode (eval_3D: gauss2screen, per-tile
+    ray-depth keys, 16-entry buffered blend) on 100k Gaussians at 640x480, device
+    image (value) and downloaded image (e2e), with the reference's own CPU render of
+    the same scene beside it."""
+    import torch
+    from aaags_claude_b200 import gs3d
+    from aaags_claude_b200 import scenes as S
+    w = S.config_render_eval3d()
+    cam = w.cameras[0]
+    cfg = S.render_config(False)
+    cfg.eval_3D = True
+    ctx = gs3d.Context(local)
+    ctx.set_raw_params(w.scene)
+    stream = torch.cuda.ExternalStream(ctx.stream_handle(), device=f"cuda:{local}")
+    for _ in range(3):
+        ctx.render(cam, cfg, download=False)
+    pairs = ctx.stat(gs3d.STAT_TOTAL_PAIRS)
+    launches = ctx.stat(gs3d.STAT_KERNELS_LAST)
+    steps = 20
+
+    def timed(download: bool) -> float:
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            ctx.render(cam, cfg, download=download)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    ms = timed(False)
+    ms_e2e = timed(True)
+    ctx.close()
+    px = cam.width * cam.height
+    out = {"workload": w.name, "gaussians": w.scene.count, "width": cam.width, "height": cam.height,
+           "tile_pairs": pairs, "steps": steps, "ms_per_render": round(ms, 4),
+           "renders_per_s": round(1e3 / ms, 1), "mpix_per_s": round(px / 1e6 / (ms * 1e-3), 1),
+           "e2e": {"renders_per_s": round(1e3 / ms_e2e, 1), "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 3 * px * 4},
+           "gpu_launches_per_render": launches}
+    if cpu:
+        out["cpu_reference"] = cpu_render_eval3d(w, cam, cfg)
+    return out
+
+
+def cpu_render_eval3d(w, cam, cfg) -> dict | None:
+    """One reference Renderer::render of the eval_3D workload (oracle/_ref) on 1 host core."""
+    from oracle import pyoracle as O
+    import ctypes
+    act = O.activate(w.scene)
+    g = O.gaussians_struct(w.scene, act)
+    img = np.zeros(3 * cam.width * cam.height, np.float32)
+    if O.have_ref():
+        L = O.lib_ref()
+        r = L.ref_renderer_create(ctypes.c_size_t(4 << 30))
+        t0 = time.perf_counter()
+        rc = L.ref_renderer_render(r, ctypes.byref(g), ctypes.byref(cam), ctypes.byref(cfg), img.ctypes.data)
+        dt = time.perf_counter() - t0
+        L.ref_renderer_destroy(r)
+        if rc:
+            return None
+        kind = "reference"
+    else:
+        t0 = time.perf_counter()
+        O.forward_eval3d(w.scene, cam, cfg, "c", act=act)
+        dt = time.perf_counter() - t0
+        kind = "port"
+    return {"value": round(1.0 / dt, 4), "unit": "renders/s", "cores": 1, "kind": kind,
+            "sample": f"1 Renderer::render, eval_3D, {w.scene.count} Gaussians {cam.width}x{cam.height}: {dt:.2f} s"}
 
 
 # ---------------------------------------------------------------- reference arm

@@ -84,10 +84,10 @@ def test_invalid_arguments_are_rejected(ctx):
     with pytest.raises(gs3d.Gs3dError) as e:
         ctx.train_step(cam, gt, bad, S.train_config(), 0)
     assert e.value.status == gs3d.ERR_INVALID_ARG
-    ev = S.render_config(False)
-    ev.eval_3D = True
+    ev = S.render_config(True)
+    ev.eval_3D = True   # the 3D-evaluation mode renders only
     with pytest.raises(gs3d.Gs3dError) as e:
-        ctx.preprocess(cam, ev)
+        ctx.train_step(cam, gt, ev, S.train_config(), 0)
     assert e.value.status == gs3d.ERR_INVALID_ARG
     with pytest.raises(gs3d.Gs3dError) as e:
         ctx.sort_pairs(np.array([5 << 32], np.uint64), np.array([0], np.uint32), 2)
