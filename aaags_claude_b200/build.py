@@ -31,6 +31,7 @@ SOURCES = {
     "plain.cu": ["-fmad=false", "-prec-div=true", "-prec-sqrt=true"],
     "raster_bwd.cu": [],   # gradients: FMA contraction allowed
     "chosen.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"],   # reduced-storage form: fast math
+    "density.cu": ["-fmad=false", "-prec-div=true", "-prec-sqrt=true"],   # density control: reference rounding
     "sort.cu": [],
     "sort_static.cu": [],
     "capi.cu": [],

@@ -98,6 +98,13 @@ struct gs3dc_ctx {
     DevBuf<float> e3_g2s, e3_ci, e3_mo, e3_view, filt3d;
     bool have_filt3d = false;   // the activated model came with GaussianData::filter_3D
     bool mode_e3 = false;       // the current screen records and pairs are of the 3D mode
+    // adaptive density control (the trainer's DensityController): statistics + scratch
+    DevBuf<float> dc_accum, dc_denom;
+    DevBuf<int> dc_maxr, dc_clone, dc_split, dc_crank, dc_srank, dc_src, dc_keep, dc_out, dc_sums, dc_radii_in;
+    DevBuf<float> dc_dm_in;              // host d_means2D uploaded by gs3dc_density_accumulate
+    DevBuf<float> dc_t[5], dc_new[5];   // post-split and final parameter arrays (pos, sc, rot, sh, op)
+    int dc_n = 0;                        // Gaussians the statistics describe
+    unsigned long long dc_rng = 12345ull;   // the split sampler's LCG state (density_controller.h)
     // control block + preprocess scan descriptors (one memset)
     DevBuf<unsigned char> ctrl_region;
     Control* ctrl = nullptr;
@@ -1107,6 +1114,9 @@ int gs3dc_set_option(gs3dc_ctx* c, int option, int64_t value) {
             CK(cudaStreamSynchronize(c->stream));
             return GS3DC_OK;
         }
+        case GS3DC_OPT_DENSITY_SEED:
+            c->dc_rng = (unsigned long long)value;
+            return GS3DC_OK;
         case GS3DC_OPT_SPIN_LIMIT:
             if (value <= 0) return fail(c, GS3DC_ERR_INVALID_ARG, "spin limit must be positive");
             c->spin_limit = (unsigned)value;
@@ -1149,6 +1159,7 @@ int gs3dc_get_stat(gs3dc_ctx* c, int stat, int64_t* value) {
         case GS3DC_STAT_SORT_PASSES: *value = c->sort_passes; return GS3DC_OK;
         case GS3DC_STAT_GRAPH_REPLAYS: *value = c->graph_replays; return GS3DC_OK;
         case GS3DC_STAT_ADAM_STEP: *value = c->adam_step; return GS3DC_OK;
+        case GS3DC_STAT_NUM_GAUSSIANS: *value = c->N; return GS3DC_OK;
         default: return fail(c, GS3DC_ERR_INVALID_ARG, "unknown stat %d", stat);
     }
 }
@@ -1179,6 +1190,7 @@ int gs3dc_set_raw_params(gs3dc_ctx* c, const gs3d_raw_params* r) {
     if (rc) return rc;
     c->model_raw = true;
     c->have_filt3d = false;
+    c->dc_n = 0;   // a new model: the density statistics restart
     if ((rc = ensure_adam(c))) return rc;
     if ((rc = zero_adam(c))) return rc;
     c->chosen_ready = false;
@@ -1948,4 +1960,245 @@ int gs3dc_load_state(gs3dc_ctx* c, const char* path) {
     return GS3DC_OK;
 }
 
+
+// ---- adaptive density control ----
+
+// The controller's LCG advanced n steps on the host (s -> a s + c, mod 2^64).
+static unsigned long long lcg_advance(unsigned long long s, unsigned long long n) {
+    unsigned long long a = 6364136223846793005ULL, cc = 1442695040888963407ULL, ja = 1ULL, jc = 0ULL;
+    while (n) {
+        if (n & 1ULL) {
+            ja = a * ja;
+            jc = a * jc + cc;
+        }
+        cc = a * cc + cc;
+        a = a * a;
+        n >>= 1;
+    }
+    return ja * s + jc;
+}
+
+static DensityPtrs dc_ptrs(gs3dc_ctx* c) {
+    return {c->dc_accum.p, c->dc_denom.p, c->dc_maxr.p, c->dc_clone.p, c->dc_split.p, c->dc_crank.p,
+            c->dc_srank.p, c->dc_src.p, c->dc_keep.p, c->dc_out.p, c->dc_sums.p};
+}
+
+// DensityController::reset (density_controller.cpp:22-26): zeroed statistics for N.
+static int dc_reset(gs3dc_ctx* c, int N) {
+    const size_t n = N > 0 ? (size_t)N : 1;
+    CK(c->dc_accum.ensure(n));
+    CK(c->dc_denom.ensure(n));
+    CK(c->dc_maxr.ensure(n));
+    CK(cudaMemsetAsync(c->dc_accum.p, 0, n * 4, c->stream));
+    CK(cudaMemsetAsync(c->dc_denom.p, 0, n * 4, c->stream));
+    CK(cudaMemsetAsync(c->dc_maxr.p, 0, n * 4, c->stream));
+    c->dc_n = N;
+    return GS3DC_OK;
+}
+
+// Exclusive scan of n int flags into out; returns the total through *total (synchronises).
+static int dc_scan(gs3dc_ctx* c, const int* in, int* out, int n, int* total) {
+    const size_t nb = ((size_t)n + 1023) / 1024;
+    CK(c->dc_sums.ensure(nb + 1));
+    CK(cudaMemsetAsync(c->dc_sums.p, 0, (nb + 1) * 4, c->stream));
+    CK(launch_scan_int(c->stream, in, out, c->dc_sums.p, n));
+    CK(cudaMemcpyAsync(total, c->dc_sums.p + nb, 4, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return GS3DC_OK;
+}
+
+// The statistics pass of Trainer::step_with_densify (trainer.cpp:113-145): forward
+// with the fused L1 and the raster backward of the current model, then the
+// accumulation of |d_means2D| and the radii.  The target sits at gt_dev.
+static int dc_stats_pass(gs3dc_ctx* c, const gs3d_camera* cam, const gs3d_render_config* cfg,
+                  const gs3d_train_config* tc, int iteration, const float* gt_dev) {
+    int rc;
+    for (int attempt = 0; attempt < 3; attempt++) {
+        if ((rc = push_params(c, cam, cfg, tc, iteration, gt_dev))) return rc;
+        if ((rc = seq_train_front(c))) return rc;
+        const int w = c->sorted_which;
+        CK(launch_raster_fwd_plain(c->stream, c->sp_dev, c->num_tiles, true, c->ranges.p, c->tile_order.p,
+                                   c->vals[w].p, screen_ptrs(c, false), pixel_ptrs(c), c->ctrl, c->fwd_ppt));
+        CK(launch_raster_bwd_plain(c->stream, c->sp_dev, c->num_tiles, true, c->ranges.p, c->tile_order.p,
+                                   c->vals[w].p, screen_ptrs(c, false), pixel_ptrs(c), rgrad_ptrs(c), c->ctrl,
+                                   c->bwd_ppt));
+        if ((rc = read_control(c))) return rc;
+        if (c->persist_host->sticky_overflow) {
+            if ((rc = acknowledge_overflow(c))) return rc;
+            const unsigned long long P = c->ctrl_host->total_pairs;
+            // the raster gradients of an overflowed pass are discarded
+            const size_t n = (size_t)c->N;
+            CK(cudaMemsetAsync(c->dm2.p, 0, 2 * n * 4, c->stream));
+            CK(cudaMemsetAsync(c->dcon.p, 0, 3 * n * 4, c->stream));
+            CK(cudaMemsetAsync(c->drgb.p, 0, 3 * n * 4, c->stream));
+            CK(cudaMemsetAsync(c->dop.p, 0, n * 4, c->stream));
+            if ((rc = ensure_pairs(c, P + P / 2 + 4096, c->num_tiles))) return rc;
+            continue;
+        }
+        if (c->dc_n != c->N && (rc = dc_reset(c, c->N))) return rc;
+        CK(launch_dc_accumulate(c->stream, c->N, c->dm2.p, c->radius.p, dc_ptrs(c), true));
+        // the other raster-gradient accumulators start at zero for the next step
+        const size_t n = (size_t)c->N;
+        CK(cudaMemsetAsync(c->dcon.p, 0, 3 * n * 4, c->stream));
+        CK(cudaMemsetAsync(c->drgb.p, 0, 3 * n * 4, c->stream));
+        CK(cudaMemsetAsync(c->dop.p, 0, n * 4, c->stream));
+        c->have_screen = c->have_pairs = c->have_sorted = c->have_raster = c->have_rgrad = false;
+        return GS3DC_OK;
+    }
+    return fail(c, GS3DC_ERR_PAIR_OVERFLOW, "tile-pair capacity kept overflowing in the statistics pass");
+}
+
+int gs3dc_density_accumulate(gs3dc_ctx* c, const float* d_means2D, const int* radii) {
+    if (!c) return GS3DC_ERR_INVALID_ARG;
+    int rc;
+    if ((rc = require_model(c)) || (rc = require_plain(c, "density control"))) return rc;
+    CK(cudaSetDevice(c->device));
+    const size_t n = (size_t)c->N;
+    if (c->dc_n != c->N && (rc = dc_reset(c, c->N))) return rc;
+    if (n == 0) return GS3DC_OK;
+    float* dm = nullptr;
+    const int* rd = nullptr;
+    if (d_means2D) {
+        CK(c->dc_dm_in.ensure(2 * n));
+        CK(cudaMemcpyAsync(c->dc_dm_in.p, d_means2D, 2 * n * 4, cudaMemcpyHostToDevice, c->stream));
+        dm = c->dc_dm_in.p;
+        if (radii) {
+            CK(c->dc_radii_in.ensure(n));
+            CK(cudaMemcpyAsync(c->dc_radii_in.p, radii, n * 4, cudaMemcpyHostToDevice, c->stream));
+            rd = c->dc_radii_in.p;
+        }
+    } else {
+        if (!c->have_rgrad)
+            return fail(c, GS3DC_ERR_STATE, "gs3dc_density_accumulate(NULL) needs gs3dc_raster_backward first");
+        dm = c->dm2.p;
+        rd = c->radius.p;
+    }
+    CK(launch_dc_accumulate(c->stream, c->N, dm, rd, dc_ptrs(c), false));
+    CK(cudaStreamSynchronize(c->stream));
+    return GS3DC_OK;
+}
+
+int gs3dc_densify_and_prune(gs3dc_ctx* c, const gs3d_densify_config* dcfg, float scene_extent, int* new_count) {
+    if (!c || !dcfg) return GS3DC_ERR_INVALID_ARG;
+    int rc;
+    if ((rc = require_model(c)) || (rc = require_plain(c, "density control"))) return rc;
+    if (!c->model_raw) return fail(c, GS3DC_ERR_STATE, "density control needs a raw model (gs3dc_set_raw_params)");
+    CK(cudaSetDevice(c->device));
+    if ((rc = gs3dc_synchronize(c))) return rc;
+    const int N = c->N;
+    if (N == 0) {
+        if (new_count) *new_count = 0;
+        return GS3DC_OK;
+    }
+    if (c->dc_n != N && (rc = dc_reset(c, N))) return rc;   // no statistics: every average is zero
+    const size_t n = (size_t)N;
+    const int mc3 = c->max_coeffs * 3;
+    CK(c->dc_clone.ensure(n));
+    CK(c->dc_split.ensure(n));
+    CK(c->dc_crank.ensure(n));
+    CK(c->dc_srank.ensure(n));
+    // clone / split classes and their ranks (density_controller.cpp:45-124)
+    const float size_thr = 0.01f * scene_extent;
+    CK(launch_dc_classify(c->stream, N, c->sc.p, dc_ptrs(c), dcfg->grad_threshold, size_thr));
+    int n_c = 0, n_s = 0;
+    if ((rc = dc_scan(c, c->dc_clone.p, c->dc_crank.p, N, &n_c)) ||
+        (rc = dc_scan(c, c->dc_split.p, c->dc_srank.p, N, &n_s)))
+        return rc;
+    const int M = N + n_c + n_s;
+    const size_t m = (size_t)M;
+    CK(c->dc_src.ensure(m));
+    CK(c->dc_keep.ensure(m));
+    CK(c->dc_out.ensure(m));
+    const size_t widths[5] = {3, 3, 4, (size_t)mc3, 1};
+    for (int k = 0; k < 5; k++) CK(c->dc_t[k].ensure(widths[k] * m));
+    const ModelPtrs t{c->dc_t[0].p, c->dc_t[1].p, c->dc_t[2].p, c->dc_t[3].p, c->dc_t[4].p};
+    const float log_factor = std::log(0.8f * 2.0f);   // density_controller.cpp:105, the reference's libm
+    CK(launch_dc_expand(c->stream, N, n_c, n_s, model_ptrs(c), mc3, dc_ptrs(c), t, c->dc_rng, log_factor));
+    // prune (density_controller.cpp:144-170) and compact
+    CK(launch_dc_keep(c->stream, M, N, t, dc_ptrs(c), dcfg->min_opacity, dcfg->max_screen_size,
+                      0.1f * scene_extent));
+    int kept = 0;
+    if ((rc = dc_scan(c, c->dc_keep.p, c->dc_out.p, M, &kept))) return rc;
+    const size_t nn = kept > 0 ? (size_t)kept : 1;
+    for (int k = 0; k < 5; k++) CK(c->dc_new[k].ensure(widths[k] * nn));
+    const ModelPtrs o{c->dc_new[0].p, c->dc_new[1].p, c->dc_new[2].p, c->dc_new[3].p, c->dc_new[4].p};
+    CK(launch_dc_compact(c->stream, M, kept, t, mc3, dc_ptrs(c), o));
+    CK(cudaStreamSynchronize(c->stream));
+    c->dc_rng = lcg_advance(c->dc_rng, 12ull * (unsigned long long)n_s);
+    // the new model replaces the old arrays
+    std::swap(c->pos.p, c->dc_new[0].p);
+    std::swap(c->pos.n, c->dc_new[0].n);
+    std::swap(c->sc.p, c->dc_new[1].p);
+    std::swap(c->sc.n, c->dc_new[1].n);
+    std::swap(c->rot.p, c->dc_new[2].p);
+    std::swap(c->rot.n, c->dc_new[2].n);
+    std::swap(c->sh.p, c->dc_new[3].p);
+    std::swap(c->sh.n, c->dc_new[3].n);
+    std::swap(c->op.p, c->dc_new[4].p);
+    std::swap(c->op.n, c->dc_new[4].n);
+    drop_graphs(c);
+    if ((rc = ensure_model(c, kept, c->max_coeffs))) return rc;
+    c->N = kept;
+    const size_t kn = (size_t)kept;
+    if (kn) {   // raster-gradient accumulators start at zero
+        CK(cudaMemsetAsync(c->dm2.p, 0, 2 * kn * 4, c->stream));
+        CK(cudaMemsetAsync(c->dcon.p, 0, 3 * kn * 4, c->stream));
+        CK(cudaMemsetAsync(c->drgb.p, 0, 3 * kn * 4, c->stream));
+        CK(cudaMemsetAsync(c->dop.p, 0, kn * 4, c->stream));
+    }
+    if ((rc = dc_reset(c, kept))) return rc;
+    // Trainer::step_with_densify resets the optimiser when the count changed (trainer.cpp:157-161)
+    if (kept != N && ((rc = ensure_adam(c)) || (rc = zero_adam(c)))) return rc;
+    c->have_screen = c->have_pairs = c->have_sorted = c->have_raster = c->have_rgrad = c->have_grads = false;
+    c->have_step_grads = false;
+    CK(cudaStreamSynchronize(c->stream));
+    if (new_count) *new_count = kept;
+    return GS3DC_OK;
+}
+
+int gs3dc_reset_opacity(gs3dc_ctx* c) {
+    if (!c) return GS3DC_ERR_INVALID_ARG;
+    int rc;
+    if ((rc = require_model(c)) || (rc = require_plain(c, "density control"))) return rc;
+    if (!c->model_raw) return fail(c, GS3DC_ERR_STATE, "gs3dc_reset_opacity needs a raw model");
+    CK(cudaSetDevice(c->device));
+    // inverse_sigmoid(0.01) with the reference's libm (density_controller.cpp:198)
+    CK(launch_fill(c->stream, c->op.p, c->N, std::log(0.01f / 0.99f)));
+    CK(cudaStreamSynchronize(c->stream));
+    return GS3DC_OK;
+}
+
+int gs3dc_train_step_densify(gs3dc_ctx* c, const gs3d_camera* cam, const float* gt, int gt_on_device,
+                             const gs3d_render_config* cfg, const gs3d_train_config* tc,
+                             const gs3d_densify_config* dcfg, float scene_extent, int iteration, float* loss,
+                             int* n_gaussians) {
+    if (!c || !gt || !tc || !dcfg) return GS3DC_ERR_INVALID_ARG;
+    int rc;
+    if ((rc = check_config(c, cam, cfg)) || (rc = require_model(c)) ||
+        (rc = require_plain(c, "gs3dc_train_step_densify")))
+        return rc;
+    CK(cudaSetDevice(c->device));
+    const float* gt_dev = gt;
+    if (!gt_on_device) {   // one device copy serves the step and the statistics pass
+        const size_t np = (size_t)cam->width * cam->height;
+        CK(c->gt.ensure(3 * np));
+        CK(cudaMemcpyAsync(c->gt.p, gt, 3 * np * 4, cudaMemcpyHostToDevice, c->stream));
+        gt_dev = c->gt.p;
+    }
+    float l = 0.0f;
+    if ((rc = gs3dc_train_step(c, cam, gt_dev, 1, cfg, tc, iteration, &l))) return rc;
+    if ((rc = dc_stats_pass(c, cam, cfg, tc, iteration, gt_dev))) return rc;
+    if (dcfg->enabled && iteration >= dcfg->densify_from_iter && iteration < dcfg->densify_until_iter &&
+        dcfg->densify_interval > 0 && iteration % dcfg->densify_interval == 0) {
+        if ((rc = gs3dc_densify_and_prune(c, dcfg, scene_extent, nullptr))) return rc;
+    }
+    if (dcfg->enabled && dcfg->opacity_reset_interval > 0 && iteration > 0 &&
+        iteration % dcfg->opacity_reset_interval == 0) {
+        if ((rc = gs3dc_reset_opacity(c))) return rc;
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    if (loss) *loss = l;
+    if (n_gaussians) *n_gaussians = c->N;
+    return GS3DC_OK;
+}
 }  // extern "C"

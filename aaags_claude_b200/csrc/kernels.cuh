@@ -69,6 +69,32 @@ struct GradPtrs {
 };
 
 // Host arrays in PreprocessOutput layout, on the device (export / import).
+// Adaptive density control: statistics and the scratch of densify_and_prune.
+struct DensityPtrs {
+    float* accum;     // [N] sum of |d_means2D|
+    float* denom;     // [N] steps counted
+    int* max_radii;   // [N] largest screen radius seen
+    int* clone;       // [N] flags
+    int* split;       // [N]
+    int* crank;       // [N] exclusive rank among the clones
+    int* srank;       // [N] exclusive rank among the splits
+    int* src;         // [M] source Gaussian of each post-split entry; reused as the gather map
+    int* keep;        // [M] kept after pruning
+    int* out;         // [M] exclusive rank among the kept
+    int* sums;        // scan block sums (+ the grand total at the end)
+};
+
+cudaError_t launch_dc_accumulate(cudaStream_t st, int N, float* dm2, const int* radii, DensityPtrs d, bool clear);
+cudaError_t launch_scan_int(cudaStream_t st, const int* in, int* out, int* sums, int n);
+cudaError_t launch_dc_classify(cudaStream_t st, int N, const float* sc, DensityPtrs d, float threshold,
+                               float size_thr);
+cudaError_t launch_dc_expand(cudaStream_t st, int N, int n_c, int n_s, ModelPtrs m, int mc3, DensityPtrs d,
+                             ModelPtrs t, unsigned long long rng0, float log_factor);
+cudaError_t launch_dc_keep(cudaStream_t st, int M, int N, ModelPtrs t, DensityPtrs d, float min_opacity,
+                           int max_screen_size, float world_thr);
+cudaError_t launch_dc_compact(cudaStream_t st, int M, int new_n, ModelPtrs t, int mc3, DensityPtrs d, ModelPtrs out);
+cudaError_t launch_fill(cudaStream_t st, float* p, long long n, float v);
+
 // Per-Gaussian arrays of the 3D-evaluation mode (RenderConfig::eval_3D).
 constexpr int kE3Rec = 8;   // float4s per raster record
 struct E3Ptrs {

@@ -26,11 +26,13 @@ ERR_INVALID_ARG, ERR_CUDA, ERR_PAIR_OVERFLOW, ERR_DEVICE_TIMEOUT, ERR_NO_MODEL, 
 OPT_PAIR_CAPACITY, OPT_USE_GRAPH, OPT_FORM, OPT_SPIN_LIMIT, OPT_STAGE_TIMING, OPT_FUSED_ADAM = 1, 2, 3, 4, 5, 6
 NUM_STAGES = 8
 STAT_TOTAL_PAIRS, STAT_PAIR_CAPACITY, STAT_KERNELS_LAST, STAT_SORT_PASSES, STAT_GRAPH_REPLAYS, STAT_ADAM_STEP = range(1, 7)
+STAT_NUM_GAUSSIANS = 9
 STAT_FWD_PPT, STAT_BWD_PPT = 7, 8
 FORM_PLAIN_FP32, FORM_BF16, FORM_FP16 = 0, 1, 2
 OPT_SORT = 7
 OPT_KEEP_GRADIENTS = 8
 OPT_AUTOTUNE = 9
+OPT_DENSITY_SEED = 10
 SORT_DEPTH_FIRST, SORT_FULL_KEY = 0, 1
 
 _f = ctypes.POINTER(ctypes.c_float)
@@ -92,6 +94,11 @@ def load_library(path: str = LIB_PATH):
         "gs3dc_selftest_bounded_wait": ([vp, ctypes.c_uint32], ctypes.c_int),
         "gs3dc_get_gradients": ([vp, vp, vp, vp, vp, vp], ctypes.c_int),
         "gs3dc_save_state": ([vp, ctypes.c_char_p], ctypes.c_int),
+        "gs3dc_density_accumulate": ([vp, vp, vp], ctypes.c_int),
+        "gs3dc_densify_and_prune": ([vp, vp, ctypes.c_float, vp], ctypes.c_int),
+        "gs3dc_reset_opacity": ([vp], ctypes.c_int),
+        "gs3dc_train_step_densify": ([vp, vp, vp, ctypes.c_int, vp, vp, vp, ctypes.c_float, ctypes.c_int, vp, vp],
+                                     ctypes.c_int),
         "gs3dc_load_state": ([vp, ctypes.c_char_p], ctypes.c_int),
         "gs3dc_train_step_batch": ([vp, ctypes.c_int, vp, vp, ctypes.c_int, vp, vp, ctypes.c_int, vp],
                                    ctypes.c_int),
@@ -332,6 +339,45 @@ class Context:
         self._chk(self.L.gs3dc_train_step_batch(self.h, len(cams), ctypes.byref(arr), gp, on_dev, _ref(cfg), _ref(tcfg),
                                                 int(iteration), ctypes.byref(loss) if want_loss else None))
         return float(loss.value) if want_loss else None
+
+    # ---- adaptive density control ----
+    def density_accumulate(self, d_means2D: np.ndarray | None = None, radii: np.ndarray | None = None):
+        """DensityController::accumulate_stats (host arrays, or None: the device's last raster backward)."""
+        d = None if d_means2D is None else np.ascontiguousarray(d_means2D, np.float32).reshape(-1)
+        r = None if radii is None else np.ascontiguousarray(radii, np.int32).reshape(-1)
+        self._chk(self.L.gs3dc_density_accumulate(self.h, _p(d), _p(r)))
+
+    def densify_and_prune(self, dcfg, scene_extent: float) -> int:
+        """DensityController::densify_and_prune on the device model; returns the new count."""
+        n = ctypes.c_int()
+        self._chk(self.L.gs3dc_densify_and_prune(self.h, _ref(dcfg), ctypes.c_float(scene_extent), ctypes.byref(n)))
+        self._model = ("raw", n.value, self._model[2])
+        return n.value
+
+    def reset_opacity(self):
+        self._chk(self.L.gs3dc_reset_opacity(self.h))
+
+    def train_step_densify(self, cam, gt, cfg, tcfg, dcfg, scene_extent: float, iteration: int,
+                           gt_device_ptr: int | None = None):
+        """Trainer::step_with_densify: (loss, Gaussian count afterwards)."""
+        loss, n = ctypes.c_float(), ctypes.c_int()
+        if gt_device_ptr is not None:
+            gptr, on_dev = ctypes.c_void_p(int(gt_device_ptr)), 1
+        else:
+            gt = np.ascontiguousarray(gt, np.float32)
+            gptr, on_dev = _p(gt), 0
+        self._chk(self.L.gs3dc_train_step_densify(self.h, _ref(cam), gptr, on_dev, _ref(cfg), _ref(tcfg), _ref(dcfg),
+                                                  ctypes.c_float(scene_extent), int(iteration), ctypes.byref(loss),
+                                                  ctypes.byref(n)))
+        self._model = ("raw", n.value, self._model[2])
+        return float(loss.value), n.value
+
+    def get_model(self, sh_degree: int = 3) -> S.Scene:
+        """The device's raw model as a new Scene (its current count)."""
+        n, k = self._model[1], self._model[2]
+        sc = S.Scene(np.zeros((n, 3), np.float32), np.zeros((n, 3), np.float32), np.zeros((n, 4), np.float32),
+                     np.zeros((n, k, 3), np.float32), np.zeros(n, np.float32), sh_degree)
+        return self.get_raw_params(sc)
 
     def save_state(self, path: str):
         """Model, optimiser moments and step counter to a file (gs3dc_save_state)."""

@@ -77,6 +77,34 @@ class TrainConfig(ctypes.Structure):
     ]
 
 
+class DensifyConfig(ctypes.Structure):
+    """Layout of ``gs3d_densify_config`` (= the reference's ``DensifyConfig``)."""
+
+    _fields_ = [
+        ("densify_from_iter", ctypes.c_int),
+        ("densify_until_iter", ctypes.c_int),
+        ("densify_interval", ctypes.c_int),
+        ("grad_threshold", ctypes.c_float),
+        ("min_opacity", ctypes.c_float),
+        ("percent_dense", ctypes.c_float),
+        ("opacity_reset_interval", ctypes.c_int),
+        ("max_screen_size", ctypes.c_int),
+        ("enabled", ctypes.c_bool),
+    ]
+
+
+def densify_config(**kw) -> DensifyConfig:
+    """DensifyConfig with the reference's defaults (train_types.h:71-81), overridden by kw."""
+    d = DensifyConfig()
+    vals = dict(densify_from_iter=500, densify_until_iter=15000, densify_interval=100, grad_threshold=0.0002,
+                min_opacity=0.005, percent_dense=0.01, opacity_reset_interval=3000, max_screen_size=20,
+                enabled=False)
+    vals.update(kw)
+    for k, v in vals.items():
+        setattr(d, k, v)
+    return d
+
+
 class GaussianData(ctypes.Structure):
     """Layout of ``gs3d_gaussians`` (= the reference's ``GaussianData``)."""
 

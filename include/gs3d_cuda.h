@@ -50,6 +50,8 @@ typedef struct gs3dc_ctx gs3dc_ctx;
 #define GS3DC_OPT_AUTOTUNE       9  /* 1: tune the rasterisers' threads per tile (pixels per thread 1 / 2 / 4) online:
                                        per workload shape the first 6 train steps try each setting twice (timed with
                                        events, un-captured) and the fastest forward / backward stay; 0 (default): 2 */
+#define GS3DC_OPT_DENSITY_SEED  10  /* state of the density controller's split sampler (LCG); 12345 at creation,
+                                        like DensityController::rng_state_ (density_controller.h:41) */
 
 /* Depth-first (default): the Gaussians are stably sorted by depth, their pairs
  * emitted in that order and stably sorted by the tile bits alone.  Full key:
@@ -78,6 +80,7 @@ typedef struct gs3dc_ctx gs3dc_ctx;
 #define GS3DC_STAT_ADAM_STEP      6  /* Adam step counter (AdamOptimizer::step_count) */
 #define GS3DC_STAT_FWD_PPT        7  /* pixels per thread of the forward rasteriser in the last train step */
 #define GS3DC_STAT_BWD_PPT        8  /* pixels per thread of the backward rasteriser in the last train step */
+#define GS3DC_STAT_NUM_GAUSSIANS  9  /* Gaussians of the device model (changes with density control) */
 
 /* Host arrays of PreprocessOutput + the per-Gaussian ForwardCache fields
  * (include/types.h:69-82, 97-107).  Any pointer may be NULL (not produced). */
@@ -271,6 +274,37 @@ int gs3dc_selftest_bounded_wait(gs3dc_ctx* ctx, uint32_t spin_limit);
  * may be NULL. */
 int gs3dc_get_gradients(gs3dc_ctx* ctx, float* d_raw_positions, float* d_raw_scales,
                         float* d_raw_rotations, float* d_raw_sh_coeffs, float* d_raw_opacities);
+
+/* ---- adaptive density control (plain FP32 form, raw model) ----
+ * The trainer's DensityController (src/density_controller.h:6-43,
+ * density_controller.cpp:9-204), its statistics kept on the device.
+ * gs3dc_density_accumulate: DensityController::accumulate_stats.  d_means2D
+ *   ([N*2] host) and radii ([N] host, may be NULL); with d_means2D == NULL the
+ *   device's d_means2D of the last gs3dc_raster_backward and the radii of the
+ *   last gs3dc_preprocess are used.  The statistics restart when N changes
+ *   and with every gs3dc_set_raw_params.
+ * gs3dc_densify_and_prune: DensityController::densify_and_prune: clone, split
+ *   (children appended after the clones, sampled from the controller's LCG,
+ *   seed 12345 per context), prune, compact; the Adam moments and step reset
+ *   when the count changes, like Trainer::step_with_densify (trainer.cpp:152-163).
+ *   *new_count = the new N (read the model with gs3dc_get_raw_params and
+ *   GS3DC_STAT_NUM_GAUSSIANS).  Every split child is kept: the reference's
+ *   compaction reads its removal mask past the end for them
+ *   (density_controller.cpp:78, train_types.h:119-124), so which survive
+ *   there depends on heap contents.
+ * gs3dc_reset_opacity: DensityController::reset_opacity (all raw opacities =
+ *   inverse_sigmoid(0.01)).
+ * gs3dc_train_step_densify: Trainer::step_with_densify (trainer.cpp:72-175): a
+ *   train step, the statistics pass (forward + raster backward of the updated
+ *   model), densify_and_prune on its iterations, opacity reset on its
+ *   iterations; *n_gaussians = the count afterwards. */
+int gs3dc_density_accumulate(gs3dc_ctx* ctx, const float* d_means2D, const int* radii);
+int gs3dc_densify_and_prune(gs3dc_ctx* ctx, const gs3d_densify_config* cfg, float scene_extent, int* new_count);
+int gs3dc_reset_opacity(gs3dc_ctx* ctx);
+int gs3dc_train_step_densify(gs3dc_ctx* ctx, const gs3d_camera* cam, const float* gt, int gt_on_device,
+                             const gs3d_render_config* cfg, const gs3d_train_config* tcfg,
+                             const gs3d_densify_config* dcfg, float scene_extent, int iteration, float* loss,
+                             int* n_gaussians);
 
 /* Checkpoint / resume of the whole training state: the model in its current
  * form's storage (FP32, or the 16-bit arrays), the optimiser moments and the

@@ -13,6 +13,7 @@
  *   gs3d_render_config  <-> RenderConfig       include/types.h:57-66
  *   gs3d_raw_params     <-> RawGaussianParams  include/train_types.h:9-22
  *   gs3d_train_config   <-> TrainConfig        include/train_types.h:46-60
+ *   gs3d_densify_config <-> DensifyConfig      include/train_types.h:70-81
  *
  * Conventions kept from the reference:
  *   - all matrices are 4x4 column-major (GLM order);
@@ -94,6 +95,19 @@ typedef struct gs3d_train_config {
     float adam_beta2;
     float adam_eps;
 } gs3d_train_config;
+
+/* Adaptive density control (clone / split / prune, opacity reset). */
+typedef struct gs3d_densify_config {
+    int densify_from_iter;      /* 500 */
+    int densify_until_iter;     /* 15000 */
+    int densify_interval;       /* 100 */
+    float grad_threshold;       /* 0.0002 */
+    float min_opacity;          /* 0.005 */
+    float percent_dense;        /* 0.01 (the reference's controller uses 0.01 whatever this holds) */
+    int opacity_reset_interval; /* 3000 */
+    int max_screen_size;        /* 20 */
+    bool enabled;               /* false: opt-in */
+} gs3d_densify_config;
 
 #ifdef __cplusplus
 }

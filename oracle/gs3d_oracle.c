@@ -51,6 +51,9 @@
 /* ---------- 3D evaluation (eval_3D), float only ---------- */
 #include "gs3d_oracle_eval3d.inc"
 
+/* ---------- adaptive density control, float only ---------- */
+#include "gs3d_oracle_density.inc"
+
 /* ---------- binning: tile_binner_cpu.cpp:33-99 ---------- */
 
 /* Inclusive scan of tiles_touched (:33-42); returns total pairs. */

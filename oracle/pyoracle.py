@@ -280,6 +280,106 @@ def forward_eval3d(scene, cam, cfg, impl: str = "c", act: dict | None = None, ca
     raise RuntimeError("oracle forward: pair capacity retry failed")
 
 
+class DensityOracle:
+    """DensityController state (density_controller.cpp) over the C restatement:
+    per-Gaussian statistics, the split sampler's LCG state (12345 at start)."""
+
+    def __init__(self):
+        self.n = 0
+        self.rng = ctypes.c_uint64(12345)
+        self.reset(0)
+
+    def reset(self, n: int):
+        self.n = n
+        self.accum = np.zeros(n, np.float32)
+        self.denom = np.zeros(n, np.float32)
+        self.max_radii = np.zeros(n, np.int32)
+
+    def accumulate(self, d_means2D: np.ndarray, radii: np.ndarray | None, n: int):
+        if n != self.n:
+            self.reset(n)
+        d = np.ascontiguousarray(d_means2D, np.float32).reshape(-1)
+        r = None if radii is None else np.ascontiguousarray(radii, np.int32)
+        lib_c().orc_dc_accumulate(ctypes.c_int(n), _ptr(d, _f), None if r is None else _ptr(r, _i),
+                                  _ptr(self.accum, _f), _ptr(self.denom, _f), _ptr(self.max_radii, _i))
+
+    def densify(self, scene, cfg, extent: float):
+        """densify_and_prune on a Scene of raw parameters; returns the new Scene."""
+        from aaags_claude_b200.scenes import Scene
+        n, k = scene.count, scene.max_coeffs
+        mc3 = 3 * k
+        if self.n != n:
+            self.reset(n)
+        o = [np.zeros((2 * n, 3), np.float32), np.zeros((2 * n, 3), np.float32), np.zeros((2 * n, 4), np.float32),
+             np.zeros((2 * n, k, 3), np.float32), np.zeros(2 * n, np.float32)]
+        ins = [np.ascontiguousarray(x, np.float32) for x in
+               (scene.positions, scene.scales, scene.rotations, scene.sh, scene.opacities)]
+        m = lib_c().orc_dc_densify(ctypes.c_int(n), ctypes.c_int(mc3), *[_ptr(x, _f) for x in ins],
+                                   _ptr(self.accum, _f), _ptr(self.denom, _f), _ptr(self.max_radii, _i),
+                                   ctypes.c_float(cfg.grad_threshold), ctypes.c_float(cfg.min_opacity),
+                                   ctypes.c_int(cfg.max_screen_size), ctypes.c_float(extent),
+                                   ctypes.byref(self.rng), *[_ptr(x, _f) for x in o])
+        self.reset(m)
+        return Scene(o[0][:m].copy(), o[1][:m].copy(), o[2][:m].copy(), o[3][:m].copy(), o[4][:m].copy(),
+                     scene.sh_degree)
+
+    @staticmethod
+    def reset_opacity(scene):
+        op = np.ascontiguousarray(scene.opacities, np.float32)
+        lib_c().orc_dc_reset_opacity(ctypes.c_int(scene.count), _ptr(op, _f))
+        scene.opacities[:] = op
+
+
+class DensityRef:
+    """The reference's own DensityController on an OwnedRawParams (oracle/_ref)."""
+
+    def __init__(self):
+        L = lib_ref()
+        L.ref_dc_create.restype = ctypes.c_void_p
+        L.ref_dc_destroy.argtypes = [ctypes.c_void_p]
+        L.ref_dc_set_model.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.ref_dc_accumulate.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+        L.ref_dc_densify.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_float]
+        L.ref_dc_densify.restype = ctypes.c_int
+        L.ref_dc_reset_opacity.argtypes = [ctypes.c_void_p]
+        L.ref_dc_get_model.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.ref_dc_get_model.restype = ctypes.c_int
+        self.L = L
+        self.h = L.ref_dc_create()
+        self.count, self.k, self.deg = 0, 1, 0
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.ref_dc_destroy(self.h)
+            self.h = None
+
+    def set_model(self, scene):
+        raw = scene.raw_struct()
+        self.L.ref_dc_set_model(self.h, ctypes.addressof(raw))
+        self.count, self.k, self.deg = scene.count, scene.max_coeffs, scene.sh_degree
+
+    def accumulate(self, d_means2D: np.ndarray, radii: np.ndarray | None, n: int):
+        d = np.ascontiguousarray(d_means2D, np.float32).reshape(-1)
+        r = None if radii is None else np.ascontiguousarray(radii, np.int32)
+        self.L.ref_dc_accumulate(self.h, d.ctypes.data, None if r is None else r.ctypes.data, n)
+
+    def densify(self, cfg, extent: float) -> int:
+        self.count = self.L.ref_dc_densify(self.h, ctypes.addressof(cfg), ctypes.c_float(extent))
+        return self.count
+
+    def reset_opacity(self):
+        self.L.ref_dc_reset_opacity(self.h)
+
+    def model(self):
+        from aaags_claude_b200.scenes import Scene
+        n, k = self.count, self.k
+        sc = Scene(np.zeros((n, 3), np.float32), np.zeros((n, 3), np.float32), np.zeros((n, 4), np.float32),
+                   np.zeros((n, k, 3), np.float32), np.zeros(n, np.float32), self.deg)
+        raw = sc.raw_struct()
+        self.L.ref_dc_get_model(self.h, ctypes.addressof(raw))
+        return sc
+
+
 class AdamOracle:
     """Adam moments for the C oracle's train step (zero-initialised)."""
 

@@ -29,6 +29,7 @@
 #include "cpu/rasterizer_cpu.h"
 #include "cpu/rasterizer_backward_cpu.h"
 #include "cpu/preprocessor_backward_cpu.h"
+#include "density_controller.h"
 
 #include "gs3d_oracle.h"
 
@@ -37,6 +38,8 @@ static_assert(sizeof(RenderConfig) == sizeof(gs3d_render_config), "RenderConfig 
 static_assert(sizeof(GaussianData) == sizeof(gs3d_gaussians), "GaussianData layout");
 static_assert(sizeof(TrainConfig) == sizeof(gs3d_train_config), "TrainConfig layout");
 static_assert(sizeof(RawGaussianParams) == sizeof(gs3d_raw_params), "RawGaussianParams layout");
+static_assert(sizeof(DensifyConfig) == sizeof(gs3d_densify_config), "DensifyConfig layout");
+static_assert(offsetof(DensifyConfig, enabled) == offsetof(gs3d_densify_config, enabled), "DensifyConfig layout");
 
 namespace {
 
@@ -146,6 +149,62 @@ int ref_forward_eval3d(const gs3d_gaussians* gp, const gs3d_camera* camp, const 
     std::memcpy(cov3D_inv, pre.cov3D_inv, sizeof(float) * 6 * (size_t)g.count);
     std::memcpy(mean_offset, pre.mean_offset, sizeof(float) * 3 * (size_t)g.count);
     return 0;
+}
+
+// DensityController with the model it densifies (density_controller.cpp):
+// accumulate, densify_and_prune and reset_opacity on an OwnedRawParams.
+struct DcHandle {
+    DensityController dc;
+    OwnedRawParams owned;
+};
+
+void* ref_dc_create(void) { return new (std::nothrow) DcHandle(); }
+void ref_dc_destroy(void* h) { delete static_cast<DcHandle*>(h); }
+
+void ref_dc_set_model(void* hp, const gs3d_raw_params* rawp) {
+    auto* h = static_cast<DcHandle*>(hp);
+    const RawGaussianParams& r = *reinterpret_cast<const RawGaussianParams*>(rawp);
+    h->owned.sh_degree = r.sh_degree;
+    h->owned.max_coeffs = r.max_coeffs;
+    const size_t n = (size_t)r.count, mc3 = (size_t)r.max_coeffs * 3;
+    h->owned.positions.assign(r.raw_positions, r.raw_positions + 3 * n);
+    h->owned.scales.assign(r.raw_scales, r.raw_scales + 3 * n);
+    h->owned.rotations.assign(r.raw_rotations, r.raw_rotations + 4 * n);
+    h->owned.sh_coeffs.assign(r.raw_sh_coeffs, r.raw_sh_coeffs + mc3 * n);
+    h->owned.opacities.assign(r.raw_opacities, r.raw_opacities + n);
+    // OwnedRawParams::append (train_types.h:108-116) pushes values read through
+    // pointers into the same vectors; a reallocating push_back would leave the
+    // rest of those reads dangling.  With room for the largest result
+    // (N + clones + 2 x splits <= 3N) no push_back reallocates.
+    h->owned.positions.reserve(9 * n);
+    h->owned.scales.reserve(9 * n);
+    h->owned.rotations.reserve(12 * n);
+    h->owned.sh_coeffs.reserve(3 * mc3 * n);
+    h->owned.opacities.reserve(3 * n);
+}
+
+void ref_dc_accumulate(void* hp, const float* d_means2D, const int* radii, int N) {
+    static_cast<DcHandle*>(hp)->dc.accumulate_stats(d_means2D, radii, N);
+}
+
+int ref_dc_densify(void* hp, const gs3d_densify_config* cfg, float extent) {
+    auto* h = static_cast<DcHandle*>(hp);
+    return h->dc.densify_and_prune(h->owned, *reinterpret_cast<const DensifyConfig*>(cfg), extent);
+}
+
+void ref_dc_reset_opacity(void* hp) { DensityController::reset_opacity(static_cast<DcHandle*>(hp)->owned); }
+
+// Copies the handle's model out (arrays sized for its count).
+int ref_dc_get_model(void* hp, gs3d_raw_params* rawp) {
+    auto* h = static_cast<DcHandle*>(hp);
+    RawGaussianParams& r = *reinterpret_cast<RawGaussianParams*>(rawp);
+    const size_t n = (size_t)h->owned.count(), mc3 = (size_t)h->owned.max_coeffs * 3;
+    std::memcpy(r.raw_positions, h->owned.positions.data(), 12 * n);
+    std::memcpy(r.raw_scales, h->owned.scales.data(), 12 * n);
+    std::memcpy(r.raw_rotations, h->owned.rotations.data(), 16 * n);
+    std::memcpy(r.raw_sh_coeffs, h->owned.sh_coeffs.data(), 4 * mc3 * n);
+    std::memcpy(r.raw_opacities, h->owned.opacities.data(), 4 * n);
+    return (int)n;
 }
 
 // RawGaussianParams::activate (train_types.cpp:6-36) into caller arrays.

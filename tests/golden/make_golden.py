@@ -14,7 +14,8 @@ Two kinds of fixtures, both produced by the reference itself:
   tiles, non-black background, antialiasing and scale modifier, SH degrees 0-2,
   a single Gaussian, every Gaussian culled, oversized splats; and the 3D-evaluation
   mode (eval_3D) on scenes that reach its frustum culling, camera-inside test and
-  view-space bounding box, with and without a 3D filter.
+  view-space bounding box, with and without a 3D filter; and the density
+  controller's densify_and_prune (clone, split, prune) and reset_opacity.
 
 It needs the reference tree at /root/reference (only this script reads it);
 the tests and the GPU runs read the committed copies.
@@ -146,6 +147,56 @@ def make_eval3d():
         print(name, "visible", int(vis.sum()), "P", r.total_pairs)
 
 
+def density_cases():
+    """(name, scene, accumulations [(d_means2D, radii)], DensifyConfig, extent) of the density fixtures.
+
+    The reference's split compaction reads its removal mask past the end for
+    the appended children (density_controller.cpp:78 with train_types.h:119-124);
+    the cases keep those reads inside the mask's last 64-bit word, which its
+    constructor zero-fills, so the reference's result is defined: either no
+    split at all, or N + clones = 650 (bits 650.. of a 704-bit mask) with three
+    splits."""
+    out = []
+    for name, seed, n, n_big, frac in (("density_clone_prune_3000", 41, 3000, 0, 0.3),
+                                       ("density_split_650_a", 42, 650, 3, 0.0),
+                                       ("density_split_650_b", 43, 650, 3, 0.0)):
+        rng = np.random.default_rng(seed)
+        sc = S.random_scene(n, seed=seed)
+        sc.scales[:] = np.minimum(sc.scales, np.log(0.0105))
+        big = rng.choice(n, n_big, replace=False)
+        sc.scales[big] = np.log(0.03)
+        sc.opacities[rng.random(n) < 0.03] = -7.0
+        hot = rng.random(n) < frac
+        hot[big] = True
+        acc = []
+        for _ in range(3):
+            d = rng.normal(0, 1e-5, (n, 2)).astype(np.float32)
+            d[hot] = rng.normal(0, 5e-4, (int(hot.sum()), 2)).astype(np.float32)
+            acc.append((d, rng.integers(0, 25, n).astype(np.int32)))
+        out.append((name, sc, acc, S.densify_config(enabled=True), 1.1))
+    return out
+
+
+def make_density():
+    dst = os.path.join(HERE, "seeded")
+    for name, sc, acc, cfg, extent in density_cases():
+        ref = O.DensityRef()
+        ref.set_model(sc)
+        for d, r in acc:
+            ref.accumulate(d, r, sc.count)
+        k = ref.densify(cfg, extent)
+        got = ref.model()
+        ref.reset_opacity()
+        reset_op = ref.model().opacities
+        np.savez_compressed(
+            os.path.join(dst, name + ".npz"), **scene_arrays(sc),
+            acc_d_means2D=np.stack([d for d, _ in acc]), acc_radii=np.stack([r for _, r in acc]),
+            cfg_bytes=np.frombuffer(bytes(cfg), np.uint8), extent=np.float32(extent), out_count=np.int32(k),
+            out_positions=got.positions, out_scales=got.scales, out_rotations=got.rotations, out_sh=got.sh,
+            out_opacities=got.opacities, out_reset_opacities=reset_op)
+        print(name, sc.count, "->", k)
+
+
 def _canon(keys, vals):
     o = np.lexsort((vals, keys))
     return keys[o], vals[o]
@@ -202,3 +253,4 @@ if __name__ == "__main__":
     copy_ref_fixtures()
     make_seeded()
     make_eval3d()
+    make_density()

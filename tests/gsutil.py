@@ -97,6 +97,20 @@ def load_eval3d(name: str):
     return sc, f3, cam, cfg, z
 
 
+def density_cases():
+    return sorted(f[:-4] for f in os.listdir(SEEDED) if f.startswith("density_"))
+
+
+def load_density(name: str):
+    """(scene, accumulations [(d_means2D, radii)], DensifyConfig, extent, fixture) of a density case."""
+    z = np.load(os.path.join(SEEDED, name + ".npz"))
+    sc = S.Scene(z["in_positions"].copy(), z["in_scales"].copy(), z["in_rotations"].copy(), z["in_sh"].copy(),
+                 z["in_opacities"].copy(), int(z["in_sh_degree"]))
+    acc = list(zip(z["acc_d_means2D"], z["acc_radii"]))
+    cfg = S.DensifyConfig.from_buffer_copy(z["cfg_bytes"].tobytes())
+    return sc, acc, cfg, float(z["extent"]), z
+
+
 def canon(keys, vals):
     """(key, value)-sorted order: the reference's std::sort leaves equal keys unordered."""
     o = np.lexsort((vals, keys))

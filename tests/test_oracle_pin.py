@@ -146,6 +146,53 @@ def test_eval3d_oracle_matches_reference_live():
     assert U.bits_equal(a.image, b.image) and U.bits_equal(a.n_contrib, b.n_contrib)
 
 
+@pytest.mark.parametrize("name", U.density_cases())
+def test_density_oracle_matches_reference_fixture(name):
+    """densify_and_prune and reset_opacity of the C restatement against the reference's."""
+    sc, acc, cfg, extent, z = U.load_density(name)
+    ora = O.DensityOracle()
+    for d, r in acc:
+        ora.accumulate(d, r, sc.count)
+    new = ora.densify(sc, cfg, extent)
+    assert new.count == int(z["out_count"])
+    for k in ("positions", "scales", "rotations", "sh", "opacities"):
+        assert U.bits_equal(getattr(new, k), z["out_" + k]), k
+    O.DensityOracle.reset_opacity(new)
+    assert U.bits_equal(new.opacities, z["out_reset_opacities"])
+
+
+@pytest.mark.skipif(not O.have_ref(), reason="oracle/_ref not built (needs the reference tree)")
+def test_density_oracle_matches_reference_live():
+    """Two rounds (the split sampler's state carries over) on a fresh seed, clones only in
+    round 2, so that the reference's compaction reads stay inside its mask."""
+    rng = np.random.default_rng(97)
+    sc = S.random_scene(650, seed=97)
+    sc.scales[:] = np.minimum(sc.scales, np.log(0.0105))
+    big = rng.choice(650, 3, replace=False)
+    sc.scales[big] = np.log(0.03)
+    cfg = S.densify_config(enabled=True)
+    ora, ref = O.DensityOracle(), O.DensityRef()
+    ref.set_model(sc)
+    cur = sc
+    for rnd in range(2):
+        n = cur.count
+        for _ in range(2):
+            d = rng.normal(0, 1e-5, (n, 2)).astype(np.float32)
+            if rnd == 0:
+                d[big] = 1e-3
+            else:
+                d[: n // 3] = rng.normal(0, 5e-4, (n // 3, 2)).astype(np.float32)
+                d[np.exp(cur.scales).max(1) > 0.011] = 0.0   # no second-round splits
+            r = rng.integers(0, 25, n).astype(np.int32)
+            ora.accumulate(d, r, n)
+            ref.accumulate(d, r, n)
+        cur = ora.densify(cur, cfg, 1.1)
+        assert cur.count == ref.densify(cfg, 1.1)
+        got = ref.model()
+        for k in ("positions", "scales", "rotations", "sh", "opacities"):
+            assert U.bits_equal(getattr(cur, k), getattr(got, k)), (rnd, k)
+
+
 @pytest.mark.skipif(not O.have_ref(), reason="oracle/_ref not built (needs the reference tree)")
 def test_oracle_matches_reference_live():
     """A fresh seed, both oracles side by side (forward of 20k Gaussians, 320x240)."""
