@@ -35,6 +35,7 @@ SOURCES = {
     "sort.cu": [],
     "sort_static.cu": [],
     "capi.cu": [],
+    "io.cpp": [],   # file formats (host code, -ffp-contract=off like the reference)
 }
 
 
@@ -56,7 +57,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     objs = []
     for src, extra in SOURCES.items():
         s = os.path.join(CSRC, src)
-        o = os.path.join(BUILD, src.replace(".cu", ".o"))
+        o = os.path.join(BUILD, os.path.splitext(src)[0] + ".o")
         objs.append(o)
         if force or not os.path.exists(o) or os.path.getmtime(o) < max(os.path.getmtime(s), hdr_time):
             cmd = [nvcc(), *ARCH, *COMMON, *extra, "-c", s, "-o", o]

@@ -95,6 +95,16 @@ def load_library(path: str = LIB_PATH):
         "gs3dc_get_gradients": ([vp, vp, vp, vp, vp, vp], ctypes.c_int),
         "gs3dc_save_state": ([vp, ctypes.c_char_p], ctypes.c_int),
         "gs3dc_density_accumulate": ([vp, vp, vp], ctypes.c_int),
+        "gs3dc_ply_info": ([ctypes.c_char_p, vp, vp, vp, vp], ctypes.c_int),
+        "gs3dc_ply_read": ([ctypes.c_char_p, ctypes.c_int, vp], ctypes.c_int),
+        "gs3dc_ply_write": ([ctypes.c_char_p, vp], ctypes.c_int),
+        "gs3dc_raw_from_gaussians": ([vp, vp], ctypes.c_int),
+        "gs3dc_cameras_read": ([ctypes.c_char_p, vp, vp, ctypes.c_int, ctypes.c_int, vp], ctypes.c_int),
+        "gs3dc_ppm_read": ([ctypes.c_char_p, vp, vp, vp], ctypes.c_int),
+        "gs3dc_ppm_write": ([ctypes.c_char_p, vp, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+        "gs3dc_image_resize_nearest": ([vp, ctypes.c_int, ctypes.c_int, vp, ctypes.c_int, ctypes.c_int],
+                                       ctypes.c_int),
+        "gs3dc_io_last_error": ([], ctypes.c_char_p),
         "gs3dc_densify_and_prune": ([vp, vp, ctypes.c_float, vp], ctypes.c_int),
         "gs3dc_reset_opacity": ([vp], ctypes.c_int),
         "gs3dc_train_step_densify": ([vp, vp, vp, ctypes.c_int, vp, vp, vp, ctypes.c_float, ctypes.c_int, vp, vp],
@@ -127,6 +137,125 @@ def _p(a):
 
 def _ref(s):
     return None if s is None else ctypes.cast(ctypes.pointer(s), ctypes.c_void_p)
+
+
+# ---- on-disk formats (host functions: no context, no GPU needed) ----
+
+def _io(rc: int):
+    if rc != 0:
+        raise Gs3dError(rc, load_library().gs3dc_io_last_error().decode(errors="replace"))
+
+
+def ply_info(path: str) -> dict:
+    """count, sh_degree, max_coeffs, has_filter_3D of a 3DGS PLY."""
+    L = load_library()
+    v = [ctypes.c_int() for _ in range(4)]
+    _io(L.gs3dc_ply_info(str(path).encode(), *[ctypes.byref(x) for x in v]))
+    return dict(count=v[0].value, sh_degree=v[1].value, max_coeffs=v[2].value, has_filter_3D=bool(v[3].value))
+
+
+def load_ply(path: str, activate: bool = True):
+    """loadPly: (Scene of the arrays, filter_3D or None).  activate: the loader's
+    activations (the arrays are a GaussianData model: opacities, scales,
+    normalised rotations); otherwise the stored raw values (a trainable Scene)."""
+    L = load_library()
+    info = ply_info(path)
+    n, k = info["count"], info["max_coeffs"]
+    sc = S.Scene(np.zeros((n, 3), np.float32), np.zeros((n, 3), np.float32), np.zeros((n, 4), np.float32),
+                 np.zeros((n, k, 3), np.float32), np.zeros(n, np.float32), info["sh_degree"])
+    g = S.GaussianData()
+    g.count, g.sh_degree, g.max_coeffs = n, info["sh_degree"], k
+    for fld, arr in (("positions", sc.positions), ("scales", sc.scales), ("rotations", sc.rotations),
+                     ("sh_coeffs", sc.sh), ("opacities", sc.opacities)):
+        setattr(g, fld, S.fptr(arr))
+    f3 = np.zeros(n, np.float32) if info["has_filter_3D"] else None
+    if f3 is not None:
+        g.filter_3D = S.fptr(f3)
+    _io(L.gs3dc_ply_read(str(path).encode(), 1 if activate else 0, _ref(g)))
+    return sc, f3
+
+
+def save_ply(path: str, scene: S.Scene):
+    """savePly of the train driver (raw parameters)."""
+    r = scene.raw_struct()
+    _io(load_library().gs3dc_ply_write(str(path).encode(), _ref(r)))
+
+
+def raw_from_gaussians(model: S.Scene) -> S.Scene:
+    """initRawFromGaussianData: a loaded (activated) model -> trainable raw parameters."""
+    n, k = model.count, model.max_coeffs
+    g = S.GaussianData()
+    g.count, g.sh_degree, g.max_coeffs = n, model.sh_degree, k
+    arrs = [np.ascontiguousarray(x, np.float32) for x in
+            (model.positions, model.scales, model.rotations, model.sh, model.opacities)]
+    for fld, arr in zip(("positions", "scales", "rotations", "sh_coeffs", "opacities"), arrs):
+        setattr(g, fld, S.fptr(arr))
+    out = S.Scene(np.zeros((n, 3), np.float32), np.zeros((n, 3), np.float32), np.zeros((n, 4), np.float32),
+                  np.zeros((n, k, 3), np.float32), np.zeros(n, np.float32), model.sh_degree)
+    r = out.raw_struct()
+    _io(load_library().gs3dc_raw_from_gaussians(_ref(g), _ref(r)))
+    return out
+
+
+def load_cameras(path: str, name_len: int = 256) -> list:
+    """loadCamerasJson: [(Camera, img_name)] in file order."""
+    L = load_library()
+    n = ctypes.c_int()
+    _io(L.gs3dc_cameras_read(str(path).encode(), None, None, 0, 0, ctypes.byref(n)))
+    cams = (S.Camera * max(n.value, 1))()
+    names = ctypes.create_string_buffer(max(n.value, 1) * name_len)
+    _io(L.gs3dc_cameras_read(str(path).encode(), ctypes.cast(cams, ctypes.c_void_p), ctypes.cast(names, ctypes.c_void_p),
+                             name_len, n.value, ctypes.byref(n)))
+    out = []
+    for i in range(n.value):
+        raw = names.raw[i * name_len:(i + 1) * name_len]
+        out.append((S.Camera.from_buffer_copy(cams[i]), raw.split(b"\0")[0].decode(errors="replace")))
+    return out
+
+
+def read_ppm(path: str):
+    """readPPM: (float32 image [H*W*3] in [0, 1], width, height)."""
+    L = load_library()
+    w, h = ctypes.c_int(), ctypes.c_int()
+    _io(L.gs3dc_ppm_read(str(path).encode(), None, ctypes.byref(w), ctypes.byref(h)))
+    img = np.zeros(w.value * h.value * 3, np.float32)
+    _io(L.gs3dc_ppm_read(str(path).encode(), _p(img), ctypes.byref(w), ctypes.byref(h)))
+    return img, w.value, h.value
+
+
+def write_ppm(path: str, image: np.ndarray, width: int, height: int):
+    img = np.ascontiguousarray(image, np.float32).reshape(-1)
+    _io(load_library().gs3dc_ppm_write(str(path).encode(), _p(img), int(width), int(height)))
+
+
+def resize_nearest(image: np.ndarray, sw: int, sh: int, dw: int, dh: int) -> np.ndarray:
+    src = np.ascontiguousarray(image, np.float32).reshape(-1)
+    dst = np.zeros(dw * dh * 3, np.float32)
+    _io(load_library().gs3dc_image_resize_nearest(_p(src), sw, sh, _p(dst), dw, dh))
+    return dst
+
+
+def load_views(cameras_json: str, gt_dir: str) -> list:
+    """The train driver's multi-view data (train_main.cpp:515-563): every camera of
+    cameras.json whose <gt_dir>/<img_name>{.ppm,.PPM,} loads, with its target
+    resized (nearest) to the camera when the sizes differ.  [(Camera, target)]."""
+    views = []
+    for cam, name in load_cameras(cameras_json):
+        if not name:
+            continue
+        for ext in (".ppm", ".PPM", ""):
+            path = os.path.join(gt_dir, name + ext)
+            if not os.path.exists(path):
+                continue
+            try:
+                img, w, h = read_ppm(path)
+            except Gs3dError:
+                continue
+            if (w, h) != (cam.width, cam.height):
+                img = resize_nearest(img, w, h, cam.width, cam.height)
+            views.append((cam, img))
+            break
+    return views
 
 
 class Context:

@@ -306,6 +306,38 @@ int gs3dc_train_step_densify(gs3dc_ctx* ctx, const gs3d_camera* cam, const float
                              const gs3d_densify_config* dcfg, float scene_extent, int iteration, float* loss,
                              int* n_gaussians);
 
+/* ---- on-disk formats of the reference's drivers (host functions, no context) ----
+ * gs3dc_ply_info / gs3dc_ply_read: loadPly (src/ply_loader.cpp:31-189): a binary
+ *   little-endian 3DGS PLY; SH degree from the f_rest count; SH reordered from
+ *   channel-first to basis-interleaved.  activate != 0: the loader's activations
+ *   (sigmoid opacity, exp scale, normalised quaternion) -> GaussianData; 0: the
+ *   stored values -> the arrays of g (same layout) without activation.
+ *   g->count / g->max_coeffs must be gs3dc_ply_info's; g->filter_3D may be NULL.
+ * gs3dc_ply_write: savePly of the train driver (src/train_main.cpp:82-138),
+ *   byte for byte.
+ * gs3dc_raw_from_gaussians: initRawFromGaussianData (src/train_main.cpp:26-65):
+ *   log(max(1e-12, scale)), inverse_sigmoid of the clamped opacity.
+ * gs3dc_cameras_read: loadCamerasJson (src/train_main.cpp:262-375): every camera
+ *   object (fx, fy > 0, with position and camera-to-world rotation) of a 3DGS
+ *   cameras.json, in file order, as view / view-projection matrices (znear 0.01,
+ *   zfar 100); names (optional) receives img_name, name_len bytes per camera;
+ *   *n_cams = cameras found (only the first max_cams are written).
+ * gs3dc_ppm_read / gs3dc_ppm_write: readPPM / writePPM (src/image_io.cpp:9-68):
+ *   8-bit P6; image == NULL reads the size only.
+ * gs3dc_image_resize_nearest: the train driver's target resize
+ *   (src/train_main.cpp:536-548).
+ * gs3dc_io_last_error: message of the last failed call of this group (per thread). */
+int gs3dc_ply_info(const char* path, int* count, int* sh_degree, int* max_coeffs, int* has_filter_3D);
+int gs3dc_ply_read(const char* path, int activate, gs3d_gaussians* g);
+int gs3dc_ply_write(const char* path, const gs3d_raw_params* raw);
+int gs3dc_raw_from_gaussians(const gs3d_gaussians* g, gs3d_raw_params* raw);
+int gs3dc_cameras_read(const char* path, gs3d_camera* cams, char* names, int name_len, int max_cams,
+                       int* n_cams);
+int gs3dc_ppm_read(const char* path, float* image, int* width, int* height);
+int gs3dc_ppm_write(const char* path, const float* image, int width, int height);
+int gs3dc_image_resize_nearest(const float* src, int src_w, int src_h, float* dst, int dst_w, int dst_h);
+const char* gs3dc_io_last_error(void);
+
 /* Checkpoint / resume of the whole training state: the model in its current
  * form's storage (FP32, or the 16-bit arrays), the optimiser moments and the
  * Adam step counter, so that a resumed run continues exactly where the saved

@@ -15,7 +15,8 @@ Two kinds of fixtures, both produced by the reference itself:
   a single Gaussian, every Gaussian culled, oversized splats; and the 3D-evaluation
   mode (eval_3D) on scenes that reach its frustum culling, camera-inside test and
   view-space bounding box, with and without a 3D filter; and the density
-  controller's densify_and_prune (clone, split, prune) and reset_opacity.
+  controller's densify_and_prune (clone, split, prune) and reset_opacity; and the
+  drivers' file formats (cameras.json, PLY load / save, PPM).
 
 It needs the reference tree at /root/reference (only this script reads it);
 the tests and the GPU runs read the committed copies.
@@ -52,6 +53,13 @@ def copy_ref_fixtures():
         for f in sorted(os.listdir(src)):
             if f.endswith((".bin", ".json")):
                 shutil.copyfile(os.path.join(src, f), os.path.join(out, f))
+    # the data files of the format tests: the repository's cameras.json and the
+    # PLY of its loader test (tests/test_ply_loader.cpp)
+    out = os.path.join(dst, "formats")
+    os.makedirs(out, exist_ok=True)
+    shutil.copyfile(os.path.join(REF, "cameras.json"), os.path.join(out, "cameras.json"))
+    shutil.copyfile(os.path.join(REF, "tests", "test_data", "tiny_3gaussians.ply"),
+                    os.path.join(out, "tiny_3gaussians.ply"))
 
 
 # ---- seeded cases ----
@@ -197,6 +205,56 @@ def make_density():
         print(name, sc.count, "->", k)
 
 
+def make_formats():
+    """The reference's loaders on the format fixtures: cameras.json -> cameras, the
+    tiny PLY -> activated model and raw parameters, savePly of those raw
+    parameters, and a writePPM / readPPM round trip of a seeded image."""
+    import ctypes
+    fx = os.path.join(HERE, "ref_fixtures", "formats")
+    L = O.lib_ref()
+    out = {}
+    cams = (S.Camera * 256)()
+    names = ctypes.create_string_buffer(256 * 64)
+    n = L.ref_io_cameras(os.path.join(fx, "cameras.json").encode(), cams, names, 64, 256)
+    out["cam_count"] = np.int32(n)
+    out["cam_bytes"] = np.frombuffer(bytes(cams)[: n * ctypes.sizeof(S.Camera)], np.uint8)
+    out["cam_names"] = np.array([names.raw[i * 64:(i + 1) * 64].split(b"\0")[0].decode() for i in range(n)])
+    ply = os.path.join(fx, "tiny_3gaussians.ply").encode()
+    cnt, deg, mc, hf = (ctypes.c_int() for _ in range(4))
+    L.ref_io_ply_count(ply, ctypes.byref(cnt), ctypes.byref(deg), ctypes.byref(mc), ctypes.byref(hf))
+    n, k = cnt.value, mc.value
+    act = dict(positions=np.zeros(3 * n, np.float32), scales=np.zeros(3 * n, np.float32),
+               rotations=np.zeros(4 * n, np.float32), sh_coeffs=np.zeros(3 * k * n, np.float32),
+               opacities=np.zeros(n, np.float32))
+    sc = S.Scene(np.zeros((n, 3), np.float32), np.zeros((n, 3), np.float32), np.zeros((n, 4), np.float32),
+                 np.zeros((n, k, 3), np.float32), np.zeros(n, np.float32), deg.value)
+    g = O.gaussians_struct(sc, act)
+    L.ref_io_ply_load(ply, ctypes.byref(g))
+    out.update({"ply_" + a: b for a, b in act.items()})
+    out["ply_shape"] = np.array([n, deg.value, k, hf.value], np.int32)
+    raw = sc.raw_struct()
+    L.ref_io_raw_from_gaussians(ctypes.byref(g), ctypes.byref(raw))
+    out.update(raw_positions=sc.positions.copy(), raw_scales=sc.scales.copy(), raw_rotations=sc.rotations.copy(),
+               raw_sh=sc.sh.copy(), raw_opacities=sc.opacities.copy())
+    tmp = os.path.join(HERE, "_tmp_saved.ply")
+    L.ref_io_ply_save(tmp.encode(), ctypes.byref(raw))
+    out["saved_ply_bytes"] = np.frombuffer(open(tmp, "rb").read(), np.uint8)
+    os.remove(tmp)
+    rng = np.random.default_rng(5)
+    img = rng.uniform(-0.2, 1.2, (37, 23, 3)).astype(np.float32)
+    tmp = os.path.join(HERE, "_tmp.ppm")
+    L.ref_io_ppm_write(tmp.encode(), img.ctypes.data_as(ctypes.c_void_p), 23, 37)
+    out["ppm_in"] = img
+    out["ppm_bytes"] = np.frombuffer(open(tmp, "rb").read(), np.uint8)
+    back = np.zeros(37 * 23 * 3, np.float32)
+    w, h = ctypes.c_int(), ctypes.c_int()
+    L.ref_io_ppm_read(tmp.encode(), back.ctypes.data_as(ctypes.c_void_p), ctypes.byref(w), ctypes.byref(h))
+    os.remove(tmp)
+    out["ppm_read"] = back
+    np.savez_compressed(os.path.join(HERE, "seeded", "formats_ref.npz"), **out)
+    print("formats: cameras", int(out["cam_count"]), "ply", n)
+
+
 def _canon(keys, vals):
     o = np.lexsort((vals, keys))
     return keys[o], vals[o]
@@ -254,3 +312,4 @@ if __name__ == "__main__":
     make_seeded()
     make_eval3d()
     make_density()
+    make_formats()
