@@ -98,6 +98,8 @@ struct gs3dc_ctx {
     DevBuf<float> e3_g2s, e3_ci, e3_mo, e3_view, filt3d;
     bool have_filt3d = false;   // the activated model came with GaussianData::filter_3D
     bool mode_e3 = false;       // the current screen records and pairs are of the 3D mode
+    int screen_n = 0;             // Gaussians of the current screen records
+    bool screen_imported = false; // the screen records came from a caller (gs3dc_rasterize_arrays)
     // adaptive density control (the trainer's DensityController): statistics + scratch
     DevBuf<float> dc_accum, dc_denom;
     DevBuf<int> dc_maxr, dc_clone, dc_split, dc_crank, dc_srank, dc_src, dc_keep, dc_out, dc_sums, dc_radii_in;
@@ -694,6 +696,8 @@ int seq_back_chosen(gs3dc_ctx* c) {
 int seq_train_front(gs3dc_ctx* c) {
     int rc;
     c->mode_e3 = false;   // training is the 2D path only
+    c->screen_n = c->N;
+    c->screen_imported = false;
     if (chosen_form(c) || c->sort_mode == GS3DC_SORT_DEPTH_FIRST) {
         if ((rc = seq_front_depth_first(c))) return rc;
     } else {
@@ -767,6 +771,8 @@ int run_preprocess(gs3dc_ctx* c, const gs3d_camera* cam, const gs3d_render_confi
     c->have_screen = true;
     c->have_pairs = true;
     c->have_sorted = c->have_raster = c->have_rgrad = false;
+    c->screen_n = c->N;
+    c->screen_imported = false;
     return GS3DC_OK;
 }
 
@@ -1160,6 +1166,7 @@ int gs3dc_get_stat(gs3dc_ctx* c, int stat, int64_t* value) {
         case GS3DC_STAT_GRAPH_REPLAYS: *value = c->graph_replays; return GS3DC_OK;
         case GS3DC_STAT_ADAM_STEP: *value = c->adam_step; return GS3DC_OK;
         case GS3DC_STAT_NUM_GAUSSIANS: *value = c->N; return GS3DC_OK;
+        case GS3DC_STAT_SCREEN_GAUSSIANS: *value = c->screen_n; return GS3DC_OK;
         default: return fail(c, GS3DC_ERR_INVALID_ARG, "unknown stat %d", stat);
     }
 }
@@ -1467,6 +1474,78 @@ int gs3dc_rasterize(gs3dc_ctx* c, const gs3d_camera* cam, const gs3d_render_conf
     return GS3DC_OK;
 }
 
+int gs3dc_rasterize_arrays(gs3dc_ctx* c, int num_gaussians, const gs3dc_screen_arrays* in, int64_t total_pairs,
+                           const uint32_t* values_sorted, int num_tiles, const uint32_t* tile_ranges,
+                           const gs3d_camera* cam, const gs3d_render_config* cfg, float* image, float* T_final,
+                           int* n_contrib) {
+    if (!c || !in || !tile_ranges) return GS3DC_ERR_INVALID_ARG;
+    if (int rc_ = require_plain(c, "gs3dc_rasterize_arrays")) return rc_;
+    int rc;
+    if ((rc = check_config(c, cam, cfg))) return rc;   // the 3D mode needs its own per-Gaussian arrays
+    const int gx = (cam->width + kTile - 1) / kTile, gy = (cam->height + kTile - 1) / kTile;
+    if (num_gaussians < 0 || total_pairs < 0 || num_tiles != gx * gy)
+        return fail(c, GS3DC_ERR_INVALID_ARG, "bad sizes: N=%d, P=%lld, %d tiles (the camera has %d)", num_gaussians,
+                    (long long)total_pairs, num_tiles, gx * gy);
+    if (num_gaussians > 0 && (!in->means2D || !in->conics || !in->opacities_2d || !in->rgb))
+        return fail(c, GS3DC_ERR_INVALID_ARG, "means2D, conics, opacities_2d and rgb are required");
+    if (total_pairs > 0 && !values_sorted) return fail(c, GS3DC_ERR_INVALID_ARG, "values_sorted is required");
+    if ((unsigned long long)total_pairs > 0xFFFFFFFFull)
+        return fail(c, GS3DC_ERR_PAIR_OVERFLOW, "%lld pairs exceed the 32-bit tile-range format", (long long)total_pairs);
+    // every index the rasteriser will follow must stay inside the caller's arrays
+    const size_t P = (size_t)total_pairs, n = (size_t)num_gaussians;
+    for (size_t j = 0; j < P; j++)
+        if (values_sorted[j] >= n)
+            return fail(c, GS3DC_ERR_INVALID_ARG, "values_sorted[%zu] = %u is not below N = %d", j, values_sorted[j],
+                        num_gaussians);
+    for (int t = 0; t < num_tiles; t++)
+        if (tile_ranges[2 * t] > tile_ranges[2 * t + 1] || tile_ranges[2 * t + 1] > P)
+            return fail(c, GS3DC_ERR_INVALID_ARG, "tile %d has range [%u, %u) outside [0, %zu)", t, tile_ranges[2 * t],
+                        tile_ranges[2 * t + 1], P);
+    CK(cudaSetDevice(c->device));
+    if ((rc = ensure_pixels(c, cam->width, cam->height))) return rc;
+    const size_t nn = n ? n : 1;
+    if (nn > c->rec0.n || nn > c->rec1.n || nn > c->col_b.n) drop_graphs(c);
+    CK(c->rec0.ensure(nn));
+    CK(c->rec1.ensure(nn));
+    CK(c->col_b.ensure(nn));
+    CK(c->dm2.ensure(2 * nn));
+    CK(c->dcon.ensure(3 * nn));
+    CK(c->drgb.ensure(3 * nn));
+    CK(c->dop.ensure(nn));
+    CK(c->x_means2D.ensure(2 * nn));
+    CK(c->x_conics.ensure(3 * nn));
+    CK(c->x_opac.ensure(nn));
+    CK(c->x_rgb.ensure(3 * nn));
+    if (n) {
+        CK(cudaMemcpyAsync(c->x_means2D.p, in->means2D, 2 * n * 4, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(c->x_conics.p, in->conics, 3 * n * 4, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(c->x_opac.p, in->opacities_2d, n * 4, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(c->x_rgb.p, in->rgb, 3 * n * 4, cudaMemcpyHostToDevice, c->stream));
+    }
+    ScreenArrays a{c->x_means2D.p, nullptr, c->x_conics.p, c->x_opac.p, c->x_rgb.p, nullptr, nullptr};
+    CK(launch_import_screen(c->stream, num_gaussians, a, screen_ptrs(c, false)));
+    if ((rc = ensure_pairs(c, P > c->cap ? P : c->cap, c->num_tiles))) return rc;
+    if (P) CK(cudaMemcpyAsync(c->vals[0].p, values_sorted, P * 4, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->ranges.p, tile_ranges, 2 * (size_t)num_tiles * 4, cudaMemcpyHostToDevice, c->stream));
+    CK(launch_tile_order(c->stream, c->ranges.p, c->num_tiles, c->tile_order.p));
+    c->sorted_which = 0;
+    c->screen_n = num_gaussians;
+    c->screen_imported = true;
+    c->mode_e3 = false;
+    c->have_screen = c->have_sorted = true;
+    c->have_pairs = c->have_raster = c->have_rgrad = false;
+    if ((rc = push_params(c, cam, cfg, nullptr, 0, nullptr))) return rc;
+    CK(launch_raster_fwd_plain(c->stream, c->sp_dev, c->num_tiles, false, c->ranges.p, c->tile_order.p, c->vals[0].p,
+                               screen_ptrs(c, false), pixel_ptrs(c), c->ctrl));
+    const size_t np = (size_t)c->W * c->H;
+    if ((rc = download(c, image, c->image.p, 3 * np * 4)) || (rc = download(c, T_final, c->T_final.p, np * 4)) ||
+        (rc = download(c, n_contrib, c->n_contrib.p, np * 4)))
+        return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    c->have_raster = true;
+    return GS3DC_OK;
+}
+
 int gs3dc_render(gs3dc_ctx* c, const gs3d_gaussians* g, const gs3d_camera* cam, const gs3d_render_config* cfg,
                  float* image) {
     if (!c) return GS3DC_ERR_INVALID_ARG;
@@ -1492,7 +1571,7 @@ int gs3dc_raster_backward(gs3dc_ctx* c, const gs3d_camera* cam, const gs3d_rende
     if ((rc = check_config(c, cam, cfg))) return rc;
     if (!c->have_raster) return fail(c, GS3DC_ERR_STATE, "gs3dc_raster_backward needs gs3dc_rasterize first");
     CK(cudaSetDevice(c->device));
-    const size_t np = (size_t)c->W * c->H, n = (size_t)c->N;
+    const size_t np = (size_t)c->W * c->H, n = (size_t)c->screen_n;
     CK(c->d_image.ensure(3 * np));
     CK(cudaMemcpyAsync(c->d_image.p, d_image, 3 * np * 4, cudaMemcpyHostToDevice, c->stream));
     if ((rc = push_params(c, cam, cfg, nullptr, 0, nullptr))) return rc;
@@ -1518,6 +1597,9 @@ int gs3dc_preprocess_backward(gs3dc_ctx* c, const gs3d_camera* cam, const gs3d_r
     if (int rc_ = require_plain(c, "gs3dc_preprocess_backward")) return rc_;
     int rc;
     if ((rc = check_config(c, cam, cfg))) return rc;
+    if (c->screen_imported)
+        return fail(c, GS3DC_ERR_STATE, "gs3dc_preprocess_backward needs the device model's own forward "
+                                        "(the screen records came from gs3dc_rasterize_arrays)");
     if (!c->have_rgrad) return fail(c, GS3DC_ERR_STATE, "gs3dc_preprocess_backward needs gs3dc_raster_backward");
     if (!c->model_raw && !raw_rotations)
         return fail(c, GS3DC_ERR_INVALID_ARG, "an activated device model needs the raw rotations");

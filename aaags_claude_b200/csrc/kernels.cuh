@@ -199,6 +199,8 @@ cudaError_t launch_emit_ranked(cudaStream_t st, const StepParams* sp, int N, con
 cudaError_t launch_bin_arrays(cudaStream_t st, const StepParams* sp, int N, ScreenArrays a,
                               PairPtrs pr, Control* ctrl);
 cudaError_t launch_export_screen(cudaStream_t st, int N, ScreenPtrs s, ScreenArrays a);
+// means2D / conics / opac2d / rgb of a caller -> rec0 / rec1 / col_b
+cudaError_t launch_import_screen(cudaStream_t st, int N, ScreenArrays a, ScreenPtrs s);
 // 3D-evaluation mode: view setup (inverse view-projection, tile rays), the
 // fused preprocess + pair emission (raw: activate the device model first;
 // filt: per-Gaussian 3D filter or NULL), the emission from host arrays (a.means2D,

@@ -329,6 +329,16 @@ __global__ void k_export_screen(int N, ScreenPtrs s, ScreenArrays a) {
 }
 
 
+// The inverse: PreprocessOutput arrays of a caller (screen means, conics,
+// opacities, colours) packed into the screen records the rasterisers read.
+__global__ void k_import_screen(int N, ScreenArrays a, ScreenPtrs s) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    s.rec0[i] = make_float4(a.means2D[2 * i], a.means2D[2 * i + 1], a.conics[3 * i], a.conics[3 * i + 1]);
+    s.rec1[i] = make_float4(a.conics[3 * i + 2], a.opac2d[i], a.rgb[3 * i], a.rgb[3 * i + 1]);
+    s.col_b[i] = a.rgb[3 * i + 2];
+}
+
 // ---- fused preprocess backward + optimiser, staged by TMA into shared memory ----
 //
 // One CTA owns kBwdG consecutive Gaussians.  A single thread issues TMA bulk
@@ -704,6 +714,12 @@ cudaError_t launch_bin_arrays(cudaStream_t st, const StepParams* sp, int N, Scre
 cudaError_t launch_export_screen(cudaStream_t st, int N, ScreenPtrs s, ScreenArrays a) {
     if (N <= 0) return cudaSuccess;
     k_export_screen<<<blocks_for(N, 256), 256, 0, st>>>(N, s, a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_import_screen(cudaStream_t st, int N, ScreenArrays a, ScreenPtrs s) {
+    if (N <= 0) return cudaSuccess;
+    k_import_screen<<<blocks_for(N, 256), 256, 0, st>>>(N, a, s);
     return cudaGetLastError();
 }
 

@@ -27,6 +27,7 @@ OPT_PAIR_CAPACITY, OPT_USE_GRAPH, OPT_FORM, OPT_SPIN_LIMIT, OPT_STAGE_TIMING, OP
 NUM_STAGES = 8
 STAT_TOTAL_PAIRS, STAT_PAIR_CAPACITY, STAT_KERNELS_LAST, STAT_SORT_PASSES, STAT_GRAPH_REPLAYS, STAT_ADAM_STEP = range(1, 7)
 STAT_NUM_GAUSSIANS = 9
+STAT_SCREEN_GAUSSIANS = 10
 STAT_FWD_PPT, STAT_BWD_PPT = 7, 8
 FORM_PLAIN_FP32, FORM_BF16, FORM_FP16 = 0, 1, 2
 OPT_SORT = 7
@@ -95,6 +96,8 @@ def load_library(path: str = LIB_PATH):
         "gs3dc_get_gradients": ([vp, vp, vp, vp, vp, vp], ctypes.c_int),
         "gs3dc_save_state": ([vp, ctypes.c_char_p], ctypes.c_int),
         "gs3dc_density_accumulate": ([vp, vp, vp], ctypes.c_int),
+        "gs3dc_rasterize_arrays": ([vp, ctypes.c_int, vp, i64, vp, ctypes.c_int, vp, vp, vp, vp, vp, vp],
+                                   ctypes.c_int),
         "gs3dc_ply_info": ([ctypes.c_char_p, vp, vp, vp, vp], ctypes.c_int),
         "gs3dc_ply_read": ([ctypes.c_char_p, ctypes.c_int, vp], ctypes.c_int),
         "gs3dc_ply_write": ([ctypes.c_char_p, vp], ctypes.c_int),
@@ -425,6 +428,22 @@ class Context:
         self._chk(self.L.gs3dc_rasterize(self.h, _ref(cam), _ref(cfg), _p(img), _p(T), _p(nc)))
         return img, T, nc
 
+    def rasterize_arrays(self, cam, cfg, means2D, conics, opacities_2d, rgb, values_sorted, tile_ranges):
+        """Rasterizer::rasterize on host PreprocessOutput / BinningOutput arrays: (image, T_final, n_contrib)."""
+        arrs = [np.ascontiguousarray(x, np.float32).reshape(-1) for x in (means2D, conics, opacities_2d, rgb)]
+        n = int(arrs[2].shape[0])
+        sa = ScreenArrays()
+        for k, v in zip(("means2D", "conics", "opacities_2d", "rgb"), arrs):
+            setattr(sa, k, v.ctypes.data_as(_f))
+        vals = np.ascontiguousarray(values_sorted, np.uint32).reshape(-1)
+        rg = np.ascontiguousarray(tile_ranges, np.uint32).reshape(-1)
+        npx = cam.width * cam.height
+        img, T, nc = np.zeros(3 * npx, np.float32), np.zeros(npx, np.float32), np.zeros(npx, np.int32)
+        self._chk(self.L.gs3dc_rasterize_arrays(self.h, n, _ref(sa), int(vals.shape[0]), _p(vals) if vals.size else None,
+                                                int(rg.shape[0] // 2), _p(rg), _ref(cam), _ref(cfg), _p(img), _p(T),
+                                                _p(nc)))
+        return img, T, nc
+
     def render(self, cam, cfg, download: bool = True) -> np.ndarray | None:
         """Renderer::render of the device model; download=False leaves the image on the device."""
         img = np.zeros(3 * cam.width * cam.height, np.float32) if download else None
@@ -432,7 +451,7 @@ class Context:
         return img
 
     def raster_backward(self, cam, cfg, d_image: np.ndarray) -> dict:
-        n = self._model[1]
+        n = self.stat(STAT_SCREEN_GAUSSIANS)   # the screen records' Gaussians (model or imported arrays)
         out = dict(d_means2D=np.zeros(2 * n, np.float32), d_conics=np.zeros(3 * n, np.float32),
                    d_rgb=np.zeros(3 * n, np.float32), d_opac=np.zeros(n, np.float32))
         d = np.ascontiguousarray(d_image, np.float32).reshape(-1)

@@ -2,6 +2,7 @@
 #include "gs3d_stages_cuda.hpp"
 
 #include <cstddef>
+#include <algorithm>
 #include <cstring>
 #include <stdexcept>
 #include <string>
@@ -152,7 +153,7 @@ void SorterCUDA::sort(BinningOutput& bin, FrameAllocator&) {
 }
 
 // Rasterizer::rasterize (src/cpu/rasterizer_cpu.cpp:9-203)
-void RasterizerCUDA::rasterize(const PreprocessOutput&, const BinningOutput&, const Camera& cam,
+void RasterizerCUDA::rasterize(const PreprocessOutput& pre, const BinningOutput& bin, const Camera& cam,
                                const RenderConfig& cfg, float* img, float* depth, ForwardCache* cache,
                                FrameAllocator* alloc) {
     if (depth) throw std::runtime_error("rasterize: the inverse-depth output is not produced by the CUDA backend");
@@ -165,7 +166,22 @@ void RasterizerCUDA::rasterize(const PreprocessOutput&, const BinningOutput&, co
         T = cache->T_final;
         nc = cache->n_contrib;
     }
-    dev_->check(gs3dc_rasterize(dev_->ctx(), C(cam), C(cfg), img, T, nc), "rasterize");
+    if (pre.device_data == dev_->ctx() && bin.device_data == dev_->ctx()) {
+        dev_->check(gs3dc_rasterize(dev_->ctx(), C(cam), C(cfg), img, T, nc), "rasterize");
+        return;
+    }
+    // a caller's own screen arrays and sorted pairs (the reference's unit-test form)
+    gs3dc_screen_arrays a{};
+    a.means2D = pre.means2D;
+    a.conics = pre.conics;
+    a.opacities_2d = pre.opacities_2d;
+    a.rgb = pre.rgb;
+    int n = 0;
+    for (uint32_t j = 0; j < (uint32_t)bin.total_pairs; j++)
+        n = std::max(n, (int)bin.values_sorted[j] + 1);   // the arrays cover every Gaussian a pair names
+    dev_->check(gs3dc_rasterize_arrays(dev_->ctx(), n, &a, bin.total_pairs, bin.values_sorted, bin.num_tiles,
+                                       bin.tile_ranges, C(cam), C(cfg), img, T, nc),
+                "rasterize (host arrays)");
 }
 
 // RasterizerBackwardCPU::backward (src/cpu/rasterizer_backward_cpu.cpp:7-138)

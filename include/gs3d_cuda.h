@@ -81,6 +81,8 @@ typedef struct gs3dc_ctx gs3dc_ctx;
 #define GS3DC_STAT_FWD_PPT        7  /* pixels per thread of the forward rasteriser in the last train step */
 #define GS3DC_STAT_BWD_PPT        8  /* pixels per thread of the backward rasteriser in the last train step */
 #define GS3DC_STAT_NUM_GAUSSIANS  9  /* Gaussians of the device model (changes with density control) */
+#define GS3DC_STAT_SCREEN_GAUSSIANS 10 /* Gaussians of the current screen records (the model's, or those of
+                                          gs3dc_rasterize_arrays): the length of the raster gradients */
 
 /* Host arrays of PreprocessOutput + the per-Gaussian ForwardCache fields
  * (include/types.h:69-82, 97-107).  Any pointer may be NULL (not produced). */
@@ -190,6 +192,19 @@ int gs3dc_sort_pairs_static(int64_t total_pairs, const uint64_t* keys, const uin
  *   n_contrib (ForwardCache, include/types.h:98-99) may be NULL. */
 int gs3dc_rasterize(gs3dc_ctx* ctx, const gs3d_camera* cam, const gs3d_render_config* cfg,
                     float* image, float* T_final, int* n_contrib);
+
+/* Rasterizer::rasterize on a caller's own PreprocessOutput / BinningOutput
+ * (include/rasterizer.h:7-15; src/cpu/rasterizer_cpu.cpp:38-198): the screen
+ * arrays means2D, conics, opacities_2d, rgb of num_gaussians Gaussians, the
+ * sorted values and the 2*num_tiles tile ranges (num_tiles = the camera's
+ * 16x16 grid) are uploaded and blended.  Every value must be below
+ * num_gaussians and every range inside [0, total_pairs) (checked on the host).
+ * gs3dc_raster_backward may follow; gs3dc_preprocess_backward may not (there
+ * is no device model behind these records).  The 2D mode only. */
+int gs3dc_rasterize_arrays(gs3dc_ctx* ctx, int num_gaussians, const gs3dc_screen_arrays* in,
+                           int64_t total_pairs, const uint32_t* values_sorted, int num_tiles,
+                           const uint32_t* tile_ranges, const gs3d_camera* cam,
+                           const gs3d_render_config* cfg, float* image, float* T_final, int* n_contrib);
 
 /* Renderer::render (include/renderer.h:17-21; src/renderer.cpp:13-39):
  *   g (may be NULL to reuse the uploaded model) -> preprocess -> bin -> sort ->

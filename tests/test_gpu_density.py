@@ -158,3 +158,80 @@ def test_train_step_densify_matches_stage_calls(ctx):
     assert abs(m_stage.count - m_fused.count) <= 0.005 * m_fused.count
     # the opacity reset of iteration 5 reached every Gaussian on both paths
     assert np.all(m_fused.opacities <= np.log(0.01 / 0.99) + 0.05)
+
+
+# ---- the reference's DensityController unit tests (tests/test_density_controller.cpp), restated ----
+
+def _params(n: int) -> S.Scene:
+    """make_test_params of the reference test: positions (0.5 i, 0, 5), scales 0.1, identity
+    rotations, opacity 0.5, SH degree 0 with every coefficient 1."""
+    pos = np.stack([np.arange(n) * 0.5, np.zeros(n), np.full(n, 5.0)], 1).astype(np.float32)
+    sc = np.full((n, 3), np.log(np.float32(0.1)), np.float32)
+    rot = np.tile(np.array([1, 0, 0, 0], np.float32), (n, 1))
+    return S.Scene(pos, sc, rot, np.ones((n, 1, 3), np.float32), np.zeros(n, np.float32), 0)
+
+
+def _inv_sigmoid(x):
+    return np.float32(np.log(np.float32(x) / (np.float32(1.0) - np.float32(x))))
+
+
+KA_CFG = dict(grad_threshold=0.0002, min_opacity=0.001, enabled=True)
+
+
+def _densify(ctx, sc, d_means2D, cfg=None):
+    ctx.set_raw_params(sc)
+    ctx.density_accumulate(np.asarray(d_means2D, np.float32), None)
+    return ctx.densify_and_prune(cfg or S.densify_config(**KA_CFG), 100.0)
+
+
+def test_known_answer_clone_small(ctx):
+    d = np.zeros((5, 2), np.float32)
+    d[0] = d[2] = 0.1
+    assert _densify(ctx, _params(5), d) == 7
+    m = ctx.get_model(0)
+    assert m.positions[5, 0] == m.positions[0, 0] and m.positions[6, 0] == m.positions[2, 0]
+
+
+def test_known_answer_split_large(ctx):
+    sc = _params(3)
+    sc.scales[1] = np.log(np.float32(5.0))
+    d = np.zeros((3, 2), np.float32)
+    d[1] = 0.5
+    assert _densify(ctx, sc, d) == 4
+    m = ctx.get_model(0)
+    assert np.all(np.exp(m.scales).max(1) < 5.0)      # the large original is gone
+    assert np.sum(np.isclose(m.scales[:, 0], np.log(np.float32(5.0)) - np.log(np.float32(1.6)))) == 2
+
+
+def test_known_answer_prune_low_opacity(ctx):
+    sc = _params(5)
+    sc.opacities[1] = _inv_sigmoid(0.001)
+    sc.opacities[3] = _inv_sigmoid(0.002)
+    assert _densify(ctx, sc, np.zeros((5, 2)), S.densify_config(grad_threshold=0.0002, min_opacity=0.005,
+                                                                  enabled=True)) == 3
+    assert np.all(1.0 / (1.0 + np.exp(-ctx.get_model(0).opacities)) > 0.005)
+
+
+def test_known_answer_single_clone_and_clone_plus_split(ctx):
+    assert _densify(ctx, _params(1), [[0.5, 0.5]]) == 2
+    m = ctx.get_model(0)
+    assert m.positions[0, 0] == m.positions[1, 0]
+    sc = _params(3)
+    sc.scales[1] = np.log(np.float32(5.0))
+    assert _densify(ctx, sc, [[0.5, 0.5], [0.5, 0.5], [0.0, 0.0]]) == 5
+
+
+def test_known_answer_cycles_empty_and_reset(ctx):
+    assert _densify(ctx, _params(2), np.full((2, 2), 0.5)) == 4
+    ctx.density_accumulate(np.full((4, 2), 0.5, np.float32), None)
+    assert ctx.densify_and_prune(S.densify_config(**KA_CFG), 100.0) == 8
+    m = ctx.get_model(0)
+    assert np.all(np.isfinite(m.positions)) and np.all(np.isfinite(m.opacities))
+    sc = _params(3)
+    sc.opacities[:] = _inv_sigmoid(0.001)
+    assert _densify(ctx, sc, np.zeros((3, 2)), S.densify_config(min_opacity=0.005, enabled=True)) == 0
+    sc = _params(3)
+    sc.opacities[:] = [_inv_sigmoid(0.9), _inv_sigmoid(0.5), _inv_sigmoid(0.1)]
+    ctx.set_raw_params(sc)
+    ctx.reset_opacity()
+    assert np.allclose(1.0 / (1.0 + np.exp(-ctx.get_model(0).opacities)), 0.01, atol=1e-4)
