@@ -254,15 +254,25 @@ __device__ __forceinline__ void opt8(const StepParams& sp, uint4& p, uint4& m, u
 constexpr int kCB = 128;          // Gaussians (= threads) per CTA of the adjoint
 constexpr int kShPitch = 49;      // padded row of the per-Gaussian SH gradients in shared memory
 
-template <typename S>
+// One view: the SH gradient of coefficient k is basis[k / 3] * geff[k % 3], so the
+// CTA keeps the 16 + 3 factors per Gaussian (SoA, conflict-free) instead of the
+// 48 products, and fits 5 CTAs per SM.  Several views sum the products: g_sh.
+template <typename S, bool MULTI>
 struct __align__(16) ChosenBwdShared {
     uint4 sh[kCB * 6];            // 16-bit SH, up to 48 per Gaussian (6 x 16 bytes)
     uint4 attr[kCB];              // 16-bit attributes, 8 per Gaussian
     float pos[3 * kCB];
     float dm2[2 * kCB], dcon[3 * kCB], drgb[3 * kCB], dop[kCB];
     float g_pos[3 * kCB], g_sc[3 * kCB], g_rot[4 * kCB], g_op[kCB];
-    float g_sh[kShPitch * kCB];
+    float g_sh[MULTI ? kShPitch * kCB : 1];
+    float basis[MULTI ? 1 : 16 * kCB];   // [basis][Gaussian]
+    float geff[MULTI ? 1 : 3 * kCB];     // [channel][Gaussian]
     unsigned long long bar;       // completion of the bulk copies into the arrays above
+    // SH gradient of coefficient kk of the CTA's Gaussian t
+    __device__ __forceinline__ float gsh(int t, int kk) const {
+        if (MULTI) return g_sh[kShPitch * t + kk];
+        return basis[(kk / 3) * kCB + t] * geff[(kk % 3) * kCB + t];
+    }
 };
 
 // One CTA per 128 consecutive Gaussians: bulk copies of their parameters and
@@ -272,11 +282,11 @@ struct __align__(16) ChosenBwdShared {
 // gradients, then Adam over the CTA's contiguous parameter slice with 16-byte
 // accesses and stochastic rounding (and, when asked, the FP32 gradients).
 template <typename S, bool MULTI>
-__global__ void __launch_bounds__(kCB) k_chosen_backward(const StepParams* __restrict__ spp, int N, int mc3,
+__global__ void __launch_bounds__(kCB, MULTI ? 4 : 5) k_chosen_backward(const StepParams* __restrict__ spp, int N, int mc3,
                                                          ChosenPtrs c, RGradPtrs rg, GradPtrs gout, Control* ctrl,
                                                          int n_views) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    ChosenBwdShared<S>& sm = *reinterpret_cast<ChosenBwdShared<S>*>(smem_raw);
+    ChosenBwdShared<S, MULTI>& sm = *reinterpret_cast<ChosenBwdShared<S, MULTI>*>(smem_raw);
     const StepParams& sp = *spp;
     if ((ctrl->status & (kStatusOverflow | kStatusTimeout)) || sp.persist->sticky_overflow) return;
     const int tid = threadIdx.x;
@@ -338,7 +348,12 @@ __global__ void __launch_bounds__(kCB) k_chosen_backward(const StepParams* __res
 #pragma unroll
         for (int k = 0; k < 4; k++) sm.g_rot[4 * tid + k] = 0.f;
         sm.g_op[tid] = 0.f;
-        for (int k = 0; k < mc3; k++) sm.g_sh[kShPitch * tid + k] = 0.f;
+        if (MULTI) {
+            for (int k = 0; k < mc3; k++) sm.g_sh[kShPitch * tid + k] = 0.f;
+        } else {
+            for (int k = 0; k < 16; k++) sm.basis[k * kCB + tid] = 0.f;
+            for (int k = 0; k < 3; k++) sm.geff[k * kCB + tid] = 0.f;
+        }
     }
     for (int v = 0; v < (MULTI ? n_views : 1); v++) {
         const long long e0 = (long long)v * N + g0;   // this view's first (view, Gaussian) entry
@@ -413,7 +428,14 @@ __global__ void __launch_bounds__(kCB) k_chosen_backward(const StepParams* __res
 #pragma unroll
                 for (int k = 0; k < 4; k++) sm.g_rot[4 * tid + k] += o.gq[k];
                 sm.g_op[tid] += o.gop;
-                for (int k = 0; k < mc3; k++) sm.g_sh[kShPitch * tid + k] += o.basis[k / 3] * o.geff[k % 3];
+                if (MULTI) {
+                    for (int k = 0; k < mc3; k++) sm.g_sh[kShPitch * tid + k] += o.basis[k / 3] * o.geff[k % 3];
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 16; k++) sm.basis[k * kCB + tid] = o.basis[k];
+#pragma unroll
+                    for (int k = 0; k < 3; k++) sm.geff[k * kCB + tid] = o.geff[k];
+                }
             }
         }
     }
@@ -428,7 +450,7 @@ __global__ void __launch_bounds__(kCB) k_chosen_backward(const StepParams* __res
         for (int e = tid; e < ng; e += kCB) gout.g_op[g0 + e] = sm.g_op[e];
         for (int e = tid; e < mc3 * ng; e += kCB) {
             const int t = e / mc3, k = e - t * mc3;
-            gout.g_sh[(size_t)mc3 * g0 + e] = sm.g_sh[kShPitch * t + k];
+            gout.g_sh[(size_t)mc3 * g0 + e] = sm.gsh(t, k);
         }
     }
     const long long sh0 = (long long)mc3 * g0;
@@ -449,7 +471,7 @@ __global__ void __launch_bounds__(kCB) k_chosen_backward(const StepParams* __res
 #pragma unroll
             for (int k = 0; k < 8; k++) {
                 const int e = 8 * q + k, t = e / mc3;
-                gg[k] = sm.g_sh[kShPitch * t + (e - t * mc3)];
+                gg[k] = sm.gsh(t, e - t * mc3);
             }
             opt8<S>(sp, pp, mm, vv, gg, lr_sh, (unsigned)(sh0 + 8 * q), 0x5bd1e995u);
             p4[q] = pp;
@@ -461,7 +483,7 @@ __global__ void __launch_bounds__(kCB) k_chosen_backward(const StepParams* __res
         for (int e = tid; e < mc3 * ng; e += kCB) {
             const int t = e / mc3;
             float m = __bfloat162float(msh[sh0 + e]), v = __bfloat162float(vsh[sh0 + e]);
-            const float pn = opt_elem(sp, ldf(shs[e]), m, v, sm.g_sh[kShPitch * t + (e - t * mc3)], sp.lr_sh);
+            const float pn = opt_elem(sp, ldf(shs[e]), m, v, sm.gsh(t, e - t * mc3), sp.lr_sh);
             unsigned rp, rm, rv;
             sr_words((unsigned)(sh0 + e) ^ 0x5bd1e995u, sp.seed, rp, rm, rv);
             shw[sh0 + e] = cvt_sr<S>(pn, rp);
@@ -568,20 +590,16 @@ cudaError_t launch_chosen_backward_adam(cudaStream_t st, const StepParams* sp, i
     if (N <= 0) return cudaSuccess;
     if (mc3 > 48) return cudaErrorInvalidValue;
     const int grid = grid_for(N, kCB);
-    const int smem = (int)sizeof(ChosenBwdShared<__half>);   // same size for both 16-bit types
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaError_t e[4] = {
-            cudaFuncSetAttribute(k_chosen_backward<__half, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
-            cudaFuncSetAttribute(k_chosen_backward<__nv_bfloat16, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 smem),
-            cudaFuncSetAttribute(k_chosen_backward<__half, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
-            cudaFuncSetAttribute(k_chosen_backward<__nv_bfloat16, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 smem)};
-        for (cudaError_t x : e)
-            if (x != cudaSuccess) return x;
-        attr_set = true;
-    }
+    // the same sizes for both 16-bit types
+    const int smem1 = (int)sizeof(ChosenBwdShared<__half, false>), smemv = (int)sizeof(ChosenBwdShared<__half, true>);
+    const int smem = n_views > 1 ? smemv : smem1;
+    static std::atomic<unsigned long long> attr_done[4];
+    cudaError_t e[4] = {set_smem_once(attr_done[0], k_chosen_backward<__half, false>, smem1),
+                        set_smem_once(attr_done[1], k_chosen_backward<__nv_bfloat16, false>, smem1),
+                        set_smem_once(attr_done[2], k_chosen_backward<__half, true>, smemv),
+                        set_smem_once(attr_done[3], k_chosen_backward<__nv_bfloat16, true>, smemv)};
+    for (cudaError_t x : e)
+        if (x != cudaSuccess) return x;
     if (n_views > 1) {
         if (fp16) k_chosen_backward<__half, true><<<grid, kCB, smem, st>>>(sp, N, mc3, c, rg, g, ctrl, n_views);
         else k_chosen_backward<__nv_bfloat16, true><<<grid, kCB, smem, st>>>(sp, N, mc3, c, rg, g, ctrl, n_views);

@@ -1,6 +1,7 @@
 // common.cuh -- device-side shared definitions of the 3DGS hot path.
 #pragma once
 
+#include <atomic>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -69,6 +70,22 @@ struct Control {
     unsigned work[2];                 // persistent multi-view rasterisers: next tile of the forward / backward
 };
 constexpr size_t kControlReadback = 24;
+
+// Raises `kernel`'s dynamic shared-memory limit to `bytes` on the current
+// device, once per device: the attribute belongs to the device's context, so a
+// process with contexts on several GPUs sets it on each.  `done` keeps one bit
+// per device ordinal.
+template <class K>
+inline cudaError_t set_smem_once(std::atomic<unsigned long long>& done, K* kernel, int bytes) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (done.load(std::memory_order_acquire) & bit) return cudaSuccess;
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) done.fetch_or(bit, std::memory_order_acq_rel);
+    return e;
+}
 
 // ---- relaxed 64-bit accesses for decoupled look-back descriptors ----
 __device__ __forceinline__ unsigned long long ld_relaxed(const unsigned long long* p) {

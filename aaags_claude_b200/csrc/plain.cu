@@ -746,13 +746,9 @@ cudaError_t launch_bin_arrays_e3(cudaStream_t st, const StepParams* sp, int N, S
 cudaError_t launch_raster_e3(cudaStream_t st, const StepParams* sp, int num_tiles, const unsigned* ranges,
                              const unsigned* order, const unsigned* vals, E3Ptrs e, PixelPtrs px, Control* ctrl) {
     if (num_tiles <= 0) return cudaSuccess;
-    static bool attr_set = false;   // per process: the kernel's dynamic shared memory above 48 KB
-    if (!attr_set) {
-        cudaError_t err =
-            cudaFuncSetAttribute(k_raster_e3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kE3RasterSmem);
-        if (err != cudaSuccess) return err;
-        attr_set = true;
-    }
+    static std::atomic<unsigned long long> attr_done{0};   // the kernel's dynamic shared memory above 48 KB
+    const cudaError_t err = set_smem_once(attr_done, k_raster_e3, (int)kE3RasterSmem);
+    if (err != cudaSuccess) return err;
     k_raster_e3<<<num_tiles, kE3Threads, kE3RasterSmem, st>>>(sp, ranges, order, vals, e, px, ctrl);
     return cudaGetLastError();
 }
@@ -781,13 +777,9 @@ template <int MODE, int MC3>
 cudaError_t launch_bwd_mc(cudaStream_t st, const StepParams* sp, int N, ModelPtrs raw, AdamPtrs adam, ScreenPtrs s,
                           RGradPtrs rg, GradPtrs gout, Control* ctrl) {
     const int smem = MODE == kBwdFused ? (int)sizeof(BwdShared) : (int)offsetof(BwdShared, m_sh);
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaError_t e =
-            cudaFuncSetAttribute(k_preprocess_bwd<MODE, MC3>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e != cudaSuccess) return e;
-        attr_set = true;
-    }
+    static std::atomic<unsigned long long> attr_done{0};
+    const cudaError_t e = set_smem_once(attr_done, k_preprocess_bwd<MODE, MC3>, smem);
+    if (e != cudaSuccess) return e;
     k_preprocess_bwd<MODE, MC3><<<blocks_for(N, kBwdG), kBwdG, smem, st>>>(sp, N, raw, adam, s, rg, gout, ctrl);
     return cudaGetLastError();
 }

@@ -261,14 +261,10 @@ cudaError_t radix_sort_impl(cudaStream_t st, const StepParams* sp, int first, in
     *which = 0;
     if (capacity == 0 || passes <= first) return cudaSuccess;
     if (!count) count = &ctrl->total_pairs;
-    static bool attr_set = false;
+    static std::atomic<unsigned long long> attr_done{0};
     const int smem = (int)sizeof(SweepShared<K>);
-    if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(k_onesweep<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e != cudaSuccess) return e;
-        attr_set = true;
-    }
-    cudaError_t e;
+    cudaError_t e = set_smem_once(attr_done, k_onesweep<K>, smem);
+    if (e != cudaSuccess) return e;
     if (!hist_done) {
         k_radix_hist<K><<<2 * 148, kHistThreads, 0, st>>>(keys0, capacity, first, passes, slot_base, count, ctrl);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
