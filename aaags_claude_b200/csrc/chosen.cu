@@ -25,11 +25,13 @@
 namespace gs3d {
 namespace {
 
-// Blend decision of the reduced-storage forward: fast exp, no exact recheck.
+// Blend decision of the reduced-storage forward on the base-2 exponent
+// q = power * log2(e) (q_coeffs / q_at): alpha = o * 2^q, no exact recheck.
 struct FastBlend {
-    __device__ __forceinline__ static int decide(float power, float o, float T, float& alpha, float& e,
+    static constexpr bool kBase2 = true;
+    __device__ __forceinline__ static int decide(float q, float o, float T, float& alpha, float& e,
                                                  float& test_T) {
-        e = __expf(power);
+        e = ex2_approx(q);
         alpha = fmin_ref(0.99f, o * e);
         if (alpha < kAlphaMin) return 0;
         test_T = T * (1.0f - alpha);

@@ -53,6 +53,7 @@ __device__ __forceinline__ int blend_decision(float power, float o, float T, flo
 
 // The plain form's blend decision for the shared forward kernel.
 struct ExactBlend {
+    static constexpr bool kBase2 = false;   // decides on the reference's power (power_rn)
     __device__ __forceinline__ static int decide(float power, float o, float T, float& alpha, float& e,
                                                  float& test_T) {
         return blend_decision(power, o, T, alpha, e, test_T);

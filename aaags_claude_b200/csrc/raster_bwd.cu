@@ -41,13 +41,15 @@ __device__ __forceinline__ bool alpha_accept_fast(float power, float o, float& a
 // forward; the reduced-storage form's forward decides on o * __expf(power)
 // alone, and so does its backward (same power_rn, same __expf, same product).
 struct PlainAccept {
+    static constexpr bool kBase2 = false;   // the reference's power (power_rn)
     __device__ __forceinline__ static bool accept(float power, float o, float& alpha, float& e) {
         return alpha_accept_fast(power, o, alpha, e);
     }
 };
 struct FastAccept {
-    __device__ __forceinline__ static bool accept(float power, float o, float& alpha, float& e) {
-        e = __expf(power);
+    static constexpr bool kBase2 = true;    // q = power * log2(e) from q_coeffs / q_at, as the forward
+    __device__ __forceinline__ static bool accept(float q, float o, float& alpha, float& e) {
+        e = ex2_approx(q);
         alpha = fmin_ref(0.99f, o * e);
         return !(alpha < kAlphaMin);
     }
@@ -62,6 +64,19 @@ struct FastAccept {
 // sums its 32 * PPT pixels with warp_sum8 + warp_sum, the warps meet in
 // shared-memory accumulators and each Gaussian gets one set of global atomics
 // per tile.  PPT = 2 by default; the autotuner may pick 1 or 4.
+//
+// Algebra that keeps the per-pixel work small (same sums, regrouped):
+//  - accum_rec (rasterizer_backward_cpu.cpp:101-108) enters d_alpha only as
+//    sum_ch accum_rec[ch] * dC[ch], so each pixel carries that one scalar D:
+//    d_alpha = T_i (cd - D) with cd = sum_ch c[ch] dC[ch], then D += alpha (cd - D);
+//  - d_power = o * t with t = d_alpha * exp(power), and the geometric factors
+//    of d_means2D / d_conics (:126-132) are polynomials in (dx, dy) with the
+//    Gaussian's conic as coefficients, where dx is fixed per thread.  A thread
+//    sums t, t dy, t dy^2 over its pixels; the warp reduces t, t dx, t dy,
+//    t dx^2, t dx dy, t dy^2 (plus d_rgb) and the conic / opacity factors are
+//    applied once per Gaussian when the tile's sums are flushed:
+//      d_mean.x = -o (a S_x + b S_y)     d_mean.y = -o (c S_y + b S_x)
+//      d_conic  = -o (S_xx / 2, S_xy, S_yy / 2)     d_opacity = S_1.
 constexpr int kBwdBatch = 256;
 
 //
@@ -82,7 +97,7 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_bwd(const StepParams* __re
     __shared__ unsigned s_idx[kBwdBatch];
     __shared__ float s_thr[kBwdBatch];
     __shared__ float4 s_box[kBwdBatch];
-    __shared__ float s_acc[9][kBwdBatch];   // r, g, b, opacity, mean.x, mean.y, conic a, b, c
+    __shared__ float s_acc[9][kBwdBatch];   // r, g, b, S_1, S_x, S_y, S_xx, S_xy, S_yy
     __shared__ unsigned s_maxlast;
     __shared__ unsigned s_next;
     constexpr int kBwdThreads = 256 / PPT;
@@ -119,7 +134,7 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_bwd(const StepParams* __re
     const int ybase = ty * kTile + 2 * PPT * (int)warp + (int)(lane >> 4);
     const unsigned rs = ranges[2 * tile];
     const float fx = (float)x;
-    float fy[PPT], T[PPT], dC[PPT][3], acc[PPT][3];
+    float fy[PPT], T[PPT], dC[PPT][3], D[PPT];
     unsigned last[PPT];
 #pragma unroll
     for (int p = 0; p < PPT; p++) {
@@ -144,8 +159,7 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_bwd(const StepParams* __re
                 dC[p][2] = px.d_image[3 * pix + 2];
             }
         }
-#pragma unroll
-        for (int ch = 0; ch < 3; ch++) acc[p][ch] = sp.cfg.bg_color[ch];
+        D[p] = sp.cfg.bg_color[0] * dC[p][0] + sp.cfg.bg_color[1] * dC[p][1] + sp.cfg.bg_color[2] * dC[p][2];
     }
     if (threadIdx.x == 0) s_maxlast = 0;
     __syncthreads();
@@ -174,7 +188,7 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_bwd(const StepParams* __re
                 s_r0[e] = r0;
                 s_r1[e] = r1;
                 s_b[e] = s.col_b[gi];
-                s_thr[e] = thr;
+                s_thr[e] = Accept::kBase2 ? __fmul_rn(thr, kLog2e) : thr;   // the forward's threshold
                 s_box[e] = skip_box(r0, r1, thr);
             }
 #pragma unroll
@@ -190,47 +204,45 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_bwd(const StepParams* __re
             const float4 c = s_r1[k];
             const float cb = s_b[k];
             const float thr = s_thr[k];
+            const float dx = a.x - fx;
+            const float3 kq = Accept::kBase2 ? q_coeffs(a, c, dx) : make_float3(0.f, 0.f, 0.f);
             bool contrib = false;
-            float gv[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-            float g_cc = 0.f;
+            float gr = 0.f, gg = 0.f, gb = 0.f;     // d_rgb
+            float t0 = 0.f, t1 = 0.f, t2 = 0.f;     // sum of t, t dy, t dy^2 over this thread's pixels
 #pragma unroll
             for (int p = 0; p < PPT; p++) {
                 if (jj < last[p]) {
-                    const float dx = a.x - fx, dy = a.y - fy[p];
-                    const float power = power_rn(a, c, dx, dy);
+                    const float dy = a.y - fy[p];
+                    const float power = Accept::kBase2 ? q_at(kq, dy) : power_rn(a, c, dx, dy);
                     float alpha, ep;
                     if (!(power < thr) && !(power > 0.0f) && Accept::accept(power, c.y, alpha, ep)) {
                         contrib = true;
                         const float oma = 1.0f - alpha;
                         const float Ti = (oma > 1e-6f) ? __fdividef(T[p], oma) : 0.0f;
                         const float aT = alpha * Ti;
-                        gv[0] += aT * dC[p][0];
-                        gv[1] += aT * dC[p][1];
-                        gv[2] += aT * dC[p][2];
-                        float d_alpha = 0.0f;
-                        d_alpha += Ti * (c.z - acc[p][0]) * dC[p][0];
-                        d_alpha += Ti * (c.w - acc[p][1]) * dC[p][1];
-                        d_alpha += Ti * (cb - acc[p][2]) * dC[p][2];
-                        acc[p][0] = alpha * c.z + oma * acc[p][0];
-                        acc[p][1] = alpha * c.w + oma * acc[p][1];
-                        acc[p][2] = alpha * cb + oma * acc[p][2];
+                        gr += aT * dC[p][0];
+                        gg += aT * dC[p][1];
+                        gb += aT * dC[p][2];
+                        const float cd = c.z * dC[p][0] + c.w * dC[p][1] + cb * dC[p][2];
+                        const float diff = cd - D[p];
+                        D[p] += alpha * diff;
                         T[p] = Ti;
                         if (alpha < 0.99f) {
-                            const float d_power = d_alpha * c.y * ep;
-                            gv[3] += d_alpha * ep;
-                            gv[4] += d_power * (-a.z * dx - a.w * dy);
-                            gv[5] += d_power * (-c.x * dy - a.w * dx);
-                            gv[6] += d_power * (-0.5f * dx * dx);
-                            gv[7] += d_power * (-dx * dy);
-                            g_cc += d_power * (-0.5f * dy * dy);
+                            const float t = Ti * diff * ep;   // d_alpha * exp(power)
+                            t0 += t;
+                            const float tdy = t * dy;
+                            t1 += tdy;
+                            t2 += tdy * dy;
                         }
                     }
                 }
             }
             if (__any_sync(0xffffffffu, contrib)) {
+                const float tx0 = t0 * dx;
+                const float gv[8] = {gr, gg, gb, t0, tx0, t1, tx0 * dx, t1 * dx};
                 int idx;
                 const float s8 = warp_sum8(gv, &idx);
-                const float s9 = warp_sum(g_cc);
+                const float s9 = warp_sum(t2);
                 if ((lane & 3) == 0 && s8 != 0.0f) atomicAdd(&s_acc[idx][k], s8);
                 if (lane == 1 && s9 != 0.0f) atomicAdd(&s_acc[8][k], s9);
             }
@@ -243,11 +255,15 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_bwd(const StepParams* __re
                 float* const dst[9] = {&g.drgb[3 * gi], &g.drgb[3 * gi + 1], &g.drgb[3 * gi + 2], &g.dop[gi],
                                        &g.dm2[2 * gi], &g.dm2[2 * gi + 1], &g.dcon[3 * gi], &g.dcon[3 * gi + 1],
                                        &g.dcon[3 * gi + 2]};
+                const float4 r0 = s_r0[e];
+                const float o = s_r1[e].y, cc = s_r1[e].x;
+                const float Sx = s_acc[4][e], Sy = s_acc[5][e];
+                const float val[9] = {s_acc[0][e], s_acc[1][e], s_acc[2][e], s_acc[3][e],
+                                      -o * (r0.z * Sx + r0.w * Sy), -o * (cc * Sy + r0.w * Sx),
+                                      -0.5f * o * s_acc[6][e], -o * s_acc[7][e], -0.5f * o * s_acc[8][e]};
 #pragma unroll
-                for (int v = 0; v < 9; v++) {
-                    const float av = s_acc[v][e];
-                    if (av != 0.0f) atomicAdd(dst[v], av);
-                }
+                for (int v = 0; v < 9; v++)
+                    if (val[v] != 0.0f) atomicAdd(dst[v], val[v]);
             }
         }
         __syncthreads();

@@ -50,6 +50,36 @@ __device__ __forceinline__ bool box_misses(float4 b, float x0, float x1, float y
     return b.y < x0 || b.x > x1 || b.w < y0 || b.z > y1;
 }
 
+// ---- base-2 exponent of the reduced-storage form ----
+// The reduced-storage rasterisers evaluate alpha = o * 2^q with
+// q = power * log2(e) written as q = A + dy (B + H dy): A = -0.5 log2(e) a dx^2
+// and B = -log2(e) b dx are shared by every pixel of a thread (its pixels share
+// the column x, so dx), H = -0.5 log2(e) c by every pixel, leaving two FMAs per
+// pixel.  Every operation carries explicit rounding, so the forward and the
+// backward (different FMA-contraction settings) get the same q, the same
+// 2^q and the same accept decisions.
+constexpr float kLog2e = 1.4426950408889634f;
+
+__device__ __forceinline__ float ex2_approx(float q) {
+    float r;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(q));
+    return r;
+}
+
+// skip_threshold in base-2 units: q below it gives alpha < 1/255 for certain
+// (the natural bound's 1e-3 margin becomes 1.44e-3, far above rounding).
+__device__ __forceinline__ float skip_threshold2(float o) { return __fmul_rn(skip_threshold(o), kLog2e); }
+
+// Per (Gaussian, thread) coefficients of q: x = A, y = B, z = H.
+__device__ __forceinline__ float3 q_coeffs(float4 r0, float4 r1, float dx) {
+    const float A = __fmul_rn(__fmul_rn(r0.z, -0.5f * kLog2e), __fmul_rn(dx, dx));
+    const float B = __fmul_rn(r0.w, __fmul_rn(-kLog2e, dx));
+    const float H = __fmul_rn(r1.x, -0.5f * kLog2e);
+    return make_float3(A, B, H);
+}
+
+__device__ __forceinline__ float q_at(float3 k, float dy) { return __fmaf_rn(dy, __fmaf_rn(k.z, dy, k.y), k.x); }
+
 __device__ __forceinline__ float warp_sum(float v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);

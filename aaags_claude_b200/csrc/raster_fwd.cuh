@@ -14,7 +14,8 @@ namespace {
 
 // Rasterizer forward (rasterizer_cpu.cpp:38-53, 137-198).  Blend::decide is
 // the alpha / transmittance decision (0 skip, 1 blend, 2 stop): exact in the
-// plain form, fast exp in the reduced-storage form.  One CTA of 128
+// plain form on the reference's power (power_rn), fast base-2 exponent in the
+// reduced-storage form (Blend::kBase2: q_coeffs / q_at, ex2).  One CTA of 128
 // threads per 16x16 tile, two pixels per thread: warp w owns the 16x4 strip
 // of rows 4w..4w+3, a thread the pixels (x, 4w + lane/16) and
 // (x, 4w + 2 + lane/16).  Batches of 256 records are gathered into shared
@@ -112,7 +113,7 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_fwd(const StepParams* __re
                 s_r0[e] = r0;
                 s_r1[e] = r1;
                 s_b[e] = s.col_b[g];
-                s_thr[e] = thr;
+                s_thr[e] = Blend::kBase2 ? __fmul_rn(thr, kLog2e) : thr;   // in the units of Blend's exponent
                 s_box[e] = skip_box(r0, r1, thr);
             }
         }
@@ -128,11 +129,12 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_fwd(const StepParams* __re
             const float4 c = s_r1[k];
             const float thr = s_thr[k];
             const float dx = a.x - fx;
+            const float3 kq = Blend::kBase2 ? q_coeffs(a, c, dx) : make_float3(0.f, 0.f, 0.f);
 #pragma unroll
             for (int p = 0; p < PPT; p++) {
                 if (done[p]) continue;
                 const float dy = a.y - fy[p];
-                const float power = power_rn(a, c, dx, dy);
+                const float power = Blend::kBase2 ? q_at(kq, dy) : power_rn(a, c, dx, dy);
                 if (power < thr || power > 0.0f) continue;
                 float alpha, e, test_T;
                 const int dec = Blend::decide(power, c.y, T[p], alpha, e, test_T);
