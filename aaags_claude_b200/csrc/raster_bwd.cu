@@ -60,6 +60,8 @@ struct FastAccept {
 // T_final instead of a replayed per-pixel list.  One CTA of 256 / PPT threads
 // per 16x16 tile, PPT pixels per thread: warp w owns the strip of rows
 // 2*PPT*w .. 2*PPT*w + 2*PPT - 1, a thread the pixels (x, 2*PPT*w + lane/16 + 2p).
+// A warp walks its compacted list of the batch entries whose alpha >= 1/255
+// ellipse reaches its strip (band_rows), from the back.
 // Per Gaussian of a batch a thread adds its pixels' contributions, the warp
 // sums its 32 * PPT pixels with warp_sum8 + warp_sum, the warps meet in
 // shared-memory accumulators and each Gaussian gets one set of global atomics
@@ -96,11 +98,13 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_bwd(const StepParams* __re
     __shared__ float s_b[kBwdBatch];
     __shared__ unsigned s_idx[kBwdBatch];
     __shared__ float s_thr[kBwdBatch];
-    __shared__ float4 s_box[kBwdBatch];
     __shared__ float s_acc[9][kBwdBatch];   // r, g, b, S_1, S_x, S_y, S_xx, S_xy, S_yy
     __shared__ unsigned s_maxlast;
     __shared__ unsigned s_next;
     constexpr int kBwdThreads = 256 / PPT;
+    constexpr int kNW = kBwdThreads / 32;
+    __shared__ unsigned char s_mask[kBwdBatch];       // warps whose strip the Gaussian can reach
+    __shared__ unsigned char s_list[kNW][kBwdBatch];  // per warp: its batch entries, ascending
     if (FROM_SIGN && ((ctrl->status & kStatusOverflow) || spp->persist->sticky_overflow)) return;
     for (int iter = 0;; iter++) {
     int tile;
@@ -171,8 +175,7 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_bwd(const StepParams* __re
     const unsigned maxlast = s_maxlast;
     if (maxlast <= rs) continue;   // uniform: nothing of this tile contributed
     const unsigned wlast = __reduce_max_sync(0xffffffffu, mylast);
-    const float wx0 = (float)(tx * kTile), wx1 = wx0 + (float)(kTile - 1);
-    const float wy0 = (float)(ty * kTile + 2 * PPT * (int)warp), wy1 = wy0 + (float)(2 * PPT - 1);
+    const float wx0 = (float)(tx * kTile), wx1 = wx0 + (float)(kTile - 1), ty0 = (float)(ty * kTile);
     // batches [bs, be) walked from the back; the first one ends at maxlast
     for (unsigned be = maxlast; be > rs;) {
         const unsigned bs = (be - rs > (unsigned)kBwdBatch) ? be - kBwdBatch : rs;
@@ -189,7 +192,7 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_bwd(const StepParams* __re
                 s_r1[e] = r1;
                 s_b[e] = s.col_b[gi];
                 s_thr[e] = Accept::kBase2 ? __fmul_rn(thr, kLog2e) : thr;   // the forward's threshold
-                s_box[e] = skip_box(r0, r1, thr);
+                s_mask[e] = (unsigned char)strip_mask<kNW, 2 * PPT>(band_rows(r0, r1, thr, wx0, wx1), ty0);
             }
 #pragma unroll
             for (int v = 0; v < 9; v++) s_acc[v][e] = 0.0f;
@@ -197,8 +200,9 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_bwd(const StepParams* __re
         __syncthreads();
         // this warp only needs the entries below its own last contributor
         const int kstart = (int)(min(be, wlast) - min(bs, wlast)) - 1;
-        for (int k = kstart; k >= 0; k--) {
-            if (box_misses(s_box[k], wx0, wx1, wy0, wy1)) continue;   // warp-uniform
+        const int nl = warp_list(s_mask, kstart + 1, warp, s_list[warp]);
+        for (int i = nl - 1; i >= 0; i--) {
+            const int k = s_list[warp][i];
             const unsigned jj = bs + (unsigned)k;
             const float4 a = s_r0[k];
             const float4 c = s_r1[k];

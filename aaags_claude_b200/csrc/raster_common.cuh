@@ -2,7 +2,7 @@
 // no FMA contraction) and the backward (raster_bwd.cu, FMA contraction on).
 // Everything here either rounds the same under both builds (power_rn, whose
 // operations carry explicit rounding) or is a conservative bound whose margin
-// dwarfs any rounding difference (skip_threshold, skip_box).
+// dwarfs any rounding difference (skip_threshold, band_rows).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -31,19 +31,74 @@ __device__ __forceinline__ float power_rn(float4 r0, float4 r1, float dx, float 
 // is the one the exact alpha test would take.
 __device__ __forceinline__ float skip_threshold(float o) { return logf(kAlphaMin / o) - 1e-3f; }
 
-// Axis-aligned box (xmin, xmax, ymin, ymax) in pixels outside of which the
-// Gaussian's power is below skip_threshold: the ellipse
-// d^T C d <= -2 thr has half extents sqrt(-2 thr * Sigma_xx), sqrt(-2 thr *
-// Sigma_yy) with Sigma = C^-1, widened by one pixel for rounding.  A warp
-// whose pixels all lie outside it skips the Gaussian without evaluating it.
-__device__ __forceinline__ float4 skip_box(float4 r0, float4 r1, float thr) {
+// Rows of a tile's column band where a Gaussian can reach power >= thr.
+// The ellipse E = {d : a dx^2 + 2 b dx dy + c dy^2 <= t2}, t2 = -2 thr, with
+// d = mean - pixel and conic (a, b, c) = (r0.z, r0.w, r1.x), is cut by the band
+// of pixel columns [x0, x1]; returns the pixel rows [y0, y1] of that cut,
+// y0 > y1 when E misses the band (or alpha can never reach 1/255).  Over
+// dx in the band the top of E is (-b dx + sqrt(t2 c - det dx^2)) / c, a concave
+// function whose maximum is E's topmost point dy = sqrt(t2 a / det) at
+// dx = -b dy / a when that lies in the band and a band edge otherwise (the
+// bottom likewise); edges outside E's x extent |dx| <= sqrt(t2 c / det) only
+// add candidates, which keeps the range conservative.  The rows are widened by
+// one pixel plus 1e-3 of the extent, above the FP32 rounding of these steps
+// for det >= 1e-3 a c; more elongated conics are not culled.  A pixel outside
+// the range has power < thr, so alpha < 1/255 (skip_threshold's margin), and
+// the blend would skip it: culling it changes no result.
+// Square root from the hardware reciprocal square root (relative error ~1e-7),
+// for the conservative bounds below; 0 for x <= 0.
+__device__ __forceinline__ float sqrt_bound(float x) { return x > 0.0f ? x * rsqrtf(x) : 0.0f; }
+
+__device__ __forceinline__ float2 band_rows(float4 r0, float4 r1, float thr, float x0, float x1) {
     const float t2 = -2.0f * thr;
-    const float det = r0.z * r1.x - r0.w * r0.w;   // conic a c - b^2
-    if (!(t2 > 0.0f)) return make_float4(1e30f, -1e30f, 1e30f, -1e30f);     // never reaches alpha 1/255
-    if (!(det > 0.0f)) return make_float4(-1e30f, 1e30f, -1e30f, 1e30f);    // not positive definite: no culling
-    const float ex = sqrtf(t2 * r1.x / det) + 1.0f;
-    const float ey = sqrtf(t2 * r0.z / det) + 1.0f;
-    return make_float4(r0.x - ex, r0.x + ex, r0.y - ey, r0.y + ey);
+    const float a = r0.z, b = r0.w, c = r1.x;
+    if (!(t2 > 0.0f)) return make_float2(1e30f, -1e30f);   // alpha never reaches 1/255
+    const float det = fmaf(a, c, -b * b);
+    if (!(a > 0.0f) || !(c > 0.0f) || !(det >= 1e-3f * a * c)) return make_float2(-1e30f, 1e30f);
+    const float idet = __fdividef(1.0f, det);
+    const float xext = sqrt_bound(t2 * c * idet), yext = sqrt_bound(t2 * a * idet);
+    const float dlo = r0.x - x1, dhi = r0.x - x0;   // dx over the band
+    const float mx = 1.0f + 1e-3f * xext;
+    if (dlo > xext + mx || dhi < -xext - mx) return make_float2(1e30f, -1e30f);
+    const float ic = __fdividef(1.0f, c);
+    const float slo = sqrt_bound(t2 * c - det * dlo * dlo);
+    const float shi = sqrt_bound(t2 * c - det * dhi * dhi);
+    float up = fmaxf((slo - b * dlo) * ic, (shi - b * dhi) * ic);
+    float dn = fminf((-slo - b * dlo) * ic, (-shi - b * dhi) * ic);
+    const float xtop = __fdividef(-b * yext, a);    // dx of the topmost point; the bottom is at -xtop
+    if (xtop >= dlo && xtop <= dhi) up = yext;
+    if (-xtop >= dlo && -xtop <= dhi) dn = -yext;
+    const float my = 1.0f + 1e-3f * yext;
+    return make_float2(r0.y - up - my, r0.y - dn + my);   // rows y = mean.y - dy
+}
+
+// Bit w set when the warp strip of rows [ty0 + ROWS w, ty0 + ROWS w + ROWS - 1]
+// meets the rows [yr.x, yr.y].
+template <int NW, int ROWS>
+__device__ __forceinline__ unsigned strip_mask(float2 yr, float ty0) {
+    unsigned m = 0;
+#pragma unroll
+    for (int w = 0; w < NW; w++) {
+        const float s0 = ty0 + (float)(ROWS * w), s1 = s0 + (float)(ROWS - 1);
+        if (yr.y >= s0 && yr.x <= s1) m |= 1u << w;
+    }
+    return m;
+}
+
+// The entries e < n of a batch whose mask has this warp's bit, in ascending
+// order, written to list; returns their number.  Whole warp.
+__device__ __forceinline__ int warp_list(const unsigned char* mask, int n, unsigned warp, unsigned char* list) {
+    const unsigned lane = threadIdx.x & 31;
+    int m = 0;
+    for (int c0 = 0; c0 < n; c0 += 32) {
+        const int e = c0 + (int)lane;
+        const bool mine = e < n && ((mask[e] >> warp) & 1u);
+        const unsigned bal = __ballot_sync(0xffffffffu, mine);
+        if (mine) list[m + __popc(bal & ((1u << lane) - 1u))] = (unsigned char)e;
+        m += __popc(bal);
+    }
+    __syncwarp();
+    return m;
 }
 
 __device__ __forceinline__ bool box_misses(float4 b, float x0, float x1, float y0, float y1) {

@@ -19,7 +19,9 @@ namespace {
 // threads per 16x16 tile, two pixels per thread: warp w owns the 16x4 strip
 // of rows 4w..4w+3, a thread the pixels (x, 4w + lane/16) and
 // (x, 4w + 2 + lane/16).  Batches of 256 records are gathered into shared
-// memory; a warp skips a Gaussian whose skip box misses its strip; the CTA
+// memory with, per record, the warps whose strip the Gaussian can reach
+// (band_rows: the rows of the tile's columns inside its alpha >= 1/255
+// ellipse); each warp walks its own compacted list of the batch; the CTA
 // stops once every pixel saturated.  Optional fused L1 (sign byte per pixel,
 // double-precision loss sum).
 //
@@ -45,8 +47,10 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_fwd(const StepParams* __re
     __shared__ float4 s_r1[kFwdBatch];
     __shared__ float s_b[kFwdBatch];
     __shared__ float s_thr[kFwdBatch];
-    __shared__ float4 s_box[kFwdBatch];
     constexpr int kFwdThreads = 256 / PPT;
+    constexpr int kNW = kFwdThreads / 32;
+    __shared__ unsigned char s_mask[kFwdBatch];       // warps whose strip the Gaussian can reach
+    __shared__ unsigned char s_list[kNW][kFwdBatch];  // per warp: its batch entries, ascending
     __shared__ double s_loss[kFwdThreads / 32];
     __shared__ unsigned s_next;
     for (int iter = 0;; iter++) {
@@ -81,8 +85,7 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_fwd(const StepParams* __re
     const int ybase = ty * kTile + 2 * PPT * (int)warp + (int)(lane >> 4);
     const unsigned rs = ranges[2 * tile], re = ranges[2 * tile + 1];
     const float fx = (float)x;
-    const float wx0 = (float)(tx * kTile), wx1 = wx0 + (float)(kTile - 1);
-    const float wy0 = (float)(ty * kTile + 2 * PPT * (int)warp), wy1 = wy0 + (float)(2 * PPT - 1);
+    const float wx0 = (float)(tx * kTile), wx1 = wx0 + (float)(kTile - 1), ty0 = (float)(ty * kTile);
     float fy[PPT], T[PPT], C[PPT][3];
     int cnt[PPT];
     unsigned last[PPT];
@@ -114,17 +117,18 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_fwd(const StepParams* __re
                 s_r1[e] = r1;
                 s_b[e] = s.col_b[g];
                 s_thr[e] = Blend::kBase2 ? __fmul_rn(thr, kLog2e) : thr;   // in the units of Blend's exponent
-                s_box[e] = skip_box(r0, r1, thr);
+                s_mask[e] = (unsigned char)strip_mask<kNW, 2 * PPT>(band_rows(r0, r1, thr, wx0, wx1), ty0);
             }
         }
         __syncthreads();
         const int nb = (int)min((unsigned)kFwdBatch, re - b);
-        for (int k = 0; k < nb; k++) {
+        const int nl = warp_list(s_mask, nb, warp, s_list[warp]);
+        for (int i = 0; i < nl; i++) {
             bool thread_done = true;
 #pragma unroll
             for (int p = 0; p < PPT; p++) thread_done = thread_done && done[p];
             if (thread_done) break;
-            if (box_misses(s_box[k], wx0, wx1, wy0, wy1)) continue;
+            const int k = s_list[warp][i];
             const float4 a = s_r0[k];
             const float4 c = s_r1[k];
             const float thr = s_thr[k];
