@@ -5,9 +5,9 @@
 // Design (one-sweep, after Adinets & Merrill, "Onesweep: A Faster Least
 // Significant Digit Radix Sort for GPUs", 2022):
 //   k_radix_hist  one read of the keys counts the 8-bit digits of every pass
-//                 (warp-aggregated with __match_any_sync).
+//                 (warp-aggregated with peer_mask8).
 //   k_onesweep    one launch per pass.  A CTA takes the next 4096-key tile by
-//                 ticket, ranks its keys per warp with __match_any_sync /
+//                 ticket, ranks its keys per warp with peer_mask8 /
 //                 popc, publishes its per-digit counts and finds its global
 //                 per-digit offsets by decoupled look-back (bounded waits),
 //                 reorders the tile in shared memory and writes it out in
@@ -28,6 +28,21 @@ namespace gs3d {
 namespace {
 
 constexpr int kHistThreads = 512;
+
+// The lanes of `mask` whose 8-bit digit equals this lane's (this lane
+// included), from eight ballots over the digit's bits: the same set
+// __match_any_sync returns, at a fraction of its cost when the digits of a
+// warp are mostly distinct.  Called by every lane of `mask`.
+__device__ __forceinline__ unsigned peer_mask8(unsigned mask, unsigned d) {
+    unsigned peers = mask;
+#pragma unroll
+    for (int b = 0; b < 8; b++) {
+        const bool bit = (d >> b) & 1u;
+        const unsigned bal = __ballot_sync(mask, bit);
+        peers &= bit ? bal : ~bal;
+    }
+    return peers;
+}
 
 // Digit histograms of digits [first, passes) (digit d = key bits 8d..8d+7)
 // into ctrl->hist[slot_base + d - first].
@@ -50,7 +65,7 @@ __global__ void __launch_bounds__(kHistThreads) k_radix_hist(const K* __restrict
             const K key = keys[i];
             for (int p = first; p < passes; p++) {
                 const unsigned d = (unsigned)(key >> (8 * p)) & 255u;
-                const unsigned peers = __match_any_sync(mask, d);
+                const unsigned peers = peer_mask8(mask, d);
                 if (lane == (unsigned)(__ffs(peers) - 1)) atomicAdd(&s_h[p * 256 + d], (unsigned)__popc(peers));
             }
         }
@@ -128,7 +143,7 @@ __global__ void __launch_bounds__(kSortThreads, sizeof(K) == 4 ? 4 : 2) k_oneswe
 #pragma unroll
     for (int it = 0; it < kSortItems; it++) {
         const unsigned d = (unsigned)(key[it] >> shift) & 255u;
-        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        const unsigned peers = peer_mask8(0xffffffffu, d);
         const unsigned prior = sm.whist[warp][d];
         __syncwarp();
         if (lane == (unsigned)(__ffs(peers) - 1)) sm.whist[warp][d] = prior + (unsigned)__popc(peers);
