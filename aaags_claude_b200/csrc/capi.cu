@@ -653,10 +653,12 @@ int seq_front_depth_first(gs3dc_ctx* c) {
         CK(launch_preprocess_plain(c->stream, c->sp_dev, c->N, c->model_raw, false, model_ptrs(c),
                                    screen_ptrs(c, false), pr, c->ctrl, DepthKeys{c->dkeys[0].p, c->dvals[0].p}));
     if ((rc = mark(c, GS3DC_STAGE_SORT_HIST))) return rc;
+    // the reduced form orders by the depth's upper 24 bits (relative steps of 2^-15; ties keep index order)
+    const int depth_first_digit = chosen ? kChosenDepthSkip : 0;
     int dw = 0;
     CK(launch_radix_sort32(c->stream, c->sp_dev, kDepthDigits, 0, false, (unsigned long long)c->N, c->dkeys[0].p,
                            c->dvals[0].p, c->dkeys[1].p, c->dvals[1].p, c->ddesc.p, c->ddesc_stride, c->ctrl, &dw,
-                           nullptr, &c->ctrl->gauss_keys));
+                           nullptr, &c->ctrl->gauss_keys, depth_first_digit));
     CK(launch_emit_ranked(c->stream, c->sp_dev, c->N, c->dvals[dw].p, screen_ptrs(c, false), pr, c->ctrl,
                           chosen ? c->c_rects.p : nullptr));
     if ((rc = mark(c, GS3DC_STAGE_SORT_PASSES))) return rc;
@@ -667,7 +669,8 @@ int seq_front_depth_first(gs3dc_ctx* c) {
     if ((rc = mark(c, GS3DC_STAGE_RANGES))) return rc;
     CK(launch_tile_ranges32(c->stream, c->cap, tk[which], c->ranges.p, c->ctrl));
     CK(launch_tile_order(c->stream, c->ranges.p, c->num_tiles, c->tile_order.p));
-    c->kernels_last += c->N > 0 ? 1 + (1 + kDepthDigits) + 1 + (tile_digits > 0 ? tile_digits : 0) + 2 : 2;
+    c->kernels_last +=
+        c->N > 0 ? 1 + (1 + kDepthDigits - depth_first_digit) + 1 + (tile_digits > 0 ? tile_digits : 0) + 2 : 2;
     return GS3DC_OK;
 }
 
@@ -925,7 +928,7 @@ int batch_buffers(gs3dc_ctx* c, const BatchShape& sh) {
 }
 
 // One multi-view step: preprocess of every (view, Gaussian), stable sort by
-// (view, depth) in 5 passes, emission in that order with global tile ids,
+// (view, depth's upper 24 bits) in 4 passes, emission in that order with global tile ids,
 // stable sort of the pairs on the tile bits, ranges and a heavy-first order of
 // all views' tiles, persistent forward and backward rasterisers over that
 // order, then the adjoint summed over the views and one Adam step.
@@ -944,10 +947,10 @@ int seq_batch(gs3dc_ctx* c, const BatchShape& sh) {
                            c->stream));
     CK(launch_chosen_preprocess(c->stream, views, c->N, c->form == GS3DC_FORM_FP16, chosen_ptrs(c), batch_screen(c),
                                 DepthKeys{nullptr, b.dvals[0].p, b.dkeys[0].p}, b.rects.p, c->ctrl, sh.V));
-    // digits 0..3: depth bits, digit 4: the view
+    // digits 1..3: the depth's upper 24 bits (as the single-view reduced form), digit 4: the view
     int dw = 0;
     CK(launch_radix_sort(c->stream, views, 5, vn, b.dkeys[0].p, b.dvals[0].p, b.dkeys[1].p, b.dvals[1].p, b.ddesc.p,
-                         dstride, c->ctrl, &dw, nullptr, 0, &c->ctrl->gauss_keys));
+                         dstride, c->ctrl, &dw, nullptr, kChosenDepthSkip, &c->ctrl->gauss_keys));
     PairPtrs pr{nullptr, b.vals[0].p, b.cap, c->scan_desc, b.keys[0].p};
     CK(launch_emit_ranked(c->stream, views, (int)vn, b.dvals[dw].p, batch_screen(c), pr, c->ctrl, b.rects.p, c->N,
                           5));
@@ -969,7 +972,7 @@ int seq_batch(gs3dc_ctx* c, const BatchShape& sh) {
                                    chosen_ptrs(c), batch_rgrads(c),
                                    c->keep_grads ? grad_ptrs(c) : GradPtrs{nullptr, nullptr, nullptr, nullptr, nullptr},
                                    c->ctrl, sh.V));
-    c->kernels_last = 1 + 1 + 5 + 1 + (sh.tile_digits > 0 ? sh.tile_digits : 0) + 2 + 3;
+    c->kernels_last = 1 + 1 + (5 - kChosenDepthSkip) + 1 + (sh.tile_digits > 0 ? sh.tile_digits : 0) + 2 + 3;
     return GS3DC_OK;
 }
 

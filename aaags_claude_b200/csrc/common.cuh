@@ -14,6 +14,8 @@ constexpr int kBlock = 256;          // threads per CTA of the per-Gaussian and 
 constexpr int kMaxPasses = 8;         // radix passes (8-bit digits over <= 64 key bits)
 constexpr int kDepthDigits = 4;       // depth-first ordering: digits of the Gaussian depth sort (control slots
                                       // 0..3); the pair sort on the tile bits uses slots kDepthDigits..
+constexpr int kChosenDepthSkip = 1;   // reduced-storage form: low depth digits left out of the depth sort
+                                      // (ordering by the upper 24 bits: sign, exponent, 15 mantissa bits)
 
 // Device-status bits (Control::status).
 constexpr unsigned kStatusOverflow = 1u;  // more tile pairs than capacity

@@ -243,15 +243,16 @@ cudaError_t launch_radix_sort(cudaStream_t st, const StepParams* sp, int sort_pa
 cudaError_t launch_tile_ranges(cudaStream_t st, unsigned long long capacity,
                                const unsigned long long* keys_sorted, unsigned* ranges, Control* ctrl);
 
-// Stable LSD sort of 32-bit keys (tile ids) over digits [0, digits), control
+// Stable LSD sort of 32-bit keys over digits [first_digit, digits), control
 // slots slot_base..; hist_done: the digit histograms are already in those slots.
-// desc holds digits * desc_stride zeroed descriptors.
+// desc holds (digits - first_digit) * desc_stride zeroed descriptors.
 // count (optional): device word with the number of keys (default: the pair count).
+// first_digit > 0 orders by the key's upper bits only (ties keep input order).
 cudaError_t launch_radix_sort32(cudaStream_t st, const StepParams* sp, int digits, int slot_base, bool hist_done,
                                 unsigned long long capacity, unsigned* keys0, unsigned* vals0, unsigned* keys1,
                                 unsigned* vals1, unsigned long long* desc, unsigned long long desc_stride,
                                 Control* ctrl, int* which, cudaEvent_t after_hist = nullptr,
-                                const unsigned long long* count = nullptr);
+                                const unsigned long long* count = nullptr, int first_digit = 0);
 cudaError_t launch_tile_ranges32(cudaStream_t st, unsigned long long capacity, const unsigned* tiles_sorted,
                                  unsigned* ranges, Control* ctrl);
 // Ranges of global tile ids (the view's tile_base + local id) over pairs

@@ -144,10 +144,14 @@ __global__ void __launch_bounds__(kSortThreads, sizeof(K) == 4 ? 4 : 2) k_oneswe
     for (int it = 0; it < kSortItems; it++) {
         const unsigned d = (unsigned)(key[it] >> shift) & 255u;
         const unsigned peers = peer_mask8(0xffffffffu, d);
-        const unsigned prior = sm.whist[warp][d];
-        __syncwarp();
-        if (lane == (unsigned)(__ffs(peers) - 1)) sm.whist[warp][d] = prior + (unsigned)__popc(peers);
-        __syncwarp();
+        // one leader per digit adds the group's size to the warp's count and
+        // shuffles the old value to its group.  The atomic has returned before
+        // the shuffle that every lane passes, so it precedes every atomic of
+        // the warp's later items: the value counts this digit in earlier items.
+        const int leader = __ffs(peers) - 1;
+        unsigned prior = 0;
+        if (lane == leader) prior = atomicAdd(&sm.whist[warp][d], (unsigned)__popc(peers));
+        prior = __shfl_sync(0xffffffffu, prior, leader);
         rank[it] = prior + (unsigned)__popc(peers & lt_mask);
     }
     __syncthreads();
@@ -323,9 +327,10 @@ cudaError_t launch_radix_sort(cudaStream_t st, const StepParams* sp, int passes,
 cudaError_t launch_radix_sort32(cudaStream_t st, const StepParams* sp, int digits, int slot_base, bool hist_done,
                                 unsigned long long capacity, unsigned* keys0, unsigned* vals0, unsigned* keys1,
                                 unsigned* vals1, unsigned long long* desc, unsigned long long desc_stride,
-                                Control* ctrl, int* which, cudaEvent_t after_hist, const unsigned long long* count) {
-    return radix_sort_impl<unsigned>(st, sp, 0, digits, slot_base, hist_done, capacity, keys0, vals0, keys1, vals1,
-                                     desc, desc_stride, ctrl, which, after_hist, count);
+                                Control* ctrl, int* which, cudaEvent_t after_hist, const unsigned long long* count,
+                                int first_digit) {
+    return radix_sort_impl<unsigned>(st, sp, first_digit, digits, slot_base, hist_done, capacity, keys0, vals0, keys1,
+                                     vals1, desc, desc_stride, ctrl, which, after_hist, count);
 }
 
 cudaError_t launch_tile_ranges(cudaStream_t st, unsigned long long capacity, const unsigned long long* keys_sorted,
