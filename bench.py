@@ -191,7 +191,7 @@ def stage_bytes(N: int, P: int, X: int, T: int, passes: int, mc3: int = 48, dept
         m16 = 24 + 2 * (16 + 2 * mc3)
         return {
             "preprocess": N * (s16 + 48 + 8 + 8),        # params in; records, depth key + index, rect out
-            "sort_hist": N * 4 + 4 * N * 16 + N * 32 + P * 8 + P * 4,
+            "sort_hist": N * 4 + 3 * N * 16 + N * 32 + P * 8 + P * 4,   # 3 depth passes (upper 24 bits)
             "sort_passes": P * 16,
             "ranges": P * 4 + T * 8,
             "raster_fwd": P * 40 + X * 37,
