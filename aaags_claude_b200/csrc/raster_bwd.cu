@@ -98,7 +98,9 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_bwd(const StepParams* __re
     __shared__ float s_b[kBwdBatch];
     __shared__ unsigned s_idx[kBwdBatch];
     __shared__ float s_thr[kBwdBatch];
-    __shared__ float s_acc[9][kBwdBatch];   // r, g, b, S_1, S_x, S_y, S_xx, S_xy, S_yy
+    // r, g, b, S_1, S_x, S_y, S_xx, S_xy, S_yy; rows padded by one word so that the
+    // eight lanes adding values 0..7 of one Gaussian hit eight different banks
+    __shared__ float s_acc[9][kBwdBatch + 1];
     __shared__ unsigned s_maxlast;
     __shared__ unsigned s_next;
     constexpr int kBwdThreads = 256 / PPT;
