@@ -34,7 +34,7 @@ struct FastBlend {
         e = ex2_approx(q);
         alpha = fmin_ref(0.99f, o * e);
         if (alpha < kAlphaMin) return 0;
-        test_T = T * (1.0f - alpha);
+        test_T = fmaf(-alpha, T, T);   // T (1 - alpha)
         if (test_T < kTMin) return 2;
         return 1;
     }

@@ -221,10 +221,11 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_bwd(const StepParams* __re
                     const float dy = a.y - fy[p];
                     const float power = Accept::kBase2 ? q_at(kq, dy) : power_rn(a, c, dx, dy);
                     float alpha, ep;
-                    if (!(power < thr) && !(power > 0.0f) && Accept::accept(power, c.y, alpha, ep)) {
+                    const bool in_range = Accept::kBase2 ? power >= thr : !(power < thr) && !(power > 0.0f);
+                    if (in_range && Accept::accept(power, c.y, alpha, ep)) {
                         contrib = true;
-                        const float oma = 1.0f - alpha;
-                        const float Ti = (oma > 1e-6f) ? __fdividef(T[p], oma) : 0.0f;
+                        // alpha <= 0.99, so 1 - alpha >= 0.01 passes the reference's 1e-6 guard (:84-85)
+                        const float Ti = __fdividef(T[p], 1.0f - alpha);
                         const float aT = alpha * Ti;
                         gr += aT * dC[p][0];
                         gg += aT * dC[p][1];

@@ -139,7 +139,9 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_fwd(const StepParams* __re
                 if (done[p]) continue;
                 const float dy = a.y - fy[p];
                 const float power = Blend::kBase2 ? q_at(kq, dy) : power_rn(a, c, dx, dy);
-                if (power < thr || power > 0.0f) continue;
+                // the reference also skips power > 0 (rasterizer_cpu.cpp:146-148); with a positive-definite
+                // conic that is rounding at the mean, where the reduced form blends alpha = o instead
+                if (Blend::kBase2 ? !(power >= thr) : (power < thr || power > 0.0f)) continue;
                 float alpha, e, test_T;
                 const int dec = Blend::decide(power, c.y, T[p], alpha, e, test_T);
                 if (dec == 0) continue;
@@ -147,9 +149,16 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_fwd(const StepParams* __re
                     done[p] = true;
                     continue;
                 }
-                C[p][0] += c.z * alpha * T[p];
-                C[p][1] += c.w * alpha * T[p];
-                C[p][2] += s_b[k] * alpha * T[p];
+                if (Blend::kBase2) {
+                    const float aT = alpha * T[p];
+                    C[p][0] += c.z * aT;
+                    C[p][1] += c.w * aT;
+                    C[p][2] += s_b[k] * aT;
+                } else {   // the reference's (c * alpha) * T
+                    C[p][0] += c.z * alpha * T[p];
+                    C[p][1] += c.w * alpha * T[p];
+                    C[p][2] += s_b[k] * alpha * T[p];
+                }
                 T[p] = test_T;
                 cnt[p]++;
                 last[p] = b + (unsigned)k + 1u;
