@@ -186,15 +186,16 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_bwd(const StepParams* __re
             const unsigned j = bs + (unsigned)e;
             if (j < be) {
                 const unsigned gi = vals[j];
-                const float4 r0 = s.rec0[gi];
-                const float4 r1 = s.rec1[gi];
+                float4 r0 = s.rec0[gi];
+                float4 r1 = s.rec1[gi];
                 const float thr = skip_threshold(r1.y);
                 s_idx[e] = gi;
-                s_r0[e] = r0;
-                s_r1[e] = r1;
                 s_b[e] = s.col_b[gi];
                 s_thr[e] = Accept::kBase2 ? __fmul_rn(thr, kLog2e) : thr;   // the forward's threshold
                 s_mask[e] = (unsigned char)strip_mask<kNW, 2 * PPT>(band_rows(r0, r1, thr, wx0, wx1), ty0);
+                if (Accept::kBase2) q_scale(r0, r1);   // as the forward stages it
+                s_r0[e] = r0;
+                s_r1[e] = r1;
             }
 #pragma unroll
             for (int v = 0; v < 9; v++) s_acc[v][e] = 0.0f;
@@ -265,8 +266,13 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_bwd(const StepParams* __re
                 const float4 r0 = s_r0[e];
                 const float o = s_r1[e].y, cc = s_r1[e].x;
                 const float Sx = s_acc[4][e], Sy = s_acc[5][e];
-                const float val[9] = {s_acc[0][e], s_acc[1][e], s_acc[2][e], s_acc[3][e],
-                                      -o * (r0.z * Sx + r0.w * Sy), -o * (cc * Sy + r0.w * Sx),
+                // d_mean = -o (a S_x + b S_y, c S_y + b S_x); from the pre-scaled conic
+                // (-a L / 2, -b L, -c L / 2), L = log2(e): (o / L) (2 A S_x + B S_y, 2 H S_y + B S_x)
+                const float dmx = Accept::kBase2 ? (o * (1.0f / kLog2e)) * (2.0f * r0.z * Sx + r0.w * Sy)
+                                                 : -o * (r0.z * Sx + r0.w * Sy);
+                const float dmy = Accept::kBase2 ? (o * (1.0f / kLog2e)) * (2.0f * cc * Sy + r0.w * Sx)
+                                                 : -o * (cc * Sy + r0.w * Sx);
+                const float val[9] = {s_acc[0][e], s_acc[1][e], s_acc[2][e], s_acc[3][e], dmx, dmy,
                                       -0.5f * o * s_acc[6][e], -o * s_acc[7][e], -0.5f * o * s_acc[8][e]};
 #pragma unroll
                 for (int v = 0; v < 9; v++)

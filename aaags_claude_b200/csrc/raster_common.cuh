@@ -125,12 +125,17 @@ __device__ __forceinline__ float ex2_approx(float q) {
 // (the natural bound's 1e-3 margin becomes 1.44e-3, far above rounding).
 __device__ __forceinline__ float skip_threshold2(float o) { return __fmul_rn(skip_threshold(o), kLog2e); }
 
-// Per (Gaussian, thread) coefficients of q: x = A, y = B, z = H.
-__device__ __forceinline__ float3 q_coeffs(float4 r0, float4 r1, float dx) {
-    const float A = __fmul_rn(__fmul_rn(r0.z, -0.5f * kLog2e), __fmul_rn(dx, dx));
-    const float B = __fmul_rn(r0.w, __fmul_rn(-kLog2e, dx));
-    const float H = __fmul_rn(r1.x, -0.5f * kLog2e);
-    return make_float3(A, B, H);
+// The staged record of the reduced form carries the conic pre-scaled for q:
+// (x, y, -0.5 log2(e) a, -log2(e) b), (-0.5 log2(e) c, o, r, g).
+__device__ __forceinline__ void q_scale(float4& r0, float4& r1) {
+    r0.z = __fmul_rn(r0.z, -0.5f * kLog2e);
+    r0.w = __fmul_rn(r0.w, -kLog2e);
+    r1.x = __fmul_rn(r1.x, -0.5f * kLog2e);
+}
+
+// Per (Gaussian, thread) coefficients of q from a pre-scaled record: x = A, y = B, z = H.
+__device__ __forceinline__ float3 q_coeffs(float4 r0s, float4 r1s, float dx) {
+    return make_float3(__fmul_rn(r0s.z, __fmul_rn(dx, dx)), __fmul_rn(r0s.w, dx), r1s.x);
 }
 
 __device__ __forceinline__ float q_at(float3 k, float dy) { return __fmaf_rn(dy, __fmaf_rn(k.z, dy, k.y), k.x); }

@@ -110,14 +110,15 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_fwd(const StepParams* __re
             const unsigned j = b + (unsigned)e;
             if (j < re) {
                 const unsigned g = vals[j];
-                const float4 r0 = s.rec0[g];
-                const float4 r1 = s.rec1[g];
+                float4 r0 = s.rec0[g];
+                float4 r1 = s.rec1[g];
                 const float thr = skip_threshold(r1.y);
-                s_r0[e] = r0;
-                s_r1[e] = r1;
                 s_b[e] = s.col_b[g];
                 s_thr[e] = Blend::kBase2 ? __fmul_rn(thr, kLog2e) : thr;   // in the units of Blend's exponent
                 s_mask[e] = (unsigned char)strip_mask<kNW, 2 * PPT>(band_rows(r0, r1, thr, wx0, wx1), ty0);
+                if (Blend::kBase2) q_scale(r0, r1);
+                s_r0[e] = r0;
+                s_r1[e] = r1;
             }
         }
         __syncthreads();
