@@ -192,7 +192,6 @@ __global__ void __launch_bounds__(kSortThreads, sizeof(K) == 4 ? 4 : 2) k_oneswe
 }
 
 __device__ __forceinline__ unsigned tile_of(unsigned long long key) { return (unsigned)(key >> 32); }
-__device__ __forceinline__ unsigned tile_of(unsigned key) { return key; }   // tile-only keys
 
 // One thread per key (the grid covers the capacity): a tile's range starts
 // where its key differs from the previous one and ends where it differs
@@ -223,6 +222,39 @@ __global__ void k_ranges(const K* __restrict__ keys, unsigned long long capacity
     const unsigned t = tile_of(keys[i]);
     if (i == 0 || tile_of(keys[i - 1]) != t) ranges[2 * t] = (unsigned)i;
     if (i == P - 1 || tile_of(keys[i + 1]) != t) ranges[2 * t + 1] = (unsigned)(i + 1);
+}
+
+// Tile ranges over sorted 32-bit tile ids, four ids per thread from one
+// 16-byte load: a run ends at i + 1 where id i differs from id i + 1 (or i is
+// the last pair), and the next run starts there.
+__global__ void k_ranges32(const unsigned* __restrict__ tiles, unsigned long long capacity,
+                           unsigned* __restrict__ ranges, Control* ctrl) {
+    const unsigned long long P = min(ctrl->total_pairs, capacity);
+    const unsigned long long i0 = 4ull * ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x);
+    if (i0 >= P) return;
+    unsigned t[5];
+    if (i0 + 4 <= capacity) {
+        const uint4 v = *reinterpret_cast<const uint4*>(tiles + i0);
+        t[0] = v.x;
+        t[1] = v.y;
+        t[2] = v.z;
+        t[3] = v.w;
+    } else {
+#pragma unroll
+        for (int j = 0; j < 4; j++) t[j] = i0 + j < P ? tiles[i0 + j] : 0u;
+    }
+    t[4] = i0 + 4 < P ? tiles[i0 + 4] : 0u;
+    if (i0 == 0) ranges[2 * t[0]] = 0u;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const unsigned long long i = i0 + (unsigned long long)j;
+        if (i >= P) break;
+        const bool last = i + 1 == P;
+        if (last || t[j + 1] != t[j]) {
+            ranges[2 * t[j] + 1] = (unsigned)(i + 1);
+            if (!last) ranges[2 * t[j + 1]] = (unsigned)(i + 1);
+        }
+    }
 }
 
 // Heavy-first tile order: one CTA buckets the tiles by floor(log2(pairs))
@@ -352,7 +384,7 @@ cudaError_t launch_tile_ranges_views(cudaStream_t st, unsigned long long capacit
 cudaError_t launch_tile_ranges32(cudaStream_t st, unsigned long long capacity, const unsigned* tiles_sorted,
                                  unsigned* ranges, Control* ctrl) {
     if (capacity == 0) return cudaSuccess;
-    k_ranges<<<(unsigned)((capacity + 255) / 256), 256, 0, st>>>(tiles_sorted, capacity, ranges, ctrl);
+    k_ranges32<<<(unsigned)((capacity + 1023) / 1024), 256, 0, st>>>(tiles_sorted, capacity, ranges, ctrl);
     return cudaGetLastError();
 }
 
