@@ -163,7 +163,17 @@ __global__ void __launch_bounds__(kBlock) k_chosen_preprocess(const StepParams* 
     load_attr<S>(c.attr, i, rsc, &rop, rq);
     activate_one(rsc, rq, rop, sc, q, &op);
     Proj r;
-    const bool vis = project_one<S>(sp, p, sc, q, op, static_cast<const S*>(c.sh) + (size_t)mc3 * i, r);
+    const S* shrow = static_cast<const S*>(c.sh) + (size_t)mc3 * i;
+    bool vis;
+    if (mc3 == 48) {
+        // degree-3 storage: the 96-byte row (16-byte aligned) as six 16-byte loads
+        uint4 shv[6];
+#pragma unroll
+        for (int k = 0; k < 6; k++) shv[k] = reinterpret_cast<const uint4*>(shrow)[k];
+        vis = project_one<S>(sp, p, sc, q, op, reinterpret_cast<const S*>(shv), r);
+    } else {
+        vis = project_one<S>(sp, p, sc, q, op, shrow, r);
+    }
     int cnt = 0;
     uint2 rect = make_uint2(0u, 0u);
     unsigned dbits = 0xFFFFFFFFu;

@@ -143,6 +143,52 @@ __device__ __forceinline__ unsigned long long lookback_exclusive_strided(
     return excl;
 }
 
+// The same look-back for one counter, run by a whole warp: lane l examines
+// block base - l, so one round covers 32 predecessors.  The prefix ends at the
+// nearest block that published an inclusive prefix; every block after it must
+// have published at least its aggregate, else the round is polled again
+// (bounded as above).  Blocks before block 0 count as a zero prefix.  Every
+// lane returns the exclusive prefix.
+__device__ __forceinline__ unsigned long long warp_lookback_exclusive(unsigned long long* desc, int blk,
+                                                                      unsigned long long aggregate,
+                                                                      unsigned* status, unsigned spin_limit) {
+    const int lane = (int)(threadIdx.x & 31);
+    unsigned long long* mine = desc + blk;
+    if (blk == 0) {
+        if (lane == 0) st_relaxed(mine, kDescPrefix | aggregate);
+        return 0ull;
+    }
+    if (lane == 0) st_relaxed(mine, kDescAgg | aggregate);
+    unsigned long long excl = 0;
+    int base = blk - 1;
+    unsigned spins = 0;
+    for (;;) {
+        const int j = base - lane;
+        const unsigned long long d = j >= 0 ? ld_relaxed(desc + j) : kDescPrefix;
+        const unsigned long long flag = d & ~kDescValue;
+        const unsigned empty = __ballot_sync(0xffffffffu, flag == 0ull);
+        const unsigned pre = __ballot_sync(0xffffffffu, flag == kDescPrefix);
+        const int first = pre ? __ffs(pre) - 1 : 31;   // lanes 0..first hold the blocks to add
+        const unsigned need = first == 31 ? 0xffffffffu : ((2u << first) - 1u);
+        if (empty & need) {
+            if (++spins > spin_limit) {
+                if (lane == 0) atomicOr(status, kStatusTimeout);
+                break;
+            }
+            __nanosleep(32);
+            continue;
+        }
+        unsigned long long v = lane <= first ? (d & kDescValue) : 0ull;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        excl += v;
+        if (pre) break;
+        base -= 32;
+    }
+    if (lane == 0) st_relaxed(mine, kDescPrefix | (excl + aggregate));
+    return excl;
+}
+
 __device__ __forceinline__ unsigned long long lookback_exclusive(unsigned long long* desc, int blk,
                                                                  unsigned long long aggregate,
                                                                  unsigned* status, unsigned spin_limit) {

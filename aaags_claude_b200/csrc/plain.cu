@@ -114,14 +114,16 @@ __device__ __forceinline__ void scan_and_emit(EmitShared& sm, int blk, unsigned 
     sm.gid[tid] = gid;
     sm.tbase[tid] = tile_base_t;
     sm.gx[tid] = grid_x_t < 0 ? grid_x : grid_x_t;
-    if (tid == 0) {
+    if (tid < 32) {
         const unsigned long long ex =
-            lookback_exclusive(pr.scan_desc, blk, (unsigned long long)total, &ctrl->status, spin_limit);
-        sm.base = ex;
-        if (blk == (int)gridDim.x - 1) ctrl->total_pairs = ex + (unsigned long long)total;
-        if (ex + (unsigned long long)total > pr.capacity) {
-            atomicOr(&ctrl->status, kStatusOverflow);
-            if (persist) atomicOr(&persist->sticky_overflow, 1u);
+            warp_lookback_exclusive(pr.scan_desc, blk, (unsigned long long)total, &ctrl->status, spin_limit);
+        if (tid == 0) {
+            sm.base = ex;
+            if (blk == (int)gridDim.x - 1) ctrl->total_pairs = ex + (unsigned long long)total;
+            if (ex + (unsigned long long)total > pr.capacity) {
+                atomicOr(&ctrl->status, kStatusOverflow);
+                if (persist) atomicOr(&persist->sticky_overflow, 1u);
+            }
         }
     }
     __syncthreads();
@@ -183,7 +185,17 @@ __global__ void __launch_bounds__(kBlock) k_preprocess(const StepParams* __restr
             op = m.op[i];
         }
         Proj r;
-        const bool vis = project_one(sp, p, sc, q, op, m.sh + (size_t)mc3 * i, r);
+        const float* shrow = m.sh + (size_t)mc3 * i;
+        bool vis;
+        if (mc3 == 48) {
+            // degree-3 storage: the 192-byte row (16-byte aligned) as twelve 16-byte loads
+            float4 shv[12];
+#pragma unroll
+            for (int k = 0; k < 12; k++) shv[k] = reinterpret_cast<const float4*>(shrow)[k];
+            vis = project_one(sp, p, sc, q, op, reinterpret_cast<const float*>(shv), r);
+        } else {
+            vis = project_one(sp, p, sc, q, op, shrow, r);
+        }
         if (vis) {
             cnt = (r.rmx[1] - r.rmn[1]) * (r.rmx[0] - r.rmn[0]);
             rx = r.rmn[0];

@@ -287,10 +287,19 @@ __global__ void __launch_bounds__(1024) k_tile_order(const unsigned* __restrict_
     }
 }
 
-// One CTA plays block 1 of a look-back whose block 0 never publishes: the
-// wait must run out after spin_limit polls and raise kStatusTimeout.
+// One warp plays block 1 of a look-back whose block 0 never publishes, first
+// with the warp-wide look-back, then with the one-thread look-back: each wait
+// must run out after spin_limit polls; kStatusTimeout is raised when both did.
 __global__ void k_wait_selftest(unsigned long long* desc, unsigned* status, unsigned spin_limit) {
-    if (threadIdx.x == 0) lookback_exclusive_strided(desc, 1, 1, 0, 5ull, status, spin_limit);
+    __shared__ unsigned s_warp, s_thread;
+    if (threadIdx.x == 0) s_warp = s_thread = 0u;
+    __syncwarp();
+    warp_lookback_exclusive(desc, 1, 5ull, &s_warp, spin_limit);
+    __syncwarp();
+    if (threadIdx.x == 0) {
+        lookback_exclusive_strided(desc, 1, 1, 0, 5ull, &s_thread, spin_limit);
+        if ((s_warp & kStatusTimeout) && (s_thread & kStatusTimeout)) atomicOr(status, kStatusTimeout);
+    }
 }
 
 }  // namespace
