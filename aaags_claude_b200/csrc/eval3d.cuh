@@ -607,11 +607,22 @@ __global__ void __launch_bounds__(kBlock) k_preprocess_e3(const StepParams* __re
             float d[3];
             view_dir(p, cam.cam_pos, d);
             const float* sh = m.sh + (size_t)sp.max_coeffs * 3 * i;
+            auto colour = [&](const float* shr) {
 #pragma unroll
-            for (int c = 0; c < 3; c++) {
-                float v = fmax_ref(0.0f, sh_channel(sp.sh_deg_fwd, sh, c, d[0], d[1], d[2]) + 0.5f);
-                if (!sp.cfg.training) v = fmin_ref(1.0f, v);
-                rgb[c] = v;
+                for (int c = 0; c < 3; c++) {
+                    float v = fmax_ref(0.0f, sh_channel(sp.sh_deg_fwd, shr, c, d[0], d[1], d[2]) + 0.5f);
+                    if (!sp.cfg.training) v = fmin_ref(1.0f, v);
+                    rgb[c] = v;
+                }
+            };
+            if (sp.max_coeffs == 16) {
+                // degree-3 storage: the 192-byte row (16-byte aligned) as twelve 16-byte loads
+                float4 shv[12];
+#pragma unroll
+                for (int k = 0; k < 12; k++) shv[k] = reinterpret_cast<const float4*>(sh)[k];
+                colour(reinterpret_cast<const float*>(shv));
+            } else {
+                colour(sh);
             }
             depth = pv[2];
             vis = true;

@@ -95,9 +95,8 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_bwd(const StepParams* __re
                                                             int n_views = 1, unsigned n_tiles = 0) {
     __shared__ float4 s_r0[kBwdBatch];
     __shared__ float4 s_r1[kBwdBatch];
-    __shared__ float s_b[kBwdBatch];
+    __shared__ float2 s_bt[kBwdBatch];   // (blue, skip threshold): one 8-byte load per Gaussian
     __shared__ unsigned s_idx[kBwdBatch];
-    __shared__ float s_thr[kBwdBatch];
     // r, g, b, S_1, S_x, S_y, S_xx, S_xy, S_yy; rows padded by one word so that the
     // eight lanes adding values 0..7 of one Gaussian hit eight different banks
     __shared__ float s_acc[9][kBwdBatch + 1];
@@ -190,8 +189,7 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_bwd(const StepParams* __re
                 float4 r1 = s.rec1[gi];
                 const float thr = skip_threshold(r1.y);
                 s_idx[e] = gi;
-                s_b[e] = s.col_b[gi];
-                s_thr[e] = Accept::kBase2 ? __fmul_rn(thr, kLog2e) : thr;   // the forward's threshold
+                s_bt[e] = make_float2(s.col_b[gi], Accept::kBase2 ? __fmul_rn(thr, kLog2e) : thr);   // forward's
                 s_mask[e] = (unsigned char)strip_mask<kNW, 2 * PPT>(band_rows(r0, r1, thr, wx0, wx1), ty0);
                 if (Accept::kBase2) q_scale(r0, r1);   // as the forward stages it
                 s_r0[e] = r0;
@@ -209,8 +207,8 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_bwd(const StepParams* __re
             const unsigned jj = bs + (unsigned)k;
             const float4 a = s_r0[k];
             const float4 c = s_r1[k];
-            const float cb = s_b[k];
-            const float thr = s_thr[k];
+            const float2 bt = s_bt[k];
+            const float cb = bt.x, thr = bt.y;
             const float dx = a.x - fx;
             const float3 kq = Accept::kBase2 ? q_coeffs(a, c, dx) : make_float3(0.f, 0.f, 0.f);
             bool contrib = false;

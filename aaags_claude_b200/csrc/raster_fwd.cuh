@@ -45,8 +45,7 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_fwd(const StepParams* __re
                                                             unsigned n_tiles = 0) {
     __shared__ float4 s_r0[kFwdBatch];
     __shared__ float4 s_r1[kFwdBatch];
-    __shared__ float s_b[kFwdBatch];
-    __shared__ float s_thr[kFwdBatch];
+    __shared__ float2 s_bt[kFwdBatch];   // (blue, skip threshold): one 8-byte load per Gaussian
     constexpr int kFwdThreads = 256 / PPT;
     constexpr int kNW = kFwdThreads / 32;
     __shared__ unsigned char s_mask[kFwdBatch];       // warps whose strip the Gaussian can reach
@@ -113,8 +112,8 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_fwd(const StepParams* __re
                 float4 r0 = s.rec0[g];
                 float4 r1 = s.rec1[g];
                 const float thr = skip_threshold(r1.y);
-                s_b[e] = s.col_b[g];
-                s_thr[e] = Blend::kBase2 ? __fmul_rn(thr, kLog2e) : thr;   // in the units of Blend's exponent
+                // the threshold in the units of Blend's exponent
+                s_bt[e] = make_float2(s.col_b[g], Blend::kBase2 ? __fmul_rn(thr, kLog2e) : thr);
                 s_mask[e] = (unsigned char)strip_mask<kNW, 2 * PPT>(band_rows(r0, r1, thr, wx0, wx1), ty0);
                 if (Blend::kBase2) q_scale(r0, r1);
                 s_r0[e] = r0;
@@ -132,7 +131,8 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_fwd(const StepParams* __re
             const int k = s_list[warp][i];
             const float4 a = s_r0[k];
             const float4 c = s_r1[k];
-            const float thr = s_thr[k];
+            const float2 bt = s_bt[k];
+            const float thr = bt.y;
             const float dx = a.x - fx;
             const float3 kq = Blend::kBase2 ? q_coeffs(a, c, dx) : make_float3(0.f, 0.f, 0.f);
 #pragma unroll
@@ -154,11 +154,11 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_fwd(const StepParams* __re
                     const float aT = alpha * T[p];
                     C[p][0] += c.z * aT;
                     C[p][1] += c.w * aT;
-                    C[p][2] += s_b[k] * aT;
+                    C[p][2] += bt.x * aT;
                 } else {   // the reference's (c * alpha) * T
                     C[p][0] += c.z * alpha * T[p];
                     C[p][1] += c.w * alpha * T[p];
-                    C[p][2] += s_b[k] * alpha * T[p];
+                    C[p][2] += bt.x * alpha * T[p];
                 }
                 T[p] = test_T;
                 cnt[p]++;
