@@ -263,12 +263,12 @@ __device__ __forceinline__ void opt8(const StepParams& sp, uint4& p, uint4& m, u
 
 // ---- adjoint (staged, coalesced) ----
 
-constexpr int kCB = 128;          // Gaussians (= threads) per CTA of the adjoint
+constexpr int kCB = 64;           // Gaussians (= threads) per CTA of the adjoint
 constexpr int kShPitch = 49;      // padded row of the per-Gaussian SH gradients in shared memory
 
 // One view: the SH gradient of coefficient k is basis[k / 3] * geff[k % 3], so the
 // CTA keeps the 16 + 3 factors per Gaussian (SoA, conflict-free) instead of the
-// 48 products, and fits 5 CTAs per SM.  Several views sum the products: g_sh.
+// 48 products (18 KB per CTA of 64, 10 CTAs per SM).  Several views sum the products: g_sh.
 template <typename S, bool MULTI>
 struct __align__(16) ChosenBwdShared {
     uint4 sh[kCB * 6];            // 16-bit SH, up to 48 per Gaussian (6 x 16 bytes)
@@ -287,14 +287,14 @@ struct __align__(16) ChosenBwdShared {
     }
 };
 
-// One CTA per 128 consecutive Gaussians: bulk copies of their parameters and
+// One CTA per 64 consecutive Gaussians: bulk copies of their parameters and
 // screen gradients into shared memory (the accumulators are zeroed for the
 // next step), the per-Gaussian adjoint of PreprocessorBackwardCPU::backward
 // (preprocessor_backward_cpu.cpp:205-645) from there into shared-memory
 // gradients, then Adam over the CTA's contiguous parameter slice with 16-byte
 // accesses and stochastic rounding (and, when asked, the FP32 gradients).
 template <typename S, bool MULTI>
-__global__ void __launch_bounds__(kCB, MULTI ? 4 : 5) k_chosen_backward(const StepParams* __restrict__ spp, int N, int mc3,
+__global__ void __launch_bounds__(kCB, MULTI ? 8 : 10) k_chosen_backward(const StepParams* __restrict__ spp, int N, int mc3,
                                                          ChosenPtrs c, RGradPtrs rg, GradPtrs gout, Control* ctrl,
                                                          int n_views) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -471,7 +471,7 @@ __global__ void __launch_bounds__(kCB, MULTI ? 4 : 5) k_chosen_backward(const St
     __nv_bfloat16* vsh = static_cast<__nv_bfloat16*>(c.v_sh);
     const float lr_sh[8] = {sp.lr_sh, sp.lr_sh, sp.lr_sh, sp.lr_sh, sp.lr_sh, sp.lr_sh, sp.lr_sh, sp.lr_sh};
     if (ng == kCB) {
-        // SH: 16 * mc3 chunks of 8 coefficients (16-byte aligned: the slice starts at 256 * mc3 * blockIdx
+        // SH: 16 * mc3 chunks of 8 coefficients (16-byte aligned: the slice starts at 128 * mc3 * blockIdx
         // bytes); the parameters are already in shared memory
         const int nq = (kCB * mc3) / 8;
         uint4* m4 = reinterpret_cast<uint4*>(msh + sh0);
