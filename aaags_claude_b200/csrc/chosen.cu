@@ -471,7 +471,7 @@ __global__ void __launch_bounds__(kCB, MULTI ? 8 : 10) k_chosen_backward(const S
     __nv_bfloat16* vsh = static_cast<__nv_bfloat16*>(c.v_sh);
     const float lr_sh[8] = {sp.lr_sh, sp.lr_sh, sp.lr_sh, sp.lr_sh, sp.lr_sh, sp.lr_sh, sp.lr_sh, sp.lr_sh};
     if (ng == kCB) {
-        // SH: 16 * mc3 chunks of 8 coefficients (16-byte aligned: the slice starts at 128 * mc3 * blockIdx
+        // SH: 8 * mc3 chunks of 8 coefficients (16-byte aligned: the slice starts at 128 * mc3 * blockIdx
         // bytes); the parameters are already in shared memory
         const int nq = (kCB * mc3) / 8;
         uint4* m4 = reinterpret_cast<uint4*>(msh + sh0);
