@@ -71,14 +71,15 @@ struct FastAccept {
 //  - accum_rec (rasterizer_backward_cpu.cpp:101-108) enters d_alpha only as
 //    sum_ch accum_rec[ch] * dC[ch], so each pixel carries that one scalar D:
 //    d_alpha = T_i (cd - D) with cd = sum_ch c[ch] dC[ch], then D += alpha (cd - D);
-//  - d_power = o * t with t = d_alpha * exp(power), and the geometric factors
+//  - d_power = o * d_alpha * exp(power) = u with u = d_alpha * alpha (alpha < 0.99,
+//    so alpha = o exp(power)), and the geometric factors
 //    of d_means2D / d_conics (:126-132) are polynomials in (dx, dy) with the
 //    Gaussian's conic as coefficients, where dx is fixed per thread.  A thread
-//    sums t, t dy, t dy^2 over its pixels; the warp reduces t, t dx, t dy,
-//    t dx^2, t dx dy, t dy^2 (plus d_rgb) and the conic / opacity factors are
+//    sums u, u dy, u dy^2 over its pixels; the warp reduces u, u dx, u dy,
+//    u dx^2, u dx dy, u dy^2 (plus d_rgb) and the conic / opacity factors are
 //    applied once per Gaussian when the tile's sums are flushed:
-//      d_mean.x = -o (a S_x + b S_y)     d_mean.y = -o (c S_y + b S_x)
-//      d_conic  = -o (S_xx / 2, S_xy, S_yy / 2)     d_opacity = S_1.
+//      d_mean.x = -(a S_x + b S_y)     d_mean.y = -(c S_y + b S_x)
+//      d_conic  = -(S_xx / 2, S_xy, S_yy / 2)     d_opacity = S_1 / o.
 constexpr int kBwdBatch = 256;
 
 //
@@ -234,7 +235,8 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_bwd(const StepParams* __re
                         D[p] += alpha * diff;
                         T[p] = Ti;
                         if (alpha < 0.99f) {
-                            const float t = Ti * diff * ep;   // d_alpha * exp(power)
+                            // d_alpha * alpha = o * (d_alpha * exp(power)): o is divided out at the flush
+                            const float t = diff * aT;
                             t0 += t;
                             const float tdy = t * dy;
                             t1 += tdy;
@@ -264,14 +266,14 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_bwd(const StepParams* __re
                 const float4 r0 = s_r0[e];
                 const float o = s_r1[e].y, cc = s_r1[e].x;
                 const float Sx = s_acc[4][e], Sy = s_acc[5][e];
-                // d_mean = -o (a S_x + b S_y, c S_y + b S_x); from the pre-scaled conic
-                // (-a L / 2, -b L, -c L / 2), L = log2(e): (o / L) (2 A S_x + B S_y, 2 H S_y + B S_x)
-                const float dmx = Accept::kBase2 ? (o * (1.0f / kLog2e)) * (2.0f * r0.z * Sx + r0.w * Sy)
-                                                 : -o * (r0.z * Sx + r0.w * Sy);
-                const float dmy = Accept::kBase2 ? (o * (1.0f / kLog2e)) * (2.0f * cc * Sy + r0.w * Sx)
-                                                 : -o * (cc * Sy + r0.w * Sx);
-                const float val[9] = {s_acc[0][e], s_acc[1][e], s_acc[2][e], s_acc[3][e], dmx, dmy,
-                                      -0.5f * o * s_acc[6][e], -o * s_acc[7][e], -0.5f * o * s_acc[8][e]};
+                // d_mean = -(a S_x + b S_y, c S_y + b S_x); from the pre-scaled conic
+                // (-a L / 2, -b L, -c L / 2), L = log2(e): (1 / L) (2 A S_x + B S_y, 2 H S_y + B S_x)
+                const float dmx = Accept::kBase2 ? (1.0f / kLog2e) * (2.0f * r0.z * Sx + r0.w * Sy)
+                                                 : -(r0.z * Sx + r0.w * Sy);
+                const float dmy = Accept::kBase2 ? (1.0f / kLog2e) * (2.0f * cc * Sy + r0.w * Sx)
+                                                 : -(cc * Sy + r0.w * Sx);
+                const float val[9] = {s_acc[0][e], s_acc[1][e], s_acc[2][e], __fdividef(s_acc[3][e], o), dmx, dmy,
+                                      -0.5f * s_acc[6][e], -s_acc[7][e], -0.5f * s_acc[8][e]};
 #pragma unroll
                 for (int v = 0; v < 9; v++)
                     if (val[v] != 0.0f) atomicAdd(dst[v], val[v]);
