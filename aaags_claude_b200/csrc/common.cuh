@@ -189,11 +189,6 @@ __device__ __forceinline__ unsigned long long warp_lookback_exclusive(unsigned l
     return excl;
 }
 
-__device__ __forceinline__ unsigned long long lookback_exclusive(unsigned long long* desc, int blk,
-                                                                 unsigned long long aggregate,
-                                                                 unsigned* status, unsigned spin_limit) {
-    return lookback_exclusive_strided(desc, blk, 1, 0, aggregate, status, spin_limit);
-}
 
 // ---- TMA bulk copies (cp.async.bulk) completing on an mbarrier ----
 __device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }

@@ -31,6 +31,10 @@ __device__ __forceinline__ float power_rn(float4 r0, float4 r1, float dx, float 
 // is the one the exact alpha test would take.
 __device__ __forceinline__ float skip_threshold(float o) { return logf(kAlphaMin / o) - 1e-3f; }
 
+// Square root from the hardware reciprocal square root (rsqrtf, within 2 ulp),
+// for the conservative bounds below; 0 for x <= 0.
+__device__ __forceinline__ float sqrt_bound(float x) { return x > 0.0f ? x * rsqrtf(x) : 0.0f; }
+
 // Rows of a tile's column band where a Gaussian can reach power >= thr.
 // The ellipse E = {d : a dx^2 + 2 b dx dy + c dy^2 <= t2}, t2 = -2 thr, with
 // d = mean - pixel and conic (a, b, c) = (r0.z, r0.w, r1.x), is cut by the band
@@ -45,10 +49,6 @@ __device__ __forceinline__ float skip_threshold(float o) { return logf(kAlphaMin
 // for det >= 1e-3 a c; more elongated conics are not culled.  A pixel outside
 // the range has power < thr, so alpha < 1/255 (skip_threshold's margin), and
 // the blend would skip it: culling it changes no result.
-// Square root from the hardware reciprocal square root (relative error ~1e-7),
-// for the conservative bounds below; 0 for x <= 0.
-__device__ __forceinline__ float sqrt_bound(float x) { return x > 0.0f ? x * rsqrtf(x) : 0.0f; }
-
 __device__ __forceinline__ float2 band_rows(float4 r0, float4 r1, float thr, float x0, float x1) {
     const float t2 = -2.0f * thr;
     const float a = r0.z, b = r0.w, c = r1.x;
@@ -120,10 +120,6 @@ __device__ __forceinline__ float ex2_approx(float q) {
     asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(q));
     return r;
 }
-
-// skip_threshold in base-2 units: q below it gives alpha < 1/255 for certain
-// (the natural bound's 1e-3 margin becomes 1.44e-3, far above rounding).
-__device__ __forceinline__ float skip_threshold2(float o) { return __fmul_rn(skip_threshold(o), kLog2e); }
 
 // The staged record of the reduced form carries the conic pre-scaled for q:
 // (x, y, -0.5 log2(e) a, -log2(e) b), (-0.5 log2(e) c, o, r, g).
