@@ -343,8 +343,11 @@ def _summary(a, r, world, X, N, T, depth_first, peak):
     achieved = nbytes[dom] / (per_launch_ms[dom] * 1e-3) / 1e9
     traffic = None
     tt = _traffic_table()
-    if tt and dom in tt.get("kernels", {}):
-        k = tt["kernels"][dom]
+    # both 16-bit forms run the same rasterisers
+    form_key = "bf16" if r["form"] == "fp16" else r["form"]
+    kernels = (tt or {}).get("forms", {}).get(form_key, (tt or {}).get("kernels", {}))
+    if dom in kernels:
+        k = kernels[dom]
         traffic = k["bytes_per_launch"] * (P / k["pairs"] if k.get("scale") == "pairs" else 1.0)
     step_bytes = sum(nbytes[s] * (pair_passes if s == "sort_passes" else 1) for s in nbytes)
     sp_ms = stage_ms[STAGES.index("sort_passes")]
