@@ -26,14 +26,14 @@ namespace gs3d {
 namespace {
 
 // Blend decision of the reduced-storage forward on the base-2 exponent
-// q = power * log2(e) (q_coeffs / q_at): alpha = o * 2^q, no exact recheck.
+// q = power * log2(e) (q_coeffs / q_at) once q has passed accept_threshold2:
+// alpha = o * 2^q, no exact recheck.
 struct FastBlend {
     static constexpr bool kBase2 = true;
     __device__ __forceinline__ static int decide(float q, float o, float T, float& alpha, float& e,
                                                  float& test_T) {
         e = ex2_approx(q);
-        alpha = fmin_ref(0.99f, o * e);
-        if (alpha < kAlphaMin) return 0;
+        alpha = fmin_ref(0.99f, o * e);   // >= 1/255: q passed accept_threshold2
         test_T = fmaf(-alpha, T, T);   // T (1 - alpha)
         if (test_T < kTMin) return 2;
         return 1;

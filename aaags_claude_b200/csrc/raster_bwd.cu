@@ -51,7 +51,7 @@ struct FastAccept {
     __device__ __forceinline__ static bool accept(float q, float o, float& alpha, float& e) {
         e = ex2_approx(q);
         alpha = fmin_ref(0.99f, o * e);
-        return !(alpha < kAlphaMin);
+        return true;   // q passed accept_threshold2, as in the forward
     }
 };
 
@@ -190,7 +190,7 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_bwd(const StepParams* __re
                 float4 r1 = s.rec1[gi];
                 const float thr = skip_threshold(r1.y);
                 s_idx[e] = gi;
-                s_bt[e] = make_float2(s.col_b[gi], Accept::kBase2 ? __fmul_rn(thr, kLog2e) : thr);   // forward's
+                s_bt[e] = make_float2(s.col_b[gi], Accept::kBase2 ? accept_threshold2(r1.y) : thr);   // forward's
                 s_mask[e] = (unsigned char)strip_mask<kNW, 2 * PPT>(band_rows(r0, r1, thr, wx0, wx1), ty0);
                 if (Accept::kBase2) q_scale(r0, r1);   // as the forward stages it
                 s_r0[e] = r0;

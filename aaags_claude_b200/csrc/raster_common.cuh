@@ -121,6 +121,11 @@ __device__ __forceinline__ float ex2_approx(float q) {
     return r;
 }
 
+// The reduced form's accept test: o 2^q >= 1/255 <=> q >= log2(1 / (255 o)),
+// decided on q alone (forward and backward stage the same value), so no
+// separate alpha comparison follows.  Culling keeps skip_threshold's margin.
+__device__ __forceinline__ float accept_threshold2(float o) { return -log2f(255.0f * o); }
+
 // The staged record of the reduced form carries the conic pre-scaled for q:
 // (x, y, -0.5 log2(e) a, -log2(e) b), (-0.5 log2(e) c, o, r, g).
 __device__ __forceinline__ void q_scale(float4& r0, float4& r1) {

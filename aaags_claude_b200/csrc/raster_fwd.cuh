@@ -113,7 +113,7 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_fwd(const StepParams* __re
                 float4 r1 = s.rec1[g];
                 const float thr = skip_threshold(r1.y);
                 // the threshold in the units of Blend's exponent
-                s_bt[e] = make_float2(s.col_b[g], Blend::kBase2 ? __fmul_rn(thr, kLog2e) : thr);
+                s_bt[e] = make_float2(s.col_b[g], Blend::kBase2 ? accept_threshold2(r1.y) : thr);
                 s_mask[e] = (unsigned char)strip_mask<kNW, 2 * PPT>(band_rows(r0, r1, thr, wx0, wx1), ty0);
                 if (Blend::kBase2) q_scale(r0, r1);
                 s_r0[e] = r0;
