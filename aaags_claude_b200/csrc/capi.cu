@@ -623,6 +623,7 @@ int ensure_depth_sort(gs3dc_ctx* c) {
     }
     c->ddesc_stride = ((n + kSortTile - 1) / kSortTile) * 256ull;
     CK(c->ddesc.ensure(kDepthDigits * c->ddesc_stride));
+    CK(c->c_rects.ensure(n));   // tile rectangles for the pair emission (both forms)
     return GS3DC_OK;
 }
 
@@ -651,7 +652,8 @@ int seq_front_depth_first(gs3dc_ctx* c) {
                                     c->ctrl));
     else
         CK(launch_preprocess_plain(c->stream, c->sp_dev, c->N, c->model_raw, false, model_ptrs(c),
-                                   screen_ptrs(c, false), pr, c->ctrl, DepthKeys{c->dkeys[0].p, c->dvals[0].p}));
+                                   screen_ptrs(c, false), pr, c->ctrl,
+                                   DepthKeys{c->dkeys[0].p, c->dvals[0].p, nullptr, c->c_rects.p}));
     if ((rc = mark(c, GS3DC_STAGE_SORT_HIST))) return rc;
     // the reduced form orders by the depth's upper 24 bits (relative steps of 2^-15; ties keep index order)
     const int depth_first_digit = chosen ? kChosenDepthSkip : 0;
@@ -660,7 +662,7 @@ int seq_front_depth_first(gs3dc_ctx* c) {
                            c->dvals[0].p, c->dkeys[1].p, c->dvals[1].p, c->ddesc.p, c->ddesc_stride, c->ctrl, &dw,
                            nullptr, &c->ctrl->gauss_keys, depth_first_digit));
     CK(launch_emit_ranked(c->stream, c->sp_dev, c->N, c->dvals[dw].p, screen_ptrs(c, false), pr, c->ctrl,
-                          chosen ? c->c_rects.p : nullptr));
+                          c->c_rects.p));
     if ((rc = mark(c, GS3DC_STAGE_SORT_PASSES))) return rc;
     int which = 0;
     CK(launch_radix_sort32(c->stream, c->sp_dev, tile_digits, kDepthDigits, true, c->cap, tk[0], c->vals[0].p, tk[1],

@@ -122,6 +122,7 @@ struct DepthKeys {
     unsigned* keys;             // [N] depth bits, ~0u for Gaussians without pairs
     unsigned* vals;             // [N] Gaussian index
     unsigned long long* keys64 = nullptr;   // several views: (view << 32 | depth bits) instead of keys
+    uint2* rects = nullptr;   // plain preprocess: tile rectangles (xmin | ymin << 16, xmax | ymax << 16), 0 if none
 };
 
 // Reduced-storage ("chosen") form: positions FP32, the other attributes and the

@@ -233,6 +233,10 @@ __global__ void __launch_bounds__(kBlock) k_preprocess(const StepParams* __restr
         // depth-sort input: Gaussians without pairs sort last (no finite depth has these bits)
         dk.keys[i] = cnt > 0 ? dbits : 0xFFFFFFFFu;
         dk.vals[i] = (unsigned)i;
+        if (dk.rects)   // the emission reads the rectangle (and its area, the pair count) in one load
+            dk.rects[i] = cnt > 0 ? make_uint2((unsigned)rx | ((unsigned)ry << 16),
+                                               (unsigned)(rx + rw) | ((unsigned)(ry + cnt / rw) << 16))
+                                  : make_uint2(0u, 0u);
         if (i == 0) ctrl->gauss_keys = (unsigned long long)N;
     }
 }
@@ -265,15 +269,21 @@ __global__ void __launch_bounds__(kBlock) k_emit_ranked(const StepParams* __rest
             // the key is the view's local tile id (the value tells the views apart)
             gx = spp[g / (unsigned)n_per_view].grid_x;
         }
-        cnt = s.tiles[g];
-        if (cnt > 0) {
-            if (rects) {
-                // tile rectangle stored by the preprocess: (xmin | ymin << 16, xmax | ymax << 16)
-                const uint2 rc = rects[g];
-                rx = (int)(rc.x & 0xffffu);
-                ry = (int)(rc.x >> 16);
-                rw = (int)(rc.y & 0xffffu) - rx;
-            } else {
+        if (rects) {
+            // tile rectangle stored by the preprocess: (xmin | ymin << 16, xmax | ymax << 16); its
+            // area is the Gaussian's pair count (0 without pairs)
+            const uint2 rc = rects[g];
+            rx = (int)(rc.x & 0xffffu);
+            ry = (int)(rc.x >> 16);
+            rw = (int)(rc.y & 0xffffu) - rx;
+            cnt = rw * ((int)(rc.y >> 16) - ry);
+            if (cnt <= 0) {
+                cnt = 0;
+                rw = 1;
+            }
+        } else {
+            cnt = s.tiles[g];
+            if (cnt > 0) {
                 const float4 r0 = s.rec0[g];
                 int rmn[2], rmx[2];
                 tile_rect(r0.x, r0.y, s.radius[g], sp.grid_x, sp.grid_y, sp.cfg.tile_w, sp.cfg.tile_h, rmn, rmx);
@@ -281,8 +291,9 @@ __global__ void __launch_bounds__(kBlock) k_emit_ranked(const StepParams* __rest
                 ry = rmn[1];
                 rw = rmx[0] - rmn[0];
             }
-            dbits = __float_as_uint(s.depth[g]);
         }
+        // the depth goes into 64-bit keys only; tile-only keys do not carry it
+        if (cnt > 0 && !pr.tiles32) dbits = __float_as_uint(s.depth[g]);
     }
     scan_and_emit(sm, blk, g, cnt, cnt, rx, ry, rw, dbits, sp.grid_x, pr, ctrl, sp.spin_limit, sp.persist,
                   &s_thist[0][0], nd, tbase, gx);
