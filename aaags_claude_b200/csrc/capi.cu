@@ -634,13 +634,20 @@ int ensure_depth_sort(gs3dc_ctx* c) {
 int seq_front_depth_first(gs3dc_ctx* c) {
     int rc = mark(c, GS3DC_STAGE_MEMSETS);
     if (rc) return rc;
-    CK(cudaMemsetAsync(c->ctrl_region.p, 0, ctrl_bytes_for(c->N), c->stream));
-    CK(cudaMemsetAsync(c->ranges.p, 0, 2 * (size_t)c->num_tiles * sizeof(unsigned), c->stream));
-    CK(cudaMemsetAsync(c->ddesc.p, 0, kDepthDigits * c->ddesc_stride * sizeof(unsigned long long), c->stream));
     const int tile_digits = c->sort_passes - kDepthDigits;
-    if (tile_digits > 0)
-        CK(cudaMemsetAsync(c->sort_desc.p, 0, (size_t)tile_digits * c->sort_desc_stride * sizeof(unsigned long long),
-                           c->stream));
+    {
+        // control block, tile ranges and both look-back descriptor sets, in one launch
+        ClearRegions z{};
+        z.p[0] = reinterpret_cast<unsigned long long*>(c->ctrl_region.p);
+        z.words[0] = ctrl_bytes_for(c->N) / 8;
+        z.p[1] = reinterpret_cast<unsigned long long*>(c->ranges.p);
+        z.words[1] = (size_t)c->num_tiles;   // 2 u32 per tile
+        z.p[2] = c->ddesc.p;
+        z.words[2] = kDepthDigits * c->ddesc_stride;
+        z.p[3] = tile_digits > 0 ? c->sort_desc.p : nullptr;
+        z.words[3] = tile_digits > 0 ? (size_t)tile_digits * c->sort_desc_stride : 0;
+        CK(launch_clear_regions(c->stream, z));
+    }
     if ((rc = mark(c, GS3DC_STAGE_PREPROCESS))) return rc;
     // tile-only keys live in the (otherwise unused) 64-bit key buffers
     unsigned* tk[2] = {reinterpret_cast<unsigned*>(c->keys[0].p), reinterpret_cast<unsigned*>(c->keys[1].p)};
@@ -671,8 +678,9 @@ int seq_front_depth_first(gs3dc_ctx* c) {
     if ((rc = mark(c, GS3DC_STAGE_RANGES))) return rc;
     CK(launch_tile_ranges32(c->stream, c->cap, tk[which], c->ranges.p, c->ctrl));
     CK(launch_tile_order(c->stream, c->ranges.p, c->num_tiles, c->tile_order.p));
+    // clearing, preprocess, depth histogram + passes, emission, tile passes, ranges + order
     c->kernels_last +=
-        c->N > 0 ? 1 + (1 + kDepthDigits - depth_first_digit) + 1 + (tile_digits > 0 ? tile_digits : 0) + 2 : 2;
+        1 + (c->N > 0 ? 1 + (1 + kDepthDigits - depth_first_digit) + 1 + (tile_digits > 0 ? tile_digits : 0) + 2 : 2);
     return GS3DC_OK;
 }
 

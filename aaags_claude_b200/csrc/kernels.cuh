@@ -267,6 +267,14 @@ cudaError_t launch_tile_ranges_views(cudaStream_t st, unsigned long long capacit
 cudaError_t launch_tile_order(cudaStream_t st, const unsigned* ranges, int num_tiles, unsigned* order);
 
 // Bounded-wait self-test: desc2 = two zeroed descriptors.
+// Zeroes up to four device regions (8-byte aligned, sizes in 8-byte words; a
+// null pointer or zero size skips a region) in one launch: the per-step
+// clearing of control block, tile ranges and look-back descriptors.
+struct ClearRegions {
+    unsigned long long* p[4];
+    unsigned long long words[4];
+};
+cudaError_t launch_clear_regions(cudaStream_t st, const ClearRegions& r);
 cudaError_t launch_wait_selftest(cudaStream_t st, unsigned long long* desc2, unsigned* status, unsigned spin_limit);
 
 constexpr int kSortThreads = 256;

@@ -304,6 +304,30 @@ __global__ void k_wait_selftest(unsigned long long* desc, unsigned* status, unsi
 
 }  // namespace
 
+namespace {
+__global__ void __launch_bounds__(256) k_clear_regions(ClearRegions r) {
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    const unsigned long long t = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        unsigned long long* p = r.p[k];
+        if (!p) continue;
+        for (unsigned long long i = t; i < r.words[k]; i += stride) p[i] = 0ull;
+    }
+}
+}  // namespace
+
+cudaError_t launch_clear_regions(cudaStream_t st, const ClearRegions& r) {
+    unsigned long long most = 0;
+    for (int k = 0; k < 4; k++)
+        if (r.p[k] && r.words[k] > most) most = r.words[k];
+    if (most == 0) return cudaSuccess;
+    const unsigned long long want = (most + 255) / 256;
+    const unsigned blocks = (unsigned)(want < 8ull * 148 ? want : 8ull * 148);
+    k_clear_regions<<<blocks, 256, 0, st>>>(r);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_wait_selftest(cudaStream_t st, unsigned long long* desc2, unsigned* status, unsigned spin_limit) {
     k_wait_selftest<<<1, 32, 0, st>>>(desc2, status, spin_limit);
     return cudaGetLastError();
