@@ -193,26 +193,50 @@ __global__ void __launch_bounds__(kSortThreads, sizeof(K) == 4 ? 4 : 2) k_oneswe
 
 __device__ __forceinline__ unsigned tile_of(unsigned long long key) { return (unsigned)(key >> 32); }
 
+// Ranges of (view, tile) runs: a run starts / ends where the global id changes.
+// Four pairs per thread from 16-byte loads of the keys and values; each id is
+// compared with its successor's (as k_ranges32).
+__global__ void k_ranges_views4(const unsigned* __restrict__ keys, const unsigned* __restrict__ vals,
+                                const StepParams* __restrict__ views, unsigned n_per_view,
+                                unsigned long long capacity, unsigned* __restrict__ ranges, Control* ctrl) {
+    const unsigned long long P = min(ctrl->total_pairs, capacity);
+    const unsigned long long i0 = 4ull * ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x);
+    if (i0 >= P) return;
+    unsigned k[5], v[5];
+    if (i0 + 4 <= capacity) {
+        const uint4 kk = *reinterpret_cast<const uint4*>(keys + i0);
+        const uint4 vv = *reinterpret_cast<const uint4*>(vals + i0);
+        k[0] = kk.x, k[1] = kk.y, k[2] = kk.z, k[3] = kk.w;
+        v[0] = vv.x, v[1] = vv.y, v[2] = vv.z, v[3] = vv.w;
+    } else {
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            k[j] = i0 + j < P ? keys[i0 + j] : 0u;
+            v[j] = i0 + j < P ? vals[i0 + j] : 0u;
+        }
+    }
+    k[4] = i0 + 4 < P ? keys[i0 + 4] : 0u;
+    v[4] = i0 + 4 < P ? vals[i0 + 4] : 0u;
+    unsigned t[5];
+#pragma unroll
+    for (int j = 0; j < 5; j++) t[j] = views[v[j] / n_per_view].tile_base + k[j];
+    if (i0 == 0) ranges[2 * t[0]] = 0u;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const unsigned long long i = i0 + (unsigned long long)j;
+        if (i >= P) break;
+        const bool last = i + 1 == P;
+        if (last || t[j + 1] != t[j]) {
+            ranges[2 * t[j] + 1] = (unsigned)(i + 1);
+            if (!last) ranges[2 * t[j + 1]] = (unsigned)(i + 1);
+        }
+    }
+}
+
+
 // One thread per key (the grid covers the capacity): a tile's range starts
 // where its key differs from the previous one and ends where it differs
 // from the next.
-__device__ __forceinline__ unsigned global_tile(const unsigned* keys, const unsigned* vals, const StepParams* views,
-                                                unsigned n_per_view, unsigned long long i) {
-    return views[vals[i] / n_per_view].tile_base + keys[i];
-}
-
-// Ranges of (view, tile) runs: a run starts / ends where the global id changes.
-__global__ void k_ranges_views(const unsigned* __restrict__ keys, const unsigned* __restrict__ vals,
-                               const StepParams* __restrict__ views, unsigned n_per_view,
-                               unsigned long long capacity, unsigned* __restrict__ ranges, Control* ctrl) {
-    const unsigned long long P = min(ctrl->total_pairs, capacity);
-    const unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P) return;
-    const unsigned t = global_tile(keys, vals, views, n_per_view, i);
-    if (i == 0 || global_tile(keys, vals, views, n_per_view, i - 1) != t) ranges[2 * t] = (unsigned)i;
-    if (i == P - 1 || global_tile(keys, vals, views, n_per_view, i + 1) != t) ranges[2 * t + 1] = (unsigned)(i + 1);
-}
-
 template <typename K>
 __global__ void k_ranges(const K* __restrict__ keys, unsigned long long capacity, unsigned* __restrict__ ranges,
                          Control* ctrl) {
@@ -409,8 +433,8 @@ cudaError_t launch_tile_ranges_views(cudaStream_t st, unsigned long long capacit
                                      const unsigned* vals_sorted, const StepParams* views, int n_per_view,
                                      unsigned* ranges, Control* ctrl) {
     if (capacity == 0 || n_per_view <= 0) return cudaSuccess;
-    k_ranges_views<<<(unsigned)((capacity + 255) / 256), 256, 0, st>>>(tiles_sorted, vals_sorted, views,
-                                                                       (unsigned)n_per_view, capacity, ranges, ctrl);
+    k_ranges_views4<<<(unsigned)((capacity + 1023) / 1024), 256, 0, st>>>(tiles_sorted, vals_sorted, views,
+                                                                         (unsigned)n_per_view, capacity, ranges, ctrl);
     return cudaGetLastError();
 }
 
