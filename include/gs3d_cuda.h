@@ -266,7 +266,7 @@ int gs3dc_train_step_batch(gs3dc_ctx* ctx, int n_views, const gs3d_camera* cams,
 /* Device time per stage of the last train step run with GS3DC_OPT_STAGE_TIMING,
  * measured with CUDA events on the context's stream.  ms[k] for k < n_stages,
  * indexed by GS3DC_STAGE_*. */
-#define GS3DC_STAGE_MEMSETS        0  /* control block, sort scratch, tile ranges */
+#define GS3DC_STAGE_MEMSETS        0  /* clearing of the control block, sort scratch, tile ranges (one kernel in the train step) */
 #define GS3DC_STAGE_PREPROCESS     1  /* activation + projection + scan + pair emission */
 #define GS3DC_STAGE_SORT_HIST      2  /* digit histograms; depth-first: also the Gaussian depth sort + pair emission */
 #define GS3DC_STAGE_SORT_PASSES    3  /* all onesweep passes over the pairs together */
