@@ -14,7 +14,7 @@
 //                   pairs.  Replaces preprocess + prefix sum + binning.
 //   k_bin_arrays    the same scan + emission from host-provided screen arrays.
 //   k_raster_fwd    one CTA per 16x16 tile, one thread per pixel; pairs are
-//                   gathered in batches of 256 into shared memory; CTA-wide
+//                   gathered in batches of 128 into shared memory; CTA-wide
 //                   early exit once every pixel saturated.  Optional fused L1.
 //   (k_raster_bwd lives in raster_bwd.cu, compiled with FMA contraction.)
 //   k_preprocess_bwd  the full per-Gaussian adjoint chain, fused with Adam.

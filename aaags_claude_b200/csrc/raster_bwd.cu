@@ -80,7 +80,7 @@ struct FastAccept {
 //    applied once per Gaussian when the tile's sums are flushed:
 //      d_mean.x = -(a S_x + b S_y)     d_mean.y = -(c S_y + b S_x)
 //      d_conic  = -(S_xx / 2, S_xy, S_yy / 2)     d_opacity = S_1 / o.
-constexpr int kBwdBatch = 256;
+constexpr int kBwdBatch = 128;
 
 //
 // MULTI: one persistent launch over the tiles of several views (spp = the views'

@@ -18,7 +18,7 @@ namespace {
 // reduced-storage form (Blend::kBase2: q_coeffs / q_at, ex2).  One CTA of 128
 // threads per 16x16 tile, two pixels per thread: warp w owns the 16x4 strip
 // of rows 4w..4w+3, a thread the pixels (x, 4w + lane/16) and
-// (x, 4w + 2 + lane/16).  Batches of 256 records are gathered into shared
+// (x, 4w + 2 + lane/16).  Batches of 128 records are gathered into shared
 // memory with, per record, the warps whose strip the Gaussian can reach
 // (band_rows: the rows of the tile's columns inside its alpha >= 1/255
 // ellipse); each warp walks its own compacted list of the batch; the CTA
@@ -27,7 +27,7 @@ namespace {
 //
 // PPT (pixels per thread: 1, 2 or 4) sets the threads per tile (256 / PPT)
 // and each warp's strip (16 x 2*PPT rows); the results do not depend on it.
-constexpr int kFwdBatch = 256;
+constexpr int kFwdBatch = 128;
 
 //
 // MULTI: one persistent launch over the tiles of several views.  spp is then
