@@ -92,7 +92,7 @@ struct gs3dc_ctx {
     bool chosen_ready = false;   // the chosen buffers hold the current model
     DevBuf<float> c_pos, cm_pos, cv_pos;
     DevBuf<unsigned short> c_attr, c_sh, cm_attr, cv_attr, cm_sh, cv_sh;
-    DevBuf<uint2> c_rects;
+    DevBuf<uint2> c_rects;   // per-Gaussian tile rectangles read by the depth-first pair emission (both forms)
     // 3D-evaluation mode (RenderConfig::eval_3D): per-Gaussian records, tile rays, view
     DevBuf<float4> e3_rec, e3_tdir;
     DevBuf<float> e3_g2s, e3_ci, e3_mo, e3_view, filt3d;
