@@ -21,7 +21,7 @@ CSRC = os.path.join(PKG, "csrc")
 BUILD = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libgs3d_cuda.so")
 HOST = os.path.join(PKG, "host")
-DEMO = os.path.join(BUILD, "stages_demo")
+ADAPTERS_OBJ = os.path.join(BUILD, "gs3d_stages_cuda.o")
 INCLUDE = os.path.join(os.path.dirname(PKG), "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -70,12 +70,13 @@ def build(force: bool = False, verbose: bool = False) -> str:
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
-    # C++ stage adapters (host/) and the driver the adapter tests run
-    host_srcs = [os.path.join(HOST, "gs3d_stages_cuda.cpp"), os.path.join(HOST, "stages_demo.cpp")]
-    deps = host_srcs + glob.glob(os.path.join(HOST, "*.hpp")) + [LIB]
-    if force or not os.path.exists(DEMO) or os.path.getmtime(DEMO) < _newest(deps):
-        cmd = [os.environ.get("CXX", "g++"), "-O2", "-std=c++17", "-Wall", f"-I{INCLUDE}", f"-I{HOST}",
-               *host_srcs, "-o", DEMO, f"-L{PKG}", "-lgs3d_cuda", "-Wl,-rpath,$ORIGIN/.."]
+    # C++ stage adapters (host/): compiled here so that a broken adapter fails the build; callers
+    # compile gs3d_stages_cuda.cpp into their own program and link libgs3d_cuda.so
+    src = os.path.join(HOST, "gs3d_stages_cuda.cpp")
+    deps = [src] + glob.glob(os.path.join(HOST, "*.hpp")) + glob.glob(os.path.join(INCLUDE, "*.h"))
+    if force or not os.path.exists(ADAPTERS_OBJ) or os.path.getmtime(ADAPTERS_OBJ) < _newest(deps):
+        cmd = [os.environ.get("CXX", "g++"), "-O2", "-std=c++17", "-Wall", "-fPIC", f"-I{INCLUDE}", f"-I{HOST}",
+               "-c", src, "-o", ADAPTERS_OBJ]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

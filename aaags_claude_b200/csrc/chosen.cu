@@ -13,6 +13,8 @@
 // rectangle (the reference's 3-sigma square) to the box of the ellipse where
 // alpha can reach 1/255, q = d^T conic d <= 2 ln(255 o): tiles outside it hold
 // no pixel the blend would accept, so they get no pair.
+#include <algorithm>
+
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
@@ -533,7 +535,7 @@ inline int grid_for(long long n, int t) { return (int)((n + t - 1) / t); }
 
 cudaError_t launch_chosen_from_raw(cudaStream_t st, int N, int mc3, bool fp16, ModelPtrs raw, ChosenPtrs c) {
     if (N <= 0) return cudaSuccess;
-    const int grid = grid_for((long long)N * mc3, 256) < 8 * 148 ? grid_for((long long)N * mc3, 256) : 8 * 148;
+    const int grid = std::min(grid_for((long long)N * mc3, 256), 8 * sm_count());
     if (fp16) k_chosen_from_raw<__half><<<grid, 256, 0, st>>>(N, mc3, raw, c);
     else k_chosen_from_raw<__nv_bfloat16><<<grid, 256, 0, st>>>(N, mc3, raw, c);
     return cudaGetLastError();
@@ -541,7 +543,7 @@ cudaError_t launch_chosen_from_raw(cudaStream_t st, int N, int mc3, bool fp16, M
 
 cudaError_t launch_chosen_to_raw(cudaStream_t st, int N, int mc3, bool fp16, ChosenPtrs c, ModelPtrs raw) {
     if (N <= 0) return cudaSuccess;
-    const int grid = grid_for((long long)N * mc3, 256) < 8 * 148 ? grid_for((long long)N * mc3, 256) : 8 * 148;
+    const int grid = std::min(grid_for((long long)N * mc3, 256), 8 * sm_count());
     if (fp16) k_chosen_to_raw<__half><<<grid, 256, 0, st>>>(N, mc3, c, raw);
     else k_chosen_to_raw<__nv_bfloat16><<<grid, 256, 0, st>>>(N, mc3, c, raw);
     return cudaGetLastError();
@@ -568,7 +570,7 @@ cudaError_t fwd_multi(cudaStream_t st, const StepParams* views, int n_views, uns
             per_sm < 1)
             per_sm = 1;
     }
-    k_raster_fwd<true, FastBlend, true, PPT><<<per_sm * 148, 256 / PPT, 0, st>>>(views, ranges, order, vals, s, px,
+    k_raster_fwd<true, FastBlend, true, PPT><<<per_sm * sm_count(), 256 / PPT, 0, st>>>(views, ranges, order, vals, s, px,
                                                                                 ctrl, n_views, n_tiles);
     return cudaGetLastError();
 }

@@ -89,6 +89,21 @@ inline cudaError_t set_smem_once(std::atomic<unsigned long long>& done, K* kerne
     return e;
 }
 
+// Streaming multiprocessors of the current device, queried once per device
+// ordinal (grid sizes of the grid-stride and persistent launches; results never
+// depend on it).  1 if the query fails, which keeps every launch valid.
+inline int sm_count() {
+    static std::atomic<int> cache[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 1;
+    std::atomic<int>& slot = cache[dev & 63];
+    int n = slot.load(std::memory_order_relaxed);
+    if (n > 0) return n;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n < 1) return 1;
+    slot.store(n, std::memory_order_relaxed);
+    return n;
+}
+
 // ---- relaxed 64-bit accesses for decoupled look-back descriptors ----
 __device__ __forceinline__ unsigned long long ld_relaxed(const unsigned long long* p) {
     unsigned long long v;

@@ -836,7 +836,7 @@ cudaError_t launch_preprocess_bwd_plain(cudaStream_t st, const StepParams* sp, i
 cudaError_t launch_optimizer_plain(cudaStream_t st, const StepParams* sp, int N, int mc3, ModelPtrs raw,
                                    AdamPtrs adam, GradPtrs g, const Control* ctrl) {
     if (N <= 0) return cudaSuccess;
-    k_optimizer<<<8 * 148, 256, 0, st>>>(sp, (long long)N, mc3, raw, adam, g, ctrl);
+    k_optimizer<<<8 * sm_count(), 256, 0, st>>>(sp, (long long)N, mc3, raw, adam, g, ctrl);
     return cudaGetLastError();
 }
 

@@ -312,7 +312,7 @@ cudaError_t bwd_multi(cudaStream_t st, const StepParams* views, int n_views, uns
                       RGradPtrs g, Control* ctrl) {
     static int per_sm = 0;
     if (!per_sm) per_sm = resident_ctas(k_raster_bwd<true, FastAccept, true, PPT>, 256 / PPT);
-    k_raster_bwd<true, FastAccept, true, PPT><<<per_sm * 148, 256 / PPT, 0, st>>>(views, ranges, order, vals, s, px,
+    k_raster_bwd<true, FastAccept, true, PPT><<<per_sm * sm_count(), 256 / PPT, 0, st>>>(views, ranges, order, vals, s, px,
                                                                                  g, ctrl, n_views, n_tiles);
     return cudaGetLastError();
 }

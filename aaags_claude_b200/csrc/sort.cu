@@ -347,7 +347,8 @@ cudaError_t launch_clear_regions(cudaStream_t st, const ClearRegions& r) {
         if (r.p[k] && r.words[k] > most) most = r.words[k];
     if (most == 0) return cudaSuccess;
     const unsigned long long want = (most + 255) / 256;
-    const unsigned blocks = (unsigned)(want < 8ull * 148 ? want : 8ull * 148);
+    const unsigned long long cap = 8ull * (unsigned long long)sm_count();
+    const unsigned blocks = (unsigned)(want < cap ? want : cap);
     k_clear_regions<<<blocks, 256, 0, st>>>(r);
     return cudaGetLastError();
 }
@@ -374,7 +375,7 @@ cudaError_t radix_sort_impl(cudaStream_t st, const StepParams* sp, int first, in
     cudaError_t e = set_smem_once(attr_done, k_onesweep<K>, smem);
     if (e != cudaSuccess) return e;
     if (!hist_done) {
-        k_radix_hist<K><<<2 * 148, kHistThreads, 0, st>>>(keys0, capacity, first, passes, slot_base, count, ctrl);
+        k_radix_hist<K><<<2 * sm_count(), kHistThreads, 0, st>>>(keys0, capacity, first, passes, slot_base, count, ctrl);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     if (after_hist && (e = cudaEventRecord(after_hist, st)) != cudaSuccess) return e;

@@ -17,16 +17,17 @@
 //     contents; each call clears the parts that must start at zero.  Calls
 //     that overlap on the GPU (on different streams or host threads) race on
 //     it and give wrong results;
-//   * the first call on each device looks up the scratch's device address
-//     (cudaGetSymbolAddress, with that device current) and sets the sort
-//     kernel's shared-memory attribute; make that first call before any stream
-//     capture.
+//   * every call looks up the scratch's device address on the current device
+//     (cudaGetSymbolAddress), so a device reset that reloads the module at a
+//     new address leaves no stale pointer behind;
+//   * a call is synchronous (it reads the status back and waits for the
+//     stream), so it cannot be captured into a CUDA graph: on a capturing
+//     stream it returns GS3DC_ERR_INVALID_ARG before doing anything.
 #include <cuda_runtime.h>
 
 #include <cstdarg>
 #include <cstdint>
 #include <cstdio>
-#include <mutex>
 
 #include "common.cuh"
 #include "gs3d_cuda.h"
@@ -61,10 +62,6 @@ static __device__ __align__(256) unsigned char g_sort_scratch[gs3d::kScratchByte
 namespace gs3d {
 namespace {
 
-constexpr int kMaxDevices = 64;
-std::mutex g_setup_mutex;
-unsigned char* g_scratch_ptr[kMaxDevices] = {};
-
 // Flags a key whose tile field is >= num_tiles (k_ranges would index past the
 // caller's tile_ranges with it).
 __global__ void k_static_check(const unsigned long long* __restrict__ keys, unsigned long long n,
@@ -96,20 +93,24 @@ int report(char* err, size_t err_len, int status, const char* fmt, ...) {
     return status;
 }
 
-// The current device's scratch address, looked up on the first call per device.
+// The current device's scratch address.  In host code g_sort_scratch names a
+// host-side stand-in, not device memory; the device address comes from the
+// runtime, looked up on every call (a cheap table lookup once the module is
+// loaded) so that it always belongs to the device's current context.
 cudaError_t scratch_for_current_device(unsigned char** out, int* device) {
     cudaError_t e = cudaGetDevice(device);
     if (e != cudaSuccess) return e;
-    if (*device < 0 || *device >= kMaxDevices) return cudaErrorInvalidDevice;
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_ptr[*device]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_sort_scratch);
-        if (e != cudaSuccess) return e;
-        g_scratch_ptr[*device] = static_cast<unsigned char*>(p);
-    }
-    *out = g_scratch_ptr[*device];
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_sort_scratch);
+    if (e != cudaSuccess) return e;
+    *out = static_cast<unsigned char*>(p);
     return cudaSuccess;
+}
+
+// True when the byte ranges [a, a + na) and [b, b + nb) share a byte.
+bool overlaps(const void* a, size_t na, const void* b, size_t nb) {
+    const uintptr_t x = reinterpret_cast<uintptr_t>(a), y = reinterpret_cast<uintptr_t>(b);
+    return na && nb && x < y + nb && y < x + na;
 }
 
 // True when p is device (or managed) memory of `device`.
@@ -140,6 +141,15 @@ extern "C" int gs3dc_sort_pairs_static(int64_t total_pairs, const uint64_t* keys
                                        int num_tiles, uint64_t* keys_sorted, uint32_t* values_sorted,
                                        uint32_t* tile_ranges, void* stream, char* err, size_t err_len) {
     if (err && err_len) err[0] = '\0';
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        CKS(cudaStreamIsCapturing(st, &cs));
+        if (cs != cudaStreamCaptureStatusNone)
+            return report(err, err_len, GS3DC_ERR_INVALID_ARG,
+                          "the stream is being captured: this call waits for the stream and reads its status "
+                          "back, so it cannot be part of a CUDA graph");
+    }
     if (total_pairs < 0 || num_tiles <= 0)
         return report(err, err_len, GS3DC_ERR_INVALID_ARG, "bad pair input (P=%lld, tiles=%d)",
                       (long long)total_pairs, num_tiles);
@@ -163,8 +173,26 @@ extern "C" int gs3dc_sort_pairs_static(int64_t total_pairs, const uint64_t* keys
         (reinterpret_cast<uintptr_t>(values) | reinterpret_cast<uintptr_t>(values_sorted) |
          reinterpret_cast<uintptr_t>(tile_ranges)) & 3u)
         return report(err, err_len, GS3DC_ERR_INVALID_ARG, "misaligned key / value / range pointer");
+    {
+        // outputs may coincide exactly with their own input (in place) but overlap nothing else
+        const size_t kb = P * sizeof(uint64_t), vb = P * sizeof(uint32_t), rb = 2 * (size_t)num_tiles * 4;
+        const struct {
+            const void* p;
+            size_t n;
+        } in_k{keys, kb}, in_v{values, vb}, out_k{keys_sorted, kb}, out_v{values_sorted, vb}, out_r{tile_ranges, rb};
+        const bool bad_overlap =
+            (overlaps(out_k.p, out_k.n, in_k.p, in_k.n) && out_k.p != in_k.p) ||
+            (overlaps(out_v.p, out_v.n, in_v.p, in_v.n) && out_v.p != in_v.p) ||
+            overlaps(out_k.p, out_k.n, in_v.p, in_v.n) || overlaps(out_v.p, out_v.n, in_k.p, in_k.n) ||
+            overlaps(out_k.p, out_k.n, out_v.p, out_v.n) || overlaps(out_r.p, out_r.n, in_k.p, in_k.n) ||
+            overlaps(out_r.p, out_r.n, in_v.p, in_v.n) || overlaps(out_r.p, out_r.n, out_k.p, out_k.n) ||
+            overlaps(out_r.p, out_r.n, out_v.p, out_v.n);
+        if (bad_overlap)
+            return report(err, err_len, GS3DC_ERR_INVALID_ARG,
+                          "output buffers overlap an input or each other (only keys == keys_sorted and "
+                          "values == values_sorted, exactly, may share memory)");
+    }
 
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
     Control* ctrl = reinterpret_cast<Control*>(scratch + kOffControl);
     StepParams* sp = reinterpret_cast<StepParams*>(scratch + kOffParams);
     unsigned* bad = reinterpret_cast<unsigned*>(scratch + kOffFlags);
@@ -197,7 +225,7 @@ extern "C" int gs3dc_sort_pairs_static(int64_t total_pairs, const uint64_t* keys
     CKS(cudaMemsetAsync(ctrl, 0, sizeof(Control), st));
     CKS(cudaMemsetAsync(bad, 0, sizeof(unsigned), st));
     CKS(cudaMemsetAsync(desc, 0, (size_t)passes * desc_stride * sizeof(unsigned long long), st));
-    k_static_check<<<2 * 148, 256, 0, st>>>(k0, P, (unsigned)num_tiles, bad);
+    k_static_check<<<2 * sm_count(), 256, 0, st>>>(k0, P, (unsigned)num_tiles, bad);
     CKS(cudaGetLastError());
     k_static_commit<<<1, 32, 0, st>>>(ctrl, sp, bad, P, 1u << 22);
     CKS(cudaGetLastError());

@@ -116,22 +116,76 @@ def _workload_name(a) -> str:
 
 # ---------------------------------------------------------------- clocks
 class ClockSampler:
-    """nvidia-smi clock / throttle-reason samples every 200 ms during a region."""
+    """SM clock and clock-event reasons sampled DURING a timed region.
 
+    NVML (read-only queries) is polled from a host thread every 2 ms, so even a
+    timed region of a few tens of milliseconds gets samples; the ctypes and CUDA
+    waits of the timed loop release the interpreter lock meanwhile.  Without
+    NVML, nvidia-smi samples every 20 ms.  `stop()` summarises the samples.
+    """
     Q = ("index,pci.bus_id,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clock-event reason bits
+    REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20, "sw_power_cap": 0x4}
 
-    def __init__(self, bus_id: str | None):
+    def __init__(self, bus_id: str | None, period_s: float = 0.002):
+        import threading
         self.bus_id = (bus_id or "").lower()
+        self.rows = []          # (sm_mhz, sm_max_mhz, reason bits)
+        self.p = None
+        self.nvml = None
+        self.stop_evt = threading.Event()
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            h = None
+            if self.bus_id:
+                try:
+                    h = pynvml.nvmlDeviceGetHandleByPciBusId(bus_id)
+                except pynvml.NVMLError:
+                    h = None
+            if h is None:
+                h = pynvml.nvmlDeviceGetHandleByIndex(0)
+            self.nvml, self.h = pynvml, h
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+
+            def poll():
+                while not self.stop_evt.is_set():
+                    try:
+                        self.rows.append((pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM), self.max_mhz,
+                                          pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)))
+                    except pynvml.NVMLError:
+                        pass
+                    self.stop_evt.wait(period_s)
+            self.t = threading.Thread(target=poll, daemon=True)
+            self.t.start()
+            return
+        except Exception:
+            self.nvml = None
         self.f = tempfile.TemporaryFile(mode="w+")
         try:
             self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+                                       "-lms", "20"], stdout=self.f, stderr=subprocess.DEVNULL)
         except OSError:
             self.p = None
 
     def stop(self) -> dict:
+        if self.nvml is not None:
+            self.stop_evt.set()
+            self.t.join(5)
+            rows = list(self.rows)
+            try:
+                self.nvml.nvmlShutdown()
+            except Exception:
+                pass
+            if not rows:
+                return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0,
+                        "source": "nvml"}
+            reasons = sorted({k for r in rows for k, bit in self.REASONS.items() if r[2] & bit})
+            return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                    "sm_mhz_min": min(r[0] for r in rows), "reasons": reasons, "samples": len(rows),
+                    "source": "nvml, 2 ms"}
         if self.p is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.p.terminate()
@@ -155,7 +209,7 @@ class ClockSampler:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[k] for r in rows for k in range(4) if r[6 + k].lower() == "active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+                "reasons": reasons, "samples": len(rows), "source": "nvidia-smi, 20 ms"}
 
 
 def _bus_id(dev: int) -> str | None:
@@ -342,6 +396,7 @@ def _summary(a, r, world, X, N, T, depth_first, peak):
     dom = max((s for s in STAGES if s != "memsets"), key=lambda s: stage_ms[STAGES.index(s)])
     achieved = nbytes[dom] / (per_launch_ms[dom] * 1e-3) / 1e9
     traffic = None
+    issue = None
     tt = _traffic_table()
     # both 16-bit forms run the same rasterisers
     form_key = "bf16" if r["form"] == "fp16" else r["form"]
@@ -349,6 +404,10 @@ def _summary(a, r, world, X, N, T, depth_first, peak):
     if dom in kernels:
         k = kernels[dom]
         traffic = k["bytes_per_launch"] * (P / k["pairs"] if k.get("scale") == "pairs" else 1.0)
+        if k.get("issue_active_pct") is not None:
+            # an issue-bound kernel: the byte fraction is an instruction-efficiency figure
+            issue = {"issue_active": round(k["issue_active_pct"] / 100.0, 3), "limit": "issue slots",
+                     "warp_instructions_per_pair": k.get("warp_inst_per_pair")}
     step_bytes = sum(nbytes[s] * (pair_passes if s == "sort_passes" else 1) for s in nbytes)
     sp_ms = stage_ms[STAGES.index("sort_passes")]
     return {
@@ -360,7 +419,8 @@ def _summary(a, r, world, X, N, T, depth_first, peak):
         "stage_ms": {s: round(float(stage_ms[k]), 4) for k, s in enumerate(STAGES)},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak[0],
                      "peak_kind": peak[1], "unit": "GB/s", "frac": round(achieved / peak[0], 4),
-                     "traffic": traffic, "algorithmic_bytes_per_launch": int(nbytes[dom])},
+                     "traffic": traffic, "algorithmic_bytes_per_launch": int(nbytes[dom]),
+                     **({"issue": issue} if issue else {})},
         "step_roofline": {"algorithmic_bytes": int(step_bytes),
                           "frac": round(step_bytes / (ms_step * 1e-3) / 1e9 / peak[0], 4)},
         "sort_keys_per_s": round(P * pair_passes / (sp_ms * 1e-3), 1) if sp_ms > 0 else None,
@@ -419,7 +479,8 @@ def run_ours(a) -> int:
         line = {
             "metric": METRIC, "value": head["value"], "unit": "steps/s", "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32",
+            "vs_baseline": None,
+            "dtype": "f32" if chosen == "plain" else f"{chosen}-storage/f32-compute",
             "data": "synthetic (seeded; no dataset or checkpoint)",
             "form": "plain_fp32" if chosen == "plain" else f"{chosen}_storage",
             "config": {"workload": _workload_name(a), "gaussians": w.scene.count, "sh_degree": 3, "width": W,

@@ -174,13 +174,18 @@ int gs3dc_sort_pairs(gs3dc_ctx* ctx, int64_t total_pairs, const uint64_t* keys,
  * synchronisation of cudaMalloc / cudaFree.
  *   keys, values, keys_sorted, values_sorted (total_pairs entries) and
  *   tile_ranges (2*num_tiles entries) are device memory of the current device;
- *   the inputs are left unchanged (or may be the same buffers as the outputs).
+ *   the inputs are left unchanged, or keys_sorted / values_sorted may be
+ *   exactly the keys / values buffers (in place); any other overlap between
+ *   the five buffers is refused (GS3DC_ERR_INVALID_ARG).
  *   The scratch is one static device array of about 16 MiB per device, so
  *   total_pairs may not exceed GS3DC_STATIC_SORT_MAX_PAIRS
  *   (GS3DC_ERR_INVALID_ARG otherwise).  All calls on a device share it: calls
- *   that overlap on the GPU race.  The first call on each device looks up the
- *   scratch address; make it before any stream capture.  Runs on `stream`
- *   (a cudaStream_t, NULL = default stream) and returns once the sort is done.
+ *   that overlap on the GPU race.  Every call looks up the scratch's device
+ *   address on the current device, so a device reset leaves nothing stale.
+ *   Runs on `stream` (a cudaStream_t, NULL = default stream) and returns once
+ *   the sort is done: the call waits for the stream and reads a status word
+ *   back, so it cannot be captured into a CUDA graph (on a capturing stream it
+ *   returns GS3DC_ERR_INVALID_ARG and does nothing).
  *   err (may be NULL) receives a message of at most err_len bytes on failure. */
 #define GS3DC_STATIC_SORT_MAX_PAIRS 1048576
 int gs3dc_sort_pairs_static(int64_t total_pairs, const uint64_t* keys, const uint32_t* values,

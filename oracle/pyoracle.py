@@ -55,11 +55,17 @@ def _ptr(a, t):
     return a.ctypes.data_as(t) if a is not None else None
 
 
+# The reference project's root (harmonyos_3dgs/): only the build recipe of
+# oracle/_ref and the fixture generator read it; the tests use the built
+# library and the committed fixtures.
+REF_ROOT = os.environ.get("GS3D_REFERENCE_ROOT", "/root/reference/harmonyos_3dgs")
+
+
 def ensure_built(ref: bool = False) -> None:
     """Build liboracle.so (and, if asked and the reference tree exists, _ref)."""
     if not os.path.exists(LIB_C):
         subprocess.run(["make", "-s", "-C", HERE], check=True)
-    if ref and not os.path.exists(LIB_REF) and os.path.isdir("/root/reference/harmonyos_3dgs"):
+    if ref and not os.path.exists(LIB_REF) and os.path.isdir(REF_ROOT):
         subprocess.run(["make", "-s", "-C", HERE, "ref", "-j8"], check=True)
 
 

@@ -18,7 +18,7 @@ Two kinds of fixtures, both produced by the reference itself:
   controller's densify_and_prune (clone, split, prune) and reset_opacity; and the
   drivers' file formats (cameras.json, PLY load / save, PPM).
 
-It needs the reference tree at /root/reference (only this script reads it);
+It needs the reference tree (GS3D_REFERENCE_ROOT; only this script reads it);
 the tests and the GPU runs read the committed copies.
 """
 from __future__ import annotations
@@ -31,11 +31,12 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REF = "/root/reference/harmonyos_3dgs"
 sys.path.insert(0, REPO)
 
 from aaags_claude_b200 import scenes as S  # noqa: E402
 from oracle import pyoracle as O  # noqa: E402
+
+REF = O.REF_ROOT
 
 
 def copy_ref_fixtures():

@@ -18,7 +18,10 @@ from aaags_claude_b200 import gs3d
 from aaags_claude_b200 import scenes as S
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF_INCLUDE = "/root/reference/harmonyos_3dgs/include"
+from oracle.pyoracle import REF_ROOT  # noqa: E402
+
+REF_INCLUDE = os.path.join(REF_ROOT, "include")
+REF_SRC = os.path.join(REF_ROOT, "src")
 
 
 def _lib_path():
@@ -137,7 +140,7 @@ int main() { return 0; }
         p = os.path.join(d, "layout.cpp")
         open(p, "w").write(src)
         subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-I", REF_INCLUDE, "-I",
-                        "/root/reference/harmonyos_3dgs/src", "-I", os.path.join(ROOT, "include"), p], check=True)
+                        REF_SRC, "-I", os.path.join(ROOT, "include"), p], check=True)
 
 
 def test_workload_generators_are_seeded_and_well_formed():
@@ -186,4 +189,4 @@ def test_stage_adapters_compile_as_a_drop_in():
     if os.path.isdir(REF_INCLUDE):
         subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-DGS3D_WITH_REFERENCE_HEADERS", "-I",
                         os.path.join(ROOT, "include"), "-I", host, "-I", REF_INCLUDE, "-I",
-                        "/root/reference/harmonyos_3dgs/src", src], check=True)
+                        REF_SRC, src], check=True)

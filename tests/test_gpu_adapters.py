@@ -1,5 +1,5 @@
 """GPU: the C++ stage adapters (aaags_claude_b200/host) driven through the
-reference's abstract interfaces by host/stages_demo.cpp -- the drop-in
+reference's abstract interfaces by tests/native/stages_demo.cpp -- the drop-in
 boundary as a maintainer would wire it into Renderer / Trainer."""
 import os
 import subprocess
@@ -19,8 +19,23 @@ def _rd(d, name, dtype=np.float32):
     return np.fromfile(os.path.join(d, name), dtype=dtype)
 
 
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def _demo(tmp_path) -> str:
+    """Compiles the driver with the adapters and links it against the in-tree library."""
+    exe = os.path.join(str(tmp_path), "stages_demo")
+    lib_dir = os.path.dirname(build.LIB)
+    subprocess.run([os.environ.get("CXX", "g++"), "-O2", "-std=c++17", "-Wall", f"-I{build.INCLUDE}",
+                    f"-I{build.HOST}", os.path.join(build.HOST, "gs3d_stages_cuda.cpp"),
+                    os.path.join(HERE, "native", "stages_demo.cpp"), "-o", exe, f"-L{lib_dir}", "-lgs3d_cuda",
+                    f"-Wl,-rpath,{lib_dir}"], check=True)
+    return exe
+
+
 def test_stage_adapters_match_the_reference(tmp_path):
     build.build()
+    demo = _demo(tmp_path)
     z = np.load(os.path.join(U.SEEDED, "train_2k_128x128_adam.npz"))
     sc = S.Scene(z["in_positions"].copy(), z["in_scales"].copy(), z["in_rotations"].copy(), z["in_sh"].copy(),
                  z["in_opacities"].copy(), 3)
@@ -32,7 +47,7 @@ def test_stage_adapters_match_the_reference(tmp_path):
     z["cfg_bytes"].tofile(os.path.join(d, "render_config.bin"))
     z["tc_bytes"].tofile(os.path.join(d, "train_config.bin"))
     open(os.path.join(d, "meta.txt"), "w").write(f"{sc.count} 3 16 2\n")
-    r = subprocess.run([build.DEMO, d], capture_output=True, text=True, timeout=300)
+    r = subprocess.run([demo, d], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr
     cam = S.Camera.from_buffer_copy(z["cam_bytes"].tobytes())
     cfg = S.RenderConfig.from_buffer_copy(z["cfg_bytes"].tobytes())

@@ -4,8 +4,9 @@ It sorts caller-owned device buffers with its scratch in a static device
 array.  Its output must equal gs3dc_sort_pairs' (keys, values and tile ranges
 bit-exact) on consecutive calls that reuse the shared scratch: an even and an
 odd number of radix passes, a smaller sort after a larger one, and a sort of
-exactly the maximum size.  Oversized and non-device inputs are rejected with a
-message.  This file is collected last so that it also runs after every other
+exactly the maximum size, in place with an even and an odd number of passes.
+Oversized, non-device, partly overlapping and out-of-grid inputs and a
+capturing stream are rejected with a message.  This file is collected last so that it also runs after every other
 GPU test of the session; it passes on its own as well.
 """
 import ctypes
@@ -69,8 +70,62 @@ def test_two_calls_in_a_row_match_sort_pairs(ctx):
 
 def test_maximum_size_and_in_place(ctx):
     _check_against_sort_pairs(ctx, MAX_PAIRS, 8160, seed=13)
-    _check_against_sort_pairs(ctx, 123_457, 8160, seed=14, in_place=True)
+    _check_against_sort_pairs(ctx, 123_457, 8160, seed=14, in_place=True)   # 6 passes (even)
+    _check_against_sort_pairs(ctx, 98_765, 200, seed=16, in_place=True)     # 5 passes (odd)
     _check_against_sort_pairs(ctx, 5_000, 1, seed=15)   # one tile: 4 passes
+
+
+def test_rejects_a_key_outside_the_tile_grid(ctx):
+    import torch
+    L = gs3d.load_library()
+    keys, vals = _pairs(10_000, 64, seed=17)
+    keys[1234] = (np.uint64(64) << np.uint64(32)) | (keys[1234] & np.uint64(0xFFFFFFFF))   # tile 64 of 0..63
+    k_in = torch.from_numpy(keys.view(np.int64)).cuda()
+    v_in = torch.from_numpy(vals.view(np.int32)).cuda()
+    k_out = torch.empty_like(k_in)
+    v_out = torch.empty_like(v_in)
+    ranges = torch.full((2 * 64,), -1, dtype=torch.int32, device="cuda")
+    err = ctypes.create_string_buffer(512)
+    rc = L.gs3dc_sort_pairs_static(keys.shape[0], k_in.data_ptr(), v_in.data_ptr(), 64, k_out.data_ptr(),
+                                   v_out.data_ptr(), ranges.data_ptr(), None, err, len(err))
+    assert rc == gs3d.ERR_INVALID_ARG and b"tile field" in err.value
+    # nothing was indexed with the bad key: the ranges stay cleared
+    assert int(ranges.abs().sum()) == 0
+    # the shared scratch is usable by the next call
+    _check_against_sort_pairs(ctx, 50_000, 64, seed=18)
+
+
+def test_rejects_partial_overlap_and_a_capturing_stream():
+    import torch
+    L = gs3d.load_library()
+    err = ctypes.create_string_buffer(512)
+    P = 1000
+    buf = torch.zeros(4 * P, dtype=torch.int64, device="cuda")
+    vals = torch.zeros(P, dtype=torch.int32, device="cuda")
+    vout = torch.zeros(P, dtype=torch.int32, device="cuda")
+    ranges = torch.zeros(8, dtype=torch.int32, device="cuda")
+    base = buf.data_ptr()
+    # keys_sorted starts inside keys (not the same buffer)
+    rc = L.gs3dc_sort_pairs_static(P, base, vals.data_ptr(), 4, base + 8 * 10, vout.data_ptr(), ranges.data_ptr(),
+                                   None, err, len(err))
+    assert rc == gs3d.ERR_INVALID_ARG and b"overlap" in err.value
+    # tile ranges inside the sorted keys
+    rc = L.gs3dc_sort_pairs_static(P, base, vals.data_ptr(), 4, base + 8 * P, vout.data_ptr(), base + 8 * (P + 5),
+                                   None, err, len(err))
+    assert rc == gs3d.ERR_INVALID_ARG and b"overlap" in err.value
+    # a capturing stream is refused before anything is enqueued
+    s = torch.cuda.Stream()
+    g = torch.cuda.CUDAGraph()
+    x = torch.zeros(4, device="cuda")
+    torch.cuda.synchronize()
+    with torch.cuda.graph(g, stream=s):
+        x.add_(1.0)
+        rc = L.gs3dc_sort_pairs_static(P, base, vals.data_ptr(), 4, base + 8 * P, vout.data_ptr(),
+                                       ranges.data_ptr(), ctypes.c_void_p(s.cuda_stream), err, len(err))
+    assert rc == gs3d.ERR_INVALID_ARG and b"captured" in err.value
+    g.replay()
+    torch.cuda.synchronize()
+    assert float(x.sum()) == 4.0
 
 
 def test_rejects_oversized_and_host_inputs():
