@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstddef>
 #include <cstdarg>
@@ -19,12 +20,22 @@ using namespace gs3d;
 
 namespace {
 
-template <class T>
+// Bumped by every device (re)allocation of a context buffer that captured
+// launches address: a captured graph holds buffer addresses, so the graph
+// cache keys include this epoch and a graph captured before any reallocation
+// is never replayed after it.
+std::atomic<unsigned long long> g_alloc_epoch{1};
+
+// A device buffer that only grows.  kGraphAddressed = false: no captured launch
+// holds its address (buffers reached through the per-step parameter block,
+// such as the host targets' device copies), so reallocating it keeps graphs.
+template <class T, bool kGraphAddressed = true>
 struct DevBuf {
     T* p = nullptr;
     size_t n = 0;
     cudaError_t ensure(size_t need) {
         if (need <= n && p) return cudaSuccess;
+        if (kGraphAddressed) g_alloc_epoch.fetch_add(1, std::memory_order_relaxed);
         if (p) cudaFree(p);
         p = nullptr;
         n = 0;
@@ -35,6 +46,7 @@ struct DevBuf {
         return e;
     }
     void release() {
+        if (p && kGraphAddressed) g_alloc_epoch.fetch_add(1, std::memory_order_relaxed);
         if (p) cudaFree(p);
         p = nullptr;
         n = 0;
@@ -47,6 +59,8 @@ constexpr int kMaxBatchViews = 255;   // views per multi-view step (one 8-bit ra
 constexpr int kTunePpt[3] = {1, 2, 4};   // autotuner candidates: pixels per thread of the rasterisers
 constexpr int kTuneReps = 2;             // timed steps per candidate
 constexpr int kTuneSteps = 3 * kTuneReps;
+constexpr int kShapeSlots = 8;           // single-view train step: workload shapes with a cached graph / tuning
+constexpr int kGraphKey = 9;             // words of a graph key
 
 }  // namespace
 
@@ -121,6 +135,9 @@ struct gs3dc_ctx {
     DevBuf<int> n_contrib;
     DevBuf<unsigned> last_j;
     DevBuf<unsigned char> dsign;
+    // stored-list raster backward (gs3dc_raster_backward_lists): per-pixel entry offsets and the lists
+    DevBuf<int> list_off;
+    DevBuf<uint2> lists;
     // per-step parameters: device copy + pinned ring
     StepParams* sp_dev = nullptr;
     Persist* persist = nullptr;       // device
@@ -136,18 +153,29 @@ struct gs3dc_ctx {
     bool fused_adam = false;   // split backward + optimiser by default (faster at this occupancy)
     bool keep_grads = false;   // GS3DC_OPT_KEEP_GRADIENTS
     bool have_step_grads = false;
-    cudaGraphExec_t graph = nullptr;        // front half: preprocess .. tile ranges
-    cudaGraphExec_t graph_back = nullptr;   // back half: rasterisers, backward, optimiser
+    // captured single-view steps, one slot per workload shape (least recently used replaced): a
+    // caller alternating between camera sizes replays each size's graphs instead of re-capturing
+    struct GraphSlot {
+        long long key[kGraphKey] = {};
+        cudaGraphExec_t front = nullptr;   // preprocess .. tile ranges
+        cudaGraphExec_t back = nullptr;    // rasterisers, backward, optimiser
+        long long kernels = 0;
+        unsigned long long used = 0;       // LRU clock of the last replay
+    };
+    GraphSlot gslots[kShapeSlots];
+    unsigned long long gclock = 0;
+    long long graph_captures = 0;
+    // shapes whose pair capacity a synchronous step has validated (N, SH width, W, H, form, order)
+    long long seen_shape[kShapeSlots][6] = {};
+    int seen_next = 0;
     // host targets: copied on their own stream into alternating buffers while the front half runs
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t ev_gt_ready = nullptr;
     cudaEvent_t ev_gt_free[2] = {};
     bool gt_free_recorded[2] = {false, false};
     int gt_slot = 0;
-    DevBuf<float> gtb[2];
-    long long graph_key[8] = {};
+    DevBuf<float, false> gtb[2];   // read through StepParams::gt
     long long graph_replays = 0;
-    long long graph_kernels = 0;
     bool pending_check = false;
     // stage timing
     bool stage_timing = false;
@@ -162,18 +190,20 @@ struct gs3dc_ctx {
         DevBuf<float> col_b, depth, dm2, dcon, drgb, dop;
         DevBuf<int> radius, tiles;
         DevBuf<uint2> rects;
-        DevBuf<unsigned long long> dkeys[2];
+        DevBuf<unsigned> dkeys[2];                 // (view << 24 | depth's upper 24 bits) of each entry
         DevBuf<unsigned> dvals[2];
         DevBuf<unsigned long long> ddesc, sort_desc;
         DevBuf<unsigned> keys[2], vals[2];
         unsigned long long cap = 0;
-        DevBuf<float> image, T, gt;
+        DevBuf<float> image, T;
+        DevBuf<float, false> gt;                   // read through the views' StepParams::gt
         DevBuf<unsigned> last;
         DevBuf<unsigned char> dsign;
         DevBuf<unsigned> ranges, order;
         size_t grads_zeroed = 0;                   // entries of the screen-gradient accumulators known zero
+        std::vector<unsigned long long> view_pix;  // first pixel of each view of the last step (+ the total)
         cudaGraphExec_t graph = nullptr;
-        long long key[8] = {};
+        long long key[kGraphKey] = {};
     } batch;
     // rasteriser pixels per thread in use (set per step; 2 unless the autotuner chose otherwise)
     int fwd_ppt = 2, bwd_ppt = 2;
@@ -185,9 +215,11 @@ struct gs3dc_ctx {
         float fwd_ms[3] = {}, bwd_ms[3] = {};
         int fwd_ppt = 2, bwd_ppt = 2;
         bool done = false;
+        unsigned long long used = 0;   // LRU clock (single-view shapes)
     };
     bool autotune = false;
-    Tune tune_single, tune_batch;
+    Tune tune_single[kShapeSlots], tune_batch;
+    unsigned long long tclock = 0;
     cudaEvent_t tune_ev[3] = {};
     // options / stats
     unsigned spin_limit = 1u << 22;
@@ -207,11 +239,46 @@ int fail(gs3dc_ctx* c, int code, const char* fmt, ...) {
     return code;
 }
 
+void drop_slot(gs3dc_ctx::GraphSlot& s) {
+    if (s.front) cudaGraphExecDestroy(s.front);
+    if (s.back) cudaGraphExecDestroy(s.back);
+    s = gs3dc_ctx::GraphSlot();
+}
+
 void drop_graphs(gs3dc_ctx* c) {
-    if (c->graph) cudaGraphExecDestroy(c->graph);
-    if (c->graph_back) cudaGraphExecDestroy(c->graph_back);
+    for (auto& s : c->gslots) drop_slot(s);
     if (c->batch.graph) cudaGraphExecDestroy(c->batch.graph);
-    c->graph = c->graph_back = c->batch.graph = nullptr;
+    c->batch.graph = nullptr;
+}
+
+// The slot holding graphs captured under `key`, or nullptr.
+gs3dc_ctx::GraphSlot* find_slot(gs3dc_ctx* c, const long long key[kGraphKey]) {
+    for (auto& s : c->gslots)
+        if (s.front && std::memcmp(s.key, key, sizeof(s.key)) == 0) return &s;
+    return nullptr;
+}
+
+// An empty slot, else the least recently replayed one (its graphs destroyed).
+gs3dc_ctx::GraphSlot* victim_slot(gs3dc_ctx* c) {
+    gs3dc_ctx::GraphSlot* v = &c->gslots[0];
+    for (auto& s : c->gslots) {
+        if (!s.front) return &s;
+        if (s.used < v->used) v = &s;
+    }
+    drop_slot(*v);
+    return v;
+}
+
+bool shape_seen(const gs3dc_ctx* c, const long long shape[6]) {
+    for (const auto& s : c->seen_shape)
+        if (std::memcmp(s, shape, sizeof(s)) == 0) return true;
+    return false;
+}
+
+void mark_shape_seen(gs3dc_ctx* c, const long long shape[6]) {
+    if (shape_seen(c, shape)) return;
+    std::memcpy(c->seen_shape[c->seen_next], shape, sizeof(c->seen_shape[0]));
+    c->seen_next = (c->seen_next + 1) % kShapeSlots;
 }
 
 #define CK(call)                                                                                  \
@@ -552,8 +619,23 @@ void tune_end(gs3dc_ctx* c, gs3dc_ctx::Tune& t, float fwd_ms, float bwd_ms) {
     }
     t.fwd_ppt = kTunePpt[bf];
     t.bwd_ppt = kTunePpt[bb];
-    t.done = true;
-    drop_graphs(c);   // the next step captures the chosen kernels
+    t.done = true;   // graph keys hold the pixels per thread: the next step captures the chosen kernels
+}
+
+// The tuning state of a single-view workload shape (least recently used replaced).
+gs3dc_ctx::Tune& tune_slot(gs3dc_ctx* c, const long long key[6]) {
+    gs3dc_ctx::Tune* v = &c->tune_single[0];
+    for (auto& t : c->tune_single) {
+        if (std::memcmp(t.key, key, sizeof(t.key)) == 0) {
+            t.used = ++c->tclock;
+            return t;
+        }
+        if (t.used < v->used) v = &t;
+    }
+    *v = gs3dc_ctx::Tune();
+    std::memcpy(v->key, key, sizeof(v->key));
+    v->used = ++c->tclock;
+    return *v;
 }
 
 // ---- launch sequences ----
@@ -660,7 +742,7 @@ int seq_front_depth_first(gs3dc_ctx* c) {
     else
         CK(launch_preprocess_plain(c->stream, c->sp_dev, c->N, c->model_raw, false, model_ptrs(c),
                                    screen_ptrs(c, false), pr, c->ctrl,
-                                   DepthKeys{c->dkeys[0].p, c->dvals[0].p, nullptr, c->c_rects.p}));
+                                   DepthKeys{c->dkeys[0].p, c->dvals[0].p, false, c->c_rects.p}));
     if ((rc = mark(c, GS3DC_STAGE_SORT_HIST))) return rc;
     // the reduced form orders by the depth's upper 24 bits (relative steps of 2^-15; ties keep index order)
     const int depth_first_digit = chosen ? kChosenDepthSkip : 0;
@@ -923,7 +1005,7 @@ int batch_buffers(gs3dc_ctx* c, const BatchShape& sh) {
         CK(b.dkeys[k].ensure(vn));
         CK(b.dvals[k].ensure(vn));
     }
-    CK(b.ddesc.ensure(5 * ((vn + kSortTile - 1) / kSortTile) * 256));
+    CK(b.ddesc.ensure(4 * ((vn + kSortTile - 1) / kSortTile) * 256));
     CK(b.image.ensure(3 * sh.pix));
     CK(b.T.ensure(sh.pix));
     CK(b.last.ensure(sh.pix));
@@ -951,16 +1033,18 @@ int seq_batch(gs3dc_ctx* c, const BatchShape& sh) {
     CK(cudaMemsetAsync(c->ctrl_region.p, 0, ctrl_bytes_for((int)std::min<long long>(sh.VN, 0x7fffffffLL)),
                        c->stream));
     CK(cudaMemsetAsync(b.ranges.p, 0, 2 * (size_t)sh.tiles * sizeof(unsigned), c->stream));
-    CK(cudaMemsetAsync(b.ddesc.p, 0, 5 * dstride * sizeof(unsigned long long), c->stream));
+    CK(cudaMemsetAsync(b.ddesc.p, 0, 4 * dstride * sizeof(unsigned long long), c->stream));
     if (sh.tile_digits > 0)
         CK(cudaMemsetAsync(b.sort_desc.p, 0, (size_t)sh.tile_digits * pstride * sizeof(unsigned long long),
                            c->stream));
+    DepthKeys dk{b.dkeys[0].p, b.dvals[0].p};
+    dk.views24 = true;
     CK(launch_chosen_preprocess(c->stream, views, c->N, c->form == GS3DC_FORM_FP16, chosen_ptrs(c), batch_screen(c),
-                                DepthKeys{nullptr, b.dvals[0].p, b.dkeys[0].p}, b.rects.p, c->ctrl, sh.V));
-    // digits 1..3: the depth's upper 24 bits (as the single-view reduced form), digit 4: the view
+                                dk, b.rects.p, c->ctrl, sh.V));
+    // 32-bit keys: digits 0..2 the depth's upper 24 bits (as the single-view reduced form), digit 3 the view
     int dw = 0;
-    CK(launch_radix_sort(c->stream, views, 5, vn, b.dkeys[0].p, b.dvals[0].p, b.dkeys[1].p, b.dvals[1].p, b.ddesc.p,
-                         dstride, c->ctrl, &dw, nullptr, kChosenDepthSkip, &c->ctrl->gauss_keys));
+    CK(launch_radix_sort32(c->stream, views, 4, 0, false, vn, b.dkeys[0].p, b.dvals[0].p, b.dkeys[1].p, b.dvals[1].p,
+                           b.ddesc.p, dstride, c->ctrl, &dw, nullptr, &c->ctrl->gauss_keys, 0));
     PairPtrs pr{nullptr, b.vals[0].p, b.cap, c->scan_desc, b.keys[0].p};
     CK(launch_emit_ranked(c->stream, views, (int)vn, b.dvals[dw].p, batch_screen(c), pr, c->ctrl, b.rects.p, c->N,
                           5));
@@ -982,7 +1066,7 @@ int seq_batch(gs3dc_ctx* c, const BatchShape& sh) {
                                    chosen_ptrs(c), batch_rgrads(c),
                                    c->keep_grads ? grad_ptrs(c) : GradPtrs{nullptr, nullptr, nullptr, nullptr, nullptr},
                                    c->ctrl, sh.V));
-    c->kernels_last = 1 + 1 + (5 - kChosenDepthSkip) + 1 + (sh.tile_digits > 0 ? sh.tile_digits : 0) + 2 + 3;
+    c->kernels_last = 1 + 1 + 4 + 1 + (sh.tile_digits > 0 ? sh.tile_digits : 0) + 2 + 3;
     return GS3DC_OK;
 }
 
@@ -1149,7 +1233,7 @@ int gs3dc_set_option(gs3dc_ctx* c, int option, int64_t value) {
             return GS3DC_OK;
         case GS3DC_OPT_AUTOTUNE:
             c->autotune = value != 0;
-            c->tune_single = gs3dc_ctx::Tune();
+            for (auto& t : c->tune_single) t = gs3dc_ctx::Tune();
             c->tune_batch = gs3dc_ctx::Tune();
             drop_graphs(c);
             return GS3DC_OK;
@@ -1177,6 +1261,7 @@ int gs3dc_get_stat(gs3dc_ctx* c, int stat, int64_t* value) {
         case GS3DC_STAT_KERNELS_LAST: *value = c->kernels_last; return GS3DC_OK;
         case GS3DC_STAT_SORT_PASSES: *value = c->sort_passes; return GS3DC_OK;
         case GS3DC_STAT_GRAPH_REPLAYS: *value = c->graph_replays; return GS3DC_OK;
+        case GS3DC_STAT_GRAPH_CAPTURES: *value = c->graph_captures; return GS3DC_OK;
         case GS3DC_STAT_ADAM_STEP: *value = c->adam_step; return GS3DC_OK;
         case GS3DC_STAT_NUM_GAUSSIANS: *value = c->N; return GS3DC_OK;
         case GS3DC_STAT_SCREEN_GAUSSIANS: *value = c->screen_n; return GS3DC_OK;
@@ -1264,6 +1349,19 @@ int gs3dc_get_image(gs3dc_ctx* c, float* image) {
     if (c->W <= 0 || !c->image.p) return fail(c, GS3DC_ERR_STATE, "nothing has been rendered");
     CK(cudaSetDevice(c->device));
     CK(cudaMemcpyAsync(image, c->image.p, (size_t)c->W * c->H * 3 * 4, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return GS3DC_OK;
+}
+
+int gs3dc_get_batch_image(gs3dc_ctx* c, int view, float* image) {
+    if (!c || !image) return GS3DC_ERR_INVALID_ARG;
+    auto& b = c->batch;
+    if (b.view_pix.size() < 2 || !b.image.p) return fail(c, GS3DC_ERR_STATE, "no multi-view step has run");
+    const int nv = (int)b.view_pix.size() - 1;
+    if (view < 0 || view >= nv) return fail(c, GS3DC_ERR_INVALID_ARG, "view %d outside 0..%d", view, nv - 1);
+    CK(cudaSetDevice(c->device));
+    const unsigned long long p0 = b.view_pix[view], p1 = b.view_pix[view + 1];
+    CK(cudaMemcpyAsync(image, b.image.p + 3 * p0, (size_t)(p1 - p0) * 3 * 4, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     return GS3DC_OK;
 }
@@ -1733,14 +1831,17 @@ int gs3dc_train_step(gs3dc_ctx* c, const gs3d_camera* cam, const float* gt, int 
         CK(cudaEventRecord(c->ev_gt_ready, c->copy_stream));
         gt_dev = c->gtb[gslot].p;
     }
-    bool first = c->cap == 0 || c->sort_num_tiles != c->num_tiles;
-    if (first) {
+    // a shape's first step runs synchronously (an overflow of the pair-capacity guess is redone at
+    // once); later steps of a shape replay its graphs
+    const long long shape[6] = {c->N, c->max_coeffs, cam->width, cam->height, c->form, c->sort_mode};
+    bool first = c->cap == 0 || !shape_seen(c, shape);
+    if (c->cap == 0 || c->sort_num_tiles != c->num_tiles) {
         unsigned long long guess = c->min_cap ? c->min_cap : (unsigned long long)c->N * 8ull;
         if ((rc = ensure_pairs(c, guess > c->cap ? guess : c->cap, c->num_tiles))) return rc;
     }
     const int step_before = c->adam_step;
     const long long tkey[6] = {c->N, cam->width, cam->height, c->form, c->sort_mode, c->fused_adam ? 1 : 0};
-    const bool tuning = tune_begin(c, c->tune_single, tkey);
+    const bool tuning = tune_begin(c, tune_slot(c, tkey), tkey);
     const bool user_timing = c->stage_timing;
     if (tuning) c->stage_timing = true;   // the trial step runs un-captured with events between stages
     struct RestoreTiming {
@@ -1751,39 +1852,48 @@ int gs3dc_train_step(gs3dc_ctx* c, const gs3d_camera* cam, const float* gt, int 
     for (int attempt = 0; attempt < 3; attempt++) {
         c->adam_step = step_before + (tc->use_adam ? 1 : 0);
         if ((rc = push_params(c, cam, cfg, tc, iteration, gt_dev))) return rc;
-        const long long key[8] = {c->N, c->max_coeffs, cam->width, cam->height, (long long)c->cap, c->sort_passes,
-                                  (long long)c->spin_limit,
-                                  (c->fused_adam ? 1 : 2) + 4 * c->sort_mode + 16 * c->form + 64 * (c->keep_grads ? 1 : 0) +
-                                      128 * c->fwd_ppt + 1024 * c->bwd_ppt};
-        const bool key_ok = c->graph && std::memcmp(key, c->graph_key, sizeof(key)) == 0;
+        const long long key[kGraphKey] = {
+            c->N, c->max_coeffs, cam->width, cam->height, (long long)c->cap, c->sort_passes,
+            (long long)c->spin_limit,
+            (c->fused_adam ? 1 : 2) + 4 * c->sort_mode + 16 * c->form + 64 * (c->keep_grads ? 1 : 0) +
+                128 * c->fwd_ppt + 1024 * c->bwd_ppt,
+            (long long)g_alloc_epoch.load(std::memory_order_relaxed)};
         c->kernels_last = 0;
         if (c->use_graph && !c->stage_timing && !first && attempt == 0) {
-            if (!key_ok) {
-                drop_graphs(c);
+            gs3dc_ctx::GraphSlot* slot = find_slot(c, key);
+            if (!slot) {
+                slot = victim_slot(c);
                 cudaGraph_t g;
                 CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
                 rc = seq_train_front(c);
                 cudaError_t ec = cudaStreamEndCapture(c->stream, &g);
                 if (rc) return rc;
                 CK(ec);
-                CK(cudaGraphInstantiate(&c->graph, g, 0));
+                cudaError_t ei = cudaGraphInstantiate(&slot->front, g, 0);
                 cudaGraphDestroy(g);
-                const long long k_front = c->kernels_last;
+                CK(ei);
                 CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
                 rc = seq_train_back(c);
                 ec = cudaStreamEndCapture(c->stream, &g);
-                if (rc) return rc;
+                if (rc) {
+                    drop_slot(*slot);
+                    return rc;
+                }
+                if (ec != cudaSuccess) drop_slot(*slot);
                 CK(ec);
-                CK(cudaGraphInstantiate(&c->graph_back, g, 0));
+                ei = cudaGraphInstantiate(&slot->back, g, 0);
                 cudaGraphDestroy(g);
-                std::memcpy(c->graph_key, key, sizeof(key));
-                c->graph_kernels = c->kernels_last;
-                (void)k_front;
+                if (ei != cudaSuccess) drop_slot(*slot);
+                CK(ei);
+                std::memcpy(slot->key, key, sizeof(key));
+                slot->kernels = c->kernels_last;
+                c->graph_captures++;
             }
-            c->kernels_last = c->graph_kernels;
-            CK(cudaGraphLaunch(c->graph, c->stream));
+            slot->used = ++c->gclock;
+            c->kernels_last = slot->kernels;
+            CK(cudaGraphLaunch(slot->front, c->stream));
             if (host_gt) CK(cudaStreamWaitEvent(c->stream, c->ev_gt_ready, 0));
-            CK(cudaGraphLaunch(c->graph_back, c->stream));
+            CK(cudaGraphLaunch(slot->back, c->stream));
             c->graph_replays++;
         } else {
             if ((rc = seq_train_front(c))) return rc;
@@ -1815,13 +1925,14 @@ int gs3dc_train_step(gs3dc_ctx* c, const gs3d_camera* cam, const float* gt, int 
             first = true;
             continue;
         }
+        mark_shape_seen(c, shape);   // the capacity holds this shape's pairs
         if (loss) *loss = (float)(c->ctrl_host->loss_sum / (double)(3.0 * (double)np));
         if (c->stage_timing) {
             for (int k = 0; k < GS3DC_NUM_STAGES; k++)
                 CK(cudaEventElapsedTime(&c->stage_ms[k], c->stage_ev[k], c->stage_ev[k + 1]));
         }
         if (tuning)
-            tune_end(c, c->tune_single, c->stage_ms[GS3DC_STAGE_RASTER_FWD], c->stage_ms[GS3DC_STAGE_RASTER_BWD]);
+            tune_end(c, tune_slot(c, tkey), c->stage_ms[GS3DC_STAGE_RASTER_FWD], c->stage_ms[GS3DC_STAGE_RASTER_BWD]);
         return GS3DC_OK;
     }
     c->adam_step = step_before;
@@ -1847,14 +1958,17 @@ int gs3dc_train_step_batch(gs3dc_ctx* c, int n_views, const gs3d_camera* cams, c
     if (sh.VN >= (1LL << 31)) return fail(c, GS3DC_ERR_INVALID_ARG, "%lld (view, Gaussian) entries exceed 2^31", sh.VN);
     std::vector<unsigned> tile_base(n_views), pix_base(n_views);
     unsigned long long tiles = 0, pix = 0, max_view_tiles = 0;
+    b.view_pix.clear();
     for (int v = 0; v < n_views; v++) {
         const int gx = (cams[v].width + cfg->tile_w - 1) / cfg->tile_w, gy = (cams[v].height + cfg->tile_h - 1) / cfg->tile_h;
         tile_base[v] = (unsigned)tiles;
         pix_base[v] = (unsigned)pix;
+        b.view_pix.push_back(pix);
         tiles += (unsigned long long)gx * gy;
         max_view_tiles = std::max(max_view_tiles, (unsigned long long)gx * gy);
         pix += (unsigned long long)cams[v].width * cams[v].height;
     }
+    b.view_pix.push_back(pix);
     if (tiles >= (1ull << 24) || pix >= (1ull << 31))
         return fail(c, GS3DC_ERR_INVALID_ARG, "the views' %llu tiles / %llu pixels exceed 2^24 / 2^31", tiles, pix);
     sh.tiles = (unsigned)tiles;
@@ -1895,9 +2009,10 @@ int gs3dc_train_step_batch(gs3dc_ctx* c, int n_views, const gs3d_camera* cams, c
         CK(cudaMemcpyAsync(b.views.p, b.views_host, (size_t)n_views * sizeof(StepParams), cudaMemcpyHostToDevice,
                            c->stream));
         CK(cudaEventRecord(b.views_event, c->stream));
-        const long long key[8] = {c->N, n_views, (long long)sh.tiles, (long long)sh.pix, (long long)b.cap,
-                                  c->form, (long long)c->spin_limit,
-                                  c->max_coeffs + 1000 * (c->keep_grads ? 1 : 0) + 2000 * c->fwd_ppt + 20000 * c->bwd_ppt};
+        const long long key[kGraphKey] = {
+            c->N, n_views, (long long)sh.tiles, (long long)sh.pix, (long long)b.cap, c->form, (long long)c->spin_limit,
+            c->max_coeffs + 1000 * (c->keep_grads ? 1 : 0) + 2000 * c->fwd_ppt + 20000 * c->bwd_ppt,
+            (long long)g_alloc_epoch.load(std::memory_order_relaxed)};
         if (c->use_graph && !first && !tuning && attempt == 0) {
             if (!b.graph || std::memcmp(key, b.key, sizeof(key)) != 0) {
                 if (b.graph) cudaGraphExecDestroy(b.graph);
@@ -1910,6 +2025,7 @@ int gs3dc_train_step_batch(gs3dc_ctx* c, int n_views, const gs3d_camera* cams, c
                 CK(ec);
                 CK(cudaGraphInstantiate(&b.graph, g, 0));
                 cudaGraphDestroy(g);
+                c->graph_captures++;
             }
             CK(cudaGraphLaunch(b.graph, c->stream));
             c->graph_replays++;
@@ -2099,6 +2215,44 @@ static int dc_scan(gs3dc_ctx* c, const int* in, int* out, int n, int* total) {
     CK(launch_scan_int(c->stream, in, out, c->dc_sums.p, n));
     CK(cudaMemcpyAsync(total, c->dc_sums.p + nb, 4, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    return GS3DC_OK;
+}
+
+int gs3dc_raster_backward_lists(gs3dc_ctx* c, const gs3d_camera* cam, const gs3d_render_config* cfg,
+                                const float* d_image, float* d_means2D, float* d_conics, float* d_rgb,
+                                float* d_opacities_2d, int64_t* list_bytes) {
+    if (!c || !d_image) return GS3DC_ERR_INVALID_ARG;
+    if (int rc_ = require_plain(c, "gs3dc_raster_backward_lists")) return rc_;
+    int rc;
+    if ((rc = check_config(c, cam, cfg))) return rc;
+    if (!c->have_raster || c->screen_imported)
+        return fail(c, GS3DC_ERR_STATE, "gs3dc_raster_backward_lists needs gs3dc_rasterize of the device model first");
+    CK(cudaSetDevice(c->device));
+    const size_t np = (size_t)c->W * c->H, n = (size_t)c->screen_n;
+    if (np >= 0x7fffffffu) return fail(c, GS3DC_ERR_INVALID_ARG, "%zu pixels: the list offsets are 32-bit", np);
+    CK(c->d_image.ensure(3 * np));
+    CK(cudaMemcpyAsync(c->d_image.p, d_image, 3 * np * 4, cudaMemcpyHostToDevice, c->stream));
+    if ((rc = push_params(c, cam, cfg, nullptr, 0, nullptr))) return rc;
+    // entry offsets: exclusive scan of the forward's contributor counts
+    CK(c->list_off.ensure(np + 1));
+    int total = 0;
+    if ((rc = dc_scan(c, c->n_contrib.p, c->list_off.p, (int)np, &total))) return rc;
+    CK(c->lists.ensure(total > 0 ? (size_t)total : 1));
+    CK(cudaMemsetAsync(c->dm2.p, 0, 2 * n * 4, c->stream));
+    CK(cudaMemsetAsync(c->dcon.p, 0, 3 * n * 4, c->stream));
+    CK(cudaMemsetAsync(c->drgb.p, 0, 3 * n * 4, c->stream));
+    CK(cudaMemsetAsync(c->dop.p, 0, n * 4, c->stream));
+    const int w = c->sorted_which;
+    CK(launch_list_fill(c->stream, c->sp_dev, c->num_tiles, c->ranges.p, c->vals[w].p, screen_ptrs(c, false),
+                        c->n_contrib.p, c->list_off.p, c->lists.p));
+    CK(launch_list_bwd(c->stream, c->sp_dev, c->num_tiles, screen_ptrs(c, false), pixel_ptrs(c), c->list_off.p,
+                       c->lists.p, rgrad_ptrs(c)));
+    if ((rc = download(c, d_means2D, c->dm2.p, 2 * n * 4)) || (rc = download(c, d_conics, c->dcon.p, 3 * n * 4)) ||
+        (rc = download(c, d_rgb, c->drgb.p, 3 * n * 4)) || (rc = download(c, d_opacities_2d, c->dop.p, n * 4)))
+        return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    if (list_bytes) *list_bytes = (int64_t)(np * sizeof(int) + (size_t)total * sizeof(uint2));
+    c->have_rgrad = true;
     return GS3DC_OK;
 }
 

@@ -221,8 +221,7 @@ __global__ void __launch_bounds__(kBlock) k_chosen_preprocess(const StepParams* 
     s.tiles[o] = cnt;
     rects[o] = rect;
     const unsigned key = cnt > 0 ? dbits : 0xFFFFFFFFu;
-    if (dk.keys64) dk.keys64[o] = ((unsigned long long)view << 32) | key;
-    else dk.keys[o] = key;
+    dk.keys[o] = dk.views24 ? ((unsigned)view << 24) | (key >> 8) : key;
     dk.vals[o] = (unsigned)o;
 }
 
@@ -356,31 +355,117 @@ __global__ void __launch_bounds__(kCB, MULTI ? 8 : 10) k_chosen_backward(const S
         __syncthreads();
     }
     // ---- phase 1: per-Gaussian adjoint (summed over the views) ----
+    if (MULTI) {
+        // Several views: the activation, cov3D, the cov3D -> scale / rotation chain and the sigmoid
+        // do not depend on the camera and every gradient is linear in the screen gradients, so
+        // one thread per Gaussian sums the views' camera-dependent parts (backward_view: SH,
+        // conic -> cov3D, position) and applies the rest once.  Each view's screen gradients are
+        // loaded one view ahead, straight into registers, and zeroed for the next step.
+        if (tid < ng) {
+            const long long gi = g0 + tid;
+            float p[3], rsc[3], rq[4], rop, sc[3], q[4], op, c3[6];
+#pragma unroll
+            for (int k = 0; k < 3; k++) p[k] = sm.pos[3 * tid + k];
+            load_attr<S>(sm.attr, tid, rsc, &rop, rq);
+            activate_one(rsc, rq, rop, sc, q, &op);
+            const float mod = sp.cfg.scale_modifier;
+            cov3d(sc, mod, q, c3);
+#pragma unroll
+            for (int k = 0; k < 48; k++)
+                if (k < mc3) sm.g_sh[kShPitch * tid + k] = 0.f;
+            float gp[3] = {0.f, 0.f, 0.f}, dcs[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, dops = 0.f;
+            float nx[9];
+            auto load_view = [&](long long e, float d[9]) {
+                const float2 m = reinterpret_cast<const float2*>(rg.dm2)[e];
+                d[0] = m.x;
+                d[1] = m.y;
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    d[2 + k] = rg.dcon[3 * e + k];
+                    d[5 + k] = rg.drgb[3 * e + k];
+                }
+                d[8] = rg.dop[e];
+            };
+            load_view(gi, nx);
+            for (int v = 0; v < n_views; v++) {
+                const long long e = (long long)v * N + gi;   // this view's (view, Gaussian) entry
+                float cur[9];
+#pragma unroll
+                for (int k = 0; k < 9; k++) cur[k] = nx[k];
+                if (v + 1 < n_views) load_view(e + N, nx);
+                // the screen-gradient accumulators restart at zero for the next step
+                reinterpret_cast<float2*>(rg.dm2)[e] = make_float2(0.f, 0.f);
+#pragma unroll
+                for (int k = 0; k < 3; k++) rg.dcon[3 * e + k] = rg.drgb[3 * e + k] = 0.f;
+                rg.dop[e] = 0.f;
+                bool any = false;
+#pragma unroll
+                for (int k = 0; k < 9; k++) any |= cur[k] != 0.f;
+                if (!any) continue;   // a view without screen gradients adds nothing
+                BwdIn in;
+                in.dm[0] = cur[0];
+                in.dm[1] = cur[1];
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    in.dcn[k] = cur[2 + k];
+                    in.drgb[k] = cur[5 + k];
+                }
+                in.dop = cur[8];
+                float shf[48];
+                if (mc3 == 48) {
+                    const uint4* row = sm.sh + 6 * tid;
+#pragma unroll
+                    for (int qd = 0; qd < 6; qd++) {
+                        const uint4 vv = row[qd];
+                        const S* h = reinterpret_cast<const S*>(&vv);
+#pragma unroll
+                        for (int k = 0; k < 8; k++) shf[8 * qd + k] = ldf(h[k]);
+                    }
+                } else {
+                    const S* shs = reinterpret_cast<const S*>(sm.sh) + mc3 * tid;
+#pragma unroll
+                    for (int k = 0; k < 48; k++) shf[k] = k < mc3 ? ldf(shs[k]) : 0.f;
+                }
+                BwdOut o;
+#pragma unroll
+                for (int k = 0; k < 3; k++) o.gp[k] = o.geff[k] = 0.f;
+#pragma unroll
+                for (int k = 0; k < 16; k++) o.basis[k] = 0.f;
+                float dcov[6];
+                if (backward_view(spp[v], p, c3, shf, in, o, dcov)) {
+#pragma unroll
+                    for (int k = 0; k < 6; k++) dcs[k] += dcov[k];
+                }
+#pragma unroll
+                for (int k = 0; k < 3; k++) gp[k] += o.gp[k];
+                dops += cur[8];
+#pragma unroll
+                for (int k = 0; k < 48; k++)
+                    if (k < mc3) sm.g_sh[kShPitch * tid + k] += o.basis[k / 3] * o.geff[k % 3];
+            }
+            BwdOut o;
+            backward_cov3d(mod, sc, q, rq, dcs, o);
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                sm.g_pos[3 * tid + k] = gp[k];
+                sm.g_sc[3 * tid + k] = o.gs[k];
+            }
+#pragma unroll
+            for (int k = 0; k < 4; k++) sm.g_rot[4 * tid + k] = o.gq[k];
+            sm.g_op[tid] = dops * op * (1.0f - op);   // chain 3 (:231-232) on the summed opacity gradient
+        }
+    } else {
     if (tid < ng) {
 #pragma unroll
         for (int k = 0; k < 3; k++) sm.g_pos[3 * tid + k] = sm.g_sc[3 * tid + k] = 0.f;
 #pragma unroll
         for (int k = 0; k < 4; k++) sm.g_rot[4 * tid + k] = 0.f;
         sm.g_op[tid] = 0.f;
-        if (MULTI) {
-            for (int k = 0; k < mc3; k++) sm.g_sh[kShPitch * tid + k] = 0.f;
-        } else {
-            for (int k = 0; k < 16; k++) sm.basis[k * kCB + tid] = 0.f;
-            for (int k = 0; k < 3; k++) sm.geff[k * kCB + tid] = 0.f;
-        }
+        for (int k = 0; k < 16; k++) sm.basis[k * kCB + tid] = 0.f;
+        for (int k = 0; k < 3; k++) sm.geff[k * kCB + tid] = 0.f;
     }
-    for (int v = 0; v < (MULTI ? n_views : 1); v++) {
-        const long long e0 = (long long)v * N + g0;   // this view's first (view, Gaussian) entry
-        if (MULTI) {
-            __syncthreads();   // the previous view's screen gradients have been read
-            for (int e = tid; e < 2 * ng; e += kCB) sm.dm2[e] = rg.dm2[2 * e0 + e];
-            for (int e = tid; e < 3 * ng; e += kCB) {
-                sm.dcon[e] = rg.dcon[3 * e0 + e];
-                sm.drgb[e] = rg.drgb[3 * e0 + e];
-            }
-            for (int e = tid; e < ng; e += kCB) sm.dop[e] = rg.dop[e0 + e];
-            __syncthreads();
-        }
+    {
+        const long long e0 = g0;
         // the screen-gradient accumulators restart at zero for the next step
         for (int e = tid; e < 2 * ng; e += kCB) rg.dm2[2 * e0 + e] = 0.f;
         for (int e = tid; e < 3 * ng; e += kCB) {
@@ -398,12 +483,11 @@ __global__ void __launch_bounds__(kCB, MULTI ? 8 : 10) k_chosen_backward(const S
             in.dm[0] = sm.dm2[2 * tid];
             in.dm[1] = sm.dm2[2 * tid + 1];
             in.dop = sm.dop[tid];
-            // every gradient is linear in the screen gradients: a view without any adds none
+            // every gradient is linear in the screen gradients: a Gaussian without any adds none
             const bool any = in.dm[0] != 0.f || in.dm[1] != 0.f || in.dcn[0] != 0.f || in.dcn[1] != 0.f ||
                              in.dcn[2] != 0.f || in.drgb[0] != 0.f || in.drgb[1] != 0.f || in.drgb[2] != 0.f ||
                              in.dop != 0.f;
             if (any) {
-                // parameters from shared memory, per view: nothing stays live across the view loop
 #pragma unroll
                 for (int k = 0; k < 3; k++) in.p[k] = sm.pos[3 * tid + k];
                 in.act = nullptr;
@@ -413,11 +497,11 @@ __global__ void __launch_bounds__(kCB, MULTI ? 8 : 10) k_chosen_backward(const S
                     // this Gaussian's 96 SH bytes as six 16-byte loads
                     const uint4* row = sm.sh + 6 * tid;
 #pragma unroll
-                    for (int q = 0; q < 6; q++) {
-                        const uint4 vv = row[q];
+                    for (int qd = 0; qd < 6; qd++) {
+                        const uint4 vv = row[qd];
                         const S* h = reinterpret_cast<const S*>(&vv);
 #pragma unroll
-                        for (int k = 0; k < 8; k++) shf[8 * q + k] = ldf(h[k]);
+                        for (int k = 0; k < 8; k++) shf[8 * qd + k] = ldf(h[k]);
                     }
                 } else {
                     const S* shs = reinterpret_cast<const S*>(sm.sh) + mc3 * tid;
@@ -433,25 +517,22 @@ __global__ void __launch_bounds__(kCB, MULTI ? 8 : 10) k_chosen_backward(const S
                 o.gop = 0.f;
 #pragma unroll
                 for (int k = 0; k < 16; k++) o.basis[k] = 0.f;
-                backward_one(spp[v], in, o);
+                backward_one(sp, in, o);
 #pragma unroll
                 for (int k = 0; k < 3; k++) {
-                    sm.g_pos[3 * tid + k] += o.gp[k];
-                    sm.g_sc[3 * tid + k] += o.gs[k];
+                    sm.g_pos[3 * tid + k] = o.gp[k];
+                    sm.g_sc[3 * tid + k] = o.gs[k];
                 }
 #pragma unroll
-                for (int k = 0; k < 4; k++) sm.g_rot[4 * tid + k] += o.gq[k];
-                sm.g_op[tid] += o.gop;
-                if (MULTI) {
-                    for (int k = 0; k < mc3; k++) sm.g_sh[kShPitch * tid + k] += o.basis[k / 3] * o.geff[k % 3];
-                } else {
+                for (int k = 0; k < 4; k++) sm.g_rot[4 * tid + k] = o.gq[k];
+                sm.g_op[tid] = o.gop;
 #pragma unroll
-                    for (int k = 0; k < 16; k++) sm.basis[k * kCB + tid] = o.basis[k];
+                for (int k = 0; k < 16; k++) sm.basis[k * kCB + tid] = o.basis[k];
 #pragma unroll
-                    for (int k = 0; k < 3; k++) sm.geff[k * kCB + tid] = o.geff[k];
-                }
+                for (int k = 0; k < 3; k++) sm.geff[k * kCB + tid] = o.geff[k];
             }
         }
+    }
     }
     __syncthreads();
     // ---- phase 2: optimiser over this CTA's slice (and the gradients, when kept) ----

@@ -828,7 +828,7 @@ __global__ void __launch_bounds__(kE3Threads) k_raster_e3(const StepParams* __re
         cnt++;
     }
     if (inside) {
-        const int pix = y * W + x;
+        const size_t pix = (size_t)y * W + x;
         px.image[3 * pix] = C0 + T * sp.cfg.bg_color[0];
         px.image[3 * pix + 1] = C1 + T * sp.cfg.bg_color[1];
         px.image[3 * pix + 2] = C2 + T * sp.cfg.bg_color[2];

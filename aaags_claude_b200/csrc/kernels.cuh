@@ -121,7 +121,7 @@ struct ScreenArrays {
 struct DepthKeys {
     unsigned* keys;             // [N] depth bits, ~0u for Gaussians without pairs
     unsigned* vals;             // [N] Gaussian index
-    unsigned long long* keys64 = nullptr;   // several views: (view << 32 | depth bits) instead of keys
+    bool views24 = false;       // several views: keys = view << 24 | the depth's upper 24 bits
     uint2* rects = nullptr;   // plain preprocess: tile rectangles (xmin | ymin << 16, xmax | ymax << 16), 0 if none
 };
 
@@ -146,7 +146,9 @@ cudaError_t launch_chosen_to_raw(cudaStream_t st, int N, int mc3, bool fp16, Cho
 // and tile rectangles (the reference's rectangle cut to the box of the
 // ellipse where alpha can reach 1/255).
 // n_views > 1: sp is the views' parameter array; the outputs hold (view,
-// Gaussian) entries view * N + i and the depth keys go to dk.keys64.
+// Gaussian) entries view * N + i and, with dk.views24, the 32-bit depth key
+// is the view above the depth's upper 24 bits (one 4-pass sort orders every
+// entry by (view, depth)).
 cudaError_t launch_chosen_preprocess(cudaStream_t st, const StepParams* sp, int N, bool fp16, ChosenPtrs c,
                                      ScreenPtrs s, DepthKeys dk, uint2* rects, Control* ctrl, int n_views = 1);
 // Forward rasteriser with the fast-exp blend decision and fused L1.
@@ -220,6 +222,15 @@ cudaError_t launch_raster_fwd_plain(cudaStream_t st, const StepParams* sp, int n
 cudaError_t launch_raster_bwd_plain(cudaStream_t st, const StepParams* sp, int num_tiles, bool from_sign,
                                     const unsigned* ranges, const unsigned* order, const unsigned* vals,
                                     ScreenPtrs s, PixelPtrs px, RGradPtrs g, Control* ctrl, int ppt = 2);
+// Stored-list raster backward (memory comparison with the recompute backward):
+// each pixel's contributors (Gaussian, alpha bits) are replayed into
+// list[offset[pix] .. offset[pix] + n_contrib[pix]), then walked back to front
+// with the explicit image gradient px.d_image.
+cudaError_t launch_list_fill(cudaStream_t st, const StepParams* sp, int num_tiles, const unsigned* ranges,
+                             const unsigned* vals, ScreenPtrs s, const int* n_contrib, const int* offset,
+                             uint2* list);
+cudaError_t launch_list_bwd(cudaStream_t st, const StepParams* sp, int num_tiles, ScreenPtrs s, PixelPtrs px,
+                            const int* offset, const uint2* list, RGradPtrs g);
 // mode: 0 = write GradientOutput (stage API), 1 = fused optimiser, 2 = write
 // GradientOutput for a following launch_optimizer_plain and zero the screen
 // gradient accumulators (split train step).  mc3 in {3, 12, 27, 48}.

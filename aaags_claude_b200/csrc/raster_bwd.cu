@@ -150,7 +150,7 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_bwd(const StepParams* __re
         last[p] = 0;
         dC[p][0] = dC[p][1] = dC[p][2] = 0.0f;
         if (x < W && y < H) {
-            const int pix = (int)sp.pix_base + y * W + x;
+            const size_t pix = (size_t)sp.pix_base + (size_t)y * W + x;   // up to 2^31 pixels, 3 floats each
             T[p] = px.T_final[pix];
             last[p] = px.last_j[pix];
             if (FROM_SIGN) {
@@ -259,7 +259,7 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_bwd(const StepParams* __re
 #pragma unroll
         for (int e = threadIdx.x; e < kBwdBatch; e += kBwdThreads) {
             if (bs + (unsigned)e < be) {
-                const unsigned gi = s_idx[e];
+                const size_t gi = s_idx[e];   // (view, Gaussian) entry: 3 * gi can pass 2^32
                 float* const dst[9] = {&g.drgb[3 * gi], &g.drgb[3 * gi + 1], &g.drgb[3 * gi + 2], &g.dop[gi],
                                        &g.dm2[2 * gi], &g.dm2[2 * gi + 1], &g.dcon[3 * gi], &g.dcon[3 * gi + 1],
                                        &g.dcon[3 * gi + 2]};
@@ -285,7 +285,108 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_bwd(const StepParams* __re
     }
 }
 
+// ---- stored-list variant (memory comparison only) ----
+// The reference holds each pixel's contributors as a list: its CPU backward
+// replays the forward into a per-pixel vector of (Gaussian, alpha)
+// (rasterizer_backward_cpu.cpp:40-67) and its OpenCL kernel into private arrays
+// of up to 128 entries (rasterize_backward.cl:79-121), then walks the list back
+// to front.  k_list_fill / k_list_bwd do the same with the lists in one device
+// buffer (entry offsets = exclusive scan of n_contrib), so that their memory
+// can be measured against the recompute backward above, which keeps no list.
+// One thread per pixel, no staging: these kernels are not on the train step.
+__global__ void __launch_bounds__(256) k_list_fill(const StepParams* __restrict__ spp,
+                                                   const unsigned* __restrict__ ranges,
+                                                   const unsigned* __restrict__ vals, ScreenPtrs s,
+                                                   const int* __restrict__ n_contrib, const int* __restrict__ offset,
+                                                   uint2* __restrict__ list) {
+    const StepParams& sp = *spp;
+    const int tile = blockIdx.x;
+    const int tx = tile % sp.grid_x, ty = tile / sp.grid_x;
+    const int x = tx * kTile + (int)(threadIdx.x & 15), y = ty * kTile + (int)(threadIdx.x >> 4);
+    if (x >= sp.cam.width || y >= sp.cam.height) return;
+    const size_t pix = (size_t)y * sp.cam.width + x;
+    const int n = n_contrib[pix];
+    uint2* out = list + offset[pix];
+    const float fx = (float)x, fy = (float)y;
+    float T = 1.0f;
+    int c = 0;
+    for (unsigned j = ranges[2 * tile]; j < ranges[2 * tile + 1] && c < n; j++) {
+        const unsigned g = vals[j];
+        const float4 r0 = s.rec0[g], r1 = s.rec1[g];
+        const float power = power_rn(r0, r1, __fsub_rn(r0.x, fx), __fsub_rn(r0.y, fy));
+        if (power > 0.0f) continue;
+        const float alpha = fmin_ref(0.99f, __fmul_rn(r1.y, exp_ref(power)));   // the forward's exact alpha
+        if (alpha < kAlphaMin) continue;
+        const float test_T = __fmul_rn(T, __fsub_rn(1.0f, alpha));
+        if (test_T < kTMin) break;
+        out[c++] = make_uint2(g, __float_as_uint(alpha));
+        T = test_T;
+    }
+}
+
+// RasterizerBackwardCPU::backward's back-to-front walk
+// (rasterizer_backward_cpu.cpp:69-133) over a pixel's stored list, with the
+// explicit image gradient d_image; nine atomics per (pixel, contributor).
+__global__ void __launch_bounds__(256) k_list_bwd(const StepParams* __restrict__ spp, ScreenPtrs s, PixelPtrs px,
+                                                  const int* __restrict__ offset, const uint2* __restrict__ list,
+                                                  RGradPtrs g) {
+    const StepParams& sp = *spp;
+    const int tile = blockIdx.x;
+    const int tx = tile % sp.grid_x, ty = tile / sp.grid_x;
+    const int x = tx * kTile + (int)(threadIdx.x & 15), y = ty * kTile + (int)(threadIdx.x >> 4);
+    if (x >= sp.cam.width || y >= sp.cam.height) return;
+    const size_t pix = (size_t)y * sp.cam.width + x;
+    const int n = px.n_contrib[pix];
+    if (n == 0) return;
+    const uint2* in = list + offset[pix];
+    const float dC[3] = {px.d_image[3 * pix], px.d_image[3 * pix + 1], px.d_image[3 * pix + 2]};
+    float T = px.T_final[pix];
+    float acc[3] = {sp.cfg.bg_color[0], sp.cfg.bg_color[1], sp.cfg.bg_color[2]};
+    for (int i = n - 1; i >= 0; i--) {
+        const unsigned gi = in[i].x;
+        const float alpha = __uint_as_float(in[i].y);
+        const float oma = 1.0f - alpha;
+        const float Ti = oma > 1e-6f ? T / oma : 0.0f;
+        const float4 r0 = s.rec0[gi], r1 = s.rec1[gi];
+        const float col[3] = {r1.z, r1.w, s.col_b[gi]};
+        const float dx = r0.x - (float)x, dy = r0.y - (float)y;
+        float d_alpha = 0.0f;
+#pragma unroll
+        for (int ch = 0; ch < 3; ch++) {
+            atomicAdd(&g.drgb[3 * (size_t)gi + ch], alpha * Ti * dC[ch]);
+            d_alpha += Ti * (col[ch] - acc[ch]) * dC[ch];
+            acc[ch] = alpha * col[ch] + oma * acc[ch];
+        }
+        T = Ti;
+        if (alpha < 0.99f) {
+            const float e = expf(-0.5f * (r0.z * dx * dx + r1.x * dy * dy) - r0.w * dx * dy);
+            const float d_power = d_alpha * r1.y * e;
+            atomicAdd(&g.dop[gi], d_alpha * e);
+            atomicAdd(&g.dm2[2 * (size_t)gi], d_power * (-r0.z * dx - r0.w * dy));
+            atomicAdd(&g.dm2[2 * (size_t)gi + 1], d_power * (-r1.x * dy - r0.w * dx));
+            atomicAdd(&g.dcon[3 * (size_t)gi], d_power * (-0.5f * dx * dx));
+            atomicAdd(&g.dcon[3 * (size_t)gi + 1], d_power * (-dx * dy));
+            atomicAdd(&g.dcon[3 * (size_t)gi + 2], d_power * (-0.5f * dy * dy));
+        }
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_list_fill(cudaStream_t st, const StepParams* sp, int num_tiles, const unsigned* ranges,
+                             const unsigned* vals, ScreenPtrs s, const int* n_contrib, const int* offset,
+                             uint2* list) {
+    if (num_tiles <= 0) return cudaSuccess;
+    k_list_fill<<<num_tiles, 256, 0, st>>>(sp, ranges, vals, s, n_contrib, offset, list);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_list_bwd(cudaStream_t st, const StepParams* sp, int num_tiles, ScreenPtrs s, PixelPtrs px,
+                            const int* offset, const uint2* list, RGradPtrs g) {
+    if (num_tiles <= 0) return cudaSuccess;
+    k_list_bwd<<<num_tiles, 256, 0, st>>>(sp, s, px, offset, list, g);
+    return cudaGetLastError();
+}
 
 namespace {
 

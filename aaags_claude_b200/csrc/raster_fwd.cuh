@@ -171,7 +171,8 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_fwd(const StepParams* __re
     for (int p = 0; p < PPT; p++) {
         const int y = ybase + 2 * p;
         if (x < W && y < H) {
-            const int pix = (int)sp.pix_base + y * W + x;
+            // 64-bit: a multi-view step holds up to 2^31 pixels, 3 floats each
+            const size_t pix = (size_t)sp.pix_base + (size_t)y * W + x;
             const float o0 = C[p][0] + T[p] * sp.cfg.bg_color[0];
             const float o1 = C[p][1] + T[p] * sp.cfg.bg_color[1];
             const float o2 = C[p][2] + T[p] * sp.cfg.bg_color[2];

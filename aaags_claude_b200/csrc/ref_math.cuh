@@ -318,24 +318,19 @@ struct BwdOut {
     float gp[3], gs[3], gq[4], gop, geff[3], basis[16];
 };
 
-// The whole per-Gaussian adjoint chain of PreprocessorBackwardCPU::backward
-// (preprocessor_backward_cpu.cpp:205-645) for a visible Gaussian, with the
-// forward quantities (activation, p_view, cov3D, cov2D, det, means2D)
-// recomputed bit-identically instead of read from a cache.
-__device__ __forceinline__ void backward_one(const StepParams& sp, const BwdIn& in, BwdOut& o) {
+// The view-dependent part of one Gaussian's adjoint of
+// PreprocessorBackwardCPU::backward (preprocessor_backward_cpu.cpp:205-645)
+// for one camera: the SH chain (:8-203) into o.geff, o.basis and the position;
+// then, when the recomputed 2D covariance is not degenerate, chains 1a-1b
+// (conic -> cov2D -> cov3D, :243-380) into dcov, path A (:536-597) and chain 4
+// (:609-643) into the position.  c3 is the forward's cov3D (cov3d of the
+// activated scale and rotation), sc / q the activated scale and rotation.
+// Returns false for det == 0, where the reference stops (dcov untouched).
+// Every output is linear in the screen gradients of `in`, so the gradients of
+// several cameras are the sums of their parts.
+__device__ __forceinline__ bool backward_view(const StepParams& sp, const float p[3], const float c3[6],
+                                              const float* shp, const BwdIn& in, BwdOut& o, float dcov[6]) {
     const gs3d_camera& cam = sp.cam;
-    const float* shp = in.sh;
-    const float* p = in.p;
-    float sc[3], q[4], op;
-    if (in.act) {
-#pragma unroll
-        for (int k = 0; k < 3; k++) sc[k] = in.act[k];
-#pragma unroll
-        for (int k = 0; k < 4; k++) q[k] = in.act[3 + k];
-        op = in.act[7];
-    } else {
-        activate_one(in.rsc, in.rq, in.rop, sc, q, &op);
-    }
     const int deg = sp.sh_deg_model;
     // ---- chain 2: SH (:8-203) ----
     float d[3];
@@ -416,11 +411,7 @@ __device__ __forceinline__ void backward_one(const StepParams& sp, const BwdIn& 
         o.gp[1] += (ddir1 - y * dot) * inv_len;
         o.gp[2] += (ddir2 - z * dot) * inv_len;
     }
-    // ---- chain 3: sigmoid (:231-232) ----
-    o.gop = in.dop * op * (1.0f - op);
     // ---- forward recompute (the ForwardCache of preprocessor_cpu.cpp:254-264) ----
-    float c3[6];
-    cov3d(sc, sp.cfg.scale_modifier, q, c3);
     Ewa e;
     ewa_setup(p, cam.view_matrix, sp.focal_x, sp.focal_y, cam.tan_fovx, cam.tan_fovy, e);
     float c2[3];
@@ -428,7 +419,7 @@ __device__ __forceinline__ void backward_one(const StepParams& sp, const BwdIn& 
     c2[0] += 0.3f;
     c2[2] += 0.3f;
     const float det = c2[0] * c2[2] - c2[1] * c2[1];
-    if (det == 0.0f) return;
+    if (det == 0.0f) return false;
     float ph[4];
     xform4x4(p, cam.viewproj_matrix, ph);
     // ---- chain 1a: conic -> cov2D (:243-306) ----
@@ -446,63 +437,12 @@ __device__ __forceinline__ void backward_one(const StepParams& sp, const BwdIn& 
 #pragma unroll
         for (int j = 0; j < 3; j++)
             dV[k][j] = d_a * e.T[0][k] * e.T[0][j] + d_b * e.T[0][k] * e.T[1][j] + d_c * e.T[1][k] * e.T[1][j];
-    const float dcov[6] = {dV[0][0], dV[0][1] + dV[1][0], dV[0][2] + dV[2][0],
-                           dV[1][1], dV[1][2] + dV[2][1], dV[2][2]};
-    // ---- chain 1c: cov3D -> M -> scale, R (:395-442) ----
-    const float mod = sp.cfg.scale_modifier;
-    const float sv[3] = {mod * sc[0], mod * sc[1], mod * sc[2]};
-    const float rr = q[0], xq = q[1], yq = q[2], zq = q[3];
-    float R[3][3], M[3][3];
-    quat_to_R(rr, xq, yq, zq, R);
-#pragma unroll
-    for (int ii = 0; ii < 3; ii++)
-#pragma unroll
-        for (int jj = 0; jj < 3; jj++) M[ii][jj] = sv[ii] * R[ii][jj];
-    float dR[3][3];
-#pragma unroll
-    for (int k = 0; k < 3; k++) {
-        const float dM0 = 2.0f * dcov[0] * M[k][0] + dcov[1] * M[k][1] + dcov[2] * M[k][2];
-        const float dM1 = dcov[1] * M[k][0] + 2.0f * dcov[3] * M[k][1] + dcov[4] * M[k][2];
-        const float dM2 = dcov[2] * M[k][0] + dcov[4] * M[k][1] + 2.0f * dcov[5] * M[k][2];
-        float ds = 0.0f;
-        ds += dM0 * R[k][0];
-        ds += dM1 * R[k][1];
-        ds += dM2 * R[k][2];
-        dR[k][0] = dM0 * sv[k];
-        dR[k][1] = dM1 * sv[k];
-        dR[k][2] = dM2 * sv[k];
-        o.gs[k] = ds * mod * sc[k];
-    }
-    // ---- d R -> d unit quaternion (:455-498) ----
-    float dq0 = 0.f, dq1 = 0.f, dq2 = 0.f, dq3 = 0.f;
-    dq2 += dR[0][0] * (-4.0f * yq);
-    dq3 += dR[0][0] * (-4.0f * zq);
-    dq0 += dR[0][1] * 2.0f * zq; dq1 += dR[0][1] * 2.0f * yq;
-    dq2 += dR[0][1] * 2.0f * xq; dq3 += dR[0][1] * 2.0f * rr;
-    dq0 += dR[0][2] * (-2.0f * yq); dq1 += dR[0][2] * 2.0f * zq;
-    dq2 += dR[0][2] * (-2.0f * rr); dq3 += dR[0][2] * 2.0f * xq;
-    dq0 += dR[1][0] * (-2.0f * zq); dq1 += dR[1][0] * 2.0f * yq;
-    dq2 += dR[1][0] * 2.0f * xq; dq3 += dR[1][0] * (-2.0f * rr);
-    dq1 += dR[1][1] * (-4.0f * xq);
-    dq3 += dR[1][1] * (-4.0f * zq);
-    dq0 += dR[1][2] * 2.0f * xq; dq1 += dR[1][2] * 2.0f * rr;
-    dq2 += dR[1][2] * 2.0f * zq; dq3 += dR[1][2] * 2.0f * yq;
-    dq0 += dR[2][0] * 2.0f * yq; dq1 += dR[2][0] * 2.0f * zq;
-    dq2 += dR[2][0] * 2.0f * rr; dq3 += dR[2][0] * 2.0f * xq;
-    dq0 += dR[2][1] * (-2.0f * xq); dq1 += dR[2][1] * (-2.0f * rr);
-    dq2 += dR[2][1] * 2.0f * zq; dq3 += dR[2][1] * 2.0f * yq;
-    dq1 += dR[2][2] * (-4.0f * xq);
-    dq2 += dR[2][2] * (-4.0f * yq);
-    // ---- normalisation backward (:503-519) ----
-    const float* rq = in.rq;
-    float qlen = sqrtf(rq[0] * rq[0] + rq[1] * rq[1] + rq[2] * rq[2] + rq[3] * rq[3]);
-    if (qlen < 1e-12f) qlen = 1e-12f;
-    const float il = 1.0f / qlen;
-    const float dot = dq0 * rr + dq1 * xq + dq2 * yq + dq3 * zq;
-    o.gq[0] = (dq0 - rr * dot) * il;
-    o.gq[1] = (dq1 - xq * dot) * il;
-    o.gq[2] = (dq2 - yq * dot) * il;
-    o.gq[3] = (dq3 - zq * dot) * il;
+    dcov[0] = dV[0][0];
+    dcov[1] = dV[0][1] + dV[1][0];
+    dcov[2] = dV[0][2] + dV[2][0];
+    dcov[3] = dV[1][1];
+    dcov[4] = dV[1][2] + dV[2][1];
+    dcov[5] = dV[2][2];
     // ---- path A: cov2D -> T -> J -> p_view -> position (:536-597) ----
     const float V[3][3] = {{c3[0], c3[1], c3[2]}, {c3[1], c3[3], c3[4]}, {c3[2], c3[4], c3[5]}};
     float VT[2][3];
@@ -565,6 +505,91 @@ __device__ __forceinline__ void backward_one(const StepParams& sp, const BwdIn& 
 #pragma unroll
     for (int dim = 0; dim < 3; dim++)
         o.gp[dim] += VP[dim * 4 + 0] * dph0 + VP[dim * 4 + 1] * dph1 + VP[dim * 4 + 2] * dph2 + VP[dim * 4 + 3] * dph3;
+    return true;
+}
+
+// The view-independent part: a cov3D gradient through M = S R (chain 1c,
+// :395-442) and the rotation matrix into the unit quaternion (:455-498), then
+// the quaternion normalisation (:503-519) against the raw quaternion rq, into
+// o.gs and o.gq.  mod = RenderConfig::scale_modifier.
+__device__ __forceinline__ void backward_cov3d(float mod, const float sc[3], const float q[4], const float rq[4],
+                                               const float dcov[6], BwdOut& o) {
+    // ---- chain 1c: cov3D -> M -> scale, R (:395-442) ----
+    const float sv[3] = {mod * sc[0], mod * sc[1], mod * sc[2]};
+    const float rr = q[0], xq = q[1], yq = q[2], zq = q[3];
+    float R[3][3], M[3][3];
+    quat_to_R(rr, xq, yq, zq, R);
+#pragma unroll
+    for (int ii = 0; ii < 3; ii++)
+#pragma unroll
+        for (int jj = 0; jj < 3; jj++) M[ii][jj] = sv[ii] * R[ii][jj];
+    float dR[3][3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const float dM0 = 2.0f * dcov[0] * M[k][0] + dcov[1] * M[k][1] + dcov[2] * M[k][2];
+        const float dM1 = dcov[1] * M[k][0] + 2.0f * dcov[3] * M[k][1] + dcov[4] * M[k][2];
+        const float dM2 = dcov[2] * M[k][0] + dcov[4] * M[k][1] + 2.0f * dcov[5] * M[k][2];
+        float ds = 0.0f;
+        ds += dM0 * R[k][0];
+        ds += dM1 * R[k][1];
+        ds += dM2 * R[k][2];
+        dR[k][0] = dM0 * sv[k];
+        dR[k][1] = dM1 * sv[k];
+        dR[k][2] = dM2 * sv[k];
+        o.gs[k] = ds * mod * sc[k];
+    }
+    // ---- d R -> d unit quaternion (:455-498) ----
+    float dq0 = 0.f, dq1 = 0.f, dq2 = 0.f, dq3 = 0.f;
+    dq2 += dR[0][0] * (-4.0f * yq);
+    dq3 += dR[0][0] * (-4.0f * zq);
+    dq0 += dR[0][1] * 2.0f * zq; dq1 += dR[0][1] * 2.0f * yq;
+    dq2 += dR[0][1] * 2.0f * xq; dq3 += dR[0][1] * 2.0f * rr;
+    dq0 += dR[0][2] * (-2.0f * yq); dq1 += dR[0][2] * 2.0f * zq;
+    dq2 += dR[0][2] * (-2.0f * rr); dq3 += dR[0][2] * 2.0f * xq;
+    dq0 += dR[1][0] * (-2.0f * zq); dq1 += dR[1][0] * 2.0f * yq;
+    dq2 += dR[1][0] * 2.0f * xq; dq3 += dR[1][0] * (-2.0f * rr);
+    dq1 += dR[1][1] * (-4.0f * xq);
+    dq3 += dR[1][1] * (-4.0f * zq);
+    dq0 += dR[1][2] * 2.0f * xq; dq1 += dR[1][2] * 2.0f * rr;
+    dq2 += dR[1][2] * 2.0f * zq; dq3 += dR[1][2] * 2.0f * yq;
+    dq0 += dR[2][0] * 2.0f * yq; dq1 += dR[2][0] * 2.0f * zq;
+    dq2 += dR[2][0] * 2.0f * rr; dq3 += dR[2][0] * 2.0f * xq;
+    dq0 += dR[2][1] * (-2.0f * xq); dq1 += dR[2][1] * (-2.0f * rr);
+    dq2 += dR[2][1] * 2.0f * zq; dq3 += dR[2][1] * 2.0f * yq;
+    dq1 += dR[2][2] * (-4.0f * xq);
+    dq2 += dR[2][2] * (-4.0f * yq);
+    // ---- normalisation backward (:503-519) ----
+    float qlen = sqrtf(rq[0] * rq[0] + rq[1] * rq[1] + rq[2] * rq[2] + rq[3] * rq[3]);
+    if (qlen < 1e-12f) qlen = 1e-12f;
+    const float il = 1.0f / qlen;
+    const float dot = dq0 * rr + dq1 * xq + dq2 * yq + dq3 * zq;
+    o.gq[0] = (dq0 - rr * dot) * il;
+    o.gq[1] = (dq1 - xq * dot) * il;
+    o.gq[2] = (dq2 - yq * dot) * il;
+    o.gq[3] = (dq3 - zq * dot) * il;
+}
+
+// The whole per-Gaussian adjoint chain of PreprocessorBackwardCPU::backward
+// (preprocessor_backward_cpu.cpp:205-645) for a visible Gaussian, with the
+// forward quantities (activation, p_view, cov3D, cov2D, det, means2D)
+// recomputed bit-identically instead of read from a cache.
+__device__ __forceinline__ void backward_one(const StepParams& sp, const BwdIn& in, BwdOut& o) {
+    float sc[3], q[4], op;
+    if (in.act) {
+#pragma unroll
+        for (int k = 0; k < 3; k++) sc[k] = in.act[k];
+#pragma unroll
+        for (int k = 0; k < 4; k++) q[k] = in.act[3 + k];
+        op = in.act[7];
+    } else {
+        activate_one(in.rsc, in.rq, in.rop, sc, q, &op);
+    }
+    // ---- chain 3: sigmoid (:231-232) ----
+    o.gop = in.dop * op * (1.0f - op);
+    float c3[6];
+    cov3d(sc, sp.cfg.scale_modifier, q, c3);
+    float dcov[6];
+    if (backward_view(sp, in.p, c3, in.sh, in, o, dcov)) backward_cov3d(sp.cfg.scale_modifier, sc, q, in.rq, dcov, o);
 }
 
 

@@ -28,6 +28,7 @@ NUM_STAGES = 8
 STAT_TOTAL_PAIRS, STAT_PAIR_CAPACITY, STAT_KERNELS_LAST, STAT_SORT_PASSES, STAT_GRAPH_REPLAYS, STAT_ADAM_STEP = range(1, 7)
 STAT_NUM_GAUSSIANS = 9
 STAT_SCREEN_GAUSSIANS = 10
+STAT_GRAPH_CAPTURES = 11
 STAT_FWD_PPT, STAT_BWD_PPT = 7, 8
 FORM_PLAIN_FP32, FORM_BF16, FORM_FP16 = 0, 1, 2
 OPT_SORT = 7
@@ -88,6 +89,8 @@ def load_library(path: str = LIB_PATH):
         "gs3dc_preprocess_backward": ([vp, vp, vp, vp, vp, vp, vp, vp, vp], ctypes.c_int),
         "gs3dc_update_raw_params": ([vp, vp], ctypes.c_int),
         "gs3dc_get_image": ([vp, vp], ctypes.c_int),
+        "gs3dc_raster_backward_lists": ([vp, vp, vp, vp, vp, vp, vp, vp, ctypes.POINTER(i64)], ctypes.c_int),
+        "gs3dc_get_batch_image": ([vp, ctypes.c_int, vp], ctypes.c_int),
         "gs3dc_optimizer_step": ([vp, vp, ctypes.c_int], ctypes.c_int),
         "gs3dc_train_step": ([vp, vp, vp, ctypes.c_int, vp, vp, ctypes.c_int, vp], ctypes.c_int),
         "gs3dc_synchronize": ([vp], ctypes.c_int),
@@ -459,6 +462,18 @@ class Context:
                                                _p(out["d_conics"]), _p(out["d_rgb"]), _p(out["d_opac"])))
         return out
 
+    def raster_backward_lists(self, cam, cfg, d_image: np.ndarray) -> tuple[dict, int]:
+        """raster_backward with stored per-pixel contributor lists; returns (gradients, list bytes)."""
+        n = self.stat(STAT_SCREEN_GAUSSIANS)
+        out = dict(d_means2D=np.zeros(2 * n, np.float32), d_conics=np.zeros(3 * n, np.float32),
+                   d_rgb=np.zeros(3 * n, np.float32), d_opac=np.zeros(n, np.float32))
+        d = np.ascontiguousarray(d_image, np.float32).reshape(-1)
+        nb = ctypes.c_int64()
+        self._chk(self.L.gs3dc_raster_backward_lists(self.h, _ref(cam), _ref(cfg), _p(d), _p(out["d_means2D"]),
+                                                     _p(out["d_conics"]), _p(out["d_rgb"]), _p(out["d_opac"]),
+                                                     ctypes.byref(nb)))
+        return out, int(nb.value)
+
     def preprocess_backward(self, cam, cfg, raw_rotations: np.ndarray | None = None) -> dict:
         """PreprocessorBackward; raw_rotations is needed when the device model is activated."""
         n, mc = self._model[1], self._model[2]
@@ -549,6 +564,12 @@ class Context:
     def get_image(self, cam) -> np.ndarray:
         img = np.zeros(3 * cam.width * cam.height, np.float32)
         self._chk(self.L.gs3dc_get_image(self.h, _p(img)))
+        return img
+
+    def get_batch_image(self, view: int, cam) -> np.ndarray:
+        """View `view`'s image (H*W*3) of the last multi-view step; cam = that view's camera."""
+        img = np.zeros(3 * cam.width * cam.height, np.float32)
+        self._chk(self.L.gs3dc_get_batch_image(self.h, int(view), _p(img)))
         return img
 
     def optimizer_step(self, tcfg, iteration: int):

@@ -569,12 +569,18 @@ def measure_batched(a, local: int) -> dict:
         batched(k)
     ctx.synchronize()
     ppt_b = {"forward": ctx.stat(gs3d.STAT_FWD_PPT), "backward": ctx.stat(gs3d.STAT_BWD_PPT)}
+
+    def graph_stats():
+        return ctx.stat(gs3d.STAT_GRAPH_REPLAYS), ctx.stat(gs3d.STAT_GRAPH_CAPTURES)
+    g0 = graph_stats()
     ms_b = timed(batched)
+    g1 = graph_stats()
     loss_b = ctx.train_step_batch(cams, None, cfg, tc, it[0], gt_device_ptr=gt_dev.data_ptr())
     launches_b = ctx.stat(gs3d.STAT_KERNELS_LAST)
 
-    # the plain FP32 path, the same views one by one (one optimiser step per view, fixed 2 pixels per thread)
-    ctx.set_option(gs3d.OPT_AUTOTUNE, 0)
+    # the plain FP32 path, the same views one by one (one optimiser step per view), with the same
+    # autotuner setting; every camera size keeps its own graphs, so the timed passes only replay
+    ctx.set_option(gs3d.OPT_AUTOTUNE, a.autotune)
     ctx.set_option(gs3d.OPT_FORM, gs3d.FORM_PLAIN_FP32)
     ctx.set_raw_params(w.scene)
 
@@ -583,17 +589,25 @@ def measure_batched(a, local: int) -> dict:
             ctx.train_step(cam, None, cfg, tc, it[0], want_loss=False,
                            gt_device_ptr=gt_dev.data_ptr() + 4 * int(offs[v]))
             it[0] += 1
-    one_by_one(0)
+    for k in range(3):   # each size's first step, the autotuner's 6 trial steps per size, graph captures
+        one_by_one(k)
     ctx.synchronize()
+    p0 = graph_stats()
     ms_p = timed(one_by_one)
+    p1 = graph_stats()
     ctx.close()
     return {"workload": "batched_64views_1M_gaussians_mixed_320x240_to_3840x2160", "views": len(cams),
             "mpix_per_step": round(pix / 1e6, 2), "steps": steps,
             "batched_bf16": {"ms_per_step": round(ms_b, 3), "mpix_per_s": round(pix / 1e6 / (ms_b * 1e-3), 1),
                              "gpu_launches_per_step": launches_b, "loss_first": loss0, "loss_last": loss_b,
-                             "raster_pixels_per_thread": ppt_b},
+                             "raster_pixels_per_thread": ppt_b,
+                             "graph_replays_per_step": (g1[0] - g0[0]) / steps,
+                             "graph_captures_in_timed_steps": g1[1] - g0[1]},
             "plain_fp32_one_by_one": {"ms_per_64_views": round(ms_p, 3),
-                                      "mpix_per_s": round(pix / 1e6 / (ms_p * 1e-3), 1)},
+                                      "mpix_per_s": round(pix / 1e6 / (ms_p * 1e-3), 1),
+                                      "autotuned": bool(a.autotune),
+                                      "graph_replays_per_64_views": (p1[0] - p0[0]) / steps,
+                                      "graph_captures_in_timed_passes": p1[1] - p0[1]},
             "mpix_ratio": round(ms_p / ms_b, 3)}
 
 

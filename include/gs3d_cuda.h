@@ -76,13 +76,15 @@ typedef struct gs3dc_ctx gs3dc_ctx;
 #define GS3DC_STAT_PAIR_CAPACITY  2
 #define GS3DC_STAT_KERNELS_LAST   3  /* kernels launched by the last train step / render */
 #define GS3DC_STAT_SORT_PASSES    4  /* radix passes of the last sort */
-#define GS3DC_STAT_GRAPH_REPLAYS  5
+#define GS3DC_STAT_GRAPH_REPLAYS  5  /* train steps replayed from a captured graph */
 #define GS3DC_STAT_ADAM_STEP      6  /* Adam step counter (AdamOptimizer::step_count) */
 #define GS3DC_STAT_FWD_PPT        7  /* pixels per thread of the forward rasteriser in the last train step */
 #define GS3DC_STAT_BWD_PPT        8  /* pixels per thread of the backward rasteriser in the last train step */
 #define GS3DC_STAT_NUM_GAUSSIANS  9  /* Gaussians of the device model (changes with density control) */
 #define GS3DC_STAT_SCREEN_GAUSSIANS 10 /* Gaussians of the current screen records (the model's, or those of
                                           gs3dc_rasterize_arrays): the length of the raster gradients */
+#define GS3DC_STAT_GRAPH_CAPTURES 11 /* train-step graphs captured (one per workload shape that repeats;
+                                        the single-view step keeps the graphs of up to 8 shapes) */
 
 /* Host arrays of PreprocessOutput + the per-Gaussian ForwardCache fields
  * (include/types.h:69-82, 97-107).  Any pointer may be NULL (not produced). */
@@ -226,6 +228,18 @@ int gs3dc_raster_backward(gs3dc_ctx* ctx, const gs3d_camera* cam, const gs3d_ren
                           const float* d_image, float* d_means2D, float* d_conics, float* d_rgb,
                           float* d_opacities_2d);
 
+/* The same backward with the reference's stored per-pixel contributor lists
+ * (src/cpu/rasterizer_backward_cpu.cpp:40-67: the forward replayed into a list
+ * of (Gaussian, alpha) per pixel, walked back to front), kept to measure what
+ * the lists cost against gs3dc_raster_backward, which recovers transmittance
+ * by division and keeps no list.  The lists live in one device buffer of
+ * sum(n_contrib) entries of 8 bytes plus a 4-byte offset per pixel;
+ * *list_bytes (may be NULL) receives that size.  Outputs as
+ * gs3dc_raster_backward. */
+int gs3dc_raster_backward_lists(gs3dc_ctx* ctx, const gs3d_camera* cam, const gs3d_render_config* cfg,
+                                const float* d_image, float* d_means2D, float* d_conics, float* d_rgb,
+                                float* d_opacities_2d, int64_t* list_bytes);
+
 /* PreprocessorBackwardCPU::backward (src/cpu/preprocessor_backward_cpu.h:7-10;
  *   src/cpu/preprocessor_backward_cpu.cpp:205-645) from the last raster
  *   backward.  With a raw device model the activation is recomputed; with an
@@ -245,6 +259,11 @@ int gs3dc_optimizer_step(gs3dc_ctx* ctx, const gs3d_train_config* tc, int iterat
 /* Trainer::step (include/trainer.h:21-23; src/trainer.cpp:7-70) with the
  *   parameters resident on the device: activate, forward, L1 loss, backward,
  *   optimiser, fused into a few kernels and replayed as one CUDA graph.
+ *   Graphs are kept per workload shape (camera size, model size, form;
+ *   up to 8 shapes, least recently used replaced), so a caller cycling through
+ *   cameras of several sizes replays each size's graph.  A shape's first step
+ *   runs un-captured and waits for the device (a pair-capacity overflow is
+ *   redone at once).
  *   gt is H*W*3 HWC; gt_on_device != 0 means it is a device pointer.
  *   loss (may be NULL) receives the mean absolute error; a NULL loss also lets
  *   the call return without waiting for the device (the next call, or
@@ -267,6 +286,11 @@ int gs3dc_train_step(gs3dc_ctx* ctx, const gs3d_camera* cam, const float* gt, in
 int gs3dc_train_step_batch(gs3dc_ctx* ctx, int n_views, const gs3d_camera* cams, const float* gt,
                            int gt_on_device, const gs3d_render_config* cfg,
                            const gs3d_train_config* tc, int iteration, float* loss);
+
+/* The forward image of view `view` (H*W*3 HWC, that view's camera size) of the
+ * last gs3dc_train_step_batch: Trainer::step's rendered image (last_rendered_,
+ * src/trainer.cpp:46-48) for each of the step's cameras.  Synchronous. */
+int gs3dc_get_batch_image(gs3dc_ctx* ctx, int view, float* image);
 
 /* Device time per stage of the last train step run with GS3DC_OPT_STAGE_TIMING,
  * measured with CUDA events on the context's stream.  ms[k] for k < n_stages,

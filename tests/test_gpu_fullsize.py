@@ -1,8 +1,12 @@
 """GPU: the training workload at full size (1M Gaussians, 1920x1080).
 
 Bit-exact against the oracle at full size for the integer outputs (the C
-oracle runs the same forward in ~10 s), plus size-independent properties:
-sortedness and stability, range coverage, idempotence, loss decrease.
+oracle runs the same forward in ~10 s); the plain form's raw-parameter
+gradients of one Trainer::step against the oracle's (the reference's
+rasterizer_backward_cpu.cpp:20-133 and preprocessor_backward_cpu.cpp:205-645
+restated) within |cuda - ref| <= 1e-4 |ref| + 1e-5 max|ref| elementwise and
+cosine >= 0.999; plus size-independent properties: sortedness and
+stability, range coverage, idempotence, loss decrease.
 """
 import numpy as np
 import pytest
@@ -61,6 +65,31 @@ def test_fullsize_sort_properties(ctx, full):
     nonempty = end > start
     assert np.all(tiles[start[nonempty]] == np.nonzero(nonempty)[0])
     assert np.all(tiles[end[nonempty] - 1] == np.nonzero(nonempty)[0])
+
+
+def test_fullsize_plain_gradients_match_the_oracle(ctx, full):
+    w, act, cam, cfg, _ = full
+    ctx.set_raw_params(w.target_scene)
+    gt = ctx.render(cam, S.render_config(False))
+    tc = S.train_config()
+    ref_scene = w.scene.copy()
+    ref = O.train_step(ref_scene, cam, gt, cfg, tc, 0, O.AdamOracle(ref_scene.count, ref_scene.max_coeffs * 3), "c",
+                       cap=12_000_000)
+    ctx.set_option(gs3d.OPT_KEEP_GRADIENTS, 1)
+    try:
+        ctx.set_raw_params(w.scene)
+        loss = ctx.train_step(cam, gt, cfg, tc, 0)
+        g = ctx.get_gradients()
+    finally:
+        ctx.set_option(gs3d.OPT_KEEP_GRADIENTS, 0)
+    assert abs(loss - ref.loss_acc64) <= 1e-6 * ref.loss_acc64, (loss, ref.loss_acc64)
+    for k, rk in (("pos", "g_pos"), ("sc", "g_sc"), ("rot", "g_rot"), ("sh", "g_sh"), ("op", "g_op")):
+        r = getattr(ref, rk)
+        ok, worst = U.rel_close(g[k], r, 1e-4, 1e-5)
+        cos = U.cosine(g[k], r)
+        print(f"{k}: worst |cuda - ref| / tolerance {worst:.3f}, cosine {cos:.8f}")
+        assert ok, (k, worst)
+        assert cos >= 0.999, (k, cos)
 
 
 def test_fullsize_training_decreases_loss(ctx, full):
