@@ -218,6 +218,7 @@ struct gs3dc_ctx {
         unsigned long long used = 0;   // LRU clock (single-view shapes)
     };
     bool autotune = false;
+    int forced_ppt = 0;   // GS3DC_OPT_RASTER_PPT
     Tune tune_single[kShapeSlots], tune_batch;
     unsigned long long tclock = 0;
     cudaEvent_t tune_ev[3] = {};
@@ -589,6 +590,10 @@ int read_control(gs3dc_ctx* c) {
 // The pixels per thread of this step: the tuned values, or the next
 // candidate while the workload shape is being tuned (returns true then).
 bool tune_begin(gs3dc_ctx* c, gs3dc_ctx::Tune& t, const long long key[6]) {
+    if (c->forced_ppt) {
+        c->fwd_ppt = c->bwd_ppt = c->forced_ppt;
+        return false;
+    }
     if (!c->autotune) {
         c->fwd_ppt = c->bwd_ppt = 2;
         return false;
@@ -1041,9 +1046,10 @@ int seq_batch(gs3dc_ctx* c, const BatchShape& sh) {
     dk.views24 = true;
     CK(launch_chosen_preprocess(c->stream, views, c->N, c->form == GS3DC_FORM_FP16, chosen_ptrs(c), batch_screen(c),
                                 dk, b.rects.p, c->ctrl, sh.V));
-    // 32-bit keys: digits 0..2 the depth's upper 24 bits (as the single-view reduced form), digit 3 the view
+    // 32-bit keys: digits 0..2 the depth's upper 24 bits (as the single-view reduced form), digit 3 the view;
+    // the preprocess counted their digit histograms into control slots 0..3
     int dw = 0;
-    CK(launch_radix_sort32(c->stream, views, 4, 0, false, vn, b.dkeys[0].p, b.dvals[0].p, b.dkeys[1].p, b.dvals[1].p,
+    CK(launch_radix_sort32(c->stream, views, 4, 0, true, vn, b.dkeys[0].p, b.dvals[0].p, b.dkeys[1].p, b.dvals[1].p,
                            b.ddesc.p, dstride, c->ctrl, &dw, nullptr, &c->ctrl->gauss_keys, 0));
     PairPtrs pr{nullptr, b.vals[0].p, b.cap, c->scan_desc, b.keys[0].p};
     CK(launch_emit_ranked(c->stream, views, (int)vn, b.dvals[dw].p, batch_screen(c), pr, c->ctrl, b.rects.p, c->N,
@@ -1053,7 +1059,7 @@ int seq_batch(gs3dc_ctx* c, const BatchShape& sh) {
                            b.vals[1].p, b.sort_desc.p, pstride, c->ctrl, &which));
     CK(launch_tile_ranges_views(c->stream, b.cap, b.keys[which].p, b.vals[which].p, views, c->N, b.ranges.p,
                                 c->ctrl));
-    CK(launch_tile_order(c->stream, b.ranges.p, (int)sh.tiles, b.order.p));
+    CK(launch_tile_order(c->stream, b.ranges.p, (int)sh.tiles, b.order.p, c->ctrl));
     const bool tuning = c->autotune && !c->tune_batch.done;
     if (tuning) CK(cudaEventRecord(c->tune_ev[0], c->stream));
     CK(launch_raster_fwd_fast_multi(c->stream, views, sh.V, sh.tiles, b.ranges.p, b.order.p, b.vals[which].p,
@@ -1066,7 +1072,8 @@ int seq_batch(gs3dc_ctx* c, const BatchShape& sh) {
                                    chosen_ptrs(c), batch_rgrads(c),
                                    c->keep_grads ? grad_ptrs(c) : GradPtrs{nullptr, nullptr, nullptr, nullptr, nullptr},
                                    c->ctrl, sh.V));
-    c->kernels_last = 1 + 1 + 4 + 1 + (sh.tile_digits > 0 ? sh.tile_digits : 0) + 2 + 3;
+    // preprocess, 4 depth passes, emission, tile passes, ranges + order, rasterisers, adjoint
+    c->kernels_last = 1 + 4 + 1 + (sh.tile_digits > 0 ? sh.tile_digits : 0) + 2 + 3;
     return GS3DC_OK;
 }
 
@@ -1236,6 +1243,11 @@ int gs3dc_set_option(gs3dc_ctx* c, int option, int64_t value) {
             for (auto& t : c->tune_single) t = gs3dc_ctx::Tune();
             c->tune_batch = gs3dc_ctx::Tune();
             drop_graphs(c);
+            return GS3DC_OK;
+        case GS3DC_OPT_RASTER_PPT:
+            if (value != 0 && value != 1 && value != 2 && value != 4)
+                return fail(c, GS3DC_ERR_INVALID_ARG, "pixels per thread %lld: 0, 1, 2 or 4", (long long)value);
+            c->forced_ppt = (int)value;
             return GS3DC_OK;
         case GS3DC_OPT_KEEP_GRADIENTS:
             c->keep_grads = value != 0;

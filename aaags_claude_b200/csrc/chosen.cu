@@ -148,34 +148,13 @@ __device__ __forceinline__ void load_attr(const void* attr, long long i, float r
 
 // ---- preprocess ----
 
-template <typename S>
-__global__ void __launch_bounds__(kBlock) k_chosen_preprocess(const StepParams* __restrict__ spp, int N, ChosenPtrs c,
-                                                              ScreenPtrs s, DepthKeys dk, uint2* __restrict__ rects,
-                                                              Control* ctrl) {
-    // several views: blockIdx.y is the view, entries are view * N + i
-    const int view = blockIdx.y;
-    const StepParams& sp = spp[view];
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i == 0 && view == 0) ctrl->gauss_keys = (unsigned long long)N * gridDim.y;
-    if (i >= N) return;
-    const long long o = (long long)view * N + i;   // output entry
-    const int mc3 = sp.max_coeffs * 3;
-    const float p[3] = {c.pos[3 * i], c.pos[3 * i + 1], c.pos[3 * i + 2]};
-    float rsc[3], rq[4], rop, sc[3], q[4], op;
-    load_attr<S>(c.attr, i, rsc, &rop, rq);
-    activate_one(rsc, rq, rop, sc, q, &op);
-    Proj r;
-    const S* shrow = static_cast<const S*>(c.sh) + (size_t)mc3 * i;
-    bool vis;
-    if (mc3 == 48) {
-        // degree-3 storage: the 96-byte row (16-byte aligned) as six 16-byte loads
-        uint4 shv[6];
-#pragma unroll
-        for (int k = 0; k < 6; k++) shv[k] = reinterpret_cast<const uint4*>(shrow)[k];
-        vis = project_one<S>(sp, p, sc, q, op, reinterpret_cast<const S*>(shv), r);
-    } else {
-        vis = project_one<S>(sp, p, sc, q, op, shrow, r);
-    }
+// One camera's screen record of a projected Gaussian (r from project_one) at
+// entry o: the FP64 inverse of a near-degenerate 2D covariance, the reference's
+// tile rectangle cut to the box of the alpha >= 1/255 ellipse, the record,
+// depth, radius, tile count and rectangle.  Returns the depth bits for the
+// depth sort, 0xFFFFFFFF for a Gaussian without pairs.
+__device__ __forceinline__ unsigned chosen_record(const StepParams& sp, bool vis, Proj& r, long long o, ScreenPtrs s,
+                                                  uint2* __restrict__ rects) {
     int cnt = 0;
     uint2 rect = make_uint2(0u, 0u);
     unsigned dbits = 0xFFFFFFFFu;
@@ -220,9 +199,97 @@ __global__ void __launch_bounds__(kBlock) k_chosen_preprocess(const StepParams* 
     }
     s.tiles[o] = cnt;
     rects[o] = rect;
-    const unsigned key = cnt > 0 ? dbits : 0xFFFFFFFFu;
-    dk.keys[o] = dk.views24 ? ((unsigned)view << 24) | (key >> 8) : key;
-    dk.vals[o] = (unsigned)o;
+    return cnt > 0 ? dbits : 0xFFFFFFFFu;
+}
+
+template <typename S>
+__global__ void __launch_bounds__(kBlock) k_chosen_preprocess(const StepParams* __restrict__ spp, int N, ChosenPtrs c,
+                                                              ScreenPtrs s, DepthKeys dk, uint2* __restrict__ rects,
+                                                              Control* ctrl) {
+    const StepParams& sp = *spp;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) ctrl->gauss_keys = (unsigned long long)N;
+    if (i >= N) return;
+    const int mc3 = sp.max_coeffs * 3;
+    const float p[3] = {c.pos[3 * i], c.pos[3 * i + 1], c.pos[3 * i + 2]};
+    float rsc[3], rq[4], rop, sc[3], q[4], op;
+    load_attr<S>(c.attr, i, rsc, &rop, rq);
+    activate_one(rsc, rq, rop, sc, q, &op);
+    Proj r;
+    const S* shrow = static_cast<const S*>(c.sh) + (size_t)mc3 * i;
+    bool vis;
+    if (mc3 == 48) {
+        // degree-3 storage: the 96-byte row (16-byte aligned) as six 16-byte loads
+        uint4 shv[6];
+#pragma unroll
+        for (int k = 0; k < 6; k++) shv[k] = reinterpret_cast<const uint4*>(shrow)[k];
+        vis = project_one<S>(sp, p, sc, q, op, reinterpret_cast<const S*>(shv), r);
+    } else {
+        vis = project_one<S>(sp, p, sc, q, op, shrow, r);
+    }
+    dk.keys[i] = chosen_record(sp, vis, r, i, s, rects);
+    dk.vals[i] = (unsigned)i;
+}
+
+// Several views: one thread per Gaussian loads, activates and forms the cov3D
+// once and projects it into every view (entries view * N + i), writing the
+// 32-bit (view, depth's upper 24 bits) keys of the depth sort and their
+// digit histograms: digits 0..2 (the depth bits 8..31) counted per CTA in
+// shared memory, one global atomic per CTA and bin; digit 3 (the view) has N
+// keys per view.  The sort then needs no histogram pass.
+template <typename S>
+__global__ void __launch_bounds__(kBlock) k_chosen_preprocess_views(const StepParams* __restrict__ spp, int N,
+                                                                    int n_views, ChosenPtrs c, ScreenPtrs s,
+                                                                    DepthKeys dk, uint2* __restrict__ rects,
+                                                                    Control* ctrl) {
+    __shared__ unsigned s_hist[3][256];
+    for (int e = threadIdx.x; e < 3 * 256; e += kBlock) (&s_hist[0][0])[e] = 0u;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) {
+        ctrl->gauss_keys = (unsigned long long)N * n_views;
+        for (int v = 0; v < n_views; v++) atomicAdd(&ctrl->hist[3][v], (unsigned)N);
+    }
+    __syncthreads();
+    const bool valid = i < N;
+    const int mc3 = spp[0].max_coeffs * 3;
+    const int gi = valid ? i : 0;   // threads past the end project Gaussian 0 and write nothing
+    const float p[3] = {c.pos[3 * gi], c.pos[3 * gi + 1], c.pos[3 * gi + 2]};
+    float rsc[3], rq[4], rop, sc[3], q[4], op, c3[6];
+    load_attr<S>(c.attr, gi, rsc, &rop, rq);
+    activate_one(rsc, rq, rop, sc, q, &op);
+    cov3d(sc, spp[0].cfg.scale_modifier, q, c3);
+    const S* shrow = static_cast<const S*>(c.sh) + (size_t)mc3 * gi;
+    uint4 shv[6];
+    if (mc3 == 48) {
+#pragma unroll
+        for (int k = 0; k < 6; k++) shv[k] = reinterpret_cast<const uint4*>(shrow)[k];
+    }
+    const unsigned lane = threadIdx.x & 31;
+    for (int v = 0; v < n_views; v++) {
+        const StepParams& sp = spp[v];
+        unsigned key = 0u;
+        if (valid) {
+            const long long o = (long long)v * N + i;
+            Proj r;
+            const bool vis = mc3 == 48 ? project_one<S>(sp, p, sc, q, op, reinterpret_cast<const S*>(shv), r, c3)
+                                       : project_one<S>(sp, p, sc, q, op, shrow, r, c3);
+            key = ((unsigned)v << 24) | (chosen_record(sp, vis, r, o, s, rects) >> 8);
+            dk.keys[o] = key;
+            dk.vals[o] = (unsigned)o;
+        }
+        // warp-aggregated digit counts (the upper depth digits are shared by most of a warp)
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            const unsigned dg = valid ? (key >> (8 * d)) & 255u : 256u;
+            const unsigned peers = __match_any_sync(0xffffffffu, dg);
+            if (valid && lane == (unsigned)(__ffs(peers) - 1)) atomicAdd(&s_hist[d][dg], (unsigned)__popc(peers));
+        }
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < 3 * 256; e += kBlock) {
+        const unsigned n = (&s_hist[0][0])[e];
+        if (n) atomicAdd(&ctrl->hist[e >> 8][e & 255], n);
+    }
 }
 
 // ---- optimiser helpers ----
@@ -265,7 +332,10 @@ __device__ __forceinline__ void opt8(const StepParams& sp, uint4& p, uint4& m, u
 // ---- adjoint (staged, coalesced) ----
 
 constexpr int kCB = 64;           // Gaussians (= threads) per CTA of the adjoint
-constexpr int kShPitch = 49;      // padded row of the per-Gaussian SH gradients in shared memory
+// Row of one Gaussian's SH gradients in shared memory (several views): 52 floats, so that a thread
+// updates its row with 16-byte accesses and the 8 threads of each 16-byte phase hit distinct banks
+// (13 t mod 8 differs for t = 0..7).
+constexpr int kShPitch = 52;
 
 // One view: the SH gradient of coefficient k is basis[k / 3] * geff[k % 3], so the
 // CTA keeps the 16 + 3 factors per Gaussian (SoA, conflict-free) instead of the
@@ -277,7 +347,7 @@ struct __align__(16) ChosenBwdShared {
     float pos[3 * kCB];
     float dm2[2 * kCB], dcon[3 * kCB], drgb[3 * kCB], dop[kCB];
     float g_pos[3 * kCB], g_sc[3 * kCB], g_rot[4 * kCB], g_op[kCB];
-    float g_sh[MULTI ? kShPitch * kCB : 1];
+    alignas(16) float g_sh[MULTI ? kShPitch * kCB : 4];
     float basis[MULTI ? 1 : 16 * kCB];   // [basis][Gaussian]
     float geff[MULTI ? 1 : 3 * kCB];     // [channel][Gaussian]
     unsigned long long bar;       // completion of the bulk copies into the arrays above
@@ -370,9 +440,10 @@ __global__ void __launch_bounds__(kCB, MULTI ? 8 : 10) k_chosen_backward(const S
             activate_one(rsc, rq, rop, sc, q, &op);
             const float mod = sp.cfg.scale_modifier;
             cov3d(sc, mod, q, c3);
+            float4* const shrow4 = reinterpret_cast<float4*>(&sm.g_sh[kShPitch * tid]);
 #pragma unroll
-            for (int k = 0; k < 48; k++)
-                if (k < mc3) sm.g_sh[kShPitch * tid + k] = 0.f;
+            for (int q4 = 0; q4 < 12; q4++)
+                if (4 * q4 < mc3) shrow4[q4] = make_float4(0.f, 0.f, 0.f, 0.f);
             float gp[3] = {0.f, 0.f, 0.f}, dcs[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, dops = 0.f;
             float nx[9];
             auto load_view = [&](long long e, float d[9]) {
@@ -439,9 +510,18 @@ __global__ void __launch_bounds__(kCB, MULTI ? 8 : 10) k_chosen_backward(const S
 #pragma unroll
                 for (int k = 0; k < 3; k++) gp[k] += o.gp[k];
                 dops += cur[8];
+                // SH gradient of coefficient k (basis k / 3, channel k % 3), four at a time
 #pragma unroll
-                for (int k = 0; k < 48; k++)
-                    if (k < mc3) sm.g_sh[kShPitch * tid + k] += o.basis[k / 3] * o.geff[k % 3];
+                for (int q4 = 0; q4 < 12; q4++) {
+                    if (4 * q4 < mc3) {
+                        float4 v4 = shrow4[q4];
+                        v4.x += o.basis[(4 * q4) / 3] * o.geff[(4 * q4) % 3];
+                        v4.y += o.basis[(4 * q4 + 1) / 3] * o.geff[(4 * q4 + 1) % 3];
+                        v4.z += o.basis[(4 * q4 + 2) / 3] * o.geff[(4 * q4 + 2) % 3];
+                        v4.w += o.basis[(4 * q4 + 3) / 3] * o.geff[(4 * q4 + 3) % 3];
+                        shrow4[q4] = v4;
+                    }
+                }
             }
             BwdOut o;
             backward_cov3d(mod, sc, q, rq, dcs, o);
@@ -633,9 +713,15 @@ cudaError_t launch_chosen_to_raw(cudaStream_t st, int N, int mc3, bool fp16, Cho
 cudaError_t launch_chosen_preprocess(cudaStream_t st, const StepParams* sp, int N, bool fp16, ChosenPtrs c,
                                      ScreenPtrs s, DepthKeys dk, uint2* rects, Control* ctrl, int n_views) {
     if (N <= 0 || n_views <= 0) return cudaSuccess;
-    const dim3 grid((unsigned)grid_for(N, kBlock), (unsigned)n_views);
-    if (fp16) k_chosen_preprocess<__half><<<grid, kBlock, 0, st>>>(sp, N, c, s, dk, rects, ctrl);
-    else k_chosen_preprocess<__nv_bfloat16><<<grid, kBlock, 0, st>>>(sp, N, c, s, dk, rects, ctrl);
+    const int grid = grid_for(N, kBlock);
+    if (n_views > 1 || dk.views24) {
+        if (!dk.views24) return cudaErrorInvalidValue;
+        if (fp16) k_chosen_preprocess_views<__half><<<grid, kBlock, 0, st>>>(sp, N, n_views, c, s, dk, rects, ctrl);
+        else k_chosen_preprocess_views<__nv_bfloat16><<<grid, kBlock, 0, st>>>(sp, N, n_views, c, s, dk, rects, ctrl);
+    } else {
+        if (fp16) k_chosen_preprocess<__half><<<grid, kBlock, 0, st>>>(sp, N, c, s, dk, rects, ctrl);
+        else k_chosen_preprocess<__nv_bfloat16><<<grid, kBlock, 0, st>>>(sp, N, c, s, dk, rects, ctrl);
+    }
     return cudaGetLastError();
 }
 

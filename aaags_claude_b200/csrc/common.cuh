@@ -70,6 +70,7 @@ struct Control {
     unsigned hist[kMaxPasses][256];   // radix digit histograms of all passes
     unsigned long long gauss_keys;    // depth-first pipeline: keys of the Gaussian depth sort
     unsigned work[2];                 // persistent multi-view rasterisers: next tile of the forward / backward
+    unsigned tile_bucket[2][33];      // heavy-first tile order over many tiles: bucket sizes, then cursors
 };
 constexpr size_t kControlReadback = 24;
 

@@ -274,8 +274,12 @@ cudaError_t launch_tile_ranges_views(cudaStream_t st, unsigned long long capacit
                                      const unsigned* vals_sorted, const StepParams* views, int n_per_view,
                                      unsigned* ranges, Control* ctrl);
 
-// Heavy-first permutation of the tiles (by pair count) for the rasterisers.
-cudaError_t launch_tile_order(cudaStream_t st, const unsigned* ranges, int num_tiles, unsigned* order);
+// Heavy-first permutation of the tiles (by pair count, in power-of-two
+// buckets) for the rasterisers.  Above 65536 tiles (several views) it runs as
+// two grid-wide kernels with scratch in ctrl->tile_bucket (zeroed with the
+// control block at the start of a step).
+cudaError_t launch_tile_order(cudaStream_t st, const unsigned* ranges, int num_tiles, unsigned* order,
+                              Control* ctrl = nullptr);
 
 // Bounded-wait self-test: desc2 = two zeroed descriptors.
 // Zeroes up to four device regions (8-byte aligned, sizes in 8-byte words; a

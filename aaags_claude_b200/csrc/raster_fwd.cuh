@@ -150,11 +150,11 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_fwd(const StepParams* __re
                     done[p] = true;
                     continue;
                 }
-                if (Blend::kBase2) {
-                    const float aT = alpha * T[p];
-                    C[p][0] += c.z * aT;
-                    C[p][1] += c.w * aT;
-                    C[p][2] += bt.x * aT;
+                if (Blend::kBase2) {   // single roundings: the image does not depend on PPT
+                    const float aT = __fmul_rn(alpha, T[p]);
+                    C[p][0] = __fmaf_rn(c.z, aT, C[p][0]);
+                    C[p][1] = __fmaf_rn(c.w, aT, C[p][1]);
+                    C[p][2] = __fmaf_rn(bt.x, aT, C[p][2]);
                 } else {   // the reference's (c * alpha) * T
                     C[p][0] += c.z * alpha * T[p];
                     C[p][1] += c.w * alpha * T[p];

@@ -219,10 +219,12 @@ struct Proj {
 
 // Returns false when the Gaussian is culled.
 // S: element type of the SH coefficients (float here; 16-bit in the
-// reduced-storage form).
+// reduced-storage form).  c3_in (optional): the Gaussian's cov3D, computed once
+// by a caller that projects it into several cameras.
 template <typename S>
 __device__ __forceinline__ bool project_one(const StepParams& sp, const float p[3], const float sc[3],
-                                            const float q[4], float op, const S* __restrict__ sh, Proj& r) {
+                                            const float q[4], float op, const S* __restrict__ sh, Proj& r,
+                                            const float* c3_in = nullptr) {
     const gs3d_camera& cam = sp.cam;
     float pv[3];
     xform4x3(p, cam.view_matrix, pv);
@@ -235,7 +237,12 @@ __device__ __forceinline__ bool project_one(const StepParams& sp, const float p[
     const float pix_y = ((ndc_y + 1.0f) * (float)cam.height - 1.0f) * 0.5f;
 
     float c3[6];
-    cov3d(sc, sp.cfg.scale_modifier, q, c3);
+    if (c3_in) {
+#pragma unroll
+        for (int k = 0; k < 6; k++) c3[k] = c3_in[k];
+    } else {
+        cov3d(sc, sp.cfg.scale_modifier, q, c3);
+    }
     Ewa e;
     ewa_setup(p, cam.view_matrix, sp.focal_x, sp.focal_y, cam.tan_fovx, cam.tan_fovy, e);
     float c2[3];

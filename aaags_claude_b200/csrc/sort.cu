@@ -19,6 +19,8 @@
 // Only the significant key bits are sorted: 32 depth bits plus
 // ceil(log2(num_tiles)) tile bits.
 #include <cuda_runtime.h>
+
+#include <algorithm>
 #include <cstdint>
 
 #include "common.cuh"
@@ -311,6 +313,56 @@ __global__ void __launch_bounds__(1024) k_tile_order(const unsigned* __restrict_
     }
 }
 
+// The same order over many tiles (several views' tiles): per-CTA bucket counts
+// into ctrl->tile_bucket[0], then every CTA reserves its bucket ranges with one
+// global atomic per bucket (cursors in ctrl->tile_bucket[1], starting at the
+// heavy-first bucket offsets) and writes its tiles there.
+__device__ __forceinline__ int tile_bucket_of(const unsigned* __restrict__ ranges, int t) {
+    const unsigned n = ranges[2 * t + 1] - ranges[2 * t];
+    return n ? 32 - __clz(n) : 0;
+}
+
+__global__ void __launch_bounds__(256) k_tile_bucket_count(const unsigned* __restrict__ ranges, int num_tiles,
+                                                          Control* ctrl) {
+    __shared__ unsigned s_cnt[33];
+    if (threadIdx.x < 33) s_cnt[threadIdx.x] = 0;
+    __syncthreads();
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < num_tiles; t += gridDim.x * blockDim.x)
+        atomicAdd(&s_cnt[tile_bucket_of(ranges, t)], 1u);
+    __syncthreads();
+    if (threadIdx.x < 33 && s_cnt[threadIdx.x]) atomicAdd(&ctrl->tile_bucket[0][threadIdx.x], s_cnt[threadIdx.x]);
+}
+
+__global__ void __launch_bounds__(256) k_tile_bucket_scatter(const unsigned* __restrict__ ranges, int num_tiles,
+                                                            Control* ctrl, unsigned* __restrict__ order) {
+    __shared__ unsigned s_cnt[33], s_base[33], s_off[33];
+    if (threadIdx.x < 33) s_cnt[threadIdx.x] = 0;
+    __syncthreads();
+    const int t0 = blockIdx.x * blockDim.x * 4;
+    int bk[4];
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        const int t = t0 + r * blockDim.x + threadIdx.x;
+        bk[r] = t < num_tiles ? tile_bucket_of(ranges, t) : -1;
+        if (bk[r] >= 0) atomicAdd(&s_cnt[bk[r]], 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x < 33) {
+        // heavy-first offset of bucket b: the sizes of the heavier buckets
+        unsigned off = 0;
+        for (int h = 32; h > (int)threadIdx.x; h--) off += ctrl->tile_bucket[0][h];
+        const unsigned n = s_cnt[threadIdx.x];
+        s_base[threadIdx.x] = off + (n ? atomicAdd(&ctrl->tile_bucket[1][threadIdx.x], n) : 0u);
+        s_off[threadIdx.x] = 0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        const int t = t0 + r * blockDim.x + threadIdx.x;
+        if (bk[r] >= 0) order[s_base[bk[r]] + atomicAdd(&s_off[bk[r]], 1u)] = (unsigned)t;
+    }
+}
+
 // One warp plays block 1 of a look-back whose block 0 never publishes, first
 // with the warp-wide look-back, then with the one-thread look-back: each wait
 // must run out after spin_limit polls; kStatusTimeout is raised when both did.
@@ -446,9 +498,16 @@ cudaError_t launch_tile_ranges32(cudaStream_t st, unsigned long long capacity, c
     return cudaGetLastError();
 }
 
-cudaError_t launch_tile_order(cudaStream_t st, const unsigned* ranges, int num_tiles, unsigned* order) {
+cudaError_t launch_tile_order(cudaStream_t st, const unsigned* ranges, int num_tiles, unsigned* order,
+                              Control* ctrl) {
     if (num_tiles <= 0) return cudaSuccess;
-    k_tile_order<<<1, 1024, 0, st>>>(ranges, num_tiles, order);
+    if (num_tiles <= 65536 || !ctrl) {   // one view: a single CTA
+        k_tile_order<<<1, 1024, 0, st>>>(ranges, num_tiles, order);
+        return cudaGetLastError();
+    }
+    const int grid = (num_tiles + 1023) / 1024;
+    k_tile_bucket_count<<<std::min(grid, 4 * sm_count()), 256, 0, st>>>(ranges, num_tiles, ctrl);
+    k_tile_bucket_scatter<<<grid, 256, 0, st>>>(ranges, num_tiles, ctrl, order);
     return cudaGetLastError();
 }
 

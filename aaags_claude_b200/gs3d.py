@@ -35,6 +35,7 @@ OPT_SORT = 7
 OPT_KEEP_GRADIENTS = 8
 OPT_AUTOTUNE = 9
 OPT_DENSITY_SEED = 10
+OPT_RASTER_PPT = 11
 SORT_DEPTH_FIRST, SORT_FULL_KEY = 0, 1
 
 _f = ctypes.POINTER(ctypes.c_float)

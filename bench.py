@@ -72,6 +72,8 @@ def _args(argv=None):
                     help="timed steps of the 64-view step (0: skip it)")
     ap.add_argument("--autotune", type=int, default=1,
                     help="1: let the library tune the rasterisers' threads per tile during the warm-up")
+    ap.add_argument("--ppt", type=int, default=0, choices=(0, 1, 2, 4),
+                    help="rasterisers' pixels per thread, fixed (profiling runs; 0: default / autotuned)")
     ap.add_argument("--eval3d", type=int, default=1,
                     help="1: also time the 3D-evaluation (eval_3D) render of 100k Gaussians at 640x480")
     ap.add_argument("--only-eval3d", dest="only_eval3d", action="store_true",
@@ -326,6 +328,7 @@ def _measure_form(a, ctx, form, w, cam, cfg, tc, gt_dev, gt_pin, local, dist):
     from aaags_claude_b200 import gs3d
     ctx.set_option(gs3d.OPT_FORM, FORMS[form])
     ctx.set_option(gs3d.OPT_AUTOTUNE, a.autotune)
+    ctx.set_option(gs3d.OPT_RASTER_PPT, a.ppt)
     ctx.set_raw_params(w.scene)
     stream = torch.cuda.ExternalStream(ctx.stream_handle(), device=f"cuda:{local}")
     it = 0
@@ -557,6 +560,7 @@ def measure_batched(a, local: int) -> dict:
     # the chosen form, all 64 views per step
     ctx.set_option(gs3d.OPT_FORM, gs3d.FORM_BF16)
     ctx.set_option(gs3d.OPT_AUTOTUNE, a.autotune)
+    ctx.set_option(gs3d.OPT_RASTER_PPT, a.ppt)
     ctx.set_raw_params(w.scene)
     it = [0]
 

@@ -52,6 +52,8 @@ typedef struct gs3dc_ctx gs3dc_ctx;
                                        events, un-captured) and the fastest forward / backward stay; 0 (default): 2 */
 #define GS3DC_OPT_DENSITY_SEED  10  /* state of the density controller's split sampler (LCG); 12345 at creation,
                                         like DensityController::rng_state_ (density_controller.h:41) */
+#define GS3DC_OPT_RASTER_PPT    11  /* 1, 2 or 4: the rasterisers' pixels per thread in train steps, fixed (the
+                                       autotuner then stays off); 0 (default): 2, or the autotuner's pick */
 
 /* Depth-first (default): the Gaussians are stably sorted by depth, their pairs
  * emitted in that order and stably sorted by the tile bits alone.  Full key:

@@ -91,6 +91,33 @@ def test_gradients_against_fp64_oracle(ctx, form):
     assert min(per.values()) >= 0.99
 
 
+def test_pixels_per_thread_keep_the_image(ctx, form):
+    """The rasterisers' pixels per thread (1, 2, 4: 256, 128, 64 threads per
+    tile) change neither the reduced-form image (bit for bit) nor, beyond
+    FP32-summation order, the gradients."""
+    sc = S.random_scene(20000, seed=35)
+    cam = S.look_at_camera((0.2, -0.3, -3.0), 333, 251)
+    cfg = S.render_config(True)
+    gt = O.forward(S.perturbed(sc), cam, S.render_config(False), "c").image
+    ctx.set_option(gs3d.OPT_KEEP_GRADIENTS, 1)
+    out = {}
+    try:
+        for ppt in (1, 2, 4):
+            ctx.set_option(gs3d.OPT_RASTER_PPT, ppt)
+            ctx.set_raw_params(sc)
+            loss = ctx.train_step(cam, gt, cfg, S.train_config(**ZERO_LR), 0)
+            out[ppt] = (loss, ctx.get_image(cam), ctx.get_gradients())
+    finally:
+        ctx.set_option(gs3d.OPT_RASTER_PPT, 0)
+        ctx.set_option(gs3d.OPT_KEEP_GRADIENTS, 0)
+    for ppt in (2, 4):
+        assert np.array_equal(out[ppt][1], out[1][1]), ppt
+        assert abs(out[ppt][0] - out[1][0]) <= 1e-7 * out[1][0]   # the loss sums tiles in another order
+        for k in ("pos", "sc", "rot", "sh", "op"):
+            a, b = out[ppt][2][k].astype(np.float64), out[1][2][k].astype(np.float64)
+            assert np.linalg.norm(a - b) <= 1e-4 * np.linalg.norm(b), (ppt, k)
+
+
 def test_fewer_pairs_than_plain(ctx):
     sc = S.random_scene(100_000, seed=34)
     cam = S.look_at_camera((0.3, 0.2, -3.0), 640, 480)

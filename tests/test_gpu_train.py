@@ -276,7 +276,8 @@ def test_recompute_backward_memory_vs_stored_lists():
           f"MiB); stored lists: {used_lists / 2**20:.1f} MiB allocated for {contributors} contributors "
           f"({list_bytes / 2**20:.1f} MiB of lists and offsets)")
     assert list_bytes == 4 * npx + 8 * contributors
-    assert used_lists >= list_bytes                      # measured by the driver (2 MiB pages)
+    # measured by the driver: 2 MiB pages, and small buffers may land in pages the runtime already holds
+    assert used_lists >= 0.95 * list_bytes
     assert used_recompute <= 12 * npx + (4 << 20)        # nothing beyond the d_image upload
     assert used_lists > 10 * used_recompute
     for k in ("d_means2D", "d_conics", "d_rgb", "d_opac"):
