@@ -57,8 +57,10 @@ struct DevBuf {
 constexpr int kParamSlots = 4;  // pinned ring of per-step parameter blocks
 constexpr int kMaxBatchViews = 255;   // views per multi-view step (one 8-bit radix digit)
 constexpr int kTunePpt[3] = {1, 2, 4};   // autotuner candidates: pixels per thread of the rasterisers
+constexpr int kTuneBatch[2] = {64, 256}; // then: records staged per round (against the default 128)
 constexpr int kTuneReps = 2;             // timed steps per candidate
-constexpr int kTuneSteps = 3 * kTuneReps;
+constexpr int kTunePptSteps = 3 * kTuneReps;
+constexpr int kTuneSteps = kTunePptSteps + 2 * kTuneReps;
 constexpr int kShapeSlots = 8;           // single-view train step: workload shapes with a cached graph / tuning
 constexpr int kGraphKey = 9;             // words of a graph key
 
@@ -205,20 +207,24 @@ struct gs3dc_ctx {
         cudaGraphExec_t graph = nullptr;
         long long key[kGraphKey] = {};
     } batch;
-    // rasteriser pixels per thread in use (set per step; 2 unless the autotuner chose otherwise)
-    int fwd_ppt = 2, bwd_ppt = 2;
+    // rasteriser pixels per thread and staging batch in use (set per step; 2 and 128 unless the
+    // autotuner chose otherwise)
+    int fwd_ppt = 2, bwd_ppt = 2, fwd_batch = 128, bwd_batch = 128;
     // online autotuner (GS3DC_OPT_AUTOTUNE): per workload shape, the first kTuneSteps train steps
-    // cycle through the candidate pixels-per-thread and time both rasterisers; the fastest stay
+    // time both rasterisers, first at each candidate pixels-per-thread (batch 128), then at the
+    // fastest ones with each other staging batch; the fastest settings stay
     struct Tune {
         long long key[6] = {};
         int trial = 0;
-        float fwd_ms[3] = {}, bwd_ms[3] = {};
-        int fwd_ppt = 2, bwd_ppt = 2;
+        float fwd_ms[3] = {}, bwd_ms[3] = {};     // per pixels-per-thread candidate, batch 128
+        float fwd_bms[2] = {}, bwd_bms[2] = {};   // per other batch, at the picked pixels per thread
+        int fwd_ppt = 2, bwd_ppt = 2, fwd_batch = 128, bwd_batch = 128;
         bool done = false;
         unsigned long long used = 0;   // LRU clock (single-view shapes)
     };
     bool autotune = false;
-    int forced_ppt = 0;   // GS3DC_OPT_RASTER_PPT
+    int forced_ppt = 0;     // GS3DC_OPT_RASTER_PPT
+    int forced_batch = 0;   // GS3DC_OPT_RASTER_BATCH
     Tune tune_single[kShapeSlots], tune_batch;
     unsigned long long tclock = 0;
     cudaEvent_t tune_ev[3] = {};
@@ -590,8 +596,10 @@ int read_control(gs3dc_ctx* c) {
 // The pixels per thread of this step: the tuned values, or the next
 // candidate while the workload shape is being tuned (returns true then).
 bool tune_begin(gs3dc_ctx* c, gs3dc_ctx::Tune& t, const long long key[6]) {
+    c->fwd_batch = c->bwd_batch = 128;
     if (c->forced_ppt) {
         c->fwd_ppt = c->bwd_ppt = c->forced_ppt;
+        if (c->forced_batch) c->fwd_batch = c->bwd_batch = c->forced_batch;
         return false;
     }
     if (!c->autotune) {
@@ -605,26 +613,59 @@ bool tune_begin(gs3dc_ctx* c, gs3dc_ctx::Tune& t, const long long key[6]) {
     if (t.done) {
         c->fwd_ppt = t.fwd_ppt;
         c->bwd_ppt = t.bwd_ppt;
+        c->fwd_batch = t.fwd_batch;
+        c->bwd_batch = t.bwd_batch;
         return false;
     }
-    c->fwd_ppt = c->bwd_ppt = kTunePpt[t.trial / kTuneReps];
+    if (t.trial < kTunePptSteps) {
+        c->fwd_ppt = c->bwd_ppt = kTunePpt[t.trial / kTuneReps];
+    } else {
+        c->fwd_ppt = t.fwd_ppt;
+        c->bwd_ppt = t.bwd_ppt;
+        c->fwd_batch = c->bwd_batch = kTuneBatch[(t.trial - kTunePptSteps) / kTuneReps];
+    }
     return true;
 }
 
-// Adds a trial's rasteriser times; after the last trial keeps the fastest.
+// Adds a trial's rasteriser times; after the pixels-per-thread trials keeps the
+// fastest of those, after the batch trials the fastest batch.
 void tune_end(gs3dc_ctx* c, gs3dc_ctx::Tune& t, float fwd_ms, float bwd_ms) {
-    const int k = t.trial / kTuneReps;
-    t.fwd_ms[k] += fwd_ms;
-    t.bwd_ms[k] += bwd_ms;
-    if (++t.trial < kTuneSteps) return;
-    int bf = 0, bb = 0;
-    for (int i = 1; i < 3; i++) {
-        if (t.fwd_ms[i] < t.fwd_ms[bf]) bf = i;
-        if (t.bwd_ms[i] < t.bwd_ms[bb]) bb = i;
+    if (t.trial < kTunePptSteps) {
+        const int k = t.trial / kTuneReps;
+        t.fwd_ms[k] += fwd_ms;
+        t.bwd_ms[k] += bwd_ms;
+    } else {
+        const int k = (t.trial - kTunePptSteps) / kTuneReps;
+        t.fwd_bms[k] += fwd_ms;
+        t.bwd_bms[k] += bwd_ms;
     }
-    t.fwd_ppt = kTunePpt[bf];
-    t.bwd_ppt = kTunePpt[bb];
-    t.done = true;   // graph keys hold the pixels per thread: the next step captures the chosen kernels
+    ++t.trial;
+    if (t.trial == kTunePptSteps) {
+        int bf = 0, bb = 0;
+        for (int i = 1; i < 3; i++) {
+            if (t.fwd_ms[i] < t.fwd_ms[bf]) bf = i;
+            if (t.bwd_ms[i] < t.bwd_ms[bb]) bb = i;
+        }
+        t.fwd_ppt = kTunePpt[bf];
+        t.bwd_ppt = kTunePpt[bb];
+        return;
+    }
+    if (t.trial < kTuneSteps) return;
+    // batch 128 at the picked pixels per thread against 64 and 256 (same number of timed steps each)
+    float best_f = t.fwd_ms[t.fwd_ppt == 1 ? 0 : t.fwd_ppt == 2 ? 1 : 2];
+    float best_b = t.bwd_ms[t.bwd_ppt == 1 ? 0 : t.bwd_ppt == 2 ? 1 : 2];
+    for (int i = 0; i < 2; i++) {
+        if (t.fwd_bms[i] < best_f) {
+            best_f = t.fwd_bms[i];
+            t.fwd_batch = kTuneBatch[i];
+        }
+        if (t.bwd_bms[i] < best_b) {
+            best_b = t.bwd_bms[i];
+            t.bwd_batch = kTuneBatch[i];
+        }
+    }
+    t.done = true;   // graph keys hold the settings: the next step captures the chosen kernels
+    (void)c;
 }
 
 // The tuning state of a single-view workload shape (least recently used replaced).
@@ -778,10 +819,11 @@ int seq_back_chosen(gs3dc_ctx* c) {
     const int w = c->sorted_which;
     if ((rc = mark(c, GS3DC_STAGE_RASTER_FWD))) return rc;
     CK(launch_raster_fwd_fast(c->stream, c->sp_dev, c->num_tiles, c->ranges.p, c->tile_order.p, c->vals[w].p,
-                              screen_ptrs(c, false), pixel_ptrs(c), c->ctrl, c->fwd_ppt));
+                              screen_ptrs(c, false), pixel_ptrs(c), c->ctrl, c->fwd_ppt, c->fwd_batch));
     if ((rc = mark(c, GS3DC_STAGE_RASTER_BWD))) return rc;
     CK(launch_raster_bwd_fast(c->stream, c->sp_dev, c->num_tiles, c->ranges.p, c->tile_order.p, c->vals[w].p,
-                              screen_ptrs(c, false), pixel_ptrs(c), rgrad_ptrs(c), c->ctrl, c->bwd_ppt));
+                              screen_ptrs(c, false), pixel_ptrs(c), rgrad_ptrs(c), c->ctrl, c->bwd_ppt,
+                              c->bwd_batch));
     if ((rc = mark(c, GS3DC_STAGE_PREPROCESS_BWD))) return rc;
     CK(launch_chosen_backward_adam(c->stream, c->sp_dev, c->N, c->max_coeffs * 3, c->form == GS3DC_FORM_FP16,
                                    chosen_ptrs(c), rgrad_ptrs(c),
@@ -815,10 +857,11 @@ int seq_train_back(gs3dc_ctx* c) {
     const int w = c->sorted_which;
     if ((rc = mark(c, GS3DC_STAGE_RASTER_FWD))) return rc;
     CK(launch_raster_fwd_plain(c->stream, c->sp_dev, c->num_tiles, true, c->ranges.p, c->tile_order.p, c->vals[w].p,
-                               screen_ptrs(c, false), pixel_ptrs(c), c->ctrl, c->fwd_ppt));
+                               screen_ptrs(c, false), pixel_ptrs(c), c->ctrl, c->fwd_ppt, c->fwd_batch));
     if ((rc = mark(c, GS3DC_STAGE_RASTER_BWD))) return rc;
     CK(launch_raster_bwd_plain(c->stream, c->sp_dev, c->num_tiles, true, c->ranges.p, c->tile_order.p, c->vals[w].p,
-                               screen_ptrs(c, false), pixel_ptrs(c), rgrad_ptrs(c), c->ctrl, c->bwd_ppt));
+                               screen_ptrs(c, false), pixel_ptrs(c), rgrad_ptrs(c), c->ctrl, c->bwd_ppt,
+                              c->bwd_batch));
     if ((rc = mark(c, GS3DC_STAGE_PREPROCESS_BWD))) return rc;
     if (c->fused_adam && !c->keep_grads) {
         CK(launch_preprocess_bwd_plain(c->stream, c->sp_dev, c->N, c->max_coeffs * 3, 1, model_ptrs(c),
@@ -1063,10 +1106,11 @@ int seq_batch(gs3dc_ctx* c, const BatchShape& sh) {
     const bool tuning = c->autotune && !c->tune_batch.done;
     if (tuning) CK(cudaEventRecord(c->tune_ev[0], c->stream));
     CK(launch_raster_fwd_fast_multi(c->stream, views, sh.V, sh.tiles, b.ranges.p, b.order.p, b.vals[which].p,
-                                    batch_screen(c), batch_pixels(c), c->ctrl, c->fwd_ppt));
+                                    batch_screen(c), batch_pixels(c), c->ctrl, c->fwd_ppt, c->fwd_batch));
     if (tuning) CK(cudaEventRecord(c->tune_ev[1], c->stream));
     CK(launch_raster_bwd_fast_multi(c->stream, views, sh.V, sh.tiles, b.ranges.p, b.order.p, b.vals[which].p,
-                                    batch_screen(c), batch_pixels(c), batch_rgrads(c), c->ctrl, c->bwd_ppt));
+                                    batch_screen(c), batch_pixels(c), batch_rgrads(c), c->ctrl, c->bwd_ppt,
+                                    c->bwd_batch));
     if (tuning) CK(cudaEventRecord(c->tune_ev[2], c->stream));
     CK(launch_chosen_backward_adam(c->stream, views, c->N, c->max_coeffs * 3, c->form == GS3DC_FORM_FP16,
                                    chosen_ptrs(c), batch_rgrads(c),
@@ -1249,6 +1293,11 @@ int gs3dc_set_option(gs3dc_ctx* c, int option, int64_t value) {
                 return fail(c, GS3DC_ERR_INVALID_ARG, "pixels per thread %lld: 0, 1, 2 or 4", (long long)value);
             c->forced_ppt = (int)value;
             return GS3DC_OK;
+        case GS3DC_OPT_RASTER_BATCH:
+            if (value != 0 && value != 64 && value != 128 && value != 256)
+                return fail(c, GS3DC_ERR_INVALID_ARG, "staging batch %lld: 0, 64, 128 or 256", (long long)value);
+            c->forced_batch = (int)value;
+            return GS3DC_OK;
         case GS3DC_OPT_KEEP_GRADIENTS:
             c->keep_grads = value != 0;
             drop_graphs(c);
@@ -1269,6 +1318,8 @@ int gs3dc_get_stat(gs3dc_ctx* c, int stat, int64_t* value) {
         case GS3DC_STAT_TOTAL_PAIRS: *value = (int64_t)c->last_pairs; return GS3DC_OK;
         case GS3DC_STAT_FWD_PPT: *value = c->fwd_ppt; return GS3DC_OK;
         case GS3DC_STAT_BWD_PPT: *value = c->bwd_ppt; return GS3DC_OK;
+        case GS3DC_STAT_FWD_BATCH: *value = c->fwd_batch; return GS3DC_OK;
+        case GS3DC_STAT_BWD_BATCH: *value = c->bwd_batch; return GS3DC_OK;
         case GS3DC_STAT_PAIR_CAPACITY: *value = (int64_t)c->cap; return GS3DC_OK;
         case GS3DC_STAT_KERNELS_LAST: *value = c->kernels_last; return GS3DC_OK;
         case GS3DC_STAT_SORT_PASSES: *value = c->sort_passes; return GS3DC_OK;
@@ -1868,7 +1919,7 @@ int gs3dc_train_step(gs3dc_ctx* c, const gs3d_camera* cam, const float* gt, int 
             c->N, c->max_coeffs, cam->width, cam->height, (long long)c->cap, c->sort_passes,
             (long long)c->spin_limit,
             (c->fused_adam ? 1 : 2) + 4 * c->sort_mode + 16 * c->form + 64 * (c->keep_grads ? 1 : 0) +
-                128 * c->fwd_ppt + 1024 * c->bwd_ppt,
+                128 * c->fwd_ppt + 1024 * c->bwd_ppt + 8192 * c->fwd_batch + 8192 * 512 * c->bwd_batch,
             (long long)g_alloc_epoch.load(std::memory_order_relaxed)};
         c->kernels_last = 0;
         if (c->use_graph && !c->stage_timing && !first && attempt == 0) {
@@ -2023,7 +2074,8 @@ int gs3dc_train_step_batch(gs3dc_ctx* c, int n_views, const gs3d_camera* cams, c
         CK(cudaEventRecord(b.views_event, c->stream));
         const long long key[kGraphKey] = {
             c->N, n_views, (long long)sh.tiles, (long long)sh.pix, (long long)b.cap, c->form, (long long)c->spin_limit,
-            c->max_coeffs + 1000 * (c->keep_grads ? 1 : 0) + 2000 * c->fwd_ppt + 20000 * c->bwd_ppt,
+            c->max_coeffs + 1000 * (c->keep_grads ? 1 : 0) + 2000 * c->fwd_ppt + 20000 * c->bwd_ppt +
+                200000LL * c->fwd_batch + 200000LL * 512 * c->bwd_batch,
             (long long)g_alloc_epoch.load(std::memory_order_relaxed)};
         if (c->use_graph && !first && !tuning && attempt == 0) {
             if (!b.graph || std::memcmp(key, b.key, sizeof(key)) != 0) {
@@ -2279,10 +2331,10 @@ static int dc_stats_pass(gs3dc_ctx* c, const gs3d_camera* cam, const gs3d_render
         if ((rc = seq_train_front(c))) return rc;
         const int w = c->sorted_which;
         CK(launch_raster_fwd_plain(c->stream, c->sp_dev, c->num_tiles, true, c->ranges.p, c->tile_order.p,
-                                   c->vals[w].p, screen_ptrs(c, false), pixel_ptrs(c), c->ctrl, c->fwd_ppt));
+                                   c->vals[w].p, screen_ptrs(c, false), pixel_ptrs(c), c->ctrl, c->fwd_ppt, c->fwd_batch));
         CK(launch_raster_bwd_plain(c->stream, c->sp_dev, c->num_tiles, true, c->ranges.p, c->tile_order.p,
                                    c->vals[w].p, screen_ptrs(c, false), pixel_ptrs(c), rgrad_ptrs(c), c->ctrl,
-                                   c->bwd_ppt));
+                                   c->bwd_ppt, c->bwd_batch));
         if ((rc = read_control(c))) return rc;
         if (c->persist_host->sticky_overflow) {
             if ((rc = acknowledge_overflow(c))) return rc;

@@ -358,12 +358,228 @@ struct __align__(16) ChosenBwdShared {
     }
 };
 
+// Thread 0: the bulk copies of slice g0's parameters (kCB Gaussians, all present) and, for one
+// view, its screen gradients into sm, completing on sm.bar; the slice's optimiser moments travel
+// to L2 meanwhile.
+template <typename S, bool MULTI>
+__device__ __forceinline__ void issue_slice_copies(ChosenBwdShared<S, MULTI>& sm, long long g0, int mc3, ChosenPtrs c,
+                                                   RGradPtrs rg) {
+    const S* shg = static_cast<const S*>(c.sh) + (size_t)mc3 * g0;
+    const unsigned sh_bytes = (unsigned)(kCB * mc3 * (int)sizeof(S));
+    const unsigned grad_bytes = MULTI ? 0u : (unsigned)kCB * (8u + 12u + 12u + 4u);
+    mbar_arrive_expect_tx(&sm.bar, sh_bytes + (unsigned)kCB * (16u + 12u) + grad_bytes);
+    tma_load_1d(sm.sh, shg, sh_bytes, &sm.bar);
+    tma_load_1d(sm.attr, reinterpret_cast<const uint4*>(c.attr) + g0, 16u * kCB, &sm.bar);
+    tma_load_1d(sm.pos, c.pos + 3 * g0, 12u * kCB, &sm.bar);
+    if (!MULTI) {
+        tma_load_1d(sm.dm2, rg.dm2 + 2 * g0, 8u * kCB, &sm.bar);
+        tma_load_1d(sm.dcon, rg.dcon + 3 * g0, 12u * kCB, &sm.bar);
+        tma_load_1d(sm.drgb, rg.drgb + 3 * g0, 12u * kCB, &sm.bar);
+        tma_load_1d(sm.dop, rg.dop + g0, 4u * kCB, &sm.bar);
+    }
+    // the optimiser's moments of this slice travel to L2 while the adjoint computes
+    const unsigned mv_sh = (unsigned)(kCB * mc3) * 2u;
+    prefetch_l2(static_cast<const __nv_bfloat16*>(c.m_sh) + (size_t)mc3 * g0, mv_sh);
+    prefetch_l2(static_cast<const __nv_bfloat16*>(c.v_sh) + (size_t)mc3 * g0, mv_sh);
+    prefetch_l2(reinterpret_cast<const uint4*>(c.m_attr) + g0, 16u * kCB);
+    prefetch_l2(reinterpret_cast<const uint4*>(c.v_attr) + g0, 16u * kCB);
+    prefetch_l2(c.m_pos + 3 * g0, 12u * kCB);
+    prefetch_l2(c.v_pos + 3 * g0, 12u * kCB);
+}
+
+// The same slice staged with plain loads (a partial last slice); the caller synchronises.
+template <typename S, bool MULTI>
+__device__ __forceinline__ void stage_slice_plain(ChosenBwdShared<S, MULTI>& sm, long long g0, int ng, int mc3,
+                                                  ChosenPtrs c, RGradPtrs rg) {
+    const int tid = threadIdx.x;
+    const S* shg = static_cast<const S*>(c.sh) + (size_t)mc3 * g0;
+    S* shs = reinterpret_cast<S*>(sm.sh);
+    for (int e = tid; e < mc3 * ng; e += kCB) shs[e] = shg[e];
+    for (int e = tid; e < ng; e += kCB) sm.attr[e] = reinterpret_cast<const uint4*>(c.attr)[g0 + e];
+    for (int e = tid; e < 3 * ng; e += kCB) sm.pos[e] = c.pos[3 * g0 + e];
+    if (!MULTI) {
+        for (int e = tid; e < 2 * ng; e += kCB) sm.dm2[e] = rg.dm2[2 * g0 + e];
+        for (int e = tid; e < 3 * ng; e += kCB) {
+            sm.dcon[e] = rg.dcon[3 * g0 + e];
+            sm.drgb[e] = rg.drgb[3 * g0 + e];
+        }
+        for (int e = tid; e < ng; e += kCB) sm.dop[e] = rg.dop[g0 + e];
+    }
+}
+
+// One view: the adjoint of PreprocessorBackwardCPU::backward
+// (preprocessor_backward_cpu.cpp:205-645) of each Gaussian of the staged slice
+// into the shared-memory gradients; the slice's screen-gradient accumulators
+// restart at zero for the next step.
+template <typename S>
+__device__ __forceinline__ void adjoint_slice(ChosenBwdShared<S, false>& sm, const StepParams& sp, long long g0,
+                                              int ng, int mc3, RGradPtrs rg) {
+    const int tid = threadIdx.x;
+    if (tid < ng) {
+#pragma unroll
+        for (int k = 0; k < 3; k++) sm.g_pos[3 * tid + k] = sm.g_sc[3 * tid + k] = 0.f;
+#pragma unroll
+        for (int k = 0; k < 4; k++) sm.g_rot[4 * tid + k] = 0.f;
+        sm.g_op[tid] = 0.f;
+        for (int k = 0; k < 16; k++) sm.basis[k * kCB + tid] = 0.f;
+        for (int k = 0; k < 3; k++) sm.geff[k * kCB + tid] = 0.f;
+    }
+    {
+        const long long e0 = g0;
+        // the screen-gradient accumulators restart at zero for the next step
+        for (int e = tid; e < 2 * ng; e += kCB) rg.dm2[2 * e0 + e] = 0.f;
+        for (int e = tid; e < 3 * ng; e += kCB) {
+            rg.dcon[3 * e0 + e] = 0.f;
+            rg.drgb[3 * e0 + e] = 0.f;
+        }
+        for (int e = tid; e < ng; e += kCB) rg.dop[e0 + e] = 0.f;
+        if (tid < ng) {
+            BwdIn in;
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                in.dcn[k] = sm.dcon[3 * tid + k];
+                in.drgb[k] = sm.drgb[3 * tid + k];
+            }
+            in.dm[0] = sm.dm2[2 * tid];
+            in.dm[1] = sm.dm2[2 * tid + 1];
+            in.dop = sm.dop[tid];
+            // every gradient is linear in the screen gradients: a Gaussian without any adds none
+            const bool any = in.dm[0] != 0.f || in.dm[1] != 0.f || in.dcn[0] != 0.f || in.dcn[1] != 0.f ||
+                             in.dcn[2] != 0.f || in.drgb[0] != 0.f || in.drgb[1] != 0.f || in.drgb[2] != 0.f ||
+                             in.dop != 0.f;
+            if (any) {
+#pragma unroll
+                for (int k = 0; k < 3; k++) in.p[k] = sm.pos[3 * tid + k];
+                in.act = nullptr;
+                load_attr<S>(sm.attr, tid, in.rsc, &in.rop, in.rq);
+                float shf[48];
+                if (mc3 == 48) {
+                    // this Gaussian's 96 SH bytes as six 16-byte loads
+                    const uint4* row = sm.sh + 6 * tid;
+#pragma unroll
+                    for (int qd = 0; qd < 6; qd++) {
+                        const uint4 vv = row[qd];
+                        const S* h = reinterpret_cast<const S*>(&vv);
+#pragma unroll
+                        for (int k = 0; k < 8; k++) shf[8 * qd + k] = ldf(h[k]);
+                    }
+                } else {
+                    const S* shs = reinterpret_cast<const S*>(sm.sh) + mc3 * tid;
+#pragma unroll
+                    for (int k = 0; k < 48; k++) shf[k] = k < mc3 ? ldf(shs[k]) : 0.f;
+                }
+                in.sh = shf;
+                BwdOut o;
+#pragma unroll
+                for (int k = 0; k < 3; k++) o.gp[k] = o.gs[k] = o.geff[k] = 0.f;
+#pragma unroll
+                for (int k = 0; k < 4; k++) o.gq[k] = 0.f;
+                o.gop = 0.f;
+#pragma unroll
+                for (int k = 0; k < 16; k++) o.basis[k] = 0.f;
+                backward_one(sp, in, o);
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    sm.g_pos[3 * tid + k] = o.gp[k];
+                    sm.g_sc[3 * tid + k] = o.gs[k];
+                }
+#pragma unroll
+                for (int k = 0; k < 4; k++) sm.g_rot[4 * tid + k] = o.gq[k];
+                sm.g_op[tid] = o.gop;
+#pragma unroll
+                for (int k = 0; k < 16; k++) sm.basis[k * kCB + tid] = o.basis[k];
+#pragma unroll
+                for (int k = 0; k < 3; k++) sm.geff[k * kCB + tid] = o.geff[k];
+            }
+        }
+    }
+}
+
+// Adam over the slice's contiguous parameters with 16-byte accesses and
+// stochastic rounding (and, when asked, the FP32 gradients).
+template <typename S, bool MULTI>
+__device__ __forceinline__ void adam_slice(ChosenBwdShared<S, MULTI>& sm, const StepParams& sp, long long g0, int ng,
+                                           int mc3, ChosenPtrs c, GradPtrs gout) {
+    const int tid = threadIdx.x;
+    if (gout.g_pos) {
+        for (int e = tid; e < 3 * ng; e += kCB) {
+            gout.g_pos[3 * g0 + e] = sm.g_pos[e];
+            gout.g_sc[3 * g0 + e] = sm.g_sc[e];
+        }
+        for (int e = tid; e < 4 * ng; e += kCB) gout.g_rot[4 * g0 + e] = sm.g_rot[e];
+        for (int e = tid; e < ng; e += kCB) gout.g_op[g0 + e] = sm.g_op[e];
+        for (int e = tid; e < mc3 * ng; e += kCB) {
+            const int t = e / mc3, k = e - t * mc3;
+            gout.g_sh[(size_t)mc3 * g0 + e] = sm.gsh(t, k);
+        }
+    }
+    const long long sh0 = (long long)mc3 * g0;
+    S* shw = static_cast<S*>(c.sh);
+    __nv_bfloat16* msh = static_cast<__nv_bfloat16*>(c.m_sh);
+    __nv_bfloat16* vsh = static_cast<__nv_bfloat16*>(c.v_sh);
+    const float lr_sh[8] = {sp.lr_sh, sp.lr_sh, sp.lr_sh, sp.lr_sh, sp.lr_sh, sp.lr_sh, sp.lr_sh, sp.lr_sh};
+    if (ng == kCB) {
+        // SH: 8 * mc3 chunks of 8 coefficients (16-byte aligned: the slice starts at 128 * mc3 * blockIdx
+        // bytes); the parameters are already in shared memory
+        const int nq = (kCB * mc3) / 8;
+        uint4* m4 = reinterpret_cast<uint4*>(msh + sh0);
+        uint4* v4 = reinterpret_cast<uint4*>(vsh + sh0);
+        uint4* p4 = reinterpret_cast<uint4*>(shw + sh0);
+        for (int q = tid; q < nq; q += kCB) {
+            uint4 pp = sm.sh[q], mm = m4[q], vv = v4[q];
+            float gg[8];
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                const int e = 8 * q + k, t = e / mc3;
+                gg[k] = sm.gsh(t, e - t * mc3);
+            }
+            opt8<S>(sp, pp, mm, vv, gg, lr_sh, (unsigned)(sh0 + 8 * q), 0x5bd1e995u);
+            p4[q] = pp;
+            m4[q] = mm;
+            v4[q] = vv;
+        }
+    } else {
+        const S* shs = reinterpret_cast<const S*>(sm.sh);
+        for (int e = tid; e < mc3 * ng; e += kCB) {
+            const int t = e / mc3;
+            float m = __bfloat162float(msh[sh0 + e]), v = __bfloat162float(vsh[sh0 + e]);
+            const float pn = opt_elem(sp, ldf(shs[e]), m, v, sm.gsh(t, e - t * mc3), sp.lr_sh);
+            unsigned rp, rm, rv;
+            sr_words((unsigned)(sh0 + e) ^ 0x5bd1e995u, sp.seed, rp, rm, rv);
+            shw[sh0 + e] = cvt_sr<S>(pn, rp);
+            msh[sh0 + e] = cvt_sr<__nv_bfloat16>(m, rm);
+            vsh[sh0 + e] = cvt_sr<__nv_bfloat16>(v, rv);
+        }
+    }
+    // attributes: one 16-byte record per Gaussian
+    const float lra[8] = {sp.lr_scale, sp.lr_scale, sp.lr_scale, sp.lr_opac, sp.lr_rot, sp.lr_rot, sp.lr_rot,
+                          sp.lr_rot};
+    for (int t = tid; t < ng; t += kCB) {
+        const float gg[8] = {sm.g_sc[3 * t], sm.g_sc[3 * t + 1], sm.g_sc[3 * t + 2], sm.g_op[t],
+                             sm.g_rot[4 * t], sm.g_rot[4 * t + 1], sm.g_rot[4 * t + 2], sm.g_rot[4 * t + 3]};
+        uint4 pp = sm.attr[t];
+        uint4 mm = reinterpret_cast<const uint4*>(c.m_attr)[g0 + t];
+        uint4 vv = reinterpret_cast<const uint4*>(c.v_attr)[g0 + t];
+        opt8<S>(sp, pp, mm, vv, gg, lra, (unsigned)(8 * (g0 + t)), 0u);
+        reinterpret_cast<uint4*>(c.attr)[g0 + t] = pp;
+        reinterpret_cast<uint4*>(c.m_attr)[g0 + t] = mm;
+        reinterpret_cast<uint4*>(c.v_attr)[g0 + t] = vv;
+    }
+    // positions: FP32 parameters and moments
+    for (int e = tid; e < 3 * ng; e += kCB) {
+        const long long ge = 3 * g0 + e;
+        float m = c.m_pos[ge], v = c.v_pos[ge];
+        c.pos[ge] = opt_elem(sp, sm.pos[e], m, v, sm.g_pos[e], sp.lr_pos);
+        c.m_pos[ge] = m;
+        c.v_pos[ge] = v;
+    }
+}
+
 // One CTA per 64 consecutive Gaussians: bulk copies of their parameters and
 // screen gradients into shared memory (the accumulators are zeroed for the
 // next step), the per-Gaussian adjoint of PreprocessorBackwardCPU::backward
 // (preprocessor_backward_cpu.cpp:205-645) from there into shared-memory
-// gradients, then Adam over the CTA's contiguous parameter slice with 16-byte
-// accesses and stochastic rounding (and, when asked, the FP32 gradients).
+// gradients, then Adam over the CTA's contiguous parameter slice.
 template <typename S, bool MULTI>
 __global__ void __launch_bounds__(kCB, MULTI ? 8 : 10) k_chosen_backward(const StepParams* __restrict__ spp, int N, int mc3,
                                                          ChosenPtrs c, RGradPtrs rg, GradPtrs gout, Control* ctrl,
@@ -376,56 +592,22 @@ __global__ void __launch_bounds__(kCB, MULTI ? 8 : 10) k_chosen_backward(const S
     if (blockIdx.x == 0 && tid == 0 && sp.use_adam) atomicAdd(&sp.persist->applied_steps, 1ull);
     const long long g0 = (long long)blockIdx.x * kCB;
     const int ng = (int)min((long long)kCB, (long long)N - g0);
-    // ---- phase 0: staging ----
-    const S* shg = static_cast<const S*>(c.sh) + (size_t)mc3 * g0;
+    // ---- phase 0: staging (several views: the screen gradients follow per view below) ----
     if (ng == kCB) {
         // a full CTA: every slice is a multiple of 16 bytes at a 16-byte aligned offset -> bulk copies
-        // (several views: the screen gradients follow per view below)
         if (tid == 0) {
             mbar_init(&sm.bar, 1);
             mbar_fence_init();
         }
         __syncthreads();
-        if (tid == 0) {
-            const unsigned sh_bytes = (unsigned)(kCB * mc3 * (int)sizeof(S));
-            const unsigned grad_bytes = MULTI ? 0u : (unsigned)kCB * (8u + 12u + 12u + 4u);
-            mbar_arrive_expect_tx(&sm.bar, sh_bytes + (unsigned)kCB * (16u + 12u) + grad_bytes);
-            tma_load_1d(sm.sh, shg, sh_bytes, &sm.bar);
-            tma_load_1d(sm.attr, reinterpret_cast<const uint4*>(c.attr) + g0, 16u * kCB, &sm.bar);
-            tma_load_1d(sm.pos, c.pos + 3 * g0, 12u * kCB, &sm.bar);
-            if (!MULTI) {
-                tma_load_1d(sm.dm2, rg.dm2 + 2 * g0, 8u * kCB, &sm.bar);
-                tma_load_1d(sm.dcon, rg.dcon + 3 * g0, 12u * kCB, &sm.bar);
-                tma_load_1d(sm.drgb, rg.drgb + 3 * g0, 12u * kCB, &sm.bar);
-                tma_load_1d(sm.dop, rg.dop + g0, 4u * kCB, &sm.bar);
-            }
-            // the optimiser's moments of this slice travel to L2 while the adjoint computes
-            const unsigned mv_sh = (unsigned)(kCB * mc3) * 2u;
-            prefetch_l2(static_cast<const __nv_bfloat16*>(c.m_sh) + (size_t)mc3 * g0, mv_sh);
-            prefetch_l2(static_cast<const __nv_bfloat16*>(c.v_sh) + (size_t)mc3 * g0, mv_sh);
-            prefetch_l2(reinterpret_cast<const uint4*>(c.m_attr) + g0, 16u * kCB);
-            prefetch_l2(reinterpret_cast<const uint4*>(c.v_attr) + g0, 16u * kCB);
-            prefetch_l2(c.m_pos + 3 * g0, 12u * kCB);
-            prefetch_l2(c.v_pos + 3 * g0, 12u * kCB);
-        }
+        if (tid == 0) issue_slice_copies(sm, g0, mc3, c, rg);
         mbar_wait(&sm.bar, 0, sp.spin_limit, &ctrl->status);
     } else {
-        S* shs = reinterpret_cast<S*>(sm.sh);
-        for (int e = tid; e < mc3 * ng; e += kCB) shs[e] = shg[e];
-        for (int e = tid; e < ng; e += kCB) sm.attr[e] = reinterpret_cast<const uint4*>(c.attr)[g0 + e];
-        for (int e = tid; e < 3 * ng; e += kCB) sm.pos[e] = c.pos[3 * g0 + e];
-        if (!MULTI) {
-            for (int e = tid; e < 2 * ng; e += kCB) sm.dm2[e] = rg.dm2[2 * g0 + e];
-            for (int e = tid; e < 3 * ng; e += kCB) {
-                sm.dcon[e] = rg.dcon[3 * g0 + e];
-                sm.drgb[e] = rg.drgb[3 * g0 + e];
-            }
-            for (int e = tid; e < ng; e += kCB) sm.dop[e] = rg.dop[g0 + e];
-        }
+        stage_slice_plain(sm, g0, ng, mc3, c, rg);
         __syncthreads();
     }
     // ---- phase 1: per-Gaussian adjoint (summed over the views) ----
-    if (MULTI) {
+    if constexpr (MULTI) {
         // Several views: the activation, cov3D, the cov3D -> scale / rotation chain and the sigmoid
         // do not depend on the camera and every gradient is linear in the screen gradients, so
         // one thread per Gaussian sums the views' camera-dependent parts (backward_view: SH,
@@ -535,162 +717,66 @@ __global__ void __launch_bounds__(kCB, MULTI ? 8 : 10) k_chosen_backward(const S
             sm.g_op[tid] = dops * op * (1.0f - op);   // chain 3 (:231-232) on the summed opacity gradient
         }
     } else {
-    if (tid < ng) {
-#pragma unroll
-        for (int k = 0; k < 3; k++) sm.g_pos[3 * tid + k] = sm.g_sc[3 * tid + k] = 0.f;
-#pragma unroll
-        for (int k = 0; k < 4; k++) sm.g_rot[4 * tid + k] = 0.f;
-        sm.g_op[tid] = 0.f;
-        for (int k = 0; k < 16; k++) sm.basis[k * kCB + tid] = 0.f;
-        for (int k = 0; k < 3; k++) sm.geff[k * kCB + tid] = 0.f;
-    }
-    {
-        const long long e0 = g0;
-        // the screen-gradient accumulators restart at zero for the next step
-        for (int e = tid; e < 2 * ng; e += kCB) rg.dm2[2 * e0 + e] = 0.f;
-        for (int e = tid; e < 3 * ng; e += kCB) {
-            rg.dcon[3 * e0 + e] = 0.f;
-            rg.drgb[3 * e0 + e] = 0.f;
-        }
-        for (int e = tid; e < ng; e += kCB) rg.dop[e0 + e] = 0.f;
-        if (tid < ng) {
-            BwdIn in;
-#pragma unroll
-            for (int k = 0; k < 3; k++) {
-                in.dcn[k] = sm.dcon[3 * tid + k];
-                in.drgb[k] = sm.drgb[3 * tid + k];
-            }
-            in.dm[0] = sm.dm2[2 * tid];
-            in.dm[1] = sm.dm2[2 * tid + 1];
-            in.dop = sm.dop[tid];
-            // every gradient is linear in the screen gradients: a Gaussian without any adds none
-            const bool any = in.dm[0] != 0.f || in.dm[1] != 0.f || in.dcn[0] != 0.f || in.dcn[1] != 0.f ||
-                             in.dcn[2] != 0.f || in.drgb[0] != 0.f || in.drgb[1] != 0.f || in.drgb[2] != 0.f ||
-                             in.dop != 0.f;
-            if (any) {
-#pragma unroll
-                for (int k = 0; k < 3; k++) in.p[k] = sm.pos[3 * tid + k];
-                in.act = nullptr;
-                load_attr<S>(sm.attr, tid, in.rsc, &in.rop, in.rq);
-                float shf[48];
-                if (mc3 == 48) {
-                    // this Gaussian's 96 SH bytes as six 16-byte loads
-                    const uint4* row = sm.sh + 6 * tid;
-#pragma unroll
-                    for (int qd = 0; qd < 6; qd++) {
-                        const uint4 vv = row[qd];
-                        const S* h = reinterpret_cast<const S*>(&vv);
-#pragma unroll
-                        for (int k = 0; k < 8; k++) shf[8 * qd + k] = ldf(h[k]);
-                    }
-                } else {
-                    const S* shs = reinterpret_cast<const S*>(sm.sh) + mc3 * tid;
-#pragma unroll
-                    for (int k = 0; k < 48; k++) shf[k] = k < mc3 ? ldf(shs[k]) : 0.f;
-                }
-                in.sh = shf;
-                BwdOut o;
-#pragma unroll
-                for (int k = 0; k < 3; k++) o.gp[k] = o.gs[k] = o.geff[k] = 0.f;
-#pragma unroll
-                for (int k = 0; k < 4; k++) o.gq[k] = 0.f;
-                o.gop = 0.f;
-#pragma unroll
-                for (int k = 0; k < 16; k++) o.basis[k] = 0.f;
-                backward_one(sp, in, o);
-#pragma unroll
-                for (int k = 0; k < 3; k++) {
-                    sm.g_pos[3 * tid + k] = o.gp[k];
-                    sm.g_sc[3 * tid + k] = o.gs[k];
-                }
-#pragma unroll
-                for (int k = 0; k < 4; k++) sm.g_rot[4 * tid + k] = o.gq[k];
-                sm.g_op[tid] = o.gop;
-#pragma unroll
-                for (int k = 0; k < 16; k++) sm.basis[k * kCB + tid] = o.basis[k];
-#pragma unroll
-                for (int k = 0; k < 3; k++) sm.geff[k * kCB + tid] = o.geff[k];
-            }
-        }
-    }
+        adjoint_slice(sm, sp, g0, ng, mc3, rg);
     }
     __syncthreads();
     // ---- phase 2: optimiser over this CTA's slice (and the gradients, when kept) ----
-    if (gout.g_pos) {
-        for (int e = tid; e < 3 * ng; e += kCB) {
-            gout.g_pos[3 * g0 + e] = sm.g_pos[e];
-            gout.g_sc[3 * g0 + e] = sm.g_sc[e];
-        }
-        for (int e = tid; e < 4 * ng; e += kCB) gout.g_rot[4 * g0 + e] = sm.g_rot[e];
-        for (int e = tid; e < ng; e += kCB) gout.g_op[g0 + e] = sm.g_op[e];
-        for (int e = tid; e < mc3 * ng; e += kCB) {
-            const int t = e / mc3, k = e - t * mc3;
-            gout.g_sh[(size_t)mc3 * g0 + e] = sm.gsh(t, k);
-        }
+    adam_slice(sm, sp, g0, ng, mc3, c, gout);
+}
+
+// One view, persistent and software-pipelined: each CTA walks slices blockIdx,
+// blockIdx + gridDim, ... with two staging buffers; the next slice's bulk
+// copies (and the L2 prefetch of its moments) are issued before this slice's
+// adjoint and optimiser run, so they are in flight while it computes.  A wait
+// that runs out ends the CTA (status kStatusTimeout).
+template <typename S>
+__global__ void __launch_bounds__(kCB, 6) k_chosen_backward_pipe(const StepParams* __restrict__ spp, int N, int mc3,
+                                                                 ChosenPtrs c, RGradPtrs rg, GradPtrs gout,
+                                                                 Control* ctrl) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    ChosenBwdShared<S, false>* buf = reinterpret_cast<ChosenBwdShared<S, false>*>(smem_raw);
+    const StepParams& sp = *spp;
+    if ((ctrl->status & (kStatusOverflow | kStatusTimeout)) || sp.persist->sticky_overflow) return;
+    const int tid = threadIdx.x;
+    if (blockIdx.x == 0 && tid == 0 && sp.use_adam) atomicAdd(&sp.persist->applied_steps, 1ull);
+    const long long n_slices = ((long long)N + kCB - 1) / kCB;
+    if (tid == 0) {
+        mbar_init(&buf[0].bar, 1);
+        mbar_init(&buf[1].bar, 1);
+        mbar_fence_init();
     }
-    const long long sh0 = (long long)mc3 * g0;
-    S* shw = static_cast<S*>(c.sh);
-    __nv_bfloat16* msh = static_cast<__nv_bfloat16*>(c.m_sh);
-    __nv_bfloat16* vsh = static_cast<__nv_bfloat16*>(c.v_sh);
-    const float lr_sh[8] = {sp.lr_sh, sp.lr_sh, sp.lr_sh, sp.lr_sh, sp.lr_sh, sp.lr_sh, sp.lr_sh, sp.lr_sh};
-    if (ng == kCB) {
-        // SH: 8 * mc3 chunks of 8 coefficients (16-byte aligned: the slice starts at 128 * mc3 * blockIdx
-        // bytes); the parameters are already in shared memory
-        const int nq = (kCB * mc3) / 8;
-        uint4* m4 = reinterpret_cast<uint4*>(msh + sh0);
-        uint4* v4 = reinterpret_cast<uint4*>(vsh + sh0);
-        uint4* p4 = reinterpret_cast<uint4*>(shw + sh0);
-        for (int q = tid; q < nq; q += kCB) {
-            uint4 pp = sm.sh[q], mm = m4[q], vv = v4[q];
-            float gg[8];
-#pragma unroll
-            for (int k = 0; k < 8; k++) {
-                const int e = 8 * q + k, t = e / mc3;
-                gg[k] = sm.gsh(t, e - t * mc3);
-            }
-            opt8<S>(sp, pp, mm, vv, gg, lr_sh, (unsigned)(sh0 + 8 * q), 0x5bd1e995u);
-            p4[q] = pp;
-            m4[q] = mm;
-            v4[q] = vv;
+    __syncthreads();
+    if (tid == 0 && (long long)blockIdx.x < n_slices && ((long long)blockIdx.x + 1) * kCB <= N)
+        issue_slice_copies(buf[0], (long long)blockIdx.x * kCB, mc3, c, rg);
+    int i = 0;
+    for (long long sl = blockIdx.x; sl < n_slices; sl += gridDim.x, i++) {
+        ChosenBwdShared<S, false>& sm = buf[i & 1];
+        const long long g0 = sl * kCB;
+        const int ng = (int)min((long long)kCB, (long long)N - g0);
+        if (ng == kCB) {
+            // buffer i & 1 completes once per use: its (i >> 1)-th phase
+            const bool ok = mbar_wait(&sm.bar, (unsigned)((i >> 1) & 1), sp.spin_limit, &ctrl->status);
+            if (__syncthreads_or(!ok)) break;
+        } else {
+            stage_slice_plain(sm, g0, ng, mc3, c, rg);
+            __syncthreads();
         }
-    } else {
-        const S* shs = reinterpret_cast<const S*>(sm.sh);
-        for (int e = tid; e < mc3 * ng; e += kCB) {
-            const int t = e / mc3;
-            float m = __bfloat162float(msh[sh0 + e]), v = __bfloat162float(vsh[sh0 + e]);
-            const float pn = opt_elem(sp, ldf(shs[e]), m, v, sm.gsh(t, e - t * mc3), sp.lr_sh);
-            unsigned rp, rm, rv;
-            sr_words((unsigned)(sh0 + e) ^ 0x5bd1e995u, sp.seed, rp, rm, rv);
-            shw[sh0 + e] = cvt_sr<S>(pn, rp);
-            msh[sh0 + e] = cvt_sr<__nv_bfloat16>(m, rm);
-            vsh[sh0 + e] = cvt_sr<__nv_bfloat16>(v, rv);
+        const long long nx = sl + gridDim.x;
+        if (tid == 0 && nx < n_slices && (nx + 1) * kCB <= N) {
+            fence_proxy_async();   // the other buffer's reads (two slices ago) come before the copies into it
+            issue_slice_copies(buf[(i + 1) & 1], nx * kCB, mc3, c, rg);
         }
-    }
-    // attributes: one 16-byte record per Gaussian
-    const float lra[8] = {sp.lr_scale, sp.lr_scale, sp.lr_scale, sp.lr_opac, sp.lr_rot, sp.lr_rot, sp.lr_rot,
-                          sp.lr_rot};
-    for (int t = tid; t < ng; t += kCB) {
-        const float gg[8] = {sm.g_sc[3 * t], sm.g_sc[3 * t + 1], sm.g_sc[3 * t + 2], sm.g_op[t],
-                             sm.g_rot[4 * t], sm.g_rot[4 * t + 1], sm.g_rot[4 * t + 2], sm.g_rot[4 * t + 3]};
-        uint4 pp = sm.attr[t];
-        uint4 mm = reinterpret_cast<const uint4*>(c.m_attr)[g0 + t];
-        uint4 vv = reinterpret_cast<const uint4*>(c.v_attr)[g0 + t];
-        opt8<S>(sp, pp, mm, vv, gg, lra, (unsigned)(8 * (g0 + t)), 0u);
-        reinterpret_cast<uint4*>(c.attr)[g0 + t] = pp;
-        reinterpret_cast<uint4*>(c.m_attr)[g0 + t] = mm;
-        reinterpret_cast<uint4*>(c.v_attr)[g0 + t] = vv;
-    }
-    // positions: FP32 parameters and moments
-    for (int e = tid; e < 3 * ng; e += kCB) {
-        const long long ge = 3 * g0 + e;
-        float m = c.m_pos[ge], v = c.v_pos[ge];
-        c.pos[ge] = opt_elem(sp, sm.pos[e], m, v, sm.g_pos[e], sp.lr_pos);
-        c.m_pos[ge] = m;
-        c.v_pos[ge] = v;
+        adjoint_slice(sm, sp, g0, ng, mc3, rg);
+        __syncthreads();
+        adam_slice(sm, sp, g0, ng, mc3, c, gout);
+        __syncthreads();
     }
 }
 
 inline int grid_for(long long n, int t) { return (int)((n + t - 1) / t); }
+
+// One view's adjoint + Adam runs as the persistent, software-pipelined kernel.
+constexpr bool kPipelinedAdjoint = true;
 
 }  // namespace
 
@@ -725,45 +811,36 @@ cudaError_t launch_chosen_preprocess(cudaStream_t st, const StepParams* sp, int 
     return cudaGetLastError();
 }
 
-namespace {
-template <int PPT>
-cudaError_t fwd_multi(cudaStream_t st, const StepParams* views, int n_views, unsigned n_tiles,
-                      const unsigned* ranges, const unsigned* order, const unsigned* vals, ScreenPtrs s, PixelPtrs px,
-                      Control* ctrl) {
-    static int per_sm = 0;
-    if (!per_sm) {
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_raster_fwd<true, FastBlend, true, PPT>, 256 / PPT,
-                                                          0) != cudaSuccess ||
-            per_sm < 1)
-            per_sm = 1;
-    }
-    k_raster_fwd<true, FastBlend, true, PPT><<<per_sm * sm_count(), 256 / PPT, 0, st>>>(views, ranges, order, vals, s, px,
-                                                                                ctrl, n_views, n_tiles);
-    return cudaGetLastError();
-}
-}  // namespace
-
 cudaError_t launch_raster_fwd_fast_multi(cudaStream_t st, const StepParams* views, int n_views, unsigned n_tiles,
                                          const unsigned* ranges, const unsigned* order, const unsigned* vals,
-                                         ScreenPtrs s, PixelPtrs px, Control* ctrl, int ppt) {
+                                         ScreenPtrs s, PixelPtrs px, Control* ctrl, int ppt, int batch) {
     if (n_tiles == 0) return cudaSuccess;
     // persistent: as many CTAs as fit resident
-    if (ppt == 1) return fwd_multi<1>(st, views, n_views, n_tiles, ranges, order, vals, s, px, ctrl);
-    if (ppt == 4) return fwd_multi<4>(st, views, n_views, n_tiles, ranges, order, vals, s, px, ctrl);
-    return fwd_multi<2>(st, views, n_views, n_tiles, ranges, order, vals, s, px, ctrl);
+    return with_ppt_batch(ppt, batch, [&](auto P, auto Bt) {
+        constexpr int kP = decltype(P)::value, kB = decltype(Bt)::value;
+        static int per_sm = 0;
+        if (!per_sm) {
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_raster_fwd<true, FastBlend, true, kP, kB>,
+                                                              256 / kP, 0) != cudaSuccess ||
+                per_sm < 1)
+                per_sm = 1;
+        }
+        k_raster_fwd<true, FastBlend, true, kP, kB><<<per_sm * sm_count(), 256 / kP, 0, st>>>(
+            views, ranges, order, vals, s, px, ctrl, n_views, n_tiles);
+        return cudaGetLastError();
+    });
 }
 
 cudaError_t launch_raster_fwd_fast(cudaStream_t st, const StepParams* sp, int num_tiles, const unsigned* ranges,
                                    const unsigned* order, const unsigned* vals, ScreenPtrs s, PixelPtrs px,
-                                   Control* ctrl, int ppt) {
+                                   Control* ctrl, int ppt, int batch) {
     if (num_tiles <= 0) return cudaSuccess;
-    if (ppt == 1)
-        k_raster_fwd<true, FastBlend, false, 1><<<num_tiles, 256, 0, st>>>(sp, ranges, order, vals, s, px, ctrl);
-    else if (ppt == 4)
-        k_raster_fwd<true, FastBlend, false, 4><<<num_tiles, 64, 0, st>>>(sp, ranges, order, vals, s, px, ctrl);
-    else
-        k_raster_fwd<true, FastBlend, false, 2><<<num_tiles, 128, 0, st>>>(sp, ranges, order, vals, s, px, ctrl);
-    return cudaGetLastError();
+    return with_ppt_batch(ppt, batch, [&](auto P, auto Bt) {
+        constexpr int kP = decltype(P)::value, kB = decltype(Bt)::value;
+        k_raster_fwd<true, FastBlend, false, kP, kB><<<num_tiles, 256 / kP, 0, st>>>(sp, ranges, order, vals, s, px,
+                                                                                    ctrl);
+        return cudaGetLastError();
+    });
 }
 
 cudaError_t launch_chosen_backward_adam(cudaStream_t st, const StepParams* sp, int N, int mc3, bool fp16,
@@ -784,6 +861,21 @@ cudaError_t launch_chosen_backward_adam(cudaStream_t st, const StepParams* sp, i
     if (n_views > 1) {
         if (fp16) k_chosen_backward<__half, true><<<grid, kCB, smem, st>>>(sp, N, mc3, c, rg, g, ctrl, n_views);
         else k_chosen_backward<__nv_bfloat16, true><<<grid, kCB, smem, st>>>(sp, N, mc3, c, rg, g, ctrl, n_views);
+    } else if (kPipelinedAdjoint) {
+        // persistent: the CTAs that fit resident (two staging buffers each), at most one per slice
+        const int smem2 = 2 * smem1;
+        static std::atomic<unsigned long long> pipe_done[2];
+        cudaError_t x = set_smem_once(pipe_done[0], k_chosen_backward_pipe<__half>, smem2);
+        if (x == cudaSuccess) x = set_smem_once(pipe_done[1], k_chosen_backward_pipe<__nv_bfloat16>, smem2);
+        if (x != cudaSuccess) return x;
+        static int per_sm = 0;
+        if (!per_sm && (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_chosen_backward_pipe<__nv_bfloat16>,
+                                                                      kCB, smem2) != cudaSuccess ||
+                        per_sm < 1))
+            per_sm = 1;
+        const int pgrid = std::min(grid, per_sm * sm_count());
+        if (fp16) k_chosen_backward_pipe<__half><<<pgrid, kCB, smem2, st>>>(sp, N, mc3, c, rg, g, ctrl);
+        else k_chosen_backward_pipe<__nv_bfloat16><<<pgrid, kCB, smem2, st>>>(sp, N, mc3, c, rg, g, ctrl);
     } else {
         if (fp16) k_chosen_backward<__half, false><<<grid, kCB, smem, st>>>(sp, N, mc3, c, rg, g, ctrl, 1);
         else k_chosen_backward<__nv_bfloat16, false><<<grid, kCB, smem, st>>>(sp, N, mc3, c, rg, g, ctrl, 1);

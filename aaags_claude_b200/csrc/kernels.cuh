@@ -2,9 +2,26 @@
 #pragma once
 
 #include <cuda_runtime.h>
+
+#include <type_traits>
+
 #include "common.cuh"
 
 namespace gs3d {
+
+// Calls f(PPT, BATCH) with the rasterisers' compile-time pixels per thread
+// (1, 2, 4; anything else: 2) and staging batch (64, 128, 256; anything else: 128).
+template <class F>
+cudaError_t with_ppt_batch(int ppt, int batch, F&& f) {
+    auto pick_batch = [&](auto P) -> cudaError_t {
+        if (batch == 64) return f(P, std::integral_constant<int, 64>{});
+        if (batch == 256) return f(P, std::integral_constant<int, 256>{});
+        return f(P, std::integral_constant<int, 128>{});
+    };
+    if (ppt == 1) return pick_batch(std::integral_constant<int, 1>{});
+    if (ppt == 4) return pick_batch(std::integral_constant<int, 4>{});
+    return pick_batch(std::integral_constant<int, 2>{});
+}
 
 // Model parameters in the reference layouts: raw (training) or activated (render).
 struct ModelPtrs {
@@ -154,19 +171,20 @@ cudaError_t launch_chosen_preprocess(cudaStream_t st, const StepParams* sp, int 
 // Forward rasteriser with the fast-exp blend decision and fused L1.
 cudaError_t launch_raster_fwd_fast(cudaStream_t st, const StepParams* sp, int num_tiles, const unsigned* ranges,
                                    const unsigned* order, const unsigned* vals, ScreenPtrs s, PixelPtrs px,
-                                   Control* ctrl, int ppt = 2);
+                                   Control* ctrl, int ppt = 2, int batch = 128);
 // One persistent launch over all tiles of n_views views (views = their
 // parameter array, order = all global tiles, heavy first).
 cudaError_t launch_raster_fwd_fast_multi(cudaStream_t st, const StepParams* views, int n_views, unsigned n_tiles,
                                          const unsigned* ranges, const unsigned* order, const unsigned* vals,
-                                         ScreenPtrs s, PixelPtrs px, Control* ctrl, int ppt = 2);
+                                         ScreenPtrs s, PixelPtrs px, Control* ctrl, int ppt = 2, int batch = 128);
 cudaError_t launch_raster_bwd_fast_multi(cudaStream_t st, const StepParams* views, int n_views, unsigned n_tiles,
                                          const unsigned* ranges, const unsigned* order, const unsigned* vals,
-                                         ScreenPtrs s, PixelPtrs px, RGradPtrs g, Control* ctrl, int ppt = 2);
+                                         ScreenPtrs s, PixelPtrs px, RGradPtrs g, Control* ctrl, int ppt = 2,
+                                         int batch = 128);
 // Backward rasteriser deciding acceptance like launch_raster_fwd_fast.
 cudaError_t launch_raster_bwd_fast(cudaStream_t st, const StepParams* sp, int num_tiles, const unsigned* ranges,
                                    const unsigned* order, const unsigned* vals, ScreenPtrs s, PixelPtrs px,
-                                   RGradPtrs g, Control* ctrl, int ppt = 2);
+                                   RGradPtrs g, Control* ctrl, int ppt = 2, int batch = 128);
 // Per-Gaussian adjoint fused with Adam (stochastic rounding into the 16-bit
 // parameters and BF16 moments); zeroes the screen-gradient accumulators.
 // With g.g_pos != NULL the FP32 raw-parameter gradients are stored too.
@@ -216,12 +234,15 @@ cudaError_t launch_bin_arrays_e3(cudaStream_t st, const StepParams* sp, int N, S
 cudaError_t launch_raster_e3(cudaStream_t st, const StepParams* sp, int num_tiles, const unsigned* ranges,
                              const unsigned* order, const unsigned* vals, E3Ptrs e, PixelPtrs px, Control* ctrl);
 // order: tile permutation (heavy first) or NULL for row-major
+// batch: the records staged per round (64, 128, 256) in the train step's launches (fused loss /
+// FROM_SIGN); the stage API's launches stage 128.
 cudaError_t launch_raster_fwd_plain(cudaStream_t st, const StepParams* sp, int num_tiles, bool fused_loss,
                                     const unsigned* ranges, const unsigned* order, const unsigned* vals,
-                                    ScreenPtrs s, PixelPtrs px, Control* ctrl, int ppt = 2);
+                                    ScreenPtrs s, PixelPtrs px, Control* ctrl, int ppt = 2, int batch = 128);
 cudaError_t launch_raster_bwd_plain(cudaStream_t st, const StepParams* sp, int num_tiles, bool from_sign,
                                     const unsigned* ranges, const unsigned* order, const unsigned* vals,
-                                    ScreenPtrs s, PixelPtrs px, RGradPtrs g, Control* ctrl, int ppt = 2);
+                                    ScreenPtrs s, PixelPtrs px, RGradPtrs g, Control* ctrl, int ppt = 2,
+                                    int batch = 128);
 // Stored-list raster backward (memory comparison with the recompute backward):
 // each pixel's contributors (Gaussian, alpha bits) are replayed into
 // list[offset[pix] .. offset[pix] + n_contrib[pix]), then walked back to front

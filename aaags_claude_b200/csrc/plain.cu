@@ -75,6 +75,7 @@ struct EmitShared {
     int excl[kBlock];
     int rect[kBlock];      // xmin | ymin << 16
     int width[kBlock];
+    float winv[kBlock];    // 1 / width (round to nearest): the row of a pair without an integer division
     int limit[kBlock];     // pairs actually emitted (rect area, <= count)
     unsigned depth[kBlock];
     unsigned gid[kBlock];  // Gaussian index written as the pair's value
@@ -109,6 +110,7 @@ __device__ __forceinline__ void scan_and_emit(EmitShared& sm, int blk, unsigned 
     sm.excl[tid] = incl - cnt;
     sm.rect[tid] = rx | (ry << 16);
     sm.width[tid] = rw;
+    sm.winv[tid] = 1.0f / (float)rw;
     sm.limit[tid] = emit;
     sm.depth[tid] = dbits;
     sm.gid[tid] = gid;
@@ -140,8 +142,13 @@ __device__ __forceinline__ void scan_and_emit(EmitShared& sm, int blk, unsigned 
         if (local >= sm.limit[lo] || dst >= pr.capacity) continue;
         const int w = sm.width[lo];
         const int r = sm.rect[lo];
-        const int x = (r & 0xffff) + local % w;
-        const int y = (r >> 16) + local / w;
+        // local / w from the rounded reciprocal: for local < 2^23 the product is within one of the
+        // quotient, and one correction step each way makes it exact
+        int row = __float2int_rz((float)local * sm.winv[lo]);
+        if ((row + 1) * w <= local) row++;
+        else if (row * w > local) row--;
+        const int x = (r & 0xffff) + (local - row * w);
+        const int y = (r >> 16) + row;
         const unsigned tile = sm.tbase[lo] + (unsigned)(y * sm.gx[lo] + x);
         if (pr.tiles32) {
             pr.tiles32[dst] = tile;
@@ -779,21 +786,19 @@ cudaError_t launch_raster_e3(cudaStream_t st, const StepParams* sp, int num_tile
 
 cudaError_t launch_raster_fwd_plain(cudaStream_t st, const StepParams* sp, int num_tiles, bool fused_loss,
                                     const unsigned* ranges, const unsigned* order, const unsigned* vals,
-                                    ScreenPtrs s, PixelPtrs px, Control* ctrl, int ppt) {
+                                    ScreenPtrs s, PixelPtrs px, Control* ctrl, int ppt, int batch) {
     if (num_tiles <= 0) return cudaSuccess;
-#define GS3D_FWD(FL, P) \
-    k_raster_fwd<FL, ExactBlend, false, P><<<num_tiles, 256 / P, 0, st>>>(sp, ranges, order, vals, s, px, ctrl)
-    if (fused_loss) {
-        if (ppt == 1) GS3D_FWD(true, 1);
-        else if (ppt == 4) GS3D_FWD(true, 4);
-        else GS3D_FWD(true, 2);
-    } else {
-        if (ppt == 1) GS3D_FWD(false, 1);
-        else if (ppt == 4) GS3D_FWD(false, 4);
-        else GS3D_FWD(false, 2);
-    }
-#undef GS3D_FWD
-    return cudaGetLastError();
+    if (!fused_loss) batch = 128;   // renders and the stage API
+    return with_ppt_batch(ppt, batch, [&](auto P, auto Bt) {
+        constexpr int kP = decltype(P)::value, kB = decltype(Bt)::value;
+        if (fused_loss)
+            k_raster_fwd<true, ExactBlend, false, kP, kB><<<num_tiles, 256 / kP, 0, st>>>(sp, ranges, order, vals, s,
+                                                                                         px, ctrl);
+        else
+            k_raster_fwd<false, ExactBlend, false, kP, kFwdBatch><<<num_tiles, 256 / kP, 0, st>>>(
+                sp, ranges, order, vals, s, px, ctrl);
+        return cudaGetLastError();
+    });
 }
 
 namespace {

@@ -87,26 +87,26 @@ constexpr int kBwdBatch = 128;
 // parameters); a CTA takes the next entry of `order` from a work counter and
 // renders the tile with its view's camera and pixel slice.  The screen
 // gradients then belong to (view, Gaussian) entries: vals holds view * N + i.
-template <bool FROM_SIGN, class Accept, bool MULTI = false, int PPT = 2>
+template <bool FROM_SIGN, class Accept, bool MULTI = false, int PPT = 2, int BATCH = kBwdBatch>
 __global__ void __launch_bounds__(256 / PPT) k_raster_bwd(const StepParams* __restrict__ spp,
                                                             const unsigned* __restrict__ ranges,
                                                             const unsigned* __restrict__ order,
                                                             const unsigned* __restrict__ vals, ScreenPtrs s,
                                                             PixelPtrs px, RGradPtrs g, Control* ctrl,
                                                             int n_views = 1, unsigned n_tiles = 0) {
-    __shared__ float4 s_r0[kBwdBatch];
-    __shared__ float4 s_r1[kBwdBatch];
-    __shared__ float2 s_bt[kBwdBatch];   // (blue, skip threshold): one 8-byte load per Gaussian
-    __shared__ unsigned s_idx[kBwdBatch];
+    __shared__ float4 s_r0[BATCH];
+    __shared__ float4 s_r1[BATCH];
+    __shared__ float2 s_bt[BATCH];   // (blue, skip threshold): one 8-byte load per Gaussian
+    __shared__ unsigned s_idx[BATCH];
     // r, g, b, S_1, S_x, S_y, S_xx, S_xy, S_yy; rows padded by one word so that the
     // eight lanes adding values 0..7 of one Gaussian hit eight different banks
-    __shared__ float s_acc[9][kBwdBatch + 1];
+    __shared__ float s_acc[9][BATCH + 1];
     __shared__ unsigned s_maxlast;
     __shared__ unsigned s_next;
     constexpr int kBwdThreads = 256 / PPT;
     constexpr int kNW = kBwdThreads / 32;
-    __shared__ unsigned char s_mask[kBwdBatch];       // warps whose strip the Gaussian can reach
-    __shared__ unsigned char s_list[kNW][kBwdBatch];  // per warp: its batch entries, ascending
+    __shared__ unsigned char s_mask[BATCH];       // warps whose strip the Gaussian can reach
+    __shared__ unsigned char s_list[kNW][BATCH];  // per warp: its batch entries, ascending
     if (FROM_SIGN && ((ctrl->status & kStatusOverflow) || spp->persist->sticky_overflow)) return;
     for (int iter = 0;; iter++) {
     int tile;
@@ -180,9 +180,9 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_bwd(const StepParams* __re
     const float wx0 = (float)(tx * kTile), wx1 = wx0 + (float)(kTile - 1), ty0 = (float)(ty * kTile);
     // batches [bs, be) walked from the back; the first one ends at maxlast
     for (unsigned be = maxlast; be > rs;) {
-        const unsigned bs = (be - rs > (unsigned)kBwdBatch) ? be - kBwdBatch : rs;
+        const unsigned bs = (be - rs > (unsigned)BATCH) ? be - BATCH : rs;
 #pragma unroll
-        for (int e = threadIdx.x; e < kBwdBatch; e += kBwdThreads) {
+        for (int e = threadIdx.x; e < BATCH; e += kBwdThreads) {
             const unsigned j = bs + (unsigned)e;
             if (j < be) {
                 const unsigned gi = vals[j];
@@ -203,8 +203,9 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_bwd(const StepParams* __re
         // this warp only needs the entries below its own last contributor
         const int kstart = (int)(min(be, wlast) - min(bs, wlast)) - 1;
         const int nl = warp_list(s_mask, kstart + 1, warp, s_list[warp]);
-        for (int i = nl - 1; i >= 0; i--) {
-            const int k = s_list[warp][i];
+        // this thread's contributions to batch entry k (walked back to front): gv = d_rgb and the
+        // moments S_1, S_x, S_y, S_xx, S_xy of its pixels, t2 = S_yy; returns whether any pixel blended
+        auto item = [&](int k, float gv[8], float& s_yy) -> bool {
             const unsigned jj = bs + (unsigned)k;
             const float4 a = s_r0[k];
             const float4 c = s_r1[k];
@@ -245,19 +246,45 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_bwd(const StepParams* __re
                     }
                 }
             }
-            if (__any_sync(0xffffffffu, contrib)) {
-                const float tx0 = t0 * dx;
-                const float gv[8] = {gr, gg, gb, t0, tx0, t1, tx0 * dx, t1 * dx};
+            const float tx0 = t0 * dx;
+            gv[0] = gr;
+            gv[1] = gg;
+            gv[2] = gb;
+            gv[3] = t0;
+            gv[4] = tx0;
+            gv[5] = t1;
+            gv[6] = tx0 * dx;
+            gv[7] = t1 * dx;
+            s_yy = t2;
+            return contrib;
+        };
+        // two entries per round: their 16 + 2 sums reduce in one butterfly each (18 shuffles
+        // instead of 28 for two separate 8 + 1 reductions)
+        for (int i = nl - 1; i >= 0; i -= 2) {
+            const int kA = s_list[warp][i];
+            float gv[16], tA, tB = 0.0f;
+            const bool cA = item(kA, gv, tA);
+            if (i >= 1) {   // warp-uniform: nl is the warp's list length
+                const int kB = s_list[warp][i - 1];
+                const bool cB = item(kB, gv + 8, tB);
+                if (__any_sync(0xffffffffu, cA || cB)) {
+                    int idx;
+                    const float s16 = warp_sum16(gv, &idx);
+                    const float s2 = warp_sum2(tA, tB);
+                    if ((lane & 1) == 0 && s16 != 0.0f) atomicAdd(&s_acc[idx & 7][idx < 8 ? kA : kB], s16);
+                    if ((lane & 15) == 0 && s2 != 0.0f) atomicAdd(&s_acc[8][lane < 16 ? kA : kB], s2);
+                }
+            } else if (__any_sync(0xffffffffu, cA)) {
                 int idx;
                 const float s8 = warp_sum8(gv, &idx);
-                const float s9 = warp_sum(t2);
-                if ((lane & 3) == 0 && s8 != 0.0f) atomicAdd(&s_acc[idx][k], s8);
-                if (lane == 1 && s9 != 0.0f) atomicAdd(&s_acc[8][k], s9);
+                const float s9 = warp_sum(tA);
+                if ((lane & 3) == 0 && s8 != 0.0f) atomicAdd(&s_acc[idx][kA], s8);
+                if (lane == 1 && s9 != 0.0f) atomicAdd(&s_acc[8][kA], s9);
             }
         }
         __syncthreads();
 #pragma unroll
-        for (int e = threadIdx.x; e < kBwdBatch; e += kBwdThreads) {
+        for (int e = threadIdx.x; e < BATCH; e += kBwdThreads) {
             if (bs + (unsigned)e < be) {
                 const size_t gi = s_idx[e];   // (view, Gaussian) entry: 3 * gi can pass 2^32
                 float* const dst[9] = {&g.drgb[3 * gi], &g.drgb[3 * gi + 1], &g.drgb[3 * gi + 2], &g.dop[gi],
@@ -398,55 +425,50 @@ int resident_ctas(F kernel, int threads) {
     return n;
 }
 
-template <bool FROM_SIGN, class Accept, int PPT>
-cudaError_t bwd_single(cudaStream_t st, const StepParams* sp, int num_tiles, const unsigned* ranges,
-                       const unsigned* order, const unsigned* vals, ScreenPtrs s, PixelPtrs px, RGradPtrs g,
-                       Control* ctrl) {
-    k_raster_bwd<FROM_SIGN, Accept, false, PPT><<<num_tiles, 256 / PPT, 0, st>>>(sp, ranges, order, vals, s, px, g,
-                                                                                ctrl);
-    return cudaGetLastError();
-}
-
-template <int PPT>
-cudaError_t bwd_multi(cudaStream_t st, const StepParams* views, int n_views, unsigned n_tiles,
-                      const unsigned* ranges, const unsigned* order, const unsigned* vals, ScreenPtrs s, PixelPtrs px,
-                      RGradPtrs g, Control* ctrl) {
-    static int per_sm = 0;
-    if (!per_sm) per_sm = resident_ctas(k_raster_bwd<true, FastAccept, true, PPT>, 256 / PPT);
-    k_raster_bwd<true, FastAccept, true, PPT><<<per_sm * sm_count(), 256 / PPT, 0, st>>>(views, ranges, order, vals, s, px,
-                                                                                 g, ctrl, n_views, n_tiles);
-    return cudaGetLastError();
-}
-
 }  // namespace
 
 cudaError_t launch_raster_bwd_plain(cudaStream_t st, const StepParams* sp, int num_tiles, bool from_sign,
                                     const unsigned* ranges, const unsigned* order, const unsigned* vals,
-                                    ScreenPtrs s, PixelPtrs px, RGradPtrs g, Control* ctrl, int ppt) {
+                                    ScreenPtrs s, PixelPtrs px, RGradPtrs g, Control* ctrl, int ppt, int batch) {
     if (num_tiles <= 0) return cudaSuccess;
-#define GS3D_BWD(FS, P) bwd_single<FS, PlainAccept, P>(st, sp, num_tiles, ranges, order, vals, s, px, g, ctrl)
-    if (from_sign) return ppt == 1 ? GS3D_BWD(true, 1) : ppt == 4 ? GS3D_BWD(true, 4) : GS3D_BWD(true, 2);
-    return ppt == 1 ? GS3D_BWD(false, 1) : ppt == 4 ? GS3D_BWD(false, 4) : GS3D_BWD(false, 2);
-#undef GS3D_BWD
+    if (!from_sign) batch = 128;   // the stage API (explicit d_image)
+    return with_ppt_batch(ppt, batch, [&](auto P, auto Bt) {
+        constexpr int kP = decltype(P)::value, kB = decltype(Bt)::value;
+        if (from_sign)
+            k_raster_bwd<true, PlainAccept, false, kP, kB><<<num_tiles, 256 / kP, 0, st>>>(sp, ranges, order, vals, s,
+                                                                                          px, g, ctrl);
+        else
+            k_raster_bwd<false, PlainAccept, false, kP, kBwdBatch><<<num_tiles, 256 / kP, 0, st>>>(
+                sp, ranges, order, vals, s, px, g, ctrl);
+        return cudaGetLastError();
+    });
 }
 
 cudaError_t launch_raster_bwd_fast(cudaStream_t st, const StepParams* sp, int num_tiles, const unsigned* ranges,
                                    const unsigned* order, const unsigned* vals, ScreenPtrs s, PixelPtrs px,
-                                   RGradPtrs g, Control* ctrl, int ppt) {
+                                   RGradPtrs g, Control* ctrl, int ppt, int batch) {
     if (num_tiles <= 0) return cudaSuccess;
-#define GS3D_BWD(P) bwd_single<true, FastAccept, P>(st, sp, num_tiles, ranges, order, vals, s, px, g, ctrl)
-    return ppt == 1 ? GS3D_BWD(1) : ppt == 4 ? GS3D_BWD(4) : GS3D_BWD(2);
-#undef GS3D_BWD
+    return with_ppt_batch(ppt, batch, [&](auto P, auto Bt) {
+        constexpr int kP = decltype(P)::value, kB = decltype(Bt)::value;
+        k_raster_bwd<true, FastAccept, false, kP, kB><<<num_tiles, 256 / kP, 0, st>>>(sp, ranges, order, vals, s, px,
+                                                                                      g, ctrl);
+        return cudaGetLastError();
+    });
 }
 
 cudaError_t launch_raster_bwd_fast_multi(cudaStream_t st, const StepParams* views, int n_views, unsigned n_tiles,
                                          const unsigned* ranges, const unsigned* order, const unsigned* vals,
-                                         ScreenPtrs s, PixelPtrs px, RGradPtrs g, Control* ctrl, int ppt) {
+                                         ScreenPtrs s, PixelPtrs px, RGradPtrs g, Control* ctrl, int ppt, int batch) {
     if (n_tiles == 0) return cudaSuccess;
     // persistent: as many CTAs as fit resident
-#define GS3D_BWD(P) bwd_multi<P>(st, views, n_views, n_tiles, ranges, order, vals, s, px, g, ctrl)
-    return ppt == 1 ? GS3D_BWD(1) : ppt == 4 ? GS3D_BWD(4) : GS3D_BWD(2);
-#undef GS3D_BWD
+    return with_ppt_batch(ppt, batch, [&](auto P, auto Bt) {
+        constexpr int kP = decltype(P)::value, kB = decltype(Bt)::value;
+        static int per_sm = 0;
+        if (!per_sm) per_sm = resident_ctas(k_raster_bwd<true, FastAccept, true, kP, kB>, 256 / kP);
+        k_raster_bwd<true, FastAccept, true, kP, kB><<<per_sm * sm_count(), 256 / kP, 0, st>>>(
+            views, ranges, order, vals, s, px, g, ctrl, n_views, n_tiles);
+        return cudaGetLastError();
+    });
 }
 
 }  // namespace gs3d

@@ -23,10 +23,12 @@ namespace {
 // (band_rows: the rows of the tile's columns inside its alpha >= 1/255
 // ellipse); each warp walks its own compacted list of the batch; the CTA
 // stops once every pixel saturated.  Optional fused L1 (sign byte per pixel,
-// double-precision loss sum).
+// double-precision loss sum); with it (a train step) the contributor counts
+// are not kept, the backward starts from each pixel's last contributor.
 //
 // PPT (pixels per thread: 1, 2 or 4) sets the threads per tile (256 / PPT)
-// and each warp's strip (16 x 2*PPT rows); the results do not depend on it.
+// and each warp's strip (16 x 2*PPT rows); BATCH (64, 128 or 256) the records
+// staged per round.  The results depend on neither.
 constexpr int kFwdBatch = 128;
 
 //
@@ -36,20 +38,20 @@ constexpr int kFwdBatch = 128;
 // by its global id and renders it with that view's camera into the view's
 // slice of the concatenated pixel buffers.  The fused loss adds each view's
 // sum weighted by its inv_n.
-template <bool FUSED_LOSS, class Blend, bool MULTI = false, int PPT = 2>
+template <bool FUSED_LOSS, class Blend, bool MULTI = false, int PPT = 2, int BATCH = kFwdBatch>
 __global__ void __launch_bounds__(256 / PPT) k_raster_fwd(const StepParams* __restrict__ spp,
                                                             const unsigned* __restrict__ ranges,
                                                             const unsigned* __restrict__ order,
                                                             const unsigned* __restrict__ vals, ScreenPtrs s,
                                                             PixelPtrs px, Control* ctrl, int n_views = 1,
                                                             unsigned n_tiles = 0) {
-    __shared__ float4 s_r0[kFwdBatch];
-    __shared__ float4 s_r1[kFwdBatch];
-    __shared__ float2 s_bt[kFwdBatch];   // (blue, skip threshold): one 8-byte load per Gaussian
+    __shared__ float4 s_r0[BATCH];
+    __shared__ float4 s_r1[BATCH];
+    __shared__ float2 s_bt[BATCH];   // (blue, skip threshold): one 8-byte load per Gaussian
     constexpr int kFwdThreads = 256 / PPT;
     constexpr int kNW = kFwdThreads / 32;
-    __shared__ unsigned char s_mask[kFwdBatch];       // warps whose strip the Gaussian can reach
-    __shared__ unsigned char s_list[kNW][kFwdBatch];  // per warp: its batch entries, ascending
+    __shared__ unsigned char s_mask[BATCH];       // warps whose strip the Gaussian can reach
+    __shared__ unsigned char s_list[kNW][BATCH];  // per warp: its batch entries, ascending
     __shared__ double s_loss[kFwdThreads / 32];
     __shared__ unsigned s_next;
     for (int iter = 0;; iter++) {
@@ -99,13 +101,13 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_fwd(const StepParams* __re
         last[p] = 0;
         done[p] = !(x < W && y < H);
     }
-    for (unsigned b = rs; b < re; b += kFwdBatch) {
+    for (unsigned b = rs; b < re; b += BATCH) {
         bool all_done = true;
 #pragma unroll
         for (int p = 0; p < PPT; p++) all_done = all_done && done[p];
         if (__syncthreads_count(all_done) == kFwdThreads) break;
 #pragma unroll
-        for (int e = threadIdx.x; e < kFwdBatch; e += kFwdThreads) {
+        for (int e = threadIdx.x; e < BATCH; e += kFwdThreads) {
             const unsigned j = b + (unsigned)e;
             if (j < re) {
                 const unsigned g = vals[j];
@@ -121,7 +123,7 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_fwd(const StepParams* __re
             }
         }
         __syncthreads();
-        const int nb = (int)min((unsigned)kFwdBatch, re - b);
+        const int nb = (int)min((unsigned)BATCH, re - b);
         const int nl = warp_list(s_mask, nb, warp, s_list[warp]);
         for (int i = 0; i < nl; i++) {
             bool thread_done = true;
@@ -161,7 +163,7 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_fwd(const StepParams* __re
                     C[p][2] += bt.x * alpha * T[p];
                 }
                 T[p] = test_T;
-                cnt[p]++;
+                if (!FUSED_LOSS) cnt[p]++;   // a train step's backward needs only the last index
                 last[p] = b + (unsigned)k + 1u;
             }
         }
@@ -180,7 +182,7 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_fwd(const StepParams* __re
             px.image[3 * pix + 1] = o1;
             px.image[3 * pix + 2] = o2;
             if (px.T_final) px.T_final[pix] = T[p];
-            if (px.n_contrib) px.n_contrib[pix] = cnt[p];
+            if (!FUSED_LOSS && px.n_contrib) px.n_contrib[pix] = cnt[p];
             if (px.last_j) px.last_j[pix] = last[p];
             if (FUSED_LOSS) {
                 // loss.cpp:8-14: diff = rendered - gt, sign gradient +-1/n

@@ -29,6 +29,7 @@ STAT_TOTAL_PAIRS, STAT_PAIR_CAPACITY, STAT_KERNELS_LAST, STAT_SORT_PASSES, STAT_
 STAT_NUM_GAUSSIANS = 9
 STAT_SCREEN_GAUSSIANS = 10
 STAT_GRAPH_CAPTURES = 11
+STAT_FWD_BATCH, STAT_BWD_BATCH = 12, 13
 STAT_FWD_PPT, STAT_BWD_PPT = 7, 8
 FORM_PLAIN_FP32, FORM_BF16, FORM_FP16 = 0, 1, 2
 OPT_SORT = 7
@@ -36,6 +37,7 @@ OPT_KEEP_GRADIENTS = 8
 OPT_AUTOTUNE = 9
 OPT_DENSITY_SEED = 10
 OPT_RASTER_PPT = 11
+OPT_RASTER_BATCH = 12
 SORT_DEPTH_FIRST, SORT_FULL_KEY = 0, 1
 
 _f = ctypes.POINTER(ctypes.c_float)

@@ -320,6 +320,7 @@ def max_over_ranks(values, dist, device: str) -> list:
 
 # ---------------------------------------------------------------- our arm
 FORMS = {"plain": 0, "bf16": 1, "fp16": 2}
+TUNE_STEPS = 10   # the library autotuner's trial steps per workload shape (6 pixels-per-thread, 4 batch)
 
 
 def _measure_form(a, ctx, form, w, cam, cfg, tc, gt_dev, gt_pin, local, dist):
@@ -334,14 +335,15 @@ def _measure_form(a, ctx, form, w, cam, cfg, tc, gt_dev, gt_pin, local, dist):
     it = 0
     loss0 = ctx.train_step(cam, None, cfg, tc, it, gt_device_ptr=gt_dev.data_ptr())   # sizes the pair buffers
     it += 1
-    for _ in range(max(a.warmup, 3) + (6 if a.autotune else 0)):   # the autotuner's 6 trial steps first
+    for _ in range(max(a.warmup, 3) + (TUNE_STEPS if a.autotune else 0)):   # the autotuner's trial steps first
         ctx.train_step(cam, None, cfg, tc, it, want_loss=False, gt_device_ptr=gt_dev.data_ptr())
         it += 1
     ctx.synchronize()
     r = {"form": form, "loss_first": loss0, "tile_pairs": ctx.stat(gs3d.STAT_TOTAL_PAIRS),
          "sort_passes": ctx.stat(gs3d.STAT_SORT_PASSES),
          "raster_pixels_per_thread": {"forward": ctx.stat(gs3d.STAT_FWD_PPT), "backward": ctx.stat(gs3d.STAT_BWD_PPT),
-                                      "autotuned": bool(a.autotune)}}
+                                      "autotuned": bool(a.autotune)},
+         "raster_staging_batch": {"forward": ctx.stat(gs3d.STAT_FWD_BATCH), "backward": ctx.stat(gs3d.STAT_BWD_BATCH)}}
     # ---- value: inputs resident in HBM, graph replay, CUDA events on the library stream ----
     clocks = ClockSampler(_bus_id(local))
     if dist:
@@ -430,6 +432,7 @@ def _summary(a, r, world, X, N, T, depth_first, peak):
         "loss_first": r["loss_first"], "loss_last": r["loss_last"], "clocks": r["clocks"],
         "cuda_graph": r["graph"], "sort_passes": passes,
         "raster_pixels_per_thread": r["raster_pixels_per_thread"],
+        "raster_staging_batch": r["raster_staging_batch"],
     }
 
 
@@ -494,7 +497,8 @@ def run_ours(a) -> int:
                        "arithmetic": "FP32 blending, transmittance and gradients",
                        "l2": "working set ~1.6 GB per step > 126 MB L2 (no flush needed)",
                        "parallelism": f"replicas x{world}", "cuda_graph": head["cuda_graph"],
-                       "raster_pixels_per_thread": head["raster_pixels_per_thread"]},
+                       "raster_pixels_per_thread": head["raster_pixels_per_thread"],
+                       "raster_staging_batch": head["raster_staging_batch"]},
             "mpix_per_s": head["mpix_per_s"],
             "e2e": head["e2e"],
             "gpu_launches": head["gpu_launches"],
@@ -509,7 +513,7 @@ def run_ours(a) -> int:
             p = summ["plain"]
             line["plain_fp32"] = {k: p[k] for k in ("value", "ms_per_step", "mpix_per_s", "e2e", "gpu_launches",
                                                     "tile_pairs", "stage_ms", "roofline", "clocks",
-                                                    "raster_pixels_per_thread")}
+                                                    "raster_pixels_per_thread", "raster_staging_batch")}
             line["chosen_vs_plain"] = round(head["value"] / p["value"], 3)
             line["gpu_launches"] = head["gpu_launches"] + p["gpu_launches"]
         if world == 1 and not a.no_cpu_baseline and _workload_name(a) == WORKLOAD:
@@ -569,10 +573,11 @@ def measure_batched(a, local: int) -> dict:
         it[0] += 1
     loss0 = ctx.train_step_batch(cams, None, cfg, tc, it[0], gt_device_ptr=gt_dev.data_ptr())
     it[0] += 1
-    for k in range(3 + (6 if a.autotune else 0)):   # the autotuner's 6 trial steps first
+    for k in range(3 + (TUNE_STEPS if a.autotune else 0)):   # the autotuner's trial steps first
         batched(k)
     ctx.synchronize()
     ppt_b = {"forward": ctx.stat(gs3d.STAT_FWD_PPT), "backward": ctx.stat(gs3d.STAT_BWD_PPT)}
+    batch_b = {"forward": ctx.stat(gs3d.STAT_FWD_BATCH), "backward": ctx.stat(gs3d.STAT_BWD_BATCH)}
 
     def graph_stats():
         return ctx.stat(gs3d.STAT_GRAPH_REPLAYS), ctx.stat(gs3d.STAT_GRAPH_CAPTURES)
@@ -593,7 +598,7 @@ def measure_batched(a, local: int) -> dict:
             ctx.train_step(cam, None, cfg, tc, it[0], want_loss=False,
                            gt_device_ptr=gt_dev.data_ptr() + 4 * int(offs[v]))
             it[0] += 1
-    for k in range(3):   # each size's first step, the autotuner's 6 trial steps per size, graph captures
+    for k in range(3):   # each size's first step, the autotuner's trial steps per size, graph captures
         one_by_one(k)
     ctx.synchronize()
     p0 = graph_stats()
@@ -604,7 +609,7 @@ def measure_batched(a, local: int) -> dict:
             "mpix_per_step": round(pix / 1e6, 2), "steps": steps,
             "batched_bf16": {"ms_per_step": round(ms_b, 3), "mpix_per_s": round(pix / 1e6 / (ms_b * 1e-3), 1),
                              "gpu_launches_per_step": launches_b, "loss_first": loss0, "loss_last": loss_b,
-                             "raster_pixels_per_thread": ppt_b,
+                             "raster_pixels_per_thread": ppt_b, "raster_staging_batch": batch_b,
                              "graph_replays_per_step": (g1[0] - g0[0]) / steps,
                              "graph_captures_in_timed_steps": g1[1] - g0[1]},
             "plain_fp32_one_by_one": {"ms_per_64_views": round(ms_p, 3),

@@ -47,13 +47,17 @@ typedef struct gs3dc_ctx gs3dc_ctx;
 #define GS3DC_OPT_FUSED_ADAM     6  /* 1: optimiser fused into the preprocess backward; 0 (default): split */
 #define GS3DC_OPT_SORT           7  /* GS3DC_SORT_*: how gs3dc_train_step orders its pairs (same result) */
 #define GS3DC_OPT_KEEP_GRADIENTS 8  /* 1: gs3dc_train_step keeps its raw-parameter gradients (gs3dc_get_gradients) */
-#define GS3DC_OPT_AUTOTUNE       9  /* 1: tune the rasterisers' threads per tile (pixels per thread 1 / 2 / 4) online:
-                                       per workload shape the first 6 train steps try each setting twice (timed with
-                                       events, un-captured) and the fastest forward / backward stay; 0 (default): 2 */
+#define GS3DC_OPT_AUTOTUNE       9  /* 1: tune the rasterisers online: per workload shape the first 6 train steps try
+                                       1 / 2 / 4 pixels per thread (threads per tile 256 / 128 / 64) twice each, the
+                                       next 4 the staging batch 64 / 256 against 128 at the fastest ones (timed with
+                                       events, un-captured); the fastest forward / backward settings stay;
+                                       0 (default): 2 pixels per thread, batch 128 */
 #define GS3DC_OPT_DENSITY_SEED  10  /* state of the density controller's split sampler (LCG); 12345 at creation,
                                         like DensityController::rng_state_ (density_controller.h:41) */
 #define GS3DC_OPT_RASTER_PPT    11  /* 1, 2 or 4: the rasterisers' pixels per thread in train steps, fixed (the
                                        autotuner then stays off); 0 (default): 2, or the autotuner's pick */
+#define GS3DC_OPT_RASTER_BATCH  12  /* 64, 128 or 256: the records the rasterisers stage per round in train steps,
+                                       fixed together with GS3DC_OPT_RASTER_PPT; 0 (default): 128 */
 
 /* Depth-first (default): the Gaussians are stably sorted by depth, their pairs
  * emitted in that order and stably sorted by the tile bits alone.  Full key:
@@ -87,6 +91,8 @@ typedef struct gs3dc_ctx gs3dc_ctx;
                                           gs3dc_rasterize_arrays): the length of the raster gradients */
 #define GS3DC_STAT_GRAPH_CAPTURES 11 /* train-step graphs captured (one per workload shape that repeats;
                                         the single-view step keeps the graphs of up to 8 shapes) */
+#define GS3DC_STAT_FWD_BATCH     12  /* records the forward rasteriser stages per round in the last train step */
+#define GS3DC_STAT_BWD_BATCH     13  /* records the backward rasteriser stages per round in the last train step */
 
 /* Host arrays of PreprocessOutput + the per-Gaussian ForwardCache fields
  * (include/types.h:69-82, 97-107).  Any pointer may be NULL (not produced). */

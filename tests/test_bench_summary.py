@@ -16,7 +16,8 @@ def _fake_result(form, P):
     stage_ms = [0.01, 0.04, 0.15, 0.13, 0.02, 0.21, 0.42, 0.29]   # bench.STAGES order
     return {"form": form, "tile_pairs": P, "sort_passes": 6, "stage_ms": stage_ms, "ms_total": 200 * 1.3,
             "e2e_s": 0.3, "launches": 6000, "loss_first": 1.0, "loss_last": 0.5, "clocks": {}, "graph": True,
-            "raster_pixels_per_thread": {"forward": 2, "backward": 2}}
+            "raster_pixels_per_thread": {"forward": 2, "backward": 2},
+            "raster_staging_batch": {"forward": 128, "backward": 128}}
 
 
 def test_traffic_table_has_both_forms():

@@ -93,24 +93,29 @@ def test_gradients_against_fp64_oracle(ctx, form):
 
 def test_pixels_per_thread_keep_the_image(ctx, form):
     """The rasterisers' pixels per thread (1, 2, 4: 256, 128, 64 threads per
-    tile) change neither the reduced-form image (bit for bit) nor, beyond
-    FP32-summation order, the gradients."""
+    tile) and staging batch (64, 128, 256 records) change neither the
+    reduced-form image (bit for bit) nor, beyond FP32-summation order, the
+    gradients."""
     sc = S.random_scene(20000, seed=35)
     cam = S.look_at_camera((0.2, -0.3, -3.0), 333, 251)
     cfg = S.render_config(True)
     gt = O.forward(S.perturbed(sc), cam, S.render_config(False), "c").image
     ctx.set_option(gs3d.OPT_KEEP_GRADIENTS, 1)
     out = {}
+    settings = [(1, 128), (2, 128), (4, 128), (2, 64), (4, 256)]
     try:
-        for ppt in (1, 2, 4):
+        for ppt, batch in settings:
             ctx.set_option(gs3d.OPT_RASTER_PPT, ppt)
+            ctx.set_option(gs3d.OPT_RASTER_BATCH, batch)
             ctx.set_raw_params(sc)
             loss = ctx.train_step(cam, gt, cfg, S.train_config(**ZERO_LR), 0)
-            out[ppt] = (loss, ctx.get_image(cam), ctx.get_gradients())
+            out[(ppt, batch)] = (loss, ctx.get_image(cam), ctx.get_gradients())
     finally:
         ctx.set_option(gs3d.OPT_RASTER_PPT, 0)
+        ctx.set_option(gs3d.OPT_RASTER_BATCH, 0)
         ctx.set_option(gs3d.OPT_KEEP_GRADIENTS, 0)
-    for ppt in (2, 4):
+    out[1] = out[(1, 128)]
+    for ppt in settings[1:]:
         assert np.array_equal(out[ppt][1], out[1][1]), ppt
         assert abs(out[ppt][0] - out[1][0]) <= 1e-7 * out[1][0]   # the loss sums tiles in another order
         for k in ("pos", "sc", "rot", "sh", "op"):

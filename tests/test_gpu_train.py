@@ -288,8 +288,9 @@ def test_recompute_backward_memory_vs_stored_lists():
 @pytest.mark.parametrize("form", [gs3d.FORM_PLAIN_FP32, gs3d.FORM_BF16])
 def test_autotuner_picks_a_setting_and_keeps_results(ctx, form):
     """GS3DC_OPT_AUTOTUNE: the first 6 steps try 1 / 2 / 4 pixels per thread,
-    then the picks stay; the forward image does not depend on the setting and
-    the trajectory matches an untuned run to FP32-summation level."""
+    the next 4 the staging batches 64 / 256, then the picks stay; the forward
+    image does not depend on the setting and the trajectory matches an untuned
+    run to FP32-summation level."""
     sc = S.random_scene(20000, seed=51)
     cam = S.look_at_camera((0.3, 0.2, -3.0), 320, 240)
     gt = O.forward(S.perturbed(sc), cam, S.render_config(False), "c").image
@@ -300,15 +301,18 @@ def test_autotuner_picks_a_setting_and_keeps_results(ctx, form):
         for tune in (0, 1):
             ctx.set_option(gs3d.OPT_AUTOTUNE, tune)
             ctx.set_raw_params(sc)
-            losses = [ctx.train_step(cam, gt, cfg, tc, it) for it in range(10)]
+            losses = [ctx.train_step(cam, gt, cfg, tc, it) for it in range(12)]
             res.append((losses, ctx.get_raw_params(sc.copy()),
-                        (ctx.stat(gs3d.STAT_FWD_PPT), ctx.stat(gs3d.STAT_BWD_PPT))))
+                        (ctx.stat(gs3d.STAT_FWD_PPT), ctx.stat(gs3d.STAT_BWD_PPT),
+                         ctx.stat(gs3d.STAT_FWD_BATCH), ctx.stat(gs3d.STAT_BWD_BATCH))))
     finally:
         ctx.set_option(gs3d.OPT_AUTOTUNE, 0)
         ctx.set_option(gs3d.OPT_FORM, gs3d.FORM_PLAIN_FP32)
     (l0, p0, k0), (l1, p1, k1) = res
-    print(f"form {form}: autotuner picked forward {k1[0]}, backward {k1[1]} pixels per thread")
-    assert k0 == (2, 2) and k1[0] in (1, 2, 4) and k1[1] in (1, 2, 4)
+    print(f"form {form}: autotuner picked forward {k1[0]}, backward {k1[1]} pixels per thread, "
+          f"staging batches {k1[2]} / {k1[3]}")
+    assert k0 == (2, 2, 128, 128) and k1[0] in (1, 2, 4) and k1[1] in (1, 2, 4)
+    assert k1[2] in (64, 128, 256) and k1[3] in (64, 128, 256)
     assert abs(l0[0] - l1[0]) <= 1e-6 * l0[0]     # same first forward whatever the setting
     assert np.allclose(l0, l1, rtol=2e-3)
     if form == gs3d.FORM_PLAIN_FP32:
