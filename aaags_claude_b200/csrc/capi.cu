@@ -202,6 +202,7 @@ struct gs3dc_ctx {
         DevBuf<unsigned> last;
         DevBuf<unsigned char> dsign;
         DevBuf<unsigned> ranges, order;
+        DevBuf<unsigned> hist_parts;               // launch_emit_ranked's spread tile-digit counts
         size_t grads_zeroed = 0;                   // entries of the screen-gradient accumulators known zero
         std::vector<unsigned long long> view_pix;  // first pixel of each view of the last step (+ the total)
         cudaGraphExec_t graph = nullptr;
@@ -1060,6 +1061,7 @@ int batch_buffers(gs3dc_ctx* c, const BatchShape& sh) {
     CK(b.dsign.ensure(sh.pix));
     CK(b.ranges.ensure(2 * (size_t)sh.tiles));
     CK(b.order.ensure(sh.tiles));
+    CK(b.hist_parts.ensure((size_t)kHistParts * (kMaxPasses - kDepthDigits) * 256));
     Control* before = c->ctrl;
     int rc = ensure_ctrl(c, (int)std::min<long long>(sh.VN, 0x7fffffffLL));
     if (rc) return rc;
@@ -1082,6 +1084,7 @@ int seq_batch(gs3dc_ctx* c, const BatchShape& sh) {
                        c->stream));
     CK(cudaMemsetAsync(b.ranges.p, 0, 2 * (size_t)sh.tiles * sizeof(unsigned), c->stream));
     CK(cudaMemsetAsync(b.ddesc.p, 0, 4 * dstride * sizeof(unsigned long long), c->stream));
+    CK(cudaMemsetAsync(b.hist_parts.p, 0, b.hist_parts.n * sizeof(unsigned), c->stream));
     if (sh.tile_digits > 0)
         CK(cudaMemsetAsync(b.sort_desc.p, 0, (size_t)sh.tile_digits * pstride * sizeof(unsigned long long),
                            c->stream));
@@ -1096,7 +1099,7 @@ int seq_batch(gs3dc_ctx* c, const BatchShape& sh) {
                            b.ddesc.p, dstride, c->ctrl, &dw, nullptr, &c->ctrl->gauss_keys, 0));
     PairPtrs pr{nullptr, b.vals[0].p, b.cap, c->scan_desc, b.keys[0].p};
     CK(launch_emit_ranked(c->stream, views, (int)vn, b.dvals[dw].p, batch_screen(c), pr, c->ctrl, b.rects.p, c->N,
-                          5));
+                          5, b.hist_parts.p));
     int which = 0;
     CK(launch_radix_sort32(c->stream, views, sh.tile_digits, 5, true, b.cap, b.keys[0].p, b.vals[0].p, b.keys[1].p,
                            b.vals[1].p, b.sort_desc.p, pstride, c->ctrl, &which));
@@ -1116,8 +1119,9 @@ int seq_batch(gs3dc_ctx* c, const BatchShape& sh) {
                                    chosen_ptrs(c), batch_rgrads(c),
                                    c->keep_grads ? grad_ptrs(c) : GradPtrs{nullptr, nullptr, nullptr, nullptr, nullptr},
                                    c->ctrl, sh.V));
-    // preprocess, 4 depth passes, emission, tile passes, ranges + order, rasterisers, adjoint
-    c->kernels_last = 1 + 4 + 1 + (sh.tile_digits > 0 ? sh.tile_digits : 0) + 2 + 3;
+    // preprocess, 4 depth passes, emission + its count reduction, tile passes, ranges + order, rasterisers,
+    // adjoint
+    c->kernels_last = 1 + 4 + 2 + (sh.tile_digits > 0 ? sh.tile_digits : 0) + 1 + (sh.tiles > 65536 ? 2 : 1) + 3;
     return GS3DC_OK;
 }
 

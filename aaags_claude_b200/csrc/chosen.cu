@@ -724,59 +724,7 @@ __global__ void __launch_bounds__(kCB, MULTI ? 8 : 10) k_chosen_backward(const S
     adam_slice(sm, sp, g0, ng, mc3, c, gout);
 }
 
-// One view, persistent and software-pipelined: each CTA walks slices blockIdx,
-// blockIdx + gridDim, ... with two staging buffers; the next slice's bulk
-// copies (and the L2 prefetch of its moments) are issued before this slice's
-// adjoint and optimiser run, so they are in flight while it computes.  A wait
-// that runs out ends the CTA (status kStatusTimeout).
-template <typename S>
-__global__ void __launch_bounds__(kCB, 6) k_chosen_backward_pipe(const StepParams* __restrict__ spp, int N, int mc3,
-                                                                 ChosenPtrs c, RGradPtrs rg, GradPtrs gout,
-                                                                 Control* ctrl) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    ChosenBwdShared<S, false>* buf = reinterpret_cast<ChosenBwdShared<S, false>*>(smem_raw);
-    const StepParams& sp = *spp;
-    if ((ctrl->status & (kStatusOverflow | kStatusTimeout)) || sp.persist->sticky_overflow) return;
-    const int tid = threadIdx.x;
-    if (blockIdx.x == 0 && tid == 0 && sp.use_adam) atomicAdd(&sp.persist->applied_steps, 1ull);
-    const long long n_slices = ((long long)N + kCB - 1) / kCB;
-    if (tid == 0) {
-        mbar_init(&buf[0].bar, 1);
-        mbar_init(&buf[1].bar, 1);
-        mbar_fence_init();
-    }
-    __syncthreads();
-    if (tid == 0 && (long long)blockIdx.x < n_slices && ((long long)blockIdx.x + 1) * kCB <= N)
-        issue_slice_copies(buf[0], (long long)blockIdx.x * kCB, mc3, c, rg);
-    int i = 0;
-    for (long long sl = blockIdx.x; sl < n_slices; sl += gridDim.x, i++) {
-        ChosenBwdShared<S, false>& sm = buf[i & 1];
-        const long long g0 = sl * kCB;
-        const int ng = (int)min((long long)kCB, (long long)N - g0);
-        if (ng == kCB) {
-            // buffer i & 1 completes once per use: its (i >> 1)-th phase
-            const bool ok = mbar_wait(&sm.bar, (unsigned)((i >> 1) & 1), sp.spin_limit, &ctrl->status);
-            if (__syncthreads_or(!ok)) break;
-        } else {
-            stage_slice_plain(sm, g0, ng, mc3, c, rg);
-            __syncthreads();
-        }
-        const long long nx = sl + gridDim.x;
-        if (tid == 0 && nx < n_slices && (nx + 1) * kCB <= N) {
-            fence_proxy_async();   // the other buffer's reads (two slices ago) come before the copies into it
-            issue_slice_copies(buf[(i + 1) & 1], nx * kCB, mc3, c, rg);
-        }
-        adjoint_slice(sm, sp, g0, ng, mc3, rg);
-        __syncthreads();
-        adam_slice(sm, sp, g0, ng, mc3, c, gout);
-        __syncthreads();
-    }
-}
-
 inline int grid_for(long long n, int t) { return (int)((n + t - 1) / t); }
-
-// One view's adjoint + Adam runs as the persistent, software-pipelined kernel.
-constexpr bool kPipelinedAdjoint = true;
 
 }  // namespace
 
@@ -861,21 +809,6 @@ cudaError_t launch_chosen_backward_adam(cudaStream_t st, const StepParams* sp, i
     if (n_views > 1) {
         if (fp16) k_chosen_backward<__half, true><<<grid, kCB, smem, st>>>(sp, N, mc3, c, rg, g, ctrl, n_views);
         else k_chosen_backward<__nv_bfloat16, true><<<grid, kCB, smem, st>>>(sp, N, mc3, c, rg, g, ctrl, n_views);
-    } else if (kPipelinedAdjoint) {
-        // persistent: the CTAs that fit resident (two staging buffers each), at most one per slice
-        const int smem2 = 2 * smem1;
-        static std::atomic<unsigned long long> pipe_done[2];
-        cudaError_t x = set_smem_once(pipe_done[0], k_chosen_backward_pipe<__half>, smem2);
-        if (x == cudaSuccess) x = set_smem_once(pipe_done[1], k_chosen_backward_pipe<__nv_bfloat16>, smem2);
-        if (x != cudaSuccess) return x;
-        static int per_sm = 0;
-        if (!per_sm && (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_chosen_backward_pipe<__nv_bfloat16>,
-                                                                      kCB, smem2) != cudaSuccess ||
-                        per_sm < 1))
-            per_sm = 1;
-        const int pgrid = std::min(grid, per_sm * sm_count());
-        if (fp16) k_chosen_backward_pipe<__half><<<pgrid, kCB, smem2, st>>>(sp, N, mc3, c, rg, g, ctrl);
-        else k_chosen_backward_pipe<__nv_bfloat16><<<pgrid, kCB, smem2, st>>>(sp, N, mc3, c, rg, g, ctrl);
     } else {
         if (fp16) k_chosen_backward<__half, false><<<grid, kCB, smem, st>>>(sp, N, mc3, c, rg, g, ctrl, 1);
         else k_chosen_backward<__nv_bfloat16, false><<<grid, kCB, smem, st>>>(sp, N, mc3, c, rg, g, ctrl, 1);

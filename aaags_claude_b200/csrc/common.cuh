@@ -12,6 +12,7 @@ namespace gs3d {
 constexpr int kTile = 16;            // 16x16 pixel tiles (RenderConfig default, include/types.h:64-65)
 constexpr int kBlock = 256;          // threads per CTA of the per-Gaussian and per-tile kernels
 constexpr int kMaxPasses = 8;         // radix passes (8-bit digits over <= 64 key bits)
+constexpr int kHistParts = 128;      // copies of the multi-view emission's tile-digit counts (atomic spread)
 constexpr int kDepthDigits = 4;       // depth-first ordering: digits of the Gaussian depth sort (control slots
                                       // 0..3); the pair sort on the tile bits uses slots kDepthDigits..
 constexpr int kChosenDepthSkip = 1;   // reduced-storage form: low depth digits left out of the depth sort
@@ -218,10 +219,6 @@ __device__ __forceinline__ void mbar_fence_init() {
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
-// Orders this CTA's earlier shared-memory accesses (generic proxy) before
-// later bulk copies (async proxy) into the same buffer.
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-
 // One arrival that also announces `bytes` of transactions to wait for.
 __device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, unsigned bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
@@ -249,6 +246,19 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned 
 
 // Bounded wait for `phase` of the barrier: false (and kStatusTimeout) if the
 // copies have not landed after spin_limit polls.
+// ---- per-thread asynchronous copies (cp.async) into shared memory ----
+// 16 bytes (both addresses 16-byte aligned; cached in L2 only) or 4 bytes; a
+// thread's copies complete in commit order, cp_async_wait_all waits for all of
+// the thread's own.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
 // Bulk prefetch of [src, src + bytes) into L2 (no shared memory, no completion
 // to wait for); src 16-byte aligned, bytes a multiple of 16.
 __device__ __forceinline__ void prefetch_l2(const void* src, unsigned bytes) {

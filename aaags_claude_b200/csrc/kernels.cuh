@@ -214,9 +214,13 @@ cudaError_t launch_preprocess_plain(cudaStream_t st, const StepParams* sp, int N
 // the views' local tile ids: the emission order groups the pairs by view, so a
 // stable sort on the local id leaves every (view, tile) run contiguous
 // (launch_tile_ranges_views).
+// hist_parts (optional, zeroed, kHistParts * (kMaxPasses - kDepthDigits) * 256
+// counters): the CTAs add their counts into copy (CTA % kHistParts) and one
+// more kernel sums the copies into the control slots -- for launches of many
+// CTAs, whose adds would otherwise meet on the same 256 * digits addresses.
 cudaError_t launch_emit_ranked(cudaStream_t st, const StepParams* sp, int N, const unsigned* rank_gid,
                                ScreenPtrs s, PairPtrs pr, Control* ctrl, const uint2* rects = nullptr,
-                               int n_per_view = 0, int hist_slot = kDepthDigits);
+                               int n_per_view = 0, int hist_slot = kDepthDigits, unsigned* hist_parts = nullptr);
 cudaError_t launch_bin_arrays(cudaStream_t st, const StepParams* sp, int N, ScreenArrays a,
                               PairPtrs pr, Control* ctrl);
 cudaError_t launch_export_screen(cudaStream_t st, int N, ScreenPtrs s, ScreenArrays a);

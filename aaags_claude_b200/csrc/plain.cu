@@ -256,7 +256,8 @@ __global__ void __launch_bounds__(kBlock) k_preprocess(const StepParams* __restr
 __global__ void __launch_bounds__(kBlock) k_emit_ranked(const StepParams* __restrict__ spp, int N,
                                                         const unsigned* __restrict__ rank_gid, ScreenPtrs s,
                                                         PairPtrs pr, const uint2* __restrict__ rects,
-                                                        Control* ctrl, int n_per_view, int hist_slot) {
+                                                        Control* ctrl, int n_per_view, int hist_slot,
+                                                        unsigned* __restrict__ hist_parts) {
     __shared__ EmitShared sm;
     __shared__ int s_blk;
     __shared__ unsigned s_thist[kMaxPasses - kDepthDigits][256];
@@ -305,9 +306,27 @@ __global__ void __launch_bounds__(kBlock) k_emit_ranked(const StepParams* __rest
     scan_and_emit(sm, blk, g, cnt, cnt, rx, ry, rw, dbits, sp.grid_x, pr, ctrl, sp.spin_limit, sp.persist,
                   &s_thist[0][0], nd, tbase, gx);
     __syncthreads();
+    // many CTAs (several views): spread the counts over kHistParts copies so that the atomics of
+    // different CTAs rarely meet on one address; k_hist_parts_reduce adds the copies up
+    unsigned* dst = hist_parts ? hist_parts + (size_t)(blk % kHistParts) * (kMaxPasses - kDepthDigits) * 256
+                               : &ctrl->hist[hist_slot][0];
     for (int e = threadIdx.x; e < nd * 256; e += kBlock) {
         const unsigned v = (&s_thist[0][0])[e];
-        if (v) atomicAdd(&ctrl->hist[hist_slot + (e >> 8)][e & 255], v);
+        if (v) atomicAdd(&dst[e], v);
+    }
+}
+
+// Sums the kHistParts copies of the tile-digit counts into the control
+// block's histogram slots hist_slot.. (one CTA; the copies are zeroed with the
+// other per-step scratch).
+__global__ void __launch_bounds__(256) k_hist_parts_reduce(const unsigned* __restrict__ hist_parts,
+                                                           const StepParams* __restrict__ spp, Control* ctrl,
+                                                           int hist_slot) {
+    const int nd = spp->sort_passes - kDepthDigits;
+    for (int e = threadIdx.x; e < nd * 256; e += blockDim.x) {
+        unsigned v = 0;
+        for (int p = 0; p < kHistParts; p++) v += hist_parts[(size_t)p * (kMaxPasses - kDepthDigits) * 256 + e];
+        ctrl->hist[hist_slot + (e >> 8)][e & 255] = v;
     }
 }
 
@@ -728,10 +747,11 @@ cudaError_t launch_preprocess_plain(cudaStream_t st, const StepParams* sp, int N
 
 cudaError_t launch_emit_ranked(cudaStream_t st, const StepParams* sp, int N, const unsigned* rank_gid,
                                ScreenPtrs s, PairPtrs pr, Control* ctrl, const uint2* rects, int n_per_view,
-                               int hist_slot) {
+                               int hist_slot, unsigned* hist_parts) {
     if (N <= 0) return cudaSuccess;
     k_emit_ranked<<<blocks_for(N, kBlock), kBlock, 0, st>>>(sp, N, rank_gid, s, pr, rects, ctrl, n_per_view,
-                                                            hist_slot);
+                                                            hist_slot, hist_parts);
+    if (hist_parts) k_hist_parts_reduce<<<1, 256, 0, st>>>(hist_parts, sp, ctrl, hist_slot);
     return cudaGetLastError();
 }
 

@@ -258,28 +258,15 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_bwd(const StepParams* __re
             s_yy = t2;
             return contrib;
         };
-        // two entries per round: their 16 + 2 sums reduce in one butterfly each (18 shuffles
-        // instead of 28 for two separate 8 + 1 reductions)
-        for (int i = nl - 1; i >= 0; i -= 2) {
-            const int kA = s_list[warp][i];
-            float gv[16], tA, tB = 0.0f;
-            const bool cA = item(kA, gv, tA);
-            if (i >= 1) {   // warp-uniform: nl is the warp's list length
-                const int kB = s_list[warp][i - 1];
-                const bool cB = item(kB, gv + 8, tB);
-                if (__any_sync(0xffffffffu, cA || cB)) {
-                    int idx;
-                    const float s16 = warp_sum16(gv, &idx);
-                    const float s2 = warp_sum2(tA, tB);
-                    if ((lane & 1) == 0 && s16 != 0.0f) atomicAdd(&s_acc[idx & 7][idx < 8 ? kA : kB], s16);
-                    if ((lane & 15) == 0 && s2 != 0.0f) atomicAdd(&s_acc[8][lane < 16 ? kA : kB], s2);
-                }
-            } else if (__any_sync(0xffffffffu, cA)) {
+        for (int i = nl - 1; i >= 0; i--) {
+            const int k = s_list[warp][i];
+            float gv[8], t2;
+            if (__any_sync(0xffffffffu, item(k, gv, t2))) {
                 int idx;
                 const float s8 = warp_sum8(gv, &idx);
-                const float s9 = warp_sum(tA);
-                if ((lane & 3) == 0 && s8 != 0.0f) atomicAdd(&s_acc[idx][kA], s8);
-                if (lane == 1 && s9 != 0.0f) atomicAdd(&s_acc[8][kA], s9);
+                const float s9 = warp_sum(t2);
+                if ((lane & 3) == 0 && s8 != 0.0f) atomicAdd(&s_acc[idx][k], s8);
+                if (lane == 1 && s9 != 0.0f) atomicAdd(&s_acc[8][k], s9);
             }
         }
         __syncthreads();

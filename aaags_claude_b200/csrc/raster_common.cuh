@@ -177,49 +177,4 @@ __device__ __forceinline__ float warp_sum8(const float v[8], int* idx) {
     return c;
 }
 
-// Sums sixteen values over the 32 lanes with 16 shuffles (the butterfly of
-// warp_sum8 with one more halving stage).  On return lane l holds the warp
-// total of value ((l>>4)&1)*8 + ((l>>3)&1)*4 + ((l>>2)&1)*2 + ((l>>1)&1) (*idx);
-// lanes l and l^1 hold the same total.
-__device__ __forceinline__ float warp_sum16(const float v[16], int* idx) {
-    const unsigned lane = threadIdx.x & 31;
-    const bool h16 = lane & 16, h8 = lane & 8, h4 = lane & 4, h2 = lane & 2;
-    float a[8];
-#pragma unroll
-    for (int i = 0; i < 8; i++) {
-        const float send = h16 ? v[i] : v[i + 8];
-        const float keep = h16 ? v[i + 8] : v[i];
-        a[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
-    }
-    float b[4];
-#pragma unroll
-    for (int i = 0; i < 4; i++) {
-        const float send = h8 ? a[i] : a[i + 4];
-        const float keep = h8 ? a[i + 4] : a[i];
-        b[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
-    }
-    float c[2];
-#pragma unroll
-    for (int i = 0; i < 2; i++) {
-        const float send = h4 ? b[i] : b[i + 2];
-        const float keep = h4 ? b[i + 2] : b[i];
-        c[i] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
-    }
-    const float send = h2 ? c[0] : c[1];
-    float d = (h2 ? c[1] : c[0]) + __shfl_xor_sync(0xffffffffu, send, 2);
-    d += __shfl_xor_sync(0xffffffffu, d, 1);
-    *idx = (h16 ? 8 : 0) + (h8 ? 4 : 0) + (h4 ? 2 : 0) + (h2 ? 1 : 0);
-    return d;
-}
-
-// Sums two values over the 32 lanes with 5 shuffles: lanes 0-15 return the
-// total of a, lanes 16-31 the total of b.
-__device__ __forceinline__ float warp_sum2(float a, float b) {
-    const bool h16 = threadIdx.x & 16;
-    float s = (h16 ? b : a) + __shfl_xor_sync(0xffffffffu, h16 ? a : b, 16);
-#pragma unroll
-    for (int o = 8; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    return s;
-}
-
 }  // namespace gs3d

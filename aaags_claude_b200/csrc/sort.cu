@@ -77,11 +77,17 @@ __global__ void __launch_bounds__(kHistThreads) k_radix_hist(const K* __restrict
         if (s_h[e]) atomicAdd(&ctrl->hist[slot_base + (e >> 8) - first][e & 255], s_h[e]);
 }
 
-// Shared memory of one onesweep CTA (dynamic; ~60 KB for 64-bit keys, ~44 KB for 32-bit).
-template <typename K>
+// Keys per thread of a onesweep CTA: 16, or 32 for large sorts of 32-bit keys
+// (8192 keys per CTA: half the CTAs, so half the per-digit look-backs; measured
+// faster from tens of millions of keys on, slower at a few million).
+constexpr unsigned long long kWideSweepKeys = 1ull << 25;
+
+// Shared memory of one onesweep CTA (dynamic; ~60 KB for 64-bit keys at 16 per
+// thread, ~44 / ~76 KB for 32-bit keys at 16 / 32).
+template <typename K, int ITEMS>
 struct SweepShared {
-    K keys[kSortTile];
-    unsigned vals[kSortTile];
+    K keys[kSortThreads * ITEMS];
+    unsigned vals[kSortThreads * ITEMS];
     unsigned whist[kSortThreads / 32][256];   // per-warp digit counts, then per-warp prefixes
     unsigned long long gbase[256];            // global output offset of this tile's first key of digit d
     unsigned dprefix[256];                    // tile-local exclusive prefix over digits
@@ -108,9 +114,9 @@ __device__ __forceinline__ unsigned long long block_exclusive_scan64(unsigned lo
 
 // One pass over digit `pass` (key bits 8*pass..); `slot` selects the digit
 // histogram and CTA ticket in the control block.
-// 64-bit keys: 2 CTAs per SM (register-bound); 32-bit keys: 4.
-template <typename K>
-__global__ void __launch_bounds__(kSortThreads, sizeof(K) == 4 ? 4 : 2) k_onesweep(const StepParams* __restrict__ sp,
+// 2 CTAs per SM (register-bound): 64-bit keys at 16 per thread, 32-bit keys at 32.
+template <typename K, int ITEMS>
+__global__ void __launch_bounds__(kSortThreads, ITEMS > 16 || sizeof(K) > 4 ? 2 : 4) k_onesweep(const StepParams* __restrict__ sp,
                                                               const K* __restrict__ kin,
                                                               const unsigned* __restrict__ vin,
                                                               K* __restrict__ kout,
@@ -119,8 +125,10 @@ __global__ void __launch_bounds__(kSortThreads, sizeof(K) == 4 ? 4 : 2) k_oneswe
                                                               unsigned long long* desc,
                                                               const unsigned long long* count,
                                                               Control* ctrl) {
+    constexpr int kItems = ITEMS;
+    constexpr int kTileKeys = kSortThreads * kItems;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    SweepShared<K>& sm = *reinterpret_cast<SweepShared<K>*>(smem_raw);
+    SweepShared<K, ITEMS>& sm = *reinterpret_cast<SweepShared<K, ITEMS>*>(smem_raw);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int shift = 8 * pass;
     const unsigned long long P = min(*count, capacity);
@@ -128,22 +136,22 @@ __global__ void __launch_bounds__(kSortThreads, sizeof(K) == 4 ? 4 : 2) k_oneswe
     for (int e = tid; e < (kSortThreads / 32) * 256; e += kSortThreads) (&sm.whist[0][0])[e] = 0;
     __syncthreads();
     const int t = sm.tile;
-    const unsigned long long base = (unsigned long long)t * kSortTile;
+    const unsigned long long base = (unsigned long long)t * kTileKeys;
     if (base >= P) return;
 
-    K key[kSortItems];
-    unsigned val[kSortItems];
-    unsigned rank[kSortItems];
+    K key[kItems];
+    unsigned val[kItems];
+    unsigned rank[kItems];
 #pragma unroll
-    for (int it = 0; it < kSortItems; it++) {
-        const unsigned long long idx = base + (unsigned long long)(warp * 32 * kSortItems + it * 32 + lane);
+    for (int it = 0; it < kItems; it++) {
+        const unsigned long long idx = base + (unsigned long long)(warp * 32 * kItems + it * 32 + lane);
         const bool valid = idx < P;
         key[it] = valid ? kin[idx] : (K)~(K)0;   // sentinel: digit 255, ranks after every real key
         val[it] = valid ? vin[idx] : 0u;
     }
     const unsigned lt_mask = (1u << lane) - 1u;
 #pragma unroll
-    for (int it = 0; it < kSortItems; it++) {
+    for (int it = 0; it < kItems; it++) {
         const unsigned d = (unsigned)(key[it] >> shift) & 255u;
         const unsigned peers = peer_mask8(0xffffffffu, d);
         // one leader per digit adds the group's size to the warp's count and
@@ -176,14 +184,14 @@ __global__ void __launch_bounds__(kSortThreads, sizeof(K) == 4 ? 4 : 2) k_oneswe
     sm.dprefix[d] = (unsigned)block_exclusive_scan64((unsigned long long)run, sm.scan);
     __syncthreads();
 #pragma unroll
-    for (int it = 0; it < kSortItems; it++) {
+    for (int it = 0; it < kItems; it++) {
         const unsigned dd = (unsigned)(key[it] >> shift) & 255u;
         const unsigned pos = sm.dprefix[dd] + sm.whist[warp][dd] + rank[it];
         sm.keys[pos] = key[it];
         sm.vals[pos] = val[it];
     }
     __syncthreads();
-    const int n_valid = (int)min((unsigned long long)kSortTile, P - base);
+    const int n_valid = (int)min((unsigned long long)kTileKeys, P - base);
     for (int j = tid; j < n_valid; j += kSortThreads) {
         const K k = sm.keys[j];
         const unsigned dd = (unsigned)(k >> shift) & 255u;
@@ -413,8 +421,9 @@ cudaError_t launch_wait_selftest(cudaStream_t st, unsigned long long* desc2, uns
 namespace {
 
 // Digits [first, passes) of the keys, slots slot_base..; desc holds
-// (passes - first) * desc_stride zeroed descriptors.
-template <typename K>
+// (passes - first) * desc_stride zeroed descriptors (strides sized for kSortTile
+// keys per CTA are an upper bound for either CTA size).
+template <typename K, int ITEMS>
 cudaError_t radix_sort_impl(cudaStream_t st, const StepParams* sp, int first, int passes, int slot_base,
                             bool hist_done, unsigned long long capacity, K* keys0, unsigned* vals0, K* keys1,
                             unsigned* vals1, unsigned long long* desc, unsigned long long desc_stride,
@@ -423,22 +432,23 @@ cudaError_t radix_sort_impl(cudaStream_t st, const StepParams* sp, int first, in
     if (capacity == 0 || passes <= first) return cudaSuccess;
     if (!count) count = &ctrl->total_pairs;
     static std::atomic<unsigned long long> attr_done{0};
-    const int smem = (int)sizeof(SweepShared<K>);
-    cudaError_t e = set_smem_once(attr_done, k_onesweep<K>, smem);
+    const int smem = (int)sizeof(SweepShared<K, ITEMS>);
+    cudaError_t e = set_smem_once(attr_done, k_onesweep<K, ITEMS>, smem);
     if (e != cudaSuccess) return e;
     if (!hist_done) {
         k_radix_hist<K><<<2 * sm_count(), kHistThreads, 0, st>>>(keys0, capacity, first, passes, slot_base, count, ctrl);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     if (after_hist && (e = cudaEventRecord(after_hist, st)) != cudaSuccess) return e;
-    const unsigned long long tiles = (capacity + kSortTile - 1) / kSortTile;
+    const unsigned long long tile_keys = (unsigned long long)kSortThreads * ITEMS;
+    const unsigned long long tiles = (capacity + tile_keys - 1) / tile_keys;
     K* kin = keys0;
     unsigned* vin = vals0;
     K* kout = keys1;
     unsigned* vout = vals1;
     for (int p = first; p < passes; p++) {
         const int slot = slot_base + p - first;
-        k_onesweep<K><<<(unsigned)tiles, kSortThreads, smem, st>>>(
+        k_onesweep<K, ITEMS><<<(unsigned)tiles, kSortThreads, smem, st>>>(
             sp, kin, vin, kout, vout, capacity, p, slot, desc + (unsigned long long)(p - first) * desc_stride, count,
             ctrl);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -461,7 +471,7 @@ cudaError_t launch_radix_sort(cudaStream_t st, const StepParams* sp, int passes,
                               Control* ctrl, int* which, cudaEvent_t after_hist, int first_pass,
                               const unsigned long long* count) {
     // 64-bit keys: digit p uses slot p, descriptors from desc + p * desc_stride
-    return radix_sort_impl<unsigned long long>(st, sp, first_pass, passes, first_pass, false, capacity, keys0,
+    return radix_sort_impl<unsigned long long, kSortItems>(st, sp, first_pass, passes, first_pass, false, capacity, keys0,
                                                vals0, keys1, vals1, desc + (unsigned long long)first_pass * desc_stride,
                                                desc_stride, ctrl, which, after_hist, count);
 }
@@ -471,7 +481,10 @@ cudaError_t launch_radix_sort32(cudaStream_t st, const StepParams* sp, int digit
                                 unsigned* vals1, unsigned long long* desc, unsigned long long desc_stride,
                                 Control* ctrl, int* which, cudaEvent_t after_hist, const unsigned long long* count,
                                 int first_digit) {
-    return radix_sort_impl<unsigned>(st, sp, first_digit, digits, slot_base, hist_done, capacity, keys0, vals0, keys1,
+    if (capacity >= kWideSweepKeys)
+        return radix_sort_impl<unsigned, 32>(st, sp, first_digit, digits, slot_base, hist_done, capacity, keys0, vals0, keys1,
+                                     vals1, desc, desc_stride, ctrl, which, after_hist, count);
+    return radix_sort_impl<unsigned, kSortItems>(st, sp, first_digit, digits, slot_base, hist_done, capacity, keys0, vals0, keys1,
                                      vals1, desc, desc_stride, ctrl, which, after_hist, count);
 }
 
