@@ -81,7 +81,8 @@ struct gs3dc_ctx {
     int adam_step = 0;
     // screen-space records + optional cache
     DevBuf<float4> rec0, rec1;
-    DevBuf<float> col_b, depth;
+    DevBuf<float2> cbt;
+    DevBuf<float> depth;
     DevBuf<int> radius, tiles;
     DevBuf<float> c_cov3D, c_pview, c_phw, c_cov2D, c_det;
     // screen arrays in the reference layout (stage import / export)
@@ -189,7 +190,8 @@ struct gs3dc_ctx {
         StepParams* views_host = nullptr;          // pinned staging, kMaxBatchViews entries
         cudaEvent_t views_event = nullptr;         // the staging's last copy has been consumed
         DevBuf<float4> rec0, rec1;
-        DevBuf<float> col_b, depth, dm2, dcon, drgb, dop;
+        DevBuf<float2> cbt;
+        DevBuf<float> depth, dm2, dcon, drgb, dop;
         DevBuf<int> radius, tiles;
         DevBuf<uint2> rects;
         DevBuf<unsigned> dkeys[2];                 // (view << 24 | depth's upper 24 bits) of each entry
@@ -322,7 +324,7 @@ AdamPtrs adam_ptrs(gs3dc_ctx* c) {
 GradPtrs grad_ptrs(gs3dc_ctx* c) { return {c->g_pos.p, c->g_sc.p, c->g_rot.p, c->g_sh.p, c->g_op.p}; }
 RGradPtrs rgrad_ptrs(gs3dc_ctx* c) { return {c->dm2.p, c->dcon.p, c->drgb.p, c->dop.p}; }
 ScreenPtrs screen_ptrs(gs3dc_ctx* c, bool cache) {
-    ScreenPtrs s{c->rec0.p, c->rec1.p, c->col_b.p, c->depth.p, c->radius.p, c->tiles.p,
+    ScreenPtrs s{c->rec0.p, c->rec1.p, c->cbt.p, c->depth.p, c->radius.p, c->tiles.p,
                  nullptr, nullptr, nullptr, nullptr, nullptr};
     if (cache) {
         s.cov3D = c->c_cov3D.p;
@@ -375,7 +377,7 @@ int ensure_model(gs3dc_ctx* c, int N, int mc) {
     CK(c->op.ensure(n));
     CK(c->rec0.ensure(n));
     CK(c->rec1.ensure(n));
-    CK(c->col_b.ensure(n));
+    CK(c->cbt.ensure(n));
     CK(c->depth.ensure(n));
     CK(c->radius.ensure(n));
     CK(c->tiles.ensure(n));
@@ -997,7 +999,7 @@ struct BatchShape {
 
 ScreenPtrs batch_screen(gs3dc_ctx* c) {
     auto& b = c->batch;
-    return {b.rec0.p, b.rec1.p, b.col_b.p, b.depth.p, b.radius.p, b.tiles.p, nullptr, nullptr, nullptr, nullptr, nullptr};
+    return {b.rec0.p, b.rec1.p, b.cbt.p, b.depth.p, b.radius.p, b.tiles.p, nullptr, nullptr, nullptr, nullptr, nullptr};
 }
 PixelPtrs batch_pixels(gs3dc_ctx* c) {
     auto& b = c->batch;
@@ -1032,7 +1034,7 @@ int batch_buffers(gs3dc_ctx* c, const BatchShape& sh) {
     CK(b.views.ensure((size_t)sh.V));
     CK(b.rec0.ensure(vn));
     CK(b.rec1.ensure(vn));
-    CK(b.col_b.ensure(vn));
+    CK(b.cbt.ensure(vn));
     CK(b.depth.ensure(vn));
     CK(b.radius.ensure(vn));
     CK(b.tiles.ensure(vn));
@@ -1193,11 +1195,12 @@ void gs3dc_destroy(gs3dc_ctx* c) {
     drop_graphs(c);
     DevBuf<float>* fb[] = {&c->pos,    &c->sc,      &c->rot,     &c->sh,     &c->op,      &c->m_pos,  &c->v_pos,
                            &c->m_sc,   &c->v_sc,    &c->m_rot,   &c->v_rot,  &c->m_sh,    &c->v_sh,   &c->m_op,
-                           &c->v_op,   &c->g_pos,   &c->g_sc,    &c->g_rot,  &c->g_sh,    &c->g_op,   &c->col_b,
+                           &c->v_op,   &c->g_pos,   &c->g_sc,    &c->g_rot,  &c->g_sh,    &c->g_op,
                            &c->depth,  &c->c_cov3D, &c->c_pview, &c->c_phw,  &c->c_cov2D, &c->c_det,  &c->x_means2D,
                            &c->x_depths, &c->x_conics, &c->x_opac, &c->x_rgb, &c->dm2,    &c->dcon,   &c->drgb,
                            &c->dop,    &c->image,   &c->T_final, &c->d_image, &c->gt};
     for (auto* b : fb) b->release();
+    c->cbt.release();
     c->rec0.release();
     c->rec1.release();
     c->radius.release();
@@ -1682,10 +1685,10 @@ int gs3dc_rasterize_arrays(gs3dc_ctx* c, int num_gaussians, const gs3dc_screen_a
     CK(cudaSetDevice(c->device));
     if ((rc = ensure_pixels(c, cam->width, cam->height))) return rc;
     const size_t nn = n ? n : 1;
-    if (nn > c->rec0.n || nn > c->rec1.n || nn > c->col_b.n) drop_graphs(c);
+    if (nn > c->rec0.n || nn > c->rec1.n || nn > c->cbt.n) drop_graphs(c);
     CK(c->rec0.ensure(nn));
     CK(c->rec1.ensure(nn));
-    CK(c->col_b.ensure(nn));
+    CK(c->cbt.ensure(nn));
     CK(c->dm2.ensure(2 * nn));
     CK(c->dcon.ensure(3 * nn));
     CK(c->drgb.ensure(3 * nn));

@@ -187,13 +187,13 @@ __device__ __forceinline__ unsigned chosen_record(const StepParams& sp, bool vis
         }
         s.rec0[o] = make_float4(r.px, r.py, r.con[0], r.con[1]);
         s.rec1[o] = make_float4(r.con[2], r.opac, r.rgb[0], r.rgb[1]);
-        s.col_b[o] = r.rgb[2];
+        s.cbt[o] = blue_thr(r.rgb[2], r.opac);
         s.depth[o] = r.depth;
         s.radius[o] = r.radius;
     } else {
         s.rec0[o] = make_float4(0.f, 0.f, 0.f, 0.f);
         s.rec1[o] = make_float4(0.f, 0.f, 0.f, 0.f);
-        s.col_b[o] = 0.f;
+        s.cbt[o] = blue_thr(0.f, 0.f);
         s.depth[o] = 0.f;
         s.radius[o] = 0;
     }

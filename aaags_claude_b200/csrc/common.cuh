@@ -246,19 +246,6 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned 
 
 // Bounded wait for `phase` of the barrier: false (and kStatusTimeout) if the
 // copies have not landed after spin_limit polls.
-// ---- per-thread asynchronous copies (cp.async) into shared memory ----
-// 16 bytes (both addresses 16-byte aligned; cached in L2 only) or 4 bytes; a
-// thread's copies complete in commit order, cp_async_wait_all waits for all of
-// the thread's own.
-__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
-
 // Bulk prefetch of [src, src + bytes) into L2 (no shared memory, no completion
 // to wait for); src 16-byte aligned, bytes a multiple of 16.
 __device__ __forceinline__ void prefetch_l2(const void* src, unsigned bytes) {

@@ -642,7 +642,7 @@ __global__ void __launch_bounds__(kBlock) k_preprocess_e3(const StepParams* __re
         }
         s.rec0[i] = make_float4(pix_x, pix_y, 0.f, 0.f);
         s.rec1[i] = make_float4(0.f, opacity, rgb[0], rgb[1]);
-        s.col_b[i] = rgb[2];
+        s.cbt[i] = blue_thr(rgb[2], opacity);
         s.depth[i] = depth;
         s.radius[i] = radius;
         s.tiles[i] = cnt;

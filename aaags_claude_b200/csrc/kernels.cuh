@@ -39,11 +39,13 @@ struct AdamPtrs {
 // Screen-space records written by the preprocess and read by both rasterisers.
 //   rec0[i] = (mean.x, mean.y, conic.a, conic.b)
 //   rec1[i] = (conic.c, opacity_2d, r, g)
-//   col_b[i] = b
+//   cbt[i]  = (b, -log2(255 opacity_2d)): the blue channel and the base-2
+//             accept threshold (blue_thr), computed once per Gaussian instead
+//             of once per (Gaussian, tile) by the rasterisers' staging
 struct ScreenPtrs {
     float4* rec0;
     float4* rec1;
-    float* col_b;
+    float2* cbt;
     float* depth;
     int* radius;
     int* tiles;

@@ -211,13 +211,13 @@ __global__ void __launch_bounds__(kBlock) k_preprocess(const StepParams* __restr
             dbits = __float_as_uint(r.depth);
             s.rec0[i] = make_float4(r.px, r.py, r.con[0], r.con[1]);
             s.rec1[i] = make_float4(r.con[2], r.opac, r.rgb[0], r.rgb[1]);
-            s.col_b[i] = r.rgb[2];
+            s.cbt[i] = blue_thr(r.rgb[2], r.opac);
             s.depth[i] = r.depth;
             s.radius[i] = r.radius;
         } else {
             s.rec0[i] = make_float4(0.f, 0.f, 0.f, 0.f);
             s.rec1[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-            s.col_b[i] = 0.f;
+            s.cbt[i] = blue_thr(0.f, 0.f);
             s.depth[i] = 0.f;
             s.radius[i] = 0;
         }
@@ -372,7 +372,7 @@ __global__ void k_export_screen(int N, ScreenPtrs s, ScreenArrays a) {
     a.opac2d[i] = r1.y;
     a.rgb[3 * i] = r1.z;
     a.rgb[3 * i + 1] = r1.w;
-    a.rgb[3 * i + 2] = s.col_b[i];
+    a.rgb[3 * i + 2] = s.cbt[i].x;
     a.depths[i] = s.depth[i];
     a.radii[i] = s.radius[i];
     a.tiles[i] = s.tiles[i];
@@ -386,7 +386,7 @@ __global__ void k_import_screen(int N, ScreenArrays a, ScreenPtrs s) {
     if (i >= N) return;
     s.rec0[i] = make_float4(a.means2D[2 * i], a.means2D[2 * i + 1], a.conics[3 * i], a.conics[3 * i + 1]);
     s.rec1[i] = make_float4(a.conics[3 * i + 2], a.opac2d[i], a.rgb[3 * i], a.rgb[3 * i + 1]);
-    s.col_b[i] = a.rgb[3 * i + 2];
+    s.cbt[i] = blue_thr(a.rgb[3 * i + 2], a.opac2d[i]);
 }
 
 // ---- fused preprocess backward + optimiser, staged by TMA into shared memory ----

@@ -96,7 +96,7 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_bwd(const StepParams* __re
                                                             int n_views = 1, unsigned n_tiles = 0) {
     __shared__ float4 s_r0[BATCH];
     __shared__ float4 s_r1[BATCH];
-    __shared__ float2 s_bt[BATCH];   // (blue, skip threshold): one 8-byte load per Gaussian
+    __shared__ float2 s_bt[BATCH];   // (blue, the forward's threshold): one 8-byte load per Gaussian
     __shared__ unsigned s_idx[BATCH];
     // r, g, b, S_1, S_x, S_y, S_xx, S_xy, S_yy; rows padded by one word so that the
     // eight lanes adding values 0..7 of one Gaussian hit eight different banks
@@ -188,9 +188,10 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_bwd(const StepParams* __re
                 const unsigned gi = vals[j];
                 float4 r0 = s.rec0[gi];
                 float4 r1 = s.rec1[gi];
-                const float thr = skip_threshold(r1.y);
+                const float2 cb = s.cbt[gi];
+                const float thr = skip_threshold_from2(cb.y);
                 s_idx[e] = gi;
-                s_bt[e] = make_float2(s.col_b[gi], Accept::kBase2 ? accept_threshold2(r1.y) : thr);   // forward's
+                s_bt[e] = make_float2(cb.x, Accept::kBase2 ? cb.y : thr);   // the forward's
                 s_mask[e] = (unsigned char)strip_mask<kNW, 2 * PPT>(band_rows(r0, r1, thr, wx0, wx1), ty0);
                 if (Accept::kBase2) q_scale(r0, r1);   // as the forward stages it
                 s_r0[e] = r0;
@@ -362,7 +363,7 @@ __global__ void __launch_bounds__(256) k_list_bwd(const StepParams* __restrict__
         const float oma = 1.0f - alpha;
         const float Ti = oma > 1e-6f ? T / oma : 0.0f;
         const float4 r0 = s.rec0[gi], r1 = s.rec1[gi];
-        const float col[3] = {r1.z, r1.w, s.col_b[gi]};
+        const float col[3] = {r1.z, r1.w, s.cbt[gi].x};
         const float dx = r0.x - (float)x, dy = r0.y - (float)y;
         float d_alpha = 0.0f;
 #pragma unroll

@@ -126,6 +126,15 @@ __device__ __forceinline__ float ex2_approx(float q) {
 // separate alpha comparison follows.  Culling keeps skip_threshold's margin.
 __device__ __forceinline__ float accept_threshold2(float o) { return -log2f(255.0f * o); }
 
+// The screen record's (blue, accept threshold) pair, written by every preprocess.
+__device__ __forceinline__ float2 blue_thr(float b, float o) { return make_float2(b, accept_threshold2(o)); }
+
+// skip_threshold recovered from the stored accept threshold: ln(2) * (-log2(255 o))
+// less the same 1e-3 margin.  Against logf(1/(255 o)) the two roundings differ by
+// a few 1e-6, far inside the margin, so the bound stays conservative.
+constexpr float kLn2 = 0.6931471805599453f;
+__device__ __forceinline__ float skip_threshold_from2(float thr2) { return fmaf(thr2, kLn2, -1e-3f); }
+
 // The staged record of the reduced form carries the conic pre-scaled for q:
 // (x, y, -0.5 log2(e) a, -log2(e) b), (-0.5 log2(e) c, o, r, g).
 __device__ __forceinline__ void q_scale(float4& r0, float4& r1) {

@@ -47,7 +47,7 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_fwd(const StepParams* __re
                                                             unsigned n_tiles = 0) {
     __shared__ float4 s_r0[BATCH];
     __shared__ float4 s_r1[BATCH];
-    __shared__ float2 s_bt[BATCH];   // (blue, skip threshold): one 8-byte load per Gaussian
+    __shared__ float2 s_bt[BATCH];   // (blue, threshold): one 8-byte load per Gaussian
     constexpr int kFwdThreads = 256 / PPT;
     constexpr int kNW = kFwdThreads / 32;
     __shared__ unsigned char s_mask[BATCH];       // warps whose strip the Gaussian can reach
@@ -113,9 +113,10 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_fwd(const StepParams* __re
                 const unsigned g = vals[j];
                 float4 r0 = s.rec0[g];
                 float4 r1 = s.rec1[g];
-                const float thr = skip_threshold(r1.y);
-                // the threshold in the units of Blend's exponent
-                s_bt[e] = make_float2(s.col_b[g], Blend::kBase2 ? accept_threshold2(r1.y) : thr);
+                const float2 cb = s.cbt[g];
+                const float thr = skip_threshold_from2(cb.y);
+                // the threshold in the units of Blend's exponent: the stored base-2 one, or the skip bound
+                s_bt[e] = make_float2(cb.x, Blend::kBase2 ? cb.y : thr);
                 s_mask[e] = (unsigned char)strip_mask<kNW, 2 * PPT>(band_rows(r0, r1, thr, wx0, wx1), ty0);
                 if (Blend::kBase2) q_scale(r0, r1);
                 s_r0[e] = r0;
