@@ -91,6 +91,20 @@ inline cudaError_t set_smem_once(std::atomic<unsigned long long>& done, K* kerne
     return e;
 }
 
+// The largest shared-memory carveout for `kernel` (kernels built for several
+// CTAs per SM that need most of the 228 KB), once per device.
+template <typename K>
+inline cudaError_t set_carveout_max_once(std::atomic<unsigned long long>& done, K* kernel) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (done.load(std::memory_order_acquire) & bit) return cudaSuccess;
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+    if (e == cudaSuccess) done.fetch_or(bit, std::memory_order_acq_rel);
+    return e;
+}
+
 // Streaming multiprocessors of the current device, queried once per device
 // ordinal (grid sizes of the grid-stride and persistent launches; results never
 // depend on it).  1 if the query fails, which keeps every launch valid.
@@ -166,16 +180,20 @@ __device__ __forceinline__ unsigned long long lookback_exclusive_strided(
 // have published at least its aggregate, else the round is polled again
 // (bounded as above).  Blocks before block 0 count as a zero prefix.  Every
 // lane returns the exclusive prefix.
-__device__ __forceinline__ unsigned long long warp_lookback_exclusive(unsigned long long* desc, int blk,
-                                                                      unsigned long long aggregate,
-                                                                      unsigned* status, unsigned spin_limit) {
+//
+// Split in two for callers with work to do between publishing and walking:
+// lookback_publish (one thread) and warp_lookback_walk (the whole warp, after
+// the publish).
+__device__ __forceinline__ void lookback_publish(unsigned long long* desc, int blk, unsigned long long aggregate) {
+    st_relaxed(desc + blk, (blk == 0 ? kDescPrefix : kDescAgg) | aggregate);
+}
+
+__device__ __forceinline__ unsigned long long warp_lookback_walk(unsigned long long* desc, int blk,
+                                                                 unsigned long long aggregate, unsigned* status,
+                                                                 unsigned spin_limit) {
     const int lane = (int)(threadIdx.x & 31);
     unsigned long long* mine = desc + blk;
-    if (blk == 0) {
-        if (lane == 0) st_relaxed(mine, kDescPrefix | aggregate);
-        return 0ull;
-    }
-    if (lane == 0) st_relaxed(mine, kDescAgg | aggregate);
+    if (blk == 0) return 0ull;
     unsigned long long excl = 0;
     int base = blk - 1;
     unsigned spins = 0;
@@ -204,6 +222,13 @@ __device__ __forceinline__ unsigned long long warp_lookback_exclusive(unsigned l
     }
     if (lane == 0) st_relaxed(mine, kDescPrefix | (excl + aggregate));
     return excl;
+}
+
+__device__ __forceinline__ unsigned long long warp_lookback_exclusive(unsigned long long* desc, int blk,
+                                                                      unsigned long long aggregate,
+                                                                      unsigned* status, unsigned spin_limit) {
+    if ((threadIdx.x & 31) == 0) lookback_publish(desc, blk, aggregate);
+    return warp_lookback_walk(desc, blk, aggregate, status, spin_limit);
 }
 
 

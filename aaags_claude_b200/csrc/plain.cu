@@ -70,6 +70,10 @@ namespace {
 
 // ---------------- block scan + look-back + pair emission ----------------
 
+constexpr int kEmitRun = 4;                      // consecutive pair slots walked by one thread
+constexpr int kEmitChunk = kBlock * kEmitRun;    // pair slots staged per round
+constexpr unsigned kNoPair = 0xffffffffu;        // staged tile of a slot left unwritten (beyond `limit`)
+
 struct EmitShared {
     int warp[8];
     int excl[kBlock];
@@ -81,6 +85,8 @@ struct EmitShared {
     unsigned gid[kBlock];  // Gaussian index written as the pair's value
     unsigned tbase[kBlock];  // first global tile id of the Gaussian's view (0 for one view)
     int gx[kBlock];          // tile-grid width of the Gaussian's view
+    alignas(16) unsigned ctile[kEmitChunk];   // one round's pairs: tile id (or kNoPair)
+    alignas(16) unsigned cown[kEmitChunk];    // and the owning thread of the CTA
     unsigned long long base;
 };
 
@@ -89,6 +95,13 @@ struct EmitShared {
 // consecutive pairs (fully coalesced, balanced however uneven the rects).
 // Pair order: Gaussian-major, then row-major inside the rect
 // (tile_binner_cpu.cpp:90-97).
+// The pairs go out in rounds of kEmitChunk slots: each thread finds the owner
+// of its first kEmitRun consecutive slots by one binary search over the
+// CTA's exclusive scan and walks them (column, row and owner advance by
+// increments), staging tile and owner in shared memory; then the CTA writes
+// the round with consecutive threads on consecutive slots.  The CTA's
+// aggregate is published before the first round is staged, so the look-back
+// (warp 0, after its staging) usually finds its predecessors' prefixes ready.
 // With pr.tiles32 set, writes tile-only keys and counts the first nd 8-bit
 // digits of every tile into thist[nd][256] (shared memory).
 //
@@ -116,47 +129,88 @@ __device__ __forceinline__ void scan_and_emit(EmitShared& sm, int blk, unsigned 
     sm.gid[tid] = gid;
     sm.tbase[tid] = tile_base_t;
     sm.gx[tid] = grid_x_t < 0 ? grid_x : grid_x_t;
-    if (tid < 32) {
-        const unsigned long long ex =
-            warp_lookback_exclusive(pr.scan_desc, blk, (unsigned long long)total, &ctrl->status, spin_limit);
-        if (tid == 0) {
-            sm.base = ex;
-            if (blk == (int)gridDim.x - 1) ctrl->total_pairs = ex + (unsigned long long)total;
-            if (ex + (unsigned long long)total > pr.capacity) {
-                atomicOr(&ctrl->status, kStatusOverflow);
-                if (persist) atomicOr(&persist->sticky_overflow, 1u);
+    if (tid == 0) lookback_publish(pr.scan_desc, blk, (unsigned long long)total);
+    __syncthreads();
+    for (int c0 = 0;; c0 += kEmitChunk) {
+        // stage this round: slots c0 + kEmitRun * tid ..
+        const int k0 = c0 + kEmitRun * tid;
+        if (k0 < total) {
+            int lo = 0, hi = kBlock;   // the owner: last thread whose exclusive offset is <= k0
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (sm.excl[mid] <= k0) lo = mid;
+                else hi = mid;
+            }
+            int local = k0 - sm.excl[lo];
+            int end = lo + 1 < kBlock ? sm.excl[lo + 1] : total;
+            int w = sm.width[lo], lim = sm.limit[lo], gx = sm.gx[lo];
+            // local / w from the rounded reciprocal: for local < 2^23 the product is within one of the
+            // quotient, and one correction step each way makes it exact
+            int row = __float2int_rz((float)local * sm.winv[lo]);
+            if ((row + 1) * w <= local) row++;
+            else if (row * w > local) row--;
+            int col = local - row * w;
+            int r = sm.rect[lo];
+            unsigned tile = sm.tbase[lo] + (unsigned)(((r >> 16) + row) * gx + (r & 0xffff) + col);
+            unsigned st[kEmitRun], so[kEmitRun];
+#pragma unroll
+            for (int i = 0; i < kEmitRun; i++) {
+                const int k = k0 + i;
+                if (k < total && k == end) {   // next thread with pairs
+                    do {
+                        lo++;
+                        end = lo + 1 < kBlock ? sm.excl[lo + 1] : total;
+                    } while (end == k);
+                    local = 0;
+                    col = 0;
+                    w = sm.width[lo];
+                    lim = sm.limit[lo];
+                    gx = sm.gx[lo];
+                    r = sm.rect[lo];
+                    tile = sm.tbase[lo] + (unsigned)((r >> 16) * gx + (r & 0xffff));
+                }
+                st[i] = local < lim ? tile : kNoPair;
+                so[i] = (unsigned)lo;
+                local++;
+                tile++;
+                if (++col == w) {
+                    col = 0;
+                    tile += (unsigned)(gx - w);
+                }
+            }
+            *reinterpret_cast<uint4*>(&sm.ctile[kEmitRun * tid]) = make_uint4(st[0], st[1], st[2], st[3]);
+            *reinterpret_cast<uint4*>(&sm.cown[kEmitRun * tid]) = make_uint4(so[0], so[1], so[2], so[3]);
+        }
+        if (c0 == 0 && tid < 32) {
+            const unsigned long long ex =
+                warp_lookback_walk(pr.scan_desc, blk, (unsigned long long)total, &ctrl->status, spin_limit);
+            if (tid == 0) {
+                sm.base = ex;
+                if (blk == (int)gridDim.x - 1) ctrl->total_pairs = ex + (unsigned long long)total;
+                if (ex + (unsigned long long)total > pr.capacity) {
+                    atomicOr(&ctrl->status, kStatusOverflow);
+                    if (persist) atomicOr(&persist->sticky_overflow, 1u);
+                }
             }
         }
-    }
-    __syncthreads();
-    const unsigned long long base = sm.base;
-    for (int k = tid; k < total; k += kBlock) {
-        int lo = 0, hi = kBlock;
-        while (hi - lo > 1) {
-            const int mid = (lo + hi) >> 1;
-            if (sm.excl[mid] <= k) lo = mid;
-            else hi = mid;
+        __syncthreads();
+        const unsigned long long base = sm.base;
+        const int n = min(kEmitChunk, total - c0);
+        for (int j = tid; j < n; j += kBlock) {
+            const unsigned tile = sm.ctile[j];
+            const unsigned long long dst = base + (unsigned long long)(c0 + j);
+            if (tile == kNoPair || dst >= pr.capacity) continue;
+            const unsigned own = sm.cown[j];
+            if (pr.tiles32) {
+                pr.tiles32[dst] = tile;
+                for (int d = 0; d < nd; d++) atomicAdd(&thist[d * 256 + ((tile >> (8 * d)) & 255u)], 1u);
+            } else {
+                pr.keys[dst] = ((unsigned long long)tile << 32) | depth_fn(sm.depth[own], sm.gid[own], tile);
+            }
+            pr.vals[dst] = sm.gid[own];
         }
-        const int local = k - sm.excl[lo];
-        const unsigned long long dst = base + (unsigned long long)k;
-        if (local >= sm.limit[lo] || dst >= pr.capacity) continue;
-        const int w = sm.width[lo];
-        const int r = sm.rect[lo];
-        // local / w from the rounded reciprocal: for local < 2^23 the product is within one of the
-        // quotient, and one correction step each way makes it exact
-        int row = __float2int_rz((float)local * sm.winv[lo]);
-        if ((row + 1) * w <= local) row++;
-        else if (row * w > local) row--;
-        const int x = (r & 0xffff) + (local - row * w);
-        const int y = (r >> 16) + row;
-        const unsigned tile = sm.tbase[lo] + (unsigned)(y * sm.gx[lo] + x);
-        if (pr.tiles32) {
-            pr.tiles32[dst] = tile;
-            for (int d = 0; d < nd; d++) atomicAdd(&thist[d * 256 + ((tile >> (8 * d)) & 255u)], 1u);
-        } else {
-            pr.keys[dst] = ((unsigned long long)tile << 32) | depth_fn(sm.depth[lo], sm.gid[lo], tile);
-        }
-        pr.vals[dst] = sm.gid[lo];
+        if (c0 + kEmitChunk >= total) break;
+        __syncthreads();   // the next round restages the buffers
     }
 }
 

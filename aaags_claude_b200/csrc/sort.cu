@@ -82,18 +82,23 @@ __global__ void __launch_bounds__(kHistThreads) k_radix_hist(const K* __restrict
 // faster from tens of millions of keys on, slower at a few million).
 constexpr unsigned long long kWideSweepKeys = 1ull << 25;
 
-// Shared memory of one onesweep CTA (dynamic; ~60 KB for 64-bit keys at 16 per
-// thread, ~44 / ~76 KB for 32-bit keys at 16 / 32).
+// Shared memory of one onesweep CTA (dynamic; ~58 KB for 64-bit keys at 16 per
+// thread, ~42 / ~74 KB for 32-bit keys at 16 / 32).
 template <typename K, int ITEMS>
 struct SweepShared {
     K keys[kSortThreads * ITEMS];
     unsigned vals[kSortThreads * ITEMS];
-    unsigned whist[kSortThreads / 32][256];   // per-warp digit counts, then per-warp prefixes
-    unsigned long long gbase[256];            // global output offset of this tile's first key of digit d
-    unsigned dprefix[256];                    // tile-local exclusive prefix over digits
+    unsigned whist[kSortThreads / 32][256];   // per-warp digit counts, then the warp's first tile slot of digit d
+    unsigned long long gdelta[256];           // output index of tile slot j holding digit d: gdelta[d] + j
     unsigned long long scan[8];
     int tile;
 };
+
+// CTAs per SM a onesweep launch is built for: with the values loaded only for
+// the scatter, a thread holds its keys and 16-bit ranks, and shared memory
+// allows 3 CTAs at 8192 32-bit keys or 4096 64-bit keys, 5 at 4096 32-bit keys.
+template <typename K, int ITEMS>
+constexpr int sweep_ctas_per_sm() { return ITEMS > 16 || sizeof(K) > 4 ? 3 : 5; }
 
 // Exclusive scan over the 256 threads of one 64-bit value each.
 __device__ __forceinline__ unsigned long long block_exclusive_scan64(unsigned long long v, unsigned long long* s_w) {
@@ -113,10 +118,11 @@ __device__ __forceinline__ unsigned long long block_exclusive_scan64(unsigned lo
 }
 
 // One pass over digit `pass` (key bits 8*pass..); `slot` selects the digit
-// histogram and CTA ticket in the control block.
-// 2 CTAs per SM (register-bound): 64-bit keys at 16 per thread, 32-bit keys at 32.
+// histogram and CTA ticket in the control block.  The values are not held in
+// registers: the CTA asks for its slice to be brought into L2 when it starts
+// and loads each value where it scatters it.
 template <typename K, int ITEMS>
-__global__ void __launch_bounds__(kSortThreads, ITEMS > 16 || sizeof(K) > 4 ? 2 : 4) k_onesweep(const StepParams* __restrict__ sp,
+__global__ void __launch_bounds__(kSortThreads, sweep_ctas_per_sm<K, ITEMS>()) k_onesweep(const StepParams* __restrict__ sp,
                                                               const K* __restrict__ kin,
                                                               const unsigned* __restrict__ vin,
                                                               K* __restrict__ kout,
@@ -139,15 +145,19 @@ __global__ void __launch_bounds__(kSortThreads, ITEMS > 16 || sizeof(K) > 4 ? 2 
     const unsigned long long base = (unsigned long long)t * kTileKeys;
     if (base >= P) return;
 
+    if (tid == 0) {
+        // the tile's values (whole 16-byte units inside [base, P), from a 16-byte aligned start: a
+        // caller's buffer may be only 4-byte aligned) into L2 for the scatter
+        const unsigned long long nv = min((unsigned long long)kTileKeys, P - base) & ~3ull;
+        if (nv && (reinterpret_cast<uintptr_t>(vin + base) & 15u) == 0)
+            prefetch_l2(vin + base, (unsigned)(nv * sizeof(unsigned)));
+    }
     K key[kItems];
-    unsigned val[kItems];
-    unsigned rank[kItems];
+    unsigned rank2[(kItems + 1) / 2];   // two 16-bit ranks per register (a rank is < 32 * kItems)
 #pragma unroll
     for (int it = 0; it < kItems; it++) {
         const unsigned long long idx = base + (unsigned long long)(warp * 32 * kItems + it * 32 + lane);
-        const bool valid = idx < P;
-        key[it] = valid ? kin[idx] : (K)~(K)0;   // sentinel: digit 255, ranks after every real key
-        val[it] = valid ? vin[idx] : 0u;
+        key[it] = idx < P ? kin[idx] : (K)~(K)0;   // sentinel: digit 255, ranks after every real key
     }
     const unsigned lt_mask = (1u << lane) - 1u;
 #pragma unroll
@@ -162,7 +172,9 @@ __global__ void __launch_bounds__(kSortThreads, ITEMS > 16 || sizeof(K) > 4 ? 2 
         unsigned prior = 0;
         if (lane == leader) prior = atomicAdd(&sm.whist[warp][d], (unsigned)__popc(peers));
         prior = __shfl_sync(0xffffffffu, prior, leader);
-        rank[it] = prior + (unsigned)__popc(peers & lt_mask);
+        const unsigned rank = prior + (unsigned)__popc(peers & lt_mask);
+        if (it & 1) rank2[it >> 1] |= rank << 16;
+        else rank2[it >> 1] = rank;
     }
     __syncthreads();
     // thread d owns digit d: per-warp exclusive prefixes and the tile count
@@ -180,22 +192,26 @@ __global__ void __launch_bounds__(kSortThreads, ITEMS > 16 || sizeof(K) > 4 ? 2 
     const unsigned long long digit_start = block_exclusive_scan64(hist_d, sm.scan);
     const unsigned long long tile_excl =
         lookback_exclusive_strided(desc, t, 256, (int)d, (unsigned long long)run, &ctrl->status, sp->spin_limit);
-    sm.gbase[d] = digit_start + tile_excl;
-    sm.dprefix[d] = (unsigned)block_exclusive_scan64((unsigned long long)run, sm.scan);
+    // tile-local start of digit d, folded into the warps' prefixes and the output offset
+    const unsigned dp = (unsigned)block_exclusive_scan64((unsigned long long)run, sm.scan);
+#pragma unroll
+    for (int w = 0; w < kSortThreads / 32; w++) sm.whist[w][d] += dp;
+    sm.gdelta[d] = digit_start + tile_excl - dp;
     __syncthreads();
 #pragma unroll
     for (int it = 0; it < kItems; it++) {
+        const unsigned long long idx = base + (unsigned long long)(warp * 32 * kItems + it * 32 + lane);
         const unsigned dd = (unsigned)(key[it] >> shift) & 255u;
-        const unsigned pos = sm.dprefix[dd] + sm.whist[warp][dd] + rank[it];
+        const unsigned pos = sm.whist[warp][dd] + ((rank2[it >> 1] >> (16 * (it & 1))) & 0xffffu);
         sm.keys[pos] = key[it];
-        sm.vals[pos] = val[it];
+        sm.vals[pos] = idx < P ? vin[idx] : 0u;
     }
     __syncthreads();
     const int n_valid = (int)min((unsigned long long)kTileKeys, P - base);
     for (int j = tid; j < n_valid; j += kSortThreads) {
         const K k = sm.keys[j];
         const unsigned dd = (unsigned)(k >> shift) & 255u;
-        const unsigned long long out = sm.gbase[dd] + (unsigned long long)(j - (int)sm.dprefix[dd]);
+        const unsigned long long out = sm.gdelta[dd] + (unsigned long long)j;
         kout[out] = k;
         vout[out] = sm.vals[j];
     }
@@ -435,6 +451,8 @@ cudaError_t radix_sort_impl(cudaStream_t st, const StepParams* sp, int first, in
     const int smem = (int)sizeof(SweepShared<K, ITEMS>);
     cudaError_t e = set_smem_once(attr_done, k_onesweep<K, ITEMS>, smem);
     if (e != cudaSuccess) return e;
+    static std::atomic<unsigned long long> carve_done{0};
+    if ((e = set_carveout_max_once(carve_done, k_onesweep<K, ITEMS>)) != cudaSuccess) return e;
     if (!hist_done) {
         k_radix_hist<K><<<2 * sm_count(), kHistThreads, 0, st>>>(keys0, capacity, first, passes, slot_base, count, ctrl);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
