@@ -1105,8 +1105,7 @@ int seq_batch(gs3dc_ctx* c, const BatchShape& sh) {
     int which = 0;
     CK(launch_radix_sort32(c->stream, views, sh.tile_digits, 5, true, b.cap, b.keys[0].p, b.vals[0].p, b.keys[1].p,
                            b.vals[1].p, b.sort_desc.p, pstride, c->ctrl, &which));
-    CK(launch_tile_ranges_views(c->stream, b.cap, b.keys[which].p, b.vals[which].p, views, c->N, b.ranges.p,
-                                c->ctrl));
+    CK(launch_tile_ranges_views(c->stream, b.cap, b.keys[which].p, views, b.ranges.p, c->ctrl));
     CK(launch_tile_order(c->stream, b.ranges.p, (int)sh.tiles, b.order.p, c->ctrl));
     const bool tuning = c->autotune && !c->tune_batch.done;
     if (tuning) CK(cudaEventRecord(c->tune_ev[0], c->stream));

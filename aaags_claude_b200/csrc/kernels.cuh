@@ -213,9 +213,9 @@ cudaError_t launch_preprocess_plain(cudaStream_t st, const StepParams* sp, int N
 // the rectangle is recomputed from the stored mean and radius.
 // n_per_view > 0: several views; N counts (view, Gaussian) entries
 // view * n_per_view + i, and sp is the views' parameter array.  The keys are
-// the views' local tile ids: the emission order groups the pairs by view, so a
-// stable sort on the local id leaves every (view, tile) run contiguous
-// (launch_tile_ranges_views).
+// the views' local tile ids with the view above the tile digits: the emission
+// order groups the pairs by view, so a stable sort on the tile digits leaves
+// every (view, tile) run contiguous (launch_tile_ranges_views).
 // hist_parts (optional, zeroed, kHistParts * (kMaxPasses - kDepthDigits) * 256
 // counters): the CTAs add their counts into copy (CTA % kHistParts) and one
 // more kernel sums the copies into the control slots -- for launches of many
@@ -295,11 +295,10 @@ cudaError_t launch_radix_sort32(cudaStream_t st, const StepParams* sp, int digit
 cudaError_t launch_tile_ranges32(cudaStream_t st, unsigned long long capacity, const unsigned* tiles_sorted,
                                  unsigned* ranges, Control* ctrl);
 // Ranges of global tile ids (the view's tile_base + local id) over pairs
-// sorted stably by local tile id from a view-grouped emission: the view of a
-// pair is its value / n_per_view.
+// sorted stably by local tile id from a view-grouped emission: a key holds the
+// local id in its low 8 * (sort_passes - kDepthDigits) bits and the view above.
 cudaError_t launch_tile_ranges_views(cudaStream_t st, unsigned long long capacity, const unsigned* tiles_sorted,
-                                     const unsigned* vals_sorted, const StepParams* views, int n_per_view,
-                                     unsigned* ranges, Control* ctrl);
+                                     const StepParams* views, unsigned* ranges, Control* ctrl);
 
 // Heavy-first permutation of the tiles (by pair count, in power-of-two
 // buckets) for the rasterisers.  Above 65536 tiles (several views) it runs as

@@ -328,8 +328,10 @@ __global__ void __launch_bounds__(kBlock) k_emit_ranked(const StepParams* __rest
         g = rank_gid[r];
         if (n_per_view > 0) {
             // several views: entry g = view * n_per_view + Gaussian, spp is the views' parameter array;
-            // the key is the view's local tile id (the value tells the views apart)
-            gx = spp[g / (unsigned)n_per_view].grid_x;
+            // the key is the view's local tile id, with the view above the nd sorted digits
+            const unsigned view = g / (unsigned)n_per_view;
+            gx = spp[view].grid_x;
+            tbase = view << (8 * nd);
         }
         if (rects) {
             // tile rectangle stored by the preprocess: (xmin | ymin << 16, xmax | ymax << 16); its

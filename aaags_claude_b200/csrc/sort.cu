@@ -220,32 +220,29 @@ __global__ void __launch_bounds__(kSortThreads, sweep_ctas_per_sm<K, ITEMS>()) k
 __device__ __forceinline__ unsigned tile_of(unsigned long long key) { return (unsigned)(key >> 32); }
 
 // Ranges of (view, tile) runs: a run starts / ends where the global id changes.
-// Four pairs per thread from 16-byte loads of the keys and values; each id is
-// compared with its successor's (as k_ranges32).
-__global__ void k_ranges_views4(const unsigned* __restrict__ keys, const unsigned* __restrict__ vals,
-                                const StepParams* __restrict__ views, unsigned n_per_view,
+// A key is the view's local tile id in its low 8 * tile digits bits and the
+// view above them (the emission puts it there; the sort leaves it alone).
+// Four pairs per thread from one 16-byte load; each id is compared with its
+// successor's (as k_ranges32).
+__global__ void k_ranges_views4(const unsigned* __restrict__ keys, const StepParams* __restrict__ views,
                                 unsigned long long capacity, unsigned* __restrict__ ranges, Control* ctrl) {
     const unsigned long long P = min(ctrl->total_pairs, capacity);
     const unsigned long long i0 = 4ull * ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x);
     if (i0 >= P) return;
-    unsigned k[5], v[5];
+    const int tile_bits = 8 * (views[0].sort_passes - kDepthDigits);
+    const unsigned local_mask = (1u << tile_bits) - 1u;   // tile_bits <= 24
+    unsigned k[5];
     if (i0 + 4 <= capacity) {
         const uint4 kk = *reinterpret_cast<const uint4*>(keys + i0);
-        const uint4 vv = *reinterpret_cast<const uint4*>(vals + i0);
         k[0] = kk.x, k[1] = kk.y, k[2] = kk.z, k[3] = kk.w;
-        v[0] = vv.x, v[1] = vv.y, v[2] = vv.z, v[3] = vv.w;
     } else {
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-            k[j] = i0 + j < P ? keys[i0 + j] : 0u;
-            v[j] = i0 + j < P ? vals[i0 + j] : 0u;
-        }
+        for (int j = 0; j < 4; j++) k[j] = i0 + j < P ? keys[i0 + j] : 0u;
     }
     k[4] = i0 + 4 < P ? keys[i0 + 4] : 0u;
-    v[4] = i0 + 4 < P ? vals[i0 + 4] : 0u;
     unsigned t[5];
 #pragma unroll
-    for (int j = 0; j < 5; j++) t[j] = views[v[j] / n_per_view].tile_base + k[j];
+    for (int j = 0; j < 5; j++) t[j] = views[k[j] >> tile_bits].tile_base + (k[j] & local_mask);
     if (i0 == 0) ranges[2 * t[0]] = 0u;
 #pragma unroll
     for (int j = 0; j < 4; j++) {
@@ -514,11 +511,10 @@ cudaError_t launch_tile_ranges(cudaStream_t st, unsigned long long capacity, con
 }
 
 cudaError_t launch_tile_ranges_views(cudaStream_t st, unsigned long long capacity, const unsigned* tiles_sorted,
-                                     const unsigned* vals_sorted, const StepParams* views, int n_per_view,
-                                     unsigned* ranges, Control* ctrl) {
-    if (capacity == 0 || n_per_view <= 0) return cudaSuccess;
-    k_ranges_views4<<<(unsigned)((capacity + 1023) / 1024), 256, 0, st>>>(tiles_sorted, vals_sorted, views,
-                                                                         (unsigned)n_per_view, capacity, ranges, ctrl);
+                                     const StepParams* views, unsigned* ranges, Control* ctrl) {
+    if (capacity == 0) return cudaSuccess;
+    k_ranges_views4<<<(unsigned)((capacity + 1023) / 1024), 256, 0, st>>>(tiles_sorted, views, capacity, ranges,
+                                                                         ctrl);
     return cudaGetLastError();
 }
 

@@ -376,9 +376,10 @@ def config_clustered_3m() -> Workload:
     return Workload("clustered_3M_1920x1080", s, cams, perturbed(s))
 
 
-def config_batched_64() -> Workload:
-    """Batched training: N=1M, 64 cameras of mixed resolution and FOV."""
-    s = random_scene(1_000_000)
+def config_batched_64(n: int = 1_000_000) -> Workload:
+    """Batched training: N=1M (n for smaller profiling cases), 64 cameras of
+    mixed resolution and FOV."""
+    s = random_scene(n)
     res = [(320, 240), (640, 480), (1280, 720), (1920, 1080), (3840, 2160)]
     cams = sphere_cameras(64, resolutions=res, fov_range=(45.0, 75.0))
-    return Workload("batched_64views_1M", s, cams, perturbed(s))
+    return Workload("batched_64views_1M" if n == 1_000_000 else f"batched_64views_{n}", s, cams, perturbed(s))

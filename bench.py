@@ -80,6 +80,8 @@ def _args(argv=None):
                     help="print only the eval_3D render measurement (profiling runs)")
     ap.add_argument("--only-batched", dest="only_batched", action="store_true",
                     help="print only the 64-view measurement (profiling runs)")
+    ap.add_argument("--batched-gaussians", dest="batched_gaussians", type=int, default=1_000_000,
+                    help="scene size of the 64-view step (profiling cases use less)")
     return ap.parse_args(argv)
 
 
@@ -537,7 +539,7 @@ def measure_batched(a, local: int) -> dict:
     import torch
     from aaags_claude_b200 import gs3d
     from aaags_claude_b200 import scenes as S
-    w = S.config_batched_64()
+    w = S.config_batched_64(a.batched_gaussians)
     cams = w.cameras
     cfg, tc = S.render_config(True), S.train_config()
     ctx = gs3d.Context(local)
@@ -605,7 +607,8 @@ def measure_batched(a, local: int) -> dict:
     ms_p = timed(one_by_one)
     p1 = graph_stats()
     ctx.close()
-    return {"workload": "batched_64views_1M_gaussians_mixed_320x240_to_3840x2160", "views": len(cams),
+    gname = "1M" if a.batched_gaussians == 1_000_000 else str(a.batched_gaussians)
+    return {"workload": f"batched_64views_{gname}_gaussians_mixed_320x240_to_3840x2160", "views": len(cams),
             "mpix_per_step": round(pix / 1e6, 2), "steps": steps,
             "batched_bf16": {"ms_per_step": round(ms_b, 3), "mpix_per_s": round(pix / 1e6 / (ms_b * 1e-3), 1),
                              "gpu_launches_per_step": launches_b, "loss_first": loss0, "loss_last": loss_b,
