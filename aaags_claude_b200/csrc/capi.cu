@@ -817,12 +817,30 @@ int seq_front_depth_first(gs3dc_ctx* c) {
 
 // Back half of a train step of the reduced-storage form: fast-exp
 // rasterisers, fused adjoint + Adam.
-int seq_back_chosen(gs3dc_ctx* c) {
+// The train step's forward rasteriser: with the fused L1, or (loss_later: the
+// target is still being copied in) without the loss.
+int seq_train_forward(gs3dc_ctx* c, bool loss_later) {
+    const int w = c->sorted_which;
+    if (chosen_form(c))
+        CK(launch_raster_fwd_fast(c->stream, c->sp_dev, c->num_tiles, c->ranges.p, c->tile_order.p, c->vals[w].p,
+                                  screen_ptrs(c, false), pixel_ptrs(c), c->ctrl, c->fwd_ppt, c->fwd_batch, loss_later));
+    else
+        CK(launch_raster_fwd_plain(c->stream, c->sp_dev, c->num_tiles, true, c->ranges.p, c->tile_order.p,
+                                   c->vals[w].p, screen_ptrs(c, false), pixel_ptrs(c), c->ctrl, c->fwd_ppt,
+                                   c->fwd_batch, loss_later));
+    return GS3DC_OK;
+}
+
+int seq_back_chosen(gs3dc_ctx* c, bool loss_later) {
     int rc;
     const int w = c->sorted_which;
-    if ((rc = mark(c, GS3DC_STAGE_RASTER_FWD))) return rc;
-    CK(launch_raster_fwd_fast(c->stream, c->sp_dev, c->num_tiles, c->ranges.p, c->tile_order.p, c->vals[w].p,
-                              screen_ptrs(c, false), pixel_ptrs(c), c->ctrl, c->fwd_ppt, c->fwd_batch));
+    if (loss_later) {
+        CK(launch_l1_loss(c->stream, c->sp_dev, pixel_ptrs(c), (size_t)c->W * c->H, c->ctrl));
+        c->kernels_last += 1;
+    } else {
+        if ((rc = mark(c, GS3DC_STAGE_RASTER_FWD))) return rc;
+        if ((rc = seq_train_forward(c, false))) return rc;
+    }
     if ((rc = mark(c, GS3DC_STAGE_RASTER_BWD))) return rc;
     CK(launch_raster_bwd_fast(c->stream, c->sp_dev, c->num_tiles, c->ranges.p, c->tile_order.p, c->vals[w].p,
                               screen_ptrs(c, false), pixel_ptrs(c), rgrad_ptrs(c), c->ctrl, c->bwd_ppt,
@@ -837,8 +855,10 @@ int seq_back_chosen(gs3dc_ctx* c) {
     return GS3DC_OK;
 }
 
-// Front half of a train step: preprocess, pair emission, sort, tile ranges.
-int seq_train_front(gs3dc_ctx* c) {
+// Front half of a train step: preprocess, pair emission, sort, tile ranges
+// (loss_later: and the forward rasteriser without the loss, which then
+// overlaps the target's copy too).
+int seq_train_front(gs3dc_ctx* c, bool loss_later = false) {
     int rc;
     c->mode_e3 = false;   // training is the 2D path only
     c->screen_n = c->N;
@@ -849,18 +869,27 @@ int seq_train_front(gs3dc_ctx* c) {
         if ((rc = seq_preprocess(c, false))) return rc;
         if ((rc = seq_sort(c))) return rc;
     }
+    if (loss_later) {
+        if ((rc = mark(c, GS3DC_STAGE_RASTER_FWD))) return rc;
+        if ((rc = seq_train_forward(c, true))) return rc;
+    }
     return GS3DC_OK;
 }
 
 // Back half: forward rasteriser with the fused L1 (the only reader of the
-// target), backward rasteriser, preprocess backward, optimiser.
-int seq_train_back(gs3dc_ctx* c) {
+// target) or, after a loss_later front half, the L1 alone; backward
+// rasteriser, preprocess backward, optimiser.
+int seq_train_back(gs3dc_ctx* c, bool loss_later = false) {
     int rc;
-    if (chosen_form(c)) return seq_back_chosen(c);
+    if (chosen_form(c)) return seq_back_chosen(c, loss_later);
     const int w = c->sorted_which;
-    if ((rc = mark(c, GS3DC_STAGE_RASTER_FWD))) return rc;
-    CK(launch_raster_fwd_plain(c->stream, c->sp_dev, c->num_tiles, true, c->ranges.p, c->tile_order.p, c->vals[w].p,
-                               screen_ptrs(c, false), pixel_ptrs(c), c->ctrl, c->fwd_ppt, c->fwd_batch));
+    if (loss_later) {
+        CK(launch_l1_loss(c->stream, c->sp_dev, pixel_ptrs(c), (size_t)c->W * c->H, c->ctrl));
+        c->kernels_last += 1;
+    } else {
+        if ((rc = mark(c, GS3DC_STAGE_RASTER_FWD))) return rc;
+        if ((rc = seq_train_forward(c, false))) return rc;
+    }
     if ((rc = mark(c, GS3DC_STAGE_RASTER_BWD))) return rc;
     CK(launch_raster_bwd_plain(c->stream, c->sp_dev, c->num_tiles, true, c->ranges.p, c->tile_order.p, c->vals[w].p,
                                screen_ptrs(c, false), pixel_ptrs(c), rgrad_ptrs(c), c->ctrl, c->bwd_ppt,
@@ -1918,6 +1947,10 @@ int gs3dc_train_step(gs3dc_ctx* c, const gs3d_camera* cam, const float* gt, int 
         bool v;
         ~RestoreTiming() { c->stage_timing = v; }
     } restore_timing{c, user_timing};
+    // a target from host memory: the forward runs before its copy has landed (front half) and the
+    // L1 follows in the back half, so the copy overlaps the forward too; timed steps keep the fused
+    // L1 (the stage events would count the wait)
+    const bool loss_later = host_gt && !c->stage_timing;
     for (int attempt = 0; attempt < 3; attempt++) {
         c->adam_step = step_before + (tc->use_adam ? 1 : 0);
         if ((rc = push_params(c, cam, cfg, tc, iteration, gt_dev))) return rc;
@@ -1925,7 +1958,8 @@ int gs3dc_train_step(gs3dc_ctx* c, const gs3d_camera* cam, const float* gt, int 
             c->N, c->max_coeffs, cam->width, cam->height, (long long)c->cap, c->sort_passes,
             (long long)c->spin_limit,
             (c->fused_adam ? 1 : 2) + 4 * c->sort_mode + 16 * c->form + 64 * (c->keep_grads ? 1 : 0) +
-                128 * c->fwd_ppt + 1024 * c->bwd_ppt + 8192 * c->fwd_batch + 8192 * 512 * c->bwd_batch,
+                128 * c->fwd_ppt + 1024 * c->bwd_ppt + 8192 * c->fwd_batch + 8192 * 512 * c->bwd_batch +
+                (loss_later ? 1ll << 40 : 0ll),
             (long long)g_alloc_epoch.load(std::memory_order_relaxed)};
         c->kernels_last = 0;
         if (c->use_graph && !c->stage_timing && !first && attempt == 0) {
@@ -1934,7 +1968,7 @@ int gs3dc_train_step(gs3dc_ctx* c, const gs3d_camera* cam, const float* gt, int 
                 slot = victim_slot(c);
                 cudaGraph_t g;
                 CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-                rc = seq_train_front(c);
+                rc = seq_train_front(c, loss_later);
                 cudaError_t ec = cudaStreamEndCapture(c->stream, &g);
                 if (rc) return rc;
                 CK(ec);
@@ -1942,7 +1976,7 @@ int gs3dc_train_step(gs3dc_ctx* c, const gs3d_camera* cam, const float* gt, int 
                 cudaGraphDestroy(g);
                 CK(ei);
                 CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-                rc = seq_train_back(c);
+                rc = seq_train_back(c, loss_later);
                 ec = cudaStreamEndCapture(c->stream, &g);
                 if (rc) {
                     drop_slot(*slot);
@@ -1965,9 +1999,9 @@ int gs3dc_train_step(gs3dc_ctx* c, const gs3d_camera* cam, const float* gt, int 
             CK(cudaGraphLaunch(slot->back, c->stream));
             c->graph_replays++;
         } else {
-            if ((rc = seq_train_front(c))) return rc;
+            if ((rc = seq_train_front(c, loss_later))) return rc;
             if (host_gt) CK(cudaStreamWaitEvent(c->stream, c->ev_gt_ready, 0));
-            if ((rc = seq_train_back(c))) return rc;
+            if ((rc = seq_train_back(c, loss_later))) return rc;
         }
         if (host_gt) {
             CK(cudaEventRecord(c->ev_gt_free[gslot], c->stream));

@@ -768,12 +768,12 @@ cudaError_t launch_raster_fwd_fast_multi(cudaStream_t st, const StepParams* view
         constexpr int kP = decltype(P)::value, kB = decltype(Bt)::value;
         static int per_sm = 0;
         if (!per_sm) {
-            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_raster_fwd<true, FastBlend, true, kP, kB>,
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_raster_fwd<kFusedL1, FastBlend, true, kP, kB>,
                                                               256 / kP, 0) != cudaSuccess ||
                 per_sm < 1)
                 per_sm = 1;
         }
-        k_raster_fwd<true, FastBlend, true, kP, kB><<<per_sm * sm_count(), 256 / kP, 0, st>>>(
+        k_raster_fwd<kFusedL1, FastBlend, true, kP, kB><<<per_sm * sm_count(), 256 / kP, 0, st>>>(
             views, ranges, order, vals, s, px, ctrl, n_views, n_tiles);
         return cudaGetLastError();
     });
@@ -781,12 +781,16 @@ cudaError_t launch_raster_fwd_fast_multi(cudaStream_t st, const StepParams* view
 
 cudaError_t launch_raster_fwd_fast(cudaStream_t st, const StepParams* sp, int num_tiles, const unsigned* ranges,
                                    const unsigned* order, const unsigned* vals, ScreenPtrs s, PixelPtrs px,
-                                   Control* ctrl, int ppt, int batch) {
+                                   Control* ctrl, int ppt, int batch, bool loss_later) {
     if (num_tiles <= 0) return cudaSuccess;
     return with_ppt_batch(ppt, batch, [&](auto P, auto Bt) {
         constexpr int kP = decltype(P)::value, kB = decltype(Bt)::value;
-        k_raster_fwd<true, FastBlend, false, kP, kB><<<num_tiles, 256 / kP, 0, st>>>(sp, ranges, order, vals, s, px,
-                                                                                    ctrl);
+        if (loss_later)
+            k_raster_fwd<kLossLater, FastBlend, false, kP, kB><<<num_tiles, 256 / kP, 0, st>>>(sp, ranges, order, vals,
+                                                                                              s, px, ctrl);
+        else
+            k_raster_fwd<kFusedL1, FastBlend, false, kP, kB><<<num_tiles, 256 / kP, 0, st>>>(sp, ranges, order, vals, s,
+                                                                                            px, ctrl);
         return cudaGetLastError();
     });
 }

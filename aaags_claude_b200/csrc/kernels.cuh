@@ -170,10 +170,11 @@ cudaError_t launch_chosen_to_raw(cudaStream_t st, int N, int mc3, bool fp16, Cho
 // entry by (view, depth)).
 cudaError_t launch_chosen_preprocess(cudaStream_t st, const StepParams* sp, int N, bool fp16, ChosenPtrs c,
                                      ScreenPtrs s, DepthKeys dk, uint2* rects, Control* ctrl, int n_views = 1);
-// Forward rasteriser with the fast-exp blend decision and fused L1.
+// Forward rasteriser with the fast-exp blend decision and fused L1
+// (loss_later: no loss; launch_l1_loss follows).
 cudaError_t launch_raster_fwd_fast(cudaStream_t st, const StepParams* sp, int num_tiles, const unsigned* ranges,
                                    const unsigned* order, const unsigned* vals, ScreenPtrs s, PixelPtrs px,
-                                   Control* ctrl, int ppt = 2, int batch = 128);
+                                   Control* ctrl, int ppt = 2, int batch = 128, bool loss_later = false);
 // One persistent launch over all tiles of n_views views (views = their
 // parameter array, order = all global tiles, heavy first).
 cudaError_t launch_raster_fwd_fast_multi(cudaStream_t st, const StepParams* views, int n_views, unsigned n_tiles,
@@ -242,9 +243,14 @@ cudaError_t launch_raster_e3(cudaStream_t st, const StepParams* sp, int num_tile
 // order: tile permutation (heavy first) or NULL for row-major
 // batch: the records staged per round (64, 128, 256) in the train step's launches (fused loss /
 // FROM_SIGN); the stage API's launches stage 128.
+// fused_loss && loss_later: a train step's forward without the loss (launch_l1_loss follows).
 cudaError_t launch_raster_fwd_plain(cudaStream_t st, const StepParams* sp, int num_tiles, bool fused_loss,
                                     const unsigned* ranges, const unsigned* order, const unsigned* vals,
-                                    ScreenPtrs s, PixelPtrs px, Control* ctrl, int ppt = 2, int batch = 128);
+                                    ScreenPtrs s, PixelPtrs px, Control* ctrl, int ppt = 2, int batch = 128,
+                                    bool loss_later = false);
+// The train step's L1 over the image of a loss_later forward and the target at
+// sp->gt: sign bytes and the loss sum, as the fused forward writes them.
+cudaError_t launch_l1_loss(cudaStream_t st, const StepParams* sp, PixelPtrs px, size_t n_pix, Control* ctrl);
 cudaError_t launch_raster_bwd_plain(cudaStream_t st, const StepParams* sp, int num_tiles, bool from_sign,
                                     const unsigned* ranges, const unsigned* order, const unsigned* vals,
                                     ScreenPtrs s, PixelPtrs px, RGradPtrs g, Control* ctrl, int ppt = 2,

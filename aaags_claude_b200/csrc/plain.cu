@@ -862,19 +862,30 @@ cudaError_t launch_raster_e3(cudaStream_t st, const StepParams* sp, int num_tile
 
 cudaError_t launch_raster_fwd_plain(cudaStream_t st, const StepParams* sp, int num_tiles, bool fused_loss,
                                     const unsigned* ranges, const unsigned* order, const unsigned* vals,
-                                    ScreenPtrs s, PixelPtrs px, Control* ctrl, int ppt, int batch) {
+                                    ScreenPtrs s, PixelPtrs px, Control* ctrl, int ppt, int batch, bool loss_later) {
     if (num_tiles <= 0) return cudaSuccess;
     if (!fused_loss) batch = 128;   // renders and the stage API
     return with_ppt_batch(ppt, batch, [&](auto P, auto Bt) {
         constexpr int kP = decltype(P)::value, kB = decltype(Bt)::value;
-        if (fused_loss)
-            k_raster_fwd<true, ExactBlend, false, kP, kB><<<num_tiles, 256 / kP, 0, st>>>(sp, ranges, order, vals, s,
-                                                                                         px, ctrl);
+        if (fused_loss && loss_later)
+            k_raster_fwd<kLossLater, ExactBlend, false, kP, kB><<<num_tiles, 256 / kP, 0, st>>>(
+                sp, ranges, order, vals, s, px, ctrl);
+        else if (fused_loss)
+            k_raster_fwd<kFusedL1, ExactBlend, false, kP, kB><<<num_tiles, 256 / kP, 0, st>>>(sp, ranges, order, vals,
+                                                                                             s, px, ctrl);
         else
-            k_raster_fwd<false, ExactBlend, false, kP, kFwdBatch><<<num_tiles, 256 / kP, 0, st>>>(
+            k_raster_fwd<kCountContrib, ExactBlend, false, kP, kFwdBatch><<<num_tiles, 256 / kP, 0, st>>>(
                 sp, ranges, order, vals, s, px, ctrl);
         return cudaGetLastError();
     });
+}
+
+cudaError_t launch_l1_loss(cudaStream_t st, const StepParams* sp, PixelPtrs px, size_t n_pix, Control* ctrl) {
+    if (n_pix == 0) return cudaSuccess;
+    const size_t want = (n_pix + 255) / 256;
+    const size_t cap = 8ull * (size_t)sm_count();
+    k_l1_loss<<<(unsigned)(want < cap ? want : cap), 256, 0, st>>>(sp, px, n_pix, ctrl);
+    return cudaGetLastError();
 }
 
 namespace {

@@ -22,14 +22,17 @@ namespace {
 // memory with, per record, the warps whose strip the Gaussian can reach
 // (band_rows: the rows of the tile's columns inside its alpha >= 1/255
 // ellipse); each warp walks its own compacted list of the batch; the CTA
-// stops once every pixel saturated.  Optional fused L1 (sign byte per pixel,
-// double-precision loss sum); with it (a train step) the contributor counts
-// are not kept, the backward starts from each pixel's last contributor.
+// stops once every pixel saturated.  LOSS: kCountContrib (renders: contributor
+// counts kept), kFusedL1 (a train step: sign byte per pixel and the
+// double-precision loss sum; the backward starts from each pixel's last
+// contributor, no counts) or kLossLater (a train step whose target is still
+// being copied in: neither, k_l1_loss follows once it has landed).
 //
 // PPT (pixels per thread: 1, 2 or 4) sets the threads per tile (256 / PPT)
 // and each warp's strip (16 x 2*PPT rows); BATCH (64, 128 or 256) the records
 // staged per round.  The results depend on neither.
 constexpr int kFwdBatch = 128;
+constexpr int kCountContrib = 0, kFusedL1 = 1, kLossLater = 2;
 
 //
 // MULTI: one persistent launch over the tiles of several views.  spp is then
@@ -38,7 +41,7 @@ constexpr int kFwdBatch = 128;
 // by its global id and renders it with that view's camera into the view's
 // slice of the concatenated pixel buffers.  The fused loss adds each view's
 // sum weighted by its inv_n.
-template <bool FUSED_LOSS, class Blend, bool MULTI = false, int PPT = 2, int BATCH = kFwdBatch>
+template <int LOSS, class Blend, bool MULTI = false, int PPT = 2, int BATCH = kFwdBatch>
 __global__ void __launch_bounds__(256 / PPT) k_raster_fwd(const StepParams* __restrict__ spp,
                                                             const unsigned* __restrict__ ranges,
                                                             const unsigned* __restrict__ order,
@@ -164,7 +167,7 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_fwd(const StepParams* __re
                     C[p][2] += bt.x * alpha * T[p];
                 }
                 T[p] = test_T;
-                if (!FUSED_LOSS) cnt[p]++;   // a train step's backward needs only the last index
+                if (LOSS == kCountContrib) cnt[p]++;   // a train step's backward needs only the last index
                 last[p] = b + (unsigned)k + 1u;
             }
         }
@@ -183,9 +186,9 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_fwd(const StepParams* __re
             px.image[3 * pix + 1] = o1;
             px.image[3 * pix + 2] = o2;
             if (px.T_final) px.T_final[pix] = T[p];
-            if (!FUSED_LOSS && px.n_contrib) px.n_contrib[pix] = cnt[p];
+            if (LOSS == kCountContrib && px.n_contrib) px.n_contrib[pix] = cnt[p];
             if (px.last_j) px.last_j[pix] = last[p];
-            if (FUSED_LOSS) {
+            if (LOSS == kFusedL1) {
                 // loss.cpp:8-14: diff = rendered - gt, sign gradient +-1/n
                 const float d0 = o0 - sp.gt[3 * pix], d1 = o1 - sp.gt[3 * pix + 1], d2 = o2 - sp.gt[3 * pix + 2];
                 const unsigned sg = (d0 > 0.f ? 1u : (d0 < 0.f ? 2u : 0u)) | (d1 > 0.f ? 4u : (d1 < 0.f ? 8u : 0u)) |
@@ -195,7 +198,7 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_fwd(const StepParams* __re
             }
         }
     }
-    if (FUSED_LOSS) {
+    if (LOSS == kFusedL1) {
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
         if (lane == 0) s_loss[warp] = lsum;
@@ -208,6 +211,35 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_fwd(const StepParams* __re
         }
         __syncthreads();
     }
+    }
+}
+
+// The train step's L1 (loss.cpp:8-14) over a forward image rendered with
+// kLossLater: per pixel the sign byte of image - target and the
+// double-precision sum |image - target|, as the fused form computes them
+// (the sum in a different order: equal to double rounding).  Grid-stride.
+__global__ void __launch_bounds__(256) k_l1_loss(const StepParams* __restrict__ spp, PixelPtrs px, size_t n_pix,
+                                                 Control* ctrl) {
+    __shared__ double s_loss[8];
+    const StepParams& sp = *spp;
+    double lsum = 0.0;
+    for (size_t pix = (size_t)blockIdx.x * blockDim.x + threadIdx.x; pix < n_pix;
+         pix += (size_t)gridDim.x * blockDim.x) {
+        const float d0 = px.image[3 * pix] - sp.gt[3 * pix], d1 = px.image[3 * pix + 1] - sp.gt[3 * pix + 1],
+                    d2 = px.image[3 * pix + 2] - sp.gt[3 * pix + 2];
+        const unsigned sg = (d0 > 0.f ? 1u : (d0 < 0.f ? 2u : 0u)) | (d1 > 0.f ? 4u : (d1 < 0.f ? 8u : 0u)) |
+                            (d2 > 0.f ? 16u : (d2 < 0.f ? 32u : 0u));
+        px.dsign[pix] = (unsigned char)sg;
+        lsum += (double)fabsf(d0) + (double)fabsf(d1) + (double)fabsf(d2);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
+    if ((threadIdx.x & 31) == 0) s_loss[threadIdx.x >> 5] = lsum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < 8; w++) t += s_loss[w];
+        atomicAdd(&ctrl->loss_sum, t);
     }
 }
 
