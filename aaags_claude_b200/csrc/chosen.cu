@@ -81,10 +81,10 @@ template <typename S>
 __device__ __forceinline__ S cvt_sr(float x, unsigned r);
 template <>
 __device__ __forceinline__ __nv_bfloat16 cvt_sr<__nv_bfloat16>(float x, unsigned r) {
-    // BF16 is the top half of the FP32 pattern: add 16 random bits below it, truncate
+    // BF16 is the top half of the FP32 pattern: add 16 random bits (r's upper half) below it, truncate
     unsigned u = __float_as_uint(x);
     if ((u & 0x7f800000u) == 0x7f800000u) return __float2bfloat16_rn(x);   // inf / nan
-    u += r & 0xffffu;
+    u += r >> 16;
     return __ushort_as_bfloat16((unsigned short)(u >> 16));
 }
 template <>
@@ -301,28 +301,33 @@ __device__ __forceinline__ float opt_elem(const StepParams& sp, float p, float& 
     return p - lr * g;
 }
 
-// Random words of one element's three roundings: the hash of (element, step)
-// and two LCG steps from it.
+// Random words of the roundings: the hash of (element, step) seeds a
+// full-period LCG modulo 2^32 (odd increment, multiplier 1 mod 4) whose
+// states follow; cvt_sr reads their upper bits.
+__device__ __forceinline__ unsigned lcg_next(unsigned s) { return s * 0x2C1B3C6Du + 0x297A2D39u; }
+
+// One element's three roundings.
 __device__ __forceinline__ void sr_words(unsigned e, unsigned seed, unsigned& rp, unsigned& rm, unsigned& rv) {
     rp = mix32(e, seed);
-    rm = rp * 0x2C1B3C6Du + 0x297A2D39u;
-    rv = rm * 0x2C1B3C6Du + 0x297A2D39u;
+    rm = lcg_next(rp);
+    rv = lcg_next(rm);
 }
 
 // Eight consecutive 16-bit parameters (p) with their BF16 moments (m, v),
-// updated in registers; e0 = the first element's global index.
+// updated in registers; e0 = the first element's global index.  One hash of
+// (e0, step) seeds the LCG that gives all 24 roundings' random words.
 template <typename S>
 __device__ __forceinline__ void opt8(const StepParams& sp, uint4& p, uint4& m, uint4& v, const float g[8],
                                      const float lr[8], unsigned e0, unsigned salt) {
     S* pb = reinterpret_cast<S*>(&p);
     __nv_bfloat16* mb = reinterpret_cast<__nv_bfloat16*>(&m);
     __nv_bfloat16* vb = reinterpret_cast<__nv_bfloat16*>(&v);
+    unsigned st = mix32(e0 ^ salt, sp.seed);
 #pragma unroll
     for (int k = 0; k < 8; k++) {
         float mm = __bfloat162float(mb[k]), vv = __bfloat162float(vb[k]);
         const float pn = opt_elem(sp, ldf(pb[k]), mm, vv, g[k], lr[k]);
-        unsigned rp, rm, rv;
-        sr_words((e0 + (unsigned)k) ^ salt, sp.seed, rp, rm, rv);
+        const unsigned rp = st = lcg_next(st), rm = st = lcg_next(st), rv = st = lcg_next(st);
         pb[k] = cvt_sr<S>(pn, rp);
         mb[k] = cvt_sr<__nv_bfloat16>(mm, rm);
         vb[k] = cvt_sr<__nv_bfloat16>(vv, rv);
@@ -528,10 +533,21 @@ __device__ __forceinline__ void adam_slice(ChosenBwdShared<S, MULTI>& sm, const 
         for (int q = tid; q < nq; q += kCB) {
             uint4 pp = sm.sh[q], mm = m4[q], vv = v4[q];
             float gg[8];
+            // (Gaussian t, coefficient kk = basis b, channel ch) of element 8q, then stepped by one
+            int t = (8 * q) / mc3, kk = 8 * q - t * mc3;
+            int b = kk / 3, ch = kk - 3 * b;
 #pragma unroll
             for (int k = 0; k < 8; k++) {
-                const int e = 8 * q + k, t = e / mc3;
-                gg[k] = sm.gsh(t, e - t * mc3);
+                gg[k] = MULTI ? sm.g_sh[kShPitch * t + kk] : sm.basis[b * kCB + t] * sm.geff[ch * kCB + t];
+                kk++;
+                if (++ch == 3) {
+                    ch = 0;
+                    b++;
+                }
+                if (kk == mc3) {   // mc3 is a multiple of 3
+                    kk = b = ch = 0;
+                    t++;
+                }
             }
             opt8<S>(sp, pp, mm, vv, gg, lr_sh, (unsigned)(sh0 + 8 * q), 0x5bd1e995u);
             p4[q] = pp;

@@ -152,3 +152,40 @@ def test_training_lowers_the_loss_1m_1080p(ctx, form):
     print(f"{form}: loss {losses[0]:.6f} -> {losses[-1]:.6f}")
     assert np.all(np.isfinite(losses))
     assert losses[-1] < 0.9 * losses[0]
+
+
+def test_stochastic_rounding_moves_parameters_in_expectation(ctx):
+    """One Adam step whose update is a fraction of a BF16 ulp for most SH
+    coefficients: round-to-nearest would leave them in place, stochastic
+    rounding moves them by the update in expectation.  Adam's first step
+    (optimizer.cpp:32-43, bias-corrected) is lr * g / (|g| + eps)."""
+    ctx.set_option(gs3d.OPT_FORM, gs3d.FORM_BF16)
+    sc = S.random_scene(200_000, seed=35)
+    cam = S.look_at_camera((0.3, 0.2, -3.0), 640, 480)
+    cfg = S.render_config(True)
+    gt = np.zeros(640 * 480 * 3, np.float32)
+    lr = 2e-5   # 0.08 ulp at the median SH coefficient, 0.001 ulp at the median raw scale
+    ctx.set_option(gs3d.OPT_KEEP_GRADIENTS, 1)
+    try:
+        ctx.set_raw_params(sc)
+        before = ctx.get_raw_params(sc.copy())
+        ctx.train_step(cam, gt, cfg, S.train_config(lr_pos=1e-30, lr_rest=lr), 0)
+        g = ctx.get_gradients()
+        after = ctx.get_raw_params(sc.copy())
+    finally:
+        ctx.set_option(gs3d.OPT_KEEP_GRADIENTS, 0)
+        ctx.set_option(gs3d.OPT_FORM, gs3d.FORM_PLAIN_FP32)
+    eps = S.train_config().adam_eps
+    for key in ("sh", "scales"):
+        gk = g["sh" if key == "sh" else "sc"].astype(np.float64).ravel()
+        d = (getattr(after, key).astype(np.float64) - getattr(before, key).astype(np.float64)).ravel()
+        sel = gk != 0.0
+        want = -lr * gk[sel] / (np.abs(gk[sel]) + eps)   # the FP32 update before rounding
+        got = d[sel]
+        resid = got - want
+        se = float(np.std(resid) / np.sqrt(resid.size))
+        frac_zero = float(np.mean(got == 0.0))
+        print(f"{key}: {got.size} coefficients, mean step {got.mean():.4e} (expected {want.mean():.4e}, "
+              f"standard error {se:.1e}), unchanged {frac_zero:.3f}")
+        assert frac_zero > 0.5, "most updates should be below half an ulp (the test would not test rounding)"
+        assert abs(float(resid.mean())) < 6.0 * se + 0.005 * lr
