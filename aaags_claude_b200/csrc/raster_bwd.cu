@@ -189,7 +189,7 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_bwd(const StepParams* __re
                 float4 r0 = s.rec0[gi];
                 float4 r1 = s.rec1[gi];
                 const float2 cb = s.cbt[gi];
-                const float thr = skip_threshold_from2(cb.y);
+                const float thr = skip_threshold(cb.y);
                 s_idx[e] = gi;
                 s_bt[e] = make_float2(cb.x, Accept::kBase2 ? cb.y : thr);   // the forward's
                 s_mask[e] = (unsigned char)strip_mask<kNW, 2 * PPT>(band_rows(r0, r1, thr, wx0, wx1), ty0);

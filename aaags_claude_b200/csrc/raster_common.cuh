@@ -26,10 +26,14 @@ __device__ __forceinline__ float power_rn(float4 r0, float4 r1, float dx, float 
 }
 
 // A power below this bound gives alpha = o * exp(power) < 1/255 for certain
-// (ln(1/(255 o)) less a margin far above the rounding of logf / expf), so the
+// (ln(1/(255 o)) less a margin far above the rounding of log / exp), so the
 // blend loops skip such Gaussians without evaluating exp; the skip they take
-// is the one the exact alpha test would take.
-__device__ __forceinline__ float skip_threshold(float o) { return logf(kAlphaMin / o) - 1e-3f; }
+// is the one the exact alpha test would take.  It is computed from the
+// accept threshold thr2 = -log2(255 o) that the preprocess stores per
+// Gaussian (blue_thr): ln(1/(255 o)) = ln(2) thr2.  The roundings of log2f and
+// of this FMA move the bound by a few 1e-6, far inside the 1e-3 margin.
+constexpr float kLn2 = 0.6931471805599453f;
+__device__ __forceinline__ float skip_threshold(float thr2) { return fmaf(thr2, kLn2, -1e-3f); }
 
 // Square root from the hardware reciprocal square root (rsqrtf, within 2 ulp),
 // for the conservative bounds below; 0 for x <= 0.
@@ -128,12 +132,6 @@ __device__ __forceinline__ float accept_threshold2(float o) { return -log2f(255.
 
 // The screen record's (blue, accept threshold) pair, written by every preprocess.
 __device__ __forceinline__ float2 blue_thr(float b, float o) { return make_float2(b, accept_threshold2(o)); }
-
-// skip_threshold recovered from the stored accept threshold: ln(2) * (-log2(255 o))
-// less the same 1e-3 margin.  Against logf(1/(255 o)) the two roundings differ by
-// a few 1e-6, far inside the margin, so the bound stays conservative.
-constexpr float kLn2 = 0.6931471805599453f;
-__device__ __forceinline__ float skip_threshold_from2(float thr2) { return fmaf(thr2, kLn2, -1e-3f); }
 
 // The staged record of the reduced form carries the conic pre-scaled for q:
 // (x, y, -0.5 log2(e) a, -log2(e) b), (-0.5 log2(e) c, o, r, g).

@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(256 / PPT) k_raster_fwd(const StepParams* __re
                 float4 r0 = s.rec0[g];
                 float4 r1 = s.rec1[g];
                 const float2 cb = s.cbt[g];
-                const float thr = skip_threshold_from2(cb.y);
+                const float thr = skip_threshold(cb.y);
                 // the threshold in the units of Blend's exponent: the stored base-2 one, or the skip bound
                 s_bt[e] = make_float2(cb.x, Blend::kBase2 ? cb.y : thr);
                 s_mask[e] = (unsigned char)strip_mask<kNW, 2 * PPT>(band_rows(r0, r1, thr, wx0, wx1), ty0);
