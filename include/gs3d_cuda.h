@@ -272,7 +272,13 @@ int gs3dc_optimizer_step(gs3dc_ctx* ctx, const gs3d_train_config* tc, int iterat
  *   cameras of several sizes replays each size's graph.  A shape's first step
  *   runs un-captured and waits for the device (a pair-capacity overflow is
  *   redone at once).
- *   gt is H*W*3 HWC; gt_on_device != 0 means it is a device pointer.
+ *   gt is H*W*3 HWC; gt_on_device != 0 means it is a device pointer.  A host
+ *   gt is copied on the context's copy stream (pinned memory makes that copy
+ *   asynchronous) while the step's preprocess, sort and forward rasteriser
+ *   run; the L1 and the backward follow once it has landed.  The host buffer
+ *   may be reused when the call returns with a non-NULL loss; with a NULL loss
+ *   the copy may still be running, so keep the buffer unchanged until the next
+ *   synchronising call.
  *   loss (may be NULL) receives the mean absolute error; a NULL loss also lets
  *   the call return without waiting for the device (the next call, or
  *   gs3dc_get_raw_params, synchronises). */
