@@ -519,6 +519,22 @@ __device__ __forceinline__ void adam_slice(ChosenBwdShared<S, MULTI>& sm, const 
         }
     }
     const long long sh0 = (long long)mc3 * g0;
+    // this thread's attribute moments (one Gaussian per thread: ng <= kCB) and position moments
+    // (elements tid, tid + kCB, tid + 2 kCB of the slice) load during the SH updates
+    uint4 am = make_uint4(0u, 0u, 0u, 0u), av = am;
+    if (tid < ng) {
+        am = reinterpret_cast<const uint4*>(c.m_attr)[g0 + tid];
+        av = reinterpret_cast<const uint4*>(c.v_attr)[g0 + tid];
+    }
+    float pm[3] = {0.f, 0.f, 0.f}, pv[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+        const int e = tid + j * kCB;
+        if (e < 3 * ng) {
+            pm[j] = c.m_pos[3 * g0 + e];
+            pv[j] = c.v_pos[3 * g0 + e];
+        }
+    }
     S* shw = static_cast<S*>(c.sh);
     __nv_bfloat16* msh = static_cast<__nv_bfloat16*>(c.m_sh);
     __nv_bfloat16* vsh = static_cast<__nv_bfloat16*>(c.v_sh);
@@ -530,8 +546,18 @@ __device__ __forceinline__ void adam_slice(ChosenBwdShared<S, MULTI>& sm, const 
         uint4* m4 = reinterpret_cast<uint4*>(msh + sh0);
         uint4* v4 = reinterpret_cast<uint4*>(vsh + sh0);
         uint4* p4 = reinterpret_cast<uint4*>(shw + sh0);
+        // each chunk's moments load one iteration ahead, so their latency overlaps the previous chunk
+        uint4 mm_n = make_uint4(0u, 0u, 0u, 0u), vv_n = mm_n;
+        if (tid < nq) {
+            mm_n = m4[tid];
+            vv_n = v4[tid];
+        }
         for (int q = tid; q < nq; q += kCB) {
-            uint4 pp = sm.sh[q], mm = m4[q], vv = v4[q];
+            uint4 pp = sm.sh[q], mm = mm_n, vv = vv_n;
+            if (q + kCB < nq) {
+                mm_n = m4[q + kCB];
+                vv_n = v4[q + kCB];
+            }
             float gg[8];
             // (Gaussian t, coefficient kk = basis b, channel ch) of element 8q, then stepped by one
             int t = (8 * q) / mc3, kk = 8 * q - t * mc3;
@@ -570,24 +596,28 @@ __device__ __forceinline__ void adam_slice(ChosenBwdShared<S, MULTI>& sm, const 
     // attributes: one 16-byte record per Gaussian
     const float lra[8] = {sp.lr_scale, sp.lr_scale, sp.lr_scale, sp.lr_opac, sp.lr_rot, sp.lr_rot, sp.lr_rot,
                           sp.lr_rot};
-    for (int t = tid; t < ng; t += kCB) {
+    if (tid < ng) {
+        const int t = tid;
         const float gg[8] = {sm.g_sc[3 * t], sm.g_sc[3 * t + 1], sm.g_sc[3 * t + 2], sm.g_op[t],
                              sm.g_rot[4 * t], sm.g_rot[4 * t + 1], sm.g_rot[4 * t + 2], sm.g_rot[4 * t + 3]};
         uint4 pp = sm.attr[t];
-        uint4 mm = reinterpret_cast<const uint4*>(c.m_attr)[g0 + t];
-        uint4 vv = reinterpret_cast<const uint4*>(c.v_attr)[g0 + t];
+        uint4 mm = am, vv = av;
         opt8<S>(sp, pp, mm, vv, gg, lra, (unsigned)(8 * (g0 + t)), 0u);
         reinterpret_cast<uint4*>(c.attr)[g0 + t] = pp;
         reinterpret_cast<uint4*>(c.m_attr)[g0 + t] = mm;
         reinterpret_cast<uint4*>(c.v_attr)[g0 + t] = vv;
     }
     // positions: FP32 parameters and moments
-    for (int e = tid; e < 3 * ng; e += kCB) {
-        const long long ge = 3 * g0 + e;
-        float m = c.m_pos[ge], v = c.v_pos[ge];
-        c.pos[ge] = opt_elem(sp, sm.pos[e], m, v, sm.g_pos[e], sp.lr_pos);
-        c.m_pos[ge] = m;
-        c.v_pos[ge] = v;
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+        const int e = tid + j * kCB;
+        if (e < 3 * ng) {
+            const long long ge = 3 * g0 + e;
+            float m = pm[j], v = pv[j];
+            c.pos[ge] = opt_elem(sp, sm.pos[e], m, v, sm.g_pos[e], sp.lr_pos);
+            c.m_pos[ge] = m;
+            c.v_pos[ge] = v;
+        }
     }
 }
 
