@@ -292,6 +292,7 @@ __device__ __forceinline__ float exp_ref(float x) { return (float)exp((double)x)
 
 // Block-wide inclusive scan of one int per thread (256 threads); returns the
 // inclusive value, *total gets the block sum.  s_warp needs 8 ints.
+template <int NW = kBlock / 32>   // warps of the CTA, <= 32
 __device__ __forceinline__ int block_inclusive_scan(int v, int* s_warp, int* total) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -302,17 +303,17 @@ __device__ __forceinline__ int block_inclusive_scan(int v, int* s_warp, int* tot
     if (lane == 31) s_warp[warp] = v;
     __syncthreads();
     if (warp == 0) {
-        int w = lane < 8 ? s_warp[lane] : 0;
+        int w = lane < NW ? s_warp[lane] : 0;
 #pragma unroll
-        for (int o = 1; o < 8; o <<= 1) {
+        for (int o = 1; o < NW; o <<= 1) {
             int n = __shfl_up_sync(0xffffffffu, w, o);
             if (lane >= o) w += n;
         }
-        if (lane < 8) s_warp[lane] = w;
+        if (lane < NW) s_warp[lane] = w;
     }
     __syncthreads();
     int add = warp > 0 ? s_warp[warp - 1] : 0;
-    *total = s_warp[7];
+    *total = s_warp[NW - 1];
     return v + add;
 }
 

@@ -525,7 +525,7 @@ template <bool RAW>
 __global__ void __launch_bounds__(kBlock) k_preprocess_e3(const StepParams* __restrict__ spp, int N, ModelPtrs m,
                                                           const float* __restrict__ filt, ScreenPtrs s, E3Ptrs e,
                                                           PairPtrs pr, Control* ctrl) {
-    __shared__ EmitShared sm;
+    __shared__ EmitShared<> sm;
     __shared__ int s_blk;
     const StepParams& sp = *spp;
     if (threadIdx.x == 0) s_blk = (int)atomicAdd(&ctrl->tickets[0], 1u);
@@ -673,7 +673,7 @@ __global__ void __launch_bounds__(kBlock) k_bin_arrays_e3(const StepParams* __re
                                                           const float* __restrict__ ci, const float* __restrict__ mo,
                                                           const float4* __restrict__ tdir, PairPtrs pr,
                                                           Control* ctrl) {
-    __shared__ EmitShared sm;
+    __shared__ EmitShared<> sm;
     __shared__ int s_blk;
     const StepParams& sp = *spp;
     if (threadIdx.x == 0) s_blk = (int)atomicAdd(&ctrl->tickets[0], 1u);

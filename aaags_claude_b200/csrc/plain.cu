@@ -71,22 +71,25 @@ namespace {
 // ---------------- block scan + look-back + pair emission ----------------
 
 constexpr int kEmitRun = 4;                      // consecutive pair slots walked by one thread
-constexpr int kEmitChunk = kBlock * kEmitRun;    // pair slots staged per round
+constexpr int kEmitBlockViews = 512;             // CTA of the multi-view pair emission
 constexpr unsigned kNoPair = 0xffffffffu;        // staged tile of a slot left unwritten (beyond `limit`)
 
+// Shared memory of a CTA of B threads (one Gaussian each) emitting its pairs.
+template <int B = kBlock>
 struct EmitShared {
-    int warp[8];
-    int excl[kBlock];
-    int rect[kBlock];      // xmin | ymin << 16
-    int width[kBlock];
-    float winv[kBlock];    // 1 / width (round to nearest): the row of a pair without an integer division
-    int limit[kBlock];     // pairs actually emitted (rect area, <= count)
-    unsigned depth[kBlock];
-    unsigned gid[kBlock];  // Gaussian index written as the pair's value
-    unsigned tbase[kBlock];  // first global tile id of the Gaussian's view (0 for one view)
-    int gx[kBlock];          // tile-grid width of the Gaussian's view
-    alignas(16) unsigned ctile[kEmitChunk];   // one round's pairs: tile id (or kNoPair)
-    alignas(16) unsigned cown[kEmitChunk];    // and the owning thread of the CTA
+    static constexpr int kChunk = B * kEmitRun;   // pair slots staged per round
+    int warp[B / 32];
+    int excl[B];
+    int rect[B];      // xmin | ymin << 16
+    int width[B];
+    float winv[B];    // 1 / width (round to nearest): the row of a pair without an integer division
+    int limit[B];     // pairs actually emitted (rect area, <= count)
+    unsigned depth[B];
+    unsigned gid[B];  // Gaussian index written as the pair's value
+    unsigned tbase[B];  // first global tile id of the Gaussian's view (0 for one view)
+    int gx[B];          // tile-grid width of the Gaussian's view
+    alignas(16) unsigned ctile[kChunk];   // one round's pairs: tile id (or kNoPair)
+    alignas(16) unsigned cown[kChunk];    // and the owning thread of the CTA
     unsigned long long base;
 };
 
@@ -111,15 +114,15 @@ struct KeepDepth {
     __device__ __forceinline__ unsigned operator()(unsigned dbits, unsigned, unsigned) const { return dbits; }
 };
 
-template <class DepthFn = KeepDepth>
-__device__ __forceinline__ void scan_and_emit(EmitShared& sm, int blk, unsigned gid, int cnt, int emit, int rx, int ry,
+template <int B = kBlock, class DepthFn = KeepDepth>
+__device__ __forceinline__ void scan_and_emit(EmitShared<B>& sm, int blk, unsigned gid, int cnt, int emit, int rx, int ry,
                                               int rw, unsigned dbits, int grid_x, PairPtrs pr,
                                               Control* ctrl, unsigned spin_limit, Persist* persist,
                                               unsigned* thist = nullptr, int nd = 0, unsigned tile_base_t = 0u,
                                               int grid_x_t = -1, DepthFn depth_fn = DepthFn()) {
     const int tid = threadIdx.x;
     int total;
-    const int incl = block_inclusive_scan(cnt, sm.warp, &total);
+    const int incl = block_inclusive_scan<B / 32>(cnt, sm.warp, &total);
     sm.excl[tid] = incl - cnt;
     sm.rect[tid] = rx | (ry << 16);
     sm.width[tid] = rw;
@@ -131,18 +134,18 @@ __device__ __forceinline__ void scan_and_emit(EmitShared& sm, int blk, unsigned 
     sm.gx[tid] = grid_x_t < 0 ? grid_x : grid_x_t;
     if (tid == 0) lookback_publish(pr.scan_desc, blk, (unsigned long long)total);
     __syncthreads();
-    for (int c0 = 0;; c0 += kEmitChunk) {
+    for (int c0 = 0;; c0 += EmitShared<B>::kChunk) {
         // stage this round: slots c0 + kEmitRun * tid ..
         const int k0 = c0 + kEmitRun * tid;
         if (k0 < total) {
-            int lo = 0, hi = kBlock;   // the owner: last thread whose exclusive offset is <= k0
+            int lo = 0, hi = B;   // the owner: last thread whose exclusive offset is <= k0
             while (hi - lo > 1) {
                 const int mid = (lo + hi) >> 1;
                 if (sm.excl[mid] <= k0) lo = mid;
                 else hi = mid;
             }
             int local = k0 - sm.excl[lo];
-            int end = lo + 1 < kBlock ? sm.excl[lo + 1] : total;
+            int end = lo + 1 < B ? sm.excl[lo + 1] : total;
             int w = sm.width[lo], lim = sm.limit[lo], gx = sm.gx[lo];
             // local / w from the rounded reciprocal: for local < 2^23 the product is within one of the
             // quotient, and one correction step each way makes it exact
@@ -159,7 +162,7 @@ __device__ __forceinline__ void scan_and_emit(EmitShared& sm, int blk, unsigned 
                 if (k < total && k == end) {   // next thread with pairs
                     do {
                         lo++;
-                        end = lo + 1 < kBlock ? sm.excl[lo + 1] : total;
+                        end = lo + 1 < B ? sm.excl[lo + 1] : total;
                     } while (end == k);
                     local = 0;
                     col = 0;
@@ -195,8 +198,8 @@ __device__ __forceinline__ void scan_and_emit(EmitShared& sm, int blk, unsigned 
         }
         __syncthreads();
         const unsigned long long base = sm.base;
-        const int n = min(kEmitChunk, total - c0);
-        for (int j = tid; j < n; j += kBlock) {
+        const int n = min(EmitShared<B>::kChunk, total - c0);
+        for (int j = tid; j < n; j += B) {
             const unsigned tile = sm.ctile[j];
             const unsigned long long dst = base + (unsigned long long)(c0 + j);
             if (tile == kNoPair || dst >= pr.capacity) continue;
@@ -209,7 +212,7 @@ __device__ __forceinline__ void scan_and_emit(EmitShared& sm, int blk, unsigned 
             }
             pr.vals[dst] = sm.gid[own];
         }
-        if (c0 + kEmitChunk >= total) break;
+        if (c0 + EmitShared<B>::kChunk >= total) break;
         __syncthreads();   // the next round restages the buffers
     }
 }
@@ -219,7 +222,7 @@ __device__ __forceinline__ void scan_and_emit(EmitShared& sm, int blk, unsigned 
 template <bool TRAIN, bool CACHE, bool EMIT>
 __global__ void __launch_bounds__(kBlock) k_preprocess(const StepParams* __restrict__ spp, int N, ModelPtrs m,
                                                        ScreenPtrs s, PairPtrs pr, DepthKeys dk, Control* ctrl) {
-    __shared__ EmitShared sm;
+    __shared__ EmitShared<> sm;
     __shared__ int s_blk;
     const StepParams& sp = *spp;
     if (EMIT) {
@@ -307,21 +310,22 @@ __global__ void __launch_bounds__(kBlock) k_preprocess(const StepParams* __restr
 // tile_rect the preprocess used) and emits its pairs row-major.  With the
 // Gaussians stably sorted by depth bits, a stable sort of these pairs by tile
 // alone gives the (tile, depth bits, Gaussian index) order of the full-key sort.
-__global__ void __launch_bounds__(kBlock) k_emit_ranked(const StepParams* __restrict__ spp, int N,
-                                                        const unsigned* __restrict__ rank_gid, ScreenPtrs s,
-                                                        PairPtrs pr, const uint2* __restrict__ rects,
-                                                        Control* ctrl, int n_per_view, int hist_slot,
-                                                        unsigned* __restrict__ hist_parts) {
-    __shared__ EmitShared sm;
+template <int B>
+__global__ void __launch_bounds__(B) k_emit_ranked(const StepParams* __restrict__ spp, int N,
+                                                   const unsigned* __restrict__ rank_gid, ScreenPtrs s,
+                                                   PairPtrs pr, const uint2* __restrict__ rects,
+                                                   Control* ctrl, int n_per_view, int hist_slot,
+                                                   unsigned* __restrict__ hist_parts) {
+    __shared__ EmitShared<B> sm;
     __shared__ int s_blk;
     __shared__ unsigned s_thist[kMaxPasses - kDepthDigits][256];
     const StepParams& sp = *spp;
     const int nd = sp.sort_passes - kDepthDigits;   // 8-bit digits of the tile ids (control slots hist_slot..)
-    for (int e = threadIdx.x; e < nd * 256; e += kBlock) (&s_thist[0][0])[e] = 0;
+    for (int e = threadIdx.x; e < nd * 256; e += B) (&s_thist[0][0])[e] = 0;
     if (threadIdx.x == 0) s_blk = (int)atomicAdd(&ctrl->tickets[0], 1u);
     __syncthreads();
     const int blk = s_blk;
-    const int r = blk * kBlock + threadIdx.x;
+    const int r = blk * B + threadIdx.x;
     int cnt = 0, rx = 0, ry = 0, rw = 1, gx = sp.grid_x;
     unsigned g = 0, dbits = 0, tbase = 0;
     if (r < N) {
@@ -366,7 +370,7 @@ __global__ void __launch_bounds__(kBlock) k_emit_ranked(const StepParams* __rest
     // different CTAs rarely meet on one address; k_hist_parts_reduce adds the copies up
     unsigned* dst = hist_parts ? hist_parts + (size_t)(blk % kHistParts) * (kMaxPasses - kDepthDigits) * 256
                                : &ctrl->hist[hist_slot][0];
-    for (int e = threadIdx.x; e < nd * 256; e += kBlock) {
+    for (int e = threadIdx.x; e < nd * 256; e += B) {
         const unsigned v = (&s_thist[0][0])[e];
         if (v) atomicAdd(&dst[e], v);
     }
@@ -390,7 +394,7 @@ __global__ void __launch_bounds__(256) k_hist_parts_reduce(const unsigned* __res
 // offsets from tiles_touched, pairs from the rect recomputed from (mean, radius).
 __global__ void __launch_bounds__(kBlock) k_bin_arrays(const StepParams* __restrict__ spp, int N,
                                                        ScreenArrays a, PairPtrs pr, Control* ctrl) {
-    __shared__ EmitShared sm;
+    __shared__ EmitShared<> sm;
     __shared__ int s_blk;
     const StepParams& sp = *spp;
     if (threadIdx.x == 0) s_blk = (int)atomicAdd(&ctrl->tickets[0], 1u);
@@ -805,8 +809,13 @@ cudaError_t launch_emit_ranked(cudaStream_t st, const StepParams* sp, int N, con
                                ScreenPtrs s, PairPtrs pr, Control* ctrl, const uint2* rects, int n_per_view,
                                int hist_slot, unsigned* hist_parts) {
     if (N <= 0) return cudaSuccess;
-    k_emit_ranked<<<blocks_for(N, kBlock), kBlock, 0, st>>>(sp, N, rank_gid, s, pr, rects, ctrl, n_per_view,
-                                                            hist_slot, hist_parts);
+    // several views: 512 Gaussians per CTA, half the CTAs (look-backs, histogram flushes)
+    if (n_per_view > 0)
+        k_emit_ranked<kEmitBlockViews><<<blocks_for(N, kEmitBlockViews), kEmitBlockViews, 0, st>>>(
+            sp, N, rank_gid, s, pr, rects, ctrl, n_per_view, hist_slot, hist_parts);
+    else
+        k_emit_ranked<kBlock><<<blocks_for(N, kBlock), kBlock, 0, st>>>(sp, N, rank_gid, s, pr, rects, ctrl,
+                                                                        n_per_view, hist_slot, hist_parts);
     if (hist_parts) k_hist_parts_reduce<<<1, 256, 0, st>>>(hist_parts, sp, ctrl, hist_slot);
     return cudaGetLastError();
 }
