@@ -71,7 +71,7 @@ namespace {
 // ---------------- block scan + look-back + pair emission ----------------
 
 constexpr int kEmitRun = 4;                      // consecutive pair slots walked by one thread
-constexpr int kEmitBlockViews = 512;             // CTA of the multi-view pair emission
+constexpr int kEmitBlock = 512;                  // CTA of the train step's pair emission (k_emit_ranked)
 constexpr unsigned kNoPair = 0xffffffffu;        // staged tile of a slot left unwritten (beyond `limit`)
 
 // Shared memory of a CTA of B threads (one Gaussian each) emitting its pairs.
@@ -809,13 +809,10 @@ cudaError_t launch_emit_ranked(cudaStream_t st, const StepParams* sp, int N, con
                                ScreenPtrs s, PairPtrs pr, Control* ctrl, const uint2* rects, int n_per_view,
                                int hist_slot, unsigned* hist_parts) {
     if (N <= 0) return cudaSuccess;
-    // several views: 512 Gaussians per CTA, half the CTAs (look-backs, histogram flushes)
-    if (n_per_view > 0)
-        k_emit_ranked<kEmitBlockViews><<<blocks_for(N, kEmitBlockViews), kEmitBlockViews, 0, st>>>(
-            sp, N, rank_gid, s, pr, rects, ctrl, n_per_view, hist_slot, hist_parts);
-    else
-        k_emit_ranked<kBlock><<<blocks_for(N, kBlock), kBlock, 0, st>>>(sp, N, rank_gid, s, pr, rects, ctrl,
-                                                                        n_per_view, hist_slot, hist_parts);
+    // 512 Gaussians per CTA: half the CTAs of the preprocess's 256, so half the look-backs and
+    // histogram flushes
+    k_emit_ranked<kEmitBlock><<<blocks_for(N, kEmitBlock), kEmitBlock, 0, st>>>(sp, N, rank_gid, s, pr, rects, ctrl,
+                                                                                n_per_view, hist_slot, hist_parts);
     if (hist_parts) k_hist_parts_reduce<<<1, 256, 0, st>>>(hist_parts, sp, ctrl, hist_slot);
     return cudaGetLastError();
 }
