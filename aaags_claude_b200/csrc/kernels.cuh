@@ -61,7 +61,7 @@ struct PairPtrs {
     unsigned long long* keys;   // [capacity]
     unsigned* vals;             // [capacity]
     unsigned long long capacity;
-    unsigned long long* scan_desc;  // look-back descriptors, one per preprocess CTA
+    unsigned long long* scan_desc;  // look-back descriptors, one per emitting CTA (at most one per 256 Gaussians)
     unsigned* tiles32 = nullptr;    // depth-ordered emission: tile-only keys [capacity] instead of keys
 };
 

@@ -98,7 +98,8 @@ struct EmitShared {
 // consecutive pairs (fully coalesced, balanced however uneven the rects).
 // Pair order: Gaussian-major, then row-major inside the rect
 // (tile_binner_cpu.cpp:90-97).
-// The pairs go out in rounds of kEmitChunk slots: each thread finds the owner
+// The pairs go out in rounds of EmitShared<B>::kChunk slots (B = the CTA's
+// threads): each thread finds the owner
 // of its first kEmitRun consecutive slots by one binary search over the
 // CTA's exclusive scan and walks them (column, row and owner advance by
 // increments), staging tile and owner in shared memory; then the CTA writes
