@@ -116,6 +116,39 @@ def test_train_step_graph_matches_eager(ctx):
         assert np.abs(getattr(res[0][1], k) - getattr(res[1][1], k)).max() <= 1e-6
 
 
+@pytest.mark.parametrize("form", ["plain", "bf16"])
+def test_host_target_steps_match_device_target_steps(ctx, form):
+    """A host target runs the forward before its copy lands and the L1 as its
+    own kernel; a device target keeps the L1 fused into the forward.  Both give
+    the same sign bytes, so the same gradients up to the order of the screen
+    gradients' atomics (parameters to 1e-6 in the plain form; in BF16 a
+    stochastic rounding may flip by one ulp, so only the losses compare)."""
+    import torch
+    sc = S.random_scene(4000, seed=6)
+    cam = S.look_at_camera((0.3, 0.2, -3.0), 176, 144)
+    gt = O.forward(S.perturbed(sc), cam, S.render_config(False), "c").image.astype(np.float32).ravel()
+    gt_dev = torch.from_numpy(gt).cuda()
+    cfg, tc = S.render_config(True), S.train_config()
+    ctx.set_option(gs3d.OPT_FORM, gs3d.FORM_BF16 if form == "bf16" else gs3d.FORM_PLAIN_FP32)
+    res = []
+    try:
+        for on_device in (False, True):
+            ctx.set_raw_params(sc)
+            losses = []
+            for it in range(4):   # later steps replay the shape's graphs
+                if on_device:
+                    losses.append(ctx.train_step(cam, None, cfg, tc, it, gt_device_ptr=gt_dev.data_ptr()))
+                else:
+                    losses.append(ctx.train_step(cam, gt, cfg, tc, it))
+            res.append((losses, ctx.get_raw_params(sc.copy())))
+    finally:
+        ctx.set_option(gs3d.OPT_FORM, gs3d.FORM_PLAIN_FP32)
+    assert np.allclose(res[0][0], res[1][0], rtol=1e-5, atol=0.0)
+    if form == "plain":
+        for k in ("positions", "scales", "rotations", "sh", "opacities"):
+            assert np.abs(getattr(res[0][1], k) - getattr(res[1][1], k)).max() <= 1e-6, k
+
+
 def test_train_step_keeps_a_graph_per_camera_size(ctx):
     """Cycling through cameras of three sizes: each size is captured once and
     replayed afterwards (no re-capture when the size changes back), with the
