@@ -205,6 +205,7 @@ struct gs3dc_ctx {
         DevBuf<unsigned char> dsign;
         DevBuf<unsigned> ranges, order;
         DevBuf<unsigned> hist_parts;               // launch_emit_ranked's spread tile-digit counts
+        DevBuf<unsigned> seg_hist;                 // per-view digit counts of the depth sort
         size_t grads_zeroed = 0;                   // entries of the screen-gradient accumulators known zero
         std::vector<unsigned long long> view_pix;  // first pixel of each view of the last step (+ the total)
         cudaGraphExec_t graph = nullptr;
@@ -1021,6 +1022,8 @@ std::vector<void*> state_arrays(gs3dc_ctx* c) {
 struct BatchShape {
     int V = 0;
     long long VN = 0;
+    long long seg = 0;         // each view's depth-sort segment: N rounded up to whole 8192-key sort tiles
+    long long VS = 0;          // V * seg: depth-sort keys (the emission's ranks)
     unsigned tiles = 0;        // all views' tiles
     unsigned long long pix = 0;  // all views' pixels
     int tile_digits = 0;
@@ -1081,11 +1084,13 @@ int batch_buffers(gs3dc_ctx* c, const BatchShape& sh) {
         CK(cudaMemsetAsync(b.dop.p, 0, b.dop.n * 4, c->stream));
         b.grads_zeroed = b.dop.n;
     }
+    const size_t vs = (size_t)sh.VS;   // the depth sort's padded per-view segments
     for (int k = 0; k < 2; k++) {
-        CK(b.dkeys[k].ensure(vn));
-        CK(b.dvals[k].ensure(vn));
+        CK(b.dkeys[k].ensure(vs));
+        CK(b.dvals[k].ensure(vs));
     }
-    CK(b.ddesc.ensure(4 * ((vn + kSortTile - 1) / kSortTile) * 256));
+    CK(b.ddesc.ensure(3 * ((vs + kSortTile - 1) / kSortTile) * 256));
+    CK(b.seg_hist.ensure((size_t)sh.V * 3 * 256));
     CK(b.image.ensure(3 * sh.pix));
     CK(b.T.ensure(sh.pix));
     CK(b.last.ensure(sh.pix));
@@ -1094,7 +1099,7 @@ int batch_buffers(gs3dc_ctx* c, const BatchShape& sh) {
     CK(b.order.ensure(sh.tiles));
     CK(b.hist_parts.ensure((size_t)kHistParts * (kMaxPasses - kDepthDigits) * 256));
     Control* before = c->ctrl;
-    int rc = ensure_ctrl(c, (int)std::min<long long>(sh.VN, 0x7fffffffLL));
+    int rc = ensure_ctrl(c, (int)std::min<long long>(sh.VS, 0x7fffffffLL));
     if (rc) return rc;
     if (c->ctrl != before) drop_graphs(c);   // captured launches hold the control block's address
     return GS3DC_OK;
@@ -1108,28 +1113,31 @@ int batch_buffers(gs3dc_ctx* c, const BatchShape& sh) {
 int seq_batch(gs3dc_ctx* c, const BatchShape& sh) {
     auto& b = c->batch;
     const StepParams* views = b.views.p;
-    const unsigned long long vn = (unsigned long long)sh.VN;
-    const unsigned long long dstride = ((vn + kSortTile - 1) / kSortTile) * 256ull;
+    const unsigned long long vs = (unsigned long long)sh.VS;
+    const unsigned long long dstride = ((vs + kSortTile - 1) / kSortTile) * 256ull;
     const unsigned long long pstride = ((b.cap + kSortTile - 1) / kSortTile) * 256ull;
-    CK(cudaMemsetAsync(c->ctrl_region.p, 0, ctrl_bytes_for((int)std::min<long long>(sh.VN, 0x7fffffffLL)),
+    CK(cudaMemsetAsync(c->ctrl_region.p, 0, ctrl_bytes_for((int)std::min<long long>(sh.VS, 0x7fffffffLL)),
                        c->stream));
     CK(cudaMemsetAsync(b.ranges.p, 0, 2 * (size_t)sh.tiles * sizeof(unsigned), c->stream));
-    CK(cudaMemsetAsync(b.ddesc.p, 0, 4 * dstride * sizeof(unsigned long long), c->stream));
+    CK(cudaMemsetAsync(b.ddesc.p, 0, 3 * dstride * sizeof(unsigned long long), c->stream));
+    CK(cudaMemsetAsync(b.seg_hist.p, 0, (size_t)sh.V * 3 * 256 * sizeof(unsigned), c->stream));
     CK(cudaMemsetAsync(b.hist_parts.p, 0, b.hist_parts.n * sizeof(unsigned), c->stream));
     if (sh.tile_digits > 0)
         CK(cudaMemsetAsync(b.sort_desc.p, 0, (size_t)sh.tile_digits * pstride * sizeof(unsigned long long),
                            c->stream));
     DepthKeys dk{b.dkeys[0].p, b.dvals[0].p};
     dk.views24 = true;
+    dk.seg_keys = (unsigned long long)sh.seg;
     CK(launch_chosen_preprocess(c->stream, views, c->N, c->form == GS3DC_FORM_FP16, chosen_ptrs(c), batch_screen(c),
                                 dk, b.rects.p, c->ctrl, sh.V));
-    // 32-bit keys: digits 0..2 the depth's upper 24 bits (as the single-view reduced form), digit 3 the view;
-    // the preprocess counted their digit histograms into control slots 0..3
+    // 32-bit keys (view << 24 | the depth's upper 24 bits), view v's in segment v (entries already
+    // grouped by view): each segment sorted apart on the three depth digits
     int dw = 0;
-    CK(launch_radix_sort32(c->stream, views, 4, 0, true, vn, b.dkeys[0].p, b.dvals[0].p, b.dkeys[1].p, b.dvals[1].p,
-                           b.ddesc.p, dstride, c->ctrl, &dw, nullptr, &c->ctrl->gauss_keys, 0));
+    CK(launch_radix_sort32_segmented(c->stream, views, 0, 3, vs, (unsigned long long)sh.seg, b.dkeys[0].p,
+                                     b.dvals[0].p, b.dkeys[1].p, b.dvals[1].p, b.ddesc.p, dstride, b.seg_hist.p,
+                                     c->ctrl, &dw));
     PairPtrs pr{nullptr, b.vals[0].p, b.cap, c->scan_desc, b.keys[0].p};
-    CK(launch_emit_ranked(c->stream, views, (int)vn, b.dvals[dw].p, batch_screen(c), pr, c->ctrl, b.rects.p, c->N,
+    CK(launch_emit_ranked(c->stream, views, (int)vs, b.dvals[dw].p, batch_screen(c), pr, c->ctrl, b.rects.p, c->N,
                           5, b.hist_parts.p));
     int which = 0;
     CK(launch_radix_sort32(c->stream, views, sh.tile_digits, 5, true, b.cap, b.keys[0].p, b.vals[0].p, b.keys[1].p,
@@ -2058,7 +2066,9 @@ int gs3dc_train_step_batch(gs3dc_ctx* c, int n_views, const gs3d_camera* cams, c
     BatchShape sh;
     sh.V = n_views;
     sh.VN = (long long)c->N * n_views;
-    if (sh.VN >= (1LL << 31)) return fail(c, GS3DC_ERR_INVALID_ARG, "%lld (view, Gaussian) entries exceed 2^31", sh.VN);
+    sh.seg = ((long long)c->N + 8191) / 8192 * 8192;
+    sh.VS = sh.seg * n_views;
+    if (sh.VS >= (1LL << 31)) return fail(c, GS3DC_ERR_INVALID_ARG, "%lld (view, Gaussian) entries exceed 2^31", sh.VN);
     std::vector<unsigned> tile_base(n_views), pix_base(n_views);
     unsigned long long tiles = 0, pix = 0, max_view_tiles = 0;
     b.view_pix.clear();

@@ -233,62 +233,47 @@ __global__ void __launch_bounds__(kBlock) k_chosen_preprocess(const StepParams* 
 
 // Several views: one thread per Gaussian loads, activates and forms the cov3D
 // once and projects it into every view (entries view * N + i), writing the
-// 32-bit (view, depth's upper 24 bits) keys of the depth sort and their
-// digit histograms: digits 0..2 (the depth bits 8..31) counted per CTA in
-// shared memory, one global atomic per CTA and bin; digit 3 (the view) has N
-// keys per view.  The sort then needs no histogram pass.
+// 32-bit (view, depth's upper 24 bits) keys of the depth sort.  The keys of
+// view v sit at v * dk.seg_keys + i (a segment padded to whole sort tiles;
+// threads N <= i < seg_keys write padding, whose key sorts last and whose value
+// 0xFFFFFFFF marks no entry), so that the sort orders each view's segment apart
+// on the depth digits (launch_radix_sort32_segmented).
 template <typename S>
 __global__ void __launch_bounds__(kBlock) k_chosen_preprocess_views(const StepParams* __restrict__ spp, int N,
                                                                     int n_views, ChosenPtrs c, ScreenPtrs s,
                                                                     DepthKeys dk, uint2* __restrict__ rects,
                                                                     Control* ctrl) {
-    __shared__ unsigned s_hist[3][256];
-    for (int e = threadIdx.x; e < 3 * 256; e += kBlock) (&s_hist[0][0])[e] = 0u;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i == 0) {
-        ctrl->gauss_keys = (unsigned long long)N * n_views;
-        for (int v = 0; v < n_views; v++) atomicAdd(&ctrl->hist[3][v], (unsigned)N);
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long seg = (long long)dk.seg_keys;
+    if (i == 0) ctrl->gauss_keys = (unsigned long long)seg * n_views;
+    if (i >= seg) return;
+    if (i >= N) {
+        for (int v = 0; v < n_views; v++) {
+            dk.keys[v * seg + i] = 0xFFFFFFFFu;
+            dk.vals[v * seg + i] = 0xFFFFFFFFu;
+        }
+        return;
     }
-    __syncthreads();
-    const bool valid = i < N;
     const int mc3 = spp[0].max_coeffs * 3;
-    const int gi = valid ? i : 0;   // threads past the end project Gaussian 0 and write nothing
-    const float p[3] = {c.pos[3 * gi], c.pos[3 * gi + 1], c.pos[3 * gi + 2]};
+    const float p[3] = {c.pos[3 * i], c.pos[3 * i + 1], c.pos[3 * i + 2]};
     float rsc[3], rq[4], rop, sc[3], q[4], op, c3[6];
-    load_attr<S>(c.attr, gi, rsc, &rop, rq);
+    load_attr<S>(c.attr, i, rsc, &rop, rq);
     activate_one(rsc, rq, rop, sc, q, &op);
     cov3d(sc, spp[0].cfg.scale_modifier, q, c3);
-    const S* shrow = static_cast<const S*>(c.sh) + (size_t)mc3 * gi;
+    const S* shrow = static_cast<const S*>(c.sh) + (size_t)mc3 * i;
     uint4 shv[6];
     if (mc3 == 48) {
 #pragma unroll
         for (int k = 0; k < 6; k++) shv[k] = reinterpret_cast<const uint4*>(shrow)[k];
     }
-    const unsigned lane = threadIdx.x & 31;
     for (int v = 0; v < n_views; v++) {
         const StepParams& sp = spp[v];
-        unsigned key = 0u;
-        if (valid) {
-            const long long o = (long long)v * N + i;
-            Proj r;
-            const bool vis = mc3 == 48 ? project_one<S>(sp, p, sc, q, op, reinterpret_cast<const S*>(shv), r, c3)
-                                       : project_one<S>(sp, p, sc, q, op, shrow, r, c3);
-            key = ((unsigned)v << 24) | (chosen_record(sp, vis, r, o, s, rects) >> 8);
-            dk.keys[o] = key;
-            dk.vals[o] = (unsigned)o;
-        }
-        // warp-aggregated digit counts (the upper depth digits are shared by most of a warp)
-#pragma unroll
-        for (int d = 0; d < 3; d++) {
-            const unsigned dg = valid ? (key >> (8 * d)) & 255u : 256u;
-            const unsigned peers = __match_any_sync(0xffffffffu, dg);
-            if (valid && lane == (unsigned)(__ffs(peers) - 1)) atomicAdd(&s_hist[d][dg], (unsigned)__popc(peers));
-        }
-    }
-    __syncthreads();
-    for (int e = threadIdx.x; e < 3 * 256; e += kBlock) {
-        const unsigned n = (&s_hist[0][0])[e];
-        if (n) atomicAdd(&ctrl->hist[e >> 8][e & 255], n);
+        const long long o = (long long)v * N + i;
+        Proj r;
+        const bool vis = mc3 == 48 ? project_one<S>(sp, p, sc, q, op, reinterpret_cast<const S*>(shv), r, c3)
+                                   : project_one<S>(sp, p, sc, q, op, shrow, r, c3);
+        dk.keys[v * seg + i] = ((unsigned)v << 24) | (chosen_record(sp, vis, r, o, s, rects) >> 8);
+        dk.vals[v * seg + i] = (unsigned)o;
     }
 }
 
@@ -795,9 +780,13 @@ cudaError_t launch_chosen_preprocess(cudaStream_t st, const StepParams* sp, int 
     if (N <= 0 || n_views <= 0) return cudaSuccess;
     const int grid = grid_for(N, kBlock);
     if (n_views > 1 || dk.views24) {
-        if (!dk.views24) return cudaErrorInvalidValue;
-        if (fp16) k_chosen_preprocess_views<__half><<<grid, kBlock, 0, st>>>(sp, N, n_views, c, s, dk, rects, ctrl);
-        else k_chosen_preprocess_views<__nv_bfloat16><<<grid, kBlock, 0, st>>>(sp, N, n_views, c, s, dk, rects, ctrl);
+        if (!dk.views24 || dk.seg_keys < (unsigned long long)N) return cudaErrorInvalidValue;
+        const int grid_v = (int)((dk.seg_keys + kBlock - 1) / kBlock);
+        if (fp16)
+            k_chosen_preprocess_views<__half><<<grid_v, kBlock, 0, st>>>(sp, N, n_views, c, s, dk, rects, ctrl);
+        else
+            k_chosen_preprocess_views<__nv_bfloat16><<<grid_v, kBlock, 0, st>>>(sp, N, n_views, c, s, dk, rects,
+                                                                                 ctrl);
     } else {
         if (fp16) k_chosen_preprocess<__half><<<grid, kBlock, 0, st>>>(sp, N, c, s, dk, rects, ctrl);
         else k_chosen_preprocess<__nv_bfloat16><<<grid, kBlock, 0, st>>>(sp, N, c, s, dk, rects, ctrl);

@@ -143,11 +143,12 @@ constexpr unsigned long long kDescValue = (1ull << 62) - 1;
 // the partial prefix is used (the result is then invalid and the host reports
 // GS3DC_ERR_DEVICE_TIMEOUT).  Block indices are tickets taken in launch order,
 // so every predecessor is resident or finished and publishes without waiting.
+// first_blk > 0: the scan restarts there (segments of blocks scanned apart).
 __device__ __forceinline__ unsigned long long lookback_exclusive_strided(
     unsigned long long* desc, int blk, int stride, int lane_off, unsigned long long aggregate,
-    unsigned* status, unsigned spin_limit) {
+    unsigned* status, unsigned spin_limit, int first_blk = 0) {
     unsigned long long* mine = desc + (size_t)blk * stride + lane_off;
-    if (blk == 0) {
+    if (blk == first_blk) {
         st_relaxed(mine, kDescPrefix | aggregate);
         return 0ull;
     }
@@ -155,7 +156,7 @@ __device__ __forceinline__ unsigned long long lookback_exclusive_strided(
     unsigned long long excl = 0;
     int j = blk - 1;
     unsigned spins = 0;
-    while (j >= 0) {
+    while (j >= first_blk) {
         const unsigned long long d = ld_relaxed(desc + (size_t)j * stride + lane_off);
         const unsigned long long flag = d & ~kDescValue;
         if (flag == 0ull) {

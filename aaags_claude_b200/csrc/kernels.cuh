@@ -142,6 +142,7 @@ struct DepthKeys {
     unsigned* vals;             // [N] Gaussian index
     bool views24 = false;       // several views: keys = view << 24 | the depth's upper 24 bits
     uint2* rects = nullptr;   // plain preprocess: tile rectangles (xmin | ymin << 16, xmax | ymax << 16), 0 if none
+    unsigned long long seg_keys = 0;   // several views: view v's keys at v * seg_keys (padded segments)
 };
 
 // Reduced-storage ("chosen") form: positions FP32, the other attributes and the
@@ -300,6 +301,17 @@ cudaError_t launch_radix_sort32(cudaStream_t st, const StepParams* sp, int digit
                                 const unsigned long long* count = nullptr, int first_digit = 0);
 cudaError_t launch_tile_ranges32(cudaStream_t st, unsigned long long capacity, const unsigned* tiles_sorted,
                                  unsigned* ranges, Control* ctrl);
+// Stable sort of 32-bit keys in segments of seg_keys keys (a multiple of 8192;
+// capacity a multiple of seg_keys), each segment sorted apart, on digits
+// [first_digit, first_digit + digits); every slot of the capacity is a key
+// (ctrl->gauss_keys = capacity).  seg_hist: digits * 256 zeroed counters per
+// segment; desc: digits * desc_stride zeroed descriptors (desc_stride as for
+// launch_radix_sort32 over the capacity).  *which: the buffer with the result.
+cudaError_t launch_radix_sort32_segmented(cudaStream_t st, const StepParams* sp, int first_digit, int digits,
+                                          unsigned long long capacity, unsigned long long seg_keys, unsigned* keys0,
+                                          unsigned* vals0, unsigned* keys1, unsigned* vals1,
+                                          unsigned long long* desc, unsigned long long desc_stride,
+                                          unsigned* seg_hist, Control* ctrl, int* which);
 // Ranges of global tile ids (the view's tile_base + local id) over pairs
 // sorted stably by local tile id from a view-grouped emission: a key holds the
 // local id in its low 8 * (sort_passes - kDepthDigits) bits and the view above.

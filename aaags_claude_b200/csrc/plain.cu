@@ -331,6 +331,8 @@ __global__ void __launch_bounds__(B) k_emit_ranked(const StepParams* __restrict_
     unsigned g = 0, dbits = 0, tbase = 0;
     if (r < N) {
         g = rank_gid[r];
+    }
+    if (r < N && g != 0xFFFFFFFFu) {   // several views: 0xFFFFFFFF is the padding of a view's sort segment
         if (n_per_view > 0) {
             // several views: entry g = view * n_per_view + Gaussian, spp is the views' parameter array;
             // the key is the view's local tile id, with the view above the nd sorted digits

@@ -77,6 +77,41 @@ __global__ void __launch_bounds__(kHistThreads) k_radix_hist(const K* __restrict
         if (s_h[e]) atomicAdd(&ctrl->hist[slot_base + (e >> 8) - first][e & 255], s_h[e]);
 }
 
+// Digit histograms per segment: the keys are segments of seg_keys keys (a
+// multiple of kSegTile), sorted apart; CTA b counts digits [first, first +
+// digits) of keys [b kSegTile, (b + 1) kSegTile), which lie in one segment,
+// into seg_hist[(segment * digits + digit - first) * 256 + value].
+constexpr unsigned long long kSegTile = 8192;
+__global__ void __launch_bounds__(kHistThreads) k_seg_hist(const unsigned* __restrict__ keys,
+                                                           unsigned long long seg_keys, int first, int digits,
+                                                           unsigned* __restrict__ seg_hist) {
+    __shared__ unsigned s_h[kMaxPasses * 256];
+    for (int e = threadIdx.x; e < digits * 256; e += blockDim.x) s_h[e] = 0;
+    __syncthreads();
+    const unsigned long long base = (unsigned long long)blockIdx.x * kSegTile;
+    const unsigned lane = threadIdx.x & 31;
+    for (unsigned long long i = base + threadIdx.x; i < base + kSegTile; i += blockDim.x) {
+        const unsigned key = keys[i];
+        for (int p = 0; p < digits; p++) {
+            const unsigned d = (key >> (8 * (first + p))) & 255u;
+            const unsigned peers = peer_mask8(0xffffffffu, d);
+            if (lane == (unsigned)(__ffs(peers) - 1)) atomicAdd(&s_h[p * 256 + d], (unsigned)__popc(peers));
+        }
+    }
+    __syncthreads();
+    const unsigned long long seg = base / seg_keys;
+    for (int e = threadIdx.x; e < digits * 256; e += blockDim.x)
+        if (s_h[e]) atomicAdd(&seg_hist[seg * (unsigned long long)digits * 256ull + (unsigned long long)e], s_h[e]);
+}
+
+// Segments of a segmented onesweep (SEG): seg_keys keys each (a multiple of
+// the CTA's keys), their digit histograms from k_seg_hist.
+struct SegSort {
+    const unsigned* hist;
+    unsigned long long seg_keys;
+    int first, digits;
+};
+
 // Keys per thread of a onesweep CTA: 16, or 32 for large sorts of 32-bit keys
 // (8192 keys per CTA: half the CTAs, so half the per-digit look-backs; measured
 // faster from tens of millions of keys on, slower at a few million).
@@ -120,8 +155,10 @@ __device__ __forceinline__ unsigned long long block_exclusive_scan64(unsigned lo
 // One pass over digit `pass` (key bits 8*pass..); `slot` selects the digit
 // histogram and CTA ticket in the control block.  The values are not held in
 // registers: the CTA asks for its slice to be brought into L2 when it starts
-// and loads each value where it scatters it.
-template <typename K, int ITEMS>
+// and loads each value where it scatters it.  SEG: the keys are segments
+// sorted apart (SegSort): a CTA's digit offsets start at its segment and its
+// look-back stops at the segment's first CTA.
+template <typename K, int ITEMS, bool SEG = false>
 __global__ void __launch_bounds__(kSortThreads, sweep_ctas_per_sm<K, ITEMS>()) k_onesweep(const StepParams* __restrict__ sp,
                                                               const K* __restrict__ kin,
                                                               const unsigned* __restrict__ vin,
@@ -130,7 +167,7 @@ __global__ void __launch_bounds__(kSortThreads, sweep_ctas_per_sm<K, ITEMS>()) k
                                                               unsigned long long capacity, int pass, int slot,
                                                               unsigned long long* desc,
                                                               const unsigned long long* count,
-                                                              Control* ctrl) {
+                                                              Control* ctrl, SegSort sg = SegSort{}) {
     constexpr int kItems = ITEMS;
     constexpr int kTileKeys = kSortThreads * kItems;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -188,10 +225,20 @@ __global__ void __launch_bounds__(kSortThreads, sweep_ctas_per_sm<K, ITEMS>()) k
     }
     // global offset of digit d for this tile: all smaller digits everywhere,
     // plus digit d in the tiles before this one (decoupled look-back)
-    const unsigned long long hist_d = ctrl->hist[slot][d];
-    const unsigned long long digit_start = block_exclusive_scan64(hist_d, sm.scan);
-    const unsigned long long tile_excl =
-        lookback_exclusive_strided(desc, t, 256, (int)d, (unsigned long long)run, &ctrl->status, sp->spin_limit);
+    unsigned long long seg_base = 0;
+    int first_t = 0;
+    unsigned long long hist_d;
+    if (SEG) {
+        const unsigned long long seg = base / sg.seg_keys;
+        seg_base = seg * sg.seg_keys;
+        first_t = (int)(seg_base / kTileKeys);
+        hist_d = sg.hist[(seg * (unsigned long long)sg.digits + (unsigned long long)(pass - sg.first)) * 256ull + d];
+    } else {
+        hist_d = ctrl->hist[slot][d];
+    }
+    const unsigned long long digit_start = seg_base + block_exclusive_scan64(hist_d, sm.scan);
+    const unsigned long long tile_excl = lookback_exclusive_strided(
+        desc, t, 256, (int)d, (unsigned long long)run, &ctrl->status, sp->spin_limit, first_t);
     // tile-local start of digit d, folded into the warps' prefixes and the output offset
     const unsigned dp = (unsigned)block_exclusive_scan64((unsigned long long)run, sm.scan);
 #pragma unroll
@@ -478,7 +525,49 @@ cudaError_t radix_sort_impl(cudaStream_t st, const StepParams* sp, int first, in
     return cudaSuccess;
 }
 
+template <int ITEMS>
+cudaError_t radix_sort_seg_impl(cudaStream_t st, const StepParams* sp, int first, int digits,
+                                unsigned long long capacity, unsigned long long seg_keys, unsigned* keys0,
+                                unsigned* vals0, unsigned* keys1, unsigned* vals1, unsigned long long* desc,
+                                unsigned long long desc_stride, unsigned* seg_hist, Control* ctrl, int* which) {
+    *which = 0;
+    if (capacity == 0 || digits <= 0) return cudaSuccess;
+    static std::atomic<unsigned long long> attr_done{0}, carve_done{0};
+    const int smem = (int)sizeof(SweepShared<unsigned, ITEMS>);
+    cudaError_t e = set_smem_once(attr_done, k_onesweep<unsigned, ITEMS, true>, smem);
+    if (e != cudaSuccess) return e;
+    if ((e = set_carveout_max_once(carve_done, k_onesweep<unsigned, ITEMS, true>)) != cudaSuccess) return e;
+    k_seg_hist<<<(unsigned)(capacity / kSegTile), kHistThreads, 0, st>>>(keys0, seg_keys, first, digits, seg_hist);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    const unsigned long long tiles = capacity / ((unsigned long long)kSortThreads * ITEMS);
+    const SegSort sg{seg_hist, seg_keys, first, digits};
+    unsigned *kin = keys0, *vin = vals0, *kout = keys1, *vout = vals1;
+    for (int p = first; p < first + digits; p++) {
+        k_onesweep<unsigned, ITEMS, true><<<(unsigned)tiles, kSortThreads, smem, st>>>(
+            sp, kin, vin, kout, vout, capacity, p, p - first, desc + (unsigned long long)(p - first) * desc_stride,
+            &ctrl->gauss_keys, ctrl, sg);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        std::swap(kin, kout);
+        std::swap(vin, vout);
+    }
+    *which = digits & 1;
+    return cudaSuccess;
+}
+
 }  // namespace
+
+cudaError_t launch_radix_sort32_segmented(cudaStream_t st, const StepParams* sp, int first_digit, int digits,
+                                          unsigned long long capacity, unsigned long long seg_keys, unsigned* keys0,
+                                          unsigned* vals0, unsigned* keys1, unsigned* vals1,
+                                          unsigned long long* desc, unsigned long long desc_stride,
+                                          unsigned* seg_hist, Control* ctrl, int* which) {
+    if (seg_keys == 0 || seg_keys % kSegTile != 0 || capacity % seg_keys != 0) return cudaErrorInvalidValue;
+    if (capacity >= kWideSweepKeys)
+        return radix_sort_seg_impl<32>(st, sp, first_digit, digits, capacity, seg_keys, keys0, vals0, keys1, vals1,
+                                       desc, desc_stride, seg_hist, ctrl, which);
+    return radix_sort_seg_impl<kSortItems>(st, sp, first_digit, digits, capacity, seg_keys, keys0, vals0, keys1,
+                                           vals1, desc, desc_stride, seg_hist, ctrl, which);
+}
 
 cudaError_t launch_radix_sort(cudaStream_t st, const StepParams* sp, int passes, unsigned long long capacity,
                               unsigned long long* keys0, unsigned* vals0, unsigned long long* keys1,
