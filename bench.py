@@ -367,6 +367,10 @@ def _measure_form(a, ctx, form, w, cam, cfg, tc, gt_dev, gt_pin, local, dist):
     r["launches"] = ctx.stat(gs3d.STAT_KERNELS_LAST) * a.steps
     r["graph"] = ctx.stat(gs3d.STAT_GRAPH_REPLAYS) > 0
     # ---- e2e: pinned host target in, loss out, every step ----
+    # a host target runs its own graphs (the forward before the copy lands): their capture is warm-up
+    for _ in range(3):
+        ctx.train_step(cam, gt_pin.numpy(), cfg, tc, it)
+        it += 1
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     loss = None
