@@ -191,8 +191,7 @@ struct gs3dc_ctx {
         cudaEvent_t views_event = nullptr;         // the staging's last copy has been consumed
         DevBuf<float4> rec0, rec1;
         DevBuf<float2> cbt;
-        DevBuf<float> depth, dm2, dcon, drgb, dop;
-        DevBuf<int> radius, tiles;
+        DevBuf<float> dm2, dcon, drgb, dop;
         DevBuf<uint2> rects;
         DevBuf<unsigned> dkeys[2];                 // (view << 24 | depth's upper 24 bits) of each entry
         DevBuf<unsigned> dvals[2];
@@ -1031,7 +1030,8 @@ struct BatchShape {
 
 ScreenPtrs batch_screen(gs3dc_ctx* c) {
     auto& b = c->batch;
-    return {b.rec0.p, b.rec1.p, b.cbt.p, b.depth.p, b.radius.p, b.tiles.p, nullptr, nullptr, nullptr, nullptr, nullptr};
+    // the reduced form keeps no depth, radius or tile-count arrays (the rectangles stand for them)
+    return {b.rec0.p, b.rec1.p, b.cbt.p, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
 }
 PixelPtrs batch_pixels(gs3dc_ctx* c) {
     auto& b = c->batch;
@@ -1067,9 +1067,6 @@ int batch_buffers(gs3dc_ctx* c, const BatchShape& sh) {
     CK(b.rec0.ensure(vn));
     CK(b.rec1.ensure(vn));
     CK(b.cbt.ensure(vn));
-    CK(b.depth.ensure(vn));
-    CK(b.radius.ensure(vn));
-    CK(b.tiles.ensure(vn));
     CK(b.rects.ensure(vn));
     if (b.dm2.n < 2 * vn) b.grads_zeroed = 0;
     CK(b.dm2.ensure(2 * vn));

@@ -14,6 +14,7 @@
 // alpha can reach 1/255, q = d^T conic d <= 2 ln(255 o): tiles outside it hold
 // no pixel the blend would accept, so they get no pair.
 #include <algorithm>
+#include <type_traits>
 
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
@@ -150,9 +151,11 @@ __device__ __forceinline__ void load_attr(const void* attr, long long i, float r
 
 // One camera's screen record of a projected Gaussian (r from project_one) at
 // entry o: the FP64 inverse of a near-degenerate 2D covariance, the reference's
-// tile rectangle cut to the box of the alpha >= 1/255 ellipse, the record,
-// depth, radius, tile count and rectangle.  Returns the depth bits for the
-// depth sort, 0xFFFFFFFF for a Gaussian without pairs.
+// tile rectangle cut to the box of the alpha >= 1/255 ellipse, the record and
+// the rectangle (whose area is the pair count).  The depth, radius and tile
+// count arrays of the FP32 form have no reader in this form (its emission reads
+// the rectangle, the sort the returned bits) and are not written.  Returns the
+// depth bits for the depth sort, 0xFFFFFFFF for a Gaussian without pairs.
 __device__ __forceinline__ unsigned chosen_record(const StepParams& sp, bool vis, Proj& r, long long o, ScreenPtrs s,
                                                   uint2* __restrict__ rects) {
     int cnt = 0;
@@ -188,16 +191,11 @@ __device__ __forceinline__ unsigned chosen_record(const StepParams& sp, bool vis
         s.rec0[o] = make_float4(r.px, r.py, r.con[0], r.con[1]);
         s.rec1[o] = make_float4(r.con[2], r.opac, r.rgb[0], r.rgb[1]);
         s.cbt[o] = blue_thr(r.rgb[2], r.opac);
-        s.depth[o] = r.depth;
-        s.radius[o] = r.radius;
     } else {
         s.rec0[o] = make_float4(0.f, 0.f, 0.f, 0.f);
         s.rec1[o] = make_float4(0.f, 0.f, 0.f, 0.f);
         s.cbt[o] = blue_thr(0.f, 0.f);
-        s.depth[o] = 0.f;
-        s.radius[o] = 0;
     }
-    s.tiles[o] = cnt;
     rects[o] = rect;
     return cnt > 0 ? dbits : 0xFFFFFFFFu;
 }
@@ -319,6 +317,63 @@ __device__ __forceinline__ void opt8(const StepParams& sp, uint4& p, uint4& m, u
     }
 }
 
+// The Adam constants of a step, read once per CTA.
+struct AdamK {
+    float b1, c1, b2, c2, bc1, bc2, eps;
+    __device__ __forceinline__ explicit AdamK(const StepParams& sp)
+        : b1(sp.beta1), c1(1.0f - sp.beta1), b2(sp.beta2), c2(1.0f - sp.beta2), bc1(sp.bc1), bc2(sp.bc2),
+          eps(sp.eps) {}
+};
+
+// BF16 storage, Adam: opt8 on 32-bit words of two elements, with the same
+// random words (p, m, v of each element in turn).  The stochastic rounding of
+// a finite x is (bits(x) + (r >> 16)) >> 16, two of which one byte permute
+// packs into a word.  A non-finite result would carry through the exponent
+// there, so the caller redoes a chunk with one (false) element-wise (opt8).
+__device__ __forceinline__ bool opt8_bf16_words(const AdamK& a, uint4& p, uint4& m, uint4& v, const float g[8],
+                                                const float lr[8], unsigned st) {
+    unsigned* pw = reinterpret_cast<unsigned*>(&p);
+    unsigned* mw = reinterpret_cast<unsigned*>(&m);
+    unsigned* vw = reinterpret_cast<unsigned*>(&v);
+    bool finite = true;
+#pragma unroll
+    for (int w = 0; w < 4; w++) {
+        unsigned pb[2], mb[2], vb[2];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int k = 2 * w + h;
+            // element k is the low (h = 0) or high (h = 1) half of word w
+            const float pk = __uint_as_float(h ? (pw[w] & 0xffff0000u) : (pw[w] << 16));
+            float mk = __uint_as_float(h ? (mw[w] & 0xffff0000u) : (mw[w] << 16));
+            float vk = __uint_as_float(h ? (vw[w] & 0xffff0000u) : (vw[w] << 16));
+            mk = fmaf(a.b1, mk, a.c1 * g[k]);
+            vk = fmaf(a.b2, vk, a.c2 * g[k] * g[k]);
+            const float pn = pk - __fdividef(lr[k] * a.bc1 * mk, sqrtf(vk * a.bc2) + a.eps);
+            const float kInf = __int_as_float(0x7f800000);
+            finite &= (fabsf(pn) < kInf) & (fabsf(mk) < kInf) & (fabsf(vk) < kInf);
+            const unsigned rp = st = lcg_next(st), rm = st = lcg_next(st), rv = st = lcg_next(st);
+            pb[h] = __float_as_uint(pn) + (rp >> 16);
+            mb[h] = __float_as_uint(mk) + (rm >> 16);
+            vb[h] = __float_as_uint(vk) + (rv >> 16);
+        }
+        pw[w] = __byte_perm(pb[0], pb[1], 0x7632);
+        mw[w] = __byte_perm(mb[0], mb[1], 0x7632);
+        vw[w] = __byte_perm(vb[0], vb[1], 0x7632);
+    }
+    return finite;
+}
+
+// The Adam step of opt8 on words, for BF16 storage with Adam; false leaves the
+// caller to redo the chunk element-wise from its stored inputs (another form,
+// SGD, or a non-finite result).
+template <typename S>
+__device__ __forceinline__ bool opt8_words(const StepParams& sp, const AdamK& a, uint4& p, uint4& m, uint4& v,
+                                           const float g[8], const float lr[8], unsigned e0, unsigned salt) {
+    if constexpr (std::is_same<S, __nv_bfloat16>::value)
+        return sp.use_adam && opt8_bf16_words(a, p, m, v, g, lr, mix32(e0 ^ salt, sp.seed));
+    return false;
+}
+
 // ---- adjoint (staged, coalesced) ----
 
 constexpr int kCB = 64;           // Gaussians (= threads) per CTA of the adjoint
@@ -328,8 +383,18 @@ constexpr int kCB = 64;           // Gaussians (= threads) per CTA of the adjoin
 constexpr int kShPitch = 52;
 
 // One view: the SH gradient of coefficient k is basis[k / 3] * geff[k % 3], so the
-// CTA keeps the 16 + 3 factors per Gaussian (SoA, conflict-free) instead of the
-// 48 products (18 KB per CTA of 64, 10 CTAs per SM).  Several views sum the products: g_sh.
+// CTA keeps the 16 + 3 factors per Gaussian instead of the 48 products (18 KB per
+// CTA of 64, 10 CTAs per SM).  Degree-3 storage (48 coefficients = six 8-wide
+// optimiser chunks per Gaussian) keeps the bases chunk-major: chunk c of
+// Gaussian t (coefficients 8c .. 8c + 7, bases b0 = 8c / 3 .. b0 + 3) reads
+// the float4 bsh4[6 t + c], so that the 32 lanes of a warp, which take 32
+// consecutive chunks, read 32 consecutive float4s.  Other storage keeps
+// [basis][Gaussian].  The channel factors are [channel][Gaussian] with a
+// pitch of 72: the lanes of a warp span at most six Gaussians, so the three
+// rows of those six fall into distinct banks.  Several views sum the products: g_sh.
+constexpr int kGeffPitch = 72;
+__host__ __device__ constexpr int chunk_base0(int c) { return (8 * c) / 3; }   // first basis of chunk c
+
 template <typename S, bool MULTI>
 struct __align__(16) ChosenBwdShared {
     uint4 sh[kCB * 6];            // 16-bit SH, up to 48 per Gaussian (6 x 16 bytes)
@@ -338,13 +403,21 @@ struct __align__(16) ChosenBwdShared {
     float dm2[2 * kCB], dcon[3 * kCB], drgb[3 * kCB], dop[kCB];
     float g_pos[3 * kCB], g_sc[3 * kCB], g_rot[4 * kCB], g_op[kCB];
     alignas(16) float g_sh[MULTI ? kShPitch * kCB : 4];
-    float basis[MULTI ? 1 : 16 * kCB];   // [basis][Gaussian]
-    float geff[MULTI ? 1 : 3 * kCB];     // [channel][Gaussian]
+    alignas(16) float bsh[MULTI ? 4 : 24 * kCB];   // bases: 6 float4 chunks per Gaussian, or [basis][Gaussian]
+    float geff[MULTI ? 1 : 3 * kGeffPitch];       // [channel][Gaussian]
     unsigned long long bar;       // completion of the bulk copies into the arrays above
     // SH gradient of coefficient kk of the CTA's Gaussian t
-    __device__ __forceinline__ float gsh(int t, int kk) const {
+    __device__ __forceinline__ float gsh(int t, int kk, int mc3) const {
         if (MULTI) return g_sh[kShPitch * t + kk];
-        return basis[(kk / 3) * kCB + t] * geff[(kk % 3) * kCB + t];
+        const int b = kk / 3, ch = kk - 3 * b;
+        float bv;
+        if (mc3 == 48) {
+            const int c = (3 * b) / 8;   // the chunk whose bases b0 .. b0 + 3 hold b
+            bv = bsh[4 * (6 * t + c) + b - chunk_base0(c)];
+        } else {
+            bv = bsh[b * kCB + t];
+        }
+        return bv * geff[ch * kGeffPitch + t];
     }
 };
 
@@ -405,83 +478,80 @@ template <typename S>
 __device__ __forceinline__ void adjoint_slice(ChosenBwdShared<S, false>& sm, const StepParams& sp, long long g0,
                                               int ng, int mc3, RGradPtrs rg) {
     const int tid = threadIdx.x;
-    if (tid < ng) {
-#pragma unroll
-        for (int k = 0; k < 3; k++) sm.g_pos[3 * tid + k] = sm.g_sc[3 * tid + k] = 0.f;
-#pragma unroll
-        for (int k = 0; k < 4; k++) sm.g_rot[4 * tid + k] = 0.f;
-        sm.g_op[tid] = 0.f;
-        for (int k = 0; k < 16; k++) sm.basis[k * kCB + tid] = 0.f;
-        for (int k = 0; k < 3; k++) sm.geff[k * kCB + tid] = 0.f;
+    const long long e0 = g0;
+    // the screen-gradient accumulators restart at zero for the next step
+    for (int e = tid; e < 2 * ng; e += kCB) rg.dm2[2 * e0 + e] = 0.f;
+    for (int e = tid; e < 3 * ng; e += kCB) {
+        rg.dcon[3 * e0 + e] = 0.f;
+        rg.drgb[3 * e0 + e] = 0.f;
     }
-    {
-        const long long e0 = g0;
-        // the screen-gradient accumulators restart at zero for the next step
-        for (int e = tid; e < 2 * ng; e += kCB) rg.dm2[2 * e0 + e] = 0.f;
-        for (int e = tid; e < 3 * ng; e += kCB) {
-            rg.dcon[3 * e0 + e] = 0.f;
-            rg.drgb[3 * e0 + e] = 0.f;
-        }
-        for (int e = tid; e < ng; e += kCB) rg.dop[e0 + e] = 0.f;
-        if (tid < ng) {
-            BwdIn in;
+    for (int e = tid; e < ng; e += kCB) rg.dop[e0 + e] = 0.f;
+    if (tid >= ng) return;
+    BwdIn in;
 #pragma unroll
-            for (int k = 0; k < 3; k++) {
-                in.dcn[k] = sm.dcon[3 * tid + k];
-                in.drgb[k] = sm.drgb[3 * tid + k];
+    for (int k = 0; k < 3; k++) {
+        in.dcn[k] = sm.dcon[3 * tid + k];
+        in.drgb[k] = sm.drgb[3 * tid + k];
+    }
+    in.dm[0] = sm.dm2[2 * tid];
+    in.dm[1] = sm.dm2[2 * tid + 1];
+    in.dop = sm.dop[tid];
+    BwdOut o;
+#pragma unroll
+    for (int k = 0; k < 3; k++) o.gp[k] = o.gs[k] = o.geff[k] = 0.f;
+#pragma unroll
+    for (int k = 0; k < 4; k++) o.gq[k] = 0.f;
+    o.gop = 0.f;
+#pragma unroll
+    for (int k = 0; k < 16; k++) o.basis[k] = 0.f;
+    // every gradient is linear in the screen gradients: a Gaussian without any adds none
+    const bool any = in.dm[0] != 0.f || in.dm[1] != 0.f || in.dcn[0] != 0.f || in.dcn[1] != 0.f ||
+                     in.dcn[2] != 0.f || in.drgb[0] != 0.f || in.drgb[1] != 0.f || in.drgb[2] != 0.f ||
+                     in.dop != 0.f;
+    if (any) {
+#pragma unroll
+        for (int k = 0; k < 3; k++) in.p[k] = sm.pos[3 * tid + k];
+        in.act = nullptr;
+        load_attr<S>(sm.attr, tid, in.rsc, &in.rop, in.rq);
+        float shf[48];
+        if (mc3 == 48) {
+            // this Gaussian's 96 SH bytes as six 16-byte loads
+            const uint4* row = sm.sh + 6 * tid;
+#pragma unroll
+            for (int qd = 0; qd < 6; qd++) {
+                const uint4 vv = row[qd];
+                const S* h = reinterpret_cast<const S*>(&vv);
+#pragma unroll
+                for (int k = 0; k < 8; k++) shf[8 * qd + k] = ldf(h[k]);
             }
-            in.dm[0] = sm.dm2[2 * tid];
-            in.dm[1] = sm.dm2[2 * tid + 1];
-            in.dop = sm.dop[tid];
-            // every gradient is linear in the screen gradients: a Gaussian without any adds none
-            const bool any = in.dm[0] != 0.f || in.dm[1] != 0.f || in.dcn[0] != 0.f || in.dcn[1] != 0.f ||
-                             in.dcn[2] != 0.f || in.drgb[0] != 0.f || in.drgb[1] != 0.f || in.drgb[2] != 0.f ||
-                             in.dop != 0.f;
-            if (any) {
+        } else {
+            const S* shs = reinterpret_cast<const S*>(sm.sh) + mc3 * tid;
 #pragma unroll
-                for (int k = 0; k < 3; k++) in.p[k] = sm.pos[3 * tid + k];
-                in.act = nullptr;
-                load_attr<S>(sm.attr, tid, in.rsc, &in.rop, in.rq);
-                float shf[48];
-                if (mc3 == 48) {
-                    // this Gaussian's 96 SH bytes as six 16-byte loads
-                    const uint4* row = sm.sh + 6 * tid;
-#pragma unroll
-                    for (int qd = 0; qd < 6; qd++) {
-                        const uint4 vv = row[qd];
-                        const S* h = reinterpret_cast<const S*>(&vv);
-#pragma unroll
-                        for (int k = 0; k < 8; k++) shf[8 * qd + k] = ldf(h[k]);
-                    }
-                } else {
-                    const S* shs = reinterpret_cast<const S*>(sm.sh) + mc3 * tid;
-#pragma unroll
-                    for (int k = 0; k < 48; k++) shf[k] = k < mc3 ? ldf(shs[k]) : 0.f;
-                }
-                in.sh = shf;
-                BwdOut o;
-#pragma unroll
-                for (int k = 0; k < 3; k++) o.gp[k] = o.gs[k] = o.geff[k] = 0.f;
-#pragma unroll
-                for (int k = 0; k < 4; k++) o.gq[k] = 0.f;
-                o.gop = 0.f;
-#pragma unroll
-                for (int k = 0; k < 16; k++) o.basis[k] = 0.f;
-                backward_one(sp, in, o);
-#pragma unroll
-                for (int k = 0; k < 3; k++) {
-                    sm.g_pos[3 * tid + k] = o.gp[k];
-                    sm.g_sc[3 * tid + k] = o.gs[k];
-                }
-#pragma unroll
-                for (int k = 0; k < 4; k++) sm.g_rot[4 * tid + k] = o.gq[k];
-                sm.g_op[tid] = o.gop;
-#pragma unroll
-                for (int k = 0; k < 16; k++) sm.basis[k * kCB + tid] = o.basis[k];
-#pragma unroll
-                for (int k = 0; k < 3; k++) sm.geff[k * kCB + tid] = o.geff[k];
-            }
+            for (int k = 0; k < 48; k++) shf[k] = k < mc3 ? ldf(shs[k]) : 0.f;
         }
+        in.sh = shf;
+        backward_one(sp, in, o);
+    }
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        sm.g_pos[3 * tid + k] = o.gp[k];
+        sm.g_sc[3 * tid + k] = o.gs[k];
+        sm.geff[k * kGeffPitch + tid] = o.geff[k];
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) sm.g_rot[4 * tid + k] = o.gq[k];
+    sm.g_op[tid] = o.gop;
+    if (mc3 == 48) {
+        float4* const b4 = reinterpret_cast<float4*>(sm.bsh) + 6 * tid;
+#pragma unroll
+        for (int c = 0; c < 6; c++) {
+            constexpr int kLast = 15;
+            const int b0 = chunk_base0(c);
+            b4[c] = make_float4(o.basis[b0], o.basis[b0 + 1], o.basis[b0 + 2], o.basis[min(b0 + 3, kLast)]);
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < 16; k++) sm.bsh[k * kCB + tid] = o.basis[k];
     }
 }
 
@@ -500,7 +570,7 @@ __device__ __forceinline__ void adam_slice(ChosenBwdShared<S, MULTI>& sm, const 
         for (int e = tid; e < ng; e += kCB) gout.g_op[g0 + e] = sm.g_op[e];
         for (int e = tid; e < mc3 * ng; e += kCB) {
             const int t = e / mc3, k = e - t * mc3;
-            gout.g_sh[(size_t)mc3 * g0 + e] = sm.gsh(t, k);
+            gout.g_sh[(size_t)mc3 * g0 + e] = sm.gsh(t, k, mc3);
         }
     }
     const long long sh0 = (long long)mc3 * g0;
@@ -537,6 +607,7 @@ __device__ __forceinline__ void adam_slice(ChosenBwdShared<S, MULTI>& sm, const 
             mm_n = m4[tid];
             vv_n = v4[tid];
         }
+        const AdamK ak(sp);
         for (int q = tid; q < nq; q += kCB) {
             uint4 pp = sm.sh[q], mm = mm_n, vv = vv_n;
             if (q + kCB < nq) {
@@ -544,23 +615,52 @@ __device__ __forceinline__ void adam_slice(ChosenBwdShared<S, MULTI>& sm, const 
                 vv_n = v4[q + kCB];
             }
             float gg[8];
-            // (Gaussian t, coefficient kk = basis b, channel ch) of element 8q, then stepped by one
-            int t = (8 * q) / mc3, kk = 8 * q - t * mc3;
-            int b = kk / 3, ch = kk - 3 * b;
-#pragma unroll
-            for (int k = 0; k < 8; k++) {
-                gg[k] = MULTI ? sm.g_sh[kShPitch * t + kk] : sm.basis[b * kCB + t] * sm.geff[ch * kCB + t];
-                kk++;
-                if (++ch == 3) {
-                    ch = 0;
-                    b++;
+            if (mc3 == 48) {
+                // chunk c of Gaussian t: coefficients 8c .. 8c + 7
+                const int t = q / 6, c = q - 6 * t;
+                if (MULTI) {
+                    const float4* gs = reinterpret_cast<const float4*>(&sm.g_sh[kShPitch * t + 8 * c]);
+                    const float4 lo = gs[0], hi = gs[1];
+                    gg[0] = lo.x, gg[1] = lo.y, gg[2] = lo.z, gg[3] = lo.w;
+                    gg[4] = hi.x, gg[5] = hi.y, gg[6] = hi.z, gg[7] = hi.w;
+                } else {
+                    // coefficient 8c + k is basis b0 + (ch0 + k) / 3, channel (ch0 + k) % 3, with
+                    // 8c = 3 b0 + ch0; bases b0 .. b0 + 3 are the chunk's float4
+                    const float4 bb = reinterpret_cast<const float4*>(sm.bsh)[q];
+                    const int ch0 = (2 * c) % 3;
+                    const float* ge = sm.geff + t;
+                    const float G0 = ge[ch0 * kGeffPitch];
+                    const float G1 = ge[(ch0 == 2 ? 0 : ch0 + 1) * kGeffPitch];
+                    const float G2 = ge[(ch0 == 0 ? 2 : ch0 - 1) * kGeffPitch];
+                    // k % 3 == 1 moves to the next basis when ch0 = 2, k % 3 == 2 when ch0 >= 1
+                    const bool up1 = ch0 == 2, up2 = ch0 != 0;
+                    gg[0] = bb.x * G0;
+                    gg[1] = (up1 ? bb.y : bb.x) * G1;
+                    gg[2] = (up2 ? bb.y : bb.x) * G2;
+                    gg[3] = bb.y * G0;
+                    gg[4] = (up1 ? bb.z : bb.y) * G1;
+                    gg[5] = (up2 ? bb.z : bb.y) * G2;
+                    gg[6] = bb.z * G0;
+                    gg[7] = (up1 ? bb.w : bb.z) * G1;
                 }
-                if (kk == mc3) {   // mc3 is a multiple of 3
-                    kk = b = ch = 0;
-                    t++;
+            } else {
+                // (Gaussian t, coefficient kk) of element 8q, then stepped by one
+                int t = (8 * q) / mc3, kk = 8 * q - t * mc3;
+#pragma unroll
+                for (int k = 0; k < 8; k++) {
+                    gg[k] = sm.gsh(t, kk, mc3);
+                    if (++kk == mc3) {
+                        kk = 0;
+                        t++;
+                    }
                 }
             }
-            opt8<S>(sp, pp, mm, vv, gg, lr_sh, (unsigned)(sh0 + 8 * q), 0x5bd1e995u);
+            if (!opt8_words<S>(sp, ak, pp, mm, vv, gg, lr_sh, (unsigned)(sh0 + 8 * q), 0x5bd1e995u)) {
+                pp = sm.sh[q];
+                mm = m4[q];
+                vv = v4[q];
+                opt8<S>(sp, pp, mm, vv, gg, lr_sh, (unsigned)(sh0 + 8 * q), 0x5bd1e995u);
+            }
             p4[q] = pp;
             m4[q] = mm;
             v4[q] = vv;
@@ -570,7 +670,7 @@ __device__ __forceinline__ void adam_slice(ChosenBwdShared<S, MULTI>& sm, const 
         for (int e = tid; e < mc3 * ng; e += kCB) {
             const int t = e / mc3;
             float m = __bfloat162float(msh[sh0 + e]), v = __bfloat162float(vsh[sh0 + e]);
-            const float pn = opt_elem(sp, ldf(shs[e]), m, v, sm.gsh(t, e - t * mc3), sp.lr_sh);
+            const float pn = opt_elem(sp, ldf(shs[e]), m, v, sm.gsh(t, e - t * mc3, mc3), sp.lr_sh);
             unsigned rp, rm, rv;
             sr_words((unsigned)(sh0 + e) ^ 0x5bd1e995u, sp.seed, rp, rm, rv);
             shw[sh0 + e] = cvt_sr<S>(pn, rp);
@@ -587,7 +687,12 @@ __device__ __forceinline__ void adam_slice(ChosenBwdShared<S, MULTI>& sm, const 
                              sm.g_rot[4 * t], sm.g_rot[4 * t + 1], sm.g_rot[4 * t + 2], sm.g_rot[4 * t + 3]};
         uint4 pp = sm.attr[t];
         uint4 mm = am, vv = av;
-        opt8<S>(sp, pp, mm, vv, gg, lra, (unsigned)(8 * (g0 + t)), 0u);
+        if (!opt8_words<S>(sp, AdamK(sp), pp, mm, vv, gg, lra, (unsigned)(8 * (g0 + t)), 0u)) {
+            pp = sm.attr[t];
+            mm = am;
+            vv = av;
+            opt8<S>(sp, pp, mm, vv, gg, lra, (unsigned)(8 * (g0 + t)), 0u);
+        }
         reinterpret_cast<uint4*>(c.attr)[g0 + t] = pp;
         reinterpret_cast<uint4*>(c.m_attr)[g0 + t] = mm;
         reinterpret_cast<uint4*>(c.v_attr)[g0 + t] = vv;
