@@ -156,8 +156,10 @@ __device__ __forceinline__ void load_attr(const void* attr, long long i, float r
 // count arrays of the FP32 form have no reader in this form (its emission reads
 // the rectangle, the sort the returned bits) and are not written.  Returns the
 // depth bits for the depth sort, 0xFFFFFFFF for a Gaussian without pairs.
+// olog, when given, holds (logf(255 o), accept_threshold2(o)) of the record's
+// opacity o, computed once for all views of a Gaussian.
 __device__ __forceinline__ unsigned chosen_record(const StepParams& sp, bool vis, Proj& r, long long o, ScreenPtrs s,
-                                                  uint2* __restrict__ rects) {
+                                                  uint2* __restrict__ rects, const float* olog = nullptr) {
     int cnt = 0;
     uint2 rect = make_uint2(0u, 0u);
     unsigned dbits = 0xFFFFFFFFu;
@@ -175,7 +177,7 @@ __device__ __forceinline__ unsigned chosen_record(const StepParams& sp, bool vis
         // box of the ellipse d^T conic d <= 2 ln(255 o) (with margin), cut from the reference's rectangle
         const float o255 = 255.0f * r.opac;
         if (o255 > 1.0f) {
-            const float tau = 2.0f * logf(o255) * 1.001f + 1e-3f;
+            const float tau = 2.0f * (olog ? olog[0] : logf(o255)) * 1.001f + 1e-3f;
             const float ex = sqrtf(tau * r.cov2[0]), ey = sqrtf(tau * r.cov2[2]);
             const float tw = (float)sp.cfg.tile_w, th = (float)sp.cfg.tile_h;
             const int x0 = max(r.rmn[0], (int)floorf((r.px - ex) / tw));
@@ -190,7 +192,7 @@ __device__ __forceinline__ unsigned chosen_record(const StepParams& sp, bool vis
         }
         s.rec0[o] = make_float4(r.px, r.py, r.con[0], r.con[1]);
         s.rec1[o] = make_float4(r.con[2], r.opac, r.rgb[0], r.rgb[1]);
-        s.cbt[o] = blue_thr(r.rgb[2], r.opac);
+        s.cbt[o] = olog ? make_float2(r.rgb[2], olog[1]) : blue_thr(r.rgb[2], r.opac);
     } else {
         s.rec0[o] = make_float4(0.f, 0.f, 0.f, 0.f);
         s.rec1[o] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -264,13 +266,16 @@ __global__ void __launch_bounds__(kBlock) k_chosen_preprocess_views(const StepPa
 #pragma unroll
         for (int k = 0; k < 6; k++) shv[k] = reinterpret_cast<const uint4*>(shrow)[k];
     }
+    // without antialiasing the record's opacity is op in every view: its two logarithms once
+    const float olog[2] = {logf(255.0f * op), accept_threshold2(op)};
     for (int v = 0; v < n_views; v++) {
         const StepParams& sp = spp[v];
         const long long o = (long long)v * N + i;
         Proj r;
         const bool vis = mc3 == 48 ? project_one<S>(sp, p, sc, q, op, reinterpret_cast<const S*>(shv), r, c3)
                                    : project_one<S>(sp, p, sc, q, op, shrow, r, c3);
-        dk.keys[v * seg + i] = ((unsigned)v << 24) | (chosen_record(sp, vis, r, o, s, rects) >> 8);
+        const float* const ol = sp.cfg.antialiasing ? nullptr : olog;
+        dk.keys[v * seg + i] = ((unsigned)v << 24) | (chosen_record(sp, vis, r, o, s, rects, ol) >> 8);
         dk.vals[v * seg + i] = (unsigned)o;
     }
 }

@@ -5,7 +5,7 @@
 // Design (one-sweep, after Adinets & Merrill, "Onesweep: A Faster Least
 // Significant Digit Radix Sort for GPUs", 2022):
 //   k_radix_hist  one read of the keys counts the 8-bit digits of every pass
-//                 (warp-aggregated with peer_mask8).
+//                 (hist_add: one shared add for a digit the warp shares).
 //   k_onesweep    one launch per pass.  A CTA takes the next 4096-key tile by
 //                 ticket, ranks its keys per warp with peer_mask8 /
 //                 popc, publishes its per-digit counts and finds its global
@@ -46,6 +46,21 @@ __device__ __forceinline__ unsigned peer_mask8(unsigned mask, unsigned d) {
     return peers;
 }
 
+// Adds one to bin d of the shared histogram h for each lane of mask (which
+// all call it).  A digit the whole warp shares (the upper digits of depth keys,
+// a segment's padding) takes one add; other digits take one add per lane.
+// (Measured against one add per distinct value, found with 8 ballots or
+// match_any: 64-view step 33.71 / 34.03 -> 33.26 ms.)
+__device__ __forceinline__ void hist_add(unsigned* h, unsigned mask, unsigned d) {
+    const int leader = __ffs(mask) - 1;
+    const unsigned d0 = __shfl_sync(mask, d, leader);
+    if (__all_sync(mask, d == d0)) {
+        if ((int)(threadIdx.x & 31) == leader) atomicAdd(&h[d0], (unsigned)__popc(mask));
+    } else {
+        atomicAdd(&h[d], 1u);
+    }
+}
+
 // Digit histograms of digits [first, passes) (digit d = key bits 8d..8d+7)
 // into ctrl->hist[slot_base + d - first].
 template <typename K>
@@ -58,18 +73,13 @@ __global__ void __launch_bounds__(kHistThreads) k_radix_hist(const K* __restrict
     __syncthreads();
     const unsigned long long P = min(*count, capacity);
     const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
-    const unsigned lane = threadIdx.x & 31;
     for (unsigned long long base = (unsigned long long)blockIdx.x * blockDim.x; base < P; base += stride) {
         const unsigned long long i = base + threadIdx.x;
         const bool valid = i < P;
         const unsigned mask = __ballot_sync(0xffffffffu, valid);
         if (valid) {
             const K key = keys[i];
-            for (int p = first; p < passes; p++) {
-                const unsigned d = (unsigned)(key >> (8 * p)) & 255u;
-                const unsigned peers = peer_mask8(mask, d);
-                if (lane == (unsigned)(__ffs(peers) - 1)) atomicAdd(&s_h[p * 256 + d], (unsigned)__popc(peers));
-            }
+            for (int p = first; p < passes; p++) hist_add(&s_h[p * 256], mask, (unsigned)(key >> (8 * p)) & 255u);
         }
     }
     __syncthreads();
@@ -89,14 +99,20 @@ __global__ void __launch_bounds__(kHistThreads) k_seg_hist(const unsigned* __res
     for (int e = threadIdx.x; e < digits * 256; e += blockDim.x) s_h[e] = 0;
     __syncthreads();
     const unsigned long long base = (unsigned long long)blockIdx.x * kSegTile;
-    const unsigned lane = threadIdx.x & 31;
-    for (unsigned long long i = base + threadIdx.x; i < base + kSegTile; i += blockDim.x) {
-        const unsigned key = keys[i];
-        for (int p = 0; p < digits; p++) {
-            const unsigned d = (key >> (8 * (first + p))) & 255u;
-            const unsigned peers = peer_mask8(0xffffffffu, d);
-            if (lane == (unsigned)(__ffs(peers) - 1)) atomicAdd(&s_h[p * 256 + d], (unsigned)__popc(peers));
-        }
+    // 16-byte loads, all issued before the counting (kSegTile / 4 / kHistThreads = 4 per thread)
+    constexpr int kVec = (int)(kSegTile / 4 / kHistThreads);
+    static_assert(kSegTile % (4 * kHistThreads) == 0, "whole 16-byte loads per thread");
+    uint4 kv[kVec];
+    const uint4* k4 = reinterpret_cast<const uint4*>(keys + base);
+#pragma unroll
+    for (int j = 0; j < kVec; j++) kv[j] = k4[j * kHistThreads + threadIdx.x];
+#pragma unroll
+    for (int j = 0; j < kVec; j++) {
+        const unsigned kk[4] = {kv[j].x, kv[j].y, kv[j].z, kv[j].w};
+#pragma unroll
+        for (int e = 0; e < 4; e++)
+            for (int p = 0; p < digits; p++)
+                hist_add(&s_h[p * 256], 0xffffffffu, (kk[e] >> (8 * (first + p))) & 255u);
     }
     __syncthreads();
     const unsigned long long seg = base / seg_keys;
