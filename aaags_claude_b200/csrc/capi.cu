@@ -2163,6 +2163,7 @@ int gs3dc_train_step_batch(gs3dc_ctx* c, int n_views, const gs3d_camera* cams, c
             continue;
         }
         if (loss) *loss = (float)c->ctrl_host->loss_sum;
+        c->last_pairs = c->ctrl_host->total_pairs;
         if (tuning) {
             float f = 0.f, bw = 0.f;
             CK(cudaEventElapsedTime(&f, c->tune_ev[0], c->tune_ev[1]));

@@ -290,31 +290,34 @@ __device__ __forceinline__ unsigned tile_of(unsigned long long key) { return (un
 __global__ void k_ranges_views4(const unsigned* __restrict__ keys, const StepParams* __restrict__ views,
                                 unsigned long long capacity, unsigned* __restrict__ ranges, Control* ctrl) {
     const unsigned long long P = min(ctrl->total_pairs, capacity);
-    const unsigned long long i0 = 4ull * ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x);
-    if (i0 >= P) return;
     const int tile_bits = 8 * (views[0].sort_passes - kDepthDigits);
     const unsigned local_mask = (1u << tile_bits) - 1u;   // tile_bits <= 24
-    unsigned k[5];
-    if (i0 + 4 <= capacity) {
-        const uint4 kk = *reinterpret_cast<const uint4*>(keys + i0);
-        k[0] = kk.x, k[1] = kk.y, k[2] = kk.z, k[3] = kk.w;
-    } else {
+    // grid-stride over the pairs present (the grid is sized for the SMs, not the capacity)
+    const unsigned long long step = 4ull * gridDim.x * blockDim.x;
+    for (unsigned long long i0 = 4ull * ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x); i0 < P;
+         i0 += step) {
+        unsigned k[5];
+        if (i0 + 4 <= capacity) {
+            const uint4 kk = *reinterpret_cast<const uint4*>(keys + i0);
+            k[0] = kk.x, k[1] = kk.y, k[2] = kk.z, k[3] = kk.w;
+        } else {
 #pragma unroll
-        for (int j = 0; j < 4; j++) k[j] = i0 + j < P ? keys[i0 + j] : 0u;
-    }
-    k[4] = i0 + 4 < P ? keys[i0 + 4] : 0u;
-    unsigned t[5];
+            for (int j = 0; j < 4; j++) k[j] = i0 + j < P ? keys[i0 + j] : 0u;
+        }
+        k[4] = i0 + 4 < P ? keys[i0 + 4] : 0u;
+        unsigned t[5];
 #pragma unroll
-    for (int j = 0; j < 5; j++) t[j] = views[k[j] >> tile_bits].tile_base + (k[j] & local_mask);
-    if (i0 == 0) ranges[2 * t[0]] = 0u;
+        for (int j = 0; j < 5; j++) t[j] = views[k[j] >> tile_bits].tile_base + (k[j] & local_mask);
+        if (i0 == 0) ranges[2 * t[0]] = 0u;
 #pragma unroll
-    for (int j = 0; j < 4; j++) {
-        const unsigned long long i = i0 + (unsigned long long)j;
-        if (i >= P) break;
-        const bool last = i + 1 == P;
-        if (last || t[j + 1] != t[j]) {
-            ranges[2 * t[j] + 1] = (unsigned)(i + 1);
-            if (!last) ranges[2 * t[j + 1]] = (unsigned)(i + 1);
+        for (int j = 0; j < 4; j++) {
+            const unsigned long long i = i0 + (unsigned long long)j;
+            if (i >= P) break;
+            const bool last = i + 1 == P;
+            if (last || t[j + 1] != t[j]) {
+                ranges[2 * t[j] + 1] = (unsigned)(i + 1);
+                if (!last) ranges[2 * t[j + 1]] = (unsigned)(i + 1);
+            }
         }
     }
 }
@@ -340,29 +343,32 @@ __global__ void k_ranges(const K* __restrict__ keys, unsigned long long capacity
 __global__ void k_ranges32(const unsigned* __restrict__ tiles, unsigned long long capacity,
                            unsigned* __restrict__ ranges, Control* ctrl) {
     const unsigned long long P = min(ctrl->total_pairs, capacity);
-    const unsigned long long i0 = 4ull * ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x);
-    if (i0 >= P) return;
-    unsigned t[5];
-    if (i0 + 4 <= capacity) {
-        const uint4 v = *reinterpret_cast<const uint4*>(tiles + i0);
-        t[0] = v.x;
-        t[1] = v.y;
-        t[2] = v.z;
-        t[3] = v.w;
-    } else {
+    // grid-stride over the pairs present (the grid is sized for the SMs, not the capacity)
+    const unsigned long long step = 4ull * gridDim.x * blockDim.x;
+    for (unsigned long long i0 = 4ull * ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x); i0 < P;
+         i0 += step) {
+        unsigned t[5];
+        if (i0 + 4 <= capacity) {
+            const uint4 v = *reinterpret_cast<const uint4*>(tiles + i0);
+            t[0] = v.x;
+            t[1] = v.y;
+            t[2] = v.z;
+            t[3] = v.w;
+        } else {
 #pragma unroll
-        for (int j = 0; j < 4; j++) t[j] = i0 + j < P ? tiles[i0 + j] : 0u;
-    }
-    t[4] = i0 + 4 < P ? tiles[i0 + 4] : 0u;
-    if (i0 == 0) ranges[2 * t[0]] = 0u;
+            for (int j = 0; j < 4; j++) t[j] = i0 + j < P ? tiles[i0 + j] : 0u;
+        }
+        t[4] = i0 + 4 < P ? tiles[i0 + 4] : 0u;
+        if (i0 == 0) ranges[2 * t[0]] = 0u;
 #pragma unroll
-    for (int j = 0; j < 4; j++) {
-        const unsigned long long i = i0 + (unsigned long long)j;
-        if (i >= P) break;
-        const bool last = i + 1 == P;
-        if (last || t[j + 1] != t[j]) {
-            ranges[2 * t[j] + 1] = (unsigned)(i + 1);
-            if (!last) ranges[2 * t[j + 1]] = (unsigned)(i + 1);
+        for (int j = 0; j < 4; j++) {
+            const unsigned long long i = i0 + (unsigned long long)j;
+            if (i >= P) break;
+            const bool last = i + 1 == P;
+            if (last || t[j + 1] != t[j]) {
+                ranges[2 * t[j] + 1] = (unsigned)(i + 1);
+                if (!last) ranges[2 * t[j + 1]] = (unsigned)(i + 1);
+            }
         }
     }
 }
@@ -615,18 +621,26 @@ cudaError_t launch_tile_ranges(cudaStream_t st, unsigned long long capacity, con
     return cudaGetLastError();
 }
 
+// CTAs of 256 threads for the four-keys-per-thread range kernels: enough for the
+// capacity, at most 8 per SM (the kernels stride over the pairs present, which
+// a step finds on the device; a grid over the whole capacity spent its time
+// starting CTAs with nothing to do).
+static unsigned ranges_grid(unsigned long long capacity) {
+    const unsigned long long need = (capacity + 1023) / 1024, cap = 8ull * (unsigned long long)sm_count();
+    return (unsigned)(need < cap ? need : cap);
+}
+
 cudaError_t launch_tile_ranges_views(cudaStream_t st, unsigned long long capacity, const unsigned* tiles_sorted,
                                      const StepParams* views, unsigned* ranges, Control* ctrl) {
     if (capacity == 0) return cudaSuccess;
-    k_ranges_views4<<<(unsigned)((capacity + 1023) / 1024), 256, 0, st>>>(tiles_sorted, views, capacity, ranges,
-                                                                         ctrl);
+    k_ranges_views4<<<ranges_grid(capacity), 256, 0, st>>>(tiles_sorted, views, capacity, ranges, ctrl);
     return cudaGetLastError();
 }
 
 cudaError_t launch_tile_ranges32(cudaStream_t st, unsigned long long capacity, const unsigned* tiles_sorted,
                                  unsigned* ranges, Control* ctrl) {
     if (capacity == 0) return cudaSuccess;
-    k_ranges32<<<(unsigned)((capacity + 1023) / 1024), 256, 0, st>>>(tiles_sorted, capacity, ranges, ctrl);
+    k_ranges32<<<ranges_grid(capacity), 256, 0, st>>>(tiles_sorted, capacity, ranges, ctrl);
     return cudaGetLastError();
 }
 

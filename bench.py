@@ -592,6 +592,7 @@ def measure_batched(a, local: int) -> dict:
     g1 = graph_stats()
     loss_b = ctx.train_step_batch(cams, None, cfg, tc, it[0], gt_device_ptr=gt_dev.data_ptr())
     launches_b = ctx.stat(gs3d.STAT_KERNELS_LAST)
+    pairs_b = ctx.stat(gs3d.STAT_TOTAL_PAIRS)
 
     # the plain FP32 path, the same views one by one (one optimiser step per view), with the same
     # autotuner setting; every camera size keeps its own graphs, so the timed passes only replay
@@ -615,7 +616,8 @@ def measure_batched(a, local: int) -> dict:
     return {"workload": f"batched_64views_{gname}_gaussians_mixed_320x240_to_3840x2160", "views": len(cams),
             "mpix_per_step": round(pix / 1e6, 2), "steps": steps,
             "batched_bf16": {"ms_per_step": round(ms_b, 3), "mpix_per_s": round(pix / 1e6 / (ms_b * 1e-3), 1),
-                             "gpu_launches_per_step": launches_b, "loss_first": loss0, "loss_last": loss_b,
+                             "gpu_launches_per_step": launches_b, "tile_pairs_per_step": pairs_b,
+                             "loss_first": loss0, "loss_last": loss_b,
                              "raster_pixels_per_thread": ppt_b, "raster_staging_batch": batch_b,
                              "graph_replays_per_step": (g1[0] - g0[0]) / steps,
                              "graph_captures_in_timed_steps": g1[1] - g0[1]},
