@@ -189,3 +189,39 @@ def test_stochastic_rounding_moves_parameters_in_expectation(ctx):
               f"standard error {se:.1e}), unchanged {frac_zero:.3f}")
         assert frac_zero > 0.5, "most updates should be below half an ulp (the test would not test rounding)"
         assert abs(float(resid.mean())) < 6.0 * se + 0.005 * lr
+
+
+def test_non_finite_parameters_stay_non_finite(ctx):
+    """The BF16 optimiser updates two elements per 32-bit word and redoes a
+    chunk element-wise when a result is not finite (adding the rounding bits
+    would otherwise carry a NaN's mantissa into its sign: NaN -> -0).  Two
+    Gaussians behind the camera (no pairs, zero gradients) hold a NaN and an
+    infinite SH coefficient: after a step both stay as they were, and the other
+    coefficients of their 8-element chunks, with a zero update, keep their
+    values."""
+    ctx.set_option(gs3d.OPT_FORM, gs3d.FORM_BF16)
+    sc = S.random_scene(20_000, seed=36)
+    cam = S.look_at_camera((0.3, 0.2, -3.0), 320, 240)
+    cfg = S.render_config(True)
+    gt = np.zeros(320 * 240 * 3, np.float32)
+    bad = {101: np.nan, 202: np.inf}     # Gaussian -> value of its SH coefficient 9 (chunk 1)
+    for i, val in bad.items():
+        sc.positions[i] = (0.6, 0.4, -6.0)   # behind the camera at (0.3, 0.2, -3) looking at the origin
+        sc.sh.reshape(sc.positions.shape[0], -1)[i, 9] = val
+    try:
+        ctx.set_raw_params(sc)
+        before = ctx.get_raw_params(sc.copy())
+        loss = ctx.train_step(cam, gt, cfg, S.train_config(lr_pos=1e-30, lr_rest=1e-3), 0)
+        after = ctx.get_raw_params(sc.copy())
+    finally:
+        ctx.set_option(gs3d.OPT_FORM, gs3d.FORM_PLAIN_FP32)
+    assert np.isfinite(loss)
+    n = sc.positions.shape[0]
+    sh_b, sh_a = before.sh.reshape(n, -1), after.sh.reshape(n, -1)
+    assert np.isnan(sh_a[101, 9]) and sh_a[202, 9] == np.inf
+    for i in bad:
+        chunk = [k for k in range(8, 16) if k != 9]
+        assert np.array_equal(sh_a[i, chunk], sh_b[i, chunk]), i
+    mask = np.ones_like(sh_a, bool)
+    mask[101, 9] = mask[202, 9] = False
+    assert np.all(np.isfinite(sh_a[mask]))
